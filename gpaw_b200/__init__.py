@@ -1,0 +1,23 @@
+"""gpaw_b200: GPAW's real-space finite-difference hot path on B200.
+
+Drop-in classes with the reference's Python signatures:
+
+* ``FDOperator``, ``Laplace``, ``GUCLaplace``  (gpaw/fd_operators.py)
+* ``Transformer``                               (gpaw/transformers.py)
+* ``FDPoissonSolver``                           (gpaw/poisson.py)
+* ``Preconditioner``                            (gpaw/preconditioner.py)
+* ``GridDescriptor``                            (gpaw/old/grid_descriptor.py)
+
+and the C-object layer ``gpaw_b200.cgpaw`` (Operator, Transformer,
+fd_precond).  All arrays are torch CUDA tensors; the arithmetic runs in the
+sm_100a kernels of ``libgpaw_b200.so`` (C ABI: include/gpaw_b200.h).
+"""
+from .grid_descriptor import BadGridError, GridDescriptor
+from .fd_operators import FDOperator, GUCLaplace, Laplace
+from .transformers import Transformer
+from .poisson import FDPoissonSolver, PoissonConvergenceError
+from .preconditioner import Preconditioner
+
+__all__ = ['GridDescriptor', 'BadGridError', 'FDOperator', 'GUCLaplace',
+           'Laplace', 'Transformer', 'FDPoissonSolver',
+           'PoissonConvergenceError', 'Preconditioner']

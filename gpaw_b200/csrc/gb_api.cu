@@ -1,0 +1,645 @@
+// C ABI of gpaw_b200 (declared in include/gpaw_b200.h): object lifetimes,
+// argument checks that mirror the reference's, and the host-side sequencing
+// of the kernels in gb_fd.cu and gb_transform.cu.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/gpaw_b200.h"
+#include "gb_internal.cuh"
+
+using namespace gb;
+
+// ------------------------------------------------------------------- errors
+static thread_local std::string g_err;
+
+static int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define GB_CUDA_TRY(expr)                                                             \
+    do {                                                                              \
+        cudaError_t e_ = (expr);                                                      \
+        if (e_ != cudaSuccess)                                                        \
+            return fail(GB_ECUDA, "%s: %s (%s:%d)", #expr, cudaGetErrorString(e_),     \
+                        __FILE__, __LINE__);                                          \
+    } while (0)
+
+#define GB_LAUNCH_CHECK()                                                             \
+    do {                                                                              \
+        cudaError_t e_ = cudaGetLastError();                                          \
+        if (e_ != cudaSuccess)                                                        \
+            return fail(GB_ECUDA, "kernel launch: %s (%s:%d)", cudaGetErrorString(e_), \
+                        __FILE__, __LINE__);                                          \
+    } while (0)
+
+extern "C" int gb_version(void) { return 100; }
+extern "C" const char* gb_last_error(void) { return g_err.c_str(); }
+
+// ------------------------------------------------------------------ scratch
+// Device buffer owned by an object; grows on demand (never inside a
+// caller's stream capture if gb_*_reserve was called first).
+struct Scratch {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    ~Scratch() {
+        if (ptr) cudaFree(ptr);
+    }
+    int ensure(size_t want) {
+        if (want <= bytes) return 0;
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&ptr, want);
+        if (e != cudaSuccess) return fail(GB_ECUDA, "cudaMalloc(%zu): %s", want, cudaGetErrorString(e));
+        bytes = want;
+        return 0;
+    }
+};
+
+static size_t elem_size(int dtype) { return dtype == GB_C128 ? 16 : 8; }
+
+static int read_phases(int dtype, const double* phases, Phases& P) {
+    memset(&P, 0, sizeof P);
+    if (dtype != GB_C128 || phases == nullptr) return 0;
+    for (int c = 0; c < 3; c++)
+        for (int d = 0; d < 2; d++) {
+            P.ph[c][d].x = phases[(c * 2 + d) * 2];
+            P.ph[c][d].y = phases[(c * 2 + d) * 2 + 1];
+        }
+    P.use = 1;
+    return 0;
+}
+
+static bool ranges_overlap(const void* a, const void* b, size_t bytes) {
+    const char* x = (const char*)a;
+    const char* y = (const char*)b;
+    return x < y + bytes && y < x + bytes;
+}
+
+// ----------------------------------------------------------------- Operator
+struct gb_operator {
+    Stencil st;
+    GridBC g;
+    int real;
+    double diag;
+    Scratch scratch;   // aliasing stage / Jacobi ping-pong / GS snapshot
+    long long ng() const { return (long long)g.n[0] * g.n[1] * g.n[2]; }
+};
+
+extern "C" int gb_operator_new(const double* coefs, const int64_t* offsets, int ncoefs,
+                               const int64_t size[3], int range, const int64_t neighbors[6],
+                               int real, int cfd, gb_operator** out) {
+    if (!out || !coefs || !offsets || !size || !neighbors)
+        return fail(GB_EINVAL, "Operator: NULL argument");
+    *out = nullptr;
+    if (ncoefs < 1 || ncoefs > GB_MAX_COEFS)
+        return fail(GB_EINVAL, "Operator: %d coefficients (1..%d supported)", ncoefs, GB_MAX_COEFS);
+    if (range < 0) return fail(GB_EINVAL, "Operator: negative range");
+    for (int c = 0; c < 3; c++)
+        if (size[c] < 1 || size[c] > (1 << 20)) return fail(GB_EINVAL, "Operator: bad size");
+    if ((double)size[0] * size[1] * size[2] >= 2147483647.0)
+        return fail(GB_EINVAL, "Operator: grid has 2^31 points or more");
+    gb_operator* op = new gb_operator();
+    memset(&op->st, 0, sizeof op->st);
+    op->st.ncoefs = ncoefs;
+    op->st.range = range;
+    op->st.cfd = cfd ? 1 : 0;
+    op->real = real ? 1 : 0;
+    for (int c = 0; c < 3; c++) {
+        op->g.n[c] = (int)size[c];
+        const int64_t lo = neighbors[2 * c], hi = neighbors[2 * c + 1];
+        if (lo > 0 || hi > 0) {
+            delete op;
+            return fail(GB_EINVAL, "Operator: neighbour ranks > 0 need domain decomposition");
+        }
+        // both sides periodic or both zero on a single domain
+        op->g.periodic[c] = (lo == 0 && hi == 0) ? 1 : 0;
+        if ((lo == 0) != (hi == 0)) {
+            delete op;
+            return fail(GB_EINVAL, "Operator: mixed periodic/zero on one axis");
+        }
+        if (op->g.periodic[c] && size[c] < range) {
+            delete op;
+            return fail(GB_EINVAL, "Stencil longer than domain");
+        }
+    }
+    // Split each flat padded offset into (o0, o1, o2) with |o_c| <= range.
+    const long long M1 = size[1] + 2 * range, M2 = size[2] + 2 * range;
+    op->diag = 0.0;
+    for (int p = 0; p < ncoefs; p++) {
+        long long f = offsets[p];
+        long long o2 = ((f % M2) + M2) % M2;
+        if (o2 > M2 / 2) o2 -= M2;
+        long long rest = (f - o2) / M2;
+        long long o1 = ((rest % M1) + M1) % M1;
+        if (o1 > M1 / 2) o1 -= M1;
+        long long o0 = (rest - o1) / M1;
+        if (llabs(o0) > range || llabs(o1) > range || llabs(o2) > range ||
+            (o0 * M1 + o1) * M2 + o2 != f) {
+            delete op;
+            return fail(GB_EINVAL, "Operator: offset %lld does not fit range %d", (long long)f, range);
+        }
+        op->st.coef[p] = coefs[p];
+        op->st.off[p][0] = (int)o0;
+        op->st.off[p][1] = (int)o1;
+        op->st.off[p][2] = (int)o2;
+        op->st.flat[p] = (o0 * size[1] + o1) * size[2] + o2;
+        if (f == 0) op->diag = coefs[p];
+    }
+    *out = op;
+    return 0;
+}
+
+extern "C" void gb_operator_free(gb_operator* op) { delete op; }
+
+extern "C" double gb_operator_get_diagonal_element(const gb_operator* op) {
+    return op ? op->diag : 0.0;
+}
+
+extern "C" int gb_operator_reserve(gb_operator* op, int64_t nin, int dtype) {
+    if (!op) return fail(GB_EINVAL, "NULL operator");
+    return op->scratch.ensure((size_t)(nin < 1 ? 1 : nin) * op->ng() * elem_size(dtype));
+}
+
+static int check_dtype(const gb_operator* op, int dtype) {
+    if (dtype != GB_F64 && dtype != GB_C128) return fail(GB_EINVAL, "unsupported dtype %d", dtype);
+    if ((dtype == GB_F64) != (op->real != 0))
+        return fail(GB_EINVAL, "dtype does not match the operator (real=%d)", op->real);
+    return 0;
+}
+
+extern "C" int gb_operator_apply(gb_operator* op, const void* in, void* out, int64_t nin,
+                                 int dtype, const double* phases, void* stream) {
+    if (!op || !in || !out) return fail(GB_EINVAL, "apply: NULL argument");
+    if (int e = check_dtype(op, dtype)) return e;
+    if (nin < 0) return fail(GB_EINVAL, "apply: negative batch");
+    if (nin == 0) return 0;
+    cudaStream_t st = (cudaStream_t)stream;
+    Phases P;
+    read_phases(dtype, phases, P);
+    const size_t bytes = (size_t)nin * op->ng() * elem_size(dtype);
+    if (ranges_overlap(in, out, bytes)) {
+        if (int e = op->scratch.ensure(bytes)) return e;
+        GB_CUDA_TRY(cudaMemcpyAsync(op->scratch.ptr, in, bytes, cudaMemcpyDeviceToDevice, st));
+        in = op->scratch.ptr;
+    }
+    if (dtype == GB_F64)
+        launch_fd<double>(in, out, (int)nin, op->g, P, op->st, st);
+    else
+        launch_fd<double2>(in, out, (int)nin, op->g, P, op->st, st);
+    GB_LAUNCH_CHECK();
+    return 0;
+}
+
+extern "C" int gb_operator_residual(gb_operator* op, const void* phi, const void* rho, void* r,
+                                    int64_t nin, int dtype, const double* phases, double scale,
+                                    double* norm2, void* stream) {
+    if (!op || !phi || !rho) return fail(GB_EINVAL, "residual: NULL argument");
+    if (int e = check_dtype(op, dtype)) return e;
+    if (nin <= 0) return 0;
+    cudaStream_t st = (cudaStream_t)stream;
+    Phases P;
+    read_phases(dtype, phases, P);
+    const size_t bytes = (size_t)nin * op->ng() * elem_size(dtype);
+    if (r && (ranges_overlap(phi, r, bytes)))
+        return fail(GB_EINVAL, "residual: r must not overlap phi");
+    double* partial = nullptr;
+    const int nblk = residual_blocks(op->g);
+    if (norm2) {
+        if (int e = op->scratch.ensure((size_t)nin * nblk * sizeof(double))) return e;
+        partial = (double*)op->scratch.ptr;
+    }
+    if (dtype == GB_F64)
+        launch_residual<double>(phi, rho, r, (int)nin, op->g, P, op->st, partial, st);
+    else
+        launch_residual<double2>(phi, rho, r, (int)nin, op->g, P, op->st, partial, st);
+    GB_LAUNCH_CHECK();
+    if (norm2) {
+        launch_reduce_partials(partial, nblk, (int)nin, scale, norm2, st);
+        GB_LAUNCH_CHECK();
+    }
+    return 0;
+}
+
+static int relax_impl(gb_operator* op, int method, double* f, const double* s, int nrelax,
+                      double w, cudaStream_t st) {
+    const size_t bytes = (size_t)op->ng() * sizeof(double);
+    if (nrelax <= 0) return 0;
+    if (int e = op->scratch.ensure(bytes)) return e;
+    double* X = (double*)op->scratch.ptr;
+    if (method == 1) {
+        // Gauss-Seidel by wavefronts; wrapped reads see the sweep's start.
+        const int r = op->st.range;
+        int wa = 1, wb = 1;
+        if (!op->st.cfd) {
+            wb = 2 * r + 1;
+            wa = (wb + 1) * r + 1;
+        }
+        const GridBC& g = op->g;
+        const int nt = wa * (g.n[0] - 1) + wb * (g.n[1] - 1) + g.n[2];
+        const bool periodic = g.periodic[0] || g.periodic[1] || g.periodic[2];
+        const double inv0 = 1.0 / op->st.coef[0];
+        for (int it = 0; it < nrelax; it++) {
+            if (periodic) GB_CUDA_TRY(cudaMemcpyAsync(X, f, bytes, cudaMemcpyDeviceToDevice, st));
+            for (int t = 0; t < nt; t++)
+                launch_gs_wave(f, periodic ? X : f, s, g, op->st, t, wa, wb, inv0, st);
+            GB_LAUNCH_CHECK();
+        }
+        return 0;
+    }
+    // weighted Jacobi: ping-pong so that the last sweep lands in f
+    const double* src = f;
+    if (nrelax % 2 == 1) {
+        GB_CUDA_TRY(cudaMemcpyAsync(X, f, bytes, cudaMemcpyDeviceToDevice, st));
+        src = X;
+    }
+    for (int it = 0; it < nrelax; it++) {
+        double* dst = (src == f) ? X : f;
+        launch_jacobi(src, dst, s, op->g, op->st, w, st);
+        src = dst;
+    }
+    GB_LAUNCH_CHECK();
+    return 0;
+}
+
+extern "C" int gb_operator_relax(gb_operator* op, int method, double* f, const double* s,
+                                 int nrelax, double w, void* stream) {
+    if (!op || !f || !s) return fail(GB_EINVAL, "relax: NULL argument");
+    if (!op->real) return fail(GB_EINVAL, "relax: float64 operators only");
+    if (method != 1 && method != 2) return fail(GB_EINVAL, "relax: method must be 1 or 2");
+    return relax_impl(op, method, f, s, nrelax, w, (cudaStream_t)stream);
+}
+
+// -------------------------------------------------------------- Transformer
+struct gb_transformer {
+    XferGeom G;
+    int k;
+    int interpolate;
+    int real;
+    long long ngin, ngout;
+};
+
+static void lagrange_weights(int k, double* w) {
+    // Weights of the order-k Lagrange interpolant at the mid-point, for the
+    // node pairs at distance 1/2, 3/2, ... (exact binary fractions, equal to
+    // the constants of c/bmgs/restrict.cpp:37-57).
+    for (int j = k / 2; j < k; j++) {
+        double num = 1.0, den = 1.0;
+        const double xj = (2.0 * j - k + 1) / 2.0;
+        for (int m = 0; m < k; m++) {
+            if (m == j) continue;
+            const double xm = (2.0 * m - k + 1) / 2.0;
+            num *= (0.0 - xm);
+            den *= (xj - xm);
+        }
+        w[j - k / 2] = num / den;
+    }
+}
+
+extern "C" int gb_transformer_new(const int64_t size_in[3], const int64_t size_out[3], int k,
+                                  const int64_t pads[6], const int64_t npads[6],
+                                  const int64_t skip[6], const int64_t neighbors[6], int real,
+                                  int interpolate, gb_transformer** out) {
+    if (!out || !size_in || !size_out || !pads || !npads || !skip || !neighbors)
+        return fail(GB_EINVAL, "Transformer: NULL argument");
+    *out = nullptr;
+    if (k != 2 && k != 4 && k != 6 && k != 8)
+        return fail(GB_EINVAL, "Transformer: k must be 2, 4, 6 or 8");
+    gb_transformer* t = new gb_transformer();
+    memset(&t->G, 0, sizeof t->G);
+    t->k = k;
+    t->interpolate = interpolate ? 1 : 0;
+    t->real = real ? 1 : 0;
+    XferGeom& G = t->G;
+    const int e = interpolate ? k - 1 : 2 * k - 3;
+    for (int c = 0; c < 3; c++) {
+        const int64_t lo = neighbors[2 * c], hi = neighbors[2 * c + 1];
+        if (lo > 0 || hi > 0 || (lo == 0) != (hi == 0)) {
+            delete t;
+            return fail(GB_EINVAL, "Transformer: single-domain neighbours only");
+        }
+        G.g.n[c] = (int)size_in[c];
+        G.g.periodic[c] = (lo == 0) ? 1 : 0;
+        if (pads[2 * c] < 0 || pads[2 * c + 1] < 0) {
+            delete t;
+            return fail(GB_EINVAL, "Transformer: negative padding");
+        }
+        if (G.g.periodic[c] && (npads[2 * c] != pads[2 * c + 1] || npads[2 * c + 1] != pads[2 * c] ||
+                                pads[2 * c] > size_in[c] || pads[2 * c + 1] > size_in[c])) {
+            delete t;
+            return fail(GB_EINVAL, "Transformer: periodic padding wider than the grid");
+        }
+        G.plo[c] = (int)pads[2 * c];
+        G.s[c] = (int)(size_in[c] + pads[2 * c] + pads[2 * c + 1]);
+        G.nout[c] = (int)size_out[c];
+        G.skip0[c] = interpolate ? (int)skip[2 * c] : 0;
+        G.skip1[c] = interpolate ? (int)skip[2 * c + 1] : 0;
+        const int expect = interpolate ? 2 * (G.s[c] - e + G.skip1[c]) - G.skip0[c] - G.skip1[c]
+                                       : (G.s[c] - e) / 2;
+        if (expect != size_out[c]) {
+            delete t;
+            return fail(GB_EINVAL, "Transformer: output size %lld does not match input geometry (%d)",
+                        (long long)size_out[c], expect);
+        }
+    }
+    lagrange_weights(k, G.w);
+    t->ngin = (long long)size_in[0] * size_in[1] * size_in[2];
+    t->ngout = (long long)size_out[0] * size_out[1] * size_out[2];
+    *out = t;
+    return 0;
+}
+
+extern "C" void gb_transformer_free(gb_transformer* t) { delete t; }
+
+static int transform_impl(gb_transformer* t, const void* in, void* out, void* out2, int64_t nin,
+                          int dtype, const Phases& P, int neg_in, int accumulate, double scale2,
+                          cudaStream_t st) {
+    XferGeom G = t->G;
+    G.neg_in = neg_in;
+    G.accumulate = accumulate;
+    G.scale2 = scale2;
+    int rc;
+    if (dtype == GB_F64)
+        rc = launch_transform<double>(t->k, t->interpolate, in, out, out2, (int)nin, G, P, st);
+    else
+        rc = launch_transform<double2>(t->k, t->interpolate, in, out, out2, (int)nin, G, P, st);
+    if (rc) return fail(GB_EINVAL, "transformer: unsupported order");
+    GB_LAUNCH_CHECK();
+    return 0;
+}
+
+extern "C" int gb_transformer_apply(gb_transformer* t, const void* in, void* out, int64_t nin,
+                                    int dtype, const double* phases, void* stream) {
+    if (!t || !in || !out) return fail(GB_EINVAL, "transformer apply: NULL argument");
+    if (dtype != GB_F64 && dtype != GB_C128) return fail(GB_EINVAL, "unsupported dtype");
+    if ((dtype == GB_F64) != (t->real != 0))
+        return fail(GB_EINVAL, "dtype does not match the transformer (real=%d)", t->real);
+    if (nin <= 0) return 0;
+    const size_t es = elem_size(dtype);
+    const char* ib = (const char*)in;
+    const char* ob = (const char*)out;
+    if (ib < ob + nin * t->ngout * es && ob < ib + nin * t->ngin * es)
+        return fail(GB_EINVAL, "transformer apply: input and output overlap");
+    Phases P;
+    read_phases(dtype, phases, P);
+    return transform_impl(t, in, out, nullptr, nin, dtype, P, 0, 0, 0.0, (cudaStream_t)stream);
+}
+
+// --------------------------------------------------------------- fd_precond
+extern "C" int gb_fd_precond(gb_transformer* rest0, gb_transformer* rest1, gb_transformer* intp1,
+                             gb_transformer* intp2, gb_operator* kin0, gb_operator* kin1,
+                             gb_operator* kin2, void* d0, void* q0, void* r1, void* d1, void* q1,
+                             void* r2, void* d2, void* q2, const void* residuals,
+                             const void* nresiduals, int64_t nin, int dtype, double step,
+                             const double* phases, void* stream) {
+    if (!rest0 || !rest1 || !intp1 || !intp2 || !kin0 || !kin1 || !kin2)
+        return fail(GB_EINVAL, "fd_precond: NULL object");
+    if (!d0 || !q0 || !r1 || !d1 || !q1 || !r2 || !d2 || !q2 || !residuals)
+        return fail(GB_EINVAL, "fd_precond: NULL array");
+    if (int e = check_dtype(kin0, dtype)) return e;
+    if (int e = check_dtype(kin1, dtype)) return e;
+    if (int e = check_dtype(kin2, dtype)) return e;
+    if (rest0->ngin != kin0->ng() || rest0->ngout != kin1->ng() || rest1->ngin != kin1->ng() ||
+        rest1->ngout != kin2->ng() || intp2->ngin != kin2->ng() || intp2->ngout != kin1->ng() ||
+        intp1->ngin != kin1->ng() || intp1->ngout != kin0->ng() || rest0->interpolate ||
+        rest1->interpolate || !intp1->interpolate || !intp2->interpolate)
+        return fail(GB_EINVAL, "fd_precond: level sizes do not match");
+    if (nin <= 0) return 0;
+    cudaStream_t st = (cudaStream_t)stream;
+    Phases P;
+    read_phases(dtype, phases, P);
+    const int n = (int)nin;
+    const double s4 = 4 * step, s16 = 16 * step;
+    auto step_launch = [&](gb_operator* op, const void* d, const void* r, void* o, double sc,
+                           int negate) {
+        if (dtype == GB_F64)
+            launch_precond_step<double>(d, r, o, n, op->g, P, op->st, sc, negate, st);
+        else
+            launch_precond_step<double2>(d, r, o, n, op->g, P, op->st, sc, negate, st);
+    };
+    int rc;
+    // r1 = restrict(-R); d1 = 4 s r1
+    if (nresiduals)
+        rc = transform_impl(rest0, nresiduals, r1, d1, nin, dtype, P, 0, 0, s4, st);
+    else
+        rc = transform_impl(rest0, residuals, r1, d1, nin, dtype, P, 1, 0, s4, st);
+    if (rc) return rc;
+    // q1 = K1 d1 - r1; r2 = restrict(q1); d2 = 16 s r2
+    if (dtype == GB_F64)
+        launch_residual<double>(d1, r1, q1, n, kin1->g, P, kin1->st, nullptr, st);
+    else
+        launch_residual<double2>(d1, r1, q1, n, kin1->g, P, kin1->st, nullptr, st);
+    GB_LAUNCH_CHECK();
+    if ((rc = transform_impl(rest1, q1, r2, d2, nin, dtype, P, 0, 0, s16, st))) return rc;
+    // d2' = d2 - 16 s (K2 d2 - r2)   (into q2)
+    step_launch(kin2, d2, r2, q2, s16, 0);
+    GB_LAUNCH_CHECK();
+    // d1 -= interpolate(d2')
+    if ((rc = transform_impl(intp2, q2, d1, nullptr, nin, dtype, P, 0, 1, 0.0, st))) return rc;
+    // d1' = d1 - 4 s (K1 d1 - r1)   (into q1)
+    step_launch(kin1, d1, r1, q1, s4, 0);
+    GB_LAUNCH_CHECK();
+    // q0 = interpolate(-d1')
+    if ((rc = transform_impl(intp1, q1, q0, nullptr, nin, dtype, P, 1, 0, 0.0, st))) return rc;
+    // d0 = -(q0 - s (K0 q0 - R))
+    step_launch(kin0, q0, residuals, d0, step, 1);
+    GB_LAUNCH_CHECK();
+    return 0;
+}
+
+// --------------------------------------------------------------- FD Poisson
+struct gb_poisson {
+    int L;  // coarsest level index
+    std::vector<gb_operator*> ops;
+    std::vector<gb_transformer*> rst, itp;
+    std::vector<int> pre, post;
+    std::vector<double> w;
+    int method;
+    double dv;
+    std::vector<double*> phi, rho, res;  // per level (phi[0], rho[0] from the caller)
+    double* partial = nullptr;
+    double* err_dev = nullptr;
+    double* err_host = nullptr;
+    double* mean_dev = nullptr;
+    ~gb_poisson() {
+        for (size_t l = 1; l < phi.size(); l++) cudaFree(phi[l]);
+        for (size_t l = 1; l < rho.size(); l++) cudaFree(rho[l]);
+        for (double* p : res) cudaFree(p);
+        cudaFree(partial);
+        cudaFree(err_dev);
+        cudaFree(mean_dev);
+        if (err_host) cudaFreeHost(err_host);
+    }
+};
+
+extern "C" int gb_poisson_new(int nlevels, gb_operator* const* operators,
+                              gb_transformer* const* restrictors,
+                              gb_transformer* const* interpolators, const int* presmooths,
+                              const int* postsmooths, const double* weights, int relax_method,
+                              double dv, gb_poisson** out) {
+    if (!out || !operators || nlevels < 1 || !presmooths || !postsmooths || !weights)
+        return fail(GB_EINVAL, "Poisson: bad arguments");
+    if (nlevels > 1 && (!restrictors || !interpolators))
+        return fail(GB_EINVAL, "Poisson: missing transformers");
+    if (relax_method != 1 && relax_method != 2)
+        return fail(GB_EINVAL, "Poisson: relax method must be 1 (GS) or 2 (J)");
+    *out = nullptr;
+    gb_poisson* p = new gb_poisson();
+    p->L = nlevels - 1;
+    p->method = relax_method;
+    p->dv = dv;
+    for (int l = 0; l < nlevels; l++) {
+        if (!operators[l] || !operators[l]->real) {
+            delete p;
+            return fail(GB_EINVAL, "Poisson: level %d operator missing or complex", l);
+        }
+        p->ops.push_back(operators[l]);
+        p->pre.push_back(presmooths[l]);
+        p->post.push_back(postsmooths[l]);
+        p->w.push_back(weights[l]);
+    }
+    for (int l = 0; l < p->L; l++) {
+        gb_transformer* r = restrictors[l];
+        gb_transformer* i = interpolators[l];
+        if (!r || !i || r->interpolate || !i->interpolate || !r->real || !i->real ||
+            r->ngin != p->ops[l]->ng() || r->ngout != p->ops[l + 1]->ng() ||
+            i->ngin != p->ops[l + 1]->ng() || i->ngout != p->ops[l]->ng()) {
+            delete p;
+            return fail(GB_EINVAL, "Poisson: transformer %d does not match the levels", l);
+        }
+        p->rst.push_back(r);
+        p->itp.push_back(i);
+    }
+    p->phi.assign(nlevels, nullptr);
+    p->rho.assign(nlevels, nullptr);
+    p->res.assign(nlevels, nullptr);
+    for (int l = 0; l < nlevels; l++) {
+        const size_t bytes = (size_t)p->ops[l]->ng() * sizeof(double);
+        cudaError_t e = cudaMalloc(&p->res[l], bytes);
+        if (e == cudaSuccess && l > 0) e = cudaMalloc(&p->phi[l], bytes);
+        if (e == cudaSuccess && l > 0) e = cudaMalloc(&p->rho[l], bytes);
+        if (e != cudaSuccess) {
+            delete p;
+            return fail(GB_ECUDA, "Poisson: cudaMalloc: %s", cudaGetErrorString(e));
+        }
+        if (int rc = gb_operator_reserve(p->ops[l], 1, GB_F64)) {
+            delete p;
+            return rc;
+        }
+    }
+    const int nblk = residual_blocks(p->ops[0]->g);
+    cudaError_t e = cudaMalloc(&p->partial, (size_t)nblk * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&p->err_dev, sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&p->mean_dev, sizeof(double));
+    if (e == cudaSuccess) e = cudaMallocHost(&p->err_host, sizeof(double));
+    if (e != cudaSuccess) {
+        delete p;
+        return fail(GB_ECUDA, "Poisson: allocation: %s", cudaGetErrorString(e));
+    }
+    *out = p;
+    return 0;
+}
+
+extern "C" void gb_poisson_free(gb_poisson* p) { delete p; }
+
+// iterate2 (gpaw/poisson.py:500-537), recursive over levels.
+static int vcycle(gb_poisson* p, int l, cudaStream_t st) {
+    gb_operator* op = p->ops[l];
+    Phases P;
+    memset(&P, 0, sizeof P);
+    if (l < p->L) {
+        if (int rc = relax_impl(op, p->method, p->phi[l], p->rho[l], p->pre[l], p->w[l], st))
+            return rc;
+        launch_residual<double>(p->phi[l], p->rho[l], p->res[l], 1, op->g, P, op->st, nullptr, st);
+        GB_LAUNCH_CHECK();
+        if (int rc = transform_impl(p->rst[l], p->res[l], p->rho[l + 1], nullptr, 1, GB_F64, P, 0,
+                                    0, 0.0, st))
+            return rc;
+        GB_CUDA_TRY(cudaMemsetAsync(p->phi[l + 1], 0, (size_t)p->ops[l + 1]->ng() * sizeof(double),
+                                    st));
+        if (int rc = vcycle(p, l + 1, st)) return rc;
+        // phi_l -= interpolate(phi_{l+1})
+        if (int rc = transform_impl(p->itp[l], p->phi[l + 1], p->phi[l], nullptr, 1, GB_F64, P, 0,
+                                    1, 0.0, st))
+            return rc;
+    }
+    if (int rc = relax_impl(op, p->method, p->phi[l], p->rho[l], p->post[l], p->w[l], st))
+        return rc;
+    if (l == 0) {
+        const int nblk = residual_blocks(op->g);
+        launch_residual<double>(p->phi[0], p->rho[0], p->res[0], 1, op->g, P, op->st, p->partial,
+                                st);
+        GB_LAUNCH_CHECK();
+        launch_reduce_partials(p->partial, nblk, 1, p->dv, p->err_dev, st);
+        GB_LAUNCH_CHECK();
+    }
+    return 0;
+}
+
+extern "C" int gb_poisson_iterate(gb_poisson* p, double* phi, const double* rho, double* error,
+                                  void* stream) {
+    if (!p || !phi || !rho) return fail(GB_EINVAL, "Poisson iterate: NULL argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    p->phi[0] = phi;
+    p->rho[0] = (double*)rho;  // never written
+    if (int rc = vcycle(p, 0, st)) return rc;
+    GB_CUDA_TRY(cudaMemcpyAsync(p->err_host, p->err_dev, sizeof(double), cudaMemcpyDeviceToHost, st));
+    GB_CUDA_TRY(cudaStreamSynchronize(st));
+    if (error) *error = *p->err_host;
+    return 0;
+}
+
+__global__ void k_sub_scalar(double* a, long long n, const double* v, double count) {
+    // phi_ave = sum(phi) / prod(N_c); phi -= phi_ave  (gpaw/poisson.py:492-496)
+    const double m = v[0] / count;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        a[i] = a[i] - m;
+}
+
+__global__ void k_block_sums(const double* a, long long n, double* partial) {
+    double v = 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        v += a[i];
+    v = block_sum(v);
+    if (threadIdx.x == 0) partial[blockIdx.x] = v;
+}
+
+extern "C" int gb_poisson_solve_neutral(gb_poisson* p, double* phi, const double* rho, double eps,
+                                        int maxiter, int* niter, double* error, void* stream) {
+    if (!p || !phi || !rho) return fail(GB_EINVAL, "Poisson solve: NULL argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    int it = 1;
+    double err = 0.0;
+    // while self.iterate2(self.step) > eps and niter < maxiter: niter += 1
+    while (true) {
+        if (int rc = gb_poisson_iterate(p, phi, rho, &err, stream)) return rc;
+        if (!(err > eps && it < maxiter)) break;
+        it++;
+    }
+    if (niter) *niter = it;
+    if (error) *error = err;
+    if (it == maxiter)
+        return fail(GB_ENOCONV, "Poisson solver did not converge in %d iterations!", maxiter);
+    const GridBC& g = p->ops[0]->g;
+    if (g.periodic[0] && g.periodic[1] && g.periodic[2]) {
+        const long long n = p->ops[0]->ng();
+        const int nb = (int)std::min<long long>(1024, (n + 255) / 256);
+        k_block_sums<<<nb, 256, 0, st>>>(phi, n, p->partial);
+        launch_reduce_partials(p->partial, nb, 1, 1.0, p->mean_dev, st);
+        k_sub_scalar<<<nb, 256, 0, st>>>(phi, n, p->mean_dev, (double)n);
+        GB_LAUNCH_CHECK();
+    }
+    return 0;
+}

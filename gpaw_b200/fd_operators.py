@@ -1,0 +1,152 @@
+"""Finite-difference operators (drop-in for gpaw/fd_operators.py).
+
+``FDOperator``, ``Laplace`` and ``GUCLaplace`` keep the reference's
+signatures (gpaw/fd_operators.py:43-238); arrays are torch CUDA tensors and
+the work runs in the sm_100a kernels behind the C ABI.  There is no CPU
+path: a non-CUDA tensor raises TypeError.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import cgpaw
+
+# Expansion coefficients of the finite-difference Laplacian,
+# J. R. Chelikowsky et al., Phys. Rev. B 50, 11355 (1994)
+# (table as in gpaw/fd_operators.py:27-34).
+laplace = [[0],
+           [-2, 1],
+           [-5 / 2, 4 / 3, -1 / 12],
+           [-49 / 18, 3 / 2, -3 / 20, 1 / 90],
+           [-205 / 72, 8 / 5, -1 / 5, 8 / 315, -1 / 560],
+           [-5269 / 1800, 5 / 3, -5 / 21, 5 / 126, -5 / 1008, 1 / 3150],
+           [-5369 / 1800, 12 / 7, -15 / 56, 10 / 189, -1 / 112, 2 / 1925,
+            -1 / 16632]]
+
+
+class FDOperator:
+    """Stencil operator ``out[g] = sum_p coef_p in[g + offset_p]`` with the
+    grid's boundary conditions (gpaw/fd_operators.py:43-147)."""
+
+    def __init__(self, coef_p, offset_pc, gd, dtype=float, description=None,
+                 xp=None):
+        offset_pc = np.asarray(offset_pc, int)
+        # central finite difference: every offset along one axis
+        cfd = True
+        for offset_c in offset_pc:
+            if sum(int(o != 0) for o in offset_c) >= 2:
+                cfd = False
+        mp = int(np.abs(offset_pc).max())
+        assert (mp <= gd.n_c).all(), 'Stencil longer than domain'
+        n_c = gd.n_c
+        M_c = n_c + 2 * mp
+        stride_c = np.array([M_c[1] * M_c[2], M_c[2], 1])
+        offset_p = np.ascontiguousarray(np.dot(offset_pc, stride_c))
+        coef_p = np.ascontiguousarray(coef_p, float)
+        assert coef_p.ndim == 1
+        assert coef_p.shape == offset_p.shape
+        assert dtype in [float, complex]
+        self.dtype = dtype
+        self.shape = tuple(int(x) for x in n_c)
+        self.mp = mp
+        self.gd = gd
+        self.npoints = len(coef_p)
+        self.coef_p = coef_p
+        self.offset_p = offset_p
+        self.offset_pc = offset_pc
+        self.cfd = cfd
+        self.xp = xp
+        self.operator = cgpaw.Operator(coef_p, offset_p, n_c, mp,
+                                       gd.neighbor_cd, dtype == float, None,
+                                       cfd)
+        if description is None:
+            description = '%d point finite-difference stencil' % self.npoints
+        self.description = description
+
+    def __str__(self):
+        return '<' + self.description + '>'
+
+    def __call__(self, in_xR, out_xR=None, phase_cd=None):
+        """Tensor interface: returns ``out_xR`` (allocated if None)."""
+        if out_xR is None:
+            out_xR = in_xR.new_empty(in_xR.shape)
+        self.apply(in_xR, out_xR, phase_cd)
+        return out_xR
+
+    def apply(self, in_xg, out_xg, phase_cd=None):
+        """gpaw/fd_operators.py:120-130; ``in_xg is out_xg`` is allowed."""
+        self.operator.apply(in_xg, out_xg, phase_cd)
+
+    def relax(self, relax_method, f_g, s_g, n, w=None):
+        """gpaw/fd_operators.py:132-141: 1 = Gauss-Seidel, 2 = weighted
+        Jacobi (float64 only)."""
+        self.operator.relax(relax_method, f_g, s_g, n,
+                            1.0 if w is None else w)
+
+    def residual(self, phi, rho, r=None, phase_cd=None, scale=None,
+                 norm2=None):
+        """r = L(phi) - rho in one pass (+ optional scaled |r|^2 per grid)."""
+        self.operator.residual(phi, rho, r, phase_cd, scale, norm2)
+
+    def get_diagonal_element(self):
+        return self.operator.get_diagonal_element()
+
+    def get_async_sizes(self):
+        return self.operator.get_async_sizes()
+
+
+def laplace_stencil(gd, scale=1.0, n=1):
+    """Coefficients and offsets of the general-cell Laplacian
+    (gpaw/fd_operators.py:184-238): pick the 3..6 shortest lattice
+    directions whose second differences reproduce x^2, y^2, z^2 and no
+    cross terms (least squares), then lay Chelikowsky's 1-D coefficients
+    along each."""
+    M_ic = np.indices((3, 3, 3)).reshape((3, -3)).T[-13:] - 1
+    u_cv = gd.h_cv / (gd.h_cv**2).sum(1)[:, np.newaxis]**0.5
+    u2_i = (np.dot(M_ic, u_cv)**2).sum(1)
+    i_d = u2_i.argsort()
+    m_mv = np.array([(2, 0, 0), (0, 2, 0), (0, 0, 2),
+                     (0, 1, 1), (1, 0, 1), (1, 1, 0)])
+    for D in range(3, 7):
+        h_dv = np.dot(M_ic[i_d[:D]], gd.h_cv)
+        A_md = (h_dv**m_mv[:, np.newaxis, :]).prod(2)
+        a_d, residual, rank, s = np.linalg.lstsq(A_md, [1, 1, 1, 0, 0, 0],
+                                                 rcond=-1)
+        if residual.sum() < 1e-14:
+            if rank != D:
+                raise ValueError(
+                    'You have a weird unit cell!  '
+                    'Try to use the maximally reduced Niggli cell.')
+            break
+    a_d *= scale
+    offsets = [(0, 0, 0)]
+    coefs = [laplace[n][0] * a_d.sum()]
+    for d in range(D):
+        M_c = M_ic[i_d[d]]
+        offsets.extend(np.arange(1, n + 1)[:, np.newaxis] * M_c)
+        coefs.extend(a_d[d] * np.array(laplace[n][1:]))
+        offsets.extend(np.arange(-1, -n - 1, -1)[:, np.newaxis] * M_c)
+        coefs.extend(a_d[d] * np.array(laplace[n][1:]))
+    return coefs, offsets
+
+
+class GUCLaplace(FDOperator):
+    """Laplacian for a general (also non-orthorhombic) cell,
+    O(h^(2n)) error; scale=-0.5 gives the kinetic-energy operator."""
+
+    def __init__(self, gd, scale=1.0, n=1, dtype=float, xp=None):
+        if not 1 <= n <= 6:
+            raise ValueError('stencil range n must be 1..6')
+        coefs, offsets = laplace_stencil(gd, scale, n)
+        super().__init__(coefs, offsets, gd, dtype, xp=xp)
+        self.description = (
+            '%d*%d+1=%d point O(h^%d) finite-difference Laplacian' %
+            ((self.npoints - 1) // n, n, self.npoints, 2 * n))
+
+
+def Laplace(gd, scale=1.0, n=1, dtype=float, xp=None):
+    """gpaw/fd_operators.py:177-181 (n = 9, the FFT Laplacian, is not part
+    of the finite-difference path)."""
+    if n == 9:
+        raise NotImplementedError('FFT Laplacian (n=9) is not provided')
+    return GUCLaplace(gd, scale, n, dtype, xp=xp)

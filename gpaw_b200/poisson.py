@@ -1,0 +1,206 @@
+"""Finite-difference multigrid Poisson solver (drop-in for the
+FDPoissonSolver of gpaw/poisson.py:321-554).
+
+The level hierarchy, smoothing counts and weights are built exactly as the
+reference builds them; one V-cycle (``iterate2``) runs in the native
+executor of the C ABI (gb_poisson_*), level 0 residual norm included, so the
+only host synchronisation per V-cycle is reading that norm.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from math import pi
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import PoissonConvergenceError, check
+from .cgpaw import _stream
+from .fd_operators import Laplace
+from .transformers import Transformer
+
+__all__ = ['FDPoissonSolver', 'PoissonConvergenceError']
+
+
+class FDPoissonSolver:
+    def __init__(self, nn=3, relax='J', eps=2e-10, maxiter=1000,
+                 remove_moment=None, use_charge_center=False,
+                 metallic_electrodes=False,
+                 use_charged_periodic_corrections=False, xp=None):
+        if remove_moment or use_charge_center or metallic_electrodes or \
+                use_charged_periodic_corrections:
+            raise NotImplementedError(
+                'moment removal / charge centre / electrodes / charged '
+                'periodic corrections are not part of this path')
+        self.eps = eps
+        self.relax = relax
+        self.nn = nn
+        self.maxiter = maxiter
+        if relax == 'GS':
+            self.relax_method = 1
+        elif relax == 'J':
+            self.relax_method = 2
+        else:
+            raise NotImplementedError('Relaxation method %s' % relax)
+        self.description = None
+        self._initialized = False
+        self._exec = None
+
+    def todict(self):
+        return {'name': 'fd', 'nn': self.nn, 'relax': self.relax,
+                'eps': self.eps}
+
+    def get_stencil(self):
+        return self.nn
+
+    def create_laplace(self, gd, scale=1.0, n=1, dtype=float):
+        return Laplace(gd, scale, n, dtype)
+
+    def set_grid_descriptor(self, gd):
+        """gpaw/poisson.py:366-430: level 0 uses the nn-order Laplacian
+        scaled by -1/(4 pi), 2 pre- and 1 post-sweep with weight 2/3; every
+        coarser level (up to 8, until coarsen() fails) a 2nd-order Laplacian,
+        4 + 4 sweeps, weight 1."""
+        if self.nn == 'M':
+            raise NotImplementedError('Mehrstellen stencil (nn="M")')
+        self.gd = gd
+        scale = -0.25 / pi
+        self.operators = [self.create_laplace(gd, scale, self.nn)]
+        self.B = None
+        self.interpolators = []
+        self.restrictors = []
+        level = 0
+        self.presmooths = [2]
+        self.postsmooths = [1]
+        self.weights = [2.0 / 3.0]
+        while level < 8:
+            try:
+                gd2 = gd.coarsen()
+            except ValueError:
+                break
+            self.operators.append(self.create_laplace(gd2, scale, 1))
+            self.interpolators.append(Transformer(gd2, gd))
+            self.restrictors.append(Transformer(gd, gd2))
+            self.presmooths.append(4)
+            self.postsmooths.append(4)
+            self.weights.append(1.0)
+            level += 1
+            gd = gd2
+        self.levels = level
+        self._initialized = False
+        self._exec = None
+
+    def get_description(self):
+        name = {1: 'Gauss-Seidel', 2: 'Jacobi'}[self.relax_method]
+        coarsest_grid = self.operators[-1].gd.N_c
+        lines = ['%s solver with %d multi-grid levels'
+                 % (name, self.levels + 1),
+                 '    Coarsest grid: %s points' % ' x '.join(
+                     str(N) for N in coarsest_grid)]
+        if coarsest_grid.max() > 24:
+            lines.extend(['    Warning: Coarse grid has more than 24 points.',
+                          '             More multi-grid levels recommended.'])
+        lines.extend(['    Stencil: %s' % self.operators[0].description,
+                      '    Max iterations: %d' % self.maxiter,
+                      '    Tolerance: %e' % self.eps])
+        return '\n'.join(lines)
+
+    def _init(self):
+        """gpaw/poisson.py:451-472: coarsest level smooths 8 + 8."""
+        if self._initialized:
+            return
+        level = self.levels
+        self.step = 0.66666666 / self.operators[0].get_diagonal_element()
+        self.presmooths[level] = 8
+        self.postsmooths[level] = 8
+        lib = _lib.load()
+        nl = self.levels + 1
+        ops = (C.c_void_p * nl)(*[o.operator._h for o in self.operators])
+        rst = (C.c_void_p * max(1, self.levels))(
+            *[t.transformer._h for t in self.restrictors])
+        itp = (C.c_void_p * max(1, self.levels))(
+            *[t.transformer._h for t in self.interpolators])
+        pre = (C.c_int * nl)(*self.presmooths)
+        post = (C.c_int * nl)(*self.postsmooths)
+        w = (C.c_double * nl)(*self.weights)
+        h = C.c_void_p()
+        check(lib.gb_poisson_new(nl, ops, rst, itp, pre, post, w,
+                                 self.relax_method, float(self.gd.dv),
+                                 C.byref(h)))
+        self._exec = _Exec(lib, h, self)
+        self._initialized = True
+
+    def solve(self, phi, rho, charge=None, maxcharge=1e-6,
+              zero_initial_phi=False, timer=None):
+        """gpaw/poisson.py:182-231: neutral systems, and charged periodic
+        ones (homogeneous background).  Returns the number of V-cycles."""
+        self._init()
+        assert tuple(phi.shape) == tuple(self.gd.n_c)
+        assert tuple(rho.shape) == tuple(self.gd.n_c)
+        actual_charge = self.gd.integrate(rho)
+        background = (actual_charge / self.gd.dv /
+                      self.gd.get_size_of_global_array().prod())
+        if charge is None:
+            charge = actual_charge
+        if abs(charge) <= maxcharge:
+            return self.solve_neutral(phi, rho - background)
+        if self.gd.pbc_c.all():
+            if zero_initial_phi:
+                phi.zero_()
+            return self.solve_neutral(phi, rho - background)
+        raise NotImplementedError(
+            'charged non-periodic system (Gaussian monopole removal)')
+
+    def solve_neutral(self, phi, rho, timer=None):
+        """gpaw/poisson.py:474-498 in the native executor."""
+        self._init()
+        rho = rho.contiguous()
+        niter = C.c_int(0)
+        err = C.c_double(0.0)
+        rc = self._exec.lib.gb_poisson_solve_neutral(
+            self._exec.h, C.c_void_p(phi.data_ptr()),
+            C.c_void_p(rho.data_ptr()), float(self.eps), int(self.maxiter),
+            C.byref(niter), C.byref(err), _stream())
+        self.last_error = err.value
+        self.niter = niter.value
+        check(rc)
+        return niter.value
+
+    def iterate2(self, step, level=0, phi=None, rho=None):
+        """One V-cycle from level 0 (gpaw/poisson.py:500-537); returns the
+        level-0 error sum(r^2) * dv."""
+        if level != 0:
+            raise NotImplementedError('V-cycles start at level 0')
+        self._init()
+        err = C.c_double(0.0)
+        check(self._exec.lib.gb_poisson_iterate(
+            self._exec.h, C.c_void_p(phi.data_ptr()),
+            C.c_void_p(rho.data_ptr()), C.byref(err), _stream()))
+        return err.value
+
+    def estimate_memory(self, mem=None):
+        gdbytes = int(np.prod(self.gd.n_c)) * 8
+        nbytes = -gdbytes
+        for level in range(self.levels):
+            nbytes += 3 * gdbytes
+            gdbytes //= 8
+        return nbytes
+
+    def __repr__(self):
+        return 'FDPoissonSolver(relax=\'%s\', nn=%s, eps=%e)' % (
+            self.relax, repr(self.nn), self.eps)
+
+
+class _Exec:
+    def __init__(self, lib, h, owner):
+        self.lib = lib
+        self.h = h
+        # keep level objects alive as long as the executor
+        self._keep = (owner.operators, owner.restrictors,
+                      owner.interpolators)
+
+    def __del__(self):
+        if self.h is not None and self.h.value:
+            self.lib.gb_poisson_free(self.h)
+            self.h = None

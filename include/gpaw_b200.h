@@ -1,0 +1,180 @@
+/* gpaw_b200 — C ABI of the B200 (sm_100a) finite-difference hot path.
+ *
+ * Each entry point replaces one GPU entry point of the reference's compiled
+ * extension (`cgpaw`), keeping the argument meaning: device pointers in,
+ * device pointers out, C-contiguous arrays, an optional leading batch
+ * dimension `nin` (the reference's ndim == 4 case), and phases as the
+ * (3, 2) complex array `phase_cd` flattened to 12 doubles (re, im, ...).
+ *
+ * Conventions
+ *   - Return value: 0 on success, GB_EINVAL for an argument the reference
+ *     would reject (TypeError / ValueError / AssertionError), GB_ECUDA for a
+ *     CUDA failure (the reference's RuntimeError via gpaw_set_runtime_error,
+ *     c/gpu/operators.cpp:381-384), GB_ENOCONV for a Poisson solve that hit
+ *     maxiter (PoissonConvergenceError, gpaw/poisson.py:487-489).
+ *     gb_last_error() returns the message of the last failure of the calling
+ *     thread.
+ *   - `stream` is a cudaStream_t (NULL = legacy default stream).  Every
+ *     launch is asynchronous on that stream except where noted; no entry
+ *     point synchronises the device.
+ *   - dtype: GB_F64 (numpy float64) or GB_C128 (numpy complex128).
+ *   - Objects own only their stencil, geometry and scratch.  One object
+ *     must not be used from two streams at the same time (its scratch is
+ *     shared between calls).
+ *   - Single domain: a neighbour equal to 0 (own rank) means periodic, -1
+ *     means zero boundary (gpaw/old/domain.py:110-138).  Domain
+ *     decomposition over several GPUs is not part of this library.
+ */
+#ifndef GPAW_B200_H
+#define GPAW_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define GB_API __attribute__((visibility("default")))
+#else
+#define GB_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GB_OK 0
+#define GB_EINVAL 1
+#define GB_ECUDA 2
+#define GB_ENOCONV 3
+
+#define GB_F64 0
+#define GB_C128 1
+
+typedef struct gb_operator gb_operator;
+typedef struct gb_transformer gb_transformer;
+typedef struct gb_poisson gb_poisson;
+
+/* Library version (major * 10000 + minor * 100 + patch). */
+GB_API int gb_version(void);
+
+/* Message of the calling thread's last failed call ("" if none). */
+GB_API const char* gb_last_error(void);
+
+/* ------------------------------------------------------------------ Operator
+ * Replaces cgpaw.Operator(coefs, offsets, size, range, neighbors, real, comm,
+ * cfd, use_gpu) — NewOperatorObject, c/operators.cpp:379-420.
+ *   coefs[ncoefs]     stencil coefficients, summed in this order
+ *   offsets[ncoefs]   offsets flattened with the PADDED strides
+ *                     (M_c = size_c + 2 * range), as FDOperator builds them
+ *                     (gpaw/fd_operators.py:60-63)
+ *   size[3]           interior grid size n_c
+ *   range             stencil half-width mp (padding)
+ *   neighbors[6]      neighbor_cd, row-major (3, 2)
+ *   real              1 for float64 data, 0 for complex128
+ *   cfd               1 if every offset lies on an axis
+ */
+GB_API int gb_operator_new(const double* coefs, const int64_t* offsets, int ncoefs,
+                    const int64_t size[3], int range, const int64_t neighbors[6],
+                    int real, int cfd, gb_operator** out);
+GB_API void gb_operator_free(gb_operator* op);
+
+/* Replaces Operator.apply_gpu(in_ptr, out_ptr, shape, dtype, phases) —
+ * Operator_apply_gpu, c/gpu/operators.cpp:344-385 (CPU twin Operator_apply,
+ * c/operators.cpp:245-316).  out[x] = sum_p coefs[p] * in_padded[x + p]
+ * for every grid of the batch.  `in == out` is allowed (the input is then
+ * staged through the operator's scratch, as the reference stages it through
+ * its padded buffer).  phases may be NULL (all ones). */
+GB_API int gb_operator_apply(gb_operator* op, const void* in, void* out, int64_t nin,
+                      int dtype, const double* phases, void* stream);
+
+/* Replaces Operator.relax_gpu(method, f_ptr, s_ptr, nrelax, w) —
+ * Operator_relax_gpu, c/gpu/operators.cpp:200-221 (CPU twin Operator_relax,
+ * c/operators.cpp:50-92).  float64 only, one grid.  method 2: weighted
+ * Jacobi with weight w; method 1: lexicographic Gauss-Seidel (w ignored),
+ * bit-identical to the reference's CPU loop (the reference's own GPU
+ * Gauss-Seidel is a no-op, c/gpu/kernels/relax.cpp:72-80). */
+GB_API int gb_operator_relax(gb_operator* op, int method, double* f, const double* s,
+                      int nrelax, double w, void* stream);
+
+/* Residual r = L(phi) - rho for a batch (gpaw/poisson.py:517-518 done in
+ * one pass).  r may be NULL.  If norm2 is not NULL it receives, per grid,
+ * scale * sum |r|^2 as a DEVICE array of nin doubles (the reference's
+ * xp.dot(r, r) * dv, gpaw/poisson.py:527-532, without the host sync). */
+GB_API int gb_operator_residual(gb_operator* op, const void* phi, const void* rho,
+                         void* r, int64_t nin, int dtype, const double* phases,
+                         double scale, double* norm2, void* stream);
+
+/* Replaces Operator.get_diagonal_element(), c/operators.cpp:319-332. */
+GB_API double gb_operator_get_diagonal_element(const gb_operator* op);
+
+/* Preallocate the operator's scratch for batches up to nin grids (so that
+ * later calls allocate nothing, e.g. inside CUDA-graph capture). */
+GB_API int gb_operator_reserve(gb_operator* op, int64_t nin, int dtype);
+
+/* --------------------------------------------------------------- Transformer
+ * Replaces cgpaw.Transformer(size_in, size_out, k, pads, npads, skip,
+ * neighbors, real, comm, interpolate, use_gpu) — NewTransformerObject,
+ * c/transformers.cpp:196-246.  k = 2 * nn in {2, 4, 6, 8}.  pads, npads,
+ * skip, neighbors are row-major (3, 2) arrays as built by _Transformer
+ * (gpaw/transformers.py:31-55). */
+GB_API int gb_transformer_new(const int64_t size_in[3], const int64_t size_out[3], int k,
+                       const int64_t pads[6], const int64_t npads[6],
+                       const int64_t skip[6], const int64_t neighbors[6], int real,
+                       int interpolate, gb_transformer** out);
+GB_API void gb_transformer_free(gb_transformer* t);
+
+/* Replaces Transformer.apply_gpu(in_ptr, out_ptr, shape, dtype, phases) —
+ * Transformer_apply_gpu, c/gpu/transformers.cpp:189-226 (CPU twin
+ * Transformer_apply, c/transformers.cpp:112-158).  in and out must not
+ * overlap. */
+GB_API int gb_transformer_apply(gb_transformer* t, const void* in, void* out, int64_t nin,
+                         int dtype, const double* phases, void* stream);
+
+/* ---------------------------------------------------------------- fd_precond
+ * Replaces cgpaw.fd_precond(rest0, rest1, intp1, intp2, kin0, kin1, kin2,
+ * d0, q0, r1, d1, q1, r2, d2, q2, residuals, nresiduals, step, phases) —
+ * c/fd_preconditioner.cpp:106-351 (the reference has no GPU version; its
+ * GPU path runs the same sequence as ~20 cupy launches,
+ * gpaw/preconditioner.py:74-93).  Writes the preconditioned residuals to
+ * d0.  nresiduals (= -residuals) may be NULL: the negation is then applied
+ * on load.  Scratch arrays q0, r1, d1, q1, r2, d2, q2 are caller-owned as
+ * in the reference; their contents on return are unspecified. */
+GB_API int gb_fd_precond(gb_transformer* rest0, gb_transformer* rest1, gb_transformer* intp1,
+                  gb_transformer* intp2, gb_operator* kin0, gb_operator* kin1,
+                  gb_operator* kin2, void* d0, void* q0, void* r1, void* d1, void* q1,
+                  void* r2, void* d2, void* q2, const void* residuals,
+                  const void* nresiduals, int64_t nin, int dtype, double step,
+                  const double* phases, void* stream);
+
+/* -------------------------------------------------------------- FD Poisson
+ * Native executor for FDPoissonSolver's multigrid V-cycle
+ * (gpaw/poisson.py:451-537).  nlevels = levels + 1 operators; levels
+ * restrictors (level l -> l+1) and interpolators (level l+1 -> l), built
+ * as FDPoissonSolver.set_grid_descriptor builds them (:366-430).
+ * presmooths/postsmooths/weights per level as in :386-403 and :470-471.
+ * dv is the volume element of level 0.  The objects passed in must outlive
+ * the executor. */
+GB_API int gb_poisson_new(int nlevels, gb_operator* const* operators,
+                   gb_transformer* const* restrictors,
+                   gb_transformer* const* interpolators, const int* presmooths,
+                   const int* postsmooths, const double* weights, int relax_method,
+                   double dv, gb_poisson** out);
+GB_API void gb_poisson_free(gb_poisson* p);
+
+/* One V-cycle, FDPoissonSolver.iterate2(step, level=0) (:500-537): updates
+ * phi in place and writes sum r^2 * dv to *error (host).  Synchronises the
+ * stream once (to read the error). */
+GB_API int gb_poisson_iterate(gb_poisson* p, double* phi, const double* rho, double* error,
+                       void* stream);
+
+/* FDPoissonSolver.solve_neutral(phi, rho) (:474-498): V-cycles until
+ * error <= eps, at most maxiter (GB_ENOCONV when the loop stops at
+ * maxiter, as the reference raises).  Periodic grids get the mean of phi
+ * removed.  *niter and *error (host) receive the iteration count and the
+ * last error. */
+GB_API int gb_poisson_solve_neutral(gb_poisson* p, double* phi, const double* rho, double eps,
+                             int maxiter, int* niter, double* error, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GPAW_B200_H */

@@ -1,0 +1,442 @@
+"""Restatement of the reference's Python layer on the FD hot path.
+
+TEST INFRASTRUCTURE ONLY (the oracle).  It drives either the reference's own
+C core compiled from source (``oracle/_ref/_gpaw_ref*.so``, built by
+``oracle/Makefile``) or, where that library is absent, the numpy restatement
+in ``oracle/port.py``.  The ``gpaw_b200`` package never imports it.
+
+Restated from (all single-domain, ``comm.size == 1``):
+
+* grid conventions  gpaw/old/grid_descriptor.py:119-160, 327-342
+* neighbours        gpaw/old/domain.py:110-138
+* Bloch phases      gpaw/core/uniform_grid.py:116-127
+* Laplacian         gpaw/fd_operators.py:27-34, 43-97, 184-238
+* transformer pads  gpaw/transformers.py:19-77
+* Poisson solver    gpaw/poisson.py:182-213, 321-537
+* preconditioner    gpaw/preconditioner.py:9-93
+"""
+from __future__ import annotations
+
+import glob
+import importlib.util
+import os
+from math import pi
+
+import numpy as np
+
+from . import port
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def load_ref():
+    """Import the compiled reference core, or return None if not built."""
+    hits = glob.glob(os.path.join(_HERE, '_ref', '_gpaw_ref*.so'))
+    if not hits:
+        return None
+    spec = importlib.util.spec_from_file_location('_gpaw_ref', hits[0])
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+_REF = load_ref()
+
+
+def backend(name='auto'):
+    """'ref' = compiled reference core, 'port' = numpy restatement."""
+    if name == 'ref' or (name == 'auto' and _REF is not None):
+        if _REF is None:
+            raise RuntimeError('reference core not built (make -C oracle)')
+        return _REF
+    return port
+
+
+class BadGridError(ValueError):
+    pass
+
+
+class PoissonConvergenceError(RuntimeError):
+    pass
+
+
+# Chelikowsky et al., PRB 50, 11355 (1994); gpaw/fd_operators.py:27-34
+LAPLACE = [[0],
+           [-2, 1],
+           [-5 / 2, 4 / 3, -1 / 12],
+           [-49 / 18, 3 / 2, -3 / 20, 1 / 90],
+           [-205 / 72, 8 / 5, -1 / 5, 8 / 315, -1 / 560],
+           [-5269 / 1800, 5 / 3, -5 / 21, 5 / 126, -5 / 1008, 1 / 3150],
+           [-5369 / 1800, 12 / 7, -15 / 56, 10 / 189, -1 / 112, 2 / 1925,
+            -1 / 16632]]
+
+
+class GridDescriptor:
+    """Single-domain grid descriptor (gpaw/old/grid_descriptor.py)."""
+
+    def __init__(self, N_c, cell_cv=(1, 1, 1), pbc_c=True):
+        if isinstance(pbc_c, (bool, int, np.bool_)):
+            pbc_c = (bool(pbc_c),) * 3
+        self.pbc_c = np.array(pbc_c, bool)
+        self.N_c = np.array(N_c, int)
+        cell = np.array(cell_cv, float)
+        if cell.ndim == 0:
+            cell = np.eye(3) * cell
+        elif cell.ndim == 1:
+            cell = np.diag(cell)
+        self.cell_cv = cell
+        self.beg_c = np.empty(3, int)
+        self.end_c = np.empty(3, int)
+        for c in range(3):
+            # gpaw/old/grid_descriptor.py:136-152 with one domain
+            n_p = np.around(np.array([0.0, float(self.N_c[c])]) + 0.4999)
+            n_p = n_p.astype(int)
+            if not self.pbc_c[c]:
+                n_p[0] = 1
+            if n_p[1] == n_p[0]:
+                raise BadGridError('Grid %s too small' % self.N_c)
+            self.beg_c[c] = n_p[0]
+            self.end_c[c] = n_p[1]
+        self.n_c = self.end_c - self.beg_c
+        self.h_cv = self.cell_cv / self.N_c[:, None]
+        self.volume = abs(np.linalg.det(self.cell_cv))
+        self.dv = self.volume / self.N_c.prod()
+        # gpaw/old/domain.py:110-138: own rank (0) or -1 across a zero BC
+        self.neighbor_cd = np.where(self.pbc_c[:, None], 0, -1) * \
+            np.ones((3, 2), int)
+        self.neighbor_cd = np.ascontiguousarray(self.neighbor_cd, np.int64)
+
+    def coarsen(self):
+        if (self.N_c % 2).any():
+            raise ValueError('Grid %s not divisible by 2!' % self.N_c)
+        return GridDescriptor(self.N_c // 2, self.cell_cv, self.pbc_c)
+
+    def refine(self):
+        return GridDescriptor(self.N_c * 2, self.cell_cv, self.pbc_c)
+
+    def zeros(self, n=(), dtype=float):
+        if isinstance(n, int):
+            n = (n,)
+        return np.zeros(tuple(n) + tuple(self.n_c), dtype)
+
+    def empty(self, n=(), dtype=float):
+        return self.zeros(n, dtype)
+
+    def integrate(self, a):
+        return a.sum(axis=(-3, -2, -1)) * self.dv
+
+    def phase_factor_cd(self, kpt_c):
+        """gpaw/core/uniform_grid.py:116-127, one domain: disp = (+1, -1)."""
+        disp_cd = np.array([[1.0, -1.0]] * 3)
+        return np.exp(2j * np.pi * disp_cd * np.asarray(kpt_c)[:, None])
+
+    def get_grid_point_coordinates(self):
+        idx = np.indices(self.n_c) + self.beg_c[:, None, None, None]
+        return np.einsum('cv,cxyz->vxyz', self.h_cv, idx)
+
+
+class FDOperator:
+    """gpaw/fd_operators.py:43-147 (single domain)."""
+
+    def __init__(self, coef_p, offset_pc, gd, dtype=float, be='auto'):
+        offset_pc = np.asarray(offset_pc, int)
+        cfd = True
+        for offset_c in offset_pc:
+            if sum([o != 0 for o in offset_c]) >= 2:
+                cfd = False
+        mp = np.abs(offset_pc).max()
+        assert (mp <= gd.n_c).all(), 'Stencil longer than domain'
+        n_c = gd.n_c
+        M_c = n_c + 2 * mp
+        stride_c = np.array([M_c[1] * M_c[2], M_c[2], 1])
+        offset_p = np.ascontiguousarray(np.dot(offset_pc, stride_c))
+        coef_p = np.ascontiguousarray(coef_p, float)
+        self.dtype = dtype
+        self.shape = tuple(n_c)
+        self.mp = mp
+        self.gd = gd
+        self.npoints = len(coef_p)
+        self.coef_p = coef_p
+        self.offset_p = offset_p
+        self.offset_pc = offset_pc
+        self.cfd = cfd
+        self.operator = backend(be).Operator(
+            coef_p, offset_p, np.ascontiguousarray(n_c, np.int64), int(mp),
+            gd.neighbor_cd, dtype == float, None, cfd)
+
+    def apply(self, in_xg, out_xg, phase_cd=None):
+        self.operator.apply(in_xg, out_xg, phase_cd)
+
+    def relax(self, relax_method, f_g, s_g, n, w=None):
+        self.operator.relax(relax_method, f_g, s_g, n,
+                            1.0 if w is None else w)
+
+    def get_diagonal_element(self):
+        return self.operator.get_diagonal_element()
+
+
+def laplace_stencil(gd, scale=1.0, n=1):
+    """Coefficients and offsets of GUCLaplace (gpaw/fd_operators.py:184-238)."""
+    M_ic = np.indices((3, 3, 3)).reshape((3, -3)).T[-13:] - 1
+    u_cv = gd.h_cv / (gd.h_cv**2).sum(1)[:, np.newaxis]**0.5
+    u2_i = (np.dot(M_ic, u_cv)**2).sum(1)
+    i_d = u2_i.argsort()
+    m_mv = np.array([(2, 0, 0), (0, 2, 0), (0, 0, 2),
+                     (0, 1, 1), (1, 0, 1), (1, 1, 0)])
+    for D in range(3, 7):
+        h_dv = np.dot(M_ic[i_d[:D]], gd.h_cv)
+        A_md = (h_dv**m_mv[:, np.newaxis, :]).prod(2)
+        a_d, residual, rank, s = np.linalg.lstsq(A_md, [1, 1, 1, 0, 0, 0],
+                                                 rcond=-1)
+        if residual.sum() < 1e-14:
+            if rank != D:
+                raise ValueError('weird unit cell')
+            break
+    a_d *= scale
+    offsets = [(0, 0, 0)]
+    coefs = [LAPLACE[n][0] * a_d.sum()]
+    for d in range(D):
+        M_c = M_ic[i_d[d]]
+        offsets.extend(np.arange(1, n + 1)[:, np.newaxis] * M_c)
+        coefs.extend(a_d[d] * np.array(LAPLACE[n][1:]))
+        offsets.extend(np.arange(-1, -n - 1, -1)[:, np.newaxis] * M_c)
+        coefs.extend(a_d[d] * np.array(LAPLACE[n][1:]))
+    return coefs, offsets
+
+
+def Laplace(gd, scale=1.0, n=1, dtype=float, be='auto'):
+    coefs, offsets = laplace_stencil(gd, scale, n)
+    return FDOperator(coefs, offsets, gd, dtype, be=be)
+
+
+def transformer_geometry(gdin, gdout, nn):
+    """Pads, neighbour pads and skip flags (gpaw/transformers.py:19-77)."""
+    pad_cd = np.empty((3, 2), int)
+    neighborpad_cd = np.empty((3, 2), int)
+    skip_cd = np.empty((3, 2), int)
+    if (gdin.N_c == 2 * gdout.N_c).all():
+        pad_cd[:, 0] = 2 * nn - 1 - 2 * gdout.beg_c + gdin.beg_c
+        pad_cd[:, 1] = 2 * nn - 2 + 2 * gdout.end_c - gdin.end_c
+        neighborpad_cd[:, 0] = 2 * nn - 2 + 2 * gdout.beg_c - gdin.beg_c
+        neighborpad_cd[:, 1] = 2 * nn - 1 - 2 * gdout.end_c + gdin.end_c
+        interpolate = False
+    else:
+        assert (gdout.N_c == 2 * gdin.N_c).all()
+        pad_cd[:, 0] = nn - 1 - gdout.beg_c // 2 + gdin.beg_c
+        pad_cd[:, 1] = nn + gdout.end_c // 2 - gdin.end_c
+        neighborpad_cd[:, 0] = nn + gdout.beg_c // 2 - gdin.beg_c
+        neighborpad_cd[:, 1] = nn - 1 - gdout.end_c // 2 + gdin.end_c
+        skip_cd[:, 0] = gdout.beg_c % 2
+        skip_cd[:, 1] = gdout.end_c % 2
+        interpolate = True
+        inpoints = (gdin.n_c[0] + 2 * nn - 1) * (gdin.n_c[1] + 2 * nn - 1)
+        outpoints = gdout.n_c[0] * gdout.n_c[1]
+        if inpoints > outpoints:
+            raise ValueError('Cannot construct interpolator.')
+        # The reference's first interpolation pass writes s0 * s1 * o2 values
+        # into the output array (c/bmgs/interpolate.cpp:87-90); its guard above
+        # uses 2nn - 1 where the padded extent is n + 2nn, so some grids pass
+        # the guard and still overflow the heap.  Refuse those here so that
+        # the oracle never runs the reference into undefined behaviour.
+        s_c = gdin.n_c + pad_cd.sum(1)
+        if s_c[0] * s_c[1] > gdout.n_c[0] * gdout.n_c[1]:
+            raise ValueError('grid too small for the reference interpolator '
+                             '(its scratch would overflow)')
+    if not interpolate:
+        skip_cd[:] = 0
+    assert (pad_cd.ravel() >= 0).all()
+    return pad_cd, neighborpad_cd, skip_cd, interpolate
+
+
+class Transformer:
+    """gpaw/transformers.py:18-94."""
+
+    def __init__(self, gdin, gdout, nn=1, dtype=float, be='auto'):
+        self.gdin = gdin
+        self.gdout = gdout
+        self.nn = nn
+        self.dtype = dtype
+        pad, npad, skip, self.interpolate = transformer_geometry(gdin, gdout,
+                                                                 nn)
+        self.pad_cd, self.neighborpad_cd, self.skip_cd = pad, npad, skip
+        self.transformer = backend(be).Transformer(
+            np.ascontiguousarray(gdin.n_c, np.int64),
+            np.ascontiguousarray(gdout.n_c, np.int64), 2 * nn,
+            np.ascontiguousarray(pad, np.int64),
+            np.ascontiguousarray(npad, np.int64),
+            np.ascontiguousarray(skip, np.int64),
+            gdin.neighbor_cd, dtype == float, None, self.interpolate)
+
+    def apply(self, input, output=None, phases=None):
+        if output is None:
+            output = self.gdout.zeros(input.shape[:-3], self.dtype)
+        self.transformer.apply(input, output, phases)
+        return output
+
+
+class FDPoissonSolver:
+    """gpaw/poisson.py:321-537 (neutral and periodic-charged branches)."""
+
+    def __init__(self, nn=3, relax='J', eps=2e-10, maxiter=1000, be='auto'):
+        self.nn = nn
+        self.eps = eps
+        self.maxiter = maxiter
+        self.relax = relax
+        self.relax_method = {'GS': 1, 'J': 2}[relax]
+        self.be = be
+        self._initialized = False
+
+    def set_grid_descriptor(self, gd):
+        self.gd = gd
+        scale = -0.25 / pi
+        self.operators = [Laplace(gd, scale, self.nn, be=self.be)]
+        self.interpolators = []
+        self.restrictors = []
+        level = 0
+        self.presmooths = [2]
+        self.postsmooths = [1]
+        self.weights = [2.0 / 3.0]
+        while level < 8:
+            try:
+                gd2 = gd.coarsen()
+            except ValueError:
+                break
+            self.operators.append(Laplace(gd2, scale, 1, be=self.be))
+            self.interpolators.append(Transformer(gd2, gd, be=self.be))
+            self.restrictors.append(Transformer(gd, gd2, be=self.be))
+            self.presmooths.append(4)
+            self.postsmooths.append(4)
+            self.weights.append(1.0)
+            level += 1
+            gd = gd2
+        self.levels = level
+        self._initialized = False
+
+    def _init(self):
+        if self._initialized:
+            return
+        gd = self.gd
+        self.rhos = [gd.empty()]
+        self.phis = [None]
+        self.residuals = [gd.empty()]
+        for level in range(self.levels):
+            gd2 = gd.coarsen()
+            self.phis.append(gd2.empty())
+            self.rhos.append(gd2.empty())
+            self.residuals.append(gd2.empty())
+            gd = gd2
+        level = self.levels
+        self.step = 0.66666666 / self.operators[0].get_diagonal_element()
+        self.presmooths[level] = 8
+        self.postsmooths[level] = 8
+        self._initialized = True
+
+    def solve(self, phi, rho, charge=None, maxcharge=1e-6,
+              zero_initial_phi=False):
+        """gpaw/poisson.py:182-213 (+ periodic charged :217-231)."""
+        self._init()
+        actual_charge = self.gd.integrate(rho)
+        # get_size_of_global_array() = N_c - 1 + pbc_c = n_c on one domain
+        # (gpaw/old/grid_descriptor.py:214-218)
+        background = (actual_charge / self.gd.dv / self.gd.n_c.prod())
+        if charge is None:
+            charge = actual_charge
+        if abs(charge) <= maxcharge:
+            return self.solve_neutral(phi, rho - background)
+        if self.gd.pbc_c.all():
+            if zero_initial_phi:
+                phi[:] = 0.0
+            return self.solve_neutral(phi, rho - background)
+        raise NotImplementedError('charged non-periodic system')
+
+    def solve_neutral(self, phi, rho):
+        self._init()
+        self.phis[0] = phi
+        self.rhos[0][:] = rho
+        niter = 1
+        self.errors = []
+        while self.iterate2(self.step) > self.eps and niter < self.maxiter:
+            niter += 1
+        if niter == self.maxiter:
+            raise PoissonConvergenceError('did not converge')
+        if self.gd.pbc_c.all():
+            phi_ave = float(np.sum(phi.ravel()))
+            phi_ave /= np.prod(self.gd.n_c)
+            phi -= phi_ave
+        return niter
+
+    def iterate2(self, step, level=0):
+        residual = self.residuals[level]
+        if level < self.levels:
+            self.operators[level].relax(self.relax_method, self.phis[level],
+                                        self.rhos[level],
+                                        self.presmooths[level],
+                                        self.weights[level])
+            self.operators[level].apply(self.phis[level], residual)
+            residual -= self.rhos[level]
+            self.restrictors[level].apply(residual, self.rhos[level + 1])
+            self.phis[level + 1][:] = 0.0
+            self.iterate2(4.0 * step, level + 1)
+            self.interpolators[level].apply(self.phis[level + 1], residual)
+            self.phis[level] -= residual
+        self.operators[level].relax(self.relax_method, self.phis[level],
+                                    self.rhos[level],
+                                    self.postsmooths[level],
+                                    self.weights[level])
+        if level == 0:
+            self.operators[level].apply(self.phis[level], residual)
+            residual -= self.rhos[level]
+            error = float(np.dot(residual.ravel(), residual.ravel())) * \
+                self.gd.dv
+            self.errors.append(error)
+            return error
+
+
+class Preconditioner:
+    """gpaw/preconditioner.py:9-73 (C path)."""
+
+    def __init__(self, gd0, kin0, dtype=float, block=1, be='auto'):
+        gd1 = gd0.coarsen()
+        gd2 = gd1.coarsen()
+        self.be = backend(be)
+        self.kin0 = kin0
+        self.kin1 = Laplace(gd1, -0.5, 1, dtype, be=be)
+        self.kin2 = Laplace(gd2, -0.5, 1, dtype, be=be)
+        self.scratch0 = gd0.zeros((2, block), dtype)
+        self.scratch1 = gd1.zeros((3, block), dtype)
+        self.scratch2 = gd2.zeros((3, block), dtype)
+        self.step = 0.66666666 / kin0.get_diagonal_element()
+        self.restrictor_object0 = Transformer(gd0, gd1, 1, dtype, be=be)
+        self.restrictor_object1 = Transformer(gd1, gd2, 1, dtype, be=be)
+        self.interpolator_object2 = Transformer(gd2, gd1, 1, dtype, be=be)
+        self.interpolator_object1 = Transformer(gd1, gd0, 1, dtype, be=be)
+
+    def __call__(self, residuals, phases=None, out=None):
+        if residuals.ndim == 3:
+            if out is None:
+                return self.__call__(residuals[np.newaxis], phases)[0]
+            return self.__call__(residuals[np.newaxis], phases,
+                                 out=out[np.newaxis])[0]
+        nb = len(residuals)
+        nb0 = self.scratch0.shape[1]
+        if nb > nb0:
+            assert out is not None
+            for n1 in range(0, nb, nb0):
+                self(residuals[n1:n1 + nb0], phases, out=out[n1:n1 + nb0])
+            return out
+        if out is None:
+            d0, q0 = self.scratch0[:, :nb]
+        else:
+            d0 = out
+            q0 = self.scratch0[0, :nb]
+        r1, d1, q1 = self.scratch1[:, :nb]
+        r2, d2, q2 = self.scratch2[:, :nb]
+        self.be.fd_precond(self.restrictor_object0.transformer,
+                           self.restrictor_object1.transformer,
+                           self.interpolator_object1.transformer,
+                           self.interpolator_object2.transformer,
+                           self.kin0.operator, self.kin1.operator,
+                           self.kin2.operator,
+                           d0, q0, r1, d1, q1, r2, d2, q2,
+                           residuals, -residuals, self.step, phases)
+        return d0

@@ -1,0 +1,150 @@
+"""Generate the golden fixtures of tests/golden/ from the reference itself.
+
+Runs the reference's own C core (built from its sources by
+``make -C oracle``) through the restatement of its Python layer in
+``oracle/gpaw_layer.py`` on small seeded inputs, and stores inputs and
+outputs in ``golden.npz``.  Re-run after changing a case:
+
+    make -C oracle && python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from oracle import gpaw_layer as L  # noqa: E402
+
+KPT = (0.25, 0.0, 0.1)
+
+
+def cases():
+    """(name, builder) pairs; every builder returns a dict of arrays."""
+    out = []
+    # FD apply: nn = 1..6, real/complex, periodic / zero / mixed
+    for nn in range(1, 7):
+        for bc in ('p', 'z', 'm'):
+            for dt in ('f', 'c'):
+                out.append((f'fd_nn{nn}_{bc}_{dt}', ('fd', nn, bc, dt)))
+    # non-orthorhombic cell (cfd = 0 stencil)
+    for dt in ('f', 'c'):
+        out.append((f'fd_hex_{dt}', ('fdhex', 2, 'p', dt)))
+    # relax
+    for m in (1, 2):
+        for bc in ('p', 'z'):
+            out.append((f'relax_m{m}_{bc}', ('relax', m, bc, 'f')))
+    # transformers
+    for nn in range(1, 4):
+        for bc in ('p', 'z', 'm'):
+            for dt in ('f', 'c'):
+                out.append((f'tr_nn{nn}_{bc}_{dt}', ('tr', nn, bc, dt)))
+    # order 8 needs larger grids (interpolator guard, gpaw/transformers.py:50)
+    for bc, dt in (('p', 'f'), ('z', 'f'), ('p', 'c')):
+        out.append((f'tr_nn4_{bc}_{dt}', ('tr', 4, bc, dt)))
+    # preconditioner
+    for bc in ('p', 'z'):
+        for dt in ('f', 'c'):
+            out.append((f'pc_{bc}_{dt}', ('pc', 3, bc, dt)))
+    # Poisson
+    for bc in ('p', 'z'):
+        out.append((f'ps_{bc}', ('ps', 3, bc, 'f')))
+    return out
+
+
+def pbc_of(bc):
+    return {'p': (1, 1, 1), 'z': (0, 0, 0), 'm': (1, 0, 1)}[bc]
+
+
+def build(kind, nn, bc, dt, rng):
+    dtype = float if dt == 'f' else complex
+    pbc = pbc_of(bc)
+    d = {}
+
+    def rand(shape):
+        a = rng.standard_normal(shape)
+        if dtype == complex:
+            a = a + 1j * rng.standard_normal(shape)
+        return a
+
+    if kind in ('fd', 'fdhex'):
+        N = (8, 7, 9) if kind == 'fd' else (8, 8, 6)
+        cell = (3.1, 2.9, 3.5) if kind == 'fd' else \
+            [(3.0, 0, 0), (1.5, 3.0 * 3**0.5 / 2, 0), (0, 0, 3.2)]
+        gd = L.GridDescriptor(N, cell, pbc)
+        op = L.Laplace(gd, -0.5, nn, dtype, be='ref')
+        a = rand((1,) + tuple(gd.n_c))
+        ph = gd.phase_factor_cd(KPT) if dtype == complex else None
+        b = np.zeros_like(a)
+        op.apply(a, b, ph)
+        d.update(N=np.array(N), cell=np.array(cell, float), pbc=np.array(pbc),
+                 inp=a, out=b, coefs=op.coef_p, offsets=op.offset_pc)
+        if ph is not None:
+            d['phases'] = ph
+    elif kind == 'relax':
+        gd = L.GridDescriptor((8, 7, 9), (3.0, 2.6, 3.3), pbc)
+        op = L.Laplace(gd, -0.25 / np.pi, 3, be='ref')
+        f = rand(tuple(gd.n_c))
+        s = rand(tuple(gd.n_c))
+        g = f.copy()
+        op.relax(nn, g, s, 3, 2.0 / 3.0)
+        d.update(N=np.array(gd.N_c), pbc=np.array(pbc), f=f, s=s, out=g)
+    elif kind == 'tr':
+        N = {1: (12, 10, 8), 2: (12, 10, 8), 3: (16, 14, 8), 4: (20, 18, 8)}[nn]
+        gd = L.GridDescriptor(N, (3.0, 3.4, 3.9), pbc)
+        gd2 = gd.coarsen()
+        ph = gd.phase_factor_cd(KPT) if dtype == complex else None
+        a = rand((1,) + tuple(gd.n_c))
+        r = L.Transformer(gd, gd2, nn, dtype, be='ref').apply(a, phases=ph)
+        c = rand((1,) + tuple(gd2.n_c))
+        i = L.Transformer(gd2, gd, nn, dtype, be='ref').apply(c, phases=ph)
+        d.update(N=np.array(gd.N_c), pbc=np.array(pbc), fine=a,
+                 restricted=r, coarse=c, interpolated=i)
+        if ph is not None:
+            d['phases'] = ph
+    elif kind == 'pc':
+        gd = L.GridDescriptor((8, 8, 12), (3.0, 3.0, 4.5), pbc)
+        kin = L.Laplace(gd, -0.5, nn, dtype, be='ref')
+        pc = L.Preconditioner(gd, kin, dtype, block=2, be='ref')
+        R = rand((3,) + tuple(gd.n_c))
+        ph = gd.phase_factor_cd(KPT) if dtype == complex else None
+        o = np.zeros_like(R)
+        pc(R, ph, out=o)
+        d.update(N=np.array(gd.N_c), pbc=np.array(pbc), res=R, out=o)
+        if ph is not None:
+            d['phases'] = ph
+    elif kind == 'ps':
+        gd = L.GridDescriptor((16, 8, 16), (4.0, 2.0, 4.0), pbc)
+        x = gd.get_grid_point_coordinates()
+        rho = np.exp(-((x[0] - 2) ** 2 + (x[1] - 0.9) ** 2 +
+                       (x[2] - 2.1) ** 2) / 0.5) - \
+            np.exp(-((x[0] - 1.5) ** 2 + (x[1] - 1.1) ** 2 +
+                     (x[2] - 2.1) ** 2) / 0.5)
+        rho = rho - rho.mean()
+        ps = L.FDPoissonSolver(nn=nn, eps=1e-18, be='ref')
+        ps.set_grid_descriptor(gd)
+        phi = gd.zeros()
+        niter = ps.solve(phi, rho)
+        d.update(N=np.array(gd.N_c), pbc=np.array(pbc), rho=rho, phi=phi,
+                 niter=np.array(niter), errors=np.array(ps.errors))
+    return d
+
+
+def main():
+    if L._REF is None:
+        raise SystemExit('reference core not built: make -C oracle')
+    rng = np.random.default_rng(20261203)
+    data = {}
+    for name, (kind, nn, bc, dt) in cases():
+        for k, v in build(kind, nn, bc, dt, rng).items():
+            data[f'{name}/{k}'] = v
+    path = os.path.join(HERE, 'golden.npz')
+    np.savez_compressed(path, **data)
+    print(path, os.path.getsize(path), 'bytes', len(cases()), 'cases')
+
+
+if __name__ == '__main__':
+    main()

@@ -1,0 +1,58 @@
+"""The C-ABI library loads without a GPU and exports every entry point that
+include/gpaw_b200.h declares, with a binding for each in gpaw_b200._lib."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from gpaw_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared():
+    names = set()
+    for fn in os.listdir(os.path.join(ROOT, 'include')):
+        if not fn.endswith('.h'):
+            continue
+        text = open(os.path.join(ROOT, 'include', fn)).read()
+        text = re.sub(r'/\*.*?\*/', '', text, flags=re.S)
+        names |= set(re.findall(r'\b(gb_[a-z0-9_]+)\s*\(', text))
+    return names
+
+
+def test_header_declares_entry_points():
+    names = declared()
+    assert {'gb_operator_new', 'gb_operator_apply', 'gb_operator_relax',
+            'gb_transformer_new', 'gb_transformer_apply', 'gb_fd_precond',
+            'gb_poisson_new', 'gb_poisson_solve_neutral'} <= names
+
+
+def test_library_exports_all_symbols():
+    lib = _lib.load()
+    for name in sorted(declared()):
+        assert hasattr(lib, name), name
+        assert name in _lib.SIGNATURES, name
+
+
+def test_library_hides_internal_symbols():
+    import subprocess
+    out = subprocess.run(['nm', '-D', '--defined-only', _lib.LIB_PATH],
+                         capture_output=True, text=True).stdout
+    exported = {l.split()[-1] for l in out.splitlines() if ' T ' in l}
+    gb = {s for s in exported if s.startswith('gb_')}
+    assert gb == declared()
+
+
+def test_errors_map_to_reference_exceptions():
+    lib = _lib.load()
+    h = ctypes.c_void_p()
+    import numpy as np
+    coefs, cp = _lib.f64([1.0])
+    offs, op = _lib.i64([0])
+    size, sp = _lib.i64([4, 4, 4])
+    nb, nbp = _lib.i64([[1, 1], [-1, -1], [-1, -1]])
+    rc = lib.gb_operator_new(cp, op, 1, sp, 1, nbp, 1, 1, ctypes.byref(h))
+    with pytest.raises(ValueError, match='domain decomposition'):
+        _lib.check(rc)

@@ -1,0 +1,315 @@
+"""GPU parity: every CUDA kernel against the oracle (the reference's own C
+core under oracle/_ref, or its numpy restatement), through the C ABI.
+
+Bar: FP64 outputs within 1e-12 relative (max norm) of the oracle; the
+kernels keep the reference's operation order without FMA contraction, so
+the tests also assert the measured difference is exactly 0 where the
+arithmetic is deterministic."""
+import numpy as np
+import pytest
+
+from oracle import gpaw_layer as L
+from tests.helpers import RTOL_FP64, max_rel, to_dev, to_np
+
+pytestmark = pytest.mark.gpu
+KPT = (0.25, 0.0, 0.1)
+
+
+def prod_gd(N, cell, pbc):
+    from gpaw_b200 import GridDescriptor
+    return GridDescriptor(N, cell, pbc)
+
+
+# ------------------------------------------------------------ golden cases
+def test_golden_fd(golden, cuda):
+    from gpaw_b200 import FDOperator
+    n = 0
+    for name, c in golden.items():
+        if not name.startswith('fd_'):
+            continue
+        gd = prod_gd(tuple(c['N']), c['cell'], tuple(c['pbc']))
+        dtype = complex if np.iscomplexobj(c['inp']) else float
+        op = FDOperator(c['coefs'], c['offsets'], gd, dtype)
+        a = to_dev(c['inp'])
+        b = a.new_zeros(a.shape)
+        op.apply(a, b, c.get('phases'))
+        got = to_np(b)
+        assert max_rel(got, c['out']) <= RTOL_FP64, name
+        assert np.array_equal(got, c['out']), name
+        n += 1
+    assert n == 38
+
+
+def test_golden_relax(golden, cuda):
+    from gpaw_b200 import Laplace
+    for name, c in golden.items():
+        if not name.startswith('relax_'):
+            continue
+        m = int(name.split('_')[1][1:])
+        gd = prod_gd(tuple(c['N']), (3.0, 2.6, 3.3), tuple(c['pbc']))
+        op = Laplace(gd, -0.25 / np.pi, 3)
+        f = to_dev(c['f'])
+        op.relax(m, f, to_dev(c['s']), 3, 2.0 / 3.0)
+        assert np.array_equal(to_np(f), c['out']), name
+
+
+def test_golden_transformers(golden, cuda):
+    from gpaw_b200 import Transformer
+    for name, c in golden.items():
+        if not name.startswith('tr_'):
+            continue
+        nn = int(name.split('_')[1][2:])
+        gd = prod_gd(tuple(c['N']), (3.0, 3.4, 3.9), tuple(c['pbc']))
+        gd2 = gd.coarsen()
+        dtype = complex if np.iscomplexobj(c['fine']) else float
+        ph = c.get('phases')
+        r = Transformer(gd, gd2, nn, dtype).apply(to_dev(c['fine']),
+                                                  phases=ph)
+        i = Transformer(gd2, gd, nn, dtype).apply(to_dev(c['coarse']),
+                                                  phases=ph)
+        assert np.array_equal(to_np(r), c['restricted']), name
+        assert np.array_equal(to_np(i), c['interpolated']), name
+
+
+def test_golden_preconditioner(golden, cuda):
+    from gpaw_b200 import Laplace, Preconditioner
+    for name, c in golden.items():
+        if not name.startswith('pc_'):
+            continue
+        gd = prod_gd(tuple(c['N']), (3.0, 3.0, 4.5), tuple(c['pbc']))
+        dtype = complex if np.iscomplexobj(c['res']) else float
+        kin = Laplace(gd, -0.5, 3, dtype)
+        pc = Preconditioner(gd, kin, dtype, block=2)
+        R = to_dev(c['res'])
+        out = R.new_zeros(R.shape)
+        pc(R, c.get('phases'), out=out)
+        assert np.array_equal(to_np(out), c['out']), name
+
+
+def test_golden_poisson(golden, cuda):
+    from gpaw_b200 import FDPoissonSolver
+    for name, c in golden.items():
+        if not name.startswith('ps_'):
+            continue
+        gd = prod_gd(tuple(c['N']), (4.0, 2.0, 4.0), tuple(c['pbc']))
+        ps = FDPoissonSolver(nn=3, eps=1e-18)
+        ps.set_grid_descriptor(gd)
+        phi = gd.zeros()
+        # the neutral branch of solve() (gpaw/poisson.py:186-213), in numpy
+        # so that the right-hand side is bit-identical to the oracle's
+        n = np.prod(c['N'] - 1 + c['pbc'])
+        dv = 4.0 * 2.0 * 4.0 / np.prod(c['N'])
+        rho = c['rho'] - c['rho'].sum() * dv / dv / n
+        niter = ps.solve_neutral(phi, to_dev(rho))
+        assert niter == int(c['niter']), name
+        got = to_np(phi)
+        # the periodic branch subtracts a mean formed by a reduction whose
+        # order differs from numpy's: allow the 1e-12 bar there
+        if c['pbc'].all():
+            assert max_rel(got, c['phi']) <= RTOL_FP64, name
+        else:
+            assert np.array_equal(got, c['phi']), name
+
+
+# -------------------------------------------------- random, larger, batched
+@pytest.mark.parametrize('nn', [1, 2, 3, 4, 5, 6])
+@pytest.mark.parametrize('pbc', [(1, 1, 1), (0, 0, 0), (0, 1, 1)])
+@pytest.mark.parametrize('dtype', [float, complex])
+def test_fd_apply_random(nn, pbc, dtype, cuda):
+    from gpaw_b200 import Laplace
+    rng = np.random.default_rng(nn * 7 + sum(pbc))
+    N = (24, 20, 26)
+    cell = (4.1, 3.3, 4.4)
+    gd = prod_gd(N, cell, pbc)
+    a = rng.standard_normal((3,) + tuple(gd.n_c))
+    if dtype == complex:
+        a = a + 1j * rng.standard_normal(a.shape)
+    ph = gd.phase_factor_cd((0.25, -0.1, 0.4)) if dtype == complex else None
+    ref = np.zeros_like(a)
+    L.Laplace(L.GridDescriptor(N, cell, pbc), -0.5, nn, dtype).apply(a, ref,
+                                                                     ph)
+    op = Laplace(gd, -0.5, nn, dtype)
+    x = to_dev(a)
+    y = x.new_zeros(x.shape)
+    op.apply(x, y, ph)
+    assert max_rel(to_np(y), ref) <= RTOL_FP64
+    assert np.array_equal(to_np(y), ref)
+    # in-place (in is out), as gpaw/new/fd/hamiltonian.py:47-49 calls it
+    op.apply(x, x, ph)
+    assert np.array_equal(to_np(x), ref)
+
+
+def test_fd_nonorthogonal_cell(cuda):
+    from gpaw_b200 import Laplace
+    cell = [(3.0, 0, 0), (1.5, 3.0 * 3**0.5 / 2, 0), (0, 0, 3.2)]
+    for pbc in ((1, 1, 1), (1, 1, 0)):
+        for dtype in (float, complex):
+            gd = prod_gd((18, 18, 16), cell, pbc)
+            rng = np.random.default_rng(3)
+            a = rng.standard_normal((2,) + tuple(gd.n_c))
+            if dtype == complex:
+                a = a + 1j * rng.standard_normal(a.shape)
+            ph = gd.phase_factor_cd(KPT) if dtype == complex else None
+            ref = np.zeros_like(a)
+            L.Laplace(L.GridDescriptor((18, 18, 16), cell, pbc), 1.0, 3,
+                      dtype).apply(a, ref, ph)
+            op = Laplace(gd, 1.0, 3, dtype)
+            assert not op.cfd
+            y = to_dev(a)
+            z = y.new_zeros(y.shape)
+            op.apply(y, z, ph)
+            assert np.array_equal(to_np(z), ref), (pbc, dtype)
+
+
+def test_fd_gaussian_analytic(cuda):
+    """gpaw/test/gpu/test_fd_laplace.py:8-60: against the analytic Laplacian
+    of a Gaussian (interior, 1e-2)."""
+    from gpaw_b200 import Laplace
+    lat = 8.0
+    gd = prod_gd((32, 32, 32), (lat, lat, lat), 0)
+    x, y, z = gd.get_grid_point_coordinates()
+    sigma, mu = 1.5, lat / 2
+    a = np.exp(-((x - mu)**2 + (y - mu)**2 + (z - mu)**2) / (2.0 * sigma))
+    ana = (((x - mu)**2 + (y - mu)**2 + (z - mu)**2) / sigma**2 -
+           3.0 / sigma) * a
+    b = to_dev(np.zeros_like(a))
+    Laplace(gd, 1.0, 3).apply(to_dev(a), b)
+    assert np.abs(to_np(b)[2:-2, 2:-2, 2:-2] - ana[2:-2, 2:-2, 2:-2]).max() \
+        < 1e-2
+
+
+@pytest.mark.parametrize('nn', [1, 2, 3, 4])
+@pytest.mark.parametrize('pbc', [(1, 1, 1), (0, 0, 0), (1, 0, 1)])
+@pytest.mark.parametrize('dtype', [float, complex])
+def test_transformers_random(nn, pbc, dtype, cuda):
+    from gpaw_b200 import Transformer
+    N = (40, 36, 44)
+    cell = (4.0, 3.6, 4.4)
+    gdp = prod_gd(N, cell, pbc)
+    gdo = L.GridDescriptor(N, cell, pbc)
+    rng = np.random.default_rng(nn)
+    ph = gdp.phase_factor_cd((0.3, 0.0, -0.15)) if dtype == complex else None
+
+    def rand(g):
+        a = rng.standard_normal((2,) + tuple(g.n_c))
+        return a + 1j * rng.standard_normal(a.shape) if dtype == complex \
+            else a
+
+    a = rand(gdo)
+    ref = L.Transformer(gdo, gdo.coarsen(), nn, dtype).apply(a, phases=ph)
+    got = Transformer(gdp, gdp.coarsen(), nn, dtype).apply(to_dev(a),
+                                                           phases=ph)
+    assert np.array_equal(to_np(got), ref)
+    c = rand(gdo.coarsen())
+    ref = L.Transformer(gdo.coarsen(), gdo, nn, dtype).apply(c, phases=ph)
+    got = Transformer(gdp.coarsen(), gdp, nn, dtype).apply(to_dev(c),
+                                                           phases=ph)
+    assert np.array_equal(to_np(got), ref)
+
+
+def test_transformers_conserve_integral(cuda):
+    """gpaw/test/fd_ops/test_transformations.py and test_non_periodic.py."""
+    from gpaw_b200 import Transformer
+    rng = np.random.RandomState(8)
+    for pbc, tol in ((1, 1e-14), (0, 1e-10)):
+        gd = prod_gd((20, 20, 20), (8.0, 8.0, 8.0), pbc)
+        a = to_dev(rng.random(tuple(gd.n_c)))
+        for k in (2, 4, 6, 8):
+            if pbc == 0 and k > 2:
+                continue
+            fine = gd.refine()
+            b = Transformer(gd, fine, k // 2).apply(a)
+            assert abs(gd.integrate(a) - fine.integrate(b)) < tol
+            if pbc:
+                coarse = gd.coarsen()
+                b = Transformer(gd, coarse, k // 2).apply(a)
+                assert abs(gd.integrate(a) - coarse.integrate(b)) < tol
+
+
+@pytest.mark.parametrize('method', [1, 2])
+@pytest.mark.parametrize('pbc', [(1, 1, 1), (0, 0, 0)])
+def test_relax_random(method, pbc, cuda):
+    from gpaw_b200 import Laplace
+    N = (24, 22, 20)
+    gd = prod_gd(N, (3.0, 2.8, 2.6), pbc)
+    rng = np.random.default_rng(5)
+    f = rng.standard_normal(tuple(gd.n_c))
+    s = rng.standard_normal(f.shape)
+    ref = f.copy()
+    L.Laplace(L.GridDescriptor(N, (3.0, 2.8, 2.6), pbc), -0.25 / np.pi,
+              3).relax(method, ref, s, 4, 2.0 / 3.0)
+    g = to_dev(f)
+    Laplace(gd, -0.25 / np.pi, 3).relax(method, g, to_dev(s), 4, 2.0 / 3.0)
+    assert np.array_equal(to_np(g), ref)
+
+
+@pytest.mark.parametrize('pbc', [(1, 1, 1), (0, 0, 0)])
+@pytest.mark.parametrize('dtype', [float, complex])
+def test_preconditioner_random(pbc, dtype, cuda):
+    from gpaw_b200 import Laplace, Preconditioner
+    N = (32, 28, 24)
+    cell = (4.0, 3.5, 3.0)
+    gdp = prod_gd(N, cell, pbc)
+    gdo = L.GridDescriptor(N, cell, pbc)
+    rng = np.random.default_rng(11)
+    R = rng.standard_normal((5,) + tuple(gdo.n_c))
+    if dtype == complex:
+        R = R + 1j * rng.standard_normal(R.shape)
+    ph = gdo.phase_factor_cd(KPT) if dtype == complex else None
+    ref = np.zeros_like(R)
+    L.Preconditioner(gdo, L.Laplace(gdo, -0.5, 3, dtype), dtype,
+                     block=2)(R, ph, out=ref)
+    pc = Preconditioner(gdp, Laplace(gdp, -0.5, 3, dtype), dtype, block=2)
+    out = to_dev(np.zeros_like(R))
+    pc(to_dev(R), ph, out=out)
+    assert np.array_equal(to_np(out), ref)
+
+
+@pytest.mark.parametrize('relax', ['J', 'GS'])
+def test_poisson_c1_against_oracle(relax, cuda):
+    """64^3 zero-BC FDPoissonSolver (nn=3): same V-cycle count and the same
+    potential as the reference, to the reference's eps=2e-10."""
+    from gpaw_b200 import FDPoissonSolver
+    h = 0.2 / 0.52917721
+    N = (64, 64, 64) if relax == 'J' else (32, 32, 32)
+    L_ = N[0] * h
+    gdo = L.GridDescriptor(N, (L_,) * 3, 0)
+    gdp = prod_gd(N, (L_,) * 3, 0)
+    x = gdo.get_grid_point_coordinates()
+    rng = np.random.default_rng(1)
+    w = 0.8 / 0.52917721
+    rho = np.zeros(tuple(gdo.n_c))
+    for i in range(8):
+        c = rng.uniform(0.25, 0.75, 3) * L_
+        q = 1.0 if i % 2 == 0 else -1.0
+        r2 = ((x - c[:, None, None, None])**2).sum(0)
+        rho += q * (np.pi * w**2)**-1.5 * np.exp(-r2 / w**2)
+    rho -= rho.mean()
+    ps_o = L.FDPoissonSolver(nn=3, relax=relax, eps=2e-10)
+    ps_o.set_grid_descriptor(gdo)
+    phi_o = gdo.zeros()
+    n_o = ps_o.solve_neutral(phi_o, rho)
+    ps = FDPoissonSolver(nn=3, relax=relax, eps=2e-10)
+    ps.set_grid_descriptor(gdp)
+    phi = gdp.zeros()
+    n = ps.solve_neutral(phi, to_dev(rho))
+    assert n == n_o
+    assert np.array_equal(to_np(phi), phi_o)
+
+
+def test_errors_are_reference_exceptions(cuda):
+    import torch
+    from gpaw_b200 import FDPoissonSolver, Laplace, PoissonConvergenceError
+    gd = prod_gd((16, 16, 16), 3.0, 0)
+    op = Laplace(gd, 1.0, 2)
+    with pytest.raises(TypeError):
+        op.apply(np.zeros(tuple(gd.n_c)), np.zeros(tuple(gd.n_c)))
+    a = gd.zeros(dtype=complex)
+    with pytest.raises(ValueError, match='dtype'):
+        op.apply(a, a.clone())
+    ps = FDPoissonSolver(eps=1e-30, maxiter=3)
+    ps.set_grid_descriptor(gd)
+    rho = torch.randn(tuple(gd.n_c), dtype=torch.float64, device='cuda')
+    rho -= rho.mean()
+    with pytest.raises(PoissonConvergenceError):
+        ps.solve_neutral(gd.zeros(), rho)

@@ -1,0 +1,148 @@
+"""Host-side logic of gpaw_b200 against the oracle's restatement of the
+reference's Python layer: stencil coefficients, grid conventions,
+transformer geometry, multigrid schedule.  No GPU needed."""
+import numpy as np
+import pytest
+
+from oracle import gpaw_layer as L
+from oracle import port
+
+CELLS = {
+    'sc': (1.1, 1.02, 1.03),
+    'hexagonal': [(1, 0, 0), (0.5, 3**0.5 / 2, 0), (0, 0, 1.1)],
+    'fcc': [(0, 1, 1), (1, 0, 1), (1, 1, 0)],
+    'bcc': [(-1, 1, 1), (1, -1, 1), (1, 1, -1)],
+    'distorted sc': [(1, 0, 0), (0.01, 1, 0), (0, 0.02, 1)],
+}
+
+
+@pytest.mark.parametrize('cell', sorted(CELLS))
+@pytest.mark.parametrize('n', range(1, 7))
+def test_laplace_coefficients_match(cell, n):
+    from gpaw_b200.fd_operators import laplace_stencil
+    from gpaw_b200.grid_descriptor import GridDescriptor
+    N = (2 * n + 2,) * 3
+    c1, o1 = laplace_stencil(GridDescriptor(N, CELLS[cell], device='cpu'),
+                             -0.5, n)
+    c2, o2 = L.laplace_stencil(L.GridDescriptor(N, CELLS[cell]), -0.5, n)
+    assert np.array_equal(np.array(c1), np.array(c2))
+    assert np.array_equal(np.array(o1), np.array(o2))
+
+
+@pytest.mark.parametrize('cell,D', [('sc', 3), ('hexagonal', 4), ('fcc', 6),
+                                    ('bcc', 4), ('distorted sc', 6)])
+@pytest.mark.parametrize('n', range(1, 5))
+def test_laplace_exact_on_polynomials(cell, D, n):
+    """Known-answer test of gpaw/test/fd_ops/test_laplace.py:15-103: the
+    stencil is exact on polynomials of degree <= 2n at the central point;
+    the product's coefficients are applied by the oracle."""
+    from gpaw_b200.fd_operators import laplace_stencil
+    from gpaw_b200.grid_descriptor import GridDescriptor
+    N = 2 * n + 2
+    gdp = GridDescriptor((N, N, N), CELLS[cell], device='cpu')
+    coefs, offsets = laplace_stencil(gdp, 1.0, n)
+    assert len(coefs) == D * 2 * n + 1
+    gd = L.GridDescriptor((N, N, N), CELLS[cell])
+    op = L.FDOperator(coefs, offsets, gd, be='port')
+    r_gv = gd.get_grid_point_coordinates().transpose((1, 2, 3, 0))
+    r_gv = r_gv - gd.cell_cv.sum(0) / 2
+    b = gd.zeros()
+    for m in range(0, 2 * n + 1):
+        for ix in range(m + 1):
+            for iy in range(m - ix + 1):
+                iz = m - ix - iy
+                a = (r_gv**(ix, iy, iz)).prod(3)
+                r = 2.0 if (m == 2 and max(ix, iy, iz) == 2) else 0.0
+                op.apply(a, b)
+                assert abs(b[n + 1, n + 1, n + 1] - r) < 2e-12
+
+
+@pytest.mark.parametrize('N,pbc', [((64, 64, 64), 0), ((96, 96, 96), 1),
+                                   ((40, 32, 128), 0), ((2, 4, 6), 1),
+                                   ((2, 2, 2), 0)])
+def test_grid_conventions(N, pbc):
+    from gpaw_b200.grid_descriptor import GridDescriptor
+    g1 = GridDescriptor(N, (5.0, 6.0, 7.0), pbc, device='cpu')
+    g2 = L.GridDescriptor(N, (5.0, 6.0, 7.0), pbc)
+    for attr in ('N_c', 'n_c', 'beg_c', 'end_c', 'neighbor_cd'):
+        assert np.array_equal(getattr(g1, attr), getattr(g2, attr)), attr
+    assert g1.dv == g2.dv
+    assert np.array_equal(g1.get_size_of_global_array(), g2.n_c)
+    # coarsening stops where the reference stops (gpaw/poisson.py:393-397)
+    levels = [0, 0]
+    for i, g in enumerate((g1, g2)):
+        while True:
+            try:
+                g = g.coarsen()
+            except ValueError:
+                break
+            levels[i] += 1
+    assert levels[0] == levels[1]
+
+
+def test_poisson_hierarchy_64_zero():
+    """64^3 zero BC: 6 grids, coarsest N = 2 (one unknown per axis)."""
+    from gpaw_b200.grid_descriptor import GridDescriptor
+    g = GridDescriptor((64, 64, 64), 1.0, 0, device='cpu')
+    sizes = [int(g.n_c[0])]
+    while True:
+        try:
+            g = g.coarsen()
+        except ValueError:
+            break
+        sizes.append(int(g.n_c[0]))
+    assert sizes == [63, 31, 15, 7, 3, 1]
+
+
+@pytest.mark.parametrize('nn', [1, 2, 3, 4])
+@pytest.mark.parametrize('pbc', [(1, 1, 1), (0, 0, 0), (1, 0, 1)])
+def test_transformer_geometry(nn, pbc):
+    from gpaw_b200.grid_descriptor import GridDescriptor
+    from gpaw_b200.transformers import transformer_geometry
+    N = (32, 28, 24)
+    a1, a2 = (GridDescriptor(N, 3.0, pbc, device='cpu'),
+              L.GridDescriptor(N, 3.0, pbc))
+    for fwd in (True, False):
+        g1 = (a1, a1.coarsen()) if fwd else (a1.coarsen(), a1)
+        g2 = (a2, a2.coarsen()) if fwd else (a2.coarsen(), a2)
+        r1 = transformer_geometry(*g1, nn)
+        r2 = L.transformer_geometry(*g2, nn)
+        for x, y in zip(r1, r2):
+            assert np.array_equal(np.asarray(x), np.asarray(y))
+
+
+def test_interpolator_guard():
+    from gpaw_b200.grid_descriptor import GridDescriptor
+    from gpaw_b200.transformers import transformer_geometry
+    gd = GridDescriptor((4, 4, 4), 1.0, 0, device='cpu')
+    with pytest.raises(ValueError, match='Cannot construct interpolator'):
+        transformer_geometry(gd.coarsen(), gd, 3)
+
+
+def test_lagrange_weights_are_the_reference_constants():
+    # c/bmgs/restrict.cpp:37-57 and c/bmgs/interpolate.cpp:29-40
+    assert port.lagrange_midpoint_weights(2) == [0.5]
+    assert port.lagrange_midpoint_weights(4) == [0.5625, -0.0625]
+    assert port.lagrange_midpoint_weights(6) == [0.58593750, -0.09765625,
+                                                 0.01171875]
+    assert port.lagrange_midpoint_weights(8) == [
+        0.59814453125, -0.11962890625, 0.02392578125, -0.00244140625]
+
+
+def test_cgpaw_objects_build_without_gpu():
+    """Operator / Transformer construction is host-only (no CUDA call)."""
+    from gpaw_b200 import cgpaw
+    from gpaw_b200.fd_operators import laplace_stencil
+    from gpaw_b200.grid_descriptor import GridDescriptor
+    gd = GridDescriptor((16, 16, 16), 3.0, 1, device='cpu')
+    coefs, offs = laplace_stencil(gd, -0.5, 3)
+    M = gd.n_c + 6
+    offp = np.dot(np.array(offs), [M[1] * M[2], M[2], 1])
+    op = cgpaw.Operator(coefs, offp, gd.n_c, 3, gd.neighbor_cd, 1, None, 1)
+    assert op.get_diagonal_element() == coefs[0]
+    with pytest.raises(ValueError):
+        cgpaw.Operator(coefs, offp * 1000, gd.n_c, 3, gd.neighbor_cd, 1,
+                       None, 1)
+    with pytest.raises(NotImplementedError):
+        cgpaw.Operator(coefs, offp, gd.n_c, 3, gd.neighbor_cd, 1, object(),
+                       1)

@@ -1,0 +1,112 @@
+"""Pin the numpy restatement of the oracle (oracle/port.py) to the golden
+vectors produced by the reference's own C core (tests/golden/)."""
+import numpy as np
+import pytest
+
+from oracle import gpaw_layer as L
+
+KPT = (0.25, 0.0, 0.1)
+
+
+def _gd(c, cell=None):
+    return L.GridDescriptor(tuple(c['N']), cell if cell is not None else
+                            c.get('cell', (3.1, 2.9, 3.5)), tuple(c['pbc']))
+
+
+def test_fd_cases(golden):
+    n = 0
+    for name, c in golden.items():
+        if not name.startswith('fd_'):
+            continue
+        nn = int(name.split('_')[1][2:]) if name.startswith('fd_nn') else 2
+        cell = c['cell']
+        gd = L.GridDescriptor(tuple(c['N']), cell, tuple(c['pbc']))
+        dtype = complex if np.iscomplexobj(c['inp']) else float
+        op = L.Laplace(gd, -0.5, nn, dtype, be='port')
+        assert np.array_equal(op.coef_p, c['coefs']), name
+        out = np.zeros_like(c['inp'])
+        op.apply(c['inp'], out, c.get('phases'))
+        assert np.array_equal(out, c['out']), name
+        n += 1
+    assert n == 38
+
+
+def test_relax_cases(golden):
+    for name, c in golden.items():
+        if not name.startswith('relax_'):
+            continue
+        m = int(name.split('_')[1][1:])
+        gd = L.GridDescriptor(tuple(c['N']), (3.0, 2.6, 3.3), tuple(c['pbc']))
+        op = L.Laplace(gd, -0.25 / np.pi, 3, be='port')
+        f = c['f'].copy()
+        op.relax(m, f, c['s'], 3, 2.0 / 3.0)
+        assert np.array_equal(f, c['out']), name
+
+
+def test_transformer_cases(golden):
+    n = 0
+    for name, c in golden.items():
+        if not name.startswith('tr_'):
+            continue
+        nn = int(name.split('_')[1][2:])
+        gd = L.GridDescriptor(tuple(c['N']), (3.0, 3.4, 3.9), tuple(c['pbc']))
+        gd2 = gd.coarsen()
+        dtype = complex if np.iscomplexobj(c['fine']) else float
+        ph = c.get('phases')
+        r = L.Transformer(gd, gd2, nn, dtype, be='port').apply(c['fine'],
+                                                              phases=ph)
+        i = L.Transformer(gd2, gd, nn, dtype, be='port').apply(c['coarse'],
+                                                              phases=ph)
+        assert np.array_equal(r, c['restricted']), name
+        assert np.array_equal(i, c['interpolated']), name
+        n += 1
+    assert n == 21
+
+
+def test_preconditioner_cases(golden):
+    for name, c in golden.items():
+        if not name.startswith('pc_'):
+            continue
+        gd = L.GridDescriptor(tuple(c['N']), (3.0, 3.0, 4.5), tuple(c['pbc']))
+        dtype = complex if np.iscomplexobj(c['res']) else float
+        kin = L.Laplace(gd, -0.5, 3, dtype, be='port')
+        pc = L.Preconditioner(gd, kin, dtype, block=2, be='port')
+        out = np.zeros_like(c['res'])
+        pc(c['res'], c.get('phases'), out=out)
+        assert np.array_equal(out, c['out']), name
+
+
+def test_poisson_cases(golden):
+    for name, c in golden.items():
+        if not name.startswith('ps_'):
+            continue
+        gd = L.GridDescriptor(tuple(c['N']), (4.0, 2.0, 4.0), tuple(c['pbc']))
+        ps = L.FDPoissonSolver(nn=3, eps=1e-18, be='port')
+        ps.set_grid_descriptor(gd)
+        phi = gd.zeros()
+        niter = ps.solve(phi, c['rho'])
+        assert niter == int(c['niter']), name
+        assert np.array_equal(phi, c['phi']), name
+        assert np.array_equal(np.array(ps.errors), c['errors']), name
+
+
+@pytest.mark.skipif(L._REF is None, reason='reference core not built')
+def test_port_equals_reference_random():
+    """Wider random sweep, port vs the compiled reference, bit for bit."""
+    rng = np.random.default_rng(7)
+    for nn in range(1, 7):
+        for pbc in [(1, 1, 1), (0, 0, 0), (0, 1, 1)]:
+            for dtype in (float, complex):
+                gd = L.GridDescriptor((14, 13, 15), (3.1, 2.9, 3.5), pbc)
+                a = rng.standard_normal((2,) + tuple(gd.n_c))
+                if dtype == complex:
+                    a = a + 1j * rng.standard_normal(a.shape)
+                ph = gd.phase_factor_cd((0.1, -0.2, 0.3)) \
+                    if dtype == complex else None
+                outs = []
+                for be in ('ref', 'port'):
+                    op = L.Laplace(gd, 0.7, nn, dtype, be=be)
+                    b = np.zeros_like(a)
+                    op.apply(a, b, ph)
+                    outs.append(b)
+                assert np.array_equal(*outs), (nn, pbc, dtype)
