@@ -1,0 +1,377 @@
+"""Benchmark: batched Bloch-periodic kinetic operator + restrict/interpolate.
+
+Workload (one "step"): 256 complex128 wave functions on a 96^3 periodic
+grid, Bloch phases at k = (0.25, 0, 0.1), kinetic operator -1/2 Laplacian
+(nn = 3, 19 points) applied to the whole batch, then Transformer restrict
+(order 3, 96^3 -> 48^3) and interpolate (48^3 -> 96^3) of the same batch.
+Inputs are N(0,1) + i N(0,1) from a fixed seed (synthetic).
+
+Metric: FD-stencil GB/s = algorithmic bytes per step / device time, with
+algorithmic bytes = every input read once + every output written once
+(apply 32 B per point, restrict and interpolate 18 B per fine point).
+Arrays are 3.6 GB each, far larger than L2, so no flush is needed.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+With N > 1 (torchrun, one process per GPU) every rank runs its own batch
+(independent replicas, weak scaling); rank 0 prints the JSON line with the
+whole-job GB/s over the max of the per-rank device times.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NBANDS = 256
+N = (96, 96, 96)
+CELL = (96 * 0.2 / 0.52917721,) * 3
+KPT = (0.25, 0.0, 0.1)
+METRIC = 'FD-stencil GB/s (kinetic nn=3 apply + restrict + interpolate)'
+WORKLOAD = ('kinetic -0.5*Lap nn=3 on 256 complex128 96^3 periodic, Bloch '
+            'k=(0.25,0,0.1) + Transformer restrict/interpolate nn=3')
+
+
+def set_batch(nb):
+    global NBANDS
+    NBANDS = int(nb)
+
+
+def algorithmic_bytes(nb=None):
+    nb = NBANDS if nb is None else nb
+    pts = nb * N[0] * N[1] * N[2]
+    apply_b = 32 * pts
+    restrict_b = 16 * pts + 16 * pts // 8
+    interp_b = 16 * pts // 8 + 16 * pts
+    return apply_b, restrict_b, interp_b
+
+
+def measured_peak():
+    path = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    try:
+        with open(path) as f:
+            return float(json.load(f)['hbm_gbs']), 'measured'
+    except (OSError, KeyError, ValueError):
+        return 6650.0, 'fallback'
+
+
+def ncu_traffic():
+    """DRAM bytes per apply launch from the committed ncu summary."""
+    path = os.path.join(ROOT, 'profiles', 'fd_apply_c128_96cube.txt')
+    try:
+        for line in open(path):
+            if line.startswith('dram_bytes_per_launch_full_batch:'):
+                return float(line.split(':')[1])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed
+    region (every 200 ms)."""
+
+    Q = ('index,clocks.sm,clocks.max.sm,power.draw,'
+         'clocks_event_reasons.hw_slowdown,'
+         'clocks_event_reasons.hw_thermal_slowdown,'
+         'clocks_event_reasons.sw_thermal_slowdown,'
+         'clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ['nvidia-smi', f'--id={self.index}',
+                 f'--query-gpu={self.Q}', '--format=csv,noheader,nounits',
+                 '-lms', '200'], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            out, _ = self.proc.communicate(timeout=10)
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown',
+                 'sw_power_cap']
+        for l in getattr(self, 'lines', []):
+            f = [x.strip() for x in l.split(',')]
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except (ValueError, IndexError):
+                continue
+            for n, v in zip(names, f[4:8]):
+                if v.lower().startswith('active'):
+                    reasons.add(n)
+        return {'sm_mhz': float(np.median(sm)) if sm else None,
+                'sm_max_mhz': smax, 'reasons': sorted(reasons),
+                'samples': len(sm)}
+
+
+def make_batch(nb, seed=0):
+    rng = np.random.default_rng(seed)
+    shape = (nb,) + N
+    a = np.empty(shape, complex)
+    a.real = rng.standard_normal(shape)
+    a.imag = rng.standard_normal(shape)
+    return a
+
+
+# --------------------------------------------------------------- CPU sides
+CPU_SAMPLE = 16   # wave functions per CPU step (bounded sample)
+
+
+def cpu_step_child(nb, reps):
+    """Run inside a fresh process: time the reference's own C core
+    (oracle/_ref) on `nb` wave functions, `reps` times; print JSON."""
+    from oracle import gpaw_layer as L
+    kind = 'reference' if L._REF is not None else 'port'
+    gd = L.GridDescriptor(N, CELL, 1)
+    gd2 = gd.coarsen()
+    ph = gd.phase_factor_cd(KPT)
+    kin = L.Laplace(gd, -0.5, 3, complex)
+    rst = L.Transformer(gd, gd2, 3, complex)
+    itp = L.Transformer(gd2, gd, 3, complex)
+    a = make_batch(nb, seed=1)
+    b = np.empty_like(a)
+    c = np.empty((nb,) + tuple(gd2.n_c), complex)
+    d = np.empty_like(a)
+    times = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        kin.apply(a, b, ph)
+        rst.apply(a, c, phases=ph)
+        itp.apply(c, d, phases=ph)
+        times.append(time.perf_counter() - t0)
+    print(json.dumps({'kind': kind, 'times': times, 'nb': nb}))
+
+
+def cpu_measure(nb=CPU_SAMPLE, reps=3):
+    cores = len(os.sched_getaffinity(0))
+    env = dict(os.environ, OMP_NUM_THREADS=str(cores), CUDA_VISIBLE_DEVICES='')
+    out = subprocess.run(
+        [sys.executable, os.path.abspath(__file__), '--_cpu-child', str(nb),
+         str(reps)], env=env, capture_output=True, text=True, check=True,
+        cwd=ROOT).stdout
+    r = json.loads(out.strip().splitlines()[-1])
+    t = float(np.median(r['times']))
+    gbs = sum(algorithmic_bytes(nb)) / t / 1e9
+    return {'value': gbs, 'unit': 'GB/s', 'cores': cores, 'kind': r['kind'],
+            'sample': f'{nb} of {NBANDS} wave functions per step, median of '
+                      f'{reps} steps ({t * 1e3:.1f} ms each), OpenMP over the '
+                      f'batch with {cores} threads'}
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU implementation of the path."""
+    rank = int(os.environ.get('RANK', '0'))
+    if rank != 0:
+        return
+    steps, warm = args.steps, args.warmup
+    cb = cpu_measure(CPU_SAMPLE, reps=max(1, min(steps, 3)))
+    line = {'metric': METRIC, 'value': cb['value'], 'unit': 'GB/s',
+            'n_gpus': args.gpus, 'steps': steps, 'warmup': warm,
+            'ms_per_step': sum(algorithmic_bytes(CPU_SAMPLE)) /
+            (cb['value'] * 1e9) * 1e3,
+            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+            'dtype': 'c128', 'data': 'synthetic',
+            'config': {'workload': WORKLOAD, 'batch': NBANDS,
+                       'grid': list(N), 'sample_batch': CPU_SAMPLE},
+            'impl': 'reference', 'cpu_baseline': cb,
+            'e2e': {'value': cb['value'], 'unit': 'GB/s',
+                    'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- GPU side
+def run_gpu(args):
+    import torch
+    import torch.distributed as dist
+
+    from gpaw_b200 import GridDescriptor, Laplace, Transformer
+
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    torch.cuda.set_device(local)
+    dev = torch.device('cuda', local)
+    if world > 1:
+        import datetime
+        dist.init_process_group('nccl', timeout=datetime.timedelta(
+            seconds=120), device_id=dev)
+
+    # CPU baseline before any heavy GPU work (rank 0, N = 1 only)
+    cpu_base = cpu_measure() if (rank == 0 and world == 1 and
+                                 not args.no_cpu) else None
+
+    gd = GridDescriptor(N, CELL, 1, device=dev)
+    gd2 = gd.coarsen()
+    ph = gd.phase_factor_cd(KPT)
+    kin = Laplace(gd, -0.5, 3, complex)
+    rst = Transformer(gd, gd2, 3, complex)
+    itp = Transformer(gd2, gd, 3, complex)
+
+    host = make_batch(NBANDS, seed=rank)
+    x = torch.from_numpy(host).to(dev)
+    y = torch.empty_like(x)
+    c = torch.empty((NBANDS,) + tuple(gd2.n_c), dtype=torch.complex128,
+                    device=dev)
+    z = torch.empty_like(x)
+    stream = torch.cuda.current_stream()
+
+    def step(ev=None):
+        if ev is not None:
+            ev[0].record(stream)
+        kin.apply(x, y, ph)
+        if ev is not None:
+            ev[1].record(stream)
+        rst.apply(x, c, phases=ph)
+        if ev is not None:
+            ev[2].record(stream)
+        itp.apply(c, z, phases=ph)
+        if ev is not None:
+            ev[3].record(stream)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)]
+           for _ in range(args.steps)]
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        t_start.record(stream)
+        for k in range(args.steps):
+            step(evs[k])
+        t_end.record(stream)
+        barrier()
+    elapsed = t_start.elapsed_time(t_end) / 1e3
+    apply_s = [e[0].elapsed_time(e[1]) / 1e3 for e in evs]
+    rst_s = [e[1].elapsed_time(e[2]) / 1e3 for e in evs]
+    itp_s = [e[2].elapsed_time(e[3]) / 1e3 for e in evs]
+    if world > 1:
+        t = torch.tensor([elapsed], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+
+    ab, rb, ib = algorithmic_bytes()
+    per_step = ab + rb + ib
+    value = world * per_step * args.steps / elapsed / 1e9
+
+    # end-to-end through the public API: pinned host in, results back out
+    e2e = None
+    if not args.no_e2e:
+        hin = torch.from_numpy(host).pin_memory()
+        hy = torch.empty(y.shape, dtype=y.dtype).pin_memory()
+        hz = torch.empty(z.shape, dtype=z.dtype).pin_memory()
+        hc = torch.empty(c.shape, dtype=c.dtype).pin_memory()
+        e_steps = max(1, min(3, args.steps))
+
+        def e2e_step():
+            x.copy_(hin, non_blocking=True)
+            step()
+            hy.copy_(y, non_blocking=True)
+            hc.copy_(c, non_blocking=True)
+            hz.copy_(z, non_blocking=True)
+
+        e2e_step()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(e_steps):
+            e2e_step()
+        e1.record(stream)
+        barrier()
+        et = e0.elapsed_time(e1) / 1e3
+        if world > 1:
+            t = torch.tensor([et], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            et = float(t.item())
+        e2e = {'value': world * per_step * e_steps / et / 1e9, 'unit': 'GB/s',
+               'h2d_bytes_per_step': int(x.numel() * 16),
+               'd2h_bytes_per_step': int((y.numel() + c.numel() +
+                                          z.numel()) * 16)}
+
+    peak, peak_src = measured_peak()
+    apply_t = float(np.mean(apply_s))
+    achieved = ab / apply_t / 1e9
+    line = {
+        'metric': METRIC, 'value': value, 'unit': 'GB/s', 'n_gpus': world,
+        'steps': args.steps, 'warmup': args.warmup,
+        'ms_per_step': elapsed / args.steps * 1e3,
+        'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+        'dtype': 'c128', 'data': 'synthetic',
+        'config': {'workload': WORKLOAD, 'batch': NBANDS, 'grid': list(N),
+                   'parallelism': f'replicas x{world}',
+                   'l2': 'inputs 3.6 GB per array, larger than L2 (no flush)'},
+        'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak,
+                     'unit': 'GB/s', 'frac': achieved / peak,
+                     'traffic': ncu_traffic(), 'kernel': 'fd apply c128',
+                     'peak_source': peak_src},
+        'kernels_ms': {'apply': apply_t * 1e3,
+                       'restrict': float(np.mean(rst_s)) * 1e3,
+                       'interpolate': float(np.mean(itp_s)) * 1e3},
+        'kernels_gbs': {'apply': achieved,
+                        'restrict': rb / float(np.mean(rst_s)) / 1e9,
+                        'interpolate': ib / float(np.mean(itp_s)) / 1e9},
+        'gpu_launches': 3 * args.steps,
+        'clocks': clk.summary(),
+        'e2e': e2e,
+        'cpu_baseline': cpu_base,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    if len(sys.argv) > 1 and sys.argv[1] == '--_cpu-child':
+        cpu_step_child(int(sys.argv[2]), int(sys.argv[3]))
+        return
+    p = argparse.ArgumentParser()
+    p.add_argument('--gpus', type=int, default=1)
+    p.add_argument('--steps', type=int, default=10)
+    p.add_argument('--warmup', type=int, default=3)
+    p.add_argument('--impl', default='gpaw_b200')
+    p.add_argument('--no-cpu', action='store_true')
+    p.add_argument('--no-e2e', action='store_true')
+    p.add_argument('--batch', type=int, default=NBANDS,
+                   help='wave functions per step (profiling runs only)')
+    args = p.parse_args()
+    set_batch(args.batch)
+    if args.impl == 'reference':
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == '__main__':
+    main()

@@ -1,7 +1,9 @@
 // C ABI of gpaw_b200 (declared in include/gpaw_b200.h): object lifetimes,
 // argument checks that mirror the reference's, and the host-side sequencing
 // of the kernels in gb_fd.cu and gb_transform.cu.
+#include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -92,9 +94,58 @@ struct gb_operator {
     GridBC g;
     int real;
     double diag;
+    CfdStencil cs;     // axis-aligned form, when the stencil has one
+    int nn = 0;        // its half-width
+    int tiled = 0;     // use the plane-marching kernels
     Scratch scratch;   // aliasing stage / Jacobi ping-pong / GS snapshot
+    Scratch partial;   // per-CTA partial sums of |r|^2
     long long ng() const { return (long long)g.n[0] * g.n[1] * g.n[2]; }
 };
+
+// Partial sums produced per grid by a residual sweep of `op`.
+static int op_resid_blocks(const gb_operator* op, int nin, int es) {
+    return op->tiled ? cfd_blocks(op->g, op->nn, es, nin) : residual_blocks(op->g);
+}
+
+// One pass of the stencil with a fused epilogue; plane-marching kernel for
+// axis-aligned stencils, the generic one otherwise.
+static int op_sweep(gb_operator* op, int mode, const void* in, void* out, const void* aux,
+                    int nin, int dtype, const Phases& P, double w, double sc, int negate,
+                    double* partial, cudaStream_t st) {
+    if (op->tiled) {
+        Epi ep{aux, w, sc, negate, partial};
+        int rc = (dtype == GB_F64)
+                     ? launch_fd_cfd<double>(mode, in, out, nin, op->g, P, op->cs, op->nn, ep, st,
+                                             nullptr)
+                     : launch_fd_cfd<double2>(mode, in, out, nin, op->g, P, op->cs, op->nn, ep,
+                                              st, nullptr);
+        if (rc == -2) return fail(GB_ECUDA, "could not raise the shared-memory limit");
+        if (rc == 0) return 0;
+    }
+    switch (mode) {
+        case EPI_APPLY:
+            if (dtype == GB_F64) launch_fd<double>(in, out, nin, op->g, P, op->st, st);
+            else launch_fd<double2>(in, out, nin, op->g, P, op->st, st);
+            break;
+        case EPI_RESID:
+            if (dtype == GB_F64)
+                launch_residual<double>(in, aux, out, nin, op->g, P, op->st, partial, st);
+            else
+                launch_residual<double2>(in, aux, out, nin, op->g, P, op->st, partial, st);
+            break;
+        case EPI_JACOBI:
+            launch_jacobi((const double*)in, (double*)out, (const double*)aux, op->g, op->st, w,
+                          st);
+            break;
+        case EPI_PRECOND:
+            if (dtype == GB_F64)
+                launch_precond_step<double>(in, aux, out, nin, op->g, P, op->st, sc, negate, st);
+            else
+                launch_precond_step<double2>(in, aux, out, nin, op->g, P, op->st, sc, negate, st);
+            break;
+    }
+    return 0;
+}
 
 extern "C" int gb_operator_new(const double* coefs, const int64_t* offsets, int ncoefs,
                                const int64_t size[3], int range, const int64_t neighbors[6],
@@ -156,6 +207,9 @@ extern "C" int gb_operator_new(const double* coefs, const int64_t* offsets, int 
         op->st.flat[p] = (o0 * size[1] + o1) * size[2] + o2;
         if (f == 0) op->diag = coefs[p];
     }
+    const char* path = getenv("GPAW_B200_FD_PATH");
+    const bool force_generic = path && strcmp(path, "generic") == 0;
+    op->tiled = (!force_generic && to_cfd_stencil(op->st, op->cs, op->nn)) ? 1 : 0;
     *out = op;
     return 0;
 }
@@ -193,10 +247,8 @@ extern "C" int gb_operator_apply(gb_operator* op, const void* in, void* out, int
         GB_CUDA_TRY(cudaMemcpyAsync(op->scratch.ptr, in, bytes, cudaMemcpyDeviceToDevice, st));
         in = op->scratch.ptr;
     }
-    if (dtype == GB_F64)
-        launch_fd<double>(in, out, (int)nin, op->g, P, op->st, st);
-    else
-        launch_fd<double2>(in, out, (int)nin, op->g, P, op->st, st);
+    if (int rc = op_sweep(op, EPI_APPLY, in, out, nullptr, (int)nin, dtype, P, 0, 0, 0, nullptr, st))
+        return rc;
     GB_LAUNCH_CHECK();
     return 0;
 }
@@ -214,15 +266,13 @@ extern "C" int gb_operator_residual(gb_operator* op, const void* phi, const void
     if (r && (ranges_overlap(phi, r, bytes)))
         return fail(GB_EINVAL, "residual: r must not overlap phi");
     double* partial = nullptr;
-    const int nblk = residual_blocks(op->g);
+    const int nblk = op_resid_blocks(op, (int)nin, (int)elem_size(dtype));
     if (norm2) {
-        if (int e = op->scratch.ensure((size_t)nin * nblk * sizeof(double))) return e;
-        partial = (double*)op->scratch.ptr;
+        if (int e = op->partial.ensure((size_t)nin * nblk * sizeof(double))) return e;
+        partial = (double*)op->partial.ptr;
     }
-    if (dtype == GB_F64)
-        launch_residual<double>(phi, rho, r, (int)nin, op->g, P, op->st, partial, st);
-    else
-        launch_residual<double2>(phi, rho, r, (int)nin, op->g, P, op->st, partial, st);
+    if (int rc = op_sweep(op, EPI_RESID, phi, r, rho, (int)nin, dtype, P, 0, 0, 0, partial, st))
+        return rc;
     GB_LAUNCH_CHECK();
     if (norm2) {
         launch_reduce_partials(partial, nblk, (int)nin, scale, norm2, st);
@@ -263,9 +313,12 @@ static int relax_impl(gb_operator* op, int method, double* f, const double* s, i
         GB_CUDA_TRY(cudaMemcpyAsync(X, f, bytes, cudaMemcpyDeviceToDevice, st));
         src = X;
     }
+    Phases P0;
+    memset(&P0, 0, sizeof P0);
     for (int it = 0; it < nrelax; it++) {
         double* dst = (src == f) ? X : f;
-        launch_jacobi(src, dst, s, op->g, op->st, w, st);
+        if (int rc = op_sweep(op, EPI_JACOBI, src, dst, s, 1, GB_F64, P0, w, 0, 0, nullptr, st))
+            return rc;
         src = dst;
     }
     GB_LAUNCH_CHECK();
@@ -422,10 +475,7 @@ extern "C" int gb_fd_precond(gb_transformer* rest0, gb_transformer* rest1, gb_tr
     const double s4 = 4 * step, s16 = 16 * step;
     auto step_launch = [&](gb_operator* op, const void* d, const void* r, void* o, double sc,
                            int negate) {
-        if (dtype == GB_F64)
-            launch_precond_step<double>(d, r, o, n, op->g, P, op->st, sc, negate, st);
-        else
-            launch_precond_step<double2>(d, r, o, n, op->g, P, op->st, sc, negate, st);
+        return op_sweep(op, EPI_PRECOND, d, o, r, n, dtype, P, 0, sc, negate, nullptr, st);
     };
     int rc;
     // r1 = restrict(-R); d1 = 4 s r1
@@ -435,24 +485,21 @@ extern "C" int gb_fd_precond(gb_transformer* rest0, gb_transformer* rest1, gb_tr
         rc = transform_impl(rest0, residuals, r1, d1, nin, dtype, P, 1, 0, s4, st);
     if (rc) return rc;
     // q1 = K1 d1 - r1; r2 = restrict(q1); d2 = 16 s r2
-    if (dtype == GB_F64)
-        launch_residual<double>(d1, r1, q1, n, kin1->g, P, kin1->st, nullptr, st);
-    else
-        launch_residual<double2>(d1, r1, q1, n, kin1->g, P, kin1->st, nullptr, st);
+    if ((rc = op_sweep(kin1, EPI_RESID, d1, q1, r1, n, dtype, P, 0, 0, 0, nullptr, st))) return rc;
     GB_LAUNCH_CHECK();
     if ((rc = transform_impl(rest1, q1, r2, d2, nin, dtype, P, 0, 0, s16, st))) return rc;
     // d2' = d2 - 16 s (K2 d2 - r2)   (into q2)
-    step_launch(kin2, d2, r2, q2, s16, 0);
+    if ((rc = step_launch(kin2, d2, r2, q2, s16, 0))) return rc;
     GB_LAUNCH_CHECK();
     // d1 -= interpolate(d2')
     if ((rc = transform_impl(intp2, q2, d1, nullptr, nin, dtype, P, 0, 1, 0.0, st))) return rc;
     // d1' = d1 - 4 s (K1 d1 - r1)   (into q1)
-    step_launch(kin1, d1, r1, q1, s4, 0);
+    if ((rc = step_launch(kin1, d1, r1, q1, s4, 0))) return rc;
     GB_LAUNCH_CHECK();
     // q0 = interpolate(-d1')
     if ((rc = transform_impl(intp1, q1, q0, nullptr, nin, dtype, P, 1, 0, 0.0, st))) return rc;
     // d0 = -(q0 - s (K0 q0 - R))
-    step_launch(kin0, q0, residuals, d0, step, 1);
+    if ((rc = step_launch(kin0, q0, residuals, d0, step, 1))) return rc;
     GB_LAUNCH_CHECK();
     return 0;
 }
@@ -537,7 +584,7 @@ extern "C" int gb_poisson_new(int nlevels, gb_operator* const* operators,
             return rc;
         }
     }
-    const int nblk = residual_blocks(p->ops[0]->g);
+    const int nblk = std::max(residual_blocks(p->ops[0]->g), op_resid_blocks(p->ops[0], 1, 8));
     cudaError_t e = cudaMalloc(&p->partial, (size_t)nblk * sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&p->err_dev, sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&p->mean_dev, sizeof(double));
@@ -560,7 +607,9 @@ static int vcycle(gb_poisson* p, int l, cudaStream_t st) {
     if (l < p->L) {
         if (int rc = relax_impl(op, p->method, p->phi[l], p->rho[l], p->pre[l], p->w[l], st))
             return rc;
-        launch_residual<double>(p->phi[l], p->rho[l], p->res[l], 1, op->g, P, op->st, nullptr, st);
+        if (int rc = op_sweep(op, EPI_RESID, p->phi[l], p->res[l], p->rho[l], 1, GB_F64, P, 0, 0, 0,
+                              nullptr, st))
+            return rc;
         GB_LAUNCH_CHECK();
         if (int rc = transform_impl(p->rst[l], p->res[l], p->rho[l + 1], nullptr, 1, GB_F64, P, 0,
                                     0, 0.0, st))
@@ -576,9 +625,10 @@ static int vcycle(gb_poisson* p, int l, cudaStream_t st) {
     if (int rc = relax_impl(op, p->method, p->phi[l], p->rho[l], p->post[l], p->w[l], st))
         return rc;
     if (l == 0) {
-        const int nblk = residual_blocks(op->g);
-        launch_residual<double>(p->phi[0], p->rho[0], p->res[0], 1, op->g, P, op->st, p->partial,
-                                st);
+        const int nblk = op_resid_blocks(op, 1, 8);
+        if (int rc = op_sweep(op, EPI_RESID, p->phi[0], p->res[0], p->rho[0], 1, GB_F64, P, 0, 0, 0,
+                              p->partial, st))
+            return rc;
         GB_LAUNCH_CHECK();
         launch_reduce_partials(p->partial, nblk, 1, p->dv, p->err_dev, st);
         GB_LAUNCH_CHECK();

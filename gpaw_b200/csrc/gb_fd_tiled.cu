@@ -1,0 +1,442 @@
+// Plane-marching FD apply for central-difference (axis-aligned) stencils.
+//
+// Same result as k_fd_generic (and as the reference's bmgs_fd over its
+// padded buffer, c/bmgs/fd.cpp:9-33): every output is
+//     x = 0;  x += v(center) c0;  then, for each of the three directions in
+//     the caller's order, x += v(+1) c(+1) ... v(+nn) c(+nn),
+//     x += v(-1) c(-1) ... v(-nn) c(-nn)
+// with separately rounded products and sums.
+//
+// Data movement (one CTA = TX x TY output columns, a chunk of planes along
+// axis 0):
+//  * a multi-stage ring of shared-memory plane tiles, each tile the TX x TY
+//    block plus an nn-wide halo on the four in-plane sides, filled with
+//    asynchronous global->shared copies (cp.async, register-free, with
+//    hardware zero fill for zero-boundary cells) D planes ahead of use;
+//  * a register queue of 2nn+1 values per output along axis 0, so the
+//    axis-0 neighbours are read from shared memory once per point;
+//  * each thread owns RY consecutive rows of one column, so the axis-1
+//    neighbours are shared between its rows.
+// Periodic halos are copied from the wrapped position; the Bloch phase of a
+// wrapped complex value is applied when it is read (register-side, exact
+// complex multiply as in bmgs_translatemz, c/bmgs/translate.cpp:28-47).
+#include "gb_internal.cuh"
+
+namespace gb {
+
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* sdst, const void* gsrc, bool valid) {
+    const unsigned s = smem_u32(sdst);
+    const int n = valid ? BYTES : 0;   // 0: zero-fill, nothing is read
+    if (BYTES == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gsrc),
+                     "r"(n));
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gsrc),
+                     "r"(n));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+template <class T>
+__device__ __forceinline__ T maybe_phase(T v, bool wrap, double2 ph);
+template <>
+__device__ __forceinline__ double maybe_phase<double>(double v, bool, double2) { return v; }
+template <>
+__device__ __forceinline__ double2 maybe_phase<double2>(double2 v, bool wrap, double2 ph) {
+    return wrap ? cmul(ph, v) : v;
+}
+
+// (1 - w) b + (w (src - x)) / c0, each operation rounded on its own
+template <class T>
+__device__ __forceinline__ T jacobi_update(T b, T src, T x, double w, double c0);
+template <>
+__device__ __forceinline__ double jacobi_update<double>(double b, double src, double x, double w,
+                                                        double c0) {
+    return __dadd_rn(__dmul_rn(1.0 - w, b), __ddiv_rn(__dmul_rn(w, __dsub_rn(src, x)), c0));
+}
+template <>
+__device__ __forceinline__ double2 jacobi_update<double2>(double2 b, double2, double2, double,
+                                                          double) {
+    return b;  // relaxation is defined for real data only
+}
+
+template <class T>
+__device__ __forceinline__ T fma_exact(T x, T v, double c) {
+    return Num<T>::add(x, Num<T>::scale(v, c));
+}
+
+// Wrap coordinate y into [0, n) for a periodic axis; returns false for a
+// zero-boundary position (or one further out than one period).
+__device__ __forceinline__ bool wrap_coord(int& y, int n, int periodic) {
+    if (y >= 0 && y < n) return true;
+    if (!periodic) return false;
+    if (y < 0) y += n;
+    else y -= n;
+    return y >= 0 && y < n;
+}
+
+template <class T, int NN, int TX, int TY, int RY, int D, int MODE>
+__global__ void __launch_bounds__(TX * (TY / RY))
+k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phases P,
+         CfdStencil cs, int chunk0, int tiles_x, Epi ep) {
+    constexpr int PX = TX + 2 * NN;          // tile pitch (elements)
+    constexpr int PY = TY + 2 * NN;
+    constexpr int S = NN + 1 + D;            // ring depth
+    constexpr int NT = TX * (TY / RY);
+    constexpr int Q = 2 * NN + 1;
+    constexpr int EB = (int)sizeof(T);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* ring = reinterpret_cast<T*>(smem_raw);
+
+    const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
+    const int x0 = (blockIdx.x % tiles_x) * TX;
+    const int y0 = (blockIdx.x / tiles_x) * TY;
+    const int pa = blockIdx.y * chunk0;
+    const int pb = min(n0, pa + chunk0);
+    const int b = blockIdx.z;
+    const int tid = threadIdx.x;
+    if (pa >= pb || b >= nin) {
+        if (MODE == EPI_RESID && ep.partial && tid == 0)
+            ep.partial[((long long)b * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = 0.0;
+        return;
+    }
+    const long long ng = (long long)n0 * n1 * n2;
+    const T* a = in + b * ng;
+    T* o = out + b * ng;
+    const T* aux = (const T*)ep.aux + b * ng;
+    double sq = 0.0;
+    const int tx = tid % TX;
+    const int ty0 = (tid / TX) * RY;
+    const int gx = x0 + tx;
+
+    // -- issue the async copy of relative plane j (absolute pa + j) -------
+    auto issue = [&](int j) {
+        int pl = pa + j;
+        const bool pvalid = wrap_coord(pl, n0, g.periodic[0]);
+        T* st = ring + (j % S) * (PX * PY);
+        const T* src = a + (long long)pl * n1 * n2;
+        // rows -NN..TY+NN-1 at columns 0..TX-1, and rows 0..TY-1 at the
+        // two x-halo strips (corners are never read by a cfd stencil)
+        constexpr int NMID = PY * TX;
+        constexpr int NSIDE = TY * 2 * NN;
+        for (int e = tid; e < NMID + NSIDE; e += NT) {
+            int ry, rx;
+            if (e < NMID) {
+                ry = e / TX - NN;
+                rx = e % TX;
+            } else {
+                const int f = e - NMID;
+                ry = f / (2 * NN);
+                const int c = f % (2 * NN);
+                rx = c < NN ? c - NN : TX + c - NN;
+            }
+            int y = y0 + ry, x = x0 + rx;
+            const bool ok = pvalid && wrap_coord(y, n1, g.periodic[1]) &&
+                            wrap_coord(x, n2, g.periodic[2]);
+            const T* gp = ok ? src + (long long)y * n2 + x : a;
+            cp_async<EB>(st + (ry + NN) * PX + (rx + NN), gp, ok);
+        }
+    };
+
+    // phases for the wrap of this thread's neighbours
+    double2 ph0hi = make_double2(1, 0), ph0lo = ph0hi, ph1hi = ph0hi, ph1lo = ph0hi,
+            ph2hi = ph0hi, ph2lo = ph0hi;
+    if (P.use) {
+        ph0hi = P.ph[0][0];
+        ph0lo = P.ph[0][1];
+        ph1hi = P.ph[1][0];
+        ph1lo = P.ph[1][1];
+        ph2hi = P.ph[2][0];
+        ph2lo = P.ph[2][1];
+    }
+    const bool cplx = P.use != 0;
+
+    // -- axis-0 queue ---------------------------------------------------------
+    // Before iteration t's push, q[k] (k < 2NN) holds relative plane t-2NN+k;
+    // iteration t pushes plane t into q[2NN] and, for t >= NN, computes the
+    // centre plane t-NN.  Planes pa-NN..pa-1 (before the chunk) come straight
+    // from global memory into q[NN..2NN-1].
+    T q[RY][Q];
+#pragma unroll
+    for (int r = 0; r < RY; r++)
+#pragma unroll
+        for (int k = 0; k < Q; k++) q[r][k] = Num<T>::zero();
+#pragma unroll
+    for (int k = 0; k < NN; k++) {
+        int pl = pa - NN + k;
+        const bool wrapped = pl < 0;
+        const bool pv = wrap_coord(pl, n0, g.periodic[0]);
+#pragma unroll
+        for (int r = 0; r < RY; r++) {
+            const int gy = y0 + ty0 + r;
+            T v = Num<T>::zero();
+            if (pv && gx < n2 && gy < n1) {
+                v = __ldg(a + ((long long)pl * n1 + gy) * n2 + gx);
+                v = maybe_phase<T>(v, cplx && wrapped, ph0lo);
+            }
+            q[r][NN + k] = v;
+        }
+    }
+
+    // prologue: relative planes 0 .. D-1 into the ring
+    const int jend = (pb - pa) + NN;   // relative planes needed: [0, jend)
+#pragma unroll 1
+    for (int j = 0; j < D; j++) {
+        if (j < jend) issue(j);
+        cp_commit();
+    }
+
+    // per-thread wrap masks of in-plane neighbours (bit d-1: distance d)
+    unsigned yhi[RY], ylo[RY], xhi = 0, xlo = 0;
+#pragma unroll
+    for (int r = 0; r < RY; r++) {
+        yhi[r] = ylo[r] = 0;
+        const int gy = y0 + ty0 + r;
+#pragma unroll
+        for (int d = 1; d <= NN; d++) {
+            if (g.periodic[1] && gy + d >= n1) yhi[r] |= 1u << (d - 1);
+            if (g.periodic[1] && gy - d < 0) ylo[r] |= 1u << (d - 1);
+        }
+    }
+#pragma unroll
+    for (int d = 1; d <= NN; d++) {
+        if (g.periodic[2] && gx + d >= n2) xhi |= 1u << (d - 1);
+        if (g.periodic[2] && gx - d < 0) xlo |= 1u << (d - 1);
+    }
+
+    const int nplanes = pb - pa;
+#pragma unroll 1
+    for (int t = 0; t < nplanes + NN; t++) {
+        // relative plane t enters the queue now (t < NN: prologue fill)
+        cp_wait<D - 1>();
+        __syncthreads();
+        {
+            // the slot of plane t+D last held plane t-NN-1, the centre of
+            // iteration t-1, which every thread has finished (barrier above)
+            const int j = t + D;
+            if (j < jend) issue(j);
+            cp_commit();
+        }
+        const T* st_in = ring + (t % S) * (PX * PY);
+        {
+            const int pl = pa + t;
+            const bool wrapped = pl >= n0;
+#pragma unroll
+            for (int r = 0; r < RY; r++) {
+                T v = st_in[(ty0 + r + NN) * PX + (tx + NN)];
+                q[r][2 * NN] = maybe_phase<T>(v, cplx && wrapped, ph0hi);
+            }
+        }
+        if (t >= NN) {
+            // center plane: relative t - NN, absolute p
+            const int p = pa + t - NN;
+            const T* sc = ring + ((t - NN) % S) * (PX * PY);
+            // axis-1 column window of this thread: rows ty0-NN .. ty0+RY-1+NN
+            T col[RY + 2 * NN];
+#pragma unroll
+            for (int k = 0; k < RY + 2 * NN; k++) col[k] = sc[(ty0 + k) * PX + (tx + NN)];
+#pragma unroll
+            for (int r = 0; r < RY; r++) {
+                const T vc = q[r][NN];
+                // x = 0; x += v c in coefficient order (Jacobi skips c0)
+                T x = Num<T>::zero();
+                if (MODE != EPI_JACOBI) x = Num<T>::add(x, Num<T>::scale(vc, cs.c0));
+                const T* row = sc + (ty0 + r + NN) * PX + (tx + NN);
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    const int ax = cs.axis[k];
+                    if (ax == 0) {
+#pragma unroll
+                        for (int d = 1; d <= NN; d++) x = fma_exact<T>(x, q[r][NN + d], cs.cp[k][d - 1]);
+#pragma unroll
+                        for (int d = 1; d <= NN; d++) x = fma_exact<T>(x, q[r][NN - d], cs.cm[k][d - 1]);
+                    } else if (ax == 1) {
+#pragma unroll
+                        for (int d = 1; d <= NN; d++) {
+                            T v = maybe_phase<T>(col[r + NN + d], cplx && ((yhi[r] >> (d - 1)) & 1), ph1hi);
+                            x = fma_exact<T>(x, v, cs.cp[k][d - 1]);
+                        }
+#pragma unroll
+                        for (int d = 1; d <= NN; d++) {
+                            T v = maybe_phase<T>(col[r + NN - d], cplx && ((ylo[r] >> (d - 1)) & 1), ph1lo);
+                            x = fma_exact<T>(x, v, cs.cm[k][d - 1]);
+                        }
+                    } else {
+#pragma unroll
+                        for (int d = 1; d <= NN; d++) {
+                            T v = maybe_phase<T>(row[d], cplx && ((xhi >> (d - 1)) & 1), ph2hi);
+                            x = fma_exact<T>(x, v, cs.cp[k][d - 1]);
+                        }
+#pragma unroll
+                        for (int d = 1; d <= NN; d++) {
+                            T v = maybe_phase<T>(row[-d], cplx && ((xlo >> (d - 1)) & 1), ph2lo);
+                            x = fma_exact<T>(x, v, cs.cm[k][d - 1]);
+                        }
+                    }
+                }
+                const int gy = y0 + ty0 + r;
+                if (gx < n2 && gy < n1) {
+                    const long long at = ((long long)p * n1 + gy) * n2 + gx;
+                    if (MODE == EPI_APPLY) {
+                        o[at] = x;
+                    } else if (MODE == EPI_RESID) {
+                        const T res = Num<T>::sub(x, aux[at]);
+                        if (out) o[at] = res;
+                        sq += sqnorm(res);
+                    } else if (MODE == EPI_JACOBI) {
+                        o[at] = jacobi_update<T>(vc, aux[at], x, ep.w, cs.c0);
+                    } else {
+                        const T y = Num<T>::sub(vc, Num<T>::scale(Num<T>::sub(x, aux[at]), ep.sc));
+                        o[at] = ep.negate ? Num<T>::neg(y) : y;
+                    }
+                }
+            }
+        }
+        // shift the queue
+#pragma unroll
+        for (int r = 0; r < RY; r++)
+#pragma unroll
+            for (int k = 0; k < Q - 1; k++) q[r][k] = q[r][k + 1];
+    }
+    cp_wait<0>();
+    if (MODE == EPI_RESID && ep.partial) {
+        sq = block_sum(sq);
+        if (tid == 0)
+            ep.partial[((long long)b * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = sq;
+    }
+}
+
+template <class T, int NN, int TX, int TY, int RY, int D, int MODE>
+static int launch_cfd_t(const void* in, void* out, int nin, const GridBC& g, const Phases& P,
+                        const CfdStencil& cs, const Epi& ep, cudaStream_t st, int* nblk) {
+    constexpr int PX = TX + 2 * NN, PY = TY + 2 * NN, S = NN + 1 + D;
+    constexpr size_t smem = (size_t)S * PX * PY * sizeof(T);
+    static bool attr_done = false;
+    if (!attr_done) {
+        cudaError_t e = cudaFuncSetAttribute(k_fd_cfd<T, NN, TX, TY, RY, D, MODE>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)smem);
+        if (e != cudaSuccess) return -2;
+        attr_done = true;
+    }
+    const int tiles_x = (g.n[2] + TX - 1) / TX;
+    const int tiles_y = (g.n[1] + TY - 1) / TY;
+    int chunk0 = g.n[0];
+    const long long tiles = (long long)tiles_x * tiles_y * nin;
+    // split axis 0 until the grid covers the GPU a few times
+    while (chunk0 > 2 * NN && tiles * ((g.n[0] + chunk0 - 1) / chunk0) < 148 * 4)
+        chunk0 = (chunk0 + 1) / 2;
+    const int nch = (g.n[0] + chunk0 - 1) / chunk0;
+    if (nblk) *nblk = tiles_x * tiles_y * nch;
+    const long long ng = (long long)g.n[0] * g.n[1] * g.n[2];
+    for (int b0 = 0; b0 < nin; b0 += 65535) {
+        const int nb = min(65535, nin - b0);
+        dim3 grid(tiles_x * tiles_y, nch, nb);
+        Epi e2 = ep;
+        if (e2.aux) e2.aux = (const T*)ep.aux + b0 * ng;
+        if (e2.partial) e2.partial = ep.partial + (long long)b0 * tiles_x * tiles_y * nch;
+        k_fd_cfd<T, NN, TX, TY, RY, D, MODE><<<grid, TX * (TY / RY), smem, st>>>(
+            (const T*)in + b0 * ng, out ? (T*)out + b0 * ng : nullptr, nb, g, P, cs, chunk0,
+            tiles_x, e2);
+    }
+    return 0;
+}
+
+// Tile shapes: 32 columns per warp row; f64 threads own 4 rows, complex 2.
+template <class T, int NN, int MODE>
+static int launch_cfd_nn(const void* in, void* out, int nin, const GridBC& g, const Phases& P,
+                         const CfdStencil& cs, const Epi& ep, cudaStream_t st, int* nblk) {
+    if constexpr (sizeof(T) == 16)
+        return launch_cfd_t<T, NN, 32, 16, 2, (NN <= 3 ? 3 : 2), MODE>(in, out, nin, g, P, cs,
+                                                                      ep, st, nblk);
+    else
+        return launch_cfd_t<T, NN, 32, 16, 4, 4, MODE>(in, out, nin, g, P, cs, ep, st, nblk);
+}
+
+template <class T, int MODE>
+static int launch_cfd_mode(const void* in, void* out, int nin, const GridBC& g, const Phases& P,
+                           const CfdStencil& cs, int nn, const Epi& ep, cudaStream_t st,
+                           int* nblk) {
+    switch (nn) {
+        case 1: return launch_cfd_nn<T, 1, MODE>(in, out, nin, g, P, cs, ep, st, nblk);
+        case 2: return launch_cfd_nn<T, 2, MODE>(in, out, nin, g, P, cs, ep, st, nblk);
+        case 3: return launch_cfd_nn<T, 3, MODE>(in, out, nin, g, P, cs, ep, st, nblk);
+        case 4: return launch_cfd_nn<T, 4, MODE>(in, out, nin, g, P, cs, ep, st, nblk);
+        case 5: return launch_cfd_nn<T, 5, MODE>(in, out, nin, g, P, cs, ep, st, nblk);
+        case 6: return launch_cfd_nn<T, 6, MODE>(in, out, nin, g, P, cs, ep, st, nblk);
+    }
+    return -1;
+}
+
+template <class T>
+int launch_fd_cfd(int mode, const void* in, void* out, int nin, const GridBC& g,
+                  const Phases& P, const CfdStencil& cs, int nn, const Epi& ep,
+                  cudaStream_t st, int* nblk) {
+    switch (mode) {
+        case EPI_APPLY: return launch_cfd_mode<T, EPI_APPLY>(in, out, nin, g, P, cs, nn, ep, st, nblk);
+        case EPI_RESID: return launch_cfd_mode<T, EPI_RESID>(in, out, nin, g, P, cs, nn, ep, st, nblk);
+        case EPI_PRECOND: return launch_cfd_mode<T, EPI_PRECOND>(in, out, nin, g, P, cs, nn, ep, st, nblk);
+        case EPI_JACOBI:
+            if constexpr (sizeof(T) != 8) return -1;
+            else return launch_cfd_mode<T, EPI_JACOBI>(in, out, nin, g, P, cs, nn, ep, st, nblk);
+    }
+    return -1;
+}
+
+template int launch_fd_cfd<double>(int, const void*, void*, int, const GridBC&, const Phases&,
+                                   const CfdStencil&, int, const Epi&, cudaStream_t, int*);
+template int launch_fd_cfd<double2>(int, const void*, void*, int, const GridBC&, const Phases&,
+                                    const CfdStencil&, int, const Epi&, cudaStream_t, int*);
+
+// Number of CTAs per grid of the EPI_RESID launch (partials per grid).
+int cfd_blocks(const GridBC& g, int nn, int elem_bytes, int nin) {
+    const int TX = 32, TY = 16;
+    const int tiles_x = (g.n[2] + TX - 1) / TX;
+    const int tiles_y = (g.n[1] + TY - 1) / TY;
+    int chunk0 = g.n[0];
+    const long long tiles = (long long)tiles_x * tiles_y * nin;
+    while (chunk0 > 2 * nn && tiles * ((g.n[0] + chunk0 - 1) / chunk0) < 148 * 4)
+        chunk0 = (chunk0 + 1) / 2;
+    (void)elem_bytes;
+    return tiles_x * tiles_y * ((g.n[0] + chunk0 - 1) / chunk0);
+}
+
+// Recognise the GUCLaplace layout of an axis-aligned stencil: centre first,
+// then three directions, each +1..+nn followed by -1..-nn along one axis.
+bool to_cfd_stencil(const Stencil& s, CfdStencil& cs, int& nn) {
+    if (!s.cfd) return false;
+    const int n = (s.ncoefs - 1) / 6;
+    if (n < 1 || n > 6 || s.ncoefs != 6 * n + 1 || s.range != n) return false;
+    if (s.off[0][0] || s.off[0][1] || s.off[0][2]) return false;
+    cs.c0 = s.coef[0];
+    int used = 0;
+    for (int k = 0; k < 3; k++) {
+        const int base = 1 + k * 2 * n;
+        int ax = -1;
+        for (int c = 0; c < 3; c++)
+            if (s.off[base][c] != 0) ax = c;
+        if (ax < 0 || (used >> ax) & 1) return false;
+        used |= 1 << ax;
+        cs.axis[k] = ax;
+        for (int d = 1; d <= n; d++) {
+            const int ip = base + d - 1, im = base + n + d - 1;
+            for (int c = 0; c < 3; c++) {
+                if (s.off[ip][c] != (c == ax ? d : 0)) return false;
+                if (s.off[im][c] != (c == ax ? -d : 0)) return false;
+            }
+            cs.cp[k][d - 1] = s.coef[ip];
+            cs.cm[k][d - 1] = s.coef[im];
+        }
+    }
+    nn = n;
+    return true;
+}
+
+}  // namespace gb

@@ -43,6 +43,32 @@ struct XferGeom {
     double scale2;  // restriction: also write out2 = scale2 * out when out2 set
 };
 
+// ------------------------------------------------------- tiled cfd stencil
+// Axis-aligned stencil in "three directions" form (coefficient order = the
+// caller's order: centre, then per direction +1..+nn, -1..-nn).
+struct CfdStencil {
+    double c0;
+    int axis[3];          // axis of direction k
+    double cp[3][8];      // coefficient of +d (d = 1..nn) along direction k
+    double cm[3][8];      // coefficient of -d
+};
+
+// Epilogues fused into the sweep (one pass over the data each):
+enum : int {
+    EPI_APPLY = 0,    // out = L in                       (bmgs_fd)
+    EPI_RESID = 1,    // out = L in - aux, |out|^2 partials (gpaw/poisson.py:517-532)
+    EPI_JACOBI = 2,   // out = (1-w) in + w (aux - L' in) / c0  (c/bmgs/relax.cpp:41-65)
+    EPI_PRECOND = 3,  // out = +-(in - sc (L in - aux))  (c/fd_preconditioner.cpp:251-333)
+};
+
+struct Epi {
+    const void* aux;
+    double w;
+    double sc;
+    int negate;
+    double* partial;  // EPI_RESID: per-CTA sums of |r|^2 (nullable)
+};
+
 // ------------------------------------------------------------------ launchers
 template <class T>
 void launch_fd(const void* in, void* out, int nin, const GridBC& g, const Phases& P,
@@ -64,5 +90,11 @@ void launch_precond_step(const void* d, const void* r, void* out, int nin, const
 void launch_reduce_partials(const double* partial, int nblk, int nin, double scale,
                             double* out, cudaStream_t stream);
 int residual_blocks(const GridBC& g);
+bool to_cfd_stencil(const Stencil& s, CfdStencil& cs, int& nn);
+template <class T>
+int launch_fd_cfd(int mode, const void* in, void* out, int nin, const GridBC& g,
+                  const Phases& P, const CfdStencil& cs, int nn, const Epi& ep,
+                  cudaStream_t st, int* nblk);
+int cfd_blocks(const GridBC& g, int nn, int elem_bytes, int nin);
 
 }  // namespace gb
