@@ -426,6 +426,7 @@ static int transform_impl(gb_transformer* t, const void* in, void* out, void* ou
         rc = launch_transform<double>(t->k, t->interpolate, in, out, out2, (int)nin, G, P, st);
     else
         rc = launch_transform<double2>(t->k, t->interpolate, in, out, out2, (int)nin, G, P, st);
+    if (rc == -2) return fail(GB_ECUDA, "transformer: could not raise the shared-memory limit");
     if (rc) return fail(GB_EINVAL, "transformer: unsupported order");
     GB_LAUNCH_CHECK();
     return 0;

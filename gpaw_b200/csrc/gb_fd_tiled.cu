@@ -44,15 +44,6 @@ __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_grou
 template <int N>
 __device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
 
-template <class T>
-__device__ __forceinline__ T maybe_phase(T v, bool wrap, double2 ph);
-template <>
-__device__ __forceinline__ double maybe_phase<double>(double v, bool, double2) { return v; }
-template <>
-__device__ __forceinline__ double2 maybe_phase<double2>(double2 v, bool wrap, double2 ph) {
-    return wrap ? cmul(ph, v) : v;
-}
-
 // (1 - w) b + (w (src - x)) / c0, each operation rounded on its own
 template <class T>
 __device__ __forceinline__ T jacobi_update(T b, T src, T x, double w, double c0);
@@ -82,8 +73,23 @@ __device__ __forceinline__ bool wrap_coord(int& y, int n, int periodic) {
     return y >= 0 && y < n;
 }
 
-template <class T, int NN, int TX, int TY, int RY, int D, int MODE>
-__global__ void __launch_bounds__(TX * (TY / RY))
+// Sum of one direction's 2*NN terms in the caller's order: +1..+NN then
+// -1..-NN.  `vp(d)` / `vm(d)` return the values at +d / -d.
+template <class T, int NN, class VP, class VM>
+__device__ __forceinline__ T add_direction(T x, const double* cp, const double* cm, VP vp, VM vm) {
+#pragma unroll
+    for (int d = 1; d <= NN; d++) x = fma_exact<T>(x, vp(d), cp[d - 1]);
+#pragma unroll
+    for (int d = 1; d <= NN; d++) x = fma_exact<T>(x, vm(d), cm[d - 1]);
+    return x;
+}
+
+// ORD = 1: directions are axis 2, axis 1, axis 0 (the order GUCLaplace
+// builds for an orthorhombic cell); ORD = 0: order read from cs.axis.
+// 128 registers a thread: two resident CTAs of 256 threads (complex) or
+// four of 128 (real) when the tile holds two or four rows per thread.
+template <class T, int NN, int TX, int TY, int RY, int D, int MODE, int ORD>
+__global__ void __launch_bounds__(TX * (TY / RY), (512 / (TX * (TY / RY))))
 k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phases P,
          CfdStencil cs, int chunk0, int tiles_x, Epi ep) {
     constexpr int PX = TX + 2 * NN;          // tile pitch (elements)
@@ -92,6 +98,7 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
     constexpr int NT = TX * (TY / RY);
     constexpr int Q = 2 * NN + 1;
     constexpr int EB = (int)sizeof(T);
+    constexpr bool CPLX = sizeof(T) == 16;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* ring = reinterpret_cast<T*>(smem_raw);
 
@@ -116,47 +123,80 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
     const int ty0 = (tid / TX) * RY;
     const int gx = x0 + tx;
 
-    // -- issue the async copy of relative plane j (absolute pa + j) -------
+    // -- async copy of relative plane j (absolute pa + j) ------------------
+    // Rows -NN..TY+NN-1 at columns 0..TX-1, and rows 0..TY-1 of the two
+    // x-halo strips (corners are never read by a cfd stencil).
+    constexpr int NMID = PY * TX;
+    constexpr int NSIDE = TY * 2 * NN;
+    auto cell = [&](int e, int& ry, int& rx) {
+        if (e < NMID) {
+            ry = e / TX - NN;
+            rx = e % TX;
+        } else {
+            const int f = e - NMID;
+            ry = f / (2 * NN);
+            const int c = f % (2 * NN);
+            rx = c < NN ? c - NN : TX + c - NN;
+        }
+    };
+    // Each thread copies the same NC cells of every plane: precompute their
+    // shared-memory offsets, in-plane source offsets (after the periodic
+    // wrap), validity and Bloch-phase code once per CTA.
+    constexpr int NC = (NMID + NSIDE + NT - 1) / NT;
+    int soff[NC], goff[NC];
+    unsigned vmask = 0, wcode = 0;   // wcode: 3 bits per cell (0 = no phase)
+#pragma unroll
+    for (int i = 0; i < NC; i++) {
+        const int e = tid + i * NT;
+        soff[i] = 0;
+        goff[i] = 0;
+        if (e >= NMID + NSIDE) continue;
+        int ry, rx;
+        cell(e, ry, rx);
+        soff[i] = (ry + NN) * PX + (rx + NN);
+        int y = y0 + ry, x = x0 + rx;
+        const bool yw = y < 0 || y >= n1, xw = x < 0 || x >= n2;
+        const int ys = y < 0, xs = x < 0;
+        if (wrap_coord(y, n1, g.periodic[1]) && wrap_coord(x, n2, g.periodic[2])) {
+            vmask |= 1u << i;
+            goff[i] = y * n2 + x;
+            // phase code: 1 + 2*axis_index + side, axis 1 -> 0, axis 2 -> 1
+            unsigned c = 0;
+            if (yw) c = 1 + ys;
+            else if (xw) c = 3 + xs;
+            wcode |= c << (3 * i);
+        }
+    }
+    if (!(CPLX && P.use)) wcode = 0;
     auto issue = [&](int j) {
         int pl = pa + j;
         const bool pvalid = wrap_coord(pl, n0, g.periodic[0]);
         T* st = ring + (j % S) * (PX * PY);
         const T* src = a + (long long)pl * n1 * n2;
-        // rows -NN..TY+NN-1 at columns 0..TX-1, and rows 0..TY-1 at the
-        // two x-halo strips (corners are never read by a cfd stencil)
-        constexpr int NMID = PY * TX;
-        constexpr int NSIDE = TY * 2 * NN;
-        for (int e = tid; e < NMID + NSIDE; e += NT) {
-            int ry, rx;
-            if (e < NMID) {
-                ry = e / TX - NN;
-                rx = e % TX;
-            } else {
-                const int f = e - NMID;
-                ry = f / (2 * NN);
-                const int c = f % (2 * NN);
-                rx = c < NN ? c - NN : TX + c - NN;
-            }
-            int y = y0 + ry, x = x0 + rx;
-            const bool ok = pvalid && wrap_coord(y, n1, g.periodic[1]) &&
-                            wrap_coord(x, n2, g.periodic[2]);
-            const T* gp = ok ? src + (long long)y * n2 + x : a;
-            cp_async<EB>(st + (ry + NN) * PX + (rx + NN), gp, ok);
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            if (tid + i * NT >= NMID + NSIDE) break;
+            const bool ok = pvalid && ((vmask >> i) & 1);
+            cp_async<EB>(st + soff[i], ok ? src + goff[i] : a, ok);
         }
     };
-
-    // phases for the wrap of this thread's neighbours
-    double2 ph0hi = make_double2(1, 0), ph0lo = ph0hi, ph1hi = ph0hi, ph1lo = ph0hi,
-            ph2hi = ph0hi, ph2lo = ph0hi;
-    if (P.use) {
-        ph0hi = P.ph[0][0];
-        ph0lo = P.ph[0][1];
-        ph1hi = P.ph[1][0];
-        ph1lo = P.ph[1][1];
-        ph2hi = P.ph[2][0];
-        ph2lo = P.ph[2][1];
-    }
-    const bool cplx = P.use != 0;
+    // After this thread's own copies of plane j completed, multiply the
+    // wrapped halo cells among them by their phase (the halo is filled from
+    // the opposite side, as bc_unpack1's translate does, c/bc.cpp:242-257).
+    // Other threads read them NN iterations later, after a barrier.
+    auto fixup = [&](int j) {
+        T* st = ring + (j % S) * (PX * PY);
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            const unsigned c = (wcode >> (3 * i)) & 7u;
+            if (c == 0) continue;
+            if constexpr (CPLX) {
+                const double2 ph = c == 1 ? P.ph[1][0] : c == 2 ? P.ph[1][1]
+                                 : c == 3 ? P.ph[2][0] : P.ph[2][1];
+                st[soff[i]] = cmul(ph, st[soff[i]]);
+            }
+        }
+    };
 
     // -- axis-0 queue ---------------------------------------------------------
     // Before iteration t's push, q[k] (k < 2NN) holds relative plane t-2NN+k;
@@ -179,7 +219,8 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
             T v = Num<T>::zero();
             if (pv && gx < n2 && gy < n1) {
                 v = __ldg(a + ((long long)pl * n1 + gy) * n2 + gx);
-                v = maybe_phase<T>(v, cplx && wrapped, ph0lo);
+                if constexpr (CPLX)
+                    if (P.use && wrapped) v = cmul(P.ph[0][1], v);
             }
             q[r][NN + k] = v;
         }
@@ -193,29 +234,13 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
         cp_commit();
     }
 
-    // per-thread wrap masks of in-plane neighbours (bit d-1: distance d)
-    unsigned yhi[RY], ylo[RY], xhi = 0, xlo = 0;
-#pragma unroll
-    for (int r = 0; r < RY; r++) {
-        yhi[r] = ylo[r] = 0;
-        const int gy = y0 + ty0 + r;
-#pragma unroll
-        for (int d = 1; d <= NN; d++) {
-            if (g.periodic[1] && gy + d >= n1) yhi[r] |= 1u << (d - 1);
-            if (g.periodic[1] && gy - d < 0) ylo[r] |= 1u << (d - 1);
-        }
-    }
-#pragma unroll
-    for (int d = 1; d <= NN; d++) {
-        if (g.periodic[2] && gx + d >= n2) xhi |= 1u << (d - 1);
-        if (g.periodic[2] && gx - d < 0) xlo |= 1u << (d - 1);
-    }
-
     const int nplanes = pb - pa;
 #pragma unroll 1
     for (int t = 0; t < nplanes + NN; t++) {
-        // relative plane t enters the queue now (t < NN: prologue fill)
         cp_wait<D - 1>();
+        // this thread's copies of plane t have landed: fix its wrapped halo
+        // cells (read as a centre NN iterations later, after a barrier)
+        if (wcode && t < nplanes) fixup(t);
         __syncthreads();
         {
             // the slot of plane t+D last held plane t-NN-1, the centre of
@@ -224,62 +249,51 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
             if (j < jend) issue(j);
             cp_commit();
         }
-        const T* st_in = ring + (t % S) * (PX * PY);
+        // push plane t's own values (uniform phase for a wrapped plane)
         {
-            const int pl = pa + t;
-            const bool wrapped = pl >= n0;
+            const T* st_in = ring + (t % S) * (PX * PY);
+            const bool wrapped = CPLX && P.use && pa + t >= n0;
 #pragma unroll
             for (int r = 0; r < RY; r++) {
                 T v = st_in[(ty0 + r + NN) * PX + (tx + NN)];
-                q[r][2 * NN] = maybe_phase<T>(v, cplx && wrapped, ph0hi);
+                if constexpr (CPLX)
+                    if (wrapped) v = cmul(P.ph[0][0], v);
+                q[r][2 * NN] = v;
             }
         }
         if (t >= NN) {
-            // center plane: relative t - NN, absolute p
             const int p = pa + t - NN;
             const T* sc = ring + ((t - NN) % S) * (PX * PY);
-            // axis-1 column window of this thread: rows ty0-NN .. ty0+RY-1+NN
-            T col[RY + 2 * NN];
-#pragma unroll
-            for (int k = 0; k < RY + 2 * NN; k++) col[k] = sc[(ty0 + k) * PX + (tx + NN)];
+            // this thread's column in the centre tile (axis-1 neighbours)
+            const T* colp = sc + ty0 * PX + (tx + NN);
 #pragma unroll
             for (int r = 0; r < RY; r++) {
                 const T vc = q[r][NN];
+                const T* row = sc + (ty0 + r + NN) * PX + (tx + NN);
                 // x = 0; x += v c in coefficient order (Jacobi skips c0)
                 T x = Num<T>::zero();
                 if (MODE != EPI_JACOBI) x = Num<T>::add(x, Num<T>::scale(vc, cs.c0));
-                const T* row = sc + (ty0 + r + NN) * PX + (tx + NN);
+                auto dir = [&](int k, int ax) {
+                    if (ax == 0)
+                        x = add_direction<T, NN>(x, cs.cp[k], cs.cm[k],
+                                                 [&](int d) { return q[r][NN + d]; },
+                                                 [&](int d) { return q[r][NN - d]; });
+                    else if (ax == 1)
+                        x = add_direction<T, NN>(x, cs.cp[k], cs.cm[k],
+                                                 [&](int d) { return colp[(r + NN + d) * PX]; },
+                                                 [&](int d) { return colp[(r + NN - d) * PX]; });
+                    else
+                        x = add_direction<T, NN>(x, cs.cp[k], cs.cm[k],
+                                                 [&](int d) { return row[d]; },
+                                                 [&](int d) { return row[-d]; });
+                };
+                if constexpr (ORD == 1) {
+                    dir(0, 2);
+                    dir(1, 1);
+                    dir(2, 0);
+                } else {
 #pragma unroll
-                for (int k = 0; k < 3; k++) {
-                    const int ax = cs.axis[k];
-                    if (ax == 0) {
-#pragma unroll
-                        for (int d = 1; d <= NN; d++) x = fma_exact<T>(x, q[r][NN + d], cs.cp[k][d - 1]);
-#pragma unroll
-                        for (int d = 1; d <= NN; d++) x = fma_exact<T>(x, q[r][NN - d], cs.cm[k][d - 1]);
-                    } else if (ax == 1) {
-#pragma unroll
-                        for (int d = 1; d <= NN; d++) {
-                            T v = maybe_phase<T>(col[r + NN + d], cplx && ((yhi[r] >> (d - 1)) & 1), ph1hi);
-                            x = fma_exact<T>(x, v, cs.cp[k][d - 1]);
-                        }
-#pragma unroll
-                        for (int d = 1; d <= NN; d++) {
-                            T v = maybe_phase<T>(col[r + NN - d], cplx && ((ylo[r] >> (d - 1)) & 1), ph1lo);
-                            x = fma_exact<T>(x, v, cs.cm[k][d - 1]);
-                        }
-                    } else {
-#pragma unroll
-                        for (int d = 1; d <= NN; d++) {
-                            T v = maybe_phase<T>(row[d], cplx && ((xhi >> (d - 1)) & 1), ph2hi);
-                            x = fma_exact<T>(x, v, cs.cp[k][d - 1]);
-                        }
-#pragma unroll
-                        for (int d = 1; d <= NN; d++) {
-                            T v = maybe_phase<T>(row[-d], cplx && ((xlo >> (d - 1)) & 1), ph2lo);
-                            x = fma_exact<T>(x, v, cs.cm[k][d - 1]);
-                        }
-                    }
+                    for (int k = 0; k < 3; k++) dir(k, cs.axis[k]);
                 }
                 const int gy = y0 + ty0 + r;
                 if (gx < n2 && gy < n1) {
@@ -299,7 +313,6 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
                 }
             }
         }
-        // shift the queue
 #pragma unroll
         for (int r = 0; r < RY; r++)
 #pragma unroll
@@ -313,14 +326,14 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
     }
 }
 
-template <class T, int NN, int TX, int TY, int RY, int D, int MODE>
+template <class T, int NN, int TX, int TY, int RY, int D, int MODE, int ORD>
 static int launch_cfd_t(const void* in, void* out, int nin, const GridBC& g, const Phases& P,
                         const CfdStencil& cs, const Epi& ep, cudaStream_t st, int* nblk) {
     constexpr int PX = TX + 2 * NN, PY = TY + 2 * NN, S = NN + 1 + D;
     constexpr size_t smem = (size_t)S * PX * PY * sizeof(T);
     static bool attr_done = false;
     if (!attr_done) {
-        cudaError_t e = cudaFuncSetAttribute(k_fd_cfd<T, NN, TX, TY, RY, D, MODE>,
+        cudaError_t e = cudaFuncSetAttribute(k_fd_cfd<T, NN, TX, TY, RY, D, MODE, ORD>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
         if (e != cudaSuccess) return -2;
@@ -342,7 +355,7 @@ static int launch_cfd_t(const void* in, void* out, int nin, const GridBC& g, con
         Epi e2 = ep;
         if (e2.aux) e2.aux = (const T*)ep.aux + b0 * ng;
         if (e2.partial) e2.partial = ep.partial + (long long)b0 * tiles_x * tiles_y * nch;
-        k_fd_cfd<T, NN, TX, TY, RY, D, MODE><<<grid, TX * (TY / RY), smem, st>>>(
+        k_fd_cfd<T, NN, TX, TY, RY, D, MODE, ORD><<<grid, TX * (TY / RY), smem, st>>>(
             (const T*)in + b0 * ng, out ? (T*)out + b0 * ng : nullptr, nb, g, P, cs, chunk0,
             tiles_x, e2);
     }
@@ -353,11 +366,19 @@ static int launch_cfd_t(const void* in, void* out, int nin, const GridBC& g, con
 template <class T, int NN, int MODE>
 static int launch_cfd_nn(const void* in, void* out, int nin, const GridBC& g, const Phases& P,
                          const CfdStencil& cs, const Epi& ep, cudaStream_t st, int* nblk) {
-    if constexpr (sizeof(T) == 16)
-        return launch_cfd_t<T, NN, 32, 16, 2, (NN <= 3 ? 3 : 2), MODE>(in, out, nin, g, P, cs,
-                                                                      ep, st, nblk);
-    else
-        return launch_cfd_t<T, NN, 32, 16, 4, 4, MODE>(in, out, nin, g, P, cs, ep, st, nblk);
+    const bool ord210 = cs.axis[0] == 2 && cs.axis[1] == 1 && cs.axis[2] == 0;
+    if constexpr (sizeof(T) == 16) {
+        constexpr int D = NN <= 3 ? 3 : 2;
+        constexpr int RY = NN <= 3 ? 2 : 1;
+        if (ord210)
+            return launch_cfd_t<T, NN, 32, 16, RY, D, MODE, 1>(in, out, nin, g, P, cs, ep, st, nblk);
+        return launch_cfd_t<T, NN, 32, 16, RY, D, MODE, 0>(in, out, nin, g, P, cs, ep, st, nblk);
+    } else {
+        constexpr int RY = NN <= 3 ? 4 : 2;
+        if (ord210)
+            return launch_cfd_t<T, NN, 32, 16, RY, 4, MODE, 1>(in, out, nin, g, P, cs, ep, st, nblk);
+        return launch_cfd_t<T, NN, 32, 16, RY, 4, MODE, 0>(in, out, nin, g, P, cs, ep, st, nblk);
+    }
 }
 
 template <class T, int MODE>

@@ -26,16 +26,69 @@ namespace gb {
 // out[I][J][L] over padded input a:  per axis, r(c) = 0.5 * (a[c] + sum_l
 // w_l * (a[c + 2l + 1] + a[c - 2l - 1])) at c = K - 1 + 2 I  (RST1D,
 // c/bmgs/restrict.cpp:18-60), applied along axis 2, then 1, then 0.
-template <class T, int K, int TJ, int TK>
+//
+// Fine padded planes stream through a ring of S shared-memory stages filled
+// by cp.async D planes ahead.  Each stage stores the tile's footprint with
+// even and odd columns in separate arrays, so that the axis-2 pass (centre
+// at an odd column, taps at even columns) reads consecutive words.
+
+__device__ __forceinline__ unsigned smem_u32x(const void* p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+template <int BYTES>
+__device__ __forceinline__ void cp_async_x(void* sdst, const void* gsrc, bool valid) {
+    const unsigned s = smem_u32x(sdst);
+    const int n = valid ? BYTES : 0;
+    if (BYTES == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gsrc), "r"(n));
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gsrc), "r"(n));
+}
+__device__ __forceinline__ void cp_commit_x() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_wait_x() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+__device__ __forceinline__ bool wrap_c(int& y, int n, int periodic) {
+    if (y >= 0 && y < n) return true;
+    if (!periodic) return false;
+    if (y < 0) y += n;
+    else y -= n;
+    return y >= 0 && y < n;
+}
+
+// Phase code of a cell: bits 0-1 axis 1 (0 none, 1 past high edge, 2 past
+// low edge), bits 2-3 axis 2.  Phases compose in axis order (the halo is
+// filled axis by axis with cfd = 0, c/bc.cpp:108-112, 242-257).
+template <class T>
+__device__ __forceinline__ T apply_code(T v, unsigned c, bool plane_wrap, double2 ph0,
+                                        const Phases& P) {
+    if constexpr (sizeof(T) == 16) {
+        if (plane_wrap) v = cmul(ph0, v);
+        const unsigned c1 = c & 3u, c2 = (c >> 2) & 3u;
+        if (c1) v = cmul(c1 == 1 ? P.ph[1][0] : P.ph[1][1], v);
+        if (c2) v = cmul(c2 == 1 ? P.ph[2][0] : P.ph[2][1], v);
+    }
+    return v;
+}
+
+template <class T, int K, int TJ, int TK, int D>
 __global__ void __launch_bounds__(TJ * TK)
 k_restrict(const T* __restrict__ in, T* __restrict__ out, T* __restrict__ out2, int nin,
            XferGeom G, Phases P, int chunk0) {
-    constexpr int H = 2 * K - 3;          // taps reach K-1+2(K/2-1)+1 = 2K-2 past 2I
+    constexpr int NT = TJ * TK;
+    constexpr int H = 2 * K - 3;
     constexpr int FY = 2 * TJ + H;        // fine rows needed by the tile
     constexpr int FZ = 2 * TK + H;        // fine columns needed by the tile
+    constexpr int FZE = (FZ + 1) / 2, FZO = FZ / 2;
+    constexpr int SE = FY * FZE, SO = FY * FZO;
+    constexpr int SS = SE + SO;           // one stage (elements)
+    constexpr int S = D + 1;              // ring depth
     constexpr int NR = 2 * K - 1;         // axis-0 ring depth
-    __shared__ T F[FY][FZ + 1];
-    __shared__ T R1[FY][TK];
+    constexpr int NC = (FY * FZ + NT - 1) / NT;
+    constexpr int EB = (int)sizeof(T);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* stage = reinterpret_cast<T*>(smem_raw);
+    T* R1 = stage + S * SS;               // [FY][TK]
 
     const int tiles2 = (G.nout[2] + TK - 1) / TK;
     const int J0 = (blockIdx.x / tiles2) * TJ;
@@ -44,60 +97,124 @@ k_restrict(const T* __restrict__ in, T* __restrict__ out, T* __restrict__ out2, 
     const int I1 = min(G.nout[0], I0 + chunk0);
     const int b = blockIdx.z;
     if (I0 >= I1 || b >= nin) return;
-    const long long ngin = (long long)G.g.n[0] * G.g.n[1] * G.g.n[2];
+    const int n1 = G.g.n[1], n2 = G.g.n[2];
+    const long long ngin = (long long)G.g.n[0] * n1 * n2;
     const long long ngout = (long long)G.nout[0] * G.nout[1] * G.nout[2];
     const T* a = in + b * ngin;
     T* o = out + b * ngout;
     const int tid = threadIdx.x;
     const int tj = tid / TK, tk = tid % TK;
+    const bool cplx = sizeof(T) == 16 && P.use;
+
+    // this thread's footprint cells: stage offset, in-plane source offset,
+    // validity, phase code
+    int soff[NC], goff[NC];
+    unsigned vmask = 0, pcode = 0;
+#pragma unroll
+    for (int i = 0; i < NC; i++) {
+        const int e = tid + i * NT;
+        soff[i] = 0;
+        goff[i] = 0;
+        if (e >= FY * FZ) continue;
+        const int y = e / FZ, z = e % FZ;
+        soff[i] = (z & 1) ? SE + y * FZO + (z >> 1) : y * FZE + (z >> 1);
+        const int py = 2 * J0 + y, pz = 2 * L0 + z;
+        if (py >= G.s[1] || pz >= G.s[2]) continue;
+        int iy = py - G.plo[1], iz = pz - G.plo[2];
+        const unsigned c1 = iy >= n1 ? 1u : (iy < 0 ? 2u : 0u);
+        const unsigned c2 = iz >= n2 ? 1u : (iz < 0 ? 2u : 0u);
+        if (wrap_c(iy, n1, G.g.periodic[1]) && wrap_c(iz, n2, G.g.periodic[2])) {
+            vmask |= 1u << i;
+            goff[i] = iy * n2 + iz;
+            pcode |= (c1 | (c2 << 2)) << (4 * i);
+        }
+    }
+    if (!cplx) pcode = 0;
+
+    // padded plane range for outputs [I0, I1): 2*I0 .. 2*(I1-1) + 2K - 2
+    const int x0a = 2 * I0;
+    const int nx = 2 * (I1 - I0) + 2 * K - 3;
+    auto plane_info = [&](int j, int& ip, int& wrapside) {
+        ip = x0a + j - G.plo[0];
+        wrapside = ip >= G.g.n[0] ? 0 : (ip < 0 ? 1 : -1);
+        return wrap_c(ip, G.g.n[0], G.g.periodic[0]);
+    };
+    auto issue = [&](int j) {
+        int ip, ws;
+        const bool pv = plane_info(j, ip, ws);
+        T* st = stage + (j % S) * SS;
+        const T* src = a + (long long)ip * n1 * n2;
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            if (tid + i * NT >= FY * FZ) break;
+            const bool ok = pv && ((vmask >> i) & 1);
+            cp_async_x<EB>(st + soff[i], ok ? src + goff[i] : a, ok);
+        }
+    };
+    auto fixup = [&](int j) {
+        int ip, ws;
+        plane_info(j, ip, ws);
+        const bool pw = cplx && ws >= 0 && G.g.periodic[0];
+        if (!pw && !pcode) return;
+        const double2 ph0 = ws == 0 ? P.ph[0][0] : P.ph[0][1];
+        T* st = stage + (j % S) * SS;
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            if (tid + i * NT >= FY * FZ) break;
+            const unsigned c = (pcode >> (4 * i)) & 15u;
+            if ((pw || c) && ((vmask >> i) & 1))
+                st[soff[i]] = apply_code<T>(st[soff[i]], c, pw, ph0, P);
+        }
+    };
 
     T ring[NR];
 #pragma unroll
     for (int i = 0; i < NR; i++) ring[i] = Num<T>::zero();
 
-    // padded plane range for outputs [I0, I1): 2*I0 .. 2*(I1-1) + 2K - 2
-    const int x0a = 2 * I0, x0b = 2 * (I1 - 1) + 2 * K - 2;
-    for (int x0 = x0a; x0 <= x0b; x0++) {
-        // 1. input footprint of the tile in this padded plane
-        for (int e = tid; e < FY * FZ; e += TJ * TK) {
-            const int y = e / FZ, z = e % FZ;
-            const int py = 2 * J0 + y, pz = 2 * L0 + z;
-            T v = Num<T>::zero();
-            if (py < G.s[1] && pz < G.s[2])
-                v = bc_read<T>(a, x0 - G.plo[0], py - G.plo[1], pz - G.plo[2], G.g, P, true);
-            F[y][z] = G.neg_in ? Num<T>::neg(v) : v;
-        }
-        __syncthreads();
-        // 2. axis-2 pass: R1[y][k] for every footprint row
-        for (int e = tid; e < FY * TK; e += TJ * TK) {
+#pragma unroll 1
+    for (int j = 0; j < D; j++) {
+        if (j < nx) issue(j);
+        cp_commit_x();
+    }
+#pragma unroll 1
+    for (int t = 0; t < nx; t++) {
+        cp_wait_x<D - 1>();
+        fixup(t);
+        __syncthreads();   // stage t visible; R1 free; slot (t+D)%S free
+        if (t + D < nx) issue(t + D);
+        cp_commit_x();
+        const T* Fe = stage + (t % S) * SS;
+        const T* Fo = Fe + SE;
+        // axis-2 pass: R1[y][k], centre at odd column K-1+2k
+        for (int e = tid; e < FY * TK; e += NT) {
             const int y = e / TK, k = e % TK;
-            const int c = K - 1 + 2 * k;
-            T x = F[y][c];
+            const T* re = Fe + y * FZE;
+            T x = Fo[y * FZO + K / 2 - 1 + k];
 #pragma unroll
             for (int l = 0; l < K / 2; l++)
-                x = Num<T>::add(x, Num<T>::scale(Num<T>::add(F[y][c + 2 * l + 1],
-                                                             F[y][c - 2 * l - 1]),
+                x = Num<T>::add(x, Num<T>::scale(Num<T>::add(re[K / 2 + k + l], re[K / 2 - 1 + k - l]),
                                                  G.w[l]));
-            R1[y][k] = Num<T>::scale(x, 0.5);
+            // restrict(-a) == -restrict(a) bit for bit (every step is odd)
+            const T r = Num<T>::scale(x, 0.5);
+            R1[y * TK + k] = G.neg_in ? Num<T>::neg(r) : r;
         }
         __syncthreads();
-        // 3. axis-1 pass for this thread's (j, k)
+        // axis-1 pass for this thread's (j, k), pushed into the axis-0 ring
         {
             const int c = K - 1 + 2 * tj;
-            T x = R1[c][tk];
+            T x = R1[c * TK + tk];
 #pragma unroll
             for (int l = 0; l < K / 2; l++)
-                x = Num<T>::add(x, Num<T>::scale(Num<T>::add(R1[c + 2 * l + 1][tk],
-                                                             R1[c - 2 * l - 1][tk]),
+                x = Num<T>::add(x, Num<T>::scale(Num<T>::add(R1[(c + 2 * l + 1) * TK + tk],
+                                                             R1[(c - 2 * l - 1) * TK + tk]),
                                                  G.w[l]));
 #pragma unroll
             for (int i = 0; i < NR - 1; i++) ring[i] = ring[i + 1];
             ring[NR - 1] = Num<T>::scale(x, 0.5);
         }
-        // 4. axis-0 pass once the ring spans planes 2I .. 2I + 2K - 2
-        const int q = x0 - 2 * I0;
-        if (q >= 2 * K - 2 && ((q - (2 * K - 2)) & 1) == 0) {
-            const int I = I0 + (q - (2 * K - 2)) / 2;
+        // axis-0 pass once the ring spans planes 2I .. 2I + 2K - 2
+        if (t >= 2 * K - 2 && ((t - (2 * K - 2)) & 1) == 0) {
+            const int I = I0 + (t - (2 * K - 2)) / 2;
             const int J = J0 + tj, L = L0 + tk;
             T x = ring[K - 1];
 #pragma unroll
@@ -113,8 +230,8 @@ k_restrict(const T* __restrict__ in, T* __restrict__ out, T* __restrict__ out2, 
                 if (out2) out2[b * ngout + at] = Num<T>::scale(r, G.scale2);
             }
         }
-        __syncthreads();
     }
+    cp_wait_x<0>();
 }
 
 // -------------------------------------------------------------- interpolate
@@ -135,14 +252,20 @@ __device__ __forceinline__ T ip_tap(const T* row, int stride, int u, int base, c
     return x;
 }
 
-template <class T, int K, int TJ, int TK>
+template <class T, int K, int TJ, int TK, int D>
 __global__ void __launch_bounds__(TJ * TK)
 k_interpolate(const T* __restrict__ in, T* __restrict__ out, int nin, XferGeom G, Phases P,
               int chunk0) {
+    constexpr int NT = TJ * TK;
     constexpr int CY = TJ / 2 + K + 1;     // coarse rows feeding TJ fine rows
     constexpr int CZ = TK / 2 + K + 1;
-    __shared__ T A[CY][CZ + 1];
-    __shared__ T Q[CY][TK];
+    constexpr int SS = CY * CZ;
+    constexpr int S = D + 1;
+    constexpr int NC = (SS + NT - 1) / NT;
+    constexpr int EB = (int)sizeof(T);
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* stage = reinterpret_cast<T*>(smem_raw);
+    T* Q = stage + S * SS;                 // [CY][TK]
 
     const int tiles2 = (G.nout[2] + TK - 1) / TK;
     const int F1 = (blockIdx.x / tiles2) * TJ;
@@ -153,69 +276,130 @@ k_interpolate(const T* __restrict__ in, T* __restrict__ out, int nin, XferGeom G
     const int ia = blockIdx.y * chunk0;
     const int ib = min(n0p, ia + chunk0);
     if (ia >= ib || b >= nin) return;
-    const long long ngin = (long long)G.g.n[0] * G.g.n[1] * G.g.n[2];
+    const int n1 = G.g.n[1], n2 = G.g.n[2];
+    const long long ngin = (long long)G.g.n[0] * n1 * n2;
     const long long ngout = (long long)G.nout[0] * G.nout[1] * G.nout[2];
     const T* a = in + b * ngin;
     T* o = out + b * ngout;
     const int tid = threadIdx.x;
     const int tj = tid / TK, tk = tid % TK;
+    const bool cplx = sizeof(T) == 16 && P.use;
 
     // coarse footprint origin along axes 1 and 2
     const int base1 = (F1 + G.skip0[1]) >> 1;
     const int base2 = (F2 + G.skip0[2]) >> 1;
+    int soff[NC], goff[NC];
+    unsigned vmask = 0, pcode = 0;
+#pragma unroll
+    for (int i = 0; i < NC; i++) {
+        const int e = tid + i * NT;
+        soff[i] = e;
+        goff[i] = 0;
+        if (e >= SS) continue;
+        const int y = e / CZ, z = e % CZ;
+        const int py = base1 + y, pz = base2 + z;
+        if (py >= G.s[1] || pz >= G.s[2]) continue;
+        int iy = py - G.plo[1], iz = pz - G.plo[2];
+        const unsigned c1 = iy >= n1 ? 1u : (iy < 0 ? 2u : 0u);
+        const unsigned c2 = iz >= n2 ? 1u : (iz < 0 ? 2u : 0u);
+        if (wrap_c(iy, n1, G.g.periodic[1]) && wrap_c(iz, n2, G.g.periodic[2])) {
+            vmask |= 1u << i;
+            goff[i] = iy * n2 + iz;
+            pcode |= (c1 | (c2 << 2)) << (4 * i);
+        }
+    }
+    if (!cplx) pcode = 0;
+
+    // coarse padded planes ia .. min(s0-1, ib-1+K-1)
+    const int nx = min(G.s[0] - 1, ib - 1 + K - 1) - ia + 1;
+    auto plane_info = [&](int j, int& ip, int& ws) {
+        ip = ia + j - G.plo[0];
+        ws = ip >= G.g.n[0] ? 0 : (ip < 0 ? 1 : -1);
+        return wrap_c(ip, G.g.n[0], G.g.periodic[0]);
+    };
+    auto issue = [&](int j) {
+        int ip, ws;
+        const bool pv = plane_info(j, ip, ws);
+        T* st = stage + (j % S) * SS;
+        const T* src = a + (long long)ip * n1 * n2;
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            if (tid + i * NT >= SS) break;
+            const bool ok = pv && ((vmask >> i) & 1);
+            cp_async_x<EB>(st + soff[i], ok ? src + goff[i] : a, ok);
+        }
+    };
+    auto fixup = [&](int j) {
+        int ip, ws;
+        plane_info(j, ip, ws);
+        const bool pw = cplx && ws >= 0 && G.g.periodic[0];
+        if (!pw && !pcode) return;
+        const double2 ph0 = ws == 0 ? P.ph[0][0] : P.ph[0][1];
+        T* st = stage + (j % S) * SS;
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            if (tid + i * NT >= SS) break;
+            const unsigned c = (pcode >> (4 * i)) & 15u;
+            if ((pw || c) && ((vmask >> i) & 1))
+                st[soff[i]] = apply_code<T>(st[soff[i]], c, pw, ph0, P);
+        }
+    };
 
     T ring[K];
 #pragma unroll
     for (int i = 0; i < K; i++) ring[i] = Num<T>::zero();
-
-    // pair i needs planes i .. i + K - 1 (odd) and K/2 - 1 + i (even)
-    const int xa = ia, xb = min(G.s[0] - 1, ib - 1 + K - 1);
-    for (int x0 = xa; x0 <= xb; x0++) {
-        for (int e = tid; e < CY * CZ; e += TJ * TK) {
-            const int y = e / CZ, z = e % CZ;
-            const int py = base1 + y, pz = base2 + z;
-            T v = Num<T>::zero();
-            if (py < G.s[1] && pz < G.s[2])
-                v = bc_read<T>(a, x0 - G.plo[0], py - G.plo[1], pz - G.plo[2], G.g, P, true);
-            A[y][z] = G.neg_in ? Num<T>::neg(v) : v;
+    const int f1 = F1 + tj, f2 = F2 + tk;
+    const bool inside = f1 < G.nout[1] && f2 < G.nout[2];
+    auto emit = [&](int u, T v) {
+        const int f0 = u - G.skip0[0];
+        if (inside && f0 >= 0 && f0 < G.nout[0]) {
+            T* dst = o + ((long long)f0 * G.nout[1] + f1) * G.nout[2] + f2;
+            // accumulate: phi -= I(phi_coarse) (gpaw/poisson.py:520-521)
+            *dst = G.accumulate ? Num<T>::sub(*dst, v) : v;
         }
+    };
+
+#pragma unroll 1
+    for (int j = 0; j < D; j++) {
+        if (j < nx) issue(j);
+        cp_commit_x();
+    }
+#pragma unroll 1
+    for (int t = 0; t < nx; t++) {
+        cp_wait_x<D - 1>();
+        fixup(t);
         __syncthreads();
-        for (int e = tid; e < CY * TK; e += TJ * TK) {
+        if (t + D < nx) issue(t + D);
+        cp_commit_x();
+        const T* A = stage + (t % S) * SS;
+        for (int e = tid; e < CY * TK; e += NT) {
             const int y = e / TK, k = e % TK;
             const int u = F2 + k + G.skip0[2];
-            Q[y][k] = (F2 + k < G.nout[2]) ? ip_tap<T, K>(&A[y][0], 1, u, base2, G.w)
-                                           : Num<T>::zero();
+            T v = (F2 + k < G.nout[2]) ? ip_tap<T, K>(A + y * CZ, 1, u, base2, G.w)
+                                        : Num<T>::zero();
+            Q[y * TK + k] = G.neg_in ? Num<T>::neg(v) : v;
         }
         __syncthreads();
         {
             const int u = F1 + tj + G.skip0[1];
-            T v = (F1 + tj < G.nout[1]) ? ip_tap<T, K>(&Q[0][tk], TK, u, base1, G.w)
+            T v = (F1 + tj < G.nout[1]) ? ip_tap<T, K>(Q + tk, TK, u, base1, G.w)
                                         : Num<T>::zero();
 #pragma unroll
             for (int i = 0; i < K - 1; i++) ring[i] = ring[i + 1];
             ring[K - 1] = v;
         }
+        const int x0 = ia + t;
         // emit the pair i = x0 - (K - 1) (or the final even point when the
         // odd one is skipped and plane i + K - 1 lies past the input)
-        const int f1 = F1 + tj, f2 = F2 + tk;
-        const bool inside = f1 < G.nout[1] && f2 < G.nout[2];
-        auto emit = [&](int u, T v) {
-            const int f0 = u - G.skip0[0];
-            if (inside && f0 >= 0 && f0 < G.nout[0]) {
-                T* dst = o + ((long long)f0 * G.nout[1] + f1) * G.nout[2] + f2;
-                // accumulate: phi -= I(phi_coarse) (gpaw/poisson.py:520-521)
-                *dst = G.accumulate ? Num<T>::sub(*dst, v) : v;
-            }
-        };
         const int i = x0 - (K - 1);
         if (i >= ia && i < ib) {
             emit(2 * i, ring[K / 2 - 1]);
             T x = Num<T>::scale(Num<T>::add(ring[K / 2 - 1], ring[K / 2]), G.w[0]);
 #pragma unroll
-            for (int j = 1; j < K / 2; j++)
-                x = Num<T>::add(x, Num<T>::scale(Num<T>::add(ring[K / 2 - 1 - j],
-                                                             ring[K / 2 + j]),
-                                                 G.w[j]));
+            for (int jj = 1; jj < K / 2; jj++)
+                x = Num<T>::add(x, Num<T>::scale(Num<T>::add(ring[K / 2 - 1 - jj],
+                                                             ring[K / 2 + jj]),
+                                                 G.w[jj]));
             emit(2 * i + 1, x);
         }
         if (x0 == G.s[0] - 1 && ib - 1 + K - 1 > x0) {
@@ -223,39 +407,63 @@ k_interpolate(const T* __restrict__ in, T* __restrict__ out, int nin, XferGeom G
             const int il = ib - 1;
             if (il >= ia && il == x0 - (K - 2)) emit(2 * il, ring[K / 2]);
         }
-        __syncthreads();
     }
+    cp_wait_x<0>();
 }
 
 // ----------------------------------------------------------------- launchers
 template <class T, int K>
-static void launch_restrict_k(const void* in, void* out, void* out2, int nin, const XferGeom& G,
-                              const Phases& P, cudaStream_t st) {
-    // 16-byte elements: a square tile keeps the footprint under 48 KB
+static int launch_restrict_k(const void* in, void* out, void* out2, int nin, const XferGeom& G,
+                             const Phases& P, cudaStream_t st) {
+    // 16-byte elements: a square 16 x 16 tile; 8-byte: 8 x 32
     constexpr int TK = sizeof(T) == 16 ? 16 : 32;
     constexpr int TJ = 256 / TK;
+    constexpr int D = sizeof(T) == 16 ? 2 : 3;
+    constexpr int H = 2 * K - 3, FY = 2 * TJ + H, FZ = 2 * TK + H;
+    constexpr int SS = FY * ((FZ + 1) / 2) + FY * (FZ / 2);
+    constexpr size_t smem = ((size_t)(D + 1) * SS + (size_t)FY * TK) * sizeof(T);
+    static bool attr = false;
+    if (!attr) {
+        if (cudaFuncSetAttribute(k_restrict<T, K, TJ, TK, D>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess)
+            return -2;
+        attr = true;
+    }
     const int t1 = (G.nout[1] + TJ - 1) / TJ, t2 = (G.nout[2] + TK - 1) / TK;
     int chunk0 = G.nout[0];
-    // enough CTAs to fill the GPU several times over
     const long long tiles = (long long)t1 * t2 * nin;
-    while (chunk0 > 4 && tiles * ((G.nout[0] + chunk0 - 1) / chunk0) < 148 * 8) chunk0 = (chunk0 + 1) / 2;
+    while (chunk0 > 4 && tiles * ((G.nout[0] + chunk0 - 1) / chunk0) < 148 * 4)
+        chunk0 = (chunk0 + 1) / 2;
     const int nchunks = (G.nout[0] + chunk0 - 1) / chunk0;
     for (int b0 = 0; b0 < nin; b0 += 65535) {
         const int nb = min(65535, nin - b0);
         dim3 grid(t1 * t2, nchunks, nb);
         const long long ngin = (long long)G.g.n[0] * G.g.n[1] * G.g.n[2];
         const long long ngout = (long long)G.nout[0] * G.nout[1] * G.nout[2];
-        k_restrict<T, K, TJ, TK><<<grid, TJ * TK, 0, st>>>(
+        k_restrict<T, K, TJ, TK, D><<<grid, TJ * TK, smem, st>>>(
             (const T*)in + b0 * ngin, (T*)out + b0 * ngout,
             out2 ? (T*)out2 + b0 * ngout : nullptr, nb, G, P, chunk0);
     }
+    return 0;
 }
 
 template <class T, int K>
-static void launch_interp_k(const void* in, void* out, int nin, const XferGeom& G,
-                            const Phases& P, cudaStream_t st) {
+static int launch_interp_k(const void* in, void* out, int nin, const XferGeom& G,
+                           const Phases& P, cudaStream_t st) {
     constexpr int TK = sizeof(T) == 16 ? 16 : 32;
     constexpr int TJ = 256 / TK;
+    constexpr int D = 3;
+    constexpr int CY = TJ / 2 + K + 1, CZ = TK / 2 + K + 1;
+    constexpr size_t smem = ((size_t)(D + 1) * CY * CZ + (size_t)CY * TK) * sizeof(T);
+    static bool attr = false;
+    if (!attr) {
+        if (cudaFuncSetAttribute(k_interpolate<T, K, TJ, TK, D>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess)
+            return -2;
+        attr = true;
+    }
     const int t1 = (G.nout[1] + TJ - 1) / TJ, t2 = (G.nout[2] + TK - 1) / TK;
     const int n0p = G.s[0] - (K - 1) + G.skip1[0];
     int chunk0 = n0p;
@@ -267,9 +475,10 @@ static void launch_interp_k(const void* in, void* out, int nin, const XferGeom& 
         dim3 grid(t1 * t2, nchunks, nb);
         const long long ngin = (long long)G.g.n[0] * G.g.n[1] * G.g.n[2];
         const long long ngout = (long long)G.nout[0] * G.nout[1] * G.nout[2];
-        k_interpolate<T, K, TJ, TK><<<grid, TJ * TK, 0, st>>>(
+        k_interpolate<T, K, TJ, TK, D><<<grid, TJ * TK, smem, st>>>(
             (const T*)in + b0 * ngin, (T*)out + b0 * ngout, nb, G, P, chunk0);
     }
+    return 0;
 }
 
 template <class T>
@@ -278,17 +487,17 @@ int launch_transform(int k, bool interpolate, const void* in, void* out, void* o
     const int K = k;
     if (interpolate) {
         switch (K) {
-            case 2: launch_interp_k<T, 2>(in, out, nin, G, P, st); return 0;
-            case 4: launch_interp_k<T, 4>(in, out, nin, G, P, st); return 0;
-            case 6: launch_interp_k<T, 6>(in, out, nin, G, P, st); return 0;
-            case 8: launch_interp_k<T, 8>(in, out, nin, G, P, st); return 0;
+            case 2: return launch_interp_k<T, 2>(in, out, nin, G, P, st);
+            case 4: return launch_interp_k<T, 4>(in, out, nin, G, P, st);
+            case 6: return launch_interp_k<T, 6>(in, out, nin, G, P, st);
+            case 8: return launch_interp_k<T, 8>(in, out, nin, G, P, st);
         }
     } else {
         switch (K) {
-            case 2: launch_restrict_k<T, 2>(in, out, out2, nin, G, P, st); return 0;
-            case 4: launch_restrict_k<T, 4>(in, out, out2, nin, G, P, st); return 0;
-            case 6: launch_restrict_k<T, 6>(in, out, out2, nin, G, P, st); return 0;
-            case 8: launch_restrict_k<T, 8>(in, out, out2, nin, G, P, st); return 0;
+            case 2: return launch_restrict_k<T, 2>(in, out, out2, nin, G, P, st);
+            case 4: return launch_restrict_k<T, 4>(in, out, out2, nin, G, P, st);
+            case 6: return launch_restrict_k<T, 6>(in, out, out2, nin, G, P, st);
+            case 8: return launch_restrict_k<T, 8>(in, out, out2, nin, G, P, st);
         }
     }
     return -1;

@@ -208,27 +208,42 @@ def test_transformers_random(nn, pbc, dtype, cuda):
 
 
 def test_transformers_conserve_integral(cuda):
-    """gpaw/test/fd_ops/test_transformations.py and test_non_periodic.py."""
+    """gpaw/test/fd_ops/test_transformations.py:11-52 (periodic, default
+    unit cell, k = 2..8, real and complex) and test_non_periodic.py:7-27."""
     from gpaw_b200 import Transformer
-    rng = np.random.RandomState(8)
 
     def integrate(g, t):
         # numpy's pairwise sum, as gd.integrate in the reference tests
         return to_np(t).sum() * g.dv
 
-    for pbc, tol in ((1, 1e-14), (0, 1e-10)):
-        gd = prod_gd((20, 20, 20), (8.0, 8.0, 8.0), pbc)
-        a = to_dev(rng.random(tuple(gd.n_c)))
-        for k in (2, 4, 6, 8):
-            if pbc == 0 and k > 2:
-                continue
-            fine = gd.refine()
-            b = Transformer(gd, fine, k // 2).apply(a)
-            assert abs(integrate(gd, a) - integrate(fine, b)) < tol
-            if pbc:
-                coarse = gd.coarsen()
-                b = Transformer(gd, coarse, k // 2).apply(a)
-                assert abs(integrate(gd, a) - integrate(coarse, b)) < tol
+    n = 20
+    gd = prod_gd((n, n, n), (1, 1, 1), 1)
+    rng = np.random.RandomState(8)
+    a = rng.random(tuple(gd.n_c))
+    for dtype, phase in ((float, None), (complex, np.ones((3, 2), complex))):
+        if dtype == complex:
+            a = np.empty(tuple(gd.n_c), complex)
+            a.real = rng.random(a.shape)
+            a.imag = rng.random(a.shape)
+        for g2 in (gd.refine(), gd.coarsen()):
+            for k in (2, 4, 6, 8):
+                b = Transformer(gd, g2, k // 2, dtype).apply(to_dev(a),
+                                                             phases=phase)
+                assert abs(integrate(gd, to_dev(a)) - integrate(g2, b)) \
+                    < 1e-14
+    # zero boundaries
+    gd1 = prod_gd((n, n, n), (8.0, 8.0, 8.0), 0)
+    rng = np.random.default_rng(8)
+    a1 = rng.random(tuple(gd1.n_c))
+    gd2 = gd1.refine()
+    a2 = to_np(Transformer(gd1, gd2).apply(to_dev(a1)))
+    assert abs(a1.sum() * gd1.dv - a2.sum() * gd2.dv) < 1e-10
+    for sl in (0, -1):
+        a2[sl] = 0.0
+        a2[:, sl] = 0.0
+        a2[:, :, sl] = 0.0
+    a1 = to_np(Transformer(gd2, gd1).apply(to_dev(a2)))
+    assert abs(a1.sum() * gd1.dv - a2.sum() * gd2.dv) < 1e-10
 
 
 @pytest.mark.parametrize('method', [1, 2])
