@@ -31,6 +31,8 @@ SIGNATURES = {
     'gb_operator_apply': (C.c_int, [_p, _p, _p, C.c_int64, C.c_int, _dp, _p]),
     'gb_operator_relax': (C.c_int, [_p, C.c_int, _p, _p, C.c_int, C.c_double,
                                     _p]),
+    'gb_operator_relax_noalloc': (C.c_int, [_p, C.c_int, _p, _p, C.c_int,
+                                            C.c_double, _p]),
     'gb_operator_residual': (C.c_int, [_p, _p, _p, _p, C.c_int64, C.c_int,
                                        _dp, C.c_double, _p, _p]),
     'gb_operator_get_diagonal_element': (C.c_double, [_p]),

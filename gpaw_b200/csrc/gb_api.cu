@@ -7,6 +7,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -692,5 +693,100 @@ extern "C" int gb_poisson_solve_neutral(gb_poisson* p, double* phi, const double
         k_sub_scalar<<<nb, 256, 0, st>>>(phi, n, p->mean_dev, (double)n);
         GB_LAUNCH_CHECK();
     }
+    return 0;
+}
+
+// ------------------------------------------------- relax without allocation
+// Some callers cannot let this library call cudaMalloc: a host program that
+// has handed all of HBM to its own memory pool (a cudaMalloc would fail or
+// force the pool to release cached blocks), a latency-critical serving loop
+// that must not risk the implicit device synchronisation cudaMalloc and
+// cudaFree may perform, or a plugin host that forbids allocations outside
+// its own allocator.  gb_operator_relax_noalloc serves them: the scratch
+// grid that relaxation needs (the Jacobi ping-pong buffer, the Gauss-Seidel
+// start-of-sweep snapshot) lives in the fixed device array below instead of
+// the operator's lazily allocated buffer.
+//
+// The array is GB_NOALLOC_MAX_POINTS doubles (16 MiB); every GPU that loads
+// the library holds it until the process exits.  All calls share it, so
+// calls that overlap on the GPU (other streams, other threads) race; calls
+// on one stream are ordered.  It keeps the last call's contents; nothing
+// needs to start at zero, because each sweep writes every point of the
+// scratch before reading it.
+static __device__ __align__(256) double g_relax_scratch[GB_NOALLOC_MAX_POINTS];
+
+namespace {
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[256] = {};   // device address of g_relax_scratch, per device
+}  // namespace
+
+// Host code must not use g_relax_scratch's name as a device address (it is a
+// host-side stand-in); the first call on each device looks the address up
+// with that device current and caches it.
+static int noalloc_scratch(double** out) {
+    int dev = 0;
+    GB_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 256) return fail(GB_EINVAL, "relax_noalloc: device index %d", dev);
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_relax_scratch);
+        if (e != cudaSuccess || !p)
+            return fail(GB_ECUDA, "relax_noalloc: cudaGetSymbolAddress: %s",
+                        cudaGetErrorString(e));
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = (double*)g_noalloc_ptr[dev];
+    return 0;
+}
+
+extern "C" int gb_operator_relax_noalloc(gb_operator* op, int method, double* f,
+                                         const double* s, int nrelax, double w, void* stream) {
+    if (!op || !f || !s) return fail(GB_EINVAL, "relax_noalloc: NULL argument");
+    if (!op->real) return fail(GB_EINVAL, "relax_noalloc: float64 operators only");
+    if (method != 1 && method != 2) return fail(GB_EINVAL, "relax_noalloc: method must be 1 or 2");
+    if (op->ng() > (long long)GB_NOALLOC_MAX_POINTS)
+        return fail(GB_EINVAL,
+                    "relax_noalloc: grid has %lld points, more than the %d this entry point "
+                    "supports; use gb_operator_relax",
+                    op->ng(), (int)GB_NOALLOC_MAX_POINTS);
+    if (nrelax <= 0) return 0;
+    double* X = nullptr;
+    if (int rc = noalloc_scratch(&X)) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t bytes = (size_t)op->ng() * sizeof(double);
+    if (method == 1) {
+        const int r = op->st.range;
+        int wa = 1, wb = 1;
+        if (!op->st.cfd) {
+            wb = 2 * r + 1;
+            wa = (wb + 1) * r + 1;
+        }
+        const GridBC& g = op->g;
+        const int nt = wa * (g.n[0] - 1) + wb * (g.n[1] - 1) + g.n[2];
+        const bool periodic = g.periodic[0] || g.periodic[1] || g.periodic[2];
+        const double inv0 = 1.0 / op->st.coef[0];
+        for (int it = 0; it < nrelax; it++) {
+            if (periodic) GB_CUDA_TRY(cudaMemcpyAsync(X, f, bytes, cudaMemcpyDeviceToDevice, st));
+            for (int t = 0; t < nt; t++)
+                launch_gs_wave(f, periodic ? X : f, s, g, op->st, t, wa, wb, inv0, st);
+            GB_LAUNCH_CHECK();
+        }
+        return 0;
+    }
+    const double* src = f;
+    if (nrelax % 2 == 1) {
+        GB_CUDA_TRY(cudaMemcpyAsync(X, f, bytes, cudaMemcpyDeviceToDevice, st));
+        src = X;
+    }
+    Phases P0;
+    memset(&P0, 0, sizeof P0);
+    for (int it = 0; it < nrelax; it++) {
+        double* dst = (src == f) ? X : f;
+        if (int rc = op_sweep(op, EPI_JACOBI, src, dst, s, 1, GB_F64, P0, w, 0, 0, nullptr, st))
+            return rc;
+        src = dst;
+    }
+    GB_LAUNCH_CHECK();
     return 0;
 }

@@ -94,6 +94,21 @@ GB_API int gb_operator_apply(gb_operator* op, const void* in, void* out, int64_t
 GB_API int gb_operator_relax(gb_operator* op, int method, double* f, const double* s,
                       int nrelax, double w, void* stream);
 
+/* Variant of gb_operator_relax that allocates nothing; it has no
+ * counterpart in the reference.  For callers that cannot let the library
+ * call cudaMalloc (all of HBM handed to their own pool, a serving loop that
+ * must not risk the implicit synchronisation of cudaMalloc/cudaFree, a plugin
+ * host that forbids foreign allocations).  Its scratch grid is a fixed
+ * device array of GB_NOALLOC_MAX_POINTS doubles (16 MiB, held by every GPU
+ * that loads the library until exit); grids with more points are rejected
+ * with GB_EINVAL.  The first call on a device looks the array's address up
+ * (cudaGetSymbolAddress), so make that first call before any stream capture.
+ * All calls share the array: calls that overlap on the GPU race.  Same
+ * results as gb_operator_relax. */
+#define GB_NOALLOC_MAX_POINTS (2 * 1024 * 1024)
+GB_API int gb_operator_relax_noalloc(gb_operator* op, int method, double* f, const double* s,
+                                     int nrelax, double w, void* stream);
+
 /* Residual r = L(phi) - rho for a batch (gpaw/poisson.py:517-518 done in
  * one pass).  r may be NULL.  If norm2 is not NULL it receives, per grid,
  * scale * sum |r|^2 as a DEVICE array of nin doubles (the reference's
