@@ -203,6 +203,46 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------- Poisson
+def poisson_c1(dev, nsolve=20):
+    """64^3 zero-BC FDPoissonSolver (nn = 3, Jacobi, reference schedule),
+    h = 0.2 A, 8 Gaussians: solves/s at the reference's eps = 2e-10 and at
+    the eps that gives 1e-10 relative residual."""
+    import torch
+    from gpaw_b200 import FDPoissonSolver, GridDescriptor
+    from gpaw_b200.workloads import (BOHR, c1_density,
+                                     eps_for_relative_residual, neutralize)
+    h = 0.2 / BOHR
+    gd = GridDescriptor((64, 64, 64), (64 * h,) * 3, 0, device=dev)
+    rho = neutralize(c1_density(gd), gd)
+    rho_d = torch.from_numpy(rho).to(dev)
+    rnorm = float(np.sqrt((rho * rho).sum()))
+    out = {'grid': [64, 64, 64], 'h_angstrom': 0.2, 'precision': 'fp64'}
+    for tag, eps in (('eps_2e-10', 2e-10),
+                     ('rel_1e-10', eps_for_relative_residual(rho, gd))):
+        ps = FDPoissonSolver(nn=3, relax='J', eps=eps)
+        ps.set_grid_descriptor(gd)
+        phi = gd.zeros()
+        ps.solve_neutral(phi, rho_d)          # warm-up (builds the graph)
+        times = []
+        for _ in range(nsolve):
+            phi.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            n = ps.solve_neutral(phi, rho_d)
+            times.append(time.perf_counter() - t0)
+        r = torch.empty_like(phi)
+        n2 = torch.zeros(1, dtype=torch.float64, device=dev)
+        ps.operators[0].residual(phi, rho_d, r, None, 1.0, n2)
+        rel = float(np.sqrt(n2.item())) / rnorm
+        t = float(np.median(times))
+        out[tag] = {'eps': eps, 'vcycles': n, 'ms_per_solve': t * 1e3,
+                    'solves_per_s': 1.0 / t, 'rel_residual': rel,
+                    'p50_ms': t * 1e3,
+                    'p99_ms': float(np.percentile(times, 99)) * 1e3}
+    return out
+
+
 # ---------------------------------------------------------------- GPU side
 def run_gpu(args):
     import torch
@@ -346,6 +386,8 @@ def run_gpu(args):
         'e2e': e2e,
         'cpu_baseline': cpu_base,
     }
+    if not args.no_poisson:
+        line['poisson'] = {'c1': poisson_c1(dev)}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -363,6 +405,7 @@ def main():
     p.add_argument('--impl', default='gpaw_b200')
     p.add_argument('--no-cpu', action='store_true')
     p.add_argument('--no-e2e', action='store_true')
+    p.add_argument('--no-poisson', action='store_true')
     p.add_argument('--batch', type=int, default=NBANDS,
                    help='wave functions per step (profiling runs only)')
     args = p.parse_args()

@@ -507,6 +507,29 @@ extern "C" int gb_fd_precond(gb_transformer* rest0, gb_transformer* rest1, gb_tr
 }
 
 // --------------------------------------------------------------- FD Poisson
+struct SolveCtl {
+    double eps;
+    double err;
+    int maxiter;
+    int niter;
+};
+
+// After each V-cycle: niter += 1; keep looping while err > eps and
+// niter < maxiter (gpaw/poisson.py:484-486).
+__global__ void k_solve_check(SolveCtl* ctl, const double* err, cudaGraphConditionalHandle h) {
+    const int n = ctl->niter + 1;
+    ctl->niter = n;
+    ctl->err = err[0];
+    cudaGraphSetConditional(h, (err[0] > ctl->eps && n < ctl->maxiter) ? 1u : 0u);
+}
+
+__global__ void k_solve_init(SolveCtl* ctl, double eps, int maxiter) {
+    ctl->eps = eps;
+    ctl->maxiter = maxiter;
+    ctl->niter = 0;
+    ctl->err = 0.0;
+}
+
 struct gb_poisson {
     int L;  // coarsest level index
     std::vector<gb_operator*> ops;
@@ -520,7 +543,21 @@ struct gb_poisson {
     double* err_dev = nullptr;
     double* err_host = nullptr;
     double* mean_dev = nullptr;
+    // device-resident solve: own copies of phi0/rho0, a control block and a
+    // graph holding   while (err > eps && niter < maxiter) { V-cycle }
+    double* phi0 = nullptr;
+    double* rho0 = nullptr;
+    SolveCtl* ctl = nullptr;
+    SolveCtl* ctl_host = nullptr;
+    cudaStream_t cap = nullptr;
+    cudaGraphExec_t solve_exec = nullptr;
     ~gb_poisson() {
+        if (solve_exec) cudaGraphExecDestroy(solve_exec);
+        if (cap) cudaStreamDestroy(cap);
+        cudaFree(phi0);
+        cudaFree(rho0);
+        cudaFree(ctl);
+        if (ctl_host) cudaFreeHost(ctl_host);
         for (size_t l = 1; l < phi.size(); l++) cudaFree(phi[l]);
         for (size_t l = 1; l < rho.size(); l++) cudaFree(rho[l]);
         for (double* p : res) cudaFree(p);
@@ -591,6 +628,12 @@ extern "C" int gb_poisson_new(int nlevels, gb_operator* const* operators,
     if (e == cudaSuccess) e = cudaMalloc(&p->err_dev, sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&p->mean_dev, sizeof(double));
     if (e == cudaSuccess) e = cudaMallocHost(&p->err_host, sizeof(double));
+    const size_t bytes0 = (size_t)p->ops[0]->ng() * sizeof(double);
+    if (e == cudaSuccess) e = cudaMalloc(&p->phi0, bytes0);
+    if (e == cudaSuccess) e = cudaMalloc(&p->rho0, bytes0);
+    if (e == cudaSuccess) e = cudaMalloc(&p->ctl, sizeof(SolveCtl));
+    if (e == cudaSuccess) e = cudaMallocHost(&p->ctl_host, sizeof(SolveCtl));
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->cap, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         delete p;
         return fail(GB_ECUDA, "Poisson: allocation: %s", cudaGetErrorString(e));
@@ -668,31 +711,97 @@ __global__ void k_block_sums(const double* a, long long n, double* partial) {
     if (threadIdx.x == 0) partial[blockIdx.x] = v;
 }
 
+static int mean_removal(gb_poisson* p, double* phi, cudaStream_t st) {
+    const GridBC& g = p->ops[0]->g;
+    if (!(g.periodic[0] && g.periodic[1] && g.periodic[2])) return 0;
+    const long long n = p->ops[0]->ng();
+    const int nb = (int)std::min<long long>(1024, (n + 255) / 256);
+    k_block_sums<<<nb, 256, 0, st>>>(phi, n, p->partial);
+    launch_reduce_partials(p->partial, nb, 1, 1.0, p->mean_dev, st);
+    k_sub_scalar<<<nb, 256, 0, st>>>(phi, n, p->mean_dev, (double)n);
+    GB_LAUNCH_CHECK();
+    return 0;
+}
+
+// Capture the whole solve_neutral loop once per executor into a graph with
+// a conditional WHILE node: the V-cycle and a check kernel that sets the
+// loop condition, then the periodic mean removal.  It works on the
+// executor's own phi0/rho0, so one graph serves every call.
+static int build_solve_graph(gb_poisson* p) {
+    cudaStream_t cs = p->cap;
+    // one uncaptured V-cycle first: sets kernel attributes, touches scratch
+    GB_CUDA_TRY(cudaMemsetAsync(p->phi0, 0, (size_t)p->ops[0]->ng() * 8, cs));
+    GB_CUDA_TRY(cudaMemsetAsync(p->rho0, 0, (size_t)p->ops[0]->ng() * 8, cs));
+    p->phi[0] = p->phi0;
+    p->rho[0] = p->rho0;
+    if (int rc = vcycle(p, 0, cs)) return rc;
+    if (int rc = mean_removal(p, p->phi0, cs)) return rc;
+    GB_CUDA_TRY(cudaStreamSynchronize(cs));
+
+    cudaGraph_t graph;
+    GB_CUDA_TRY(cudaGraphCreate(&graph, 0));
+    cudaGraphConditionalHandle h;
+    GB_CUDA_TRY(cudaGraphConditionalHandleCreate(&h, graph, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t wnode;
+    GB_CUDA_TRY(cudaGraphAddNode(&wnode, graph, nullptr, 0, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    GB_CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0,
+                                              cudaStreamCaptureModeThreadLocal));
+    int rc = vcycle(p, 0, cs);
+    if (!rc) k_solve_check<<<1, 1, 0, cs>>>(p->ctl, p->err_dev, h);
+    cudaGraph_t body_out = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(cs, &body_out);
+    if (rc) {
+        cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (ce != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        return fail(GB_ECUDA, "Poisson: capture of the V-cycle: %s", cudaGetErrorString(ce));
+    }
+    // mean removal after the loop (periodic grids)
+    GB_CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, graph, &wnode, nullptr, 1,
+                                              cudaStreamCaptureModeThreadLocal));
+    rc = mean_removal(p, p->phi0, cs);
+    cudaGraph_t g2 = nullptr;
+    ce = cudaStreamEndCapture(cs, &g2);
+    if (rc || ce != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        return rc ? rc : fail(GB_ECUDA, "Poisson: capture: %s", cudaGetErrorString(ce));
+    }
+    cudaError_t ie = cudaGraphInstantiate(&p->solve_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) return fail(GB_ECUDA, "Poisson: instantiate: %s", cudaGetErrorString(ie));
+    return 0;
+}
+
 extern "C" int gb_poisson_solve_neutral(gb_poisson* p, double* phi, const double* rho, double eps,
                                         int maxiter, int* niter, double* error, void* stream) {
     if (!p || !phi || !rho) return fail(GB_EINVAL, "Poisson solve: NULL argument");
+    if (maxiter < 1) return fail(GB_EINVAL, "Poisson solve: maxiter must be >= 1");
     cudaStream_t st = (cudaStream_t)stream;
-    int it = 1;
-    double err = 0.0;
-    // while self.iterate2(self.step) > eps and niter < maxiter: niter += 1
-    while (true) {
-        if (int rc = gb_poisson_iterate(p, phi, rho, &err, stream)) return rc;
-        if (!(err > eps && it < maxiter)) break;
-        it++;
-    }
+    if (!p->solve_exec)
+        if (int rc = build_solve_graph(p)) return rc;
+    const size_t bytes = (size_t)p->ops[0]->ng() * sizeof(double);
+    // rhos[0][:] = rho; phis[0] = phi  (gpaw/poisson.py:476-482)
+    GB_CUDA_TRY(cudaMemcpyAsync(p->rho0, rho, bytes, cudaMemcpyDeviceToDevice, st));
+    GB_CUDA_TRY(cudaMemcpyAsync(p->phi0, phi, bytes, cudaMemcpyDeviceToDevice, st));
+    k_solve_init<<<1, 1, 0, st>>>(p->ctl, eps, maxiter);
+    GB_LAUNCH_CHECK();
+    GB_CUDA_TRY(cudaGraphLaunch(p->solve_exec, st));
+    GB_CUDA_TRY(cudaMemcpyAsync(phi, p->phi0, bytes, cudaMemcpyDeviceToDevice, st));
+    GB_CUDA_TRY(cudaMemcpyAsync(p->ctl_host, p->ctl, sizeof(SolveCtl), cudaMemcpyDeviceToHost, st));
+    GB_CUDA_TRY(cudaStreamSynchronize(st));
+    const int it = p->ctl_host->niter;
     if (niter) *niter = it;
-    if (error) *error = err;
-    if (it == maxiter)
+    if (error) *error = p->ctl_host->err;
+    if (it >= maxiter)
         return fail(GB_ENOCONV, "Poisson solver did not converge in %d iterations!", maxiter);
-    const GridBC& g = p->ops[0]->g;
-    if (g.periodic[0] && g.periodic[1] && g.periodic[2]) {
-        const long long n = p->ops[0]->ng();
-        const int nb = (int)std::min<long long>(1024, (n + 255) / 256);
-        k_block_sums<<<nb, 256, 0, st>>>(phi, n, p->partial);
-        launch_reduce_partials(p->partial, nb, 1, 1.0, p->mean_dev, st);
-        k_sub_scalar<<<nb, 256, 0, st>>>(phi, n, p->mean_dev, (double)n);
-        GB_LAUNCH_CHECK();
-    }
     return 0;
 }
 

@@ -1,0 +1,59 @@
+"""Seeded synthetic inputs with the shapes of the benchmark configurations.
+
+No dataset is involved: densities are sums of normalised Gaussians
+q (pi w^2)^(-3/2) exp(-|r - c|^2 / w^2) at seeded positions, as the
+benchmark configurations describe them; lengths in Bohr.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+BOHR = 0.52917721  # Angstrom
+
+
+def gaussian_density(gd, centers, widths, charges):
+    """Sum of normalised Gaussians on the points of ``gd`` (numpy, float64).
+
+    Evaluated one Gaussian at a time (float64 throughout)."""
+    r = gd.get_grid_point_coordinates()
+    rho = np.zeros(tuple(int(x) for x in gd.n_c))
+    for c, w, q in zip(centers, widths, charges):
+        d2 = ((r - np.asarray(c)[:, None, None, None])**2).sum(0)
+        rho += q * (np.pi * w * w)**-1.5 * np.exp(-d2 / (w * w))
+    return rho
+
+
+def c1_density(gd, seed=0):
+    """8 Gaussians, width 0.8 A, centres uniform in [0.25, 0.75] of the box,
+    charges +1/-1 alternating (net zero before discretisation)."""
+    rng = np.random.default_rng(seed)
+    L = np.diag(gd.cell_cv)
+    centers = [rng.uniform(0.25, 0.75, 3) * L for _ in range(8)]
+    widths = [0.8 / BOHR] * 8
+    charges = [1.0 if i % 2 == 0 else -1.0 for i in range(8)]
+    return gaussian_density(gd, centers, widths, charges)
+
+
+def c3_density(gd, ngauss=64, seed=0):
+    """`ngauss` Gaussians, widths U[0.5, 1.2] A, charges +-U[0.5, 2] with a
+    random sign, centres uniform in [0.2, 0.8] of the box; the caller
+    neutralises by subtracting the mean."""
+    rng = np.random.default_rng(seed)
+    L = np.diag(gd.cell_cv)
+    centers = [rng.uniform(0.2, 0.8, 3) * L for _ in range(ngauss)]
+    widths = rng.uniform(0.5, 1.2, ngauss) / BOHR
+    charges = rng.uniform(0.5, 2.0, ngauss) * rng.choice([-1.0, 1.0], ngauss)
+    return gaussian_density(gd, centers, widths, charges)
+
+
+def neutralize(rho, gd):
+    """rho - background, as the neutral branch of the solver forms it
+    (gpaw/poisson.py:186-213): charge / dv / number of points."""
+    charge = rho.sum() * gd.dv
+    return rho - charge / gd.dv / np.prod(gd.n_c)
+
+
+def eps_for_relative_residual(rho, gd, rel=1e-10):
+    """The reference stops when sum(r^2) dv <= eps (gpaw/poisson.py:485,
+    527-537); this eps corresponds to ||L phi - rho|| / ||rho|| = rel."""
+    return (rel * float(np.sqrt((rho * rho).sum())))**2 * gd.dv
