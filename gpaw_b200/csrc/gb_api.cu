@@ -11,15 +11,14 @@
 #include <string>
 #include <vector>
 
-#include "../../include/gpaw_b200.h"
-#include "gb_internal.cuh"
+#include "gb_objects.cuh"
 
 using namespace gb;
 
 // ------------------------------------------------------------------- errors
 static thread_local std::string g_err;
 
-static int fail(int code, const char* fmt, ...) {
+int gb::fail(int code, const char* fmt, ...) {
     char buf[512];
     va_list ap;
     va_start(ap, fmt);
@@ -29,124 +28,9 @@ static int fail(int code, const char* fmt, ...) {
     return code;
 }
 
-#define GB_CUDA_TRY(expr)                                                             \
-    do {                                                                              \
-        cudaError_t e_ = (expr);                                                      \
-        if (e_ != cudaSuccess)                                                        \
-            return fail(GB_ECUDA, "%s: %s (%s:%d)", #expr, cudaGetErrorString(e_),     \
-                        __FILE__, __LINE__);                                          \
-    } while (0)
-
-#define GB_LAUNCH_CHECK()                                                             \
-    do {                                                                              \
-        cudaError_t e_ = cudaGetLastError();                                          \
-        if (e_ != cudaSuccess)                                                        \
-            return fail(GB_ECUDA, "kernel launch: %s (%s:%d)", cudaGetErrorString(e_), \
-                        __FILE__, __LINE__);                                          \
-    } while (0)
 
 extern "C" int gb_version(void) { return 100; }
 extern "C" const char* gb_last_error(void) { return g_err.c_str(); }
-
-// ------------------------------------------------------------------ scratch
-// Device buffer owned by an object; grows on demand (never inside a
-// caller's stream capture if gb_*_reserve was called first).
-struct Scratch {
-    void* ptr = nullptr;
-    size_t bytes = 0;
-    ~Scratch() {
-        if (ptr) cudaFree(ptr);
-    }
-    int ensure(size_t want) {
-        if (want <= bytes) return 0;
-        if (ptr) cudaFree(ptr);
-        ptr = nullptr;
-        bytes = 0;
-        cudaError_t e = cudaMalloc(&ptr, want);
-        if (e != cudaSuccess) return fail(GB_ECUDA, "cudaMalloc(%zu): %s", want, cudaGetErrorString(e));
-        bytes = want;
-        return 0;
-    }
-};
-
-static size_t elem_size(int dtype) { return dtype == GB_C128 ? 16 : 8; }
-
-static int read_phases(int dtype, const double* phases, Phases& P) {
-    memset(&P, 0, sizeof P);
-    if (dtype != GB_C128 || phases == nullptr) return 0;
-    for (int c = 0; c < 3; c++)
-        for (int d = 0; d < 2; d++) {
-            P.ph[c][d].x = phases[(c * 2 + d) * 2];
-            P.ph[c][d].y = phases[(c * 2 + d) * 2 + 1];
-        }
-    P.use = 1;
-    return 0;
-}
-
-static bool ranges_overlap(const void* a, const void* b, size_t bytes) {
-    const char* x = (const char*)a;
-    const char* y = (const char*)b;
-    return x < y + bytes && y < x + bytes;
-}
-
-// ----------------------------------------------------------------- Operator
-struct gb_operator {
-    Stencil st;
-    GridBC g;
-    int real;
-    double diag;
-    CfdStencil cs;     // axis-aligned form, when the stencil has one
-    int nn = 0;        // its half-width
-    int tiled = 0;     // use the plane-marching kernels
-    Scratch scratch;   // aliasing stage / Jacobi ping-pong / GS snapshot
-    Scratch partial;   // per-CTA partial sums of |r|^2
-    long long ng() const { return (long long)g.n[0] * g.n[1] * g.n[2]; }
-};
-
-// Partial sums produced per grid by a residual sweep of `op`.
-static int op_resid_blocks(const gb_operator* op, int nin, int es) {
-    return op->tiled ? cfd_blocks(op->g, op->nn, es, nin) : residual_blocks(op->g);
-}
-
-// One pass of the stencil with a fused epilogue; plane-marching kernel for
-// axis-aligned stencils, the generic one otherwise.
-static int op_sweep(gb_operator* op, int mode, const void* in, void* out, const void* aux,
-                    int nin, int dtype, const Phases& P, double w, double sc, int negate,
-                    double* partial, cudaStream_t st) {
-    if (op->tiled) {
-        Epi ep{aux, w, sc, negate, partial};
-        int rc = (dtype == GB_F64)
-                     ? launch_fd_cfd<double>(mode, in, out, nin, op->g, P, op->cs, op->nn, ep, st,
-                                             nullptr)
-                     : launch_fd_cfd<double2>(mode, in, out, nin, op->g, P, op->cs, op->nn, ep,
-                                              st, nullptr);
-        if (rc == -2) return fail(GB_ECUDA, "could not raise the shared-memory limit");
-        if (rc == 0) return 0;
-    }
-    switch (mode) {
-        case EPI_APPLY:
-            if (dtype == GB_F64) launch_fd<double>(in, out, nin, op->g, P, op->st, st);
-            else launch_fd<double2>(in, out, nin, op->g, P, op->st, st);
-            break;
-        case EPI_RESID:
-            if (dtype == GB_F64)
-                launch_residual<double>(in, aux, out, nin, op->g, P, op->st, partial, st);
-            else
-                launch_residual<double2>(in, aux, out, nin, op->g, P, op->st, partial, st);
-            break;
-        case EPI_JACOBI:
-            launch_jacobi((const double*)in, (double*)out, (const double*)aux, op->g, op->st, w,
-                          st);
-            break;
-        case EPI_PRECOND:
-            if (dtype == GB_F64)
-                launch_precond_step<double>(in, aux, out, nin, op->g, P, op->st, sc, negate, st);
-            else
-                launch_precond_step<double2>(in, aux, out, nin, op->g, P, op->st, sc, negate, st);
-            break;
-    }
-    return 0;
-}
 
 extern "C" int gb_operator_new(const double* coefs, const int64_t* offsets, int ncoefs,
                                const int64_t size[3], int range, const int64_t neighbors[6],
@@ -335,13 +219,6 @@ extern "C" int gb_operator_relax(gb_operator* op, int method, double* f, const d
 }
 
 // -------------------------------------------------------------- Transformer
-struct gb_transformer {
-    XferGeom G;
-    int k;
-    int interpolate;
-    int real;
-    long long ngin, ngout;
-};
 
 static void lagrange_weights(int k, double* w) {
     // Weights of the order-k Lagrange interpolant at the mid-point, for the
@@ -414,24 +291,6 @@ extern "C" int gb_transformer_new(const int64_t size_in[3], const int64_t size_o
 }
 
 extern "C" void gb_transformer_free(gb_transformer* t) { delete t; }
-
-static int transform_impl(gb_transformer* t, const void* in, void* out, void* out2, int64_t nin,
-                          int dtype, const Phases& P, int neg_in, int accumulate, double scale2,
-                          cudaStream_t st) {
-    XferGeom G = t->G;
-    G.neg_in = neg_in;
-    G.accumulate = accumulate;
-    G.scale2 = scale2;
-    int rc;
-    if (dtype == GB_F64)
-        rc = launch_transform<double>(t->k, t->interpolate, in, out, out2, (int)nin, G, P, st);
-    else
-        rc = launch_transform<double2>(t->k, t->interpolate, in, out, out2, (int)nin, G, P, st);
-    if (rc == -2) return fail(GB_ECUDA, "transformer: could not raise the shared-memory limit");
-    if (rc) return fail(GB_EINVAL, "transformer: unsupported order");
-    GB_LAUNCH_CHECK();
-    return 0;
-}
 
 extern "C" int gb_transformer_apply(gb_transformer* t, const void* in, void* out, int64_t nin,
                                     int dtype, const double* phases, void* stream) {

@@ -36,8 +36,11 @@ __device__ __forceinline__ void cp_async(void* sdst, const void* gsrc, bool vali
     if (BYTES == 16)
         asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gsrc),
                      "r"(n));
-    else
+    else if (BYTES == 8)
         asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gsrc),
+                     "r"(n));
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gsrc),
                      "r"(n));
 }
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
@@ -56,6 +59,11 @@ template <>
 __device__ __forceinline__ double2 jacobi_update<double2>(double2 b, double2, double2, double,
                                                           double) {
     return b;  // relaxation is defined for real data only
+}
+template <>
+__device__ __forceinline__ float jacobi_update<float>(float b, float src, float x, double w,
+                                                      double c0) {
+    return (1.0f - (float)w) * b + (float)w * (src - x) / (float)c0;
 }
 
 template <class T>
@@ -110,7 +118,7 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
     const int b = blockIdx.z;
     const int tid = threadIdx.x;
     if (pa >= pb || b >= nin) {
-        if (MODE == EPI_RESID && ep.partial && tid == 0)
+        if ((MODE == EPI_RESID || MODE == EPI_LIN) && ep.partial && tid == 0)
             ep.partial[((long long)b * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = 0.0;
         return;
     }
@@ -118,6 +126,7 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
     const T* a = in + b * ng;
     T* o = out + b * ng;
     const T* aux = (const T*)ep.aux + b * ng;
+    const T* aux2 = (const T*)ep.aux2 + b * ng;
     double sq = 0.0;
     const int tx = tid % TX;
     const int ty0 = (tid / TX) * RY;
@@ -306,6 +315,16 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
                         sq += sqnorm(res);
                     } else if (MODE == EPI_JACOBI) {
                         o[at] = jacobi_update<T>(vc, aux[at], x, ep.w, cs.c0);
+                    } else if (MODE == EPI_LIN) {
+                        if constexpr (sizeof(T) != 16) {
+                            T y = (T)ep.p1 * vc + (T)ep.p2 * x;
+                            if (ep.aux) y += (T)ep.p0 * aux[at];
+                            if (ep.aux2) y += (T)ep.p3 * aux2[at];
+                            if (ep.partial) sq += (double)y * (double)y;
+                            if (ep.acc64) ep.acc64[b * ng + at] += (double)y;
+                            else if (ep.out32) ep.out32[b * ng + at] = (float)y;
+                            else o[at] = y;
+                        }
                     } else {
                         const T y = Num<T>::sub(vc, Num<T>::scale(Num<T>::sub(x, aux[at]), ep.sc));
                         o[at] = ep.negate ? Num<T>::neg(y) : y;
@@ -319,7 +338,7 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
             for (int k = 0; k < Q - 1; k++) q[r][k] = q[r][k + 1];
     }
     cp_wait<0>();
-    if (MODE == EPI_RESID && ep.partial) {
+    if ((MODE == EPI_RESID || MODE == EPI_LIN) && ep.partial) {
         sq = block_sum(sq);
         if (tid == 0)
             ep.partial[((long long)b * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = sq;
@@ -402,8 +421,15 @@ int launch_fd_cfd(int mode, const void* in, void* out, int nin, const GridBC& g,
                   cudaStream_t st, int* nblk) {
     switch (mode) {
         case EPI_APPLY: return launch_cfd_mode<T, EPI_APPLY>(in, out, nin, g, P, cs, nn, ep, st, nblk);
-        case EPI_RESID: return launch_cfd_mode<T, EPI_RESID>(in, out, nin, g, P, cs, nn, ep, st, nblk);
-        case EPI_PRECOND: return launch_cfd_mode<T, EPI_PRECOND>(in, out, nin, g, P, cs, nn, ep, st, nblk);
+        case EPI_RESID:
+            if constexpr (sizeof(T) == 4) return -1;
+            else return launch_cfd_mode<T, EPI_RESID>(in, out, nin, g, P, cs, nn, ep, st, nblk);
+        case EPI_PRECOND:
+            if constexpr (sizeof(T) == 4) return -1;
+            else return launch_cfd_mode<T, EPI_PRECOND>(in, out, nin, g, P, cs, nn, ep, st, nblk);
+        case EPI_LIN:
+            if constexpr (sizeof(T) == 16) return -1;
+            else return launch_cfd_mode<T, EPI_LIN>(in, out, nin, g, P, cs, nn, ep, st, nblk);
         case EPI_JACOBI:
             if constexpr (sizeof(T) != 8) return -1;
             else return launch_cfd_mode<T, EPI_JACOBI>(in, out, nin, g, P, cs, nn, ep, st, nblk);
@@ -415,6 +441,8 @@ template int launch_fd_cfd<double>(int, const void*, void*, int, const GridBC&, 
                                    const CfdStencil&, int, const Epi&, cudaStream_t, int*);
 template int launch_fd_cfd<double2>(int, const void*, void*, int, const GridBC&, const Phases&,
                                     const CfdStencil&, int, const Epi&, cudaStream_t, int*);
+template int launch_fd_cfd<float>(int, const void*, void*, int, const GridBC&, const Phases&,
+                                  const CfdStencil&, int, const Epi&, cudaStream_t, int*);
 
 // Number of CTAs per grid of the EPI_RESID launch (partials per grid).
 int cfd_blocks(const GridBC& g, int nn, int elem_bytes, int nin) {

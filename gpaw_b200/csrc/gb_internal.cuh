@@ -59,6 +59,7 @@ enum : int {
     EPI_RESID = 1,    // out = L in - aux, |out|^2 partials (gpaw/poisson.py:517-532)
     EPI_JACOBI = 2,   // out = (1-w) in + w (aux - L' in) / c0  (c/bmgs/relax.cpp:41-65)
     EPI_PRECOND = 3,  // out = +-(in - sc (L in - aux))  (c/fd_preconditioner.cpp:251-333)
+    EPI_LIN = 4,      // y = p0 aux + p1 in + p2 L in + p3 aux2 (mixed-precision solver)
 };
 
 struct Epi {
@@ -66,7 +67,12 @@ struct Epi {
     double w;
     double sc;
     int negate;
-    double* partial;  // EPI_RESID: per-CTA sums of |r|^2 (nullable)
+    double* partial;  // EPI_RESID / EPI_LIN: per-CTA sums of |out|^2 (nullable)
+    // EPI_LIN only
+    const void* aux2;
+    double p0, p1, p2, p3;
+    double* acc64;    // if set: acc64 += y (instead of writing out)
+    float* out32;     // if set: out32 = (float) y (instead of writing out)
 };
 
 // ------------------------------------------------------------------ launchers

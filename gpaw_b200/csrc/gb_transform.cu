@@ -41,8 +41,10 @@ __device__ __forceinline__ void cp_async_x(void* sdst, const void* gsrc, bool va
     const int n = valid ? BYTES : 0;
     if (BYTES == 16)
         asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gsrc), "r"(n));
-    else
+    else if (BYTES == 8)
         asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gsrc), "r"(n));
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gsrc), "r"(n));
 }
 __device__ __forceinline__ void cp_commit_x() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
