@@ -243,6 +243,55 @@ def poisson_c1(dev, nsolve=20):
     return out
 
 
+def poisson_c3(dev, nsolve=5):
+    """192^3 zero-BC, h = 0.18 A, 64 Gaussians: plain FP64 V-cycle with the
+    reference schedule (7 grids) versus FP32 V-cycles (4 levels, 2 + 2
+    smoothing sweeps) in FP64 defect correction, both to 1e-10 relative
+    residual."""
+    import torch
+    from gpaw_b200 import FDPoissonSolver, GridDescriptor, MixedPoissonSolver
+    from gpaw_b200.workloads import (BOHR, c3_density,
+                                     eps_for_relative_residual, neutralize)
+    h = 0.18 / BOHR
+    gd = GridDescriptor((192, 192, 192), (192 * h,) * 3, 0, device=dev)
+    rho = neutralize(c3_density(gd, 64), gd)
+    rho_d = torch.from_numpy(rho).to(dev)
+    rnorm = float(np.sqrt((rho * rho).sum()))
+    fp64 = FDPoissonSolver(nn=3, relax='J',
+                           eps=eps_for_relative_residual(rho, gd))
+    fp64.set_grid_descriptor(gd)
+    mixed = MixedPoissonSolver(nn=3, tol=1e-10, levels=4)
+    mixed.set_grid_descriptor(gd)
+    out = {'grid': [192, 192, 192], 'h_angstrom': 0.18, 'gaussians': 64}
+    phis = {}
+    for tag, ps in (('fp64_reference_schedule', fp64),
+                    ('mixed_fp32_in_fp64', mixed)):
+        phi = gd.zeros()
+        ps.solve_neutral(phi, rho_d)      # warm-up (builds the graph)
+        times = []
+        for _ in range(nsolve):
+            phi.zero_()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            n = ps.solve_neutral(phi, rho_d)
+            times.append(time.perf_counter() - t0)
+        r = torch.empty_like(phi)
+        n2 = torch.zeros(1, dtype=torch.float64, device=dev)
+        fp64.operators[0].residual(phi, rho_d, r, None, 1.0, n2)
+        t = float(np.median(times))
+        phis[tag] = phi
+        out[tag] = {'vcycles': n, 'ms_per_solve': t * 1e3,
+                    'solves_per_s': 1.0 / t,
+                    'rel_residual': float(np.sqrt(n2.item())) / rnorm}
+    a, b = phis['mixed_fp32_in_fp64'], phis['fp64_reference_schedule']
+    out['max_rel_diff_mixed_vs_fp64'] = float(
+        (a - b).abs().max() / b.abs().max())
+    out['speedup_mixed_over_fp64'] = (
+        out['mixed_fp32_in_fp64']['solves_per_s'] /
+        out['fp64_reference_schedule']['solves_per_s'])
+    return out
+
+
 # ---------------------------------------------------------------- GPU side
 def run_gpu(args):
     import torch
@@ -387,7 +436,7 @@ def run_gpu(args):
         'cpu_baseline': cpu_base,
     }
     if not args.no_poisson:
-        line['poisson'] = {'c1': poisson_c1(dev)}
+        line['poisson'] = {'c1': poisson_c1(dev), 'c3': poisson_c3(dev)}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

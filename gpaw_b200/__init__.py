@@ -15,9 +15,10 @@ sm_100a kernels of ``libgpaw_b200.so`` (C ABI: include/gpaw_b200.h).
 from .grid_descriptor import BadGridError, GridDescriptor
 from .fd_operators import FDOperator, GUCLaplace, Laplace
 from .transformers import Transformer
-from .poisson import FDPoissonSolver, PoissonConvergenceError
+from .poisson import (FDPoissonSolver, MixedPoissonSolver,
+                      PoissonConvergenceError)
 from .preconditioner import Preconditioner
 
 __all__ = ['GridDescriptor', 'BadGridError', 'FDOperator', 'GUCLaplace',
            'Laplace', 'Transformer', 'FDPoissonSolver',
-           'PoissonConvergenceError', 'Preconditioner']
+           'MixedPoissonSolver', 'PoissonConvergenceError', 'Preconditioner']

@@ -51,6 +51,12 @@ SIGNATURES = {
                                  C.POINTER(C.c_int), _dp, C.c_int,
                                  C.c_double, C.POINTER(_p)]),
     'gb_poisson_free': (None, [_p]),
+    'gb_mixed_new': (C.c_int, [C.c_int, _p, C.POINTER(_p), C.POINTER(_p),
+                               C.POINTER(_p), _dp, C.c_double, C.c_int,
+                               C.POINTER(_p)]),
+    'gb_mixed_free': (None, [_p]),
+    'gb_mixed_solve': (C.c_int, [_p, _p, _p, C.c_double, C.c_int,
+                                 C.POINTER(C.c_int), _dp, _p]),
     'gb_poisson_iterate': (C.c_int, [_p, _p, _p, _dp, _p]),
     'gb_poisson_solve_neutral': (C.c_int, [_p, _p, _p, C.c_double, C.c_int,
                                            C.POINTER(C.c_int), _dp, _p]),

@@ -1,0 +1,427 @@
+// Mixed-precision multigrid Poisson solver: FP32 V-cycles inside FP64
+// defect correction.  No counterpart in the reference (its FDPoissonSolver is
+// FP64 throughout, gpaw/poisson.py:321-537); the operators, transformers and
+// level hierarchy are the reference's.
+//
+//   d = rho - L64 phi                (FP64 stencil, |d|^2 in FP64)
+//   while |d| / |rho| > tol:
+//       e = V32(float(d))            (FP32 V-cycle, Chebyshev smoothing)
+//       phi += e                     (FP64 accumulate, fused in the last sweep)
+//       d = rho - L64 phi
+//
+// V32 on levels 0..L-1: pre-smooth (degree-2 Chebyshev from zero, one
+// stencil pass), residual, restriction, coarse correction, interpolation and
+// correction, post-smooth (degree-2 Chebyshev, two stencil passes).  Level L
+// (coarsest) is solved in FP64 with a fixed-degree Chebyshev iteration over
+// the spectrum of D^-1 A, in one single-CTA kernel.  The whole loop runs on
+// the device: a CUDA graph with a conditional WHILE node.
+#include <vector>
+
+#include "gb_objects.cuh"
+
+using namespace gb;
+
+namespace {
+
+// Degree-2 Chebyshev smoother on D^-1 A over [a, b] (Saad, Iterative
+// Methods for Sparse Linear Systems, Alg. 12.1), folded into stencil passes:
+//   from e = 0:  e2 = pre_u * b + pre_Lu * (A b)
+//   from e:      t  = (b - A e) / (theta c0)
+//                e2 = e + k1 * t - k2 * (A t)
+struct ChebLevel {
+    double pre_u, pre_Lu;     // pre-smooth coefficients
+    double inv_tc0;           // 1 / (theta c0)
+    double k1, k2;            // post-smooth coefficients
+};
+
+ChebLevel cheb_level(double lam_max, double c0) {
+    const double a = lam_max / 8.0, b = 1.05 * lam_max;
+    const double theta = 0.5 * (b + a), delta = 0.5 * (b - a);
+    const double sigma = theta / delta;
+    const double rho0 = 1.0 / sigma;
+    const double rho1 = 1.0 / (2.0 * sigma - rho0);
+    ChebLevel c;
+    c.k1 = 1.0 + rho1 * rho0 + 2.0 * rho1 * theta / delta;
+    c.k2 = 2.0 * rho1 / (delta * c0);
+    c.inv_tc0 = 1.0 / (theta * c0);
+    c.pre_u = c.k1 * c.inv_tc0;
+    c.pre_Lu = -c.k2 * c.inv_tc0;
+    return c;
+}
+
+// Value of d at interior coordinate (x0, x1, x2) with the grid's boundary
+// (zero or periodic); plain loads, since d changes during the kernel.
+__device__ __forceinline__ double coarse_read(const double* d, int x0, int x1, int x2,
+                                              const GridBC& g) {
+    int x[3] = {x0, x1, x2};
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        if (x[c] < 0 || x[c] >= g.n[c]) {
+            if (!g.periodic[c]) return 0.0;
+            x[c] += x[c] < 0 ? g.n[c] : -g.n[c];
+        }
+    }
+    return d[((long long)x[0] * g.n[1] + x[1]) * g.n[2] + x[2]];
+}
+
+struct Ctl {
+    double rho2;      // |rho|^2
+    double rel;       // last |d| / |rho|
+    double tol;
+    int maxiter;
+    int niter;
+};
+
+// Coarsest level: x = Chebyshev_deg(D^-1 A, [lo, hi]) applied to b, from
+// x = 0, in FP64, by one CTA.  b is the FP32 restricted residual; the FP32
+// correction is written to e.  r, da, db, x are FP64 scratch of n points.
+__global__ void __launch_bounds__(1024)
+k_coarse_cheb(const float* __restrict__ b, float* __restrict__ e, double* __restrict__ x,
+              double* __restrict__ r, double* __restrict__ da, double* __restrict__ db,
+              GridBC g, const __grid_constant__ Stencil s, double lo, double hi, int deg) {
+    const int n = g.n[0] * g.n[1] * g.n[2];
+    const double c0 = s.coef[0];
+    const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo);
+    const double sigma = theta / delta;
+    double rho = 1.0 / sigma;
+    for (int p = threadIdx.x; p < n; p += blockDim.x) {
+        const double r0 = (double)b[p] / c0;
+        r[p] = r0;
+        x[p] = 0.0;
+        da[p] = r0 / theta;
+    }
+    __syncthreads();
+    double* d = da;
+    double* dn = db;
+    for (int k = 0; k < deg; k++) {
+        const double rho_n = 1.0 / (2.0 * sigma - rho);
+        for (int p = threadIdx.x; p < n; p += blockDim.x) {
+            const int i2 = p % g.n[2];
+            const int t = p / g.n[2];
+            const int i1 = t % g.n[1];
+            const int i0 = t / g.n[1];
+            double ad = 0.0;
+            for (int c = 0; c < s.ncoefs; c++)
+                ad += s.coef[c] * coarse_read(d, i0 + s.off[c][0], i1 + s.off[c][1],
+                                              i2 + s.off[c][2], g);
+            const double dk = d[p];
+            x[p] += dk;
+            const double rn = r[p] - ad / c0;
+            r[p] = rn;
+            dn[p] = rho_n * rho * dk + 2.0 * rho_n / delta * rn;
+        }
+        rho = rho_n;
+        __syncthreads();
+        double* tmp = d;
+        d = dn;
+        dn = tmp;
+    }
+    for (int p = threadIdx.x; p < n; p += blockDim.x) e[p] = (float)x[p];
+}
+
+__global__ void k_sumsq(const double* __restrict__ a, long long n, double* __restrict__ partial) {
+    double v = 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        v += a[i] * a[i];
+    v = block_sum(v);
+    if (threadIdx.x == 0) partial[blockIdx.x] = v;
+}
+
+__global__ void k_mixed_init(Ctl* ctl, const double* rho2, double tol, int maxiter) {
+    ctl->rho2 = rho2[0];
+    ctl->tol = tol;
+    ctl->maxiter = maxiter;
+    ctl->niter = 0;
+    ctl->rel = 0.0;
+}
+
+// After the defect: rel = |d| / |rho|; continue while rel > tol and fewer
+// than maxiter V-cycles ran.  `count` adds the V-cycle just finished.
+__global__ void k_mixed_check(Ctl* ctl, const double* d2, int count,
+                              cudaGraphConditionalHandle h) {
+    const int n = ctl->niter + count;
+    ctl->niter = n;
+    const double rel = ctl->rho2 > 0.0 ? sqrt(d2[0] / ctl->rho2) : 0.0;
+    ctl->rel = rel;
+    cudaGraphSetConditional(h, (rel > ctl->tol && n < ctl->maxiter) ? 1u : 0u);
+}
+
+}  // namespace
+
+struct gb_mixed {
+    int L = 0;
+    gb_operator* op64 = nullptr;
+    std::vector<gb_operator*> ops;
+    std::vector<gb_transformer*> rst, itp;
+    std::vector<ChebLevel> ch;
+    double coarse_lo = 0, coarse_hi = 0;
+    int coarse_deg = 0;
+    std::vector<float*> b, e, t;       // levels 0..L (b[L], e[L] used at L)
+    double *x = nullptr, *r = nullptr, *da = nullptr, *db = nullptr;
+    double *phi0 = nullptr, *rho0 = nullptr;
+    double *partial = nullptr, *nrm = nullptr;
+    Ctl* ctl = nullptr;
+    Ctl* ctl_host = nullptr;
+    int nblk64 = 0;   // partial-sum buffer length
+    int nres = 0;     // partials written by the level-0 defect sweep
+    cudaStream_t cap = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    ~gb_mixed() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (cap) cudaStreamDestroy(cap);
+        for (float* p : b) cudaFree(p);
+        for (float* p : e) cudaFree(p);
+        for (float* p : t) cudaFree(p);
+        cudaFree(x);
+        cudaFree(r);
+        cudaFree(da);
+        cudaFree(db);
+        cudaFree(phi0);
+        cudaFree(rho0);
+        cudaFree(partial);
+        cudaFree(nrm);
+        cudaFree(ctl);
+        if (ctl_host) cudaFreeHost(ctl_host);
+    }
+};
+
+// One stencil pass of the linear epilogue on level l (float) or on the
+// level-0 FP64 operator (double).
+template <class T>
+static int lin(gb_operator* op, const T* in, T* out, const T* aux, const T* aux2, double p0,
+               double p1, double p2, double p3, double* acc64, float* out32, double* partial,
+               cudaStream_t st) {
+    Epi ep{};
+    ep.aux = aux;
+    ep.aux2 = aux2;
+    ep.p0 = p0;
+    ep.p1 = p1;
+    ep.p2 = p2;
+    ep.p3 = p3;
+    ep.acc64 = acc64;
+    ep.out32 = out32;
+    ep.partial = partial;
+    Phases P{};
+    const int rc = launch_fd_cfd<T>(EPI_LIN, in, out, 1, op->g, P, op->cs, op->nn, ep, st, nullptr);
+    if (rc == -2) return fail(GB_ECUDA, "mixed: could not raise the shared-memory limit");
+    if (rc) return fail(GB_EINVAL, "mixed: operator is not an axis-aligned stencil");
+    GB_LAUNCH_CHECK();
+    return 0;
+}
+
+// V-cycle on levels l..L for the FP32 right-hand side b[l]; at level 0 the
+// final correction is added to phi0 (FP64).
+static int vcycle32(gb_mixed* m, int l, cudaStream_t st) {
+    if (l == m->L) {
+        gb_operator* op = m->ops[l];
+        k_coarse_cheb<<<1, 1024, 0, st>>>(m->b[l], m->e[l], m->x, m->r, m->da, m->db, op->g,
+                                           op->st, m->coarse_lo, m->coarse_hi, m->coarse_deg);
+        GB_LAUNCH_CHECK();
+        return 0;
+    }
+    gb_operator* op = m->ops[l];
+    const ChebLevel& c = m->ch[l];
+    float *b = m->b[l], *e = m->e[l], *t = m->t[l];
+    int rc;
+    // pre-smooth from zero
+    if ((rc = lin<float>(op, b, e, nullptr, nullptr, 0, c.pre_u, c.pre_Lu, 0, nullptr, nullptr,
+                         nullptr, st)))
+        return rc;
+    // residual t = b - A e, restricted to the next level
+    if ((rc = lin<float>(op, e, t, b, nullptr, 1.0, 0.0, -1.0, 0, nullptr, nullptr, nullptr, st)))
+        return rc;
+    Phases P{};
+    if ((rc = transform_impl(m->rst[l], t, m->b[l + 1], nullptr, 1, GB_F32_INTERNAL, P, 0, 0, 0.0, st)))
+        return rc;
+    if ((rc = vcycle32(m, l + 1, st))) return rc;
+    // e += I(e_{l+1})   (as e -= I(-e_{l+1}), negation exact)
+    if ((rc = transform_impl(m->itp[l], m->e[l + 1], e, nullptr, 1, GB_F32_INTERNAL, P, 1, 1, 0.0, st)))
+        return rc;
+    // post-smooth: t = (b - A e) / (theta c0); e += k1 t - k2 A t
+    if ((rc = lin<float>(op, e, t, b, nullptr, c.inv_tc0, 0.0, -c.inv_tc0, 0, nullptr, nullptr,
+                         nullptr, st)))
+        return rc;
+    if (l == 0)
+        rc = lin<float>(op, t, e, nullptr, e, 0, c.k1, -c.k2, 1.0, m->phi0, nullptr, nullptr, st);
+    else
+        rc = lin<float>(op, t, e, nullptr, e, 0, c.k1, -c.k2, 1.0, nullptr, nullptr, nullptr, st);
+    return rc;
+}
+
+// d = rho - L64 phi  ->  b[0] (float) and |d|^2 -> nrm[0]
+static int defect(gb_mixed* m, cudaStream_t st) {
+    if (int rc = lin<double>(m->op64, m->phi0, nullptr, m->rho0, nullptr, 1.0, 0.0, -1.0, 0,
+                             nullptr, m->b[0], m->partial, st))
+        return rc;
+    launch_reduce_partials(m->partial, m->nres, 1, 1.0, m->nrm, st);
+    GB_LAUNCH_CHECK();
+    return 0;
+}
+
+extern "C" int gb_mixed_new(int nlevels, gb_operator* op64, gb_operator* const* operators,
+                            gb_transformer* const* restrictors,
+                            gb_transformer* const* interpolators, const double* lam_max,
+                            double lam_min_coarse, int coarse_degree, gb_mixed** out) {
+    if (!out || !op64 || !operators || !lam_max || nlevels < 2 || !restrictors || !interpolators)
+        return fail(GB_EINVAL, "mixed: bad arguments (needs at least two levels)");
+    *out = nullptr;
+    if (!op64->real || !op64->tiled)
+        return fail(GB_EINVAL, "mixed: level-0 operator must be a real axis-aligned stencil");
+    if (coarse_degree < 1 || lam_min_coarse <= 0.0)
+        return fail(GB_EINVAL, "mixed: coarse degree >= 1 and a positive lower bound needed");
+    gb_mixed* m = new gb_mixed();
+    m->L = nlevels - 1;
+    m->op64 = op64;
+    for (int l = 0; l < nlevels; l++) {
+        gb_operator* op = operators[l];
+        if (!op || !op->real || (l < m->L && !op->tiled)) {
+            delete m;
+            return fail(GB_EINVAL, "mixed: level %d operator must be a real axis-aligned stencil", l);
+        }
+        m->ops.push_back(op);
+        if (l < m->L) m->ch.push_back(cheb_level(lam_max[l], op->st.coef[0]));
+    }
+    if (m->ops[0]->ng() != op64->ng()) {
+        delete m;
+        return fail(GB_EINVAL, "mixed: level-0 operators differ in size");
+    }
+    for (int l = 0; l < m->L; l++) {
+        gb_transformer* rr = restrictors[l];
+        gb_transformer* ii = interpolators[l];
+        if (!rr || !ii || rr->interpolate || !ii->interpolate || rr->ngin != m->ops[l]->ng() ||
+            rr->ngout != m->ops[l + 1]->ng() || ii->ngin != m->ops[l + 1]->ng() ||
+            ii->ngout != m->ops[l]->ng()) {
+            delete m;
+            return fail(GB_EINVAL, "mixed: transformer %d does not match the levels", l);
+        }
+        m->rst.push_back(rr);
+        m->itp.push_back(ii);
+    }
+    m->coarse_hi = 1.02 * lam_max[m->L];
+    m->coarse_lo = lam_min_coarse;
+    m->coarse_deg = coarse_degree;
+    cudaError_t ce = cudaSuccess;
+    for (int l = 0; l <= m->L && ce == cudaSuccess; l++) {
+        const size_t bytes = (size_t)m->ops[l]->ng() * sizeof(float);
+        float *bb = nullptr, *ee = nullptr, *tt = nullptr;
+        ce = cudaMalloc(&bb, bytes);
+        if (ce == cudaSuccess) ce = cudaMalloc(&ee, bytes);
+        if (ce == cudaSuccess) ce = cudaMalloc(&tt, bytes);
+        m->b.push_back(bb);
+        m->e.push_back(ee);
+        m->t.push_back(tt);
+    }
+    const size_t nc = (size_t)m->ops[m->L]->ng() * sizeof(double);
+    const size_t n0 = (size_t)op64->ng() * sizeof(double);
+    m->nres = op_resid_blocks(op64, 1, 8);
+    m->nblk64 = std::max(m->nres, 1024);
+    if (ce == cudaSuccess) ce = cudaMalloc(&m->x, nc);
+    if (ce == cudaSuccess) ce = cudaMalloc(&m->r, nc);
+    if (ce == cudaSuccess) ce = cudaMalloc(&m->da, nc);
+    if (ce == cudaSuccess) ce = cudaMalloc(&m->db, nc);
+    if (ce == cudaSuccess) ce = cudaMalloc(&m->phi0, n0);
+    if (ce == cudaSuccess) ce = cudaMalloc(&m->rho0, n0);
+    if (ce == cudaSuccess) ce = cudaMalloc(&m->partial, (size_t)m->nblk64 * sizeof(double));
+    if (ce == cudaSuccess) ce = cudaMalloc(&m->nrm, 2 * sizeof(double));
+    if (ce == cudaSuccess) ce = cudaMalloc(&m->ctl, sizeof(Ctl));
+    if (ce == cudaSuccess) ce = cudaMallocHost(&m->ctl_host, sizeof(Ctl));
+    if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&m->cap, cudaStreamNonBlocking);
+    if (ce != cudaSuccess) {
+        delete m;
+        return fail(GB_ECUDA, "mixed: allocation: %s", cudaGetErrorString(ce));
+    }
+    *out = m;
+    return 0;
+}
+
+extern "C" void gb_mixed_free(gb_mixed* m) { delete m; }
+
+// Graph:  defect; check -> WHILE { V32 (phi += e); defect; check }
+static int build_mixed_graph(gb_mixed* m) {
+    cudaStream_t cs = m->cap;
+    const size_t n0 = (size_t)m->op64->ng() * sizeof(double);
+    // one uncaptured pass: sets kernel attributes
+    GB_CUDA_TRY(cudaMemsetAsync(m->phi0, 0, n0, cs));
+    GB_CUDA_TRY(cudaMemsetAsync(m->rho0, 0, n0, cs));
+    if (int rc = defect(m, cs)) return rc;
+    if (int rc = vcycle32(m, 0, cs)) return rc;
+    GB_CUDA_TRY(cudaStreamSynchronize(cs));
+
+    cudaGraph_t graph;
+    GB_CUDA_TRY(cudaGraphCreate(&graph, 0));
+    cudaGraphConditionalHandle h;
+    GB_CUDA_TRY(cudaGraphConditionalHandleCreate(&h, graph, 0, 0));
+    // head: initial defect and check (sets the loop condition)
+    GB_CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, graph, nullptr, nullptr, 0,
+                                              cudaStreamCaptureModeThreadLocal));
+    int rc = defect(m, cs);
+    if (!rc) k_mixed_check<<<1, 1, 0, cs>>>(m->ctl, m->nrm, 0, h);
+    cudaGraph_t gout = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(cs, &gout);
+    if (rc || ce != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        return rc ? rc : fail(GB_ECUDA, "mixed: capture: %s", cudaGetErrorString(ce));
+    }
+    size_t nleaf = 0;
+    GB_CUDA_TRY(cudaGraphGetNodes(graph, nullptr, &nleaf));
+    std::vector<cudaGraphNode_t> nodes(nleaf);
+    GB_CUDA_TRY(cudaGraphGetNodes(graph, nodes.data(), &nleaf));
+    // the check kernel is the only node without dependents
+    cudaGraphNode_t tail = nullptr;
+    for (auto nd : nodes) {
+        size_t nout = 0;
+        GB_CUDA_TRY(cudaGraphNodeGetDependentNodes(nd, nullptr, &nout));
+        if (nout == 0) tail = nd;
+    }
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t wnode;
+    GB_CUDA_TRY(cudaGraphAddNode(&wnode, graph, &tail, 1, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    GB_CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0,
+                                              cudaStreamCaptureModeThreadLocal));
+    rc = vcycle32(m, 0, cs);
+    if (!rc) rc = defect(m, cs);
+    if (!rc) k_mixed_check<<<1, 1, 0, cs>>>(m->ctl, m->nrm, 1, h);
+    ce = cudaStreamEndCapture(cs, &gout);
+    if (rc || ce != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        return rc ? rc : fail(GB_ECUDA, "mixed: capture of the V-cycle: %s", cudaGetErrorString(ce));
+    }
+    cudaError_t ie = cudaGraphInstantiate(&m->exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) return fail(GB_ECUDA, "mixed: instantiate: %s", cudaGetErrorString(ie));
+    return 0;
+}
+
+extern "C" int gb_mixed_solve(gb_mixed* m, double* phi, const double* rho, double tol,
+                              int maxiter, int* niter, double* rel_residual, void* stream) {
+    if (!m || !phi || !rho) return fail(GB_EINVAL, "mixed solve: NULL argument");
+    if (maxiter < 1) return fail(GB_EINVAL, "mixed solve: maxiter must be >= 1");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!m->exec)
+        if (int rc = build_mixed_graph(m)) return rc;
+    const long long n = m->op64->ng();
+    const size_t bytes = (size_t)n * sizeof(double);
+    GB_CUDA_TRY(cudaMemcpyAsync(m->rho0, rho, bytes, cudaMemcpyDeviceToDevice, st));
+    GB_CUDA_TRY(cudaMemcpyAsync(m->phi0, phi, bytes, cudaMemcpyDeviceToDevice, st));
+    const int nb = (int)std::min<long long>(1024, (n + 255) / 256);
+    k_sumsq<<<nb, 256, 0, st>>>(m->rho0, n, m->partial);
+    launch_reduce_partials(m->partial, nb, 1, 1.0, m->nrm + 1, st);
+    k_mixed_init<<<1, 1, 0, st>>>(m->ctl, m->nrm + 1, tol, maxiter);
+    GB_LAUNCH_CHECK();
+    GB_CUDA_TRY(cudaGraphLaunch(m->exec, st));
+    GB_CUDA_TRY(cudaMemcpyAsync(phi, m->phi0, bytes, cudaMemcpyDeviceToDevice, st));
+    GB_CUDA_TRY(cudaMemcpyAsync(m->ctl_host, m->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
+    GB_CUDA_TRY(cudaStreamSynchronize(st));
+    if (niter) *niter = m->ctl_host->niter;
+    if (rel_residual) *rel_residual = m->ctl_host->rel;
+    if (m->ctl_host->rel > tol)
+        return fail(GB_ENOCONV, "mixed-precision Poisson solver did not reach %g in %d V-cycles",
+                    tol, maxiter);
+    return 0;
+}

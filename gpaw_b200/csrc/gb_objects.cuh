@@ -14,6 +14,9 @@
 
 namespace gb {
 
+// float32 data inside the library (mixed-precision solver); not an ABI dtype
+constexpr int GB_F32_INTERNAL = 100;
+
 // Record the message of a failed call for gb_last_error(); returns code.
 int fail(int code, const char* fmt, ...);
 
@@ -158,6 +161,8 @@ inline int transform_impl(gb_transformer* t, const void* in, void* out, void* ou
     int rc;
     if (dtype == GB_F64)
         rc = launch_transform<double>(t->k, t->interpolate, in, out, out2, (int)nin, G, P, st);
+    else if (dtype == GB_F32_INTERNAL)
+        rc = launch_transform<float>(t->k, t->interpolate, in, out, out2, (int)nin, G, P, st);
     else
         rc = launch_transform<double2>(t->k, t->interpolate, in, out, out2, (int)nin, G, P, st);
     if (rc == -2) return fail(GB_ECUDA, "transformer: could not raise the shared-memory limit");

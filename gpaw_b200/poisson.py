@@ -20,7 +20,7 @@ from .cgpaw import _stream
 from .fd_operators import Laplace
 from .transformers import Transformer
 
-__all__ = ['FDPoissonSolver', 'PoissonConvergenceError']
+__all__ = ['FDPoissonSolver', 'MixedPoissonSolver', 'PoissonConvergenceError']
 
 
 class FDPoissonSolver:
@@ -203,4 +203,137 @@ class _Exec:
     def __del__(self):
         if self.h is not None and self.h.value:
             self.lib.gb_poisson_free(self.h)
+            self.h = None
+
+
+def stencil_spectrum(op, gd):
+    """(min over non-constant modes, max) of the eigenvalues of D^-1 A for
+    an axis-aligned stencil on ``gd`` (zero boundary: sine modes
+    theta = pi j / N, j = 1..N-1; periodic: theta = 2 pi j / N)."""
+    c0 = op.coef_p[0]
+    f = []
+    for a in range(3):
+        N = int(gd.N_c[a])
+        if gd.pbc_c[a]:
+            th = 2 * np.pi * np.arange(N) / N
+        else:
+            th = np.pi * np.arange(1, N) / N
+        fa = np.zeros_like(th)
+        for c, o in zip(op.coef_p[1:], op.offset_pc[1:]):
+            if o[a] != 0:
+                fa += c * np.cos(th * o[a])
+        f.append(fa / c0)
+    lam = 1.0 + f[0][:, None, None] + f[1][None, :, None] + f[2][None, None, :]
+    lmax = float(lam.max())
+    flat = np.sort(lam.ravel())
+    lmin = float(flat[1] if gd.pbc_c.all() else flat[0])
+    return lmin, lmax
+
+
+class MixedPoissonSolver:
+    """FP32 V-cycles inside FP64 defect correction (no counterpart in the
+    reference, whose FDPoissonSolver is FP64 throughout).
+
+    Same problem and operators as FDPoissonSolver: level 0 is the nn-order
+    Laplacian scaled by -1/(4 pi), coarser levels the 2nd-order one, grids
+    coarsened as set_grid_descriptor does (gpaw/poisson.py:366-430).  The
+    V-cycle spans ``levels`` grids with degree-2 Chebyshev smoothing (two
+    sweeps before, two after); the coarsest grid is solved in FP64 by a
+    Chebyshev iteration; the residual, its norm, |rho| and the stopping test
+    ||rho - L phi|| <= tol ||rho|| are FP64, on the device.
+    """
+
+    def __init__(self, nn=3, tol=1e-10, maxiter=200, levels=4,
+                 coarse_accuracy=0.05):
+        self.nn = nn
+        self.tol = tol
+        self.maxiter = maxiter
+        self.nlevels = levels
+        self.coarse_accuracy = coarse_accuracy
+        self._h = None
+
+    def set_grid_descriptor(self, gd):
+        from .fd_operators import Laplace
+        from .transformers import Transformer
+        self.gd = gd
+        scale = -0.25 / pi
+        gds = [gd]
+        while len(gds) < self.nlevels:
+            try:
+                gds.append(gds[-1].coarsen())
+            except ValueError:
+                break
+        if len(gds) < 2:
+            raise ValueError('grid %s cannot be coarsened' % gd.N_c)
+        self.gds = gds
+        self.operators = [Laplace(gds[0], scale, self.nn)] + \
+            [Laplace(g, scale, 1) for g in gds[1:]]
+        self.restrictors = [Transformer(gds[i], gds[i + 1])
+                            for i in range(len(gds) - 1)]
+        self.interpolators = [Transformer(gds[i + 1], gds[i])
+                              for i in range(len(gds) - 1)]
+        bounds = [stencil_spectrum(op, g)
+                  for op, g in zip(self.operators, gds)]
+        self.lam_max = [b[1] for b in bounds]
+        lmin, lmax = bounds[-1]
+        kappa = lmax / lmin
+        q = (np.sqrt(kappa) - 1) / (np.sqrt(kappa) + 1)
+        self.coarse_degree = int(np.clip(
+            np.ceil(np.log(self.coarse_accuracy / 2) / np.log(q)), 4, 256))
+        self.lam_min_coarse = 0.98 * lmin
+        lib = _lib.load()
+        nl = len(gds)
+        ops = (C.c_void_p * nl)(*[o.operator._h for o in self.operators])
+        rst = (C.c_void_p * (nl - 1))(*[t.transformer._h
+                                        for t in self.restrictors])
+        itp = (C.c_void_p * (nl - 1))(*[t.transformer._h
+                                        for t in self.interpolators])
+        lam = (C.c_double * nl)(*self.lam_max)
+        h = C.c_void_p()
+        check(lib.gb_mixed_new(nl, self.operators[0].operator._h, ops, rst,
+                               itp, lam, float(self.lam_min_coarse),
+                               int(self.coarse_degree), C.byref(h)))
+        self._h = _MixedHandle(lib, h, self)
+
+    def solve(self, phi, rho, charge=None, maxcharge=1e-6,
+              zero_initial_phi=False, timer=None):
+        """Neutral and charged-periodic branches of gpaw/poisson.py:182-231."""
+        actual_charge = self.gd.integrate(rho)
+        background = (actual_charge / self.gd.dv /
+                      self.gd.get_size_of_global_array().prod())
+        if charge is None:
+            charge = actual_charge
+        if abs(charge) <= maxcharge or self.gd.pbc_c.all():
+            if zero_initial_phi:
+                phi.zero_()
+            return self.solve_neutral(phi, rho - background)
+        raise NotImplementedError(
+            'charged non-periodic system (Gaussian monopole removal)')
+
+    def solve_neutral(self, phi, rho, timer=None):
+        rho = rho.contiguous()
+        niter = C.c_int(0)
+        rel = C.c_double(0.0)
+        rc = self._h.lib.gb_mixed_solve(
+            self._h.h, C.c_void_p(phi.data_ptr()), C.c_void_p(rho.data_ptr()),
+            float(self.tol), int(self.maxiter), C.byref(niter), C.byref(rel),
+            _stream())
+        self.niter = niter.value
+        self.rel_residual = rel.value
+        check(rc)
+        if self.gd.pbc_c.all():
+            phi -= phi.mean()
+        return niter.value
+
+
+class _MixedHandle:
+    def __init__(self, lib, h, owner):
+        self.lib = lib
+        self.h = h
+        self._keep = (owner.operators, owner.restrictors,
+                      owner.interpolators)
+
+    def __del__(self):
+        if self.h is not None and self.h.value:
+            self.lib.gb_mixed_free(self.h)
             self.h = None

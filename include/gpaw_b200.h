@@ -188,6 +188,32 @@ GB_API int gb_poisson_iterate(gb_poisson* p, double* phi, const double* rho, dou
 GB_API int gb_poisson_solve_neutral(gb_poisson* p, double* phi, const double* rho, double eps,
                              int maxiter, int* niter, double* error, void* stream);
 
+/* ------------------------------------------------ mixed-precision Poisson
+ * No counterpart in the reference (its Poisson solver is FP64 throughout):
+ * FP32 V-cycles inside FP64 defect correction, for the neutral problem
+ * L phi = rho of FDPoissonSolver.solve_neutral.  operators[0..nlevels-1]
+ * are the levels' stencils (used in FP32 below the coarsest level, FP64 on
+ * it), op64 the level-0 stencil applied in FP64 for the defect (normally
+ * operators[0] itself); restrictors/interpolators connect the levels.
+ * lam_max[l] is an upper bound of the spectrum of D^-1 A on level l (it sets
+ * the degree-2 Chebyshev smoother, interval [lam_max/8, 1.05 lam_max]);
+ * lam_min_coarse a lower bound on the coarsest level, which is solved with a
+ * degree-`coarse_degree` FP64 Chebyshev iteration.  The objects passed in
+ * must outlive the solver. */
+typedef struct gb_mixed gb_mixed;
+GB_API int gb_mixed_new(int nlevels, gb_operator* op64, gb_operator* const* operators,
+                        gb_transformer* const* restrictors,
+                        gb_transformer* const* interpolators, const double* lam_max,
+                        double lam_min_coarse, int coarse_degree, gb_mixed** out);
+GB_API void gb_mixed_free(gb_mixed* m);
+
+/* Solve until ||rho - L phi|| / ||rho|| <= tol (both norms in FP64, on the
+ * device), starting from phi; at most maxiter V-cycles (GB_ENOCONV
+ * otherwise).  Synchronises the stream once; *niter and *rel_residual
+ * (host) receive the V-cycle count and the final relative residual. */
+GB_API int gb_mixed_solve(gb_mixed* m, double* phi, const double* rho, double tol, int maxiter,
+                          int* niter, double* rel_residual, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,67 @@
+"""Mixed-precision Poisson solver (FP32 V-cycles in FP64 defect correction)
+against the FP64 oracle.
+
+Bar: the relative residual ||rho - L phi|| / ||rho||, recomputed here in
+FP64 by the oracle's own operator, is at most 1e-10 (x 1.01 for the
+different summation order), and the potential agrees with the oracle's FP64
+solution (solved to 1e-12) within 1e-7 relative (max norm); the measured
+maximum error is printed."""
+import numpy as np
+import pytest
+
+from oracle import gpaw_layer as L
+from tests.helpers import to_dev, to_np
+
+pytestmark = pytest.mark.gpu
+
+
+def _case(N, pbc, seed):
+    from gpaw_b200.workloads import BOHR, c1_density, neutralize
+    h = 0.2 / BOHR
+    gdo = L.GridDescriptor(N, tuple(n * h for n in N), pbc)
+    rho = neutralize(c1_density(gdo, seed=seed), gdo)
+    return gdo, rho
+
+
+@pytest.mark.parametrize('N,pbc', [((64, 64, 64), 0), ((48, 40, 56), 0),
+                                   ((48, 48, 48), 1)])
+def test_mixed_reaches_1e10_and_matches_fp64(N, pbc, cuda, capsys):
+    from gpaw_b200 import GridDescriptor, MixedPoissonSolver
+    gdo, rho = _case(N, pbc, seed=3)
+    gdp = GridDescriptor(N, np.diag(gdo.cell_cv), pbc)
+    ps = MixedPoissonSolver(nn=3, tol=1e-10)
+    ps.set_grid_descriptor(gdp)
+    phi = gdp.zeros()
+    n = ps.solve_neutral(phi, to_dev(rho))
+    got = to_np(phi)
+    # FP64 relative residual with the oracle's operator
+    op = L.Laplace(gdo, -0.25 / np.pi, 3)
+    lphi = np.zeros_like(got)
+    op.apply(got, lphi)
+    rel = np.sqrt(((rho - lphi)**2).sum() / (rho**2).sum())
+    # oracle FP64 solution to 1e-12 relative
+    eps = (1e-12 * np.sqrt((rho * rho).sum()))**2 * gdo.dv
+    po = L.FDPoissonSolver(nn=3, eps=eps, maxiter=2000)
+    po.set_grid_descriptor(gdo)
+    ref = gdo.zeros()
+    po.solve_neutral(ref, rho)
+    err = np.abs(got - ref).max() / np.abs(ref).max()
+    with capsys.disabled():
+        print(f'\nmixed {N} pbc={pbc}: {n} V-cycles, rel residual {rel:.3e} '
+              f'(device {ps.rel_residual:.3e}), max rel error vs FP64 '
+              f'{err:.3e}')
+    assert rel <= 1.01e-10
+    assert err <= 1e-7
+    assert n < 40
+
+
+def test_mixed_nonconvergence_raises(cuda):
+    from gpaw_b200 import (GridDescriptor, MixedPoissonSolver,
+                           PoissonConvergenceError)
+    gdo, rho = _case((32, 32, 32), 0, seed=1)
+    gdp = GridDescriptor((32, 32, 32), np.diag(gdo.cell_cv), 0)
+    ps = MixedPoissonSolver(tol=1e-10, maxiter=2)
+    ps.set_grid_descriptor(gdp)
+    with pytest.raises(PoissonConvergenceError):
+        ps.solve_neutral(gdp.zeros(), to_dev(rho))
+    assert ps.niter == 2
