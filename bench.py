@@ -455,11 +455,18 @@ def main():
     p.add_argument('--no-cpu', action='store_true')
     p.add_argument('--no-e2e', action='store_true')
     p.add_argument('--no-poisson', action='store_true')
+    p.add_argument('--poisson-only', default=None, choices=['c1', 'c3'],
+                   help='run one Poisson configuration only (profiling)')
     p.add_argument('--batch', type=int, default=NBANDS,
                    help='wave functions per step (profiling runs only)')
     args = p.parse_args()
     set_batch(args.batch)
-    if args.impl == 'reference':
+    if args.poisson_only:
+        import torch
+        dev = torch.device('cuda', 0)
+        f = poisson_c1 if args.poisson_only == 'c1' else poisson_c3
+        print(json.dumps(f(dev, nsolve=max(1, args.steps))), flush=True)
+    elif args.impl == 'reference':
         run_reference(args)
     else:
         run_gpu(args)

@@ -17,6 +17,8 @@
 // the device: a CUDA graph with a conditional WHILE node.
 #include <vector>
 
+#include <cooperative_groups.h>
+
 #include "gb_objects.cuh"
 
 using namespace gb;
@@ -119,6 +121,185 @@ k_coarse_cheb(const float* __restrict__ b, float* __restrict__ e, double* __rest
     for (int p = threadIdx.x; p < n; p += blockDim.x) e[p] = (float)x[p];
 }
 
+// Same iteration with the search direction in shared memory (double
+// buffered) and each thread's points (x, r) in registers: for coarsest grids
+// of at most KP * 1024 points.
+constexpr int KP = 14;
+constexpr int SMEM_COARSE_MAX = KP * 1024;
+
+// Axis-aligned 7-point stencil by axis (coefficients of +1 / -1 along each).
+struct Seven {
+    double c0, cp[3], cm[3];
+};
+
+__global__ void __launch_bounds__(1024, 1)
+k_coarse_cheb_smem(const float* __restrict__ b, float* __restrict__ e, GridBC g,
+                   const __grid_constant__ Stencil s, Seven s7, int seven, double lo,
+                   double hi, int deg) {
+    extern __shared__ __align__(16) double sm[];
+    const int n = g.n[0] * g.n[1] * g.n[2];
+    double* dA = sm;
+    double* dB = sm + n;
+    const double inv_c0 = 1.0 / s.coef[0];
+    const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo);
+    const double sigma = theta / delta;
+    double rho = 1.0 / sigma;
+    double x[KP], r[KP];
+    int ijk[KP];
+#pragma unroll
+    for (int k = 0; k < KP; k++) {
+        const int p = threadIdx.x + k * 1024;
+        x[k] = 0.0;
+        r[k] = 0.0;
+        ijk[k] = 0;
+        if (p < n) {
+            const int i2 = p % g.n[2];
+            const int t = p / g.n[2];
+            ijk[k] = ((t / g.n[1]) << 20) | ((t % g.n[1]) << 10) | i2;
+            r[k] = (double)b[p] * inv_c0;
+            dA[p] = r[k] / theta;
+        }
+    }
+    __syncthreads();
+    double* d = dA;
+    double* dn = dB;
+    for (int it = 0; it < deg; it++) {
+        const double rho_n = 1.0 / (2.0 * sigma - rho);
+        const double c1 = rho_n * rho, c2 = 2.0 * rho_n / delta;
+#pragma unroll
+        for (int k = 0; k < KP; k++) {
+            const int p = threadIdx.x + k * 1024;
+            if (p >= n) break;
+            const int i0 = ijk[k] >> 20, i1 = (ijk[k] >> 10) & 1023, i2 = ijk[k] & 1023;
+            const double dk = d[p];
+            double ad;
+            if (seven) {
+                // 7-point stencil: neighbour = p +- stride, wrapped or zero
+                // at the grid's edge
+                const int st1 = g.n[2], st0 = g.n[1] * g.n[2];
+                auto nb = [&](int i, int nax, int stride, int per, int dir) -> double {
+                    const int j = i + dir;
+                    if (j >= 0 && j < nax) return d[p + dir * stride];
+                    if (!per) return 0.0;
+                    return d[p + dir * stride - dir * nax * stride];
+                };
+                ad = s7.c0 * dk;
+                ad += s7.cp[0] * nb(i0, g.n[0], st0, g.periodic[0], +1) +
+                      s7.cm[0] * nb(i0, g.n[0], st0, g.periodic[0], -1);
+                ad += s7.cp[1] * nb(i1, g.n[1], st1, g.periodic[1], +1) +
+                      s7.cm[1] * nb(i1, g.n[1], st1, g.periodic[1], -1);
+                ad += s7.cp[2] * nb(i2, g.n[2], 1, g.periodic[2], +1) +
+                      s7.cm[2] * nb(i2, g.n[2], 1, g.periodic[2], -1);
+            } else {
+                ad = 0.0;
+                for (int c = 0; c < s.ncoefs; c++)
+                    ad += s.coef[c] * coarse_read(d, i0 + s.off[c][0], i1 + s.off[c][1],
+                                                  i2 + s.off[c][2], g);
+            }
+            x[k] += dk;
+            r[k] -= ad * inv_c0;
+            dn[p] = c1 * dk + c2 * r[k];
+        }
+        rho = rho_n;
+        __syncthreads();
+        double* tmp = d;
+        d = dn;
+        dn = tmp;
+    }
+#pragma unroll
+    for (int k = 0; k < KP; k++) {
+        const int p = threadIdx.x + k * 1024;
+        if (p < n) e[p] = (float)x[k];
+    }
+}
+
+// Same iteration spread over a cluster of CL CTAs: CTA r owns the flat
+// points [r * chunk, (r + 1) * chunk); its slab of the search direction
+// (double buffered) lives in its shared memory, and neighbours owned by other
+// CTAs are read through distributed shared memory.  One hardware cluster
+// barrier per step.  For coarsest grids of at most CL * 1024 * KPC points.
+constexpr int CL = 8;
+constexpr int KPC = 4;
+constexpr int CLUSTER_COARSE_MAX = CL * 1024 * KPC;
+
+__global__ void __cluster_dims__(CL, 1, 1) __launch_bounds__(1024, 1)
+k_coarse_cheb_cluster(const float* __restrict__ b, float* __restrict__ e, GridBC g, Seven s7,
+                      double lo, double hi, int deg) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    extern __shared__ __align__(16) double smc[];
+    const int n = g.n[0] * g.n[1] * g.n[2];
+    const int chunk = (n + CL - 1) / CL;
+    const int rank = (int)cluster.block_rank();
+    double* bufA = smc;
+    double* bufB = smc + chunk;
+    const double inv_c0 = 1.0 / s7.c0;
+    const double theta = 0.5 * (hi + lo), delta = 0.5 * (hi - lo);
+    const double sigma = theta / delta;
+    double rho = 1.0 / sigma;
+    const int st1 = g.n[2], st0 = g.n[1] * g.n[2];
+    double x[KPC], r[KPC];
+#pragma unroll
+    for (int k = 0; k < KPC; k++) {
+        const int li = threadIdx.x + k * 1024;
+        const int p = rank * chunk + li;
+        x[k] = 0.0;
+        r[k] = 0.0;
+        if (li < chunk && p < n) {
+            r[k] = (double)b[p] * inv_c0;
+            bufA[li] = r[k] / theta;
+        }
+    }
+    cluster.sync();
+    bool useA = true;
+    for (int it = 0; it < deg; it++) {
+        double* d = useA ? bufA : bufB;
+        double* dn = useA ? bufB : bufA;
+        auto at = [&](int q) -> double {
+            double* base = cluster.map_shared_rank(d, q / chunk);
+            return base[q % chunk];
+        };
+        const double rho_n = 1.0 / (2.0 * sigma - rho);
+        const double c1 = rho_n * rho, c2 = 2.0 * rho_n / delta;
+#pragma unroll
+        for (int k = 0; k < KPC; k++) {
+            const int li = threadIdx.x + k * 1024;
+            const int p = rank * chunk + li;
+            if (li >= chunk || p >= n) break;
+            const int i2 = p % g.n[2];
+            const int t = p / g.n[2];
+            const int i1 = t % g.n[1];
+            const int i0 = t / g.n[1];
+            auto nb = [&](int i, int nax, int stride, int per, int dir) -> double {
+                const int j = i + dir;
+                if (j >= 0 && j < nax) return at(p + dir * stride);
+                if (!per) return 0.0;
+                return at(p + dir * stride - dir * nax * stride);
+            };
+            const double dk = d[li];
+            double ad = s7.c0 * dk;
+            ad += s7.cp[0] * nb(i0, g.n[0], st0, g.periodic[0], +1) +
+                  s7.cm[0] * nb(i0, g.n[0], st0, g.periodic[0], -1);
+            ad += s7.cp[1] * nb(i1, g.n[1], st1, g.periodic[1], +1) +
+                  s7.cm[1] * nb(i1, g.n[1], st1, g.periodic[1], -1);
+            ad += s7.cp[2] * nb(i2, g.n[2], 1, g.periodic[2], +1) +
+                  s7.cm[2] * nb(i2, g.n[2], 1, g.periodic[2], -1);
+            x[k] += dk;
+            r[k] -= ad * inv_c0;
+            dn[li] = c1 * dk + c2 * r[k];
+        }
+        rho = rho_n;
+        cluster.sync();
+        useA = !useA;
+    }
+#pragma unroll
+    for (int k = 0; k < KPC; k++) {
+        const int li = threadIdx.x + k * 1024;
+        const int p = rank * chunk + li;
+        if (li < chunk && p < n) e[p] = (float)x[k];
+    }
+}
+
 __global__ void k_sumsq(const double* __restrict__ a, long long n, double* __restrict__ partial) {
     double v = 0.0;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
@@ -215,8 +396,52 @@ static int lin(gb_operator* op, const T* in, T* out, const T* aux, const T* aux2
 static int vcycle32(gb_mixed* m, int l, cudaStream_t st) {
     if (l == m->L) {
         gb_operator* op = m->ops[l];
-        k_coarse_cheb<<<1, 1024, 0, st>>>(m->b[l], m->e[l], m->x, m->r, m->da, m->db, op->g,
-                                           op->st, m->coarse_lo, m->coarse_hi, m->coarse_deg);
+        const long long n = op->ng();
+        // the 7-point form of the coarsest operator, if it has one
+        Seven s7{};
+        int seven = op->st.ncoefs == 7 && op->st.range == 1 && op->st.cfd;
+        if (seven) {
+            for (int c = 0; c < 7; c++) {
+                int ax = -1, dir = 0;
+                for (int a = 0; a < 3; a++)
+                    if (op->st.off[c][a]) {
+                        ax = a;
+                        dir = op->st.off[c][a];
+                    }
+                if (ax < 0) s7.c0 += op->st.coef[c];
+                else if (dir > 0) s7.cp[ax] = op->st.coef[c];
+                else s7.cm[ax] = op->st.coef[c];
+            }
+        }
+        if (seven && n <= CLUSTER_COARSE_MAX) {
+            const int chunk = (int)((n + CL - 1) / CL);
+            const size_t smem = (size_t)2 * chunk * sizeof(double);
+            static bool cattr = false;
+            if (!cattr) {
+                GB_CUDA_TRY(cudaFuncSetAttribute(k_coarse_cheb_cluster,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)((size_t)2 * (CLUSTER_COARSE_MAX / CL) *
+                                                       sizeof(double))));
+                cattr = true;
+            }
+            k_coarse_cheb_cluster<<<CL, 1024, smem, st>>>(m->b[l], m->e[l], op->g, s7,
+                                                          m->coarse_lo, m->coarse_hi,
+                                                          m->coarse_deg);
+        } else if (n <= SMEM_COARSE_MAX && op->g.n[1] < 1024 && op->g.n[2] < 1024) {
+            const size_t smem = (size_t)2 * n * sizeof(double);
+            static bool attr = false;
+            if (!attr) {
+                GB_CUDA_TRY(cudaFuncSetAttribute(k_coarse_cheb_smem,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                 (int)((size_t)2 * SMEM_COARSE_MAX * sizeof(double))));
+                attr = true;
+            }
+            k_coarse_cheb_smem<<<1, 1024, smem, st>>>(m->b[l], m->e[l], op->g, op->st, s7, seven,
+                                                       m->coarse_lo, m->coarse_hi, m->coarse_deg);
+        } else {
+            k_coarse_cheb<<<1, 1024, 0, st>>>(m->b[l], m->e[l], m->x, m->r, m->da, m->db, op->g,
+                                               op->st, m->coarse_lo, m->coarse_hi, m->coarse_deg);
+        }
         GB_LAUNCH_CHECK();
         return 0;
     }

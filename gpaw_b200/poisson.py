@@ -244,7 +244,7 @@ class MixedPoissonSolver:
     """
 
     def __init__(self, nn=3, tol=1e-10, maxiter=200, levels=4,
-                 coarse_accuracy=0.05):
+                 coarse_accuracy=0.2):
         self.nn = nn
         self.tol = tol
         self.maxiter = maxiter
