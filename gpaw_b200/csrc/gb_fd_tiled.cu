@@ -20,10 +20,32 @@
 // Periodic halos are copied from the wrapped position; the Bloch phase of a
 // wrapped complex value is applied when it is read (register-side, exact
 // complex multiply as in bmgs_translatemz, c/bmgs/translate.cpp:28-47).
+#include <cstdlib>
+#include <utility>
+
 #include "gb_internal.cuh"
 
 namespace gb {
 
+
+// Planes per CTA along axis 0.  A batch of grids already gives enough
+// CTAs; a single grid is split along axis 0 until the launch has at least
+// `target` CTAs (default 148 * 2, tunable by GPAW_B200_CTA_TARGET), but
+// never into chunks shorter than 2 nn planes.
+int cfd_chunk(const GridBC& g, int nn, int nin) {
+    static int target = [] {
+        const char* v = getenv("GPAW_B200_CTA_TARGET");
+        const int t = v ? atoi(v) : 0;
+        return t > 0 ? t : 148 * 2;
+    }();
+    const int tiles_x = (g.n[2] + 31) / 32;
+    const int tiles_y = (g.n[1] + 15) / 16;
+    const long long tiles = (long long)tiles_x * tiles_y * nin;
+    int chunk0 = g.n[0];
+    while (chunk0 > 2 * nn && tiles * ((g.n[0] + chunk0 - 1) / chunk0) < target)
+        chunk0 = (chunk0 + 1) / 2;
+    return chunk0;
+}
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
     return (unsigned)__cvta_generic_to_shared(p);
@@ -81,6 +103,16 @@ __device__ __forceinline__ bool wrap_coord(int& y, int n, int periodic) {
     return y >= 0 && y < n;
 }
 
+// Call f(std::integral_constant<int, I>) for I = 0 .. N-1.
+template <class F, int... Is>
+__device__ __forceinline__ void static_for_impl(F&& f, std::integer_sequence<int, Is...>) {
+    (f(std::integral_constant<int, Is>{}), ...);
+}
+template <int N, class F>
+__device__ __forceinline__ void static_for(F&& f) {
+    static_for_impl(f, std::make_integer_sequence<int, N>{});
+}
+
 // Sum of one direction's 2*NN terms in the caller's order: +1..+NN then
 // -1..-NN.  `vp(d)` / `vm(d)` return the values at +d / -d.
 template <class T, int NN, class VP, class VM>
@@ -92,8 +124,8 @@ __device__ __forceinline__ T add_direction(T x, const double* cp, const double* 
     return x;
 }
 
-// ORD = 1: directions are axis 2, axis 1, axis 0 (the order GUCLaplace
-// builds for an orthorhombic cell); ORD = 0: order read from cs.axis.
+// Directions are summed in the order GUCLaplace builds for an orthorhombic
+// cell: axis 2, axis 1, axis 0 (ORD = 1, the only instantiation).
 // 128 registers a thread: two resident CTAs of 256 threads (complex) or
 // four of 128 (real) when the tile holds two or four rows per thread.
 template <class T, int NN, int TX, int TY, int RY, int D, int MODE, int ORD>
@@ -208,10 +240,9 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
     };
 
     // -- axis-0 queue ---------------------------------------------------------
-    // Before iteration t's push, q[k] (k < 2NN) holds relative plane t-2NN+k;
-    // iteration t pushes plane t into q[2NN] and, for t >= NN, computes the
-    // centre plane t-NN.  Planes pa-NN..pa-1 (before the chunk) come straight
-    // from global memory into q[NN..2NN-1].
+    // Slot j % Q of the queue holds relative plane j (j = -NN .. nplanes +
+    // NN - 1).  Planes pa-NN..pa-1 (before the chunk) come straight from
+    // global memory.
     T q[RY][Q];
 #pragma unroll
     for (int r = 0; r < RY; r++)
@@ -231,7 +262,7 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
                 if constexpr (CPLX)
                     if (P.use && wrapped) v = cmul(P.ph[0][1], v);
             }
-            q[r][NN + k] = v;
+            q[r][NN + 1 + k] = v;   // relative plane k - NN sits in slot k + NN + 1
         }
     }
 
@@ -244,8 +275,13 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
     }
 
     const int nplanes = pb - pa;
-#pragma unroll 1
-    for (int t = 0; t < nplanes + NN; t++) {
+    const int total = nplanes + NN;
+    // Iteration t pushes relative plane t into queue slot t % Q and, for
+    // t >= NN, computes centre plane t - NN.  The loop is unrolled by Q so
+    // that every slot index is a compile-time constant (no register moves).
+    auto step = [&](int t, auto U_) {
+        constexpr int U = decltype(U_)::value;           // t % Q
+        constexpr int CU = (U + Q - NN) % Q;              // slot of the centre
         cp_wait<D - 1>();
         // this thread's copies of plane t have landed: fix its wrapped halo
         // cells (read as a centre NN iterations later, after a barrier)
@@ -267,7 +303,7 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
                 T v = st_in[(ty0 + r + NN) * PX + (tx + NN)];
                 if constexpr (CPLX)
                     if (wrapped) v = cmul(P.ph[0][0], v);
-                q[r][2 * NN] = v;
+                q[r][U] = v;
             }
         }
         if (t >= NN) {
@@ -277,33 +313,21 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
             const T* colp = sc + ty0 * PX + (tx + NN);
 #pragma unroll
             for (int r = 0; r < RY; r++) {
-                const T vc = q[r][NN];
+                const T vc = q[r][CU];
                 const T* row = sc + (ty0 + r + NN) * PX + (tx + NN);
                 // x = 0; x += v c in coefficient order (Jacobi skips c0)
                 T x = Num<T>::zero();
                 if (MODE != EPI_JACOBI) x = Num<T>::add(x, Num<T>::scale(vc, cs.c0));
-                auto dir = [&](int k, int ax) {
-                    if (ax == 0)
-                        x = add_direction<T, NN>(x, cs.cp[k], cs.cm[k],
-                                                 [&](int d) { return q[r][NN + d]; },
-                                                 [&](int d) { return q[r][NN - d]; });
-                    else if (ax == 1)
-                        x = add_direction<T, NN>(x, cs.cp[k], cs.cm[k],
-                                                 [&](int d) { return colp[(r + NN + d) * PX]; },
-                                                 [&](int d) { return colp[(r + NN - d) * PX]; });
-                    else
-                        x = add_direction<T, NN>(x, cs.cp[k], cs.cm[k],
-                                                 [&](int d) { return row[d]; },
-                                                 [&](int d) { return row[-d]; });
-                };
-                if constexpr (ORD == 1) {
-                    dir(0, 2);
-                    dir(1, 1);
-                    dir(2, 0);
-                } else {
-#pragma unroll
-                    for (int k = 0; k < 3; k++) dir(k, cs.axis[k]);
-                }
+                // directions: axis 2, axis 1, axis 0 (GUCLaplace's order)
+                x = add_direction<T, NN>(x, cs.cp[0], cs.cm[0],
+                                         [&](int d) { return row[d]; },
+                                         [&](int d) { return row[-d]; });
+                x = add_direction<T, NN>(x, cs.cp[1], cs.cm[1],
+                                         [&](int d) { return colp[(r + NN + d) * PX]; },
+                                         [&](int d) { return colp[(r + NN - d) * PX]; });
+                x = add_direction<T, NN>(x, cs.cp[2], cs.cm[2],
+                                         [&](int d) { return q[r][(CU + d) % Q]; },
+                                         [&](int d) { return q[r][(CU + Q - d) % Q]; });
                 const int gy = y0 + ty0 + r;
                 if (gx < n2 && gy < n1) {
                     const long long at = ((long long)p * n1 + gy) * n2 + gx;
@@ -332,11 +356,13 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
                 }
             }
         }
-#pragma unroll
-        for (int r = 0; r < RY; r++)
-#pragma unroll
-            for (int k = 0; k < Q - 1; k++) q[r][k] = q[r][k + 1];
-    }
+    };
+#pragma unroll 1
+    for (int t0 = 0; t0 < total; t0 += Q)
+        static_for<Q>([&](auto U_) {
+            const int t = t0 + decltype(U_)::value;
+            if (t < total) step(t, U_);
+        });
     cp_wait<0>();
     if ((MODE == EPI_RESID || MODE == EPI_LIN) && ep.partial) {
         sq = block_sum(sq);
@@ -360,11 +386,7 @@ static int launch_cfd_t(const void* in, void* out, int nin, const GridBC& g, con
     }
     const int tiles_x = (g.n[2] + TX - 1) / TX;
     const int tiles_y = (g.n[1] + TY - 1) / TY;
-    int chunk0 = g.n[0];
-    const long long tiles = (long long)tiles_x * tiles_y * nin;
-    // split axis 0 until the grid covers the GPU a few times
-    while (chunk0 > 2 * NN && tiles * ((g.n[0] + chunk0 - 1) / chunk0) < 148 * 4)
-        chunk0 = (chunk0 + 1) / 2;
+    const int chunk0 = cfd_chunk(g, NN, nin);
     const int nch = (g.n[0] + chunk0 - 1) / chunk0;
     if (nblk) *nblk = tiles_x * tiles_y * nch;
     const long long ng = (long long)g.n[0] * g.n[1] * g.n[2];
@@ -385,18 +407,16 @@ static int launch_cfd_t(const void* in, void* out, int nin, const GridBC& g, con
 template <class T, int NN, int MODE>
 static int launch_cfd_nn(const void* in, void* out, int nin, const GridBC& g, const Phases& P,
                          const CfdStencil& cs, const Epi& ep, cudaStream_t st, int* nblk) {
-    const bool ord210 = cs.axis[0] == 2 && cs.axis[1] == 1 && cs.axis[2] == 0;
+    // only the direction order GUCLaplace builds (axis 2, 1, 0); other
+    // axis-aligned stencils take the generic kernel
+    if (!(cs.axis[0] == 2 && cs.axis[1] == 1 && cs.axis[2] == 0)) return -1;
     if constexpr (sizeof(T) == 16) {
         constexpr int D = NN <= 3 ? 3 : 2;
         constexpr int RY = NN <= 3 ? 2 : 1;
-        if (ord210)
-            return launch_cfd_t<T, NN, 32, 16, RY, D, MODE, 1>(in, out, nin, g, P, cs, ep, st, nblk);
-        return launch_cfd_t<T, NN, 32, 16, RY, D, MODE, 0>(in, out, nin, g, P, cs, ep, st, nblk);
+        return launch_cfd_t<T, NN, 32, 16, RY, D, MODE, 1>(in, out, nin, g, P, cs, ep, st, nblk);
     } else {
         constexpr int RY = NN <= 3 ? 4 : 2;
-        if (ord210)
-            return launch_cfd_t<T, NN, 32, 16, RY, 4, MODE, 1>(in, out, nin, g, P, cs, ep, st, nblk);
-        return launch_cfd_t<T, NN, 32, 16, RY, 4, MODE, 0>(in, out, nin, g, P, cs, ep, st, nblk);
+        return launch_cfd_t<T, NN, 32, 16, RY, 4, MODE, 1>(in, out, nin, g, P, cs, ep, st, nblk);
     }
 }
 
@@ -449,10 +469,7 @@ int cfd_blocks(const GridBC& g, int nn, int elem_bytes, int nin) {
     const int TX = 32, TY = 16;
     const int tiles_x = (g.n[2] + TX - 1) / TX;
     const int tiles_y = (g.n[1] + TY - 1) / TY;
-    int chunk0 = g.n[0];
-    const long long tiles = (long long)tiles_x * tiles_y * nin;
-    while (chunk0 > 2 * nn && tiles * ((g.n[0] + chunk0 - 1) / chunk0) < 148 * 4)
-        chunk0 = (chunk0 + 1) / 2;
+    const int chunk0 = cfd_chunk(g, nn, nin);
     (void)elem_bytes;
     return tiles_x * tiles_y * ((g.n[0] + chunk0 - 1) / chunk0);
 }
