@@ -292,6 +292,92 @@ def poisson_c3(dev, nsolve=5):
     return out
 
 
+def poisson_c4(dev, count=512, precisions=('mixed', 'fp64')):
+    """512 zero-BC grids, every side from {32, 40, ..., 128}, each with 4-16
+    seeded Gaussians (C3 distributions), solved to 1e-10 relative residual:
+    every solve enqueued on one of 16 streams, one synchronisation."""
+    import torch
+    from gpaw_b200.batch import PoissonBatch, c4_grids
+    from gpaw_b200.workloads import neutral_density_device
+    gds = c4_grids(count, seed=0, device=dev)
+    rng = np.random.default_rng(1)
+    rhos = [neutral_density_device(gd, int(rng.integers(4, 17)), 100 + i)
+            for i, gd in enumerate(gds)]
+    npts = sum(int(np.prod(gd.n_c)) for gd in gds)
+    out = {'grids': count, 'points': npts,
+           'sides': '{32,40,...,128} per axis, zero BC, h = 0.18 A'}
+    for prec in precisions:
+        t0 = time.perf_counter()
+        batch = PoissonBatch(gds, tol=1e-10, precision=prec, nstreams=16)
+        phis = [gd.zeros() for gd in gds]
+        batch.prepare(rhos)
+        batch.solve(phis, rhos)                # warm-up: builds the graphs
+        setup = time.perf_counter() - t0
+        for p in phis:
+            p.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        n = batch.solve(phis, rhos)
+        t = time.perf_counter() - t0
+        out[prec] = {'solves_per_s': count / t, 'seconds': t,
+                     'vcycles_mean': float(np.mean(n)),
+                     'vcycles_max': int(np.max(n)), 'setup_s': setup}
+        del batch
+    if 'mixed' in out and 'fp64' in out:
+        out['speedup_mixed_over_fp64'] = (out['mixed']['solves_per_s'] /
+                                          out['fp64']['solves_per_s'])
+    return out
+
+
+def precond_c4(dev, nbands=128):
+    """Preconditioner (gpaw/preconditioner.py) on 128 float64 band residuals,
+    112^3 periodic (Gamma point), kinetic operator nn = 3."""
+    import torch
+    from gpaw_b200 import GridDescriptor, Laplace, Preconditioner
+    from gpaw_b200.workloads import BOHR
+    N = (112, 112, 112)
+    gd = GridDescriptor(N, (112 * 0.18 / BOHR,) * 3, 1, device=dev)
+    pc = Preconditioner(gd, Laplace(gd, -0.5, 3), float, block=nbands)
+    g = torch.Generator(device=dev)
+    g.manual_seed(0)
+    R = torch.randn((nbands,) + N, dtype=torch.float64, device=dev,
+                    generator=g)
+    out = torch.empty_like(R)
+    for _ in range(2):
+        pc(R, None, out=out)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    reps = 5
+    e0.record()
+    for _ in range(reps):
+        pc(R, None, out=out)
+    e1.record()
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / 1e3 / reps
+    return {'bands': nbands, 'grid': list(N), 'ms_per_call': t * 1e3,
+            'blackbox_gbs': 16 * R.numel() / t / 1e9}
+
+
+def serving_c5(dev, rates=(50, 100, 200, 500, 1000, 2000), count=60):
+    """Poisson-arrival stream of mixed-precision Poisson solves (to 1e-10)
+    and nn = 3 stencil applications, grid sides log-uniform in [24, 160]
+    (multiples of 8), admitted against a 16 GB budget, 8 slots."""
+    from gpaw_b200.serving import Server, latency_stats, make_requests
+    srv = Server(hbm_budget=16 << 30, nslots=8, device=dev)
+    srv.warm([(s, s, s) for s in range(24, 161, 8)])
+    out = {'slots': 8, 'hbm_budget_gb': 16, 'requests_per_rate': count}
+    for lam in rates:
+        reqs = make_requests(lam, count, seed=lam)
+        inputs = {r.rid: srv.host_input(r) for r in reqs}
+        srv.run(reqs, inputs)
+        st = latency_stats(reqs)
+        st['poisson_vcycles_mean'] = float(np.mean(
+            [r.niter for r in reqs if r.kind == 'poisson'] or [0]))
+        out[f'lambda_{lam}'] = st
+    return out
+
+
 # ---------------------------------------------------------------- GPU side
 def run_gpu(args):
     import torch
@@ -437,6 +523,11 @@ def run_gpu(args):
     }
     if not args.no_poisson:
         line['poisson'] = {'c1': poisson_c1(dev), 'c3': poisson_c3(dev)}
+    if not args.no_batch:
+        line.setdefault('poisson', {})['c4_batch'] = poisson_c4(dev)
+        line['preconditioner_c4'] = precond_c4(dev)
+    if not args.no_serving:
+        line['serving_c5'] = serving_c5(dev)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -455,7 +546,10 @@ def main():
     p.add_argument('--no-cpu', action='store_true')
     p.add_argument('--no-e2e', action='store_true')
     p.add_argument('--no-poisson', action='store_true')
-    p.add_argument('--poisson-only', default=None, choices=['c1', 'c3'],
+    p.add_argument('--no-batch', action='store_true')
+    p.add_argument('--no-serving', action='store_true')
+    p.add_argument('--poisson-only', default=None,
+                   choices=['c1', 'c3', 'c4', 'pc', 'c5'],
                    help='run one Poisson configuration only (profiling)')
     p.add_argument('--batch', type=int, default=NBANDS,
                    help='wave functions per step (profiling runs only)')
@@ -464,8 +558,13 @@ def main():
     if args.poisson_only:
         import torch
         dev = torch.device('cuda', 0)
-        f = poisson_c1 if args.poisson_only == 'c1' else poisson_c3
-        print(json.dumps(f(dev, nsolve=max(1, args.steps))), flush=True)
+        if args.poisson_only in ('c1', 'c3'):
+            f = poisson_c1 if args.poisson_only == 'c1' else poisson_c3
+            r = f(dev, nsolve=max(1, args.steps))
+        else:
+            r = {'c4': poisson_c4, 'pc': precond_c4,
+                 'c5': serving_c5}[args.poisson_only](dev)
+        print(json.dumps(r), flush=True)
     elif args.impl == 'reference':
         run_reference(args)
     else:

@@ -55,6 +55,11 @@ SIGNATURES = {
                                C.POINTER(_p), _dp, C.c_double, C.c_int,
                                C.POINTER(_p)]),
     'gb_mixed_free': (None, [_p]),
+    'gb_mixed_solve_async': (C.c_int, [_p, _p, _p, C.c_double, C.c_int, _p]),
+    'gb_mixed_result': (C.c_int, [_p, C.POINTER(C.c_int), _dp]),
+    'gb_poisson_solve_neutral_async': (C.c_int, [_p, _p, _p, C.c_double,
+                                                 C.c_int, _p]),
+    'gb_poisson_result': (C.c_int, [_p, C.POINTER(C.c_int), _dp]),
     'gb_mixed_solve': (C.c_int, [_p, _p, _p, C.c_double, C.c_int,
                                  C.POINTER(C.c_int), _dp, _p]),
     'gb_poisson_iterate': (C.c_int, [_p, _p, _p, _dp, _p]),

@@ -410,6 +410,7 @@ struct gb_poisson {
     SolveCtl* ctl_host = nullptr;
     cudaStream_t cap = nullptr;
     cudaGraphExec_t solve_exec = nullptr;
+    int last_maxiter = 0;
     ~gb_poisson() {
         if (solve_exec) cudaGraphExecDestroy(solve_exec);
         if (cap) cudaStreamDestroy(cap);
@@ -639,8 +640,8 @@ static int build_solve_graph(gb_poisson* p) {
     return 0;
 }
 
-extern "C" int gb_poisson_solve_neutral(gb_poisson* p, double* phi, const double* rho, double eps,
-                                        int maxiter, int* niter, double* error, void* stream) {
+extern "C" int gb_poisson_solve_neutral_async(gb_poisson* p, double* phi, const double* rho,
+                                              double eps, int maxiter, void* stream) {
     if (!p || !phi || !rho) return fail(GB_EINVAL, "Poisson solve: NULL argument");
     if (maxiter < 1) return fail(GB_EINVAL, "Poisson solve: maxiter must be >= 1");
     cudaStream_t st = (cudaStream_t)stream;
@@ -655,13 +656,26 @@ extern "C" int gb_poisson_solve_neutral(gb_poisson* p, double* phi, const double
     GB_CUDA_TRY(cudaGraphLaunch(p->solve_exec, st));
     GB_CUDA_TRY(cudaMemcpyAsync(phi, p->phi0, bytes, cudaMemcpyDeviceToDevice, st));
     GB_CUDA_TRY(cudaMemcpyAsync(p->ctl_host, p->ctl, sizeof(SolveCtl), cudaMemcpyDeviceToHost, st));
-    GB_CUDA_TRY(cudaStreamSynchronize(st));
+    p->last_maxiter = maxiter;
+    return 0;
+}
+
+extern "C" int gb_poisson_result(gb_poisson* p, int* niter, double* error) {
+    if (!p) return fail(GB_EINVAL, "Poisson result: NULL executor");
     const int it = p->ctl_host->niter;
     if (niter) *niter = it;
     if (error) *error = p->ctl_host->err;
-    if (it >= maxiter)
-        return fail(GB_ENOCONV, "Poisson solver did not converge in %d iterations!", maxiter);
+    if (it >= p->last_maxiter)
+        return fail(GB_ENOCONV, "Poisson solver did not converge in %d iterations!",
+                    p->last_maxiter);
     return 0;
+}
+
+extern "C" int gb_poisson_solve_neutral(gb_poisson* p, double* phi, const double* rho, double eps,
+                                        int maxiter, int* niter, double* error, void* stream) {
+    if (int rc = gb_poisson_solve_neutral_async(p, phi, rho, eps, maxiter, stream)) return rc;
+    GB_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+    return gb_poisson_result(p, niter, error);
 }
 
 // ------------------------------------------------- relax without allocation

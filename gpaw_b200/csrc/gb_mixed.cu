@@ -338,6 +338,8 @@ struct gb_mixed {
     std::vector<ChebLevel> ch;
     double coarse_lo = 0, coarse_hi = 0;
     int coarse_deg = 0;
+    double last_tol = 0.0;
+    int last_maxiter = 0;
     std::vector<float*> b, e, t;       // levels 0..L (b[L], e[L] used at L)
     double *x = nullptr, *r = nullptr, *da = nullptr, *db = nullptr;
     double *phi0 = nullptr, *rho0 = nullptr;
@@ -623,8 +625,8 @@ static int build_mixed_graph(gb_mixed* m) {
     return 0;
 }
 
-extern "C" int gb_mixed_solve(gb_mixed* m, double* phi, const double* rho, double tol,
-                              int maxiter, int* niter, double* rel_residual, void* stream) {
+extern "C" int gb_mixed_solve_async(gb_mixed* m, double* phi, const double* rho, double tol,
+                                    int maxiter, void* stream) {
     if (!m || !phi || !rho) return fail(GB_EINVAL, "mixed solve: NULL argument");
     if (maxiter < 1) return fail(GB_EINVAL, "mixed solve: maxiter must be >= 1");
     cudaStream_t st = (cudaStream_t)stream;
@@ -642,11 +644,24 @@ extern "C" int gb_mixed_solve(gb_mixed* m, double* phi, const double* rho, doubl
     GB_CUDA_TRY(cudaGraphLaunch(m->exec, st));
     GB_CUDA_TRY(cudaMemcpyAsync(phi, m->phi0, bytes, cudaMemcpyDeviceToDevice, st));
     GB_CUDA_TRY(cudaMemcpyAsync(m->ctl_host, m->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, st));
-    GB_CUDA_TRY(cudaStreamSynchronize(st));
+    m->last_tol = tol;
+    m->last_maxiter = maxiter;
+    return 0;
+}
+
+extern "C" int gb_mixed_result(gb_mixed* m, int* niter, double* rel_residual) {
+    if (!m) return fail(GB_EINVAL, "mixed result: NULL solver");
     if (niter) *niter = m->ctl_host->niter;
     if (rel_residual) *rel_residual = m->ctl_host->rel;
-    if (m->ctl_host->rel > tol)
+    if (m->ctl_host->rel > m->last_tol)
         return fail(GB_ENOCONV, "mixed-precision Poisson solver did not reach %g in %d V-cycles",
-                    tol, maxiter);
+                    m->last_tol, m->last_maxiter);
     return 0;
+}
+
+extern "C" int gb_mixed_solve(gb_mixed* m, double* phi, const double* rho, double tol,
+                              int maxiter, int* niter, double* rel_residual, void* stream) {
+    if (int rc = gb_mixed_solve_async(m, phi, rho, tol, maxiter, stream)) return rc;
+    GB_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+    return gb_mixed_result(m, niter, rel_residual);
 }

@@ -167,6 +167,29 @@ class FDPoissonSolver:
         check(rc)
         return niter.value
 
+    def solve_neutral_async(self, phi, rho, eps=None):
+        """Enqueue solve_neutral on the current stream; read the outcome with
+        result() once the stream has reached this point.  ``rho`` must stay
+        alive and unchanged until then."""
+        self._init()
+        check(self._exec.lib.gb_poisson_solve_neutral_async(
+            self._exec.h, C.c_void_p(phi.data_ptr()),
+            C.c_void_p(rho.data_ptr()),
+            float(self.eps if eps is None else eps), int(self.maxiter),
+            _stream()))
+
+    def result(self):
+        """V-cycle count of the last asynchronous solve (raises
+        PoissonConvergenceError if it stopped at maxiter)."""
+        niter = C.c_int(0)
+        err = C.c_double(0.0)
+        rc = self._exec.lib.gb_poisson_result(self._exec.h, C.byref(niter),
+                                              C.byref(err))
+        self.niter = niter.value
+        self.last_error = err.value
+        check(rc)
+        return niter.value
+
     def iterate2(self, step, level=0, phi=None, rho=None):
         """One V-cycle from level 0 (gpaw/poisson.py:500-537); returns the
         level-0 error sum(r^2) * dv."""
@@ -324,6 +347,29 @@ class MixedPoissonSolver:
         if self.gd.pbc_c.all():
             phi -= phi.mean()
         return niter.value
+
+
+def _mixed_async(self, phi, rho):
+    """Enqueue solve_neutral on the current stream (no host sync); the
+    periodic mean removal is left to the caller."""
+    check(self._h.lib.gb_mixed_solve_async(
+        self._h.h, C.c_void_p(phi.data_ptr()), C.c_void_p(rho.data_ptr()),
+        float(self.tol), int(self.maxiter), _stream()))
+
+
+def _mixed_result(self):
+    niter = C.c_int(0)
+    rel = C.c_double(0.0)
+    rc = self._h.lib.gb_mixed_result(self._h.h, C.byref(niter),
+                                     C.byref(rel))
+    self.niter = niter.value
+    self.rel_residual = rel.value
+    check(rc)
+    return niter.value
+
+
+MixedPoissonSolver.solve_neutral_async = _mixed_async
+MixedPoissonSolver.result = _mixed_result
 
 
 class _MixedHandle:

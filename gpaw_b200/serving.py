@@ -1,0 +1,227 @@
+"""Continuous-batching request loop for Poisson solves and FD applications.
+
+Requests arrive over time (``Request.arrival``, seconds after start).  The
+loop admits an arrived request as soon as a slot (a CUDA stream) is free and
+its memory fits the HBM budget, and keeps admitting while earlier requests
+are still running, so the work of many requests overlaps on the GPU.  Each
+request brings its input from pinned host memory and gets its result back
+into pinned host memory: its latency is completion minus arrival, measured
+on the host clock.
+
+Solvers and operators are kept resident per grid shape (a pool of
+instances, one per concurrently running request of that shape), so the
+multigrid hierarchies, their buffers and their captured CUDA graphs are
+built once and reused.  Every kernel is deterministic and a request never
+shares a buffer with another, so a request's result does not depend on what
+else runs beside it.
+"""
+from __future__ import annotations
+
+import collections
+import dataclasses
+import time
+from math import pi
+
+import numpy as np
+import torch
+
+
+@dataclasses.dataclass
+class Request:
+    rid: int
+    kind: str            # 'poisson' (mixed-precision solve) or 'apply'
+    N: tuple             # grid points per axis (zero boundaries)
+    arrival: float       # seconds after the start of the run
+    seed: int = 0
+    # filled in by the server
+    start: float = 0.0
+    done: float = 0.0
+    niter: int = 0
+    result: np.ndarray = None
+
+
+def make_requests(rate, count, seed=0, poisson_fraction=0.5, smin=24,
+                  smax=160):
+    """Poisson-process arrivals at `rate` per second; grid side log-uniform
+    in [smin, smax], rounded to a multiple of 8 (so every grid has at least
+    three multigrid levels)."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, count))
+    out = []
+    for i in range(count):
+        side = np.exp(rng.uniform(np.log(smin), np.log(smax)))
+        side = int(max(smin, min(smax, 8 * round(side / 8))))
+        kind = 'poisson' if rng.random() < poisson_fraction else 'apply'
+        out.append(Request(i, kind, (side, side, side), float(t[i]),
+                           int(rng.integers(1 << 30))))
+    return out
+
+
+class Server:
+    """Continuous-batching loop on one GPU.
+
+    hbm_budget: bytes of device memory the loop may hold for requests and
+    their resident solvers; nslots: requests in flight at most."""
+
+    SPACING = 0.18 / 0.52917721   # Bohr
+
+    def __init__(self, hbm_budget=8 << 30, nslots=8, tol=1e-10,
+                 device=None):
+        self.device = torch.device(device if device is not None else 'cuda')
+        self.budget = int(hbm_budget)
+        self.tol = tol
+        self.streams = [torch.cuda.Stream(device=self.device)
+                        for _ in range(nslots)]
+        self.free_slots = list(range(nslots))
+        self.pools = collections.defaultdict(list)   # (kind, N) -> free objs
+        self.resident = 0        # bytes held by pooled solvers/operators
+        self.in_use = 0          # bytes held by running requests
+        self.ops = {}            # N -> Laplace for apply requests
+
+    # -- resources ---------------------------------------------------------
+    def _gd(self, N):
+        from .grid_descriptor import GridDescriptor
+        return GridDescriptor(N, tuple(n * self.SPACING for n in N), 0,
+                              device=self.device)
+
+    @staticmethod
+    def request_bytes(req):
+        n = int(np.prod([x - 1 for x in req.N]))
+        return 2 * 8 * n     # input and output array
+
+    @staticmethod
+    def solver_bytes(N):
+        n = int(np.prod([x - 1 for x in N]))
+        return 48 * n        # FP64 copies, FP32 levels, scratch (estimate)
+
+    def _take_solver(self, req):
+        from .poisson import MixedPoissonSolver
+        pool = self.pools[('poisson', req.N)]
+        if pool:
+            return pool.pop(), 0
+        ps = MixedPoissonSolver(nn=3, tol=self.tol, levels=4)
+        ps.set_grid_descriptor(self._gd(req.N))
+        return ps, self.solver_bytes(req.N)
+
+    def warm(self, shapes):
+        """Build one resident solver and operator per shape ahead of time."""
+        for N in shapes:
+            req = Request(-1, 'poisson', N, 0.0)
+            ps, nb = self._take_solver(req)
+            self.resident += nb
+            phi = ps.gd.zeros()
+            rho = ps.gd.zeros()
+            rho[0, 0, 0] = 1.0
+            rho -= rho.mean()
+            try:
+                ps.solve_neutral(phi, rho)
+            except RuntimeError:
+                pass
+            self.pools[('poisson', N)].append(ps)
+            self._op(N)
+        torch.cuda.synchronize()
+
+    def _op(self, N):
+        from .fd_operators import Laplace
+        if N not in self.ops:
+            self.ops[N] = Laplace(self._gd(N), -0.25 / pi, 3)
+        return self.ops[N]
+
+    # -- inputs --------------------------------------------------------------
+    def host_input(self, req):
+        """Pinned host input of a request: a neutral sum of Gaussians for a
+        solve, N(0,1) values for an apply (seeded per request)."""
+        from .workloads import neutral_density_device
+        gd = self._gd(req.N)
+        if req.kind == 'poisson':
+            a = neutral_density_device(gd, 8, req.seed).cpu()
+        else:
+            a = torch.from_numpy(np.random.default_rng(req.seed)
+                                 .standard_normal(tuple(int(x)
+                                                        for x in gd.n_c)))
+        return a.pin_memory()
+
+    # -- one request ----------------------------------------------------------
+    def _launch(self, req, host_in, host_out, slot):
+        st = self.streams[slot]
+        shape = tuple(host_in.shape)
+        with torch.cuda.stream(st):
+            x = torch.empty(shape, dtype=torch.float64, device=self.device)
+            y = torch.empty(shape, dtype=torch.float64, device=self.device)
+            x.copy_(host_in, non_blocking=True)
+            solver = None
+            extra = 0
+            if req.kind == 'poisson':
+                solver, extra = self._take_solver(req)
+                self.resident += extra      # the new solver stays resident
+                y.zero_()
+                solver.solve_neutral_async(y, x)
+            else:
+                self._op(req.N).apply(x, y)
+            out = host_out
+            out.copy_(y, non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(st)
+        return {'req': req, 'slot': slot, 'event': ev, 'solver': solver,
+                'out': out, 'keep': (x, y), 'extra': extra}
+
+    def _finish(self, job, now):
+        req = job['req']
+        req.done = now
+        req.result = job['out'].numpy().copy()
+        if job['solver'] is not None:
+            req.niter = job['solver'].result()
+            self.pools[('poisson', req.N)].append(job['solver'])
+        self.in_use -= self.request_bytes(req)
+        self.free_slots.append(job['slot'])
+
+    # -- the loop --------------------------------------------------------------
+    def run(self, requests, inputs=None):
+        """Serve `requests` in arrival order; returns them with start/done
+        times (seconds after the run began) and results."""
+        reqs = sorted(requests, key=lambda r: r.arrival)
+        if inputs is None:
+            inputs = {r.rid: self.host_input(r) for r in reqs}
+        outputs = {r.rid: torch.empty(tuple(inputs[r.rid].shape),
+                                      dtype=torch.float64).pin_memory()
+                   for r in reqs}
+        pending = collections.deque(reqs)
+        active = []
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        while pending or active:
+            now = time.perf_counter() - t0
+            progressed = False
+            for job in list(active):
+                if job['event'].query():
+                    active.remove(job)
+                    self._finish(job, time.perf_counter() - t0)
+                    progressed = True
+            while pending and pending[0].arrival <= now and self.free_slots:
+                req = pending[0]
+                need = self.request_bytes(req)
+                if not self.pools[('poisson', req.N)] and \
+                        req.kind == 'poisson':
+                    need += self.solver_bytes(req.N)
+                if self.resident + self.in_use + need > self.budget and \
+                        active:
+                    break      # wait for memory to free up
+                pending.popleft()
+                slot = self.free_slots.pop()
+                self.in_use += self.request_bytes(req)
+                req.start = time.perf_counter() - t0
+                active.append(self._launch(req, inputs[req.rid],
+                                           outputs[req.rid], slot))
+                progressed = True
+            if not progressed:
+                time.sleep(20e-6)
+        return reqs
+
+
+def latency_stats(reqs):
+    lat = np.array([r.done - r.arrival for r in reqs])
+    span = max(r.done for r in reqs) - min(r.arrival for r in reqs)
+    return {'requests': len(reqs), 'throughput_per_s': len(reqs) / span,
+            'p50_ms': float(np.percentile(lat, 50) * 1e3),
+            'p99_ms': float(np.percentile(lat, 99) * 1e3),
+            'mean_ms': float(lat.mean() * 1e3)}

@@ -57,3 +57,39 @@ def eps_for_relative_residual(rho, gd, rel=1e-10):
     """The reference stops when sum(r^2) dv <= eps (gpaw/poisson.py:485,
     527-537); this eps corresponds to ||L phi - rho|| / ||rho|| = rel."""
     return (rel * float(np.sqrt((rho * rho).sum())))**2 * gd.dv
+
+
+def gaussian_density_device(gd, centers, widths, charges):
+    """gaussian_density evaluated on the GPU (torch, float64)."""
+    import torch
+    dev = gd.device
+    idx = [torch.arange(int(n), dtype=torch.float64, device=dev) + int(b)
+           for n, b in zip(gd.n_c, gd.beg_c)]
+    h = torch.tensor(np.diag(gd.h_cv), dtype=torch.float64, device=dev)
+    x = (idx[0] * h[0])[:, None, None]
+    y = (idx[1] * h[1])[None, :, None]
+    z = (idx[2] * h[2])[None, None, :]
+    rho = torch.zeros(tuple(int(n) for n in gd.n_c), dtype=torch.float64,
+                      device=dev)
+    for c, w, q in zip(centers, widths, charges):
+        d2 = (x - c[0])**2 + (y - c[1])**2 + (z - c[2])**2
+        rho += q * (np.pi * w * w)**-1.5 * torch.exp(-d2 / (w * w))
+    return rho
+
+
+def random_gaussians(gd, ngauss, rng):
+    """C3 distributions: widths U[0.5, 1.2] A, charges +-U[0.5, 2], centres
+    uniform in [0.2, 0.8] of the (orthorhombic) box."""
+    L = np.diag(gd.cell_cv)
+    centers = [rng.uniform(0.2, 0.8, 3) * L for _ in range(ngauss)]
+    widths = rng.uniform(0.5, 1.2, ngauss) / BOHR
+    charges = rng.uniform(0.5, 2.0, ngauss) * rng.choice([-1.0, 1.0], ngauss)
+    return centers, widths, charges
+
+
+def neutral_density_device(gd, ngauss, seed):
+    """Seeded neutral density on the GPU (mean removed as the neutral
+    branch does, charge / dv / number of points)."""
+    rng = np.random.default_rng(seed)
+    rho = gaussian_density_device(gd, *random_gaussians(gd, ngauss, rng))
+    return rho - rho.sum() / rho.numel()

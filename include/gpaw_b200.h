@@ -214,6 +214,20 @@ GB_API void gb_mixed_free(gb_mixed* m);
 GB_API int gb_mixed_solve(gb_mixed* m, double* phi, const double* rho, double tol, int maxiter,
                           int* niter, double* rel_residual, void* stream);
 
+/* Asynchronous forms (no counterpart in the reference): enqueue the whole
+ * solve on `stream` and return at once; after the stream (or an event
+ * recorded after the call) completes, *_result reports the V-cycle count and
+ * the final error / relative residual, and GB_ENOCONV if the solve stopped
+ * at maxiter.  A solver object serves one solve at a time: enqueue the next
+ * solve on the same object only after the previous one's result was read or
+ * on the same stream. */
+GB_API int gb_poisson_solve_neutral_async(gb_poisson* p, double* phi, const double* rho,
+                                          double eps, int maxiter, void* stream);
+GB_API int gb_poisson_result(gb_poisson* p, int* niter, double* error);
+GB_API int gb_mixed_solve_async(gb_mixed* m, double* phi, const double* rho, double tol,
+                                int maxiter, void* stream);
+GB_API int gb_mixed_result(gb_mixed* m, int* niter, double* rel_residual);
+
 #ifdef __cplusplus
 }
 #endif

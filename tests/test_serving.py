@@ -1,0 +1,52 @@
+"""Serving loop: request generation (CPU) and, on the GPU, continuous
+batching with every result equal to the same request served alone."""
+import numpy as np
+import pytest
+
+from gpaw_b200.serving import Request, latency_stats, make_requests
+
+
+def test_request_stream_properties():
+    reqs = make_requests(rate=500.0, count=400, seed=3)
+    sides = np.array([r.N[0] for r in reqs])
+    assert ((sides % 8) == 0).all()
+    assert sides.min() >= 24 and sides.max() <= 160
+    t = np.array([r.arrival for r in reqs])
+    assert (np.diff(t) > 0).all()
+    # mean inter-arrival close to 1 / rate
+    assert abs(np.diff(t).mean() * 500.0 - 1.0) < 0.15
+    kinds = {r.kind for r in reqs}
+    assert kinds == {'poisson', 'apply'}
+    # log-uniform: more small grids than large ones
+    assert (sides <= 64).sum() > (sides >= 112).sum()
+
+
+def test_latency_stats():
+    reqs = [Request(i, 'apply', (8, 8, 8), arrival=0.1 * i) for i in range(10)]
+    for r in reqs:
+        r.done = r.arrival + 0.01 * (r.rid + 1)
+    s = latency_stats(reqs)
+    assert s['requests'] == 10
+    assert abs(s['p50_ms'] - 55.0) < 1e-6
+    assert s['p99_ms'] > 99.0
+
+
+@pytest.mark.gpu
+def test_mixed_equals_alone(cuda):
+    from gpaw_b200.serving import Server
+    reqs = make_requests(rate=5000.0, count=24, seed=5, smin=24, smax=64)
+    srv = Server(hbm_budget=2 << 30, nslots=6)
+    srv.warm(sorted({r.N for r in reqs}))
+    inputs = {r.rid: srv.host_input(r) for r in reqs}
+    mixed = {r.rid: r.result for r in srv.run(reqs, inputs)}
+    # the same requests one at a time
+    alone = {}
+    for r in reqs:
+        one = Request(r.rid, r.kind, r.N, 0.0, r.seed)
+        alone[r.rid] = srv.run([one], {r.rid: inputs[r.rid]})[0]
+    for r in reqs:
+        assert np.array_equal(mixed[r.rid], alone[r.rid].result), r
+        if r.kind == 'poisson':
+            assert alone[r.rid].niter > 0
+    stats = latency_stats(reqs)
+    assert stats['requests'] == 24
