@@ -103,21 +103,25 @@ class Server:
         ps.set_grid_descriptor(self._gd(req.N))
         return ps, self.solver_bytes(req.N)
 
-    def warm(self, shapes):
-        """Build one resident solver and operator per shape ahead of time."""
+    def warm(self, shapes, per_shape=2):
+        """Build `per_shape` resident solvers (graphs captured) and one
+        operator per shape ahead of time."""
         for N in shapes:
-            req = Request(-1, 'poisson', N, 0.0)
-            ps, nb = self._take_solver(req)
-            self.resident += nb
-            phi = ps.gd.zeros()
-            rho = ps.gd.zeros()
-            rho[0, 0, 0] = 1.0
-            rho -= rho.mean()
-            try:
-                ps.solve_neutral(phi, rho)
-            except RuntimeError:
-                pass
-            self.pools[('poisson', N)].append(ps)
+            built = []
+            for _ in range(per_shape):
+                req = Request(-1, 'poisson', N, 0.0)
+                ps, nb = self._take_solver(req)
+                self.resident += nb
+                phi = ps.gd.zeros()
+                rho = ps.gd.zeros()
+                rho[0, 0, 0] = 1.0
+                rho -= rho.mean()
+                try:
+                    ps.solve_neutral(phi, rho)
+                except RuntimeError:
+                    pass
+                built.append(ps)
+            self.pools[('poisson', N)].extend(built)
             self._op(N)
         torch.cuda.synchronize()
 
