@@ -276,6 +276,30 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
 
     const int nplanes = pb - pa;
     const int total = nplanes + NN;
+    // Epilogue operands (aux, aux2, FP64 accumulator) of the centre plane,
+    // loaded one iteration ahead so that their latency overlaps the stencil
+    // work instead of stalling every plane.
+    constexpr bool NEED_AUX = MODE != EPI_APPLY;
+    T pa1[RY], pa2[RY];
+    double pac[RY];
+    auto prefetch = [&](int p) {
+#pragma unroll
+        for (int r = 0; r < RY; r++) {
+            const int gy = y0 + ty0 + r;
+            pa1[r] = Num<T>::zero();
+            pa2[r] = Num<T>::zero();
+            pac[r] = 0.0;
+            if (p < pb && gx < n2 && gy < n1) {
+                const long long at = ((long long)p * n1 + gy) * n2 + gx;
+                if (NEED_AUX && ep.aux) pa1[r] = aux[at];
+                if constexpr (MODE == EPI_LIN) {
+                    if (ep.aux2) pa2[r] = aux2[at];
+                    if (ep.acc64) pac[r] = ep.acc64[b * ng + at];
+                }
+            }
+        }
+    };
+    if (NEED_AUX) prefetch(pa);
     // Iteration t pushes relative plane t into queue slot t % Q and, for
     // t >= NN, computes centre plane t - NN.  The loop is unrolled by Q so
     // that every slot index is a compile-time constant (no register moves).
@@ -334,27 +358,30 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
                     if (MODE == EPI_APPLY) {
                         o[at] = x;
                     } else if (MODE == EPI_RESID) {
-                        const T res = Num<T>::sub(x, aux[at]);
+                        const T res = Num<T>::sub(x, pa1[r]);
                         if (out) o[at] = res;
                         sq += sqnorm(res);
                     } else if (MODE == EPI_JACOBI) {
-                        o[at] = jacobi_update<T>(vc, aux[at], x, ep.w, cs.c0);
+                        o[at] = jacobi_update<T>(vc, pa1[r], x, ep.w, cs.c0);
                     } else if (MODE == EPI_LIN) {
                         if constexpr (sizeof(T) != 16) {
                             T y = (T)ep.p1 * vc + (T)ep.p2 * x;
-                            if (ep.aux) y += (T)ep.p0 * aux[at];
-                            if (ep.aux2) y += (T)ep.p3 * aux2[at];
+                            if (ep.aux) y += (T)ep.p0 * pa1[r];
+                            if (ep.aux2) y += (T)ep.p3 * pa2[r];
                             if (ep.partial) sq += (double)y * (double)y;
-                            if (ep.acc64) ep.acc64[b * ng + at] += (double)y;
+                            if (ep.acc64) ep.acc64[b * ng + at] = pac[r] + (double)y;
                             else if (ep.out32) ep.out32[b * ng + at] = (float)y;
                             else o[at] = y;
                         }
                     } else {
-                        const T y = Num<T>::sub(vc, Num<T>::scale(Num<T>::sub(x, aux[at]), ep.sc));
+                        const T y = Num<T>::sub(vc, Num<T>::scale(Num<T>::sub(x, pa1[r]), ep.sc));
                         o[at] = ep.negate ? Num<T>::neg(y) : y;
                     }
                 }
             }
+            // operands of the next centre plane: in flight while the next
+            // iteration waits for its plane and computes the stencil
+            if (NEED_AUX) prefetch(p + 1);
         }
     };
 #pragma unroll 1
@@ -410,12 +437,15 @@ static int launch_cfd_nn(const void* in, void* out, int nin, const GridBC& g, co
     // only the direction order GUCLaplace builds (axis 2, 1, 0); other
     // axis-aligned stencils take the generic kernel
     if (!(cs.axis[0] == 2 && cs.axis[1] == 1 && cs.axis[2] == 0)) return -1;
+    // rows per thread: fewer when the epilogue reads other arrays (their
+    // prefetched values need registers too)
+    constexpr bool AUX = MODE != EPI_APPLY;
     if constexpr (sizeof(T) == 16) {
         constexpr int D = NN <= 3 ? 3 : 2;
-        constexpr int RY = NN <= 3 ? 2 : 1;
+        constexpr int RY = (NN <= 3 && !AUX) ? 2 : 1;
         return launch_cfd_t<T, NN, 32, 16, RY, D, MODE, 1>(in, out, nin, g, P, cs, ep, st, nblk);
     } else {
-        constexpr int RY = NN <= 3 ? 4 : 2;
+        constexpr int RY = (NN <= 3 && !AUX) ? 4 : 2;
         return launch_cfd_t<T, NN, 32, 16, RY, 4, MODE, 1>(in, out, nin, g, P, cs, ep, st, nblk);
     }
 }
