@@ -384,6 +384,7 @@ def run_gpu(args):
     import torch.distributed as dist
 
     from gpaw_b200 import GridDescriptor, Laplace, Transformer
+    from gpaw_b200.replicas import max_over_ranks
 
     world = int(os.environ.get('WORLD_SIZE', '1'))
     rank = int(os.environ.get('RANK', '0'))
@@ -451,9 +452,7 @@ def run_gpu(args):
     rst_s = [e[1].elapsed_time(e[2]) / 1e3 for e in evs]
     itp_s = [e[2].elapsed_time(e[3]) / 1e3 for e in evs]
     if world > 1:
-        t = torch.tensor([elapsed], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
+        elapsed = max_over_ranks(elapsed, device=dev)
 
     ab, rb, ib = algorithmic_bytes()
     per_step = ab + rb + ib
@@ -486,9 +485,7 @@ def run_gpu(args):
         barrier()
         et = e0.elapsed_time(e1) / 1e3
         if world > 1:
-            t = torch.tensor([et], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            et = float(t.item())
+            et = max_over_ranks(et, device=dev)
         e2e = {'value': world * per_step * e_steps / et / 1e9, 'unit': 'GB/s',
                'h2d_bytes_per_step': int(x.numel() * 16),
                'd2h_bytes_per_step': int((y.numel() + c.numel() +
