@@ -47,6 +47,15 @@ int cfd_chunk(const GridBC& g, int nn, int nin) {
     return chunk0;
 }
 
+// GPAW_B200_FMA=1 selects the fused-multiply-add form of the complex
+// nn = 3 apply: not bit-identical to the reference (each product is no
+// longer rounded before its sum), within a few ulp per point.  Read at
+// every launch so it can be switched on and off inside one process.
+bool fused_apply() {
+    const char* e = getenv("GPAW_B200_FMA");
+    return e != nullptr && atoi(e) != 0;
+}
+
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
     return (unsigned)__cvta_generic_to_shared(p);
 }
@@ -88,6 +97,22 @@ __device__ __forceinline__ float jacobi_update<float>(float b, float src, float 
     return (1.0f - (float)w) * b + (float)w * (src - x) / (float)c0;
 }
 
+// x + v c with one rounding (fused multiply-add): the opt-in fast form.
+template <class T>
+__device__ __forceinline__ T fma_fused(T x, T v, double c);
+template <>
+__device__ __forceinline__ double fma_fused<double>(double x, double v, double c) {
+    return __fma_rn(v, c, x);
+}
+template <>
+__device__ __forceinline__ double2 fma_fused<double2>(double2 x, double2 v, double c) {
+    return make_double2(__fma_rn(v.x, c, x.x), __fma_rn(v.y, c, x.y));
+}
+template <>
+__device__ __forceinline__ float fma_fused<float>(float x, float v, double c) {
+    return __fmaf_rn(v, (float)c, x);
+}
+
 template <class T>
 __device__ __forceinline__ T fma_exact(T x, T v, double c) {
     return Num<T>::add(x, Num<T>::scale(v, c));
@@ -115,17 +140,21 @@ __device__ __forceinline__ void static_for(F&& f) {
 
 // Sum of one direction's 2*NN terms in the caller's order: +1..+NN then
 // -1..-NN.  `vp(d)` / `vm(d)` return the values at +d / -d.
-template <class T, int NN, class VP, class VM>
+template <class T, int NN, bool FUSED, class VP, class VM>
 __device__ __forceinline__ T add_direction(T x, const double* cp, const double* cm, VP vp, VM vm) {
 #pragma unroll
-    for (int d = 1; d <= NN; d++) x = fma_exact<T>(x, vp(d), cp[d - 1]);
+    for (int d = 1; d <= NN; d++)
+        x = FUSED ? fma_fused<T>(x, vp(d), cp[d - 1]) : fma_exact<T>(x, vp(d), cp[d - 1]);
 #pragma unroll
-    for (int d = 1; d <= NN; d++) x = fma_exact<T>(x, vm(d), cm[d - 1]);
+    for (int d = 1; d <= NN; d++)
+        x = FUSED ? fma_fused<T>(x, vm(d), cm[d - 1]) : fma_exact<T>(x, vm(d), cm[d - 1]);
     return x;
 }
 
 // Directions are summed in the order GUCLaplace builds for an orthorhombic
-// cell: axis 2, axis 1, axis 0 (ORD = 1, the only instantiation).
+// cell: axis 2, axis 1, axis 0.  ORD = 1: every product and sum rounded on
+// its own (bit-identical to the reference); ORD = 2: fused multiply-adds
+// (fewer instructions, results within a few ulp; opt-in, apply only).
 // 128 registers a thread: two resident CTAs of 256 threads (complex) or
 // four of 128 (real) when the tile holds two or four rows per thread.
 template <class T, int NN, int TX, int TY, int RY, int D, int MODE, int ORD>
@@ -343,13 +372,13 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
                 T x = Num<T>::zero();
                 if (MODE != EPI_JACOBI) x = Num<T>::add(x, Num<T>::scale(vc, cs.c0));
                 // directions: axis 2, axis 1, axis 0 (GUCLaplace's order)
-                x = add_direction<T, NN>(x, cs.cp[0], cs.cm[0],
+                x = add_direction<T, NN, ORD == 2>(x, cs.cp[0], cs.cm[0],
                                          [&](int d) { return row[d]; },
                                          [&](int d) { return row[-d]; });
-                x = add_direction<T, NN>(x, cs.cp[1], cs.cm[1],
+                x = add_direction<T, NN, ORD == 2>(x, cs.cp[1], cs.cm[1],
                                          [&](int d) { return colp[(r + NN + d) * PX]; },
                                          [&](int d) { return colp[(r + NN - d) * PX]; });
-                x = add_direction<T, NN>(x, cs.cp[2], cs.cm[2],
+                x = add_direction<T, NN, ORD == 2>(x, cs.cp[2], cs.cm[2],
                                          [&](int d) { return q[r][(CU + d) % Q]; },
                                          [&](int d) { return q[r][(CU + Q - d) % Q]; });
                 const int gy = y0 + ty0 + r;
@@ -443,6 +472,10 @@ static int launch_cfd_nn(const void* in, void* out, int nin, const GridBC& g, co
     if constexpr (sizeof(T) == 16) {
         constexpr int D = NN <= 3 ? 3 : 2;
         constexpr int RY = (NN <= 3 && !AUX) ? 2 : 1;
+        if constexpr (MODE == EPI_APPLY && NN == 3)
+            if (fused_apply())
+                return launch_cfd_t<T, NN, 32, 16, RY, D, MODE, 2>(in, out, nin, g, P, cs, ep,
+                                                                    st, nblk);
         return launch_cfd_t<T, NN, 32, 16, RY, D, MODE, 1>(in, out, nin, g, P, cs, ep, st, nblk);
     } else {
         constexpr int RY = (NN <= 3 && !AUX) ? 4 : 2;

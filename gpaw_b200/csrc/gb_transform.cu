@@ -28,9 +28,11 @@ namespace gb {
 // c/bmgs/restrict.cpp:18-60), applied along axis 2, then 1, then 0.
 //
 // Fine padded planes stream through a ring of S shared-memory stages filled
-// by cp.async D planes ahead.  Each stage stores the tile's footprint with
-// even and odd columns in separate arrays, so that the axis-2 pass (centre
-// at an odd column, taps at even columns) reads consecutive words.
+// by cp.async D planes ahead.  A stage holds the tile's footprint row-major,
+// element i stored at i ^ ((i >> LB) & 1) with 2^LB elements per 128-byte
+// line: the copy keeps consecutive lanes on consecutive global and shared
+// addresses (so the copies coalesce into full L2 requests), and the axis-2
+// pass, whose lanes read every second column, hits 32 distinct banks.
 
 __device__ __forceinline__ unsigned smem_u32x(const void* p) {
     return (unsigned)__cvta_generic_to_shared(p);
@@ -81,16 +83,16 @@ k_restrict(const T* __restrict__ in, T* __restrict__ out, T* __restrict__ out2, 
     constexpr int H = 2 * K - 3;
     constexpr int FY = 2 * TJ + H;        // fine rows needed by the tile
     constexpr int FZ = 2 * TK + H;        // fine columns needed by the tile
-    constexpr int FZE = (FZ + 1) / 2, FZO = FZ / 2;
-    constexpr int SE = FY * FZE, SO = FY * FZO;
-    constexpr int SS = SE + SO;           // one stage (elements)
+    constexpr int SS = (FY * FZ + 1) & ~1; // one stage (even: swz maps [0, SS) onto itself)
+    constexpr int LB = sizeof(T) == 16 ? 3 : (sizeof(T) == 8 ? 4 : 5);
+    auto swz = [](int i) { return i ^ ((i >> LB) & 1); };
     constexpr int S = D + 1;              // ring depth
     constexpr int NR = 2 * K - 1;         // axis-0 ring depth
     constexpr int NC = (FY * FZ + NT - 1) / NT;
     constexpr int EB = (int)sizeof(T);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* stage = reinterpret_cast<T*>(smem_raw);
-    T* R1 = stage + S * SS;               // [FY][TK]
+    T* R1 = stage + S * SS;               // [2][FY][TK]
 
     const int tiles2 = (G.nout[2] + TK - 1) / TK;
     const int J0 = (blockIdx.x / tiles2) * TJ;
@@ -119,7 +121,7 @@ k_restrict(const T* __restrict__ in, T* __restrict__ out, T* __restrict__ out2, 
         goff[i] = 0;
         if (e >= FY * FZ) continue;
         const int y = e / FZ, z = e % FZ;
-        soff[i] = (z & 1) ? SE + y * FZO + (z >> 1) : y * FZE + (z >> 1);
+        soff[i] = swz(e);
         const int py = 2 * J0 + y, pz = 2 * L0 + z;
         if (py >= G.s[1] || pz >= G.s[2]) continue;
         int iy = py - G.plo[1], iz = pz - G.plo[2];
@@ -173,65 +175,87 @@ k_restrict(const T* __restrict__ in, T* __restrict__ out, T* __restrict__ out2, 
 #pragma unroll
     for (int i = 0; i < NR; i++) ring[i] = Num<T>::zero();
 
-#pragma unroll 1
-    for (int j = 0; j < D; j++) {
-        if (j < nx) issue(j);
-        cp_commit_x();
-    }
-#pragma unroll 1
-    for (int t = 0; t < nx; t++) {
-        cp_wait_x<D - 1>();
-        fixup(t);
-        __syncthreads();   // stage t visible; R1 free; slot (t+D)%S free
-        if (t + D < nx) issue(t + D);
-        cp_commit_x();
-        const T* Fe = stage + (t % S) * SS;
-        const T* Fo = Fe + SE;
-        // axis-2 pass: R1[y][k], centre at odd column K-1+2k
-        for (int e = tid; e < FY * TK; e += NT) {
-            const int y = e / TK, k = e % TK;
-            const T* re = Fe + y * FZE;
-            T x = Fo[y * FZO + K / 2 - 1 + k];
+    // axis-2 pass of plane t: R1[t & 1][y][k], centre at odd column K-1+2k
+    auto axis2 = [&](int t) {
+        const T* F = stage + (t % S) * SS;
+        T* R = R1 + (t & 1) * (FY * TK);
+        constexpr int NE = FY * TK;
 #pragma unroll
-            for (int l = 0; l < K / 2; l++)
-                x = Num<T>::add(x, Num<T>::scale(Num<T>::add(re[K / 2 + k + l], re[K / 2 - 1 + k - l]),
-                                                 G.w[l]));
-            // restrict(-a) == -restrict(a) bit for bit (every step is odd)
-            const T r = Num<T>::scale(x, 0.5);
-            R1[y * TK + k] = G.neg_in ? Num<T>::neg(r) : r;
+        for (int r = 0; r < (NE + NT - 1) / NT; r++) {
+            const int e = tid + r * NT;
+            if (NE % NT == 0 || e < NE) {
+                const int y = e / TK, k = e % TK;
+                const int c = y * FZ + K - 1 + 2 * k;
+                T x = F[swz(c)];
+#pragma unroll
+                for (int l = 0; l < K / 2; l++)
+                    x = Num<T>::add(x, Num<T>::scale(Num<T>::add(F[swz(c + 2 * l + 1)],
+                                                                 F[swz(c - 2 * l - 1)]),
+                                                     G.w[l]));
+                // restrict(-a) == -restrict(a) bit for bit (every step is odd)
+                const T v = Num<T>::scale(x, 0.5);
+                R[y * TK + k] = G.neg_in ? Num<T>::neg(v) : v;
+            }
         }
-        __syncthreads();
-        // axis-1 pass for this thread's (j, k), pushed into the axis-0 ring
-        {
-            const int c = K - 1 + 2 * tj;
-            T x = R1[c * TK + tk];
+    };
+    // axis-1 pass of plane t for this thread's (j, k), into the axis-0 ring;
+    // the axis-0 pass once the ring spans planes 2I .. 2I + 2K - 2
+    auto axis10 = [&](int t) {
+        const T* R = R1 + (t & 1) * (FY * TK);
+        const int c = K - 1 + 2 * tj;
+        T x = R[c * TK + tk];
 #pragma unroll
-            for (int l = 0; l < K / 2; l++)
-                x = Num<T>::add(x, Num<T>::scale(Num<T>::add(R1[(c + 2 * l + 1) * TK + tk],
-                                                             R1[(c - 2 * l - 1) * TK + tk]),
-                                                 G.w[l]));
+        for (int l = 0; l < K / 2; l++)
+            x = Num<T>::add(x, Num<T>::scale(Num<T>::add(R[(c + 2 * l + 1) * TK + tk],
+                                                         R[(c - 2 * l - 1) * TK + tk]),
+                                             G.w[l]));
 #pragma unroll
-            for (int i = 0; i < NR - 1; i++) ring[i] = ring[i + 1];
-            ring[NR - 1] = Num<T>::scale(x, 0.5);
-        }
-        // axis-0 pass once the ring spans planes 2I .. 2I + 2K - 2
+        for (int i = 0; i < NR - 1; i++) ring[i] = ring[i + 1];
+        ring[NR - 1] = Num<T>::scale(x, 0.5);
         if (t >= 2 * K - 2 && ((t - (2 * K - 2)) & 1) == 0) {
             const int I = I0 + (t - (2 * K - 2)) / 2;
             const int J = J0 + tj, L = L0 + tk;
-            T x = ring[K - 1];
+            T y = ring[K - 1];
 #pragma unroll
             for (int l = 0; l < K / 2; l++)
-                x = Num<T>::add(x, Num<T>::scale(Num<T>::add(ring[K - 1 + 2 * l + 1],
+                y = Num<T>::add(y, Num<T>::scale(Num<T>::add(ring[K - 1 + 2 * l + 1],
                                                              ring[K - 1 - 2 * l - 1]),
                                                  G.w[l]));
             if (J < G.nout[1] && L < G.nout[2]) {
                 const long long at = ((long long)I * G.nout[1] + J) * G.nout[2] + L;
-                const T r = Num<T>::scale(x, 0.5);
+                const T r = Num<T>::scale(y, 0.5);
                 o[at] = r;
                 // fd_precond's "d = 4 * step * r" (c/fd_preconditioner.cpp:222-226)
                 if (out2) out2[b * ngout + at] = Num<T>::scale(r, G.scale2);
             }
         }
+    };
+
+    // One barrier per plane: after barrier t, stage t+1 and R1[t & 1] are
+    // visible, so the axis-2 pass of plane t+1 (into the other R1 buffer)
+    // and the axis-1/axis-0 passes of plane t run in the same interval.
+    // R1[(t+1) & 1] was last read by the axis-1 pass of plane t-1 and stage
+    // slot t % S by the axis-2 pass of plane t, both before barrier t.
+#pragma unroll 1
+    for (int j = 0; j < D; j++) {
+        if (j < nx) issue(j);
+        cp_commit_x();
+    }
+    cp_wait_x<D - 1>();
+    fixup(0);
+    __syncthreads();
+    if (D < nx) issue(D);
+    cp_commit_x();
+    axis2(0);
+#pragma unroll 1
+    for (int t = 0; t < nx; t++) {
+        cp_wait_x<D - 1>();
+        if (t + 1 < nx) fixup(t + 1);
+        __syncthreads();
+        if (t + 1 + D < nx) issue(t + 1 + D);
+        cp_commit_x();
+        if (t + 1 < nx) axis2(t + 1);
+        axis10(t);
     }
     cp_wait_x<0>();
 }
@@ -422,8 +446,8 @@ static int launch_restrict_k(const void* in, void* out, void* out2, int nin, con
     constexpr int TJ = 256 / TK;
     constexpr int D = sizeof(T) == 16 ? 2 : 3;
     constexpr int H = 2 * K - 3, FY = 2 * TJ + H, FZ = 2 * TK + H;
-    constexpr int SS = FY * ((FZ + 1) / 2) + FY * (FZ / 2);
-    constexpr size_t smem = ((size_t)(D + 1) * SS + (size_t)FY * TK) * sizeof(T);
+    constexpr int SS = (FY * FZ + 1) & ~1;
+    constexpr size_t smem = ((size_t)(D + 1) * SS + (size_t)2 * FY * TK) * sizeof(T);
     static bool attr = false;
     if (!attr) {
         if (cudaFuncSetAttribute(k_restrict<T, K, TJ, TK, D>,

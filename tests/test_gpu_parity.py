@@ -380,3 +380,31 @@ def test_tiled_and_generic_paths_agree(nn, dtype, cuda, monkeypatch):
                 op.relax(2, g, to_dev(rho[0]), 3, 0.7)
                 f[path] = to_np(g)
             assert np.array_equal(f['generic'], f['tiled'])
+
+
+def test_fused_apply_opt_in(cuda, monkeypatch):
+    """GPAW_B200_FMA=1 switches the complex nn = 3 apply to fused
+    multiply-adds: within 1e-12 relative of the reference, and the default
+    (switch off) stays bit-identical."""
+    from gpaw_b200 import Laplace
+    rng = np.random.default_rng(77)
+    N, pbc = (40, 36, 44), (1, 1, 1)
+    cell = (6.0, 5.4, 6.6)
+    gref = L.GridDescriptor(N, cell, pbc)
+    want_op = L.Laplace(gref, -0.5, 3, complex)
+    gd = prod_gd(N, cell, pbc)
+    op = Laplace(gd, -0.5, 3, complex)
+    a = rng.standard_normal((2,) + tuple(gd.n_c)) + \
+        1j * rng.standard_normal((2,) + tuple(gd.n_c))
+    ph = gref.phase_factor_cd(KPT)
+    want = np.zeros_like(a)
+    want_op.apply(a, want, ph)
+    x = to_dev(a)
+    for fma in ('1', '0'):
+        monkeypatch.setenv('GPAW_B200_FMA', fma)
+        y = x.new_zeros(x.shape)
+        op.apply(x, y, gd.phase_factor_cd(KPT))
+        got = to_np(y)
+        assert max_rel(got, want) <= RTOL_FP64
+        if fma == '0':
+            assert np.array_equal(got, want)
