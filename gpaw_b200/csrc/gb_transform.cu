@@ -20,19 +20,18 @@
 
 namespace gb {
 
-
-
 // ----------------------------------------------------------------- restrict
 // out[I][J][L] over padded input a:  per axis, r(c) = 0.5 * (a[c] + sum_l
 // w_l * (a[c + 2l + 1] + a[c - 2l - 1])) at c = K - 1 + 2 I  (RST1D,
 // c/bmgs/restrict.cpp:18-60), applied along axis 2, then 1, then 0.
 //
 // Fine padded planes stream through a ring of S shared-memory stages filled
-// by cp.async D planes ahead.  A stage holds the tile's footprint row-major,
-// element i stored at i ^ ((i >> LB) & 1) with 2^LB elements per 128-byte
-// line: the copy keeps consecutive lanes on consecutive global and shared
-// addresses (so the copies coalesce into full L2 requests), and the axis-2
-// pass, whose lanes read every second column, hits 32 distinct banks.
+// by cp.async D planes ahead.  A stage holds the tile's footprint row-major
+// with an odd row pitch, so consecutive lanes copy consecutive global and
+// shared addresses (full L2 requests).  The axis-2 pass, whose outputs read
+// every second column, gives each bank phase of a warp half its lanes on
+// one row and half on the next: the odd pitch puts the two halves on
+// disjoint banks, and every read is the thread's base plus a constant.
 
 __device__ __forceinline__ unsigned smem_u32x(const void* p) {
     return (unsigned)__cvta_generic_to_shared(p);
@@ -83,16 +82,19 @@ k_restrict(const T* __restrict__ in, T* __restrict__ out, T* __restrict__ out2, 
     constexpr int H = 2 * K - 3;
     constexpr int FY = 2 * TJ + H;        // fine rows needed by the tile
     constexpr int FZ = 2 * TK + H;        // fine columns needed by the tile
-    constexpr int SS = (FY * FZ + 1) & ~1; // one stage (even: swz maps [0, SS) onto itself)
-    constexpr int LB = sizeof(T) == 16 ? 3 : (sizeof(T) == 8 ? 4 : 5);
-    auto swz = [](int i) { return i ^ ((i >> LB) & 1); };
+    constexpr int SS = FY * FZ;           // one stage (elements); FZ is odd
+    // lanes of one shared-memory bank phase (16-byte words: 8, 8-byte: 16,
+    // 4-byte: 32) and the R1 pitch that keeps a phase's two rows apart
+    constexpr int PG = sizeof(T) == 16 ? 8 : (sizeof(T) == 8 ? 16 : 32);
+    constexpr int HG = PG / 2;
+    constexpr int RP = TK + HG;
     constexpr int S = D + 1;              // ring depth
     constexpr int NR = 2 * K - 1;         // axis-0 ring depth
     constexpr int NC = (FY * FZ + NT - 1) / NT;
     constexpr int EB = (int)sizeof(T);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* stage = reinterpret_cast<T*>(smem_raw);
-    T* R1 = stage + S * SS;               // [2][FY][TK]
+    T* R1 = stage + S * SS;               // [2][FY][RP]
 
     const int tiles2 = (G.nout[2] + TK - 1) / TK;
     const int J0 = (blockIdx.x / tiles2) * TJ;
@@ -121,7 +123,7 @@ k_restrict(const T* __restrict__ in, T* __restrict__ out, T* __restrict__ out2, 
         goff[i] = 0;
         if (e >= FY * FZ) continue;
         const int y = e / FZ, z = e % FZ;
-        soff[i] = swz(e);
+        soff[i] = e;
         const int py = 2 * J0 + y, pz = 2 * L0 + z;
         if (py >= G.s[1] || pz >= G.s[2]) continue;
         int iy = py - G.plo[1], iz = pz - G.plo[2];
@@ -158,10 +160,10 @@ k_restrict(const T* __restrict__ in, T* __restrict__ out, T* __restrict__ out2, 
     auto fixup = [&](int j) {
         int ip, ws;
         plane_info(j, ip, ws);
+        T* st = stage + (j % S) * SS;
         const bool pw = cplx && ws >= 0 && G.g.periodic[0];
         if (!pw && !pcode) return;
         const double2 ph0 = ws == 0 ? P.ph[0][0] : P.ph[0][1];
-        T* st = stage + (j % S) * SS;
 #pragma unroll
         for (int i = 0; i < NC; i++) {
             if (tid + i * NT >= FY * FZ) break;
@@ -175,39 +177,41 @@ k_restrict(const T* __restrict__ in, T* __restrict__ out, T* __restrict__ out2, 
 #pragma unroll
     for (int i = 0; i < NR; i++) ring[i] = Num<T>::zero();
 
-    // axis-2 pass of plane t: R1[t & 1][y][k], centre at odd column K-1+2k
+    // axis-2 pass of plane t: R1[t & 1][y][k], centre at odd column K-1+2k.
+    // Items come in blocks of two rows x TK columns; within a block, a bank
+    // phase takes HG consecutive columns of both rows.
     auto axis2 = [&](int t) {
         const T* F = stage + (t % S) * SS;
-        T* R = R1 + (t & 1) * (FY * TK);
-        constexpr int NE = FY * TK;
+        T* R = R1 + (t & 1) * (FY * RP);
+        constexpr int NE = ((FY + 1) / 2) * 2 * TK;
 #pragma unroll
         for (int r = 0; r < (NE + NT - 1) / NT; r++) {
             const int e = tid + r * NT;
-            if (NE % NT == 0 || e < NE) {
-                const int y = e / TK, k = e % TK;
-                const int c = y * FZ + K - 1 + 2 * k;
-                T x = F[swz(c)];
+            const int j = e % (2 * TK);
+            const int k = (j / PG) * HG + j % HG;
+            const int y = 2 * (e / (2 * TK)) + (j / HG) % 2;
+            if ((NE % NT == 0 || e < NE) && y < FY) {
+                const T* f = F + y * FZ + K - 1 + 2 * k;
+                T x = f[0];
 #pragma unroll
                 for (int l = 0; l < K / 2; l++)
-                    x = Num<T>::add(x, Num<T>::scale(Num<T>::add(F[swz(c + 2 * l + 1)],
-                                                                 F[swz(c - 2 * l - 1)]),
+                    x = Num<T>::add(x, Num<T>::scale(Num<T>::add(f[2 * l + 1], f[-2 * l - 1]),
                                                      G.w[l]));
                 // restrict(-a) == -restrict(a) bit for bit (every step is odd)
                 const T v = Num<T>::scale(x, 0.5);
-                R[y * TK + k] = G.neg_in ? Num<T>::neg(v) : v;
+                R[y * RP + k] = G.neg_in ? Num<T>::neg(v) : v;
             }
         }
     };
     // axis-1 pass of plane t for this thread's (j, k), into the axis-0 ring;
     // the axis-0 pass once the ring spans planes 2I .. 2I + 2K - 2
     auto axis10 = [&](int t) {
-        const T* R = R1 + (t & 1) * (FY * TK);
-        const int c = K - 1 + 2 * tj;
-        T x = R[c * TK + tk];
+        const T* R = R1 + (t & 1) * (FY * RP) + (K - 1 + 2 * tj) * RP + tk;
+        T x = R[0];
 #pragma unroll
         for (int l = 0; l < K / 2; l++)
-            x = Num<T>::add(x, Num<T>::scale(Num<T>::add(R[(c + 2 * l + 1) * TK + tk],
-                                                         R[(c - 2 * l - 1) * TK + tk]),
+            x = Num<T>::add(x, Num<T>::scale(Num<T>::add(R[(2 * l + 1) * RP],
+                                                         R[-(2 * l + 1) * RP]),
                                              G.w[l]));
 #pragma unroll
         for (int i = 0; i < NR - 1; i++) ring[i] = ring[i + 1];
@@ -446,8 +450,9 @@ static int launch_restrict_k(const void* in, void* out, void* out2, int nin, con
     constexpr int TJ = 256 / TK;
     constexpr int D = sizeof(T) == 16 ? 2 : 3;
     constexpr int H = 2 * K - 3, FY = 2 * TJ + H, FZ = 2 * TK + H;
-    constexpr int SS = (FY * FZ + 1) & ~1;
-    constexpr size_t smem = ((size_t)(D + 1) * SS + (size_t)2 * FY * TK) * sizeof(T);
+    constexpr int SS = FY * FZ;
+    constexpr int RP = TK + (sizeof(T) == 16 ? 4 : (sizeof(T) == 8 ? 8 : 16));
+    constexpr size_t smem = ((size_t)(D + 1) * SS + (size_t)2 * FY * RP) * sizeof(T);
     static bool attr = false;
     if (!attr) {
         if (cudaFuncSetAttribute(k_restrict<T, K, TJ, TK, D>,
