@@ -362,14 +362,21 @@ def precond_c4(dev, nbands=128):
 def serving_c5(dev, rates=(50, 100, 200, 500, 1000, 2000), count=60):
     """Poisson-arrival stream of mixed-precision Poisson solves (to 1e-10)
     and nn = 3 stencil applications, grid sides log-uniform in [24, 160]
-    (multiples of 8), admitted against a 16 GB budget, 8 slots."""
+    (multiples of 8), admitted against a 16 GB budget, 8 slots, three
+    resident solvers per shape; each rate's stream is served once untimed,
+    then timed."""
     from gpaw_b200.serving import Server, latency_stats, make_requests
-    srv = Server(hbm_budget=16 << 30, nslots=8, device=dev)
-    srv.warm([(s, s, s) for s in range(24, 161, 8)])
+    # every shape of the stream has resident solvers (graphs captured)
+    # before serving starts; the loop never builds one while it serves
+    srv = Server(hbm_budget=16 << 30, nslots=8, device=dev, grow=False)
+    srv.warm([(s, s, s) for s in range(24, 161, 8)], per_shape=3)
     out = {'slots': 8, 'hbm_budget_gb': 16, 'requests_per_rate': count}
     for lam in rates:
         reqs = make_requests(lam, count, seed=lam)
         inputs = {r.rid: srv.host_input(r) for r in reqs}
+        # one untimed pass of the same stream first: the first launch of
+        # each captured solver graph on each slot stream costs extra
+        srv.run(make_requests(lam, count, seed=lam), inputs)
         srv.run(reqs, inputs)
         st = latency_stats(reqs)
         st['poisson_vcycles_mean'] = float(np.mean(

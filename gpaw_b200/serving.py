@@ -11,9 +11,12 @@ on the host clock.
 Solvers and operators are kept resident per grid shape (a pool of
 instances, one per concurrently running request of that shape), so the
 multigrid hierarchies, their buffers and their captured CUDA graphs are
-built once and reused.  Every kernel is deterministic and a request never
-shares a buffer with another, so a request's result does not depend on what
-else runs beside it.
+built once and reused.  Building a solver allocates device memory and
+captures a graph, which stalls the loop; with ``grow=False`` the loop never
+builds one while serving: a solve whose shape has no free solver waits, and
+later arrivals that can run are admitted past it.  Every kernel is
+deterministic and a request never shares a buffer with another, so a
+request's result does not depend on what else runs beside it.
 """
 from __future__ import annotations
 
@@ -66,10 +69,11 @@ class Server:
     SPACING = 0.18 / 0.52917721   # Bohr
 
     def __init__(self, hbm_budget=8 << 30, nslots=8, tol=1e-10,
-                 device=None):
+                 device=None, grow=True):
         self.device = torch.device(device if device is not None else 'cuda')
         self.budget = int(hbm_budget)
         self.tol = tol
+        self.grow = grow
         self.streams = [torch.cuda.Stream(device=self.device)
                         for _ in range(nslots)]
         self.free_slots = list(range(nslots))
@@ -77,6 +81,10 @@ class Server:
         self.resident = 0        # bytes held by pooled solvers/operators
         self.in_use = 0          # bytes held by running requests
         self.ops = {}            # N -> Laplace for apply requests
+        # one input/output slab per slot, sized before serving starts, so
+        # that the loop allocates no device memory (an allocation can stall
+        # every stream)
+        self.slabs = [None] * nslots
 
     # -- resources ---------------------------------------------------------
     def _gd(self, N):
@@ -105,7 +113,8 @@ class Server:
 
     def warm(self, shapes, per_shape=2):
         """Build `per_shape` resident solvers (graphs captured) and one
-        operator per shape ahead of time."""
+        operator per shape ahead of time, run each once, and size the
+        slot slabs."""
         for N in shapes:
             built = []
             for _ in range(per_shape):
@@ -122,7 +131,21 @@ class Server:
                     pass
                 built.append(ps)
             self.pools[('poisson', N)].extend(built)
-            self._op(N)
+            # first launch of each kernel loads it (lazy module loading):
+            # do that here, not while serving
+            op = self._op(N)
+            x = op.gd.zeros()
+            op.apply(x, op.gd.zeros())
+        self.reserve(shapes)
+
+    def reserve(self, shapes):
+        """Size every slot's input/output slab for the largest of `shapes`
+        (call before serving; allocates)."""
+        n = max(int(np.prod([x - 1 for x in N])) for N in shapes)
+        for i, sl in enumerate(self.slabs):
+            if sl is None or sl.numel() < 2 * n:
+                self.slabs[i] = torch.empty(2 * n, dtype=torch.float64,
+                                            device=self.device)
         torch.cuda.synchronize()
 
     def _op(self, N):
@@ -149,9 +172,11 @@ class Server:
     def _launch(self, req, host_in, host_out, slot):
         st = self.streams[slot]
         shape = tuple(host_in.shape)
+        n = int(np.prod(shape))
+        slab = self.slabs[slot]
         with torch.cuda.stream(st):
-            x = torch.empty(shape, dtype=torch.float64, device=self.device)
-            y = torch.empty(shape, dtype=torch.float64, device=self.device)
+            x = slab[:n].view(shape)
+            y = slab[n:2 * n].view(shape)
             x.copy_(host_in, non_blocking=True)
             solver = None
             extra = 0
@@ -189,7 +214,8 @@ class Server:
         outputs = {r.rid: torch.empty(tuple(inputs[r.rid].shape),
                                       dtype=torch.float64).pin_memory()
                    for r in reqs}
-        pending = collections.deque(reqs)
+        self.reserve({r.N for r in reqs})
+        pending = list(reqs)
         active = []
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -201,16 +227,23 @@ class Server:
                     active.remove(job)
                     self._finish(job, time.perf_counter() - t0)
                     progressed = True
-            while pending and pending[0].arrival <= now and self.free_slots:
-                req = pending[0]
+            # admit arrived requests in arrival order; a solve whose shape
+            # has no free solver (and may not build one) lets later ones by
+            i = 0
+            while i < len(pending) and pending[i].arrival <= now and \
+                    self.free_slots:
+                req = pending[i]
+                pooled = bool(self.pools[('poisson', req.N)])
+                if req.kind == 'poisson' and not pooled and not self.grow:
+                    i += 1
+                    continue
                 need = self.request_bytes(req)
-                if not self.pools[('poisson', req.N)] and \
-                        req.kind == 'poisson':
+                if req.kind == 'poisson' and not pooled:
                     need += self.solver_bytes(req.N)
                 if self.resident + self.in_use + need > self.budget and \
                         active:
                     break      # wait for memory to free up
-                pending.popleft()
+                del pending[i]
                 slot = self.free_slots.pop()
                 self.in_use += self.request_bytes(req)
                 req.start = time.perf_counter() - t0

@@ -50,3 +50,29 @@ def test_mixed_equals_alone(cuda):
             assert alone[r.rid].niter > 0
     stats = latency_stats(reqs)
     assert stats['requests'] == 24
+
+
+@pytest.mark.gpu
+def test_no_grow_waits_for_a_resident_solver(cuda):
+    """With grow=False the loop builds no solver while serving: three solves
+    of one shape share its single resident solver one after another, the
+    apply request runs past them, and every result equals the request
+    served alone."""
+    from gpaw_b200.serving import Server
+    reqs = [Request(i, 'poisson', (32, 32, 32), 0.0, seed=11 + i)
+            for i in range(3)]
+    reqs.append(Request(3, 'apply', (40, 40, 40), 0.0, seed=9))
+    srv = Server(hbm_budget=1 << 30, nslots=4, grow=False)
+    srv.warm([(32, 32, 32), (40, 40, 40)], per_shape=1)
+    inputs = {r.rid: srv.host_input(r) for r in reqs}
+    out = srv.run(reqs, inputs)
+    assert len(srv.pools[('poisson', (32, 32, 32))]) == 1
+    solves = sorted((r for r in out if r.kind == 'poisson'),
+                    key=lambda r: r.start)
+    for a, b in zip(solves, solves[1:]):
+        assert b.start >= a.done
+    got = {r.rid: r.result for r in out}
+    for r in reqs:
+        one = Request(r.rid, r.kind, r.N, 0.0, r.seed)
+        alone = srv.run([one], {r.rid: inputs[r.rid]})[0]
+        assert np.array_equal(got[r.rid], alone.result)
