@@ -525,6 +525,25 @@ def run_gpu(args):
         'e2e': e2e,
         'cpu_baseline': cpu_base,
     }
+    # FD Hamiltonian local part on the same batch: kin(psi) + v psi fused
+    if rank == 0 or world == 1:
+        from gpaw_b200 import FDHamiltonian
+        ham = FDHamiltonian(gd, kin_stencil=3, dtype=complex)
+        vt = torch.randn(tuple(gd.n_c), dtype=torch.float64, device=dev)
+        ham.apply_local_potential(vt, x, y, ph)
+        h0 = torch.cuda.Event(enable_timing=True)
+        h1 = torch.cuda.Event(enable_timing=True)
+        h0.record(stream)
+        for _ in range(5):
+            ham.apply_local_potential(vt, x, y, ph)
+        h1.record(stream)
+        torch.cuda.synchronize()
+        ht = h0.elapsed_time(h1) / 1e3 / 5
+        hb = ab + vt.numel() * 8
+        line['hamiltonian_c2'] = {
+            'what': 'kin(psi) + v psi, 256 x 96^3 complex128, one kernel',
+            'ms': ht * 1e3, 'gbs': hb / ht / 1e9,
+            'vs_apply_alone': ht / apply_t}
     if not args.no_poisson:
         line['poisson'] = {'c1': poisson_c1(dev), 'c3': poisson_c3(dev)}
     if not args.no_batch:

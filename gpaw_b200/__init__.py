@@ -18,7 +18,8 @@ from .transformers import Transformer
 from .poisson import (FDPoissonSolver, MixedPoissonSolver,
                       PoissonConvergenceError)
 from .preconditioner import Preconditioner
+from .hamiltonian import FDHamiltonian
 
-__all__ = ['GridDescriptor', 'BadGridError', 'FDOperator', 'GUCLaplace',
+__all__ = ['FDHamiltonian', 'GridDescriptor', 'BadGridError', 'FDOperator', 'GUCLaplace',
            'Laplace', 'Transformer', 'FDPoissonSolver',
            'MixedPoissonSolver', 'PoissonConvergenceError', 'Preconditioner']

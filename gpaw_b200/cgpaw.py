@@ -104,6 +104,27 @@ class Operator:
         self.apply_gpu(input.data_ptr(), output.data_ptr(),
                        tuple(input.shape), input.dtype, phases)
 
+    def apply_potential(self, input, output, v, phases=None):
+        """output = L input + input * v (v: float64 grid shared by the
+        batch) in one pass; FDHamiltonian.apply_local_potential's
+        arithmetic (gpaw/new/fd/hamiltonian.py:23-32)."""
+        _check_tensor(input, 'input')
+        _check_tensor(output, 'output')
+        _check_tensor(v, 'v')
+        if input.shape != output.shape or input.dtype != output.dtype:
+            raise TypeError('input and output differ in shape or dtype')
+        if tuple(input.shape[-3:]) != self.size or \
+                tuple(v.shape) != self.size:
+            raise TypeError('apply_potential: grid shapes do not match')
+        if v.dtype != torch.float64:
+            raise TypeError('apply_potential: v must be float64')
+        ph, ph_p = phases_arg(phases)
+        check(self._lib.gb_operator_apply_potential(
+            self._h, C.c_void_p(input.data_ptr()),
+            C.c_void_p(output.data_ptr()), _nin(input.shape),
+            _dtype_code(input.dtype), ph_p, C.c_void_p(v.data_ptr()),
+            _stream()))
+
     def relax(self, relax_method, f, s, nrelax, w=1.0):
         _check_tensor(f, 'f')
         _check_tensor(s, 's')

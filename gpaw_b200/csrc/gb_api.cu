@@ -138,6 +138,32 @@ extern "C" int gb_operator_apply(gb_operator* op, const void* in, void* out, int
     return 0;
 }
 
+extern "C" int gb_operator_apply_potential(gb_operator* op, const void* in, void* out,
+                                           int64_t nin, int dtype, const double* phases,
+                                           const double* v, void* stream) {
+    if (!op || !in || !out || !v) return fail(GB_EINVAL, "apply_potential: NULL argument");
+    if (int e = check_dtype(op, dtype)) return e;
+    if (nin < 0) return fail(GB_EINVAL, "apply_potential: negative batch");
+    if (nin == 0) return 0;
+    cudaStream_t st = (cudaStream_t)stream;
+    Phases P;
+    read_phases(dtype, phases, P);
+    const size_t bytes = (size_t)nin * op->ng() * elem_size(dtype);
+    const char* vb = (const char*)v;
+    const char* ob = (const char*)out;
+    if (vb < ob + bytes && ob < vb + (size_t)op->ng() * sizeof(double))
+        return fail(GB_EINVAL, "apply_potential: v must not overlap out");
+    if (ranges_overlap(in, out, bytes)) {
+        if (int e = op->scratch.ensure(bytes)) return e;
+        GB_CUDA_TRY(cudaMemcpyAsync(op->scratch.ptr, in, bytes, cudaMemcpyDeviceToDevice, st));
+        in = op->scratch.ptr;
+    }
+    if (int rc = op_sweep(op, EPI_POT, in, out, v, (int)nin, dtype, P, 0, 0, 0, nullptr, st))
+        return rc;
+    GB_LAUNCH_CHECK();
+    return 0;
+}
+
 extern "C" int gb_operator_residual(gb_operator* op, const void* phi, const void* rho, void* r,
                                     int64_t nin, int dtype, const double* phases, double scale,
                                     double* norm2, void* stream) {

@@ -10,6 +10,8 @@
 // the padded buffer.  Here the halo is never materialised: a read past an
 // edge is resolved in the load path (zero, or periodic wrap times the Bloch
 // phase), so each launch touches only its inputs and outputs.
+#include <algorithm>
+
 #include "gb_internal.cuh"
 
 namespace gb {
@@ -236,6 +238,29 @@ template void launch_fd<double2>(const void*, void*, int, const GridBC&, const P
                                  const Stencil&, cudaStream_t);
 template void launch_fd<float>(const void*, void*, int, const GridBC&, const Phases&,
                                const Stencil&, cudaStream_t);
+
+// o += p * v per point, in numpy's order for `o += p * vt_R.data`
+// (gpaw/new/fd/hamiltonian.py:31-32): the product rounded, then the sum.
+template <class T>
+__global__ void k_add_pot(const T* __restrict__ in, T* __restrict__ out,
+                          const double* __restrict__ v, int nin, long long ng) {
+    const long long n = (long long)nin * ng;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        out[i] = Num<T>::add(out[i], Num<T>::scale(in[i], v[i % ng]));
+}
+
+template <class T>
+void launch_add_pot(const void* in, void* out, const double* v, int nin, long long ng,
+                    cudaStream_t stream) {
+    const long long n = (long long)nin * ng;
+    const int nb = (int)std::min<long long>(148 * 16, (n + 255) / 256);
+    k_add_pot<T><<<nb, 256, 0, stream>>>((const T*)in, (T*)out, v, nin, ng);
+}
+template void launch_add_pot<double>(const void*, void*, const double*, int, long long,
+                                     cudaStream_t);
+template void launch_add_pot<double2>(const void*, void*, const double*, int, long long,
+                                      cudaStream_t);
 
 template <class T>
 void launch_residual(const void* phi, const void* rho, void* res, int nin, const GridBC& g,

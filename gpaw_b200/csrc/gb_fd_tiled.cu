@@ -238,10 +238,12 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
         }
     }
     if (!(CPLX && P.use)) wcode = 0;
-    auto issue = [&](int j) {
+    // slot = j % S (a compile-time constant inside the unrolled march when
+    // the ring depth equals the queue length)
+    auto issue = [&](int j, int slot) {
         int pl = pa + j;
         const bool pvalid = wrap_coord(pl, n0, g.periodic[0]);
-        T* st = ring + (j % S) * (PX * PY);
+        T* st = ring + slot * (PX * PY);
         const T* src = a + (long long)pl * n1 * n2;
 #pragma unroll
         for (int i = 0; i < NC; i++) {
@@ -254,8 +256,8 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
     // wrapped halo cells among them by their phase (the halo is filled from
     // the opposite side, as bc_unpack1's translate does, c/bc.cpp:242-257).
     // Other threads read them NN iterations later, after a barrier.
-    auto fixup = [&](int j) {
-        T* st = ring + (j % S) * (PX * PY);
+    auto fixup = [&](int slot) {
+        T* st = ring + slot * (PX * PY);
 #pragma unroll
         for (int i = 0; i < NC; i++) {
             const unsigned c = (wcode >> (3 * i)) & 7u;
@@ -299,7 +301,7 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
     const int jend = (pb - pa) + NN;   // relative planes needed: [0, jend)
 #pragma unroll 1
     for (int j = 0; j < D; j++) {
-        if (j < jend) issue(j);
+        if (j < jend) issue(j, j % S);
         cp_commit();
     }
 
@@ -309,6 +311,8 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
     // loaded one iteration ahead so that their latency overlaps the stencil
     // work instead of stalling every plane.
     constexpr bool NEED_AUX = MODE != EPI_APPLY;
+    // EPI_POT: the potential, one real grid shared by the batch
+    const double* vpot = (const double*)ep.aux;
     T pa1[RY], pa2[RY];
     double pac[RY];
     auto prefetch = [&](int p) {
@@ -320,7 +324,8 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
             pac[r] = 0.0;
             if (p < pb && gx < n2 && gy < n1) {
                 const long long at = ((long long)p * n1 + gy) * n2 + gx;
-                if (NEED_AUX && ep.aux) pa1[r] = aux[at];
+                if constexpr (MODE == EPI_POT) pac[r] = vpot[at];
+                else if (NEED_AUX && ep.aux) pa1[r] = aux[at];
                 if constexpr (MODE == EPI_LIN) {
                     if (ep.aux2) pa2[r] = aux2[at];
                     if (ep.acc64) pac[r] = ep.acc64[b * ng + at];
@@ -335,21 +340,25 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
     auto step = [&](int t, auto U_) {
         constexpr int U = decltype(U_)::value;           // t % Q
         constexpr int CU = (U + Q - NN) % Q;              // slot of the centre
+        constexpr bool FIXED = S == Q;                    // ring slots = U-based
+        const int s_t = FIXED ? U : t % S;
+        const int s_c = FIXED ? CU : (t - NN) % S;
+        const int s_d = FIXED ? (U + D) % Q : (t + D) % S;
         cp_wait<D - 1>();
         // this thread's copies of plane t have landed: fix its wrapped halo
         // cells (read as a centre NN iterations later, after a barrier)
-        if (wcode && t < nplanes) fixup(t);
+        if (wcode && t < nplanes) fixup(s_t);
         __syncthreads();
         {
             // the slot of plane t+D last held plane t-NN-1, the centre of
             // iteration t-1, which every thread has finished (barrier above)
             const int j = t + D;
-            if (j < jend) issue(j);
+            if (j < jend) issue(j, s_d);
             cp_commit();
         }
         // push plane t's own values (uniform phase for a wrapped plane)
         {
-            const T* st_in = ring + (t % S) * (PX * PY);
+            const T* st_in = ring + s_t * (PX * PY);
             const bool wrapped = CPLX && P.use && pa + t >= n0;
 #pragma unroll
             for (int r = 0; r < RY; r++) {
@@ -361,7 +370,7 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
         }
         if (t >= NN) {
             const int p = pa + t - NN;
-            const T* sc = ring + ((t - NN) % S) * (PX * PY);
+            const T* sc = ring + s_c * (PX * PY);
             // this thread's column in the centre tile (axis-1 neighbours)
             const T* colp = sc + ty0 * PX + (tx + NN);
 #pragma unroll
@@ -386,6 +395,9 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
                     const long long at = ((long long)p * n1 + gy) * n2 + gx;
                     if (MODE == EPI_APPLY) {
                         o[at] = x;
+                    } else if (MODE == EPI_POT) {
+                        // numpy's o += p * v: product rounded, then the sum
+                        o[at] = Num<T>::add(x, Num<T>::scale(vc, pac[r]));
                     } else if (MODE == EPI_RESID) {
                         const T res = Num<T>::sub(x, pa1[r]);
                         if (out) o[at] = res;
@@ -471,7 +483,8 @@ static int launch_cfd_nn(const void* in, void* out, int nin, const GridBC& g, co
     constexpr bool AUX = MODE != EPI_APPLY;
     if constexpr (sizeof(T) == 16) {
         constexpr int D = NN <= 3 ? 3 : 2;
-        constexpr int RY = (NN <= 3 && !AUX) ? 2 : 1;
+        // the potential of EPI_POT is one double a row: two rows still fit
+        constexpr int RY = (NN <= 3 && (!AUX || MODE == EPI_POT)) ? 2 : 1;
         if constexpr (MODE == EPI_APPLY && NN == 3)
             if (fused_apply())
                 return launch_cfd_t<T, NN, 32, 16, RY, D, MODE, 2>(in, out, nin, g, P, cs, ep,
@@ -479,7 +492,10 @@ static int launch_cfd_nn(const void* in, void* out, int nin, const GridBC& g, co
         return launch_cfd_t<T, NN, 32, 16, RY, D, MODE, 1>(in, out, nin, g, P, cs, ep, st, nblk);
     } else {
         constexpr int RY = (NN <= 3 && !AUX) ? 4 : 2;
-        return launch_cfd_t<T, NN, 32, 16, RY, 4, MODE, 1>(in, out, nin, g, P, cs, ep, st, nblk);
+        // nn = 3: three planes ahead makes the ring exactly 2nn+1 deep, so
+        // every ring slot in the unrolled march is a constant
+        constexpr int D = NN == 3 ? 3 : 4;
+        return launch_cfd_t<T, NN, 32, 16, RY, D, MODE, 1>(in, out, nin, g, P, cs, ep, st, nblk);
     }
 }
 
@@ -516,6 +532,9 @@ int launch_fd_cfd(int mode, const void* in, void* out, int nin, const GridBC& g,
         case EPI_JACOBI:
             if constexpr (sizeof(T) != 8) return -1;
             else return launch_cfd_mode<T, EPI_JACOBI>(in, out, nin, g, P, cs, nn, ep, st, nblk);
+        case EPI_POT:
+            if constexpr (sizeof(T) == 4) return -1;
+            else return launch_cfd_mode<T, EPI_POT>(in, out, nin, g, P, cs, nn, ep, st, nblk);
     }
     return -1;
 }

@@ -60,6 +60,8 @@ enum : int {
     EPI_JACOBI = 2,   // out = (1-w) in + w (aux - L' in) / c0  (c/bmgs/relax.cpp:41-65)
     EPI_PRECOND = 3,  // out = +-(in - sc (L in - aux))  (c/fd_preconditioner.cpp:251-333)
     EPI_LIN = 4,      // y = p0 aux + p1 in + p2 L in + p3 aux2 (mixed-precision solver)
+    EPI_POT = 5,      // out = L in + in * v, v real, one grid for the whole batch
+                      // (FDHamiltonian.apply_local_potential, gpaw/new/fd/hamiltonian.py:23-32)
 };
 
 struct Epi {
@@ -79,6 +81,10 @@ struct Epi {
 template <class T>
 void launch_fd(const void* in, void* out, int nin, const GridBC& g, const Phases& P,
                const Stencil& st, cudaStream_t stream);
+// out += in * v (v real, the same grid for every batch member)
+template <class T>
+void launch_add_pot(const void* in, void* out, const double* v, int nin, long long ng,
+                    cudaStream_t stream);
 template <class T>
 void launch_residual(const void* phi, const void* rho, void* res, int nin, const GridBC& g,
                      const Phases& P, const Stencil& st, double* partial, cudaStream_t stream);

@@ -130,6 +130,16 @@ inline int op_sweep(gb_operator* op, int mode, const void* in, void* out, const 
             if (dtype == GB_F64) launch_fd<double>(in, out, nin, op->g, P, op->st, st);
             else launch_fd<double2>(in, out, nin, op->g, P, op->st, st);
             break;
+        case EPI_POT:
+            // generic stencils: the apply, then o += p * v in a second pass
+            if (dtype == GB_F64) {
+                launch_fd<double>(in, out, nin, op->g, P, op->st, st);
+                launch_add_pot<double>(in, out, (const double*)aux, nin, op->ng(), st);
+            } else {
+                launch_fd<double2>(in, out, nin, op->g, P, op->st, st);
+                launch_add_pot<double2>(in, out, (const double*)aux, nin, op->ng(), st);
+            }
+            break;
         case EPI_RESID:
             if (dtype == GB_F64)
                 launch_residual<double>(in, aux, out, nin, op->g, P, op->st, partial, st);

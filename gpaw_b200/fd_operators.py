@@ -77,6 +77,13 @@ class FDOperator:
         """gpaw/fd_operators.py:120-130; ``in_xg is out_xg`` is allowed."""
         self.operator.apply(in_xg, out_xg, phase_cd)
 
+    def apply_potential(self, in_xg, out_xg, v_g, phase_cd=None):
+        """out = L in + in * v (v real, one grid for the whole batch) in
+        one pass: FDHamiltonian.apply_local_potential's ``self.kin(psit,
+        out)`` then ``o += p * vt`` (gpaw/new/fd/hamiltonian.py:23-32),
+        bit for bit."""
+        self.operator.apply_potential(in_xg, out_xg, v_g, phase_cd)
+
     def relax(self, relax_method, f_g, s_g, n, w=None):
         """gpaw/fd_operators.py:132-141: 1 = Gauss-Seidel, 2 = weighted
         Jacobi (float64 only)."""

@@ -85,6 +85,16 @@ GB_API void gb_operator_free(gb_operator* op);
 GB_API int gb_operator_apply(gb_operator* op, const void* in, void* out, int64_t nin,
                       int dtype, const double* phases, void* stream);
 
+/* FDHamiltonian.apply_local_potential (gpaw/new/fd/hamiltonian.py:23-32):
+ * out = L in + in * v for every batch member, v a real float64 grid
+ * (n0, n1, n2) shared by the batch; the same arithmetic as the reference's
+ * `self.kin(psit_nR, out)` followed by `o += p * vt_R.data` (product
+ * rounded, then the sum), in one pass over the data.  in == out allowed;
+ * v must not overlap out. */
+GB_API int gb_operator_apply_potential(gb_operator* op, const void* in, void* out, int64_t nin,
+                                       int dtype, const double* phases, const double* v,
+                                       void* stream);
+
 /* Replaces Operator.relax_gpu(method, f_ptr, s_ptr, nrelax, w) —
  * Operator_relax_gpu, c/gpu/operators.cpp:200-221 (CPU twin Operator_relax,
  * c/operators.cpp:50-92).  float64 only, one grid.  method 2: weighted

@@ -440,3 +440,18 @@ class Preconditioner:
                            d0, q0, r1, d1, q1, r2, d2, q2,
                            residuals, -residuals, self.step, phases)
         return d0
+
+
+class FDHamiltonian:
+    """gpaw/new/fd/hamiltonian.py:14-32: kinetic operator -1/2 Laplacian of
+    order kin_stencil and the local-potential product."""
+
+    def __init__(self, gd, kin_stencil=3, dtype=float, be='auto'):
+        self.kin = Laplace(gd, -0.5, kin_stencil, dtype, be=be)
+
+    def apply_local_potential(self, vt_R, psit_nR, out, phase_cd=None):
+        """:23-32: ``self.kin(psit_nR, out)``, then ``o += p * vt_R`` per
+        band (numpy: the product rounded, then the sum)."""
+        self.kin.apply(psit_nR, out, phase_cd)
+        for p, o in zip(psit_nR, out):
+            o += p * vt_R

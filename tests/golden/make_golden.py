@@ -52,6 +52,11 @@ def cases():
     # Poisson
     for bc in ('p', 'z'):
         out.append((f'ps_{bc}', ('ps', 3, bc, 'f')))
+    # FD Hamiltonian local part (appended last: earlier cases keep their
+    # random draws)
+    for nn, bc, dt in ((3, 'p', 'c'), (3, 'z', 'f'), (2, 'm', 'c'),
+                       (1, 'p', 'f')):
+        out.append((f'ham_nn{nn}_{bc}_{dt}', ('ham', nn, bc, dt)))
     return out
 
 
@@ -114,6 +119,18 @@ def build(kind, nn, bc, dt, rng):
         o = np.zeros_like(R)
         pc(R, ph, out=o)
         d.update(N=np.array(gd.N_c), pbc=np.array(pbc), res=R, out=o)
+        if ph is not None:
+            d['phases'] = ph
+    elif kind == 'ham':
+        gd = L.GridDescriptor((10, 9, 12), (3.0, 2.8, 3.6), pbc)
+        ham = L.FDHamiltonian(gd, nn, dtype, be='ref')
+        psit = rand((3,) + tuple(gd.n_c))
+        vt = rng.standard_normal(tuple(gd.n_c))
+        ph = gd.phase_factor_cd(KPT) if dtype == complex else None
+        out = np.zeros_like(psit)
+        ham.apply_local_potential(vt, psit, out, ph)
+        d.update(N=np.array(gd.N_c), pbc=np.array(pbc), psit=psit, vt=vt,
+                 out=out)
         if ph is not None:
             d['phases'] = ph
     elif kind == 'ps':

@@ -110,3 +110,19 @@ def test_port_equals_reference_random():
                     op.apply(a, b, ph)
                     outs.append(b)
                 assert np.array_equal(*outs), (nn, pbc, dtype)
+
+
+def test_hamiltonian_cases(golden):
+    n = 0
+    for name, c in golden.items():
+        if not name.startswith('ham_'):
+            continue
+        nn = int(name.split('_')[1][2:])
+        gd = L.GridDescriptor(tuple(c['N']), (3.0, 2.8, 3.6), tuple(c['pbc']))
+        dtype = complex if np.iscomplexobj(c['psit']) else float
+        ham = L.FDHamiltonian(gd, nn, dtype, be='port')
+        out = np.zeros_like(c['psit'])
+        ham.apply_local_potential(c['vt'], c['psit'], out, c.get('phases'))
+        assert np.array_equal(out, c['out']), name
+        n += 1
+    assert n == 4
