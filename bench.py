@@ -422,6 +422,13 @@ def run_gpu(args):
     z = torch.empty_like(x)
     stream = torch.cuda.current_stream()
 
+    # z-block depths of the three kernels picked by timing (autotuner)
+    from gpaw_b200 import autotune
+    depth = {'apply': autotune.tune_operator(kin, x, y, ph, reps=2)[0],
+             'restrict': autotune.tune_transformer(rst, x, c, ph, reps=2)[0],
+             'interpolate': autotune.tune_transformer(itp, c, z, ph,
+                                                      reps=2)[0]}
+
     def step(ev=None):
         if ev is not None:
             ev[0].record(stream)
@@ -509,7 +516,9 @@ def run_gpu(args):
         'dtype': 'c128', 'data': 'synthetic',
         'config': {'workload': WORKLOAD, 'batch': NBANDS, 'grid': list(N),
                    'parallelism': f'replicas x{world}',
-                   'l2': 'inputs 3.6 GB per array, larger than L2 (no flush)'},
+                   'l2': 'inputs 3.6 GB per array, larger than L2 (no flush)',
+                   'z_block_depth': {k: (v or 'auto') for k, v in depth.items()},
+                   'depth_picked_by': 'gpaw_b200.autotune (timed)'},
         'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak,
                      'unit': 'GB/s', 'frac': achieved / peak,
                      'traffic': ncu_traffic(), 'kernel': 'fd apply c128',

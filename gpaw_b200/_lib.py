@@ -29,6 +29,8 @@ SIGNATURES = {
                                   C.c_int, C.c_int, C.POINTER(_p)]),
     'gb_operator_free': (None, [_p]),
     'gb_operator_apply': (C.c_int, [_p, _p, _p, C.c_int64, C.c_int, _dp, _p]),
+    'gb_operator_set_chunk': (C.c_int, [_p, C.c_int]),
+    'gb_transformer_set_chunk': (C.c_int, [_p, C.c_int]),
     'gb_operator_apply_potential': (C.c_int, [_p, _p, _p, C.c_int64, C.c_int,
                                               _dp, _p, _p]),
     'gb_operator_relax': (C.c_int, [_p, C.c_int, _p, _p, C.c_int, C.c_double,

@@ -155,6 +155,11 @@ class Operator:
     def get_diagonal_element(self):
         return self._lib.gb_operator_get_diagonal_element(self._h)
 
+    def set_chunk(self, chunk):
+        """Axis-0 planes per CTA of the plane-marching kernels (0 = the
+        automatic rule); results do not depend on it."""
+        check(self._lib.gb_operator_set_chunk(self._h, int(chunk)))
+
     def get_async_sizes(self):
         # c/operators.cpp:335-345 without GPAW_ASYNC
         return (0, 1, 1)
@@ -207,6 +212,10 @@ class Transformer:
             raise TypeError('transformer: batch shape or dtype mismatch')
         self.apply_gpu(input.data_ptr(), output.data_ptr(),
                        tuple(input.shape), input.dtype, phases)
+
+    def set_chunk(self, chunk):
+        """Output planes of axis 0 per CTA (0 = the automatic rule)."""
+        check(self._lib.gb_transformer_set_chunk(self._h, int(chunk)))
 
     def get_async_sizes(self):
         return (0, 1)

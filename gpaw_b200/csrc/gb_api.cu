@@ -164,6 +164,20 @@ extern "C" int gb_operator_apply_potential(gb_operator* op, const void* in, void
     return 0;
 }
 
+extern "C" int gb_operator_set_chunk(gb_operator* op, int chunk) {
+    if (!op) return fail(GB_EINVAL, "set_chunk: NULL operator");
+    if (chunk < 0) return fail(GB_EINVAL, "set_chunk: chunk must be >= 0");
+    op->chunk = chunk;
+    return 0;
+}
+
+extern "C" int gb_transformer_set_chunk(gb_transformer* t, int chunk) {
+    if (!t) return fail(GB_EINVAL, "set_chunk: NULL transformer");
+    if (chunk < 0) return fail(GB_EINVAL, "set_chunk: chunk must be >= 0");
+    t->G.chunk = chunk;
+    return 0;
+}
+
 extern "C" int gb_operator_residual(gb_operator* op, const void* phi, const void* rho, void* r,
                                     int64_t nin, int dtype, const double* phases, double scale,
                                     double* norm2, void* stream) {

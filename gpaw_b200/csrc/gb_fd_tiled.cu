@@ -23,6 +23,8 @@
 #include <cstdlib>
 #include <utility>
 
+#include <algorithm>
+
 #include "gb_internal.cuh"
 
 namespace gb {
@@ -454,7 +456,7 @@ static int launch_cfd_t(const void* in, void* out, int nin, const GridBC& g, con
     }
     const int tiles_x = (g.n[2] + TX - 1) / TX;
     const int tiles_y = (g.n[1] + TY - 1) / TY;
-    const int chunk0 = cfd_chunk(g, NN, nin);
+    const int chunk0 = ep.chunk > 0 ? min(ep.chunk, g.n[0]) : cfd_chunk(g, NN, nin);
     const int nch = (g.n[0] + chunk0 - 1) / chunk0;
     if (nblk) *nblk = tiles_x * tiles_y * nch;
     const long long ng = (long long)g.n[0] * g.n[1] * g.n[2];
@@ -547,11 +549,11 @@ template int launch_fd_cfd<float>(int, const void*, void*, int, const GridBC&, c
                                   const CfdStencil&, int, const Epi&, cudaStream_t, int*);
 
 // Number of CTAs per grid of the EPI_RESID launch (partials per grid).
-int cfd_blocks(const GridBC& g, int nn, int elem_bytes, int nin) {
+int cfd_blocks(const GridBC& g, int nn, int elem_bytes, int nin, int chunk) {
     const int TX = 32, TY = 16;
     const int tiles_x = (g.n[2] + TX - 1) / TX;
     const int tiles_y = (g.n[1] + TY - 1) / TY;
-    const int chunk0 = cfd_chunk(g, nn, nin);
+    const int chunk0 = chunk > 0 ? std::min(chunk, g.n[0]) : cfd_chunk(g, nn, nin);
     (void)elem_bytes;
     return tiles_x * tiles_y * ((g.n[0] + chunk0 - 1) / chunk0);
 }

@@ -41,6 +41,7 @@ struct XferGeom {
     int neg_in;     // negate every input value on load (exact)
     int accumulate; // interpolation: out -= value instead of out = value
     double scale2;  // restriction: also write out2 = scale2 * out when out2 set
+    int chunk;      // output planes of axis 0 per CTA (0: the launcher's rule)
 };
 
 // ------------------------------------------------------- tiled cfd stencil
@@ -75,6 +76,7 @@ struct Epi {
     double p0, p1, p2, p3;
     double* acc64;    // if set: acc64 += y (instead of writing out)
     float* out32;     // if set: out32 = (float) y (instead of writing out)
+    int chunk;        // planes of axis 0 per CTA (0: cfd_chunk's rule)
 };
 
 // ------------------------------------------------------------------ launchers
@@ -107,7 +109,7 @@ template <class T>
 int launch_fd_cfd(int mode, const void* in, void* out, int nin, const GridBC& g,
                   const Phases& P, const CfdStencil& cs, int nn, const Epi& ep,
                   cudaStream_t st, int* nblk);
-int cfd_blocks(const GridBC& g, int nn, int elem_bytes, int nin);
+int cfd_blocks(const GridBC& g, int nn, int elem_bytes, int nin, int chunk = 0);
 int cfd_chunk(const GridBC& g, int nn, int nin);
 
 }  // namespace gb

@@ -385,6 +385,7 @@ static int lin(gb_operator* op, const T* in, T* out, const T* aux, const T* aux2
     ep.acc64 = acc64;
     ep.out32 = out32;
     ep.partial = partial;
+    ep.chunk = op->chunk;
     Phases P{};
     const int rc = launch_fd_cfd<T>(EPI_LIN, in, out, 1, op->g, P, op->cs, op->nn, ep, st, nullptr);
     if (rc == -2) return fail(GB_ECUDA, "mixed: could not raise the shared-memory limit");

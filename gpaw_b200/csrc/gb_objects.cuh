@@ -88,6 +88,7 @@ struct gb_operator {
     gb::CfdStencil cs;     // axis-aligned form, when the stencil has one
     int nn = 0;        // its half-width
     int tiled = 0;     // use the plane-marching kernels
+    int chunk = 0;     // axis-0 planes per CTA of those kernels (0: automatic)
     gb::Scratch scratch;   // aliasing stage / Jacobi ping-pong / GS snapshot
     gb::Scratch partial;   // per-CTA partial sums of |r|^2
     long long ng() const { return (long long)g.n[0] * g.n[1] * g.n[2]; }
@@ -107,7 +108,7 @@ namespace gb {
 
 // Partial sums produced per grid by a residual sweep of `op`.
 inline int op_resid_blocks(const gb_operator* op, int nin, int es) {
-    return op->tiled ? cfd_blocks(op->g, op->nn, es, nin) : residual_blocks(op->g);
+    return op->tiled ? cfd_blocks(op->g, op->nn, es, nin, op->chunk) : residual_blocks(op->g);
 }
 
 // One pass of the stencil with a fused epilogue; plane-marching kernel for
@@ -117,6 +118,7 @@ inline int op_sweep(gb_operator* op, int mode, const void* in, void* out, const 
                     double* partial, cudaStream_t st) {
     if (op->tiled) {
         Epi ep{aux, w, sc, negate, partial};
+        ep.chunk = op->chunk;
         int rc = (dtype == GB_F64)
                      ? launch_fd_cfd<double>(mode, in, out, nin, op->g, P, op->cs, op->nn, ep, st,
                                              nullptr)

@@ -16,6 +16,8 @@
 // of recent planes, from which the axis-0 pass produces finished outputs.
 // Every intermediate value is formed with the same operations in the same
 // order as in the reference's passes, so outputs are bit-identical.
+#include <algorithm>
+
 #include "gb_internal.cuh"
 
 namespace gb {
@@ -464,8 +466,10 @@ static int launch_restrict_k(const void* in, void* out, void* out2, int nin, con
     const int t1 = (G.nout[1] + TJ - 1) / TJ, t2 = (G.nout[2] + TK - 1) / TK;
     int chunk0 = G.nout[0];
     const long long tiles = (long long)t1 * t2 * nin;
-    while (chunk0 > 4 && tiles * ((G.nout[0] + chunk0 - 1) / chunk0) < 148 * 4)
-        chunk0 = (chunk0 + 1) / 2;
+    if (G.chunk > 0) chunk0 = std::min(G.chunk, G.nout[0]);
+    else
+        while (chunk0 > 4 && tiles * ((G.nout[0] + chunk0 - 1) / chunk0) < 148 * 4)
+            chunk0 = (chunk0 + 1) / 2;
     const int nchunks = (G.nout[0] + chunk0 - 1) / chunk0;
     for (int b0 = 0; b0 < nin; b0 += 65535) {
         const int nb = min(65535, nin - b0);
@@ -499,7 +503,10 @@ static int launch_interp_k(const void* in, void* out, int nin, const XferGeom& G
     const int n0p = G.s[0] - (K - 1) + G.skip1[0];
     int chunk0 = n0p;
     const long long tiles = (long long)t1 * t2 * nin;
-    while (chunk0 > 4 && tiles * ((n0p + chunk0 - 1) / chunk0) < 148 * 8) chunk0 = (chunk0 + 1) / 2;
+    if (G.chunk > 0) chunk0 = std::min(G.chunk, n0p);
+    else
+        while (chunk0 > 4 && tiles * ((n0p + chunk0 - 1) / chunk0) < 148 * 8)
+            chunk0 = (chunk0 + 1) / 2;
     const int nchunks = (n0p + chunk0 - 1) / chunk0;
     for (int b0 = 0; b0 < nin; b0 += 65535) {
         const int nb = min(65535, nin - b0);

@@ -98,6 +98,11 @@ class FDOperator:
     def get_diagonal_element(self):
         return self.operator.get_diagonal_element()
 
+    def set_chunk(self, chunk):
+        """Axis-0 planes per CTA (z-block depth) of the plane-marching
+        kernels; 0 = automatic.  See gpaw_b200.autotune."""
+        self.operator.set_chunk(chunk)
+
     def get_async_sizes(self):
         return self.operator.get_async_sizes()
 

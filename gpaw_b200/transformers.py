@@ -70,6 +70,11 @@ class _Transformer:
         self.transformer.apply(input, output, phases)
         return output
 
+    def set_chunk(self, chunk):
+        """Output planes of axis 0 per CTA; 0 = automatic.  See
+        gpaw_b200.autotune."""
+        self.transformer.set_chunk(chunk)
+
     def get_async_sizes(self):
         return self.transformer.get_async_sizes()
 

@@ -85,6 +85,15 @@ GB_API void gb_operator_free(gb_operator* op);
 GB_API int gb_operator_apply(gb_operator* op, const void* in, void* out, int64_t nin,
                       int dtype, const double* phases, void* stream);
 
+/* Tuning knob (no reference counterpart): planes of axis 0 that one CTA of
+ * the plane-marching kernels handles (the "z-block depth"; outputs planes
+ * for transformers).  0 restores the automatic rule (enough CTAs for two
+ * per SM).  Results do not depend on it; gpaw_b200.autotune picks it by
+ * timing.  Solvers capture their launches in a graph at their first solve:
+ * set it on their operators before that. */
+GB_API int gb_operator_set_chunk(gb_operator* op, int chunk);
+GB_API int gb_transformer_set_chunk(gb_transformer* t, int chunk);
+
 /* FDHamiltonian.apply_local_potential (gpaw/new/fd/hamiltonian.py:23-32):
  * out = L in + in * v for every batch member, v a real float64 grid
  * (n0, n1, n2) shared by the batch; the same arithmetic as the reference's
