@@ -182,6 +182,80 @@ def cpu_measure(nb=CPU_SAMPLE, reps=3):
                       f'batch with {cores} threads'}
 
 
+# ------------------------------------------ CPU baselines of the Poisson path
+def _c4_geometry(count, seed=0):
+    """Sides and Gaussian counts of the C4 batch (the same draws as
+    gpaw_b200.batch.c4_grids and poisson_c4)."""
+    sides = np.random.default_rng(seed).choice(np.arange(32, 129, 8),
+                                               size=(count, 3))
+    rng = np.random.default_rng(1)
+    ngs = [int(rng.integers(4, 17)) for _ in range(count)]
+    return sides, ngs
+
+
+def _c4_cpu_one(i):
+    """One C4 grid solved by the reference's C core (oracle/_ref) to
+    1e-10 relative residual; returns its V-cycle count."""
+    from oracle import gpaw_layer as L
+    from gpaw_b200.workloads import (BOHR, eps_for_relative_residual,
+                                     gaussian_density, random_gaussians)
+    sides, ngs = _c4_geometry(i + 1)
+    h = 0.18 / BOHR
+    Nc = tuple(int(x) for x in sides[i])
+    gd = L.GridDescriptor(Nc, tuple(x * h for x in Nc), 0)
+    rng = np.random.default_rng(100 + i)
+    rho = gaussian_density(gd, *random_gaussians(gd, ngs[i], rng))
+    rho = rho - rho.sum() / rho.size
+    ps = L.FDPoissonSolver(nn=3, eps=eps_for_relative_residual(rho, gd),
+                           maxiter=400)
+    ps.set_grid_descriptor(gd)
+    return ps.solve_neutral(gd.zeros(), rho)
+
+
+def cpu_poisson_child(which, arg):
+    """Fresh process: the reference's C core on a Poisson configuration;
+    prints JSON.  c1: two solves (OMP threads from the environment), the
+    potential saved to `arg` (.npy).  c4: the first `arg` grids of the C4
+    batch over a pool of single-threaded processes, one per core."""
+    from oracle import gpaw_layer as L
+    kind = 'reference' if L._REF is not None else 'port'
+    if which == 'c1':
+        from gpaw_b200.workloads import BOHR, c1_density, neutralize
+        h = 0.2 / BOHR
+        gd = L.GridDescriptor((64, 64, 64), (64 * h,) * 3, 0)
+        rho = neutralize(c1_density(gd), gd)
+        ps = L.FDPoissonSolver(nn=3, eps=2e-10)
+        ps.set_grid_descriptor(gd)
+        times = []
+        for _ in range(2):
+            phi = gd.zeros()
+            t0 = time.perf_counter()
+            n = ps.solve_neutral(phi, rho)
+            times.append(time.perf_counter() - t0)
+        np.save(arg, phi)
+        print(json.dumps({'kind': kind, 'times': times, 'niter': n}))
+    else:
+        import multiprocessing as mp
+        count = int(arg)
+        cores = len(os.sched_getaffinity(0))
+        t0 = time.perf_counter()
+        with mp.get_context('spawn').Pool(cores) as pool:
+            ns = pool.map(_c4_cpu_one, range(count), chunksize=1)
+        t = time.perf_counter() - t0
+        print(json.dumps({'kind': kind, 'seconds': t, 'grids': count,
+                          'workers': cores, 'vcycles': ns}))
+
+
+def cpu_poisson(which, arg, threads):
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads),
+               CUDA_VISIBLE_DEVICES='')
+    out = subprocess.run(
+        [sys.executable, os.path.abspath(__file__), '--_cpu-poisson-child',
+         which, str(arg)], env=env, capture_output=True, text=True,
+        check=True, cwd=ROOT).stdout
+    return json.loads(out.strip().splitlines()[-1])
+
+
 def run_reference(args):
     """--impl reference: the reference's CPU implementation of the path."""
     rank = int(os.environ.get('RANK', '0'))
@@ -204,7 +278,7 @@ def run_reference(args):
 
 
 # ------------------------------------------------------------- Poisson
-def poisson_c1(dev, nsolve=20):
+def poisson_c1(dev, nsolve=20, cpu=True):
     """64^3 zero-BC FDPoissonSolver (nn = 3, Jacobi, reference schedule),
     h = 0.2 A, 8 Gaussians: solves/s at the reference's eps = 2e-10 and at
     the eps that gives 1e-10 relative residual."""
@@ -240,7 +314,36 @@ def poisson_c1(dev, nsolve=20):
                     'solves_per_s': 1.0 / t, 'rel_residual': rel,
                     'p50_ms': t * 1e3,
                     'p99_ms': float(np.percentile(times, 99)) * 1e3}
+        if tag == 'eps_2e-10' and cpu:
+            out[tag]['cpu_reference'] = c1_cpu(phi.cpu().numpy(), n)
     return out
+
+
+def c1_cpu(phi_gpu, n_gpu):
+    """The same C1 solve by the reference's C core on the host cores (one
+    thread and all threads, the better reported) and the GPU potential's
+    max error against it."""
+    import tempfile
+    cores = len(os.sched_getaffinity(0))
+    best = None
+    fd, path = tempfile.mkstemp(suffix='.npy')
+    os.close(fd)
+    try:
+        for threads in sorted({1, cores}):
+            r = cpu_poisson('c1', path, threads)
+            t = float(min(r['times']))
+            if best is None or t < best['ms_per_solve'] / 1e3:
+                phi_cpu = np.load(path)
+                err = float(np.abs(phi_gpu - phi_cpu).max() /
+                            np.abs(phi_cpu).max())
+                best = {'ms_per_solve': t * 1e3, 'solves_per_s': 1.0 / t,
+                        'threads': threads, 'cores': cores,
+                        'kind': r['kind'], 'vcycles': r['niter'],
+                        'same_vcycles_as_gpu': r['niter'] == n_gpu,
+                        'max_rel_err_gpu_vs_cpu': err}
+    finally:
+        os.unlink(path)
+    return best
 
 
 def poisson_c3(dev, nsolve=5):
@@ -292,7 +395,7 @@ def poisson_c3(dev, nsolve=5):
     return out
 
 
-def poisson_c4(dev, count=512, precisions=('mixed', 'fp64')):
+def poisson_c4(dev, count=512, precisions=('mixed', 'fp64'), cpu=True):
     """512 zero-BC grids, every side from {32, 40, ..., 128}, each with 4-16
     seeded Gaussians (C3 distributions), solved to 1e-10 relative residual:
     every solve enqueued on one of 16 streams, one synchronisation."""
@@ -326,6 +429,16 @@ def poisson_c4(dev, count=512, precisions=('mixed', 'fp64')):
     if 'mixed' in out and 'fp64' in out:
         out['speedup_mixed_over_fp64'] = (out['mixed']['solves_per_s'] /
                                           out['fp64']['solves_per_s'])
+    if cpu:
+        cores = len(os.sched_getaffinity(0))
+        ncpu = min(count, cores)
+        r = cpu_poisson('c4', ncpu, 1)
+        out['cpu_reference'] = {
+            'solves_per_s': r['grids'] / r['seconds'], 'kind': r['kind'],
+            'sample': f'first {r["grids"]} grids of the batch, FP64 '
+                      f'reference schedule to 1e-10, {r["workers"]} '
+                      f'single-threaded processes',
+            'cores': r['workers'], 'vcycles_mean': float(np.mean(r['vcycles']))}
     return out
 
 
@@ -553,10 +666,14 @@ def run_gpu(args):
             'what': 'kin(psi) + v psi, 256 x 96^3 complex128, one kernel',
             'ms': ht * 1e3, 'gbs': hb / ht / 1e9,
             'vs_apply_alone': ht / apply_t}
+    # CPU references of the Poisson path: rank 0 at N = 1 only
+    cpu_ok = not args.no_cpu and rank == 0 and world == 1
     if not args.no_poisson:
-        line['poisson'] = {'c1': poisson_c1(dev), 'c3': poisson_c3(dev)}
+        line['poisson'] = {'c1': poisson_c1(dev, cpu=cpu_ok),
+                           'c3': poisson_c3(dev)}
     if not args.no_batch:
-        line.setdefault('poisson', {})['c4_batch'] = poisson_c4(dev)
+        line.setdefault('poisson', {})['c4_batch'] = poisson_c4(dev,
+                                                                cpu=cpu_ok)
         line['preconditioner_c4'] = precond_c4(dev)
     if not args.no_serving:
         line['serving_c5'] = serving_c5(dev)
@@ -569,6 +686,9 @@ def run_gpu(args):
 def main():
     if len(sys.argv) > 1 and sys.argv[1] == '--_cpu-child':
         cpu_step_child(int(sys.argv[2]), int(sys.argv[3]))
+        return
+    if len(sys.argv) > 1 and sys.argv[1] == '--_cpu-poisson-child':
+        cpu_poisson_child(sys.argv[2], sys.argv[3])
         return
     p = argparse.ArgumentParser()
     p.add_argument('--gpus', type=int, default=1)
