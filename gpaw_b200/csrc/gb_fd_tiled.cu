@@ -34,14 +34,14 @@ namespace gb {
 // CTAs; a single grid is split along axis 0 until the launch has at least
 // `target` CTAs (default 148 * 2, tunable by GPAW_B200_CTA_TARGET), but
 // never into chunks shorter than 2 nn planes.
-int cfd_chunk(const GridBC& g, int nn, int nin) {
+int cfd_chunk(const GridBC& g, int nn, int nin, int ty) {
     static int target = [] {
         const char* v = getenv("GPAW_B200_CTA_TARGET");
         const int t = v ? atoi(v) : 0;
         return t > 0 ? t : 148 * 2;
     }();
     const int tiles_x = (g.n[2] + 31) / 32;
-    const int tiles_y = (g.n[1] + 15) / 16;
+    const int tiles_y = (g.n[1] + ty - 1) / ty;
     const long long tiles = (long long)tiles_x * tiles_y * nin;
     int chunk0 = g.n[0];
     while (chunk0 > 2 * nn && tiles * ((g.n[0] + chunk0 - 1) / chunk0) < target)
@@ -157,10 +157,15 @@ __device__ __forceinline__ T add_direction(T x, const double* cp, const double* 
 // cell: axis 2, axis 1, axis 0.  ORD = 1: every product and sum rounded on
 // its own (bit-identical to the reference); ORD = 2: fused multiply-adds
 // (fewer instructions, results within a few ulp; opt-in, apply only).
-// 128 registers a thread: two resident CTAs of 256 threads (complex) or
-// four of 128 (real) when the tile holds two or four rows per thread.
+// Register caps: three resident CTAs of 256 threads for the complex apply
+// (nn <= 3), two for the other complex modes, four CTAs of 128 threads for
+// real data.
 template <class T, int NN, int TX, int TY, int RY, int D, int MODE, int ORD>
-__global__ void __launch_bounds__(TX * (TY / RY), (512 / (TX * (TY / RY))))
+__global__ void __launch_bounds__(TX * (TY / RY),
+                                  (sizeof(T) == 16 && NN <= 3 &&
+                                   (MODE == EPI_APPLY || MODE == EPI_POT))
+                                      ? 3
+                                      : (512 / (TX * (TY / RY))))
 k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phases P,
          CfdStencil cs, int chunk0, int tiles_x, Epi ep) {
     constexpr int PX = TX + 2 * NN;          // tile pitch (elements)
@@ -456,7 +461,7 @@ static int launch_cfd_t(const void* in, void* out, int nin, const GridBC& g, con
     }
     const int tiles_x = (g.n[2] + TX - 1) / TX;
     const int tiles_y = (g.n[1] + TY - 1) / TY;
-    const int chunk0 = ep.chunk > 0 ? min(ep.chunk, g.n[0]) : cfd_chunk(g, NN, nin);
+    const int chunk0 = ep.chunk > 0 ? min(ep.chunk, g.n[0]) : cfd_chunk(g, NN, nin, TY);
     const int nch = (g.n[0] + chunk0 - 1) / chunk0;
     if (nblk) *nblk = tiles_x * tiles_y * nch;
     const long long ng = (long long)g.n[0] * g.n[1] * g.n[2];
@@ -484,14 +489,16 @@ static int launch_cfd_nn(const void* in, void* out, int nin, const GridBC& g, co
     // prefetched values need registers too)
     constexpr bool AUX = MODE != EPI_APPLY;
     if constexpr (sizeof(T) == 16) {
+        // 32 x 8 tiles, one row a thread: 80 registers and 60 KB of ring
+        // (nn = 3) let three CTAs share an SM; measured faster than 32 x 16
+        // tiles of two rows a thread at two CTAs an SM (the rows' shared
+        // axis-1 loads do not make up for the lost warps)
         constexpr int D = NN <= 3 ? 3 : 2;
-        // the potential of EPI_POT is one double a row: two rows still fit
-        constexpr int RY = (NN <= 3 && (!AUX || MODE == EPI_POT)) ? 2 : 1;
         if constexpr (MODE == EPI_APPLY && NN == 3)
             if (fused_apply())
-                return launch_cfd_t<T, NN, 32, 16, RY, D, MODE, 2>(in, out, nin, g, P, cs, ep,
-                                                                    st, nblk);
-        return launch_cfd_t<T, NN, 32, 16, RY, D, MODE, 1>(in, out, nin, g, P, cs, ep, st, nblk);
+                return launch_cfd_t<T, NN, 32, 8, 1, D, MODE, 2>(in, out, nin, g, P, cs, ep, st,
+                                                                  nblk);
+        return launch_cfd_t<T, NN, 32, 8, 1, D, MODE, 1>(in, out, nin, g, P, cs, ep, st, nblk);
     } else {
         constexpr int RY = (NN <= 3 && !AUX) ? 4 : 2;
         // nn = 3: three planes ahead makes the ring exactly 2nn+1 deep, so
@@ -550,11 +557,11 @@ template int launch_fd_cfd<float>(int, const void*, void*, int, const GridBC&, c
 
 // Number of CTAs per grid of the EPI_RESID launch (partials per grid).
 int cfd_blocks(const GridBC& g, int nn, int elem_bytes, int nin, int chunk) {
-    const int TX = 32, TY = 16;
+    // the tile of launch_cfd_nn: 32 x 8 for 16-byte elements, else 32 x 16
+    const int TX = 32, TY = elem_bytes == 16 ? 8 : 16;
     const int tiles_x = (g.n[2] + TX - 1) / TX;
     const int tiles_y = (g.n[1] + TY - 1) / TY;
-    const int chunk0 = chunk > 0 ? std::min(chunk, g.n[0]) : cfd_chunk(g, nn, nin);
-    (void)elem_bytes;
+    const int chunk0 = chunk > 0 ? std::min(chunk, g.n[0]) : cfd_chunk(g, nn, nin, TY);
     return tiles_x * tiles_y * ((g.n[0] + chunk0 - 1) / chunk0);
 }
 

@@ -110,6 +110,6 @@ int launch_fd_cfd(int mode, const void* in, void* out, int nin, const GridBC& g,
                   const Phases& P, const CfdStencil& cs, int nn, const Epi& ep,
                   cudaStream_t st, int* nblk);
 int cfd_blocks(const GridBC& g, int nn, int elem_bytes, int nin, int chunk = 0);
-int cfd_chunk(const GridBC& g, int nn, int nin);
+int cfd_chunk(const GridBC& g, int nn, int nin, int ty);
 
 }  // namespace gb

@@ -77,7 +77,7 @@ __device__ __forceinline__ T apply_code(T v, unsigned c, bool plane_wrap, double
 }
 
 template <class T, int K, int TJ, int TK, int D>
-__global__ void __launch_bounds__(TJ * TK)
+__global__ void __launch_bounds__(TJ * TK, 3)
 k_restrict(const T* __restrict__ in, T* __restrict__ out, T* __restrict__ out2, int nin,
            XferGeom G, Phases P, int chunk0) {
     constexpr int NT = TJ * TK;
@@ -89,7 +89,9 @@ k_restrict(const T* __restrict__ in, T* __restrict__ out, T* __restrict__ out2, 
     // 4-byte: 32) and the R1 pitch that keeps a phase's two rows apart
     constexpr int PG = sizeof(T) == 16 ? 8 : (sizeof(T) == 8 ? 16 : 32);
     constexpr int HG = PG / 2;
-    constexpr int RP = TK + HG;
+    // (16-byte elements: pitch TK, which costs a two-way conflict on the R1
+    // writes but keeps three CTAs in the shared memory of an SM)
+    constexpr int RP = sizeof(T) == 16 ? TK : TK + HG;
     constexpr int S = D + 1;              // ring depth
     constexpr int NR = 2 * K - 1;         // axis-0 ring depth
     constexpr int NC = (FY * FZ + NT - 1) / NT;
@@ -147,22 +149,24 @@ k_restrict(const T* __restrict__ in, T* __restrict__ out, T* __restrict__ out2, 
         wrapside = ip >= G.g.n[0] ? 0 : (ip < 0 ? 1 : -1);
         return wrap_c(ip, G.g.n[0], G.g.periodic[0]);
     };
-    auto issue = [&](int j) {
+    // slot: j % S, kept by the caller as a running counter
+    auto issue = [&](int j, int slot) {
         int ip, ws;
         const bool pv = plane_info(j, ip, ws);
-        T* st = stage + (j % S) * SS;
-        const T* src = a + (long long)ip * n1 * n2;
+        T* st = stage + slot * SS;
+        // a plane outside a zero boundary copies nothing (size 0) from
+        // plane 0's cells, which always exist
+        const T* src = pv ? a + (long long)ip * n1 * n2 : a;
 #pragma unroll
         for (int i = 0; i < NC; i++) {
             if (tid + i * NT >= FY * FZ) break;
-            const bool ok = pv && ((vmask >> i) & 1);
-            cp_async_x<EB>(st + soff[i], ok ? src + goff[i] : a, ok);
+            cp_async_x<EB>(st + soff[i], src + goff[i], pv && ((vmask >> i) & 1));
         }
     };
-    auto fixup = [&](int j) {
+    auto fixup = [&](int j, int slot) {
         int ip, ws;
         plane_info(j, ip, ws);
-        T* st = stage + (j % S) * SS;
+        T* st = stage + slot * SS;
         const bool pw = cplx && ws >= 0 && G.g.periodic[0];
         if (!pw && !pcode) return;
         const double2 ph0 = ws == 0 ? P.ph[0][0] : P.ph[0][1];
@@ -182,18 +186,27 @@ k_restrict(const T* __restrict__ in, T* __restrict__ out, T* __restrict__ out2, 
     // axis-2 pass of plane t: R1[t & 1][y][k], centre at odd column K-1+2k.
     // Items come in blocks of two rows x TK columns; within a block, a bank
     // phase takes HG consecutive columns of both rows.
-    auto axis2 = [&](int t) {
-        const T* F = stage + (t % S) * SS;
-        T* R = R1 + (t & 1) * (FY * RP);
-        constexpr int NE = ((FY + 1) / 2) * 2 * TK;
+    constexpr int NE2 = ((FY + 1) / 2) * 2 * TK;
+    constexpr int NR2 = (NE2 + NT - 1) / NT;
+    int foff[NR2], roff[NR2];     // this thread's axis-2 items: stage / R1 offsets
+    unsigned imask = 0;
 #pragma unroll
-        for (int r = 0; r < (NE + NT - 1) / NT; r++) {
-            const int e = tid + r * NT;
-            const int j = e % (2 * TK);
-            const int k = (j / PG) * HG + j % HG;
-            const int y = 2 * (e / (2 * TK)) + (j / HG) % 2;
-            if ((NE % NT == 0 || e < NE) && y < FY) {
-                const T* f = F + y * FZ + K - 1 + 2 * k;
+    for (int r = 0; r < NR2; r++) {
+        const int e = tid + r * NT;
+        const int j = e % (2 * TK);
+        const int k = (j / PG) * HG + j % HG;
+        const int y = 2 * (e / (2 * TK)) + (j / HG) % 2;
+        foff[r] = y * FZ + K - 1 + 2 * k;
+        roff[r] = y * RP + k;
+        if ((NE2 % NT == 0 || e < NE2) && y < FY) imask |= 1u << r;
+    }
+    auto axis2 = [&](int t, int slot) {
+        const T* F = stage + slot * SS;
+        T* R = R1 + (t & 1) * (FY * RP);
+#pragma unroll
+        for (int r = 0; r < NR2; r++) {
+            if ((imask >> r) & 1) {
+                const T* f = F + foff[r];
                 T x = f[0];
 #pragma unroll
                 for (int l = 0; l < K / 2; l++)
@@ -201,12 +214,16 @@ k_restrict(const T* __restrict__ in, T* __restrict__ out, T* __restrict__ out2, 
                                                      G.w[l]));
                 // restrict(-a) == -restrict(a) bit for bit (every step is odd)
                 const T v = Num<T>::scale(x, 0.5);
-                R[y * RP + k] = G.neg_in ? Num<T>::neg(v) : v;
+                R[roff[r]] = G.neg_in ? Num<T>::neg(v) : v;
             }
         }
     };
     // axis-1 pass of plane t for this thread's (j, k), into the axis-0 ring;
-    // the axis-0 pass once the ring spans planes 2I .. 2I + 2K - 2
+    // the axis-0 pass once the ring spans planes 2I .. 2I + 2K - 2.  Planes
+    // enter in pairs (odd, even): an odd plane waits in `pend`; an even one
+    // shifts the ring by two and fills its last two entries, so the ring
+    // holds planes t - NR + 1 .. t whenever t is even.
+    T pend = Num<T>::zero();
     auto axis10 = [&](int t) {
         const T* R = R1 + (t & 1) * (FY * RP) + (K - 1 + 2 * tj) * RP + tk;
         T x = R[0];
@@ -215,10 +232,15 @@ k_restrict(const T* __restrict__ in, T* __restrict__ out, T* __restrict__ out2, 
             x = Num<T>::add(x, Num<T>::scale(Num<T>::add(R[(2 * l + 1) * RP],
                                                          R[-(2 * l + 1) * RP]),
                                              G.w[l]));
+        if (t & 1) {
+            pend = Num<T>::scale(x, 0.5);
+            return;
+        }
 #pragma unroll
-        for (int i = 0; i < NR - 1; i++) ring[i] = ring[i + 1];
+        for (int i = 0; i < NR - 2; i++) ring[i] = ring[i + 2];
+        ring[NR - 2] = pend;
         ring[NR - 1] = Num<T>::scale(x, 0.5);
-        if (t >= 2 * K - 2 && ((t - (2 * K - 2)) & 1) == 0) {
+        if (t >= 2 * K - 2) {
             const int I = I0 + (t - (2 * K - 2)) / 2;
             const int J = J0 + tj, L = L0 + tk;
             T y = ring[K - 1];
@@ -244,24 +266,29 @@ k_restrict(const T* __restrict__ in, T* __restrict__ out, T* __restrict__ out2, 
     // slot t % S by the axis-2 pass of plane t, both before barrier t.
 #pragma unroll 1
     for (int j = 0; j < D; j++) {
-        if (j < nx) issue(j);
+        if (j < nx) issue(j, j);
         cp_commit_x();
     }
     cp_wait_x<D - 1>();
-    fixup(0);
+    fixup(0, 0);
     __syncthreads();
-    if (D < nx) issue(D);
+    if (D < nx) issue(D, D);
     cp_commit_x();
-    axis2(0);
+    axis2(0, 0);
+    // ring slots of planes t and t + 1 (mod S), advanced each iteration
+    int s_t = 0, s_n = 1 % S;
 #pragma unroll 1
     for (int t = 0; t < nx; t++) {
         cp_wait_x<D - 1>();
-        if (t + 1 < nx) fixup(t + 1);
+        if (t + 1 < nx) fixup(t + 1, s_n);
         __syncthreads();
-        if (t + 1 + D < nx) issue(t + 1 + D);
+        // plane t + 1 + D goes into slot (t + 1 + D) % S = t % S
+        if (t + 1 + D < nx) issue(t + 1 + D, s_t);
         cp_commit_x();
-        if (t + 1 < nx) axis2(t + 1);
+        if (t + 1 < nx) axis2(t + 1, s_n);
         axis10(t);
+        s_t = s_n;
+        s_n = s_n + 1 == S ? 0 : s_n + 1;
     }
     cp_wait_x<0>();
 }
@@ -447,13 +474,15 @@ k_interpolate(const T* __restrict__ in, T* __restrict__ out, int nin, XferGeom G
 template <class T, int K>
 static int launch_restrict_k(const void* in, void* out, void* out2, int nin, const XferGeom& G,
                              const Phases& P, cudaStream_t st) {
-    // 16-byte elements: a square 16 x 16 tile; 8-byte: 8 x 32
+    // 16-byte elements: a square 16 x 16 tile; 8-byte: 8 x 32.  Complex
+    // stages are 27 KB: one plane ahead (two stages) leaves room for three
+    // CTAs an SM, which hides more latency than a deeper ring (measured).
     constexpr int TK = sizeof(T) == 16 ? 16 : 32;
     constexpr int TJ = 256 / TK;
-    constexpr int D = sizeof(T) == 16 ? 2 : 3;
+    constexpr int D = sizeof(T) == 16 ? 1 : 3;
     constexpr int H = 2 * K - 3, FY = 2 * TJ + H, FZ = 2 * TK + H;
     constexpr int SS = FY * FZ;
-    constexpr int RP = TK + (sizeof(T) == 16 ? 4 : (sizeof(T) == 8 ? 8 : 16));
+    constexpr int RP = TK + (sizeof(T) == 16 ? 0 : (sizeof(T) == 8 ? 8 : 16));
     constexpr size_t smem = ((size_t)(D + 1) * SS + (size_t)2 * FY * RP) * sizeof(T);
     static bool attr = false;
     if (!attr) {
