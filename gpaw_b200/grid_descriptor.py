@@ -55,6 +55,7 @@ class GridDescriptor:
                 str(n) for n in self.N_c))
         self.n_c = self.end_c - self.beg_c
         self.h_cv = self.cell_cv / self.N_c[:, np.newaxis]
+        self.icell_cv = np.linalg.inv(self.cell_cv).T
         self.volume = abs(np.linalg.det(self.cell_cv))
         self.dv = self.volume / self.N_c.prod()
         self.orthogonal = not (self.cell_cv -
@@ -107,6 +108,17 @@ class GridDescriptor:
         column 0 multiplies reads past the high edge, column 1 the low."""
         disp_cd = np.array([[1.0, -1.0]] * 3)
         return np.exp(2j * np.pi * disp_cd * np.asarray(kpt_c)[:, None])
+
+    def get_grid_point_distance_vectors(self, r_v, mic=True):
+        """Vectors from r_v to every grid point, minimum image along
+        periodic axes (gpaw/old/grid_descriptor.py:716-737); numpy."""
+        s_Gc = (np.indices(self.n_c, float).T + self.beg_c) / self.N_c
+        r_c = np.linalg.solve(self.cell_cv.T, r_v)
+        r_c = np.where(self.pbc_c, r_c % 1.0, r_c)
+        s_Gc -= np.where(self.pbc_c, r_c % 1.0, r_c)
+        if mic:
+            s_Gc -= self.pbc_c * (2 * s_Gc).astype(int)
+        return np.dot(s_Gc, self.cell_cv).T.copy()
 
     def get_grid_point_coordinates(self):
         idx = np.indices(self.n_c) + self.beg_c[:, None, None, None]

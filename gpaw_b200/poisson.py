@@ -149,8 +149,12 @@ class FDPoissonSolver:
             if zero_initial_phi:
                 phi.zero_()
             return self.solve_neutral(phi, rho - background)
+        if not self.gd.pbc_c.any():
+            return _solve_monopole(self, phi, rho, actual_charge,
+                                   zero_initial_phi)
         raise NotImplementedError(
-            'charged non-periodic system (Gaussian monopole removal)')
+            'charged system with mixed boundary conditions (dipole '
+            'correction / metallic electrodes)')
 
     def solve_neutral(self, phi, rho, timer=None):
         """gpaw/poisson.py:474-498 in the native executor."""
@@ -253,6 +257,28 @@ def stencil_spectrum(op, gd):
     return lmin, lmax
 
 
+def _solve_monopole(ps, phi, rho, actual_charge, zero_initial_phi):
+    """Charged system in a non-periodic cell (gpaw/poisson.py:233-283):
+    subtract a Gaussian carrying the charge, solve the neutral problem,
+    add the Gaussian's potential back.  The Gaussian and its potential are
+    computed once per grid (host, float64) and kept on the device."""
+    if getattr(ps, '_gauss_gd', None) is not ps.gd:
+        from .gauss import monopole_gaussian
+        rg, pg = monopole_gaussian(ps.gd)
+        ps.rho_gauss = torch.from_numpy(rg).to(phi.device)
+        ps.phi_gauss = torch.from_numpy(pg).to(phi.device)
+        ps._gauss_gd = ps.gd
+    q = actual_charge / np.sqrt(4 * pi)
+    rho_neutral = rho - q * ps.rho_gauss
+    if zero_initial_phi:
+        phi.zero_()
+    else:
+        phi -= q * ps.phi_gauss
+    niter = ps.solve_neutral(phi, rho_neutral)
+    phi += q * ps.phi_gauss
+    return niter
+
+
 class MixedPoissonSolver:
     """FP32 V-cycles inside FP64 defect correction (no counterpart in the
     reference, whose FDPoissonSolver is FP64 throughout).
@@ -330,8 +356,12 @@ class MixedPoissonSolver:
             if zero_initial_phi:
                 phi.zero_()
             return self.solve_neutral(phi, rho - background)
+        if not self.gd.pbc_c.any():
+            return _solve_monopole(self, phi, rho, actual_charge,
+                                   zero_initial_phi)
         raise NotImplementedError(
-            'charged non-periodic system (Gaussian monopole removal)')
+            'charged system with mixed boundary conditions (dipole '
+            'correction / metallic electrodes)')
 
     def solve_neutral(self, phi, rho, timer=None):
         rho = rho.contiguous()

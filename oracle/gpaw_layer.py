@@ -274,8 +274,33 @@ class Transformer:
         return output
 
 
+def gauss_l0(gd, a=19.0):
+    """Gaussian(gd).get_gauss(0) and .get_gauss_pot(0) with the centre in
+    the middle of the cell (gpaw/utilities/gauss.py:33-56, 94-123;
+    coordinates: gpaw/utilities/tools.py:81-100; distance vectors:
+    gpaw/old/grid_descriptor.py:716-737, no periodic axis here)."""
+    from scipy.special import erf
+    origin = 0.5 * gd.cell_cv.sum(0)
+    s_Gc = (np.indices(gd.n_c, float).T + gd.beg_c) / gd.N_c
+    r_c = np.linalg.solve(gd.cell_cv.T, origin)
+    r_c = np.where(gd.pbc_c, r_c % 1.0, r_c)
+    s_Gc -= np.where(gd.pbc_c, r_c % 1.0, r_c)
+    s_Gc -= gd.pbc_c * (2 * s_Gc).astype(int)
+    r_vG = np.dot(s_Gc, gd.cell_cv).T.copy()
+    r2 = np.sum(r_vG**2, axis=0)
+    r2 = np.where(r2 < 1e-12, 1e-12, r2)
+    r = np.sqrt(r2)
+    icell_cv = np.linalg.inv(gd.cell_cv).T
+    a = 4 * a * (icell_cv**2).sum(1).max()
+    exp_ar2 = np.exp(-a * r2)
+    rho = np.sqrt(a**3 * 4) / pi * exp_ar2
+    phi = 2.0 * 1.7724538509055159 * erf(np.sqrt(a) * r) / r
+    return rho, phi
+
+
 class FDPoissonSolver:
-    """gpaw/poisson.py:321-537 (neutral and periodic-charged branches)."""
+    """gpaw/poisson.py:321-537 (neutral, periodic-charged and non-periodic
+    charged (Gaussian monopole) branches)."""
 
     def __init__(self, nn=3, relax='J', eps=2e-10, maxiter=1000, be='auto'):
         self.nn = nn
@@ -347,7 +372,20 @@ class FDPoissonSolver:
             if zero_initial_phi:
                 phi[:] = 0.0
             return self.solve_neutral(phi, rho - background)
-        raise NotImplementedError('charged non-periodic system')
+        if not self.gd.pbc_c.any():
+            # :233-283 without use_charge_center: Gaussian monopole removal
+            if not hasattr(self, 'rho_gauss'):
+                self.rho_gauss, self.phi_gauss = gauss_l0(self.gd)
+            q = actual_charge / np.sqrt(4 * pi)
+            rho_neutral = rho - q * self.rho_gauss
+            if zero_initial_phi:
+                phi[:] = 0.0
+            else:
+                phi -= q * self.phi_gauss
+            niter = self.solve_neutral(phi, rho_neutral)
+            phi += q * self.phi_gauss
+            return niter
+        raise NotImplementedError('charged system, mixed boundaries')
 
     def solve_neutral(self, phi, rho):
         self._init()

@@ -476,3 +476,55 @@ def test_hamiltonian_random(nn, dtype, cuda):
         o = to_dev(np.zeros_like(p))
         kin.apply_potential(to_dev(p), o, to_dev(v), phh)
         assert np.array_equal(to_np(o), w)
+
+
+# ---------------------------------------- charged non-periodic Poisson
+def _charged_blob(gdo):
+    x = gdo.get_grid_point_coordinates()
+    L_ = np.diag(gdo.cell_cv)
+    rho = np.zeros(tuple(gdo.n_c))
+    for c, w, q in (((0.45, 0.5, 0.55), 1.1, 1.0), ((0.6, 0.4, 0.5), 0.9, 0.6),
+                    ((0.35, 0.6, 0.4), 1.3, -0.3)):
+        r2 = ((x - (np.array(c) * L_)[:, None, None, None])**2).sum(0)
+        rho += q * (np.pi * w**2)**-1.5 * np.exp(-r2 / w**2)
+    return rho                      # net charge +1.3
+
+
+def test_poisson_charged_nonperiodic(cuda):
+    """FDPoissonSolver.solve on a charged zero-boundary system (Gaussian
+    monopole removal, gpaw/poisson.py:233-283) against the reference."""
+    from gpaw_b200 import FDPoissonSolver
+    N, cell = (40, 36, 48), (10.0, 9.0, 12.0)
+    gdo = L.GridDescriptor(N, cell, 0)
+    gdp = prod_gd(N, cell, 0)
+    rho = _charged_blob(gdo)
+    assert abs(gdo.integrate(rho) - 1.3) < 1e-3
+    ps_o = L.FDPoissonSolver(nn=3, eps=1e-16)
+    ps_o.set_grid_descriptor(gdo)
+    phi_o = gdo.zeros()
+    n_o = ps_o.solve(phi_o, rho)
+    ps = FDPoissonSolver(nn=3, eps=1e-16)
+    ps.set_grid_descriptor(gdp)
+    phi = gdp.zeros()
+    n = ps.solve(phi, to_dev(rho))
+    assert n == n_o
+    # the charge is summed on the device (another order than numpy's), so
+    # agreement is to rounding, not bit for bit
+    assert max_rel(to_np(phi), phi_o) <= RTOL_FP64
+
+
+def test_mixed_poisson_charged_nonperiodic(cuda):
+    from gpaw_b200 import MixedPoissonSolver
+    N, cell = (48, 40, 48), (10.0, 9.0, 10.0)
+    gdo = L.GridDescriptor(N, cell, 0)
+    gdp = prod_gd(N, cell, 0)
+    rho = _charged_blob(gdo)
+    ps_o = L.FDPoissonSolver(nn=3, eps=1e-24)
+    ps_o.set_grid_descriptor(gdo)
+    phi_o = gdo.zeros()
+    ps_o.solve(phi_o, rho)
+    ps = MixedPoissonSolver(nn=3, tol=1e-11)
+    ps.set_grid_descriptor(gdp)
+    phi = gdp.zeros()
+    ps.solve(phi, to_dev(rho))
+    assert max_rel(to_np(phi), phi_o) < 1e-9

@@ -126,3 +126,16 @@ def test_hamiltonian_cases(golden):
         assert np.array_equal(out, c['out']), name
         n += 1
     assert n == 4
+
+
+def test_gauss_l0_carries_unit_charge():
+    """The monopole Gaussian holds sqrt(4 pi) of charge (so q g carries q
+    sqrt(4 pi) / sqrt(4 pi) = q) and its potential solves the Poisson
+    equation far from the centre: v(r) -> 2 sqrt(pi) / r."""
+    gd = L.GridDescriptor((40, 40, 40), (10.0, 10.0, 10.0), (0, 0, 0))
+    rho, phi = L.gauss_l0(gd)
+    assert abs(gd.integrate(rho) - np.sqrt(4 * np.pi)) < 1e-6
+    r_vG = gd.get_grid_point_coordinates() - 5.0
+    r = np.sqrt((r_vG**2).sum(0))
+    far = r > 6.0            # erfc(sqrt(a) r) < 1e-12 there
+    assert np.allclose(phi[far], 2 * np.sqrt(np.pi) / r[far], rtol=1e-9)
