@@ -162,3 +162,38 @@ def Laplace(gd, scale=1.0, n=1, dtype=float, xp=None):
     if n == 9:
         raise NotImplementedError('FFT Laplacian (n=9) is not provided')
     return GUCLaplace(gd, scale, n, dtype, xp=xp)
+
+
+class LaplaceA(FDOperator):
+    """O(h^4) Mehrstellen Laplacian, left-hand side (gpaw/fd_operators.py:
+    357-384): 19 points (centre, 6 faces, 12 edges); orthorhombic cells."""
+
+    def __init__(self, gd, scale, dtype=float, xp=None):
+        assert gd.orthogonal
+        c = np.divide(-1 / 12, gd.h_cv.diagonal()**2) * scale
+        c0 = c[1] + c[2]
+        c1 = c[0] + c[2]
+        c2 = c[1] + c[0]
+        a = -16.0 * np.sum(c)
+        b = 10.0 * c + 0.125 * a
+        super().__init__([a, b[0], b[0], b[1], b[1], b[2], b[2],
+                          c0, c0, c0, c0, c1, c1, c1, c1, c2, c2, c2, c2],
+                         [(0, 0, 0), (-1, 0, 0), (1, 0, 0), (0, -1, 0),
+                          (0, 1, 0), (0, 0, -1), (0, 0, 1),
+                          (0, -1, -1), (0, -1, 1), (0, 1, -1), (0, 1, 1),
+                          (-1, 0, -1), (-1, 0, 1), (1, 0, -1), (1, 0, 1),
+                          (-1, -1, 0), (-1, 1, 0), (1, -1, 0), (1, 1, 0)],
+                         gd, dtype, 'O(h^4) Mehrstellen Laplacian (A)', xp)
+
+
+class LaplaceB(FDOperator):
+    """Mehrstellen right-hand side B = 1/2 + 1/12 (6 faces)
+    (gpaw/fd_operators.py:387-396)."""
+
+    def __init__(self, gd, dtype=float, xp=None):
+        a = 0.5
+        b = 1.0 / 12.0
+        super().__init__([a, b, b, b, b, b, b],
+                         [(0, 0, 0), (-1, 0, 0), (1, 0, 0), (0, -1, 0),
+                          (0, 1, 0), (0, 0, -1), (0, 0, 1)],
+                         gd, dtype, 'O(h^4) Mehrstellen Laplacian (B)', xp)

@@ -62,12 +62,19 @@ class FDPoissonSolver:
         scaled by -1/(4 pi), 2 pre- and 1 post-sweep with weight 2/3; every
         coarser level (up to 8, until coarsen() fails) a 2nd-order Laplacian,
         4 + 4 sweeps, weight 1."""
-        if self.nn == 'M':
-            raise NotImplementedError('Mehrstellen stencil (nn="M")')
         self.gd = gd
         scale = -0.25 / pi
-        self.operators = [self.create_laplace(gd, scale, self.nn)]
-        self.B = None
+        if self.nn == 'M':
+            # :371-377: Mehrstellen A on level 0; B is applied to rho
+            from .fd_operators import LaplaceA, LaplaceB
+            if not gd.orthogonal:
+                raise RuntimeError('Cannot use Mehrstellen stencil with '
+                                   'non orthogonal cell.')
+            self.operators = [LaplaceA(gd, -scale)]
+            self.B = LaplaceB(gd)
+        else:
+            self.operators = [self.create_laplace(gd, scale, self.nn)]
+            self.B = None
         self.interpolators = []
         self.restrictors = []
         level = 0
@@ -156,10 +163,22 @@ class FDPoissonSolver:
             'charged system with mixed boundary conditions (dipole '
             'correction / metallic electrodes)')
 
+    def _rhs(self, rho):
+        """rho, or B rho for the Mehrstellen stencil (gpaw/poisson.py:
+        478-481); the B-applied copy lives in a buffer of the solver."""
+        rho = rho.contiguous()
+        if self.B is None:
+            return rho
+        if getattr(self, '_rhoB', None) is None or \
+                self._rhoB.device != rho.device:
+            self._rhoB = torch.empty_like(rho)
+        self.B.apply(rho, self._rhoB)
+        return self._rhoB
+
     def solve_neutral(self, phi, rho, timer=None):
         """gpaw/poisson.py:474-498 in the native executor."""
         self._init()
-        rho = rho.contiguous()
+        rho = self._rhs(rho)
         niter = C.c_int(0)
         err = C.c_double(0.0)
         rc = self._exec.lib.gb_poisson_solve_neutral(
@@ -176,6 +195,7 @@ class FDPoissonSolver:
         result() once the stream has reached this point.  ``rho`` must stay
         alive and unchanged until then."""
         self._init()
+        rho = self._rhs(rho)
         check(self._exec.lib.gb_poisson_solve_neutral_async(
             self._exec.h, C.c_void_p(phi.data_ptr()),
             C.c_void_p(rho.data_ptr()),
@@ -294,6 +314,9 @@ class MixedPoissonSolver:
 
     def __init__(self, nn=3, tol=1e-10, maxiter=200, levels=4,
                  coarse_accuracy=0.2):
+        if nn == 'M':
+            raise NotImplementedError(
+                'Mehrstellen stencil: use FDPoissonSolver(nn="M")')
         self.nn = nn
         self.tol = tol
         self.maxiter = maxiter

@@ -209,6 +209,37 @@ def Laplace(gd, scale=1.0, n=1, dtype=float, be='auto'):
     return FDOperator(coefs, offsets, gd, dtype, be=be)
 
 
+def _mehrstellen_a(gd, scale):
+    """LaplaceA's coefficients and offsets (gpaw/fd_operators.py:357-384)."""
+    c = np.divide(-1 / 12, gd.h_cv.diagonal()**2) * scale
+    c0 = c[1] + c[2]
+    c1 = c[0] + c[2]
+    c2 = c[1] + c[0]
+    a = -16.0 * np.sum(c)
+    b = 10.0 * c + 0.125 * a
+    coefs = [a, b[0], b[0], b[1], b[1], b[2], b[2],
+             c0, c0, c0, c0, c1, c1, c1, c1, c2, c2, c2, c2]
+    offsets = [(0, 0, 0), (-1, 0, 0), (1, 0, 0), (0, -1, 0), (0, 1, 0),
+               (0, 0, -1), (0, 0, 1),
+               (0, -1, -1), (0, -1, 1), (0, 1, -1), (0, 1, 1),
+               (-1, 0, -1), (-1, 0, 1), (1, 0, -1), (1, 0, 1),
+               (-1, -1, 0), (-1, 1, 0), (1, -1, 0), (1, 1, 0)]
+    return coefs, offsets
+
+
+def LaplaceA(gd, scale, dtype=float, be='auto'):
+    """O(h^4) Mehrstellen Laplacian, A (gpaw/fd_operators.py:357-384)."""
+    return FDOperator(*_mehrstellen_a(gd, scale), gd, dtype, be=be)
+
+
+def LaplaceB(gd, dtype=float, be='auto'):
+    """Mehrstellen right-hand-side operator B (:387-396)."""
+    b = 1.0 / 12.0
+    return FDOperator([0.5, b, b, b, b, b, b],
+                      [(0, 0, 0), (-1, 0, 0), (1, 0, 0), (0, -1, 0),
+                       (0, 1, 0), (0, 0, -1), (0, 0, 1)], gd, dtype, be=be)
+
+
 def transformer_geometry(gdin, gdout, nn):
     """Pads, neighbour pads and skip flags (gpaw/transformers.py:19-77)."""
     pad_cd = np.empty((3, 2), int)
@@ -314,7 +345,13 @@ class FDPoissonSolver:
     def set_grid_descriptor(self, gd):
         self.gd = gd
         scale = -0.25 / pi
-        self.operators = [Laplace(gd, scale, self.nn, be=self.be)]
+        if self.nn == 'M':
+            # :371-377: Mehrstellen A on level 0, B applied to rho
+            self.operators = [LaplaceA(gd, -scale, be=self.be)]
+            self.B = LaplaceB(gd, be=self.be)
+        else:
+            self.operators = [Laplace(gd, scale, self.nn, be=self.be)]
+            self.B = None
         self.interpolators = []
         self.restrictors = []
         level = 0
@@ -390,7 +427,10 @@ class FDPoissonSolver:
     def solve_neutral(self, phi, rho):
         self._init()
         self.phis[0] = phi
-        self.rhos[0][:] = rho
+        if self.B is None:
+            self.rhos[0][:] = rho
+        else:
+            self.B.apply(rho, self.rhos[0])
         niter = 1
         self.errors = []
         while self.iterate2(self.step) > self.eps and niter < self.maxiter:

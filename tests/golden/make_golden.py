@@ -57,6 +57,11 @@ def cases():
     for nn, bc, dt in ((3, 'p', 'c'), (3, 'z', 'f'), (2, 'm', 'c'),
                        (1, 'p', 'f')):
         out.append((f'ham_nn{nn}_{bc}_{dt}', ('ham', nn, bc, dt)))
+    # Mehrstellen operators and the nn='M' Poisson solver (appended last)
+    for bc, dt in (('p', 'f'), ('z', 'f'), ('m', 'c')):
+        out.append((f'mst_{bc}_{dt}', ('mst', 0, bc, dt)))
+    for bc in ('p', 'z'):
+        out.append((f'psM_{bc}', ('psM', 0, bc, 'f')))
     return out
 
 
@@ -133,6 +138,32 @@ def build(kind, nn, bc, dt, rng):
                  out=out)
         if ph is not None:
             d['phases'] = ph
+    elif kind == 'mst':
+        gd = L.GridDescriptor((10, 12, 9), (3.0, 3.3, 2.8), pbc)
+        a = rand((2,) + tuple(gd.n_c))
+        ph = gd.phase_factor_cd(KPT) if dtype == complex else None
+        oa = np.zeros_like(a)
+        ob = np.zeros_like(a)
+        L.LaplaceA(gd, 0.3, dtype, be='ref').apply(a, oa, ph)
+        L.LaplaceB(gd, dtype, be='ref').apply(a, ob, ph)
+        d.update(N=np.array(gd.N_c), pbc=np.array(pbc), inp=a, outA=oa,
+                 outB=ob)
+        if ph is not None:
+            d['phases'] = ph
+    elif kind == 'psM':
+        gd = L.GridDescriptor((16, 16, 8), (4.0, 4.0, 2.0), pbc)
+        x = gd.get_grid_point_coordinates()
+        rho = np.exp(-((x[0] - 2) ** 2 + (x[1] - 1.9) ** 2 +
+                       (x[2] - 1.1) ** 2) / 0.6) - \
+            np.exp(-((x[0] - 1.6) ** 2 + (x[1] - 2.3) ** 2 +
+                     (x[2] - 0.9) ** 2) / 0.6)
+        rho = rho - rho.mean()
+        ps = L.FDPoissonSolver(nn='M', eps=1e-18, be='ref')
+        ps.set_grid_descriptor(gd)
+        phi = gd.zeros()
+        niter = ps.solve(phi, rho)
+        d.update(N=np.array(gd.N_c), pbc=np.array(pbc), rho=rho, phi=phi,
+                 niter=np.array(niter), errors=np.array(ps.errors))
     elif kind == 'ps':
         gd = L.GridDescriptor((16, 8, 16), (4.0, 2.0, 4.0), pbc)
         x = gd.get_grid_point_coordinates()

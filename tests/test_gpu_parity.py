@@ -528,3 +528,32 @@ def test_mixed_poisson_charged_nonperiodic(cuda):
     phi = gdp.zeros()
     ps.solve(phi, to_dev(rho))
     assert max_rel(to_np(phi), phi_o) < 1e-9
+
+
+# ------------------------------------------------------------ Mehrstellen
+def test_golden_mehrstellen(golden, cuda):
+    """LaplaceA / LaplaceB (gpaw/fd_operators.py:357-396) and the
+    FDPoissonSolver(nn='M') branch, bit for bit."""
+    from gpaw_b200 import FDPoissonSolver
+    from gpaw_b200.fd_operators import LaplaceA, LaplaceB
+    n = 0
+    for name, c in golden.items():
+        if name.startswith('mst_'):
+            gd = prod_gd(tuple(c['N']), (3.0, 3.3, 2.8), tuple(c['pbc']))
+            dtype = complex if np.iscomplexobj(c['inp']) else float
+            a = to_dev(c['inp'])
+            oa, ob = a.new_zeros(a.shape), a.new_zeros(a.shape)
+            LaplaceA(gd, 0.3, dtype).apply(a, oa, c.get('phases'))
+            LaplaceB(gd, dtype).apply(a, ob, c.get('phases'))
+            assert np.array_equal(to_np(oa), c['outA']), name
+            assert np.array_equal(to_np(ob), c['outB']), name
+            n += 1
+        elif name.startswith('psM_'):
+            gd = prod_gd(tuple(c['N']), (4.0, 4.0, 2.0), tuple(c['pbc']))
+            ps = FDPoissonSolver(nn='M', eps=1e-18)
+            ps.set_grid_descriptor(gd)
+            phi = gd.zeros()
+            assert ps.solve(phi, to_dev(c['rho'])) == int(c['niter']), name
+            assert max_rel(to_np(phi), c['phi']) <= RTOL_FP64, name
+            n += 1
+    assert n == 5

@@ -139,3 +139,31 @@ def test_gauss_l0_carries_unit_charge():
     r = np.sqrt((r_vG**2).sum(0))
     far = r > 6.0            # erfc(sqrt(a) r) < 1e-12 there
     assert np.allclose(phi[far], 2 * np.sqrt(np.pi) / r[far], rtol=1e-9)
+
+
+def test_mehrstellen_cases(golden):
+    n = 0
+    for name, c in golden.items():
+        if name.startswith('mst_'):
+            gd = L.GridDescriptor(tuple(c['N']), (3.0, 3.3, 2.8),
+                                  tuple(c['pbc']))
+            dtype = complex if np.iscomplexobj(c['inp']) else float
+            oa = np.zeros_like(c['inp'])
+            ob = np.zeros_like(c['inp'])
+            L.LaplaceA(gd, 0.3, dtype, be='port').apply(c['inp'], oa,
+                                                        c.get('phases'))
+            L.LaplaceB(gd, dtype, be='port').apply(c['inp'], ob,
+                                                   c.get('phases'))
+            assert np.array_equal(oa, c['outA']), name
+            assert np.array_equal(ob, c['outB']), name
+            n += 1
+        elif name.startswith('psM_'):
+            gd = L.GridDescriptor(tuple(c['N']), (4.0, 4.0, 2.0),
+                                  tuple(c['pbc']))
+            ps = L.FDPoissonSolver(nn='M', eps=1e-18, be='port')
+            ps.set_grid_descriptor(gd)
+            phi = gd.zeros()
+            assert ps.solve(phi, c['rho']) == int(c['niter']), name
+            assert np.array_equal(phi, c['phi']), name
+            n += 1
+    assert n == 5
