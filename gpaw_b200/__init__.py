@@ -13,13 +13,15 @@ fd_precond).  All arrays are torch CUDA tensors; the arithmetic runs in the
 sm_100a kernels of ``libgpaw_b200.so`` (C ABI: include/gpaw_b200.h).
 """
 from .grid_descriptor import BadGridError, GridDescriptor
-from .fd_operators import FDOperator, GUCLaplace, Laplace
+from .fd_operators import (FDOperator, Gradient, GUCLaplace, Laplace,
+                           LaplaceA, LaplaceB)
 from .transformers import Transformer
 from .poisson import (FDPoissonSolver, MixedPoissonSolver,
                       PoissonConvergenceError)
 from .preconditioner import Preconditioner
 from .hamiltonian import FDHamiltonian
 
-__all__ = ['FDHamiltonian', 'GridDescriptor', 'BadGridError', 'FDOperator', 'GUCLaplace',
+__all__ = ['FDHamiltonian', 'Gradient', 'LaplaceA', 'LaplaceB',
+           'GridDescriptor', 'BadGridError', 'FDOperator', 'GUCLaplace',
            'Laplace', 'Transformer', 'FDPoissonSolver',
            'MixedPoissonSolver', 'PoissonConvergenceError', 'Preconditioner']

@@ -197,3 +197,74 @@ class LaplaceB(FDOperator):
                          [(0, 0, 0), (-1, 0, 0), (1, 0, 0), (0, -1, 0),
                           (0, 1, 0), (0, 0, -1), (0, 0, 1)],
                          gd, dtype, 'O(h^4) Mehrstellen Laplacian (B)', xp)
+
+
+# Central-difference first-derivative coefficients, orders 2..8
+# (gpaw/fd_operators.py:36-39).
+derivatives = [[1 / 2],
+               [2 / 3, -1 / 12],
+               [3 / 4, -3 / 20, 1 / 60],
+               [4 / 5, -1 / 5, 4 / 105, -1 / 280]]
+
+
+def find_neighbors_orthogonal(h_cv):
+    """Neighbour directions of an orthorhombic grid sorted by distance, as
+    gpaw/fd_operators.py:240-282 finds them (Voronoi ridges of the centre
+    of the 27-point block; an orthogonal basis is already Minkowski
+    reduced, so no reduction step)."""
+    from scipy.spatial import Voronoi
+    M_ib = np.indices((3, 3, 3)).reshape((3, -1)).T - 1
+    h_iv = M_ib.dot(h_cv)
+    voro = Voronoi(h_iv)
+    i_d = []
+    for i1, i2 in voro.ridge_points:
+        if i1 == 13 and i2 > 13:
+            i_d.append(i2)
+        elif i2 == 13 and i1 > 13:
+            i_d.append(i1)
+    h2_d = (h_iv[i_d]**2).sum(1)
+    return M_ib[[i_d[d] for d in h2_d.argsort()]]
+
+
+class Gradient(FDOperator):
+    """Symmetric finite-difference derivative along x, y or z
+    (gpaw/fd_operators.py:285-354), O(h^(2n)) error.  Orthorhombic cells:
+    the reference reduces general cells with ASE's Minkowski reduction,
+    which is not available here."""
+
+    def __init__(self, gd, v, scale=1.0, n=1, dtype=float, xp=None):
+        if not gd.orthogonal:
+            raise NotImplementedError(
+                'Gradient on a non-orthorhombic cell needs the Minkowski '
+                'reduction of the cell')
+        M_dc = find_neighbors_orthogonal(gd.h_cv)
+        h_dv = M_dc @ gd.h_cv
+        D = len(h_dv)
+        invh_vc = np.linalg.inv(gd.h_cv)
+        n_cv = (invh_vc / (invh_vc**2).sum(axis=0)**0.5).T
+        coef_cd = np.zeros((3, D))
+        for c, n_v in enumerate(n_cv):
+            ok_d = abs(h_dv.dot(n_v)) > 1e-10
+            h_mv = h_dv[ok_d]
+            A_jm = np.array([h_mv.dot(n_v),
+                             h_mv.dot(gd.h_cv[c - 1]),
+                             h_mv.dot(gd.h_cv[c - 2])])
+            U_jm, S_m, V_mm = np.linalg.svd(A_jm, full_matrices=False)
+            coef_m = V_mm.T.dot(np.diag(S_m**-1).dot(U_jm.T.dot([1, 0, 0])))
+            coef_cd[c, ok_d] = coef_m
+        coef_d = np.linalg.inv(n_cv)[v].dot(coef_cd) * scale
+        offsets = []
+        coefs = []
+        stencil = np.array(derivatives[n - 1])
+        for d, c in enumerate(coef_d):
+            if abs(c) < 1e-10:
+                continue
+            M_c = M_dc[d]
+            offsets.extend(np.arange(1, n + 1)[:, np.newaxis] * M_c)
+            coefs.extend(c * stencil)
+            offsets.extend(np.arange(-1, -n - 1, -1)[:, np.newaxis] * M_c)
+            coefs.extend(-c * stencil)
+        super().__init__(coefs, offsets, gd, dtype, xp=xp)
+        self.description = (
+            'Finite-difference {}-derivative with O(h^{}) error ({} points)'
+            .format('xyz'[v], 2 * n, self.npoints))

@@ -557,3 +557,28 @@ def test_golden_mehrstellen(golden, cuda):
             assert max_rel(to_np(phi), c['phi']) <= RTOL_FP64, name
             n += 1
     assert n == 5
+
+
+@pytest.mark.parametrize('n', [1, 2, 3, 4])
+def test_gradient_polynomial_exact(n, cuda):
+    """The order-2n central difference differentiates polynomials of degree
+    <= 2n exactly (away from the zero boundary); the stencil runs through
+    the generic kernel against the oracle's apply of the same stencil."""
+    from gpaw_b200.fd_operators import Gradient
+    N, cell = (24, 20, 28), (4.8, 4.0, 5.6)
+    gd = prod_gd(N, cell, 0)
+    gref = L.GridDescriptor(N, cell, 0)
+    x = gref.get_grid_point_coordinates()
+    f = 0.3 * x[0]**2 * x[1] - 0.2 * x[2]**2 + x[1] * x[2]
+    df = [0.6 * x[0] * x[1], 0.3 * x[0]**2 + x[2], -0.4 * x[2] + x[1]]
+    m = 2 * n
+    for v in range(3):
+        gr = Gradient(gd, v, 1.0, n)
+        want = np.zeros_like(f)
+        L.FDOperator(gr.coef_p, gr.offset_pc, gref).apply(f, want)
+        out = to_dev(np.zeros_like(f))
+        gr.apply(to_dev(f), out)
+        got = to_np(out)
+        assert np.array_equal(got, want)
+        inner = (slice(m, -m),) * 3
+        assert np.allclose(got[inner], df[v][inner], rtol=1e-9, atol=1e-9)
