@@ -297,17 +297,16 @@ k_restrict(const T* __restrict__ in, T* __restrict__ out, T* __restrict__ out2, 
 // IP1D (c/bmgs/interpolate.cpp:10-46): raw fine index u along an axis maps
 // to coarse base m = K/2 - 1 + u/2 in the padded input; even u copies a[m],
 // odd u gives sum_j w_j (a[m - j] + a[m + 1 + j]).  Fine index f = u - skip0.
+// One interpolated value from a column of padded input `c` (stride apart):
+// the even fine point copies c[0]; the odd one is
+// sum_j w_j (c[-j] + c[1 + j]) in IP1D's order.
 template <class T, int K>
-__device__ __forceinline__ T ip_tap(const T* row, int stride, int u, int base, const double* w) {
-    const int i = u >> 1;
-    const int m = K / 2 - 1 + i - base;
-    if ((u & 1) == 0) return row[m * stride];
-    T x = Num<T>::scale(Num<T>::add(row[m * stride], row[(m + 1) * stride]), w[0]);
+__device__ __forceinline__ T ip_value(const T* c, int stride, bool odd, const double* w) {
+    if (!odd) return c[0];
+    T x = Num<T>::scale(Num<T>::add(c[0], c[stride]), w[0]);
 #pragma unroll
     for (int j = 1; j < K / 2; j++)
-        x = Num<T>::add(x, Num<T>::scale(Num<T>::add(row[(m - j) * stride],
-                                                     row[(m + 1 + j) * stride]),
-                                         w[j]));
+        x = Num<T>::add(x, Num<T>::scale(Num<T>::add(c[-j * stride], c[(1 + j) * stride]), w[j]));
     return x;
 }
 
@@ -321,6 +320,7 @@ k_interpolate(const T* __restrict__ in, T* __restrict__ out, int nin, XferGeom G
     constexpr int SS = CY * CZ;
     constexpr int S = D + 1;
     constexpr int NC = (SS + NT - 1) / NT;
+    constexpr int NQ = (CY * TK + NT - 1) / NT;   // axis-2 items per thread
     constexpr int EB = (int)sizeof(T);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* stage = reinterpret_cast<T*>(smem_raw);
@@ -369,6 +369,28 @@ k_interpolate(const T* __restrict__ in, T* __restrict__ out, int nin, XferGeom G
     }
     if (!cplx) pcode = 0;
 
+    // This thread's axis-2 items (row y, fine column k of the tile): raw
+    // fine index u = F2 + k + skip0 maps to coarse base m = K/2 - 1 + u/2
+    // (IP1D, c/bmgs/interpolate.cpp:10-46) in the stage row; parity of u
+    // picks copy or taps.  Fixed for the whole march.
+    int qsrc[NQ], qdst[NQ];
+    unsigned qodd = 0, qok = 0;
+#pragma unroll
+    for (int r = 0; r < NQ; r++) {
+        const int e = tid + r * NT;
+        const int y = e / TK, k = e % TK;
+        const int u = F2 + k + G.skip0[2];
+        qsrc[r] = y * CZ + K / 2 - 1 + (u >> 1) - base2;
+        qdst[r] = y * TK + k;
+        if (u & 1) qodd |= 1u << r;
+        if (e < CY * TK) qok |= 1u << r;
+    }
+    // the axis-1 value of this thread's fine row F1 + tj from Q's column tk
+    const int u1 = F1 + tj + G.skip0[1];
+    const int qcol = (K / 2 - 1 + (u1 >> 1) - base1) * TK + tk;
+    const bool odd1 = u1 & 1;
+    const bool row_ok = F1 + tj < G.nout[1];
+
     // coarse padded planes ia .. min(s0-1, ib-1+K-1)
     const int nx = min(G.s[0] - 1, ib - 1 + K - 1) - ia + 1;
     auto plane_info = [&](int j, int& ip, int& ws) {
@@ -376,25 +398,24 @@ k_interpolate(const T* __restrict__ in, T* __restrict__ out, int nin, XferGeom G
         ws = ip >= G.g.n[0] ? 0 : (ip < 0 ? 1 : -1);
         return wrap_c(ip, G.g.n[0], G.g.periodic[0]);
     };
-    auto issue = [&](int j) {
+    auto issue = [&](int j, int slot) {
         int ip, ws;
         const bool pv = plane_info(j, ip, ws);
-        T* st = stage + (j % S) * SS;
-        const T* src = a + (long long)ip * n1 * n2;
+        T* st = stage + slot * SS;
+        const T* src = pv ? a + (long long)ip * n1 * n2 : a;
 #pragma unroll
         for (int i = 0; i < NC; i++) {
             if (tid + i * NT >= SS) break;
-            const bool ok = pv && ((vmask >> i) & 1);
-            cp_async_x<EB>(st + soff[i], ok ? src + goff[i] : a, ok);
+            cp_async_x<EB>(st + soff[i], src + goff[i], pv && ((vmask >> i) & 1));
         }
     };
-    auto fixup = [&](int j) {
+    auto fixup = [&](int j, int slot) {
         int ip, ws;
         plane_info(j, ip, ws);
         const bool pw = cplx && ws >= 0 && G.g.periodic[0];
         if (!pw && !pcode) return;
         const double2 ph0 = ws == 0 ? P.ph[0][0] : P.ph[0][1];
-        T* st = stage + (j % S) * SS;
+        T* st = stage + slot * SS;
 #pragma unroll
         for (int i = 0; i < NC; i++) {
             if (tid + i * NT >= SS) break;
@@ -408,11 +429,14 @@ k_interpolate(const T* __restrict__ in, T* __restrict__ out, int nin, XferGeom G
 #pragma unroll
     for (int i = 0; i < K; i++) ring[i] = Num<T>::zero();
     const int f1 = F1 + tj, f2 = F2 + tk;
-    const bool inside = f1 < G.nout[1] && f2 < G.nout[2];
+    const bool inside = row_ok && f2 < G.nout[2];
+    // this thread's output column; fine plane f0 adds f0 * plane stride
+    T* ocol = o + (long long)f1 * G.nout[2] + f2;
+    const long long pstride = (long long)G.nout[1] * G.nout[2];
     auto emit = [&](int u, T v) {
         const int f0 = u - G.skip0[0];
         if (inside && f0 >= 0 && f0 < G.nout[0]) {
-            T* dst = o + ((long long)f0 * G.nout[1] + f1) * G.nout[2] + f2;
+            T* dst = ocol + f0 * pstride;
             // accumulate: phi -= I(phi_coarse) (gpaw/poisson.py:520-521)
             *dst = G.accumulate ? Num<T>::sub(*dst, v) : v;
         }
@@ -420,29 +444,31 @@ k_interpolate(const T* __restrict__ in, T* __restrict__ out, int nin, XferGeom G
 
 #pragma unroll 1
     for (int j = 0; j < D; j++) {
-        if (j < nx) issue(j);
+        if (j < nx) issue(j, j);
         cp_commit_x();
     }
+    int slot = 0;   // t % S
 #pragma unroll 1
     for (int t = 0; t < nx; t++) {
         cp_wait_x<D - 1>();
-        fixup(t);
+        fixup(t, slot);
         __syncthreads();
-        if (t + D < nx) issue(t + D);
+        // plane t + D goes into slot (t + D) % S = (t - 1) % S
+        if (t + D < nx) issue(t + D, slot == 0 ? S - 1 : slot - 1);
         cp_commit_x();
-        const T* A = stage + (t % S) * SS;
-        for (int e = tid; e < CY * TK; e += NT) {
-            const int y = e / TK, k = e % TK;
-            const int u = F2 + k + G.skip0[2];
-            T v = (F2 + k < G.nout[2]) ? ip_tap<T, K>(A + y * CZ, 1, u, base2, G.w)
-                                        : Num<T>::zero();
-            Q[y * TK + k] = G.neg_in ? Num<T>::neg(v) : v;
+        const T* A = stage + slot * SS;
+#pragma unroll
+        for (int r = 0; r < NQ; r++) {
+            if ((qok >> r) & 1) {
+                const int k = (tid + r * NT) % TK;
+                T v = (F2 + k < G.nout[2]) ? ip_value<T, K>(A + qsrc[r], 1, (qodd >> r) & 1, G.w)
+                                            : Num<T>::zero();
+                Q[qdst[r]] = G.neg_in ? Num<T>::neg(v) : v;
+            }
         }
         __syncthreads();
         {
-            const int u = F1 + tj + G.skip0[1];
-            T v = (F1 + tj < G.nout[1]) ? ip_tap<T, K>(Q + tk, TK, u, base1, G.w)
-                                        : Num<T>::zero();
+            T v = row_ok ? ip_value<T, K>(Q + qcol, TK, odd1, G.w) : Num<T>::zero();
 #pragma unroll
             for (int i = 0; i < K - 1; i++) ring[i] = ring[i + 1];
             ring[K - 1] = v;
@@ -466,6 +492,7 @@ k_interpolate(const T* __restrict__ in, T* __restrict__ out, int nin, XferGeom G
             const int il = ib - 1;
             if (il >= ia && il == x0 - (K - 2)) emit(2 * il, ring[K / 2]);
         }
+        slot = slot + 1 == S ? 0 : slot + 1;
     }
     cp_wait_x<0>();
 }
