@@ -22,6 +22,7 @@ from __future__ import annotations
 
 import collections
 import dataclasses
+import gc
 import time
 from math import pi
 
@@ -218,6 +219,19 @@ class Server:
         pending = list(reqs)
         active = []
         torch.cuda.synchronize()
+        # no garbage-collector pauses inside the loop (it allocates little:
+        # per-request bookkeeping only)
+        gc_was_on = gc.isenabled()
+        gc.collect()
+        gc.disable()
+        try:
+            return self._serve(pending, active, inputs, outputs)
+        finally:
+            if gc_was_on:
+                gc.enable()
+
+    def _serve(self, pending, active, inputs, outputs):
+        reqs = list(pending)
         t0 = time.perf_counter()
         while pending or active:
             now = time.perf_counter() - t0
