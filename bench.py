@@ -664,7 +664,7 @@ def run_gpu(args):
         'cpu_baseline': cpu_base,
     }
     # FD Hamiltonian local part on the same batch: kin(psi) + v psi fused
-    if rank == 0 or world == 1:
+    if (rank == 0 or world == 1) and not args.no_ham:
         from gpaw_b200 import FDHamiltonian
         ham = FDHamiltonian(gd, kin_stencil=3, dtype=complex)
         vt = torch.randn(tuple(gd.n_c), dtype=torch.float64, device=dev)
@@ -718,6 +718,8 @@ def main():
     p.add_argument('--no-poisson', action='store_true')
     p.add_argument('--no-batch', action='store_true')
     p.add_argument('--no-serving', action='store_true')
+    p.add_argument('--no-ham', action='store_true',
+                   help='skip the fused Hamiltonian section')
     p.add_argument('--poisson-only', default=None,
                    choices=['c1', 'c3', 'c4', 'pc', 'c5'],
                    help='run one Poisson configuration only (profiling)')
