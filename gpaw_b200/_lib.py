@@ -59,6 +59,12 @@ SIGNATURES = {
                                C.POINTER(_p), _dp, C.c_double, C.c_int,
                                C.POINTER(_p)]),
     'gb_mixed_free': (None, [_p]),
+    'gb_mixed_batch_new': (C.c_int, [C.c_int, C.POINTER(_p), C.c_double,
+                                     C.c_int, C.POINTER(_p)]),
+    'gb_mixed_batch_free': (None, [_p]),
+    'gb_mixed_batch_solve_async': (C.c_int, [_p, C.POINTER(_p),
+                                             C.POINTER(_p), _p]),
+    'gb_mixed_batch_result': (C.c_int, [_p, C.POINTER(C.c_int), _dp]),
     'gb_mixed_solve_async': (C.c_int, [_p, _p, _p, C.c_double, C.c_int, _p]),
     'gb_mixed_result': (C.c_int, [_p, C.POINTER(C.c_int), _dp]),
     'gb_poisson_solve_neutral_async': (C.c_int, [_p, _p, _p, C.c_double,

@@ -2,23 +2,28 @@
 one GPU.
 
 Each grid gets its own solver: its own device-resident level hierarchy,
-buffers and captured CUDA graph (the whole V-cycle loop runs on the device,
-see gb_poisson_* / gb_mixed_*).  A batch enqueues every solve on one of
-``nstreams`` CUDA streams without any host synchronisation, so solves of
-small grids — each far too small to fill a B200 alone — run side by side;
-one synchronisation at the end reads all results.
+buffers and captured V-cycle loop (the whole solve runs on the device, see
+gb_poisson_* / gb_mixed_*).  A mixed-precision batch is, by default, ONE
+CUDA graph with a branch per grid (gb_mixed_batch_*): a single launch runs
+every solve, the branches side by side.  Otherwise (FP64, or graph=False)
+the batch enqueues every solve on one of ``nstreams`` CUDA streams.  Either
+way there is no host synchronisation until the results are read.
 """
 from __future__ import annotations
 
 import numpy as np
 import torch
 
+import ctypes as C
+
+from ._lib import check
+from .cgpaw import _stream
 from .poisson import FDPoissonSolver, MixedPoissonSolver
 
 
 class PoissonBatch:
     def __init__(self, gds, nn=3, tol=1e-10, precision='mixed', nstreams=16,
-                 maxiter=400, levels=4):
+                 maxiter=400, levels=4, graph=True):
         if precision not in ('mixed', 'fp64'):
             raise ValueError("precision must be 'mixed' or 'fp64'")
         self.gds = list(gds)
@@ -37,6 +42,21 @@ class PoissonBatch:
         dev = self.gds[0].device if self.gds else torch.device('cuda')
         self.streams = [torch.cuda.Stream(device=dev)
                         for _ in range(max(1, nstreams))]
+        self._batch = None
+        if precision == 'mixed' and graph and self.solvers:
+            lib = self.solvers[0]._h.lib
+            hs = (C.c_void_p * len(self.solvers))(
+                *[ps._h.h for ps in self.solvers])
+            h = C.c_void_p()
+            check(lib.gb_mixed_batch_new(len(self.solvers), hs, float(tol),
+                                         int(maxiter), C.byref(h)))
+            self._batch = (lib, h)
+
+    def __del__(self):
+        b = getattr(self, '_batch', None)
+        if b is not None and b[1].value:
+            b[0].gb_mixed_batch_free(b[1])
+            self._batch = None
 
     def prepare(self, rhos):
         """FP64 batches stop at ||L phi - rho|| <= tol ||rho|| through the
@@ -52,6 +72,18 @@ class PoissonBatch:
             raise ValueError('one phi and one rho per grid')
         if self.precision == 'fp64' and getattr(self, '_eps', None) is None:
             self.prepare(rhos)
+        if self._batch is not None:
+            lib, h = self._batch
+            n = len(self.solvers)
+            for ps, phi, rho in zip(self.solvers, phis, rhos):
+                if not (phi.is_contiguous() and rho.is_contiguous()) or \
+                        tuple(phi.shape) != tuple(ps.gd.n_c):
+                    raise ValueError('contiguous arrays of each grid\'s shape')
+            pp = (C.c_void_p * n)(*[p.data_ptr() for p in phis])
+            rr = (C.c_void_p * n)(*[r.data_ptr() for r in rhos])
+            self._keep = (phis, rhos)
+            check(lib.gb_mixed_batch_solve_async(h, pp, rr, _stream()))
+            return
         cur = torch.cuda.current_stream()
         for st in self.streams:
             st.wait_stream(cur)
@@ -67,6 +99,13 @@ class PoissonBatch:
     def results(self):
         """V-cycle counts (after the enqueued work completed)."""
         torch.cuda.synchronize()
+        if self._batch is not None:
+            lib, h = self._batch
+            n = len(self.solvers)
+            ni = (C.c_int * n)()
+            rel = (C.c_double * n)()
+            check(lib.gb_mixed_batch_result(h, ni, rel))
+            return list(ni)
         return [ps.result() for ps in self.solvers]
 
     def solve(self, phis, rhos):

@@ -666,3 +666,242 @@ extern "C" int gb_mixed_solve(gb_mixed* m, double* phi, const double* rho, doubl
     GB_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
     return gb_mixed_result(m, niter, rel_residual);
 }
+
+// --------------------------------------------------------------- batches
+// Many mixed-precision solves (grids of any sizes) as ONE CUDA graph:
+//   copy-in kernel (every solver's phi and rho into its buffers)
+//   -> per solver a branch  |rho|^2 -> init -> defect -> check ->
+//      WHILE { V-cycle; defect; check } -> control block to the host
+//   -> copy-out kernel (every phi back)
+// The branches are independent, so the graph runs the solves concurrently;
+// one launch replaces a stream of per-solve launches.  The caller's array
+// addresses live in a device table that one copy refreshes before each
+// launch.
+struct gb_mixed_batch {
+    std::vector<gb_mixed*> s;
+    double tol = 0.0;
+    int maxiter = 0;
+    int n = 0;
+    double** d_user = nullptr;     // [2n]: phi_i, rho_i (caller's arrays)
+    double** h_user = nullptr;     // pinned host copy of the table
+    double** d_own = nullptr;      // [2n]: phi0_i, rho0_i (solver buffers)
+    long long* d_len = nullptr;    // [n] points of grid i
+    cudaStream_t cap = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    ~gb_mixed_batch() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (cap) cudaStreamDestroy(cap);
+        cudaFree(d_user);
+        cudaFree(d_own);
+        cudaFree(d_len);
+        if (h_user) cudaFreeHost(h_user);
+    }
+};
+
+namespace {
+
+// in: phi0_i = phi_i, rho0_i = rho_i; out: phi_i = phi0_i (blockIdx.y = i)
+__global__ void k_batch_copy(int n, double* const* user, double* const* own,
+                             const long long* len, int out) {
+    const int i = blockIdx.y;
+    if (i >= n) return;
+    const long long m = len[i];
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long j0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (out) {
+        double* dst = user[2 * i];
+        const double* src = own[2 * i];
+        for (long long j = j0; j < m; j += stride) dst[j] = src[j];
+    } else {
+        for (int k = 0; k < 2; k++) {
+            double* dst = own[2 * i + k];
+            const double* src = user[2 * i + k];
+            for (long long j = j0; j < m; j += stride) dst[j] = src[j];
+        }
+    }
+}
+
+// the single node a capture has produced since its last dependency set
+int capture_tail(cudaStream_t cs, cudaGraphNode_t* tail) {
+    cudaStreamCaptureStatus stat;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    GB_CUDA_TRY(cudaStreamGetCaptureInfo(cs, &stat, nullptr, nullptr, &deps, &ndeps));
+    if (stat != cudaStreamCaptureStatusActive || ndeps != 1)
+        return fail(GB_ECUDA, "mixed batch: unexpected capture state (%zu tail nodes)", ndeps);
+    *tail = deps[0];
+    return 0;
+}
+
+// one solver's branch after `root`; *wnode receives its WHILE node
+int add_branch(gb_mixed_batch* bt, cudaGraph_t G, gb_mixed* m, cudaGraphNode_t root,
+               cudaGraphNode_t* wnode) {
+    cudaStream_t cs = bt->cap;
+    const long long n = m->op64->ng();
+    cudaGraphConditionalHandle h;
+    GB_CUDA_TRY(cudaGraphConditionalHandleCreate(&h, G, 0, 0));
+    GB_CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, G, &root, nullptr, 1,
+                                              cudaStreamCaptureModeThreadLocal));
+    const int nb = (int)std::min<long long>(1024, (n + 255) / 256);
+    k_sumsq<<<nb, 256, 0, cs>>>(m->rho0, n, m->partial);
+    launch_reduce_partials(m->partial, nb, 1, 1.0, m->nrm + 1, cs);
+    k_mixed_init<<<1, 1, 0, cs>>>(m->ctl, m->nrm + 1, bt->tol, bt->maxiter);
+    int rc = defect(m, cs);
+    if (!rc) k_mixed_check<<<1, 1, 0, cs>>>(m->ctl, m->nrm, 0, h);
+    cudaGraphNode_t tail = nullptr;
+    if (!rc) rc = capture_tail(cs, &tail);
+    cudaGraph_t gout = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(cs, &gout);
+    if (rc) return rc;
+    if (ce != cudaSuccess) return fail(GB_ECUDA, "mixed batch: capture: %s", cudaGetErrorString(ce));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    GB_CUDA_TRY(cudaGraphAddNode(wnode, G, &tail, 1, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    GB_CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0,
+                                              cudaStreamCaptureModeThreadLocal));
+    rc = vcycle32(m, 0, cs);
+    if (!rc) rc = defect(m, cs);
+    if (!rc) k_mixed_check<<<1, 1, 0, cs>>>(m->ctl, m->nrm, 1, h);
+    ce = cudaStreamEndCapture(cs, &gout);
+    if (rc) return rc;
+    if (ce != cudaSuccess)
+        return fail(GB_ECUDA, "mixed batch: capture of the V-cycle: %s", cudaGetErrorString(ce));
+    cudaGraphNode_t co;
+    GB_CUDA_TRY(cudaGraphAddMemcpyNode1D(&co, G, wnode, 1, m->ctl_host, m->ctl, sizeof(Ctl),
+                                         cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+int build_batch(gb_mixed_batch* bt) {
+    const int n = bt->n;
+    long long maxlen = 0;
+    std::vector<double*> own(2 * n);
+    std::vector<long long> len(n);
+    for (int i = 0; i < n; i++) {
+        own[2 * i] = bt->s[i]->phi0;
+        own[2 * i + 1] = bt->s[i]->rho0;
+        len[i] = bt->s[i]->op64->ng();
+        maxlen = std::max(maxlen, len[i]);
+    }
+    GB_CUDA_TRY(cudaMalloc(&bt->d_user, 2 * n * sizeof(double*)));
+    GB_CUDA_TRY(cudaMalloc(&bt->d_own, 2 * n * sizeof(double*)));
+    GB_CUDA_TRY(cudaMalloc(&bt->d_len, n * sizeof(long long)));
+    GB_CUDA_TRY(cudaMallocHost(&bt->h_user, 2 * n * sizeof(double*)));
+    GB_CUDA_TRY(cudaMemcpy(bt->d_own, own.data(), 2 * n * sizeof(double*),
+                           cudaMemcpyHostToDevice));
+    GB_CUDA_TRY(cudaMemcpy(bt->d_len, len.data(), n * sizeof(long long),
+                           cudaMemcpyHostToDevice));
+    cudaGraph_t G;
+    GB_CUDA_TRY(cudaGraphCreate(&G, 0));
+    const dim3 cgrid((unsigned)std::min<long long>(64, (maxlen + 255) / 256), (unsigned)n);
+    cudaStream_t cs = bt->cap;
+    int rc = 0;
+    cudaGraphNode_t root = nullptr;
+    std::vector<cudaGraphNode_t> whiles(n);
+    cudaError_t ce = cudaStreamBeginCaptureToGraph(cs, G, nullptr, nullptr, 0,
+                                                   cudaStreamCaptureModeThreadLocal);
+    if (ce == cudaSuccess) {
+        k_batch_copy<<<cgrid, 256, 0, cs>>>(n, bt->d_user, bt->d_own, bt->d_len, 0);
+        rc = capture_tail(cs, &root);
+        cudaGraph_t gout = nullptr;
+        const cudaError_t e2 = cudaStreamEndCapture(cs, &gout);
+        if (!rc && e2 != cudaSuccess)
+            rc = fail(GB_ECUDA, "mixed batch: capture: %s", cudaGetErrorString(e2));
+    } else {
+        rc = fail(GB_ECUDA, "mixed batch: capture: %s", cudaGetErrorString(ce));
+    }
+    for (int i = 0; i < n && !rc; i++) rc = add_branch(bt, G, bt->s[i], root, &whiles[i]);
+    if (!rc) {
+        ce = cudaStreamBeginCaptureToGraph(cs, G, whiles.data(), nullptr, n,
+                                           cudaStreamCaptureModeThreadLocal);
+        if (ce == cudaSuccess) {
+            k_batch_copy<<<cgrid, 256, 0, cs>>>(n, bt->d_user, bt->d_own, bt->d_len, 1);
+            cudaGraph_t gout = nullptr;
+            ce = cudaStreamEndCapture(cs, &gout);
+        }
+        if (ce != cudaSuccess)
+            rc = fail(GB_ECUDA, "mixed batch: capture: %s", cudaGetErrorString(ce));
+    }
+    if (!rc) {
+        ce = cudaGraphInstantiate(&bt->exec, G, 0);
+        if (ce != cudaSuccess)
+            rc = fail(GB_ECUDA, "mixed batch: instantiate: %s", cudaGetErrorString(ce));
+    }
+    cudaGraphDestroy(G);
+    return rc;
+}
+
+}  // namespace
+
+extern "C" int gb_mixed_batch_new(int n, gb_mixed* const* solvers, double tol, int maxiter,
+                                  gb_mixed_batch** out) {
+    if (!out || !solvers || n < 1) return fail(GB_EINVAL, "mixed batch: bad arguments");
+    if (maxiter < 1) return fail(GB_EINVAL, "mixed batch: maxiter must be >= 1");
+    if (n > 65535) return fail(GB_EINVAL, "mixed batch: at most 65535 solvers");
+    *out = nullptr;
+    for (int i = 0; i < n; i++) {
+        if (!solvers[i]) return fail(GB_EINVAL, "mixed batch: NULL solver %d", i);
+        for (int j = 0; j < i; j++)
+            if (solvers[j] == solvers[i])
+                return fail(GB_EINVAL, "mixed batch: solver %d appears twice", i);
+        // one uncaptured pass of every kernel (sets kernel attributes)
+        if (!solvers[i]->exec)
+            if (int rc = build_mixed_graph(solvers[i])) return rc;
+    }
+    gb_mixed_batch* bt = new gb_mixed_batch();
+    bt->tol = tol;
+    bt->maxiter = maxiter;
+    bt->n = n;
+    bt->s.assign(solvers, solvers + n);
+    cudaError_t e = cudaStreamCreateWithFlags(&bt->cap, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete bt;
+        return fail(GB_ECUDA, "mixed batch: stream: %s", cudaGetErrorString(e));
+    }
+    if (int rc = build_batch(bt)) {
+        delete bt;
+        return rc;
+    }
+    *out = bt;
+    return 0;
+}
+
+extern "C" void gb_mixed_batch_free(gb_mixed_batch* bt) { delete bt; }
+
+extern "C" int gb_mixed_batch_solve_async(gb_mixed_batch* bt, double* const* phis,
+                                          const double* const* rhos, void* stream) {
+    if (!bt || !phis || !rhos) return fail(GB_EINVAL, "mixed batch solve: NULL argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    // the previous launch on this stream may still read the table
+    GB_CUDA_TRY(cudaStreamSynchronize(st));
+    for (int i = 0; i < bt->n; i++) {
+        if (!phis[i] || !rhos[i]) return fail(GB_EINVAL, "mixed batch solve: NULL array %d", i);
+        bt->h_user[2 * i] = phis[i];
+        bt->h_user[2 * i + 1] = const_cast<double*>(rhos[i]);
+        bt->s[i]->last_tol = bt->tol;
+        bt->s[i]->last_maxiter = bt->maxiter;
+    }
+    GB_CUDA_TRY(cudaMemcpyAsync(bt->d_user, bt->h_user, 2 * bt->n * sizeof(double*),
+                                cudaMemcpyHostToDevice, st));
+    GB_CUDA_TRY(cudaGraphLaunch(bt->exec, st));
+    return 0;
+}
+
+extern "C" int gb_mixed_batch_result(gb_mixed_batch* bt, int* niters, double* rel_residuals) {
+    if (!bt) return fail(GB_EINVAL, "mixed batch result: NULL batch");
+    int bad = -1;
+    for (int i = 0; i < bt->n; i++) {
+        const Ctl* c = bt->s[i]->ctl_host;
+        if (niters) niters[i] = c->niter;
+        if (rel_residuals) rel_residuals[i] = c->rel;
+        if (c->rel > bt->tol && bad < 0) bad = i;
+    }
+    if (bad >= 0)
+        return fail(GB_ENOCONV, "mixed batch: solve %d did not reach %g in %d V-cycles", bad,
+                    bt->tol, bt->maxiter);
+    return 0;
+}

@@ -247,6 +247,26 @@ GB_API int gb_mixed_solve_async(gb_mixed* m, double* phi, const double* rho, dou
                                 int maxiter, void* stream);
 GB_API int gb_mixed_result(gb_mixed* m, int* niter, double* rel_residual);
 
+/* Many mixed-precision solves as one CUDA graph (no reference counterpart):
+ * one branch per solver (distinct solvers, grids of any sizes), each the
+ * solve of gb_mixed_solve_async with tolerance `tol` and at most `maxiter`
+ * V-cycles; the branches run concurrently.  gb_mixed_batch_solve_async
+ * takes one phi and one rho per solver (device arrays of that solver's
+ * grid), enqueues the whole batch with one graph launch and returns;
+ * gb_mixed_batch_result (after the stream reached that point) fills
+ * niters[n] and rel_residuals[n] and returns GB_ENOCONV if any solve
+ * stopped at maxiter.  The solvers must outlive the batch and must not be
+ * used on their own while a batch launch is in flight.  A new launch first
+ * waits for the stream's earlier work (the launch refreshes a table of
+ * array addresses the previous one may still read). */
+typedef struct gb_mixed_batch gb_mixed_batch;
+GB_API int gb_mixed_batch_new(int n, gb_mixed* const* solvers, double tol, int maxiter,
+                              gb_mixed_batch** out);
+GB_API void gb_mixed_batch_free(gb_mixed_batch* b);
+GB_API int gb_mixed_batch_solve_async(gb_mixed_batch* b, double* const* phis,
+                                      const double* const* rhos, void* stream);
+GB_API int gb_mixed_batch_result(gb_mixed_batch* b, int* niters, double* rel_residuals);
+
 #ifdef __cplusplus
 }
 #endif
