@@ -320,7 +320,11 @@ k_interpolate(const T* __restrict__ in, T* __restrict__ out, int nin, XferGeom G
     constexpr int SS = CY * CZ;
     constexpr int S = D + 1;
     constexpr int NC = (SS + NT - 1) / NT;
-    constexpr int NQ = (CY * TK + NT - 1) / NT;   // axis-2 items per thread
+    // axis-2 items per thread: each warp takes items of one parity of the
+    // fine index (copies or taps), so its lanes never diverge
+    constexpr int NW = NT / 32;
+    constexpr int NIP = CY * (TK / 2);                  // items per parity
+    constexpr int NQ = (NIP + (NW / 2) * 32 - 1) / ((NW / 2) * 32);
     constexpr int EB = (int)sizeof(T);
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* stage = reinterpret_cast<T*>(smem_raw);
@@ -341,7 +345,13 @@ k_interpolate(const T* __restrict__ in, T* __restrict__ out, int nin, XferGeom G
     const T* a = in + b * ngin;
     T* o = out + b * ngout;
     const int tid = threadIdx.x;
-    const int tj = tid / TK, tk = tid % TK;
+    const int lane = tid & 31, wid = tid >> 5;
+    // fine row of this thread: a warp's rows share the parity of their
+    // fine index (two rows a warp for 16-wide tiles, one for 32-wide)
+    int tj;
+    if constexpr (TK == 16) tj = 4 * (wid >> 1) + (wid & 1) + 2 * (lane >> 4);
+    else tj = wid;
+    const int tk = lane & (TK - 1);
     const bool cplx = sizeof(T) == 16 && P.use;
 
     // coarse footprint origin along axes 1 and 2
@@ -374,16 +384,22 @@ k_interpolate(const T* __restrict__ in, T* __restrict__ out, int nin, XferGeom G
     // (IP1D, c/bmgs/interpolate.cpp:10-46) in the stage row; parity of u
     // picks copy or taps.  Fixed for the whole march.
     int qsrc[NQ], qdst[NQ];
-    unsigned qodd = 0, qok = 0;
+    unsigned qok = 0;
+    // warps 0 .. NW/2-1: fine index even; the others: odd
+    const bool qodd = wid >= NW / 2;
+    {
+        const int s2 = G.skip0[2] & 1;
+        const int c = qodd ? 1 - s2 : s2;       // column parity with that u parity
 #pragma unroll
-    for (int r = 0; r < NQ; r++) {
-        const int e = tid + r * NT;
-        const int y = e / TK, k = e % TK;
-        const int u = F2 + k + G.skip0[2];
-        qsrc[r] = y * CZ + K / 2 - 1 + (u >> 1) - base2;
-        qdst[r] = y * TK + k;
-        if (u & 1) qodd |= 1u << r;
-        if (e < CY * TK) qok |= 1u << r;
+        for (int r = 0; r < NQ; r++) {
+            const int j = (wid % (NW / 2)) * 32 + lane + r * (NW / 2) * 32;
+            const int y = j / (TK / 2), kk = j % (TK / 2);
+            const int k = 2 * kk + c;
+            const int u = F2 + k + G.skip0[2];
+            qsrc[r] = y * CZ + K / 2 - 1 + (u >> 1) - base2;
+            qdst[r] = y * TK + k;
+            if (j < NIP && F2 + k < G.nout[2]) qok |= 1u << r;
+        }
     }
     // the axis-1 value of this thread's fine row F1 + tj from Q's column tk
     const int u1 = F1 + tj + G.skip0[1];
@@ -460,9 +476,7 @@ k_interpolate(const T* __restrict__ in, T* __restrict__ out, int nin, XferGeom G
 #pragma unroll
         for (int r = 0; r < NQ; r++) {
             if ((qok >> r) & 1) {
-                const int k = (tid + r * NT) % TK;
-                T v = (F2 + k < G.nout[2]) ? ip_value<T, K>(A + qsrc[r], 1, (qodd >> r) & 1, G.w)
-                                            : Num<T>::zero();
+                const T v = ip_value<T, K>(A + qsrc[r], 1, qodd, G.w);
                 Q[qdst[r]] = G.neg_in ? Num<T>::neg(v) : v;
             }
         }
