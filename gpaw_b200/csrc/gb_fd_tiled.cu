@@ -191,6 +191,7 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
         return;
     }
     const long long ng = (long long)n0 * n1 * n2;
+    const long long pstride = (long long)n1 * n2;   // one plane
     const T* a = in + b * ng;
     T* o = out + b * ng;
     const T* aux = (const T*)ep.aux + b * ng;
@@ -199,6 +200,9 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
     const int tx = tid % TX;
     const int ty0 = (tid / TX) * RY;
     const int gx = x0 + tx;
+    long long colr[RY];      // in-plane offset of this thread's rows
+#pragma unroll
+    for (int r = 0; r < RY; r++) colr[r] = (long long)(y0 + ty0 + r) * n2 + gx;
 
     // -- async copy of relative plane j (absolute pa + j) ------------------
     // Rows -NN..TY+NN-1 at columns 0..TX-1, and rows 0..TY-1 of the two
@@ -251,7 +255,7 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
         int pl = pa + j;
         const bool pvalid = wrap_coord(pl, n0, g.periodic[0]);
         T* st = ring + slot * (PX * PY);
-        const T* src = a + (long long)pl * n1 * n2;
+        const T* src = a + pl * pstride;
 #pragma unroll
         for (int i = 0; i < NC; i++) {
             if (tid + i * NT >= NMID + NSIDE) break;
@@ -330,7 +334,7 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
             pa2[r] = Num<T>::zero();
             pac[r] = 0.0;
             if (p < pb && gx < n2 && gy < n1) {
-                const long long at = ((long long)p * n1 + gy) * n2 + gx;
+                const long long at = p * pstride + colr[r];
                 if constexpr (MODE == EPI_POT) pac[r] = vpot[at];
                 else if (NEED_AUX && ep.aux) pa1[r] = aux[at];
                 if constexpr (MODE == EPI_LIN) {
@@ -399,7 +403,7 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
                                          [&](int d) { return q[r][(CU + Q - d) % Q]; });
                 const int gy = y0 + ty0 + r;
                 if (gx < n2 && gy < n1) {
-                    const long long at = ((long long)p * n1 + gy) * n2 + gx;
+                    const long long at = p * pstride + colr[r];
                     if (MODE == EPI_APPLY) {
                         o[at] = x;
                     } else if (MODE == EPI_POT) {
