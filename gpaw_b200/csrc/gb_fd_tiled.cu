@@ -164,7 +164,7 @@ template <class T, int NN, int TX, int TY, int RY, int D, int MODE, int ORD>
 __global__ void __launch_bounds__(TX * (TY / RY),
                                   (sizeof(T) == 16 && NN <= 3 &&
                                    (MODE == EPI_APPLY || MODE == EPI_POT))
-                                      ? 3
+                                      ? 4
                                       : (512 / (TX * (TY / RY))))
 k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phases P,
          CfdStencil cs, int chunk0, int tiles_x, Epi ep) {
@@ -497,7 +497,7 @@ static int launch_cfd_nn(const void* in, void* out, int nin, const GridBC& g, co
         // (nn = 3) let three CTAs share an SM; measured faster than 32 x 16
         // tiles of two rows a thread at two CTAs an SM (the rows' shared
         // axis-1 loads do not make up for the lost warps)
-        constexpr int D = NN <= 3 ? 3 : 2;
+        constexpr int D = NN <= 3 ? 2 : 2;
         if constexpr (MODE == EPI_APPLY && NN == 3)
             if (fused_apply())
                 return launch_cfd_t<T, NN, 32, 8, 1, D, MODE, 2>(in, out, nin, g, P, cs, ep, st,
