@@ -680,16 +680,19 @@ def run_gpu(args):
             'what': 'kin(psi) + v psi, 256 x 96^3 complex128, one kernel',
             'ms': ht * 1e3, 'gbs': hb / ht / 1e9,
             'vs_apply_alone': ht / apply_t}
-    # CPU references of the Poisson path: rank 0 at N = 1 only
+    # CPU references of the Poisson path: rank 0 at N = 1 only.  The
+    # Poisson, batch and serving sections are single-GPU configurations:
+    # they run at N = 1 (the scaling runs time the C2 step alone).
     cpu_ok = not args.no_cpu and rank == 0 and world == 1
-    if not args.no_poisson:
+    single = world == 1
+    if not args.no_poisson and single:
         line['poisson'] = {'c1': poisson_c1(dev, cpu=cpu_ok),
                            'c3': poisson_c3(dev)}
-    if not args.no_batch:
+    if not args.no_batch and single:
         line.setdefault('poisson', {})['c4_batch'] = poisson_c4(dev,
                                                                 cpu=cpu_ok)
         line['preconditioner_c4'] = precond_c4(dev)
-    if not args.no_serving:
+    if not args.no_serving and single:
         # in a fresh process: the host-driven loop's latencies should not
         # depend on what this process did before (measured: they do)
         line['serving_c5'] = serving_subprocess()
