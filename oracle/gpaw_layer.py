@@ -533,3 +533,44 @@ class FDHamiltonian:
         self.kin.apply(psit_nR, out, phase_cd)
         for p, o in zip(psit_nR, out):
             o += p * vt_R
+
+
+def calculate_dipole_moment(gd, rho_g):
+    """gpaw/old/grid_descriptor.py:648-663 (center=False, no origin)."""
+    r_cz = [np.arange(gd.beg_c[c], gd.end_c[c]) for c in range(3)]
+    rho_01 = rho_g.sum(axis=2)
+    rho_02 = rho_g.sum(axis=1)
+    rho_cz = [rho_01.sum(axis=1), rho_01.sum(axis=0), rho_02.sum(axis=0)]
+    rhog_c = [np.dot(r_cz[c], rho_cz[c]) for c in range(3)]
+    return -np.dot(rhog_c, gd.h_cv) * gd.dv
+
+
+def dipole_correction(c, gd, rhot_g):
+    """gpaw/dipole_correction.py:125-172 (center=False)."""
+    from scipy.special import erf
+    moment = calculate_dipole_moment(gd, rhot_g)[c]
+    if abs(moment) < 1e-12:
+        return gd.zeros(), gd.zeros(), 0.0
+    r_g = gd.get_grid_point_coordinates()[c]
+    cellsize = abs(gd.cell_cv[c, c])
+    sr_g = 2.0 / cellsize * r_g - 1.0
+    alpha = 12.0
+    drho_g = sr_g * np.exp(-alpha * sr_g**2)
+    moment2 = calculate_dipole_moment(gd, drho_g)[c]
+    factor = -moment / moment2
+    drho_g *= factor
+    phifactor = factor * (np.pi / alpha)**1.5 * cellsize**2 / 4.0
+    dphi_g = -phifactor * erf(sr_g * np.sqrt(alpha))
+    return drho_g, dphi_g, phifactor
+
+
+def dipole_fdsolve(poissonsolver, c, vHt_g, rhot_g, zero_vacuum=False):
+    """DipoleCorrection.fdsolve (gpaw/dipole_correction.py:84-92)."""
+    drhot_g, dvHt_g, correction = dipole_correction(c, poissonsolver.gd,
+                                                    rhot_g)
+    if zero_vacuum:
+        dvHt_g += correction
+    vHt_g -= dvHt_g
+    iters = poissonsolver.solve(vHt_g, rhot_g + drhot_g)
+    vHt_g += dvHt_g
+    return iters

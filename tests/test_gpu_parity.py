@@ -582,3 +582,30 @@ def test_gradient_polynomial_exact(n, cuda):
         assert np.array_equal(got, want)
         inner = (slice(m, -m),) * 3
         assert np.allclose(got[inner], df[v][inner], rtol=1e-9, atol=1e-9)
+
+
+# ------------------------------------------------------- dipole correction
+def test_dipole_correction_slab(cuda):
+    """A neutral slab with a dipole along z (periodic in x and y, zero
+    boundary along z): DipoleCorrection around FDPoissonSolver against the
+    reference's wrapper around its own solver."""
+    from gpaw_b200 import FDPoissonSolver
+    from gpaw_b200.dipole import DipoleCorrection
+    N, cell, pbc = (24, 24, 48), (5.0, 5.0, 12.0), (1, 1, 0)
+    go = L.GridDescriptor(N, cell, pbc)
+    gp = prod_gd(N, cell, pbc)
+    x = go.get_grid_point_coordinates()
+    rho = np.exp(-((x[2] - 5.0)**2) / 0.8) - np.exp(-((x[2] - 7.0)**2) / 0.8)
+    rho = rho * (1.0 + 0.2 * np.cos(2 * np.pi * x[0] / 5.0))
+    rho -= rho.mean()
+    po = L.FDPoissonSolver(nn=3, eps=1e-20)
+    po.set_grid_descriptor(go)
+    want = go.zeros()
+    n_o = L.dipole_fdsolve(po, 2, want, rho)
+    ps = DipoleCorrection(FDPoissonSolver(nn=3, eps=1e-20), 2)
+    ps.set_grid_descriptor(gp)
+    phi = gp.zeros()
+    n = ps.solve(phi, to_dev(rho))
+    assert n == n_o
+    assert max_rel(to_np(phi), want) <= RTOL_FP64
+    assert abs(ps.correction) > 0

@@ -146,3 +146,19 @@ def test_cgpaw_objects_build_without_gpu():
     with pytest.raises(NotImplementedError):
         cgpaw.Operator(coefs, offp, gd.n_c, 3, gd.neighbor_cd, 1, object(),
                        1)
+
+
+def test_dipole_moment_matches_oracle():
+    """The dipole moment of the product's wrapper (numpy path) equals the
+    restatement of the reference's grid method."""
+    import numpy as np
+    from gpaw_b200 import GridDescriptor
+    from gpaw_b200.dipole import calculate_dipole_moment
+    from oracle import gpaw_layer as L
+    rng = np.random.default_rng(5)
+    for pbc in ((0, 0, 0), (1, 1, 0)):
+        gd = GridDescriptor((12, 10, 14), (3.0, 2.5, 3.5), pbc, device='cpu')
+        go = L.GridDescriptor((12, 10, 14), (3.0, 2.5, 3.5), pbc)
+        rho = rng.standard_normal(tuple(go.n_c))
+        assert np.array_equal(calculate_dipole_moment(gd, rho),
+                              L.calculate_dipole_moment(go, rho))
