@@ -55,6 +55,7 @@ SIGNATURES = {
                                  C.POINTER(C.c_int), _dp, C.c_int,
                                  C.c_double, C.POINTER(_p)]),
     'gb_poisson_free': (None, [_p]),
+    'gb_poisson_fused_levels': (C.c_int, [_p]),
     'gb_mixed_new': (C.c_int, [C.c_int, _p, C.POINTER(_p), C.POINTER(_p),
                                C.POINTER(_p), _dp, C.c_double, C.c_int,
                                C.POINTER(_p)]),

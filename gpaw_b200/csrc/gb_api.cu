@@ -429,8 +429,242 @@ __global__ void k_solve_init(SolveCtl* ctl, double eps, int maxiter) {
     ctl->err = 0.0;
 }
 
+// ------------------------------------------------ fused coarse-level V-cycle
+// The coarse levels of a multigrid hierarchy hold a few thousand points or
+// fewer, so each of their sweeps, residuals and transfers is one short
+// launch.  When every level from `lf` down is small, one CTA runs the whole
+// V-cycle below lf (iterate2 from level lf on, gpaw/poisson.py:500-537)
+// with all arrays in shared memory: weighted-Jacobi sweeps, the residual,
+// the K = 2 restriction and interpolation (three separable passes each, axis
+// 2, then 1, then 0, as bmgs_restrict / bmgs_interpolate order them,
+// c/bmgs/restrict.cpp:137-156, c/bmgs/interpolate.cpp:70-99).  Every value
+// is computed with the same operations in the same order as the per-level
+// kernels, so the V-cycle is bit-identical to them.
+namespace gb {
+constexpr int TAIL_MAX = 8;
+struct TailLevel {
+    int n[3];
+    int per[3];
+    int ng;
+    int phi, rho, tmp;        // offsets (doubles) of this level's arrays
+    double c0, cp[3], cm[3];  // 2nd-order stencil: direction k runs along axis 2 - k
+    int pre, post;
+    double w;
+    int rplo[3];              // restriction to the next level: input padding
+    double rw;                //   and mid-point weight
+    int iplo[3], iskip[3];    // interpolation from the next level: padding, skip
+    double iw;
+};
+struct TailPlan {
+    int nl;        // levels handled (lf .. L)
+    int scratch;   // offset of the transfer passes' intermediate arrays
+    TailLevel lv[TAIL_MAX];
+};
+
+// index along one axis after the boundary condition; -1 reads zero
+__device__ __forceinline__ int tail_at(int j, int n, int per) {
+    if (j >= 0 && j < n) return j;
+    if (!per) return -1;
+    j = j < 0 ? j + n : j - n;
+    return (j >= 0 && j < n) ? j : -1;
+}
+
+// value of A at (i0, i1, i2) moved by d along axis ax
+__device__ __forceinline__ double tail_nb(const double* A, const TailLevel& L, int i0, int i1,
+                                          int i2, int ax, int d) {
+    int i[3] = {i0, i1, i2};
+    const int j = tail_at(i[ax] + d, L.n[ax], L.per[ax]);
+    if (j < 0) return 0.0;
+    i[ax] = j;
+    return A[(i[0] * L.n[1] + i[1]) * L.n[2] + i[2]];
+}
+
+// x = 0 (+ v c0) + v(+1) c(+1) + v(-1) c(-1) per direction, axis 2, 1, 0
+__device__ __forceinline__ double tail_stencil(const double* A, const TailLevel& L, int i0, int i1,
+                                               int i2, bool centre) {
+    double x = 0.0;
+    if (centre) x = __dadd_rn(x, __dmul_rn(A[(i0 * L.n[1] + i1) * L.n[2] + i2], L.c0));
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const int ax = 2 - k;
+        x = __dadd_rn(x, __dmul_rn(tail_nb(A, L, i0, i1, i2, ax, 1), L.cp[k]));
+        x = __dadd_rn(x, __dmul_rn(tail_nb(A, L, i0, i1, i2, ax, -1), L.cm[k]));
+    }
+    return x;
+}
+
+// one weighted-Jacobi sweep src -> dst (c/bmgs/relax.cpp:41-65)
+__device__ void tail_jacobi(double* sm, const TailLevel& L, int src, int dst) {
+    const double* A = sm + src;
+    const double* R = sm + L.rho;
+    double* B = sm + dst;
+    const double w1 = 1.0 - L.w;
+    for (int i = threadIdx.x; i < L.ng; i += blockDim.x) {
+        const int i2 = i % L.n[2], t = i / L.n[2];
+        const int i1 = t % L.n[1], i0 = t / L.n[1];
+        const double x = tail_stencil(A, L, i0, i1, i2, false);
+        B[i] = __dadd_rn(__dmul_rn(w1, A[i]), __ddiv_rn(__dmul_rn(L.w, __dsub_rn(R[i], x)), L.c0));
+    }
+    __syncthreads();
+}
+
+// weighted-Jacobi sweeps of phi (held in *cur); the result lands in *cur
+__device__ void tail_relax(double* sm, const TailLevel& L, int& cur, int& alt, int n) {
+    for (int it = 0; it < n; it++) {
+        tail_jacobi(sm, L, cur, alt);
+        const int t = cur;
+        cur = alt;
+        alt = t;
+    }
+}
+
+// mid-point restriction of one line value, K = 2: 0.5 (a + w (a+ + a-))
+__device__ __forceinline__ double tail_r1(double a, double ap, double am, double w) {
+    return __dmul_rn(0.5, __dadd_rn(a, __dmul_rn(w, __dadd_rn(ap, am))));
+}
+
+// restriction of A (level F, extents n) into out (level C, extents m)
+__device__ void tail_restrict(double* sm, const TailLevel& F, const TailLevel& C, const double* A,
+                              double* out, double* tA, double* tB) {
+    const int n0 = F.n[0], n1 = F.n[1], n2 = F.n[2];
+    const int m0 = C.n[0], m1 = C.n[1], m2 = C.n[2];
+    // axis 2: (n0, n1, m2)
+    for (int i = threadIdx.x; i < n0 * n1 * m2; i += blockDim.x) {
+        const int c = i % m2, r = i / m2;
+        const int j = 2 * c + 1 - F.rplo[2];
+        const double* row = A + r * n2;
+        const int j0 = tail_at(j, n2, F.per[2]), jp = tail_at(j + 1, n2, F.per[2]),
+                  jm = tail_at(j - 1, n2, F.per[2]);
+        tA[i] = tail_r1(j0 < 0 ? 0.0 : row[j0], jp < 0 ? 0.0 : row[jp], jm < 0 ? 0.0 : row[jm],
+                        F.rw);
+    }
+    __syncthreads();
+    // axis 1: (n0, m1, m2)
+    for (int i = threadIdx.x; i < n0 * m1 * m2; i += blockDim.x) {
+        const int c2 = i % m2, t = i / m2;
+        const int c1 = t % m1, i0 = t / m1;
+        const int j = 2 * c1 + 1 - F.rplo[1];
+        const int j0 = tail_at(j, n1, F.per[1]), jp = tail_at(j + 1, n1, F.per[1]),
+                  jm = tail_at(j - 1, n1, F.per[1]);
+        const double* col = tA + i0 * n1 * m2 + c2;
+        tB[i] = tail_r1(j0 < 0 ? 0.0 : col[j0 * m2], jp < 0 ? 0.0 : col[jp * m2],
+                        jm < 0 ? 0.0 : col[jm * m2], F.rw);
+    }
+    __syncthreads();
+    // axis 0: (m0, m1, m2)
+    for (int i = threadIdx.x; i < m0 * m1 * m2; i += blockDim.x) {
+        const int r = i % (m1 * m2), c0 = i / (m1 * m2);
+        const int j = 2 * c0 + 1 - F.rplo[0];
+        const int j0 = tail_at(j, n0, F.per[0]), jp = tail_at(j + 1, n0, F.per[0]),
+                  jm = tail_at(j - 1, n0, F.per[0]);
+        const double* col = tB + r;
+        out[i] = tail_r1(j0 < 0 ? 0.0 : col[j0 * m1 * m2], jp < 0 ? 0.0 : col[jp * m1 * m2],
+                         jm < 0 ? 0.0 : col[jm * m1 * m2], F.rw);
+    }
+    __syncthreads();
+}
+
+// interpolated value at fine index f of one line a(.) of length n (coarse
+// level with its boundary condition): the even output copies, the odd one
+// is w (a(k) + a(k+1)) (c/bmgs/interpolate.cpp:10-46, K = 2)
+template <class GET>
+__device__ __forceinline__ double tail_i1(int f, int skip, int plo, int n, int per, double w,
+                                          GET get) {
+    const int u = f + skip;
+    const int k = u >> 1;
+    const int j = tail_at(k - plo, n, per);
+    const double a = j < 0 ? 0.0 : get(j);
+    if (!(u & 1)) return a;
+    const int j1 = tail_at(k + 1 - plo, n, per);
+    return __dmul_rn(w, __dadd_rn(a, j1 < 0 ? 0.0 : get(j1)));
+}
+
+// phi (level F, extents n) -= interpolation of B (level C, extents m)
+__device__ void tail_interp_sub(const TailLevel& F, const TailLevel& C, const double* B,
+                                double* phi, double* tA, double* tB) {
+    const int n0 = F.n[0], n1 = F.n[1], n2 = F.n[2];
+    const int m0 = C.n[0], m1 = C.n[1], m2 = C.n[2];
+    // axis 2: (m0, m1, n2)
+    for (int i = threadIdx.x; i < m0 * m1 * n2; i += blockDim.x) {
+        const int f = i % n2, r = i / n2;
+        const double* row = B + r * m2;
+        tA[i] = tail_i1(f, F.iskip[2], F.iplo[2], m2, C.per[2], F.iw,
+                        [&](int j) { return row[j]; });
+    }
+    __syncthreads();
+    // axis 1: (m0, n1, n2)
+    for (int i = threadIdx.x; i < m0 * n1 * n2; i += blockDim.x) {
+        const int f2 = i % n2, t = i / n2;
+        const int f1 = t % n1, c0 = t / n1;
+        const double* col = tA + c0 * m1 * n2 + f2;
+        tB[i] = tail_i1(f1, F.iskip[1], F.iplo[1], m1, C.per[1], F.iw,
+                        [&](int j) { return col[j * n2]; });
+    }
+    __syncthreads();
+    // axis 0: (n0, n1, n2), subtracted from phi
+    for (int i = threadIdx.x; i < n0 * n1 * n2; i += blockDim.x) {
+        const int r = i % (n1 * n2), f0 = i / (n1 * n2);
+        const double* col = tB + r;
+        const double v = tail_i1(f0, F.iskip[0], F.iplo[0], m0, C.per[0], F.iw,
+                                 [&](int j) { return col[j * n1 * n2]; });
+        phi[i] = __dsub_rn(phi[i], v);
+    }
+    __syncthreads();
+}
+
+// The V-cycle from level lf down: rho_g is that level's right-hand side,
+// phi_g receives its correction (the level starts from zero).
+__global__ void __launch_bounds__(1024, 1)
+k_tail_vcycle(const double* __restrict__ rho_g, double* __restrict__ phi_g, TailPlan plan) {
+    extern __shared__ __align__(16) double tail_sm[];
+    double* sm = tail_sm;
+    const TailLevel& L0 = plan.lv[0];
+    for (int i = threadIdx.x; i < L0.ng; i += blockDim.x) {
+        sm[L0.rho + i] = rho_g[i];
+        sm[L0.phi + i] = 0.0;
+    }
+    __syncthreads();
+    int cur[TAIL_MAX], alt[TAIL_MAX];
+    double* tA = sm + plan.scratch;
+    const int last = plan.nl - 1;
+    for (int l = 0; l < last; l++) {
+        const TailLevel& L = plan.lv[l];
+        const TailLevel& C = plan.lv[l + 1];
+        cur[l] = L.phi;
+        alt[l] = L.tmp;
+        tail_relax(sm, L, cur[l], alt[l], L.pre);
+        // residual L phi - rho into the free buffer
+        for (int i = threadIdx.x; i < L.ng; i += blockDim.x) {
+            const int i2 = i % L.n[2], t = i / L.n[2];
+            const int i1 = t % L.n[1], i0 = t / L.n[1];
+            const double x = tail_stencil(sm + cur[l], L, i0, i1, i2, true);
+            sm[alt[l] + i] = __dsub_rn(x, sm[L.rho + i]);
+        }
+        __syncthreads();
+        const int nA = L.n[0] * L.n[1] * C.n[2];
+        tail_restrict(sm, L, C, sm + alt[l], sm + C.rho, tA, tA + nA);
+        for (int i = threadIdx.x; i < C.ng; i += blockDim.x) sm[C.phi + i] = 0.0;
+        __syncthreads();
+    }
+    cur[last] = plan.lv[last].phi;
+    alt[last] = plan.lv[last].tmp;
+    tail_relax(sm, plan.lv[last], cur[last], alt[last], plan.lv[last].post);
+    for (int l = last - 1; l >= 0; l--) {
+        const TailLevel& L = plan.lv[l];
+        const TailLevel& C = plan.lv[l + 1];
+        const int nA = C.n[0] * C.n[1] * L.n[2];
+        tail_interp_sub(L, C, sm + cur[l + 1], sm + cur[l], tA, tA + nA);
+        tail_relax(sm, L, cur[l], alt[l], L.post);
+    }
+    for (int i = threadIdx.x; i < L0.ng; i += blockDim.x) phi_g[i] = sm[cur[0] + i];
+}
+}  // namespace gb
+
 struct gb_poisson {
     int L;  // coarsest level index
+    int tail_lf = -1;           // first level of the fused coarse V-cycle (-1: none)
+    size_t tail_smem = 0;
+    gb::TailPlan tail;
     std::vector<gb_operator*> ops;
     std::vector<gb_transformer*> rst, itp;
     std::vector<int> pre, post;
@@ -467,6 +701,115 @@ struct gb_poisson {
         if (err_host) cudaFreeHost(err_host);
     }
 };
+
+// Pick the first level of the fused coarse V-cycle: the coarsest run of
+// levels (below level 0) whose operators are 2nd-order axis-aligned
+// Laplacians, whose transfers are K = 2, that relax by weighted Jacobi,
+// whose first level holds at most TAIL_POINTS points and whose arrays fit
+// in shared memory.  GPAW_B200_POISSON_TAIL=0 keeps every level on the
+// per-level kernels (same results).
+static void plan_tail(gb_poisson* p) {
+    constexpr long long TAIL_POINTS = 4096;
+    constexpr size_t TAIL_SMEM = 200 * 1024;
+    p->tail_lf = -1;
+    const char* env = getenv("GPAW_B200_POISSON_TAIL");
+    if ((env && atoi(env) == 0) || p->method != 2 || p->L < 1) return;
+    auto level_ok = [&](int l) {
+        const gb_operator* op = p->ops[l];
+        if (!op->tiled || op->nn != 1 || !op->real) return false;
+        if (!(op->cs.axis[0] == 2 && op->cs.axis[1] == 1 && op->cs.axis[2] == 0)) return false;
+        if (l < p->L) {
+            const gb_transformer* r = p->rst[l];
+            const gb_transformer* i = p->itp[l];
+            if (r->k != 2 || i->k != 2) return false;
+            for (int c = 0; c < 3; c++) {
+                if (r->G.g.n[c] != op->g.n[c] || r->G.g.periodic[c] != op->g.periodic[c] ||
+                    r->G.nout[c] != p->ops[l + 1]->g.n[c] ||
+                    i->G.g.n[c] != p->ops[l + 1]->g.n[c] ||
+                    i->G.g.periodic[c] != p->ops[l + 1]->g.periodic[c] ||
+                    i->G.nout[c] != op->g.n[c])
+                    return false;
+            }
+        }
+        return true;
+    };
+    auto smem_from = [&](int lf) {
+        size_t d = 0, scratch = 0;
+        for (int l = lf; l <= p->L; l++) {
+            d += 3 * (size_t)p->ops[l]->ng();
+            if (l < p->L) {
+                const int* n = p->ops[l]->g.n;
+                const int* m = p->ops[l + 1]->g.n;
+                const size_t r = (size_t)n[0] * n[1] * m[2] + (size_t)n[0] * m[1] * m[2];
+                const size_t i = (size_t)m[0] * m[1] * n[2] + (size_t)m[0] * n[1] * n[2];
+                scratch = std::max(scratch, std::max(r, i));
+            }
+        }
+        return (d + scratch) * sizeof(double);
+    };
+    int lf = -1;
+    for (int l = p->L; l >= 1; l--) {
+        if (!level_ok(l) || p->ops[l]->ng() > TAIL_POINTS || smem_from(l) > TAIL_SMEM ||
+            p->L - l + 1 > gb::TAIL_MAX)
+            break;
+        lf = l;
+    }
+    if (lf < 0) return;
+    gb::TailPlan& T = p->tail;
+    memset(&T, 0, sizeof T);
+    T.nl = p->L - lf + 1;
+    int off = 0;
+    for (int k = 0; k < T.nl; k++) {
+        const int l = lf + k;
+        const gb_operator* op = p->ops[l];
+        gb::TailLevel& V = T.lv[k];
+        V.ng = (int)op->ng();
+        for (int c = 0; c < 3; c++) {
+            V.n[c] = op->g.n[c];
+            V.per[c] = op->g.periodic[c];
+        }
+        V.phi = off;
+        V.rho = off + V.ng;
+        V.tmp = off + 2 * V.ng;
+        off += 3 * V.ng;
+        V.c0 = op->cs.c0;
+        for (int d = 0; d < 3; d++) {
+            V.cp[d] = op->cs.cp[d][0];
+            V.cm[d] = op->cs.cm[d][0];
+        }
+        V.pre = p->pre[l];
+        V.post = p->post[l];
+        V.w = p->w[l];
+        if (l < p->L) {
+            const gb_transformer* r = p->rst[l];
+            const gb_transformer* i = p->itp[l];
+            for (int c = 0; c < 3; c++) {
+                V.rplo[c] = r->G.plo[c];
+                V.iplo[c] = i->G.plo[c];
+                V.iskip[c] = i->G.skip0[c];
+            }
+            V.rw = r->G.w[0];
+            V.iw = i->G.w[0];
+        }
+    }
+    T.scratch = off;
+    p->tail_smem = smem_from(lf);
+    p->tail_lf = lf;
+}
+
+static int launch_tail(gb_poisson* p, cudaStream_t st) {
+    static bool attr_done = false;
+    if (!attr_done) {
+        GB_CUDA_TRY(cudaFuncSetAttribute(gb::k_tail_vcycle,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         227 * 1024));
+        attr_done = true;
+    }
+    const int lf = p->tail_lf;
+    gb::k_tail_vcycle<<<1, 1024, p->tail_smem, st>>>(p->rho[lf], p->phi[lf], p->tail);
+    GB_LAUNCH_CHECK();
+    return 0;
+}
 
 extern "C" int gb_poisson_new(int nlevels, gb_operator* const* operators,
                               gb_transformer* const* restrictors,
@@ -506,6 +849,7 @@ extern "C" int gb_poisson_new(int nlevels, gb_operator* const* operators,
         p->rst.push_back(r);
         p->itp.push_back(i);
     }
+    plan_tail(p);
     p->phi.assign(nlevels, nullptr);
     p->rho.assign(nlevels, nullptr);
     p->res.assign(nlevels, nullptr);
@@ -544,8 +888,13 @@ extern "C" int gb_poisson_new(int nlevels, gb_operator* const* operators,
 
 extern "C" void gb_poisson_free(gb_poisson* p) { delete p; }
 
+extern "C" int gb_poisson_fused_levels(const gb_poisson* p) {
+    return (p && p->tail_lf >= 0) ? p->tail.nl : 0;
+}
+
 // iterate2 (gpaw/poisson.py:500-537), recursive over levels.
 static int vcycle(gb_poisson* p, int l, cudaStream_t st) {
+    if (l == p->tail_lf) return launch_tail(p, st);   // starts from phi_l = 0 itself
     gb_operator* op = p->ops[l];
     Phases P;
     memset(&P, 0, sizeof P);
@@ -559,8 +908,9 @@ static int vcycle(gb_poisson* p, int l, cudaStream_t st) {
         if (int rc = transform_impl(p->rst[l], p->res[l], p->rho[l + 1], nullptr, 1, GB_F64, P, 0,
                                     0, 0.0, st))
             return rc;
-        GB_CUDA_TRY(cudaMemsetAsync(p->phi[l + 1], 0, (size_t)p->ops[l + 1]->ng() * sizeof(double),
-                                    st));
+        if (l + 1 != p->tail_lf)
+            GB_CUDA_TRY(cudaMemsetAsync(p->phi[l + 1], 0,
+                                        (size_t)p->ops[l + 1]->ng() * sizeof(double), st));
         if (int rc = vcycle(p, l + 1, st)) return rc;
         // phi_l -= interpolate(phi_{l+1})
         if (int rc = transform_impl(p->itp[l], p->phi[l + 1], p->phi[l], nullptr, 1, GB_F64, P, 0,

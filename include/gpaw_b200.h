@@ -193,6 +193,12 @@ GB_API int gb_poisson_new(int nlevels, gb_operator* const* operators,
                    double dv, gb_poisson** out);
 GB_API void gb_poisson_free(gb_poisson* p);
 
+/* Number of coarse levels the executor runs as one fused kernel (the
+ * coarsest levels, when they are small enough for shared memory; 0 when
+ * every level runs on its own kernels).  Introspection only: both forms
+ * give the same V-cycle bit for bit.  No reference counterpart. */
+GB_API int gb_poisson_fused_levels(const gb_poisson* p);
+
 /* One V-cycle, FDPoissonSolver.iterate2(step, level=0) (:500-537): updates
  * phi in place and writes sum r^2 * dv to *error (host).  Synchronises the
  * stream once (to read the error). */

@@ -317,6 +317,36 @@ def test_poisson_c1_against_oracle(relax, cuda):
     assert np.array_equal(to_np(phi), phi_o)
 
 
+@pytest.mark.parametrize('N,pbc', [((64, 64, 64), (0, 0, 0)),
+                                   ((32, 32, 32), (1, 1, 1)),
+                                   ((48, 32, 40), (1, 1, 0)),
+                                   ((40, 24, 56), (0, 1, 0))])
+def test_poisson_fused_coarse_levels(N, pbc, cuda, monkeypatch):
+    """The coarse levels run as one kernel (all arrays in shared memory)
+    give the same V-cycles as the per-level kernels, bit for bit: zero,
+    periodic and mixed boundaries; the fused run starting at level 1, at
+    level 2, and holding only the coarsest level."""
+    from gpaw_b200 import FDPoissonSolver
+    gd = prod_gd(N, tuple(0.35 * n for n in N), pbc)
+    rng = np.random.default_rng(sum(N))
+    rho = rng.standard_normal(tuple(gd.n_c))
+    rho -= rho.mean()
+    rho_d = to_dev(rho)
+    runs = {}
+    for tail in ('1', '0'):
+        monkeypatch.setenv('GPAW_B200_POISSON_TAIL', tail)
+        ps = FDPoissonSolver(nn=3, relax='J')
+        ps.set_grid_descriptor(gd)
+        phi = gd.zeros()
+        errs = [ps.iterate2(0.0, phi=phi, rho=rho_d) for _ in range(5)]
+        runs[tail] = (to_np(phi), errs)
+        fused = ps._exec.lib.gb_poisson_fused_levels(ps._exec.h)
+        assert (fused > 0) == (tail == '1')
+    assert np.array_equal(runs['1'][0], runs['0'][0])
+    assert runs['1'][1] == runs['0'][1]
+    assert runs['1'][1][-1] < runs['1'][1][0]
+
+
 def test_errors_are_reference_exceptions(cuda):
     import torch
     from gpaw_b200 import FDPoissonSolver, Laplace, PoissonConvergenceError
