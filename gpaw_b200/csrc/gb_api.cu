@@ -461,6 +461,17 @@ struct TailPlan {
     TailLevel lv[TAIL_MAX];
 };
 
+// i / n for 0 <= i < 2^22 through a float reciprocal (inv = 1/n rounded):
+// the float quotient is within 1e-3 of i / n, so one correction step gives
+// the exact integer quotient
+__device__ __forceinline__ int tail_div(int i, int n, float inv) {
+    int q = __float2int_rz(__fmul_rn((float)i, inv));
+    const int r = i - q * n;
+    if (r < 0) q -= 1;
+    else if (r >= n) q += 1;
+    return q;
+}
+
 // index along one axis after the boundary condition; -1 reads zero
 __device__ __forceinline__ int tail_at(int j, int n, int per) {
     if (j >= 0 && j < n) return j;
@@ -469,144 +480,156 @@ __device__ __forceinline__ int tail_at(int j, int n, int per) {
     return (j >= 0 && j < n) ? j : -1;
 }
 
-// value of A at (i0, i1, i2) moved by d along axis ax
-__device__ __forceinline__ double tail_nb(const double* A, const TailLevel& L, int i0, int i1,
-                                          int i2, int ax, int d) {
-    int i[3] = {i0, i1, i2};
-    const int j = tail_at(i[ax] + d, L.n[ax], L.per[ax]);
-    if (j < 0) return 0.0;
-    i[ax] = j;
-    return A[(i[0] * L.n[1] + i[1]) * L.n[2] + i[2]];
+// neighbour at +1 / -1 of point i (coordinate c, extent n, stride s)
+__device__ __forceinline__ double tail_up(const double* __restrict__ A, int i, int c, int n,
+                                          int per, int s) {
+    return (c + 1 < n) ? A[i + s] : (per ? A[i + s - n * s] : 0.0);
+}
+__device__ __forceinline__ double tail_dn(const double* __restrict__ A, int i, int c, int n,
+                                          int per, int s) {
+    return (c > 0) ? A[i - s] : (per ? A[i - s + n * s] : 0.0);
 }
 
 // x = 0 (+ v c0) + v(+1) c(+1) + v(-1) c(-1) per direction, axis 2, 1, 0
-__device__ __forceinline__ double tail_stencil(const double* A, const TailLevel& L, int i0, int i1,
-                                               int i2, bool centre) {
+template <bool CENTRE>
+__device__ __forceinline__ double tail_stencil(const double* __restrict__ A, const TailLevel& L,
+                                               int i, int i0, int i1, int i2) {
+    const int n1 = L.n[1], n2 = L.n[2];
     double x = 0.0;
-    if (centre) x = __dadd_rn(x, __dmul_rn(A[(i0 * L.n[1] + i1) * L.n[2] + i2], L.c0));
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-        const int ax = 2 - k;
-        x = __dadd_rn(x, __dmul_rn(tail_nb(A, L, i0, i1, i2, ax, 1), L.cp[k]));
-        x = __dadd_rn(x, __dmul_rn(tail_nb(A, L, i0, i1, i2, ax, -1), L.cm[k]));
-    }
+    if (CENTRE) x = __dadd_rn(x, __dmul_rn(A[i], L.c0));
+    x = __dadd_rn(x, __dmul_rn(tail_up(A, i, i2, n2, L.per[2], 1), L.cp[0]));
+    x = __dadd_rn(x, __dmul_rn(tail_dn(A, i, i2, n2, L.per[2], 1), L.cm[0]));
+    x = __dadd_rn(x, __dmul_rn(tail_up(A, i, i1, n1, L.per[1], n2), L.cp[1]));
+    x = __dadd_rn(x, __dmul_rn(tail_dn(A, i, i1, n1, L.per[1], n2), L.cm[1]));
+    x = __dadd_rn(x, __dmul_rn(tail_up(A, i, i0, L.n[0], L.per[0], n1 * n2), L.cp[2]));
+    x = __dadd_rn(x, __dmul_rn(tail_dn(A, i, i0, L.n[0], L.per[0], n1 * n2), L.cm[2]));
     return x;
 }
 
-// one weighted-Jacobi sweep src -> dst (c/bmgs/relax.cpp:41-65)
-__device__ void tail_jacobi(double* sm, const TailLevel& L, int src, int dst) {
-    const double* A = sm + src;
-    const double* R = sm + L.rho;
-    double* B = sm + dst;
+// split a flat index of an (., b, c) array into its three coordinates
+__device__ __forceinline__ void tail_split(int i, int b, int c, float ibc, float ic, int& i0,
+                                           int& i1, int& i2) {
+    i0 = tail_div(i, b * c, ibc);
+    const int r = i - i0 * b * c;
+    i1 = tail_div(r, c, ic);
+    i2 = r - i1 * c;
+}
+
+// MODE 0: one weighted-Jacobi sweep A -> B (c/bmgs/relax.cpp:41-65);
+// MODE 1: the residual B = L A - rho
+template <int MODE>
+__device__ void tail_pass(const double* __restrict__ A, const double* __restrict__ R,
+                          double* __restrict__ B, const TailLevel& L) {
+    const int n1 = L.n[1], n2 = L.n[2];
+    const float i12 = __frcp_rn((float)(n1 * n2)), i2f = __frcp_rn((float)n2);
     const double w1 = 1.0 - L.w;
     for (int i = threadIdx.x; i < L.ng; i += blockDim.x) {
-        const int i2 = i % L.n[2], t = i / L.n[2];
-        const int i1 = t % L.n[1], i0 = t / L.n[1];
-        const double x = tail_stencil(A, L, i0, i1, i2, false);
-        B[i] = __dadd_rn(__dmul_rn(w1, A[i]), __ddiv_rn(__dmul_rn(L.w, __dsub_rn(R[i], x)), L.c0));
+        int i0, i1, i2;
+        tail_split(i, n1, n2, i12, i2f, i0, i1, i2);
+        if (MODE == 0) {
+            const double x = tail_stencil<false>(A, L, i, i0, i1, i2);
+            B[i] = __dadd_rn(__dmul_rn(w1, A[i]),
+                             __ddiv_rn(__dmul_rn(L.w, __dsub_rn(R[i], x)), L.c0));
+        } else {
+            B[i] = __dsub_rn(tail_stencil<true>(A, L, i, i0, i1, i2), R[i]);
+        }
     }
     __syncthreads();
 }
 
-// weighted-Jacobi sweeps of phi (held in *cur); the result lands in *cur
-__device__ void tail_relax(double* sm, const TailLevel& L, int& cur, int& alt, int n) {
+// n weighted-Jacobi sweeps of the level's phi, held in buffer b (phi or
+// tmp); returns the buffer that holds the result
+__device__ __forceinline__ int tail_other(const TailLevel& L, int b) {
+    return b == L.phi ? L.tmp : L.phi;
+}
+__device__ __forceinline__ int tail_after(const TailLevel& L, int b, int n) {
+    return (n & 1) ? tail_other(L, b) : b;
+}
+__device__ int tail_relax(double* sm, const TailLevel& L, int b, int n) {
     for (int it = 0; it < n; it++) {
-        tail_jacobi(sm, L, cur, alt);
-        const int t = cur;
-        cur = alt;
-        alt = t;
+        tail_pass<0>(sm + b, sm + L.rho, sm + tail_other(L, b), L);
+        b = tail_other(L, b);
     }
+    return b;
 }
 
 // mid-point restriction of one line value, K = 2: 0.5 (a + w (a+ + a-))
-__device__ __forceinline__ double tail_r1(double a, double ap, double am, double w) {
-    return __dmul_rn(0.5, __dadd_rn(a, __dmul_rn(w, __dadd_rn(ap, am))));
+__device__ __forceinline__ double tail_r1(const double* __restrict__ a, int j, int n, int per,
+                                          int s, double w) {
+    const int j0 = tail_at(j, n, per), jp = tail_at(j + 1, n, per), jm = tail_at(j - 1, n, per);
+    const double v = j0 < 0 ? 0.0 : a[j0 * s];
+    const double vp = jp < 0 ? 0.0 : a[jp * s];
+    const double vm = jm < 0 ? 0.0 : a[jm * s];
+    return __dmul_rn(0.5, __dadd_rn(v, __dmul_rn(w, __dadd_rn(vp, vm))));
 }
 
 // restriction of A (level F, extents n) into out (level C, extents m)
-__device__ void tail_restrict(double* sm, const TailLevel& F, const TailLevel& C, const double* A,
-                              double* out, double* tA, double* tB) {
+__device__ void tail_restrict(const TailLevel& F, const TailLevel& C,
+                              const double* __restrict__ A, double* __restrict__ out,
+                              double* __restrict__ tA, double* __restrict__ tB) {
     const int n0 = F.n[0], n1 = F.n[1], n2 = F.n[2];
     const int m0 = C.n[0], m1 = C.n[1], m2 = C.n[2];
+    const float im2 = __frcp_rn((float)m2), im12 = __frcp_rn((float)(m1 * m2));
     // axis 2: (n0, n1, m2)
     for (int i = threadIdx.x; i < n0 * n1 * m2; i += blockDim.x) {
-        const int c = i % m2, r = i / m2;
-        const int j = 2 * c + 1 - F.rplo[2];
-        const double* row = A + r * n2;
-        const int j0 = tail_at(j, n2, F.per[2]), jp = tail_at(j + 1, n2, F.per[2]),
-                  jm = tail_at(j - 1, n2, F.per[2]);
-        tA[i] = tail_r1(j0 < 0 ? 0.0 : row[j0], jp < 0 ? 0.0 : row[jp], jm < 0 ? 0.0 : row[jm],
-                        F.rw);
+        const int r = tail_div(i, m2, im2), c = i - r * m2;
+        tA[i] = tail_r1(A + r * n2, 2 * c + 1 - F.rplo[2], n2, F.per[2], 1, F.rw);
     }
     __syncthreads();
     // axis 1: (n0, m1, m2)
     for (int i = threadIdx.x; i < n0 * m1 * m2; i += blockDim.x) {
-        const int c2 = i % m2, t = i / m2;
-        const int c1 = t % m1, i0 = t / m1;
-        const int j = 2 * c1 + 1 - F.rplo[1];
-        const int j0 = tail_at(j, n1, F.per[1]), jp = tail_at(j + 1, n1, F.per[1]),
-                  jm = tail_at(j - 1, n1, F.per[1]);
-        const double* col = tA + i0 * n1 * m2 + c2;
-        tB[i] = tail_r1(j0 < 0 ? 0.0 : col[j0 * m2], jp < 0 ? 0.0 : col[jp * m2],
-                        jm < 0 ? 0.0 : col[jm * m2], F.rw);
+        int i0, c1, c2;
+        tail_split(i, m1, m2, im12, im2, i0, c1, c2);
+        tB[i] = tail_r1(tA + i0 * n1 * m2 + c2, 2 * c1 + 1 - F.rplo[1], n1, F.per[1], m2, F.rw);
     }
     __syncthreads();
     // axis 0: (m0, m1, m2)
     for (int i = threadIdx.x; i < m0 * m1 * m2; i += blockDim.x) {
-        const int r = i % (m1 * m2), c0 = i / (m1 * m2);
-        const int j = 2 * c0 + 1 - F.rplo[0];
-        const int j0 = tail_at(j, n0, F.per[0]), jp = tail_at(j + 1, n0, F.per[0]),
-                  jm = tail_at(j - 1, n0, F.per[0]);
-        const double* col = tB + r;
-        out[i] = tail_r1(j0 < 0 ? 0.0 : col[j0 * m1 * m2], jp < 0 ? 0.0 : col[jp * m1 * m2],
-                         jm < 0 ? 0.0 : col[jm * m1 * m2], F.rw);
+        const int c0 = tail_div(i, m1 * m2, im12), r = i - c0 * m1 * m2;
+        out[i] = tail_r1(tB + r, 2 * c0 + 1 - F.rplo[0], n0, F.per[0], m1 * m2, F.rw);
     }
     __syncthreads();
 }
 
-// interpolated value at fine index f of one line a(.) of length n (coarse
-// level with its boundary condition): the even output copies, the odd one
-// is w (a(k) + a(k+1)) (c/bmgs/interpolate.cpp:10-46, K = 2)
-template <class GET>
-__device__ __forceinline__ double tail_i1(int f, int skip, int plo, int n, int per, double w,
-                                          GET get) {
+// interpolated value at fine index f of one line a[j * s] of the coarse
+// level (length n, its boundary condition): the even outputs copy, the odd
+// ones are w (a(k) + a(k+1)) (c/bmgs/interpolate.cpp:10-46, K = 2)
+__device__ __forceinline__ double tail_i1(const double* __restrict__ a, int f, int skip, int plo,
+                                          int n, int per, int s, double w) {
     const int u = f + skip;
     const int k = u >> 1;
     const int j = tail_at(k - plo, n, per);
-    const double a = j < 0 ? 0.0 : get(j);
-    if (!(u & 1)) return a;
+    const double v = j < 0 ? 0.0 : a[j * s];
+    if (!(u & 1)) return v;
     const int j1 = tail_at(k + 1 - plo, n, per);
-    return __dmul_rn(w, __dadd_rn(a, j1 < 0 ? 0.0 : get(j1)));
+    return __dmul_rn(w, __dadd_rn(v, j1 < 0 ? 0.0 : a[j1 * s]));
 }
 
 // phi (level F, extents n) -= interpolation of B (level C, extents m)
-__device__ void tail_interp_sub(const TailLevel& F, const TailLevel& C, const double* B,
-                                double* phi, double* tA, double* tB) {
+__device__ void tail_interp_sub(const TailLevel& F, const TailLevel& C,
+                                const double* __restrict__ B, double* __restrict__ phi,
+                                double* __restrict__ tA, double* __restrict__ tB) {
     const int n0 = F.n[0], n1 = F.n[1], n2 = F.n[2];
     const int m0 = C.n[0], m1 = C.n[1], m2 = C.n[2];
+    const float in2 = __frcp_rn((float)n2), in12 = __frcp_rn((float)(n1 * n2));
     // axis 2: (m0, m1, n2)
     for (int i = threadIdx.x; i < m0 * m1 * n2; i += blockDim.x) {
-        const int f = i % n2, r = i / n2;
-        const double* row = B + r * m2;
-        tA[i] = tail_i1(f, F.iskip[2], F.iplo[2], m2, C.per[2], F.iw,
-                        [&](int j) { return row[j]; });
+        const int r = tail_div(i, n2, in2), f = i - r * n2;
+        tA[i] = tail_i1(B + r * m2, f, F.iskip[2], F.iplo[2], m2, C.per[2], 1, F.iw);
     }
     __syncthreads();
     // axis 1: (m0, n1, n2)
     for (int i = threadIdx.x; i < m0 * n1 * n2; i += blockDim.x) {
-        const int f2 = i % n2, t = i / n2;
-        const int f1 = t % n1, c0 = t / n1;
-        const double* col = tA + c0 * m1 * n2 + f2;
-        tB[i] = tail_i1(f1, F.iskip[1], F.iplo[1], m1, C.per[1], F.iw,
-                        [&](int j) { return col[j * n2]; });
+        int c0, f1, f2;
+        tail_split(i, n1, n2, in12, in2, c0, f1, f2);
+        tB[i] = tail_i1(tA + c0 * m1 * n2 + f2, f1, F.iskip[1], F.iplo[1], m1, C.per[1], n2,
+                        F.iw);
     }
     __syncthreads();
     // axis 0: (n0, n1, n2), subtracted from phi
     for (int i = threadIdx.x; i < n0 * n1 * n2; i += blockDim.x) {
-        const int r = i % (n1 * n2), f0 = i / (n1 * n2);
-        const double* col = tB + r;
-        const double v = tail_i1(f0, F.iskip[0], F.iplo[0], m0, C.per[0], F.iw,
-                                 [&](int j) { return col[j * n1 * n2]; });
+        const int f0 = tail_div(i, n1 * n2, in12), r = i - f0 * n1 * n2;
+        const double v = tail_i1(tB + r, f0, F.iskip[0], F.iplo[0], m0, C.per[0], n1 * n2, F.iw);
         phi[i] = __dsub_rn(phi[i], v);
     }
     __syncthreads();
@@ -624,39 +647,28 @@ k_tail_vcycle(const double* __restrict__ rho_g, double* __restrict__ phi_g, Tail
         sm[L0.phi + i] = 0.0;
     }
     __syncthreads();
-    int cur[TAIL_MAX], alt[TAIL_MAX];
     double* tA = sm + plan.scratch;
     const int last = plan.nl - 1;
     for (int l = 0; l < last; l++) {
         const TailLevel& L = plan.lv[l];
         const TailLevel& C = plan.lv[l + 1];
-        cur[l] = L.phi;
-        alt[l] = L.tmp;
-        tail_relax(sm, L, cur[l], alt[l], L.pre);
-        // residual L phi - rho into the free buffer
-        for (int i = threadIdx.x; i < L.ng; i += blockDim.x) {
-            const int i2 = i % L.n[2], t = i / L.n[2];
-            const int i1 = t % L.n[1], i0 = t / L.n[1];
-            const double x = tail_stencil(sm + cur[l], L, i0, i1, i2, true);
-            sm[alt[l] + i] = __dsub_rn(x, sm[L.rho + i]);
-        }
-        __syncthreads();
-        const int nA = L.n[0] * L.n[1] * C.n[2];
-        tail_restrict(sm, L, C, sm + alt[l], sm + C.rho, tA, tA + nA);
+        const int cur = tail_relax(sm, L, L.phi, L.pre);
+        const int fre = tail_other(L, cur);
+        tail_pass<1>(sm + cur, sm + L.rho, sm + fre, L);
+        tail_restrict(L, C, sm + fre, sm + C.rho, tA, tA + L.n[0] * L.n[1] * C.n[2]);
         for (int i = threadIdx.x; i < C.ng; i += blockDim.x) sm[C.phi + i] = 0.0;
         __syncthreads();
     }
-    cur[last] = plan.lv[last].phi;
-    alt[last] = plan.lv[last].tmp;
-    tail_relax(sm, plan.lv[last], cur[last], alt[last], plan.lv[last].post);
+    const TailLevel& LL = plan.lv[last];
+    int fin = tail_relax(sm, LL, LL.phi, LL.post);
     for (int l = last - 1; l >= 0; l--) {
         const TailLevel& L = plan.lv[l];
         const TailLevel& C = plan.lv[l + 1];
-        const int nA = C.n[0] * C.n[1] * L.n[2];
-        tail_interp_sub(L, C, sm + cur[l + 1], sm + cur[l], tA, tA + nA);
-        tail_relax(sm, L, cur[l], alt[l], L.post);
+        const int cur = tail_after(L, L.phi, L.pre);
+        tail_interp_sub(L, C, sm + fin, sm + cur, tA, tA + C.n[0] * C.n[1] * L.n[2]);
+        fin = tail_relax(sm, L, cur, L.post);
     }
-    for (int i = threadIdx.x; i < L0.ng; i += blockDim.x) phi_g[i] = sm[cur[0] + i];
+    for (int i = threadIdx.x; i < L0.ng; i += blockDim.x) phi_g[i] = sm[fin + i];
 }
 }  // namespace gb
 
