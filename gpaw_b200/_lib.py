@@ -56,6 +56,13 @@ SIGNATURES = {
                                  C.c_double, C.POINTER(_p)]),
     'gb_poisson_free': (None, [_p]),
     'gb_poisson_fused_levels': (C.c_int, [_p]),
+    'gb_woperator_new': (C.c_int, [C.c_int, _p, _p, _p, _p, _p, C.c_int, _p,
+                                   C.c_int, C.c_int, _p]),
+    'gb_woperator_free': (None, [_p]),
+    'gb_woperator_apply': (C.c_int, [_p, _p, _p, C.c_int64, C.c_int, _p, _p]),
+    'gb_woperator_relax': (C.c_int, [_p, C.c_int, _p, _p, C.c_int, C.c_double,
+                                     _p]),
+    'gb_woperator_get_diagonal_element': (C.c_int, [_p, _p, _p]),
     'gb_mixed_new': (C.c_int, [C.c_int, _p, C.POINTER(_p), C.POINTER(_p),
                                C.POINTER(_p), _dp, C.c_double, C.c_int,
                                C.POINTER(_p)]),

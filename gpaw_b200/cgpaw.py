@@ -165,6 +165,95 @@ class Operator:
         return (0, 1, 1)
 
 
+class WOperator:
+    """Weighted stencil object: ``WOperator(nweights, weights, coefs,
+    offsets, size, range, neighbors, real, comm, cfd)``
+    (NewWOperatorObject, c/woperators.cpp:416-460).  ``weights``: float64
+    CUDA tensors of the grid shape, one per operator, kept by reference as
+    the reference keeps its arrays."""
+
+    def __init__(self, nweights, weights, coefs, offsets, size, range,
+                 neighbors, real, comm, cfd):
+        if comm is not None:
+            raise NotImplementedError('domain decomposition (comm) is not '
+                                      'supported: one grid per GPU')
+        nweights = int(nweights)
+        if not (len(weights) == len(coefs) == len(offsets) == nweights):
+            raise TypeError('weights, coefs and offsets need nweights items')
+        lib = _lib.load()
+        size_a, size_p = i64(size)
+        nb_a, nb_p = i64(neighbors)
+        for w in weights:
+            _check_tensor(w, 'weight')
+            if w.dtype != torch.float64 or \
+                    tuple(w.shape) != tuple(int(x) for x in size_a):
+                raise TypeError('weights must be float64 grids of the '
+                                'operator size')
+        cs = [f64(c) for c in coefs]
+        os_ = [i64(o) for o in offsets]
+        for (ca, _), (oa, _) in zip(cs, os_):
+            if len(ca) != len(oa):
+                raise TypeError('coefs and offsets differ in length')
+        W = (C.c_void_p * nweights)(*[w.data_ptr() for w in weights])
+        CP = (C.c_void_p * nweights)(*[C.cast(p, C.c_void_p) for _, p in cs])
+        OP = (C.c_void_p * nweights)(*[C.cast(p, C.c_void_p) for _, p in os_])
+        NC = (C.c_int * nweights)(*[len(a) for a, _ in cs])
+        h = C.c_void_p()
+        check(lib.gb_woperator_new(nweights, W, CP, OP, NC, size_p,
+                                   int(range), nb_p, int(bool(real)),
+                                   int(bool(cfd)), C.byref(h)))
+        self._h = h
+        self._lib = lib
+        self._keep = (weights, cs, os_)
+        self.size = tuple(int(x) for x in size_a)
+        self.real = bool(real)
+
+    def __del__(self):
+        h = getattr(self, '_h', None)
+        if h is not None and h.value:
+            self._lib.gb_woperator_free(h)
+            self._h = None
+
+    def apply(self, input, output, phases=None):
+        """WOperator_apply (c/woperators.cpp:318-370)."""
+        _check_tensor(input, 'input')
+        _check_tensor(output, 'output')
+        if input.shape != output.shape or input.dtype != output.dtype:
+            raise TypeError('input and output differ in shape or dtype')
+        if tuple(input.shape[-3:]) != self.size:
+            raise TypeError(f'grid shape {tuple(input.shape[-3:])} != '
+                            f'{self.size}')
+        ph, ph_p = phases_arg(phases)
+        check(self._lib.gb_woperator_apply(
+            self._h, C.c_void_p(input.data_ptr()),
+            C.c_void_p(output.data_ptr()), _nin(input.shape),
+            _dtype_code(input.dtype), ph_p, _stream()))
+
+    def relax(self, relax_method, f, s, nrelax, w=1.0):
+        """WOperator_relax (c/woperators.cpp:53-96)."""
+        _check_tensor(f, 'f')
+        _check_tensor(s, 's')
+        if tuple(f.shape) != self.size or tuple(s.shape) != self.size:
+            raise TypeError('relax: arrays must have the grid shape')
+        if f.dtype != torch.float64 or s.dtype != torch.float64:
+            raise TypeError('relax: float64 arrays only')
+        check(self._lib.gb_woperator_relax(
+            self._h, int(relax_method), C.c_void_p(f.data_ptr()),
+            C.c_void_p(s.data_ptr()), int(nrelax),
+            float(1.0 if w is None else w), _stream()))
+
+    def get_diagonal_element(self):
+        """c/woperators.cpp:372-398 (synchronises the stream)."""
+        d = C.c_double(0.0)
+        check(self._lib.gb_woperator_get_diagonal_element(
+            self._h, C.byref(d), _stream()))
+        return d.value
+
+    def get_async_sizes(self):
+        # c/woperators.cpp:400-410 without GPAW_ASYNC
+        return (0, 1, 1)
+
+
 class Transformer:
     """``Transformer(size_in, size_out, k, pads, npads, skip, neighbors,
     real, comm, interpolate, use_gpu=1)``."""

@@ -70,26 +70,19 @@ extern "C" int gb_operator_new(const double* coefs, const int64_t* offsets, int 
         }
     }
     // Split each flat padded offset into (o0, o1, o2) with |o_c| <= range.
-    const long long M1 = size[1] + 2 * range, M2 = size[2] + 2 * range;
     op->diag = 0.0;
     for (int p = 0; p < ncoefs; p++) {
-        long long f = offsets[p];
-        long long o2 = ((f % M2) + M2) % M2;
-        if (o2 > M2 / 2) o2 -= M2;
-        long long rest = (f - o2) / M2;
-        long long o1 = ((rest % M1) + M1) % M1;
-        if (o1 > M1 / 2) o1 -= M1;
-        long long o0 = (rest - o1) / M1;
-        if (llabs(o0) > range || llabs(o1) > range || llabs(o2) > range ||
-            (o0 * M1 + o1) * M2 + o2 != f) {
+        const long long f = offsets[p];
+        int o[3];
+        if (!split_offset(f, size, range, o)) {
             delete op;
-            return fail(GB_EINVAL, "Operator: offset %lld does not fit range %d", (long long)f, range);
+            return fail(GB_EINVAL, "Operator: offset %lld does not fit range %d", f, range);
         }
         op->st.coef[p] = coefs[p];
-        op->st.off[p][0] = (int)o0;
-        op->st.off[p][1] = (int)o1;
-        op->st.off[p][2] = (int)o2;
-        op->st.flat[p] = (o0 * size[1] + o1) * size[2] + o2;
+        op->st.off[p][0] = o[0];
+        op->st.off[p][1] = o[1];
+        op->st.off[p][2] = o[2];
+        op->st.flat[p] = ((long long)o[0] * size[1] + o[1]) * size[2] + o[2];
         if (f == 0) op->diag = coefs[p];
     }
     const char* path = getenv("GPAW_B200_FD_PATH");

@@ -4,6 +4,7 @@
 #pragma once
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -69,6 +70,26 @@ inline int read_phases(int dtype, const double* phases, Phases& P) {
         }
     P.use = 1;
     return 0;
+}
+
+// Split an offset flattened with the padded strides (M_c = size_c + 2 range,
+// gpaw/fd_operators.py:60-63) into (o0, o1, o2) with |o_c| <= range; false
+// when it does not fit the range.
+inline bool split_offset(long long f, const int64_t size[3], int range, int o[3]) {
+    const long long M1 = size[1] + 2 * range, M2 = size[2] + 2 * range;
+    long long o2 = ((f % M2) + M2) % M2;
+    if (o2 > M2 / 2) o2 -= M2;
+    const long long rest = (f - o2) / M2;
+    long long o1 = ((rest % M1) + M1) % M1;
+    if (o1 > M1 / 2) o1 -= M1;
+    const long long o0 = (rest - o1) / M1;
+    if (llabs(o0) > range || llabs(o1) > range || llabs(o2) > range ||
+        (o0 * M1 + o1) * M2 + o2 != f)
+        return false;
+    o[0] = (int)o0;
+    o[1] = (int)o1;
+    o[2] = (int)o2;
+    return true;
 }
 
 inline bool ranges_overlap(const void* a, const void* b, size_t bytes) {

@@ -1,0 +1,344 @@
+// Weighted finite-difference operator: A = sum_i w_i(x) L_i with per-point
+// weights (cgpaw.WOperator, c/woperators.cpp; bmgs_wfd / bmgs_wfdz,
+// c/bmgs/wfd.cpp; bmgs_wrelax, c/bmgs/wrelax.cpp).  The dielectric Poisson
+// solver of the solvation model builds it from a Laplacian and the three
+// gradients with weights eps, d_x eps, d_y eps, d_z eps.
+//
+// One thread per grid point.  Every operator's inner sum starts from 0 and
+// adds c_p v(x + o_p) in coefficient order (each product and sum rounded
+// on its own), is scaled by its weight, and is added to the total, as the
+// reference's loops do, so results are bit-identical to them.  Values off
+// the grid come from the same boundary read as the plain operator (zero,
+// or wrapped with the Bloch phase; corners zero when every operator is
+// axis-aligned, as bc_unpack leaves them for cfd = 1).
+#include <cstdlib>
+#include <cstring>
+
+#include "gb_objects.cuh"
+
+using namespace gb;
+
+namespace gb {
+
+constexpr int GB_MAX_WCOEFS = 256;
+
+struct WStencil {
+    int nw;
+    int range;
+    int cfd;
+    int ncoefs[GB_MAX_WEIGHTS];
+    int start[GB_MAX_WEIGHTS];   // first coefficient of operator i
+    const double* w[GB_MAX_WEIGHTS];
+    double coef[GB_MAX_WCOEFS];
+    int off[GB_MAX_WCOEFS][3];
+    long long flat[GB_MAX_WCOEFS];
+};
+
+template <class T>
+__device__ __forceinline__ T wread(const T* __restrict__ a, int p, int i0, int i1, int i2, bool inner,
+                                   const GridBC& g, const Phases& P, const WStencil& s, int c) {
+    if (inner) return __ldg(a + p + s.flat[c]);
+    return bc_read<T>(a, i0 + s.off[c][0], i1 + s.off[c][1], i2 + s.off[c][2], g, P, !s.cfd);
+}
+
+// out = sum_i w_i (sum_p c_ip in(x + o_ip))   (bmgs_wfd, c/bmgs/wfd.cpp:10-40)
+template <class T>
+__global__ void __launch_bounds__(256)
+k_wfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phases P,
+      const __grid_constant__ WStencil s) {
+    const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
+    const int ng = n0 * n1 * n2;
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= ng) return;
+    const int i2 = p % n2;
+    const int t = p / n2;
+    const int i1 = t % n1;
+    const int i0 = t / n1;
+    const int r = s.range;
+    const bool inner = i0 >= r && i0 + r < n0 && i1 >= r && i1 + r < n1 && i2 >= r && i2 + r < n2;
+    for (int b = blockIdx.y; b < nin; b += gridDim.y) {
+        const T* a = in + (long long)b * ng;
+        T x = Num<T>::zero();
+        for (int iw = 0; iw < s.nw; iw++) {
+            T tmp = Num<T>::zero();
+            const int c0 = s.start[iw], c1 = c0 + s.ncoefs[iw];
+            for (int c = c0; c < c1; c++)
+                tmp = Num<T>::add(tmp, Num<T>::scale(wread<T>(a, p, i0, i1, i2, inner, g, P, s, c),
+                                                     s.coef[c]));
+            tmp = Num<T>::scale(tmp, __ldg(s.w[iw] + p));
+            x = Num<T>::add(x, tmp);
+        }
+        out[(long long)b * ng + p] = x;
+    }
+}
+
+// Off-diagonal part and diagonal of the weighted operator at point p:
+// x = sum_i w_i (sum_{p>0} c_ip a(x + o_ip)),  d = sum_i w_i c_i0
+// (bmgs_wrelax's inner loops, c/bmgs/wrelax.cpp:33-48 and 71-86)
+__device__ __forceinline__ void wrelax_terms(const double* __restrict__ a, int p, int i0, int i1,
+                                             int i2, bool inner, const GridBC& g,
+                                             const WStencil& s, double& x, double& d) {
+    const Phases P{};
+    x = 0.0;
+    d = 0.0;
+    for (int iw = 0; iw < s.nw; iw++) {
+        const double weight = __ldg(s.w[iw] + p);
+        double tmp = 0.0;
+        const int c0 = s.start[iw], c1 = c0 + s.ncoefs[iw];
+        for (int c = c0 + 1; c < c1; c++)
+            tmp = __dadd_rn(tmp, __dmul_rn(wread<double>(a, p, i0, i1, i2, inner, g, P, s, c),
+                                           s.coef[c]));
+        tmp = __dmul_rn(tmp, weight);
+        x = __dadd_rn(x, tmp);
+        d = __dadd_rn(d, __dmul_rn(weight, s.coef[c0]));
+    }
+}
+
+// weighted Jacobi: nw = (1 - w) old + w (src - x) / d, neighbours from old
+__global__ void __launch_bounds__(256)
+k_wjacobi(const double* __restrict__ old, double* __restrict__ nw, const double* __restrict__ src,
+          GridBC g, const __grid_constant__ WStencil s, double w) {
+    const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n0 * n1 * n2) return;
+    const int i2 = p % n2;
+    const int t = p / n2;
+    const int i1 = t % n1;
+    const int i0 = t / n1;
+    const int r = s.range;
+    const bool inner = i0 >= r && i0 + r < n0 && i1 >= r && i1 + r < n1 && i2 >= r && i2 + r < n2;
+    double x, d;
+    wrelax_terms(old, p, i0, i1, i2, inner, g, s, x, d);
+    nw[p] = __dadd_rn(__dmul_rn(1.0 - w, old[p]),
+                      __ddiv_rn(__dmul_rn(w, __dsub_rn(src[p], x)), d));
+}
+
+// One wavefront of weighted Gauss-Seidel (points with wa i0 + wb i1 + i2 =
+// t): neighbours inside the grid are read live, wrapped ones from the
+// sweep's starting copy `snap`, as the reference's padded buffer holds them.
+__global__ void __launch_bounds__(256)
+k_wgs_wave(double* __restrict__ f, const double* __restrict__ snap, const double* __restrict__ src,
+           GridBC g, const __grid_constant__ WStencil s, int t, int wa, int wb) {
+    const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n0 * n1) return;
+    const int i1 = q % n1;
+    const int i0 = q / n1;
+    const int i2 = t - wa * i0 - wb * i1;
+    if (i2 < 0 || i2 >= n2) return;
+    const int p = (i0 * n1 + i1) * n2 + i2;
+    const Phases P{};
+    double x = 0.0, d = 0.0;
+    for (int iw = 0; iw < s.nw; iw++) {
+        const double weight = s.w[iw][p];
+        double tmp = 0.0;
+        const int c0 = s.start[iw], c1 = c0 + s.ncoefs[iw];
+        for (int c = c0 + 1; c < c1; c++) {
+            const int y0 = i0 + s.off[c][0], y1 = i1 + s.off[c][1], y2 = i2 + s.off[c][2];
+            double v;
+            if (y0 >= 0 && y0 < n0 && y1 >= 0 && y1 < n1 && y2 >= 0 && y2 < n2)
+                v = f[(y0 * n1 + y1) * n2 + y2];
+            else
+                v = bc_read<double>(snap, y0, y1, y2, g, P, !s.cfd);
+            tmp = __dadd_rn(tmp, __dmul_rn(v, s.coef[c]));
+        }
+        tmp = __dmul_rn(tmp, weight);
+        x = __dadd_rn(x, tmp);
+        d = __dadd_rn(d, __dmul_rn(weight, s.coef[c0]));
+    }
+    f[p] = __ddiv_rn(__dsub_rn(src[p], x), d);
+}
+
+// max over points of |sum_i w_i c_i0| (c/woperators.cpp:372-398); the
+// non-negative doubles order like their bit patterns, so an integer
+// atomicMax on the bits gives the maximum
+__global__ void __launch_bounds__(256)
+k_wdiag(int ng, const __grid_constant__ WStencil s, unsigned long long* out) {
+    double m = 0.0;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < ng; p += gridDim.x * blockDim.x) {
+        double d = 0.0;
+        for (int iw = 0; iw < s.nw; iw++) d = __dadd_rn(d, __dmul_rn(s.w[iw][p], s.coef[s.start[iw]]));
+        if (d < 0) d = -d;
+        if (d > m) m = d;
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+}  // namespace gb
+
+struct gb_woperator {
+    WStencil s;
+    GridBC g;
+    int real;
+    Scratch scratch;
+    unsigned long long* diag_dev = nullptr;
+    ~gb_woperator() {
+        if (diag_dev) cudaFree(diag_dev);
+    }
+    long long ng() const { return (long long)g.n[0] * g.n[1] * g.n[2]; }
+};
+
+extern "C" int gb_woperator_new(int nweights, const double* const* weights,
+                                const double* const* coefs, const int64_t* const* offsets,
+                                const int* ncoefs, const int64_t size[3], int range,
+                                const int64_t neighbors[6], int real, int cfd,
+                                gb_woperator** out) {
+    if (!out || !weights || !coefs || !offsets || !ncoefs || !size || !neighbors)
+        return fail(GB_EINVAL, "WOperator: NULL argument");
+    *out = nullptr;
+    if (nweights < 1 || nweights > GB_MAX_WEIGHTS)
+        return fail(GB_EINVAL, "WOperator: %d weights (1..%d supported)", nweights, GB_MAX_WEIGHTS);
+    if (range < 0) return fail(GB_EINVAL, "WOperator: negative range");
+    for (int c = 0; c < 3; c++)
+        if (size[c] < 1 || size[c] > (1 << 20)) return fail(GB_EINVAL, "WOperator: bad size");
+    if ((double)size[0] * size[1] * size[2] >= 2147483647.0)
+        return fail(GB_EINVAL, "WOperator: grid has 2^31 points or more");
+    gb_woperator* op = new gb_woperator();
+    memset(&op->s, 0, sizeof op->s);
+    op->s.nw = nweights;
+    op->s.range = range;
+    op->s.cfd = cfd ? 1 : 0;
+    op->real = real ? 1 : 0;
+    for (int c = 0; c < 3; c++) {
+        const int64_t lo = neighbors[2 * c], hi = neighbors[2 * c + 1];
+        if (lo > 0 || hi > 0 || (lo == 0) != (hi == 0)) {
+            delete op;
+            return fail(GB_EINVAL, "WOperator: single-domain neighbours only");
+        }
+        op->g.n[c] = (int)size[c];
+        op->g.periodic[c] = lo == 0 ? 1 : 0;
+        if (op->g.periodic[c] && size[c] < range) {
+            delete op;
+            return fail(GB_EINVAL, "Stencil longer than domain");
+        }
+    }
+    int k = 0;
+    for (int iw = 0; iw < nweights; iw++) {
+        if (!weights[iw] || !coefs[iw] || !offsets[iw] || ncoefs[iw] < 1) {
+            delete op;
+            return fail(GB_EINVAL, "WOperator: operator %d is empty", iw);
+        }
+        if (offsets[iw][0] != 0) {
+            delete op;
+            return fail(GB_EINVAL, "WOperator: operator %d does not start at offset 0", iw);
+        }
+        if (k + ncoefs[iw] > GB_MAX_WCOEFS) {
+            delete op;
+            return fail(GB_EINVAL, "WOperator: more than %d coefficients in all", GB_MAX_WCOEFS);
+        }
+        op->s.w[iw] = weights[iw];
+        op->s.start[iw] = k;
+        op->s.ncoefs[iw] = ncoefs[iw];
+        for (int p = 0; p < ncoefs[iw]; p++, k++) {
+            int o[3];
+            if (!split_offset(offsets[iw][p], size, range, o)) {
+                delete op;
+                return fail(GB_EINVAL, "WOperator: offset %lld does not fit range %d",
+                            (long long)offsets[iw][p], range);
+            }
+            op->s.coef[k] = coefs[iw][p];
+            for (int c = 0; c < 3; c++) op->s.off[k][c] = o[c];
+            op->s.flat[k] = ((long long)o[0] * size[1] + o[1]) * size[2] + o[2];
+        }
+    }
+    *out = op;
+    return 0;
+}
+
+extern "C" void gb_woperator_free(gb_woperator* op) { delete op; }
+
+extern "C" int gb_woperator_apply(gb_woperator* op, const void* in, void* out, int64_t nin,
+                                  int dtype, const double* phases, void* stream) {
+    if (!op || !in || !out) return fail(GB_EINVAL, "WOperator apply: NULL argument");
+    if (dtype != GB_F64 && dtype != GB_C128) return fail(GB_EINVAL, "unsupported dtype %d", dtype);
+    if ((dtype == GB_F64) != (op->real != 0))
+        return fail(GB_EINVAL, "dtype does not match the operator (real=%d)", op->real);
+    if (nin < 0) return fail(GB_EINVAL, "WOperator apply: negative batch");
+    if (nin == 0) return 0;
+    cudaStream_t st = (cudaStream_t)stream;
+    Phases P;
+    read_phases(dtype, phases, P);
+    const size_t bytes = (size_t)nin * op->ng() * elem_size(dtype);
+    if (ranges_overlap(in, out, bytes)) {
+        if (int e = op->scratch.ensure(bytes)) return e;
+        GB_CUDA_TRY(cudaMemcpyAsync(op->scratch.ptr, in, bytes, cudaMemcpyDeviceToDevice, st));
+        in = op->scratch.ptr;
+    }
+    const int ng = (int)op->ng();
+    const dim3 grid((unsigned)((ng + 255) / 256), (unsigned)(nin < 65535 ? nin : 65535));
+    if (dtype == GB_F64)
+        k_wfd<double><<<grid, 256, 0, st>>>((const double*)in, (double*)out, (int)nin, op->g, P,
+                                            op->s);
+    else
+        k_wfd<double2><<<grid, 256, 0, st>>>((const double2*)in, (double2*)out, (int)nin, op->g,
+                                             P, op->s);
+    GB_LAUNCH_CHECK();
+    return 0;
+}
+
+extern "C" int gb_woperator_relax(gb_woperator* op, int method, double* f, const double* s,
+                                  int nrelax, double w, void* stream) {
+    if (!op || !f || !s) return fail(GB_EINVAL, "WOperator relax: NULL argument");
+    if (!op->real) return fail(GB_EINVAL, "WOperator relax: float64 operators only");
+    if (method != 1 && method != 2) return fail(GB_EINVAL, "relax method must be 1 or 2");
+    if (nrelax <= 0) return 0;
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t bytes = (size_t)op->ng() * sizeof(double);
+    if (int e = op->scratch.ensure(bytes)) return e;
+    double* X = (double*)op->scratch.ptr;
+    const GridBC& g = op->g;
+    if (method == 1) {
+        // wavefronts: every neighbour earlier in the lexicographic order
+        // lies on an earlier front (c/bmgs/wrelax.cpp:23-56)
+        const int r = op->s.range;
+        int wa = 1, wb = 1;
+        if (!op->s.cfd) {
+            wb = 2 * r + 1;
+            wa = (wb + 1) * r + 1;
+        }
+        const int nt = wa * (g.n[0] - 1) + wb * (g.n[1] - 1) + g.n[2];
+        const bool periodic = g.periodic[0] || g.periodic[1] || g.periodic[2];
+        const int nq = g.n[0] * g.n[1];
+        for (int it = 0; it < nrelax; it++) {
+            if (periodic) GB_CUDA_TRY(cudaMemcpyAsync(X, f, bytes, cudaMemcpyDeviceToDevice, st));
+            for (int t = 0; t < nt; t++)
+                k_wgs_wave<<<(nq + 255) / 256, 256, 0, st>>>(f, periodic ? X : f, s, g, op->s, t,
+                                                            wa, wb);
+            GB_LAUNCH_CHECK();
+        }
+        return 0;
+    }
+    // weighted Jacobi, ping-pong so that the last sweep lands in f
+    const double* src = f;
+    if (nrelax % 2 == 1) {
+        GB_CUDA_TRY(cudaMemcpyAsync(X, f, bytes, cudaMemcpyDeviceToDevice, st));
+        src = X;
+    }
+    const int ng = (int)op->ng();
+    for (int it = 0; it < nrelax; it++) {
+        double* dst = (src == f) ? X : f;
+        k_wjacobi<<<(ng + 255) / 256, 256, 0, st>>>(src, dst, s, g, op->s, w);
+        src = dst;
+    }
+    GB_LAUNCH_CHECK();
+    return 0;
+}
+
+extern "C" int gb_woperator_get_diagonal_element(gb_woperator* op, double* out, void* stream) {
+    if (!op || !out) return fail(GB_EINVAL, "WOperator get_diagonal_element: NULL argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!op->diag_dev) GB_CUDA_TRY(cudaMalloc(&op->diag_dev, sizeof(unsigned long long)));
+    GB_CUDA_TRY(cudaMemsetAsync(op->diag_dev, 0, sizeof(unsigned long long), st));
+    const int ng = (int)op->ng();
+    const int nb = std::min(1184, (ng + 255) / 256);
+    k_wdiag<<<nb, 256, 0, st>>>(ng, op->s, op->diag_dev);
+    GB_LAUNCH_CHECK();
+    unsigned long long bits = 0;
+    GB_CUDA_TRY(cudaMemcpyAsync(&bits, op->diag_dev, sizeof bits, cudaMemcpyDeviceToHost, st));
+    GB_CUDA_TRY(cudaStreamSynchronize(st));
+    double d;
+    memcpy(&d, &bits, sizeof d);
+    *out = d;
+    return 0;
+}

@@ -51,6 +51,7 @@ extern "C" {
 typedef struct gb_operator gb_operator;
 typedef struct gb_transformer gb_transformer;
 typedef struct gb_poisson gb_poisson;
+typedef struct gb_woperator gb_woperator;
 
 /* Library version (major * 10000 + minor * 100 + patch). */
 GB_API int gb_version(void);
@@ -142,6 +143,49 @@ GB_API double gb_operator_get_diagonal_element(const gb_operator* op);
 /* Preallocate the operator's scratch for batches up to nin grids (so that
  * later calls allocate nothing, e.g. inside CUDA-graph capture). */
 GB_API int gb_operator_reserve(gb_operator* op, int64_t nin, int dtype);
+
+/* ----------------------------------------------------------------- WOperator
+ * Replaces cgpaw.WOperator(nweights, weights, coefs, offsets, size, range,
+ * neighbors, real, comm, cfd) — NewWOperatorObject, c/woperators.cpp:416-460,
+ * built by WeightedFDOperator.set_weights (gpaw/wfd_operators.py:64-81).
+ * A = sum_i weights_i * operators_i with per-point weights:
+ *   nweights          number of operators (1..GB_MAX_WEIGHTS)
+ *   weights[i]        DEVICE pointer to a float64 grid (size[0..2]) for
+ *                     operator i; not copied, must outlive the object
+ *   coefs[i], offsets[i], ncoefs[i]
+ *                     stencil i, offsets flattened with the padded strides
+ *                     (M_c = size_c + 2 * range); offsets[i][0] must be 0
+ *                     (WeightedFDOperator puts the centre first, with
+ *                     coefficient 0 when the operator has none)
+ *   size, range, neighbors, real, cfd as for gb_operator_new (cfd = 1 when
+ *   every operator is axis-aligned) */
+#define GB_MAX_WEIGHTS 8
+GB_API int gb_woperator_new(int nweights, const double* const* weights,
+                            const double* const* coefs, const int64_t* const* offsets,
+                            const int* ncoefs, const int64_t size[3], int range,
+                            const int64_t neighbors[6], int real, int cfd,
+                            gb_woperator** out);
+GB_API void gb_woperator_free(gb_woperator* op);
+
+/* WOperator.apply(in, out[, phases]) — WOperator_apply,
+ * c/woperators.cpp:318-370 with bmgs_wfd / bmgs_wfdz (c/bmgs/wfd.cpp):
+ * out[x] = sum_i w_i[x] (sum_p c_ip in[x + o_ip]), every inner sum from 0
+ * in coefficient order, scaled by the weight, then added to the total.
+ * Every grid of the batch uses the same weights.  in == out is allowed. */
+GB_API int gb_woperator_apply(gb_woperator* op, const void* in, void* out, int64_t nin,
+                              int dtype, const double* phases, void* stream);
+
+/* WOperator.relax(method, f, s, nrelax, w=1.0) — WOperator_relax,
+ * c/woperators.cpp:53-96 with bmgs_wrelax (c/bmgs/wrelax.cpp).  float64,
+ * one grid.  method 2: weighted Jacobi; method 1: lexicographic
+ * Gauss-Seidel.  The diagonal is sum_i w_i[x] c_i0 per point. */
+GB_API int gb_woperator_relax(gb_woperator* op, int method, double* f, const double* s,
+                              int nrelax, double w, void* stream);
+
+/* WOperator.get_diagonal_element() — c/woperators.cpp:372-398: the largest
+ * |sum_i w_i[x] c_i0| over the grid (0 for an all-zero grid), written to
+ * *out (host).  Synchronises the stream. */
+GB_API int gb_woperator_get_diagonal_element(gb_woperator* op, double* out, void* stream);
 
 /* --------------------------------------------------------------- Transformer
  * Replaces cgpaw.Transformer(size_in, size_out, k, pads, npads, skip,

@@ -175,6 +175,52 @@ class FDOperator:
         return self.operator.get_diagonal_element()
 
 
+class WeightedFDOperator:
+    """gpaw/wfd_operators.py:7-81: sum_i weights_i * operators_i, the
+    stencils stored with offset 0 first."""
+
+    def __init__(self, operators, be='auto'):
+        self.gd = operators[0].gd
+        self.shape = tuple(self.gd.n_c)
+        self.coef_ps = []
+        self.offset_ps = []
+        for op in operators:
+            if 0 in op.offset_p:
+                assert op.offset_p[0] == 0
+                self.offset_ps.append(np.ascontiguousarray(op.offset_p.copy()))
+                self.coef_ps.append(np.ascontiguousarray(op.coef_p.copy()))
+            else:
+                self.offset_ps.append(
+                    np.ascontiguousarray(np.hstack(([0], op.offset_p))))
+                self.coef_ps.append(
+                    np.ascontiguousarray(np.hstack(([.0], op.coef_p))))
+        self.nweights = len(operators)
+        self.cfd = all([op.cfd for op in operators])
+        self.mp = max([op.mp for op in operators])
+        self.dtype = operators[0].dtype
+        self.be = be
+        self.operator = None
+
+    def set_weights(self, weights):
+        assert len(weights) == self.nweights
+        self.weights = [np.ascontiguousarray(w, float) for w in weights]
+        self.operator = backend(self.be).WOperator(
+            self.nweights, self.weights, self.coef_ps,
+            [np.ascontiguousarray(o, np.int64) for o in self.offset_ps],
+            np.ascontiguousarray(self.gd.n_c, np.int64), int(self.mp),
+            self.gd.neighbor_cd, self.dtype == float, None, self.cfd)
+
+    def apply(self, in_xg, out_xg, phase_cd=None):
+        self.operator.apply(in_xg, out_xg, phase_cd)
+
+    def relax(self, relax_method, f_g, s_g, n, w=None):
+        self.operator.relax(relax_method, f_g, s_g, n,
+                            1.0 if w is None else w)
+
+    def get_diagonal_element(self):
+        return self.operator.get_diagonal_element()
+
+
 def laplace_stencil(gd, scale=1.0, n=1):
     """Coefficients and offsets of GUCLaplace (gpaw/fd_operators.py:184-238)."""
     M_ic = np.indices((3, 3, 3)).reshape((3, -3)).T[-13:] - 1
@@ -533,6 +579,25 @@ class FDHamiltonian:
         self.kin.apply(psit_nR, out, phase_cd)
         for p, o in zip(psit_nR, out):
             o += p * vt_R
+
+
+def interpolate_density(gd, finegd, nt_sR, n=3):
+    """FDPotentialCalculator._interpolate_density
+    (gpaw/new/fd/pot_calc.py:37-41, 72-80): interpolate with the order-2n
+    transformer; off fully periodic grids rescale each spin's fine density
+    to the coarse integral when the fine integral exceeds 1e-14."""
+    nt_sR = np.asarray(nt_sR)
+    one = nt_sR.ndim == 3
+    c = nt_sR[None] if one else nt_sR
+    f = np.zeros((c.shape[0],) + tuple(finegd.n_c))
+    Transformer(gd, finegd, n).apply(c, f)
+    if not gd.pbc_c.all():
+        Nt1_s = gd.integrate(c)
+        Nt2_s = finegd.integrate(f)
+        for Nt1, Nt2, nt_r in zip(Nt1_s, Nt2_s, f):
+            if float(Nt2) > 1e-14:
+                nt_r *= Nt1 / Nt2
+    return f[0] if one else f
 
 
 def calculate_dipole_moment(gd, rho_g):

@@ -215,6 +215,102 @@ class Operator:
         return d
 
 
+class WOperator:
+    """Restatement of the reference ``WOperator`` object
+    (c/woperators.cpp:416-460): A = sum_i w_i(x) L_i with per-point
+    weights; apply = bmgs_wfd / bmgs_wfdz (c/bmgs/wfd.cpp:10-40), relax =
+    bmgs_wrelax (c/bmgs/wrelax.cpp:8-95).  ``weights`` are kept by
+    reference, as the reference keeps its array pointers."""
+
+    def __init__(self, nweights, weights, coefs, offsets, size, r, neighbors,
+                 real, comm, cfd):
+        assert comm is None
+        self.nw = int(nweights)
+        self.weights = list(weights)
+        self.coefs = [np.ascontiguousarray(c, float) for c in coefs]
+        self.offsets = [np.ascontiguousarray(o, np.int64) for o in offsets]
+        self.n = [int(x) for x in size]
+        self.r = int(r)
+        pad = np.full((3, 2), self.r, int)
+        self.bc = BoundaryConditions(self.n, pad, pad, neighbors, real, cfd)
+        n0, n1, n2 = self.n
+        M = [x + 2 * self.r for x in self.n]
+        i0, i1, i2 = np.meshgrid(np.arange(n0), np.arange(n1), np.arange(n2),
+                                 indexing='ij')
+        self._idx = (((i0 + self.r) * M[1] + i1 + self.r) * M[2] +
+                     i2 + self.r).ravel()
+
+    def apply(self, inp, out, phases=None):
+        """WOperator_apply (c/woperators.cpp:318-370): every grid of the
+        batch with the same weights."""
+        nin = inp.shape[0] if inp.ndim == 4 else 1
+        src = inp.reshape((nin,) + tuple(self.n))
+        dst = out.reshape((nin,) + tuple(self.n))
+        for m in range(nin):
+            flat = self.bc.unpack(src[m], phases).ravel()
+            x = np.zeros(self._idx.shape, flat.dtype)
+            for iw in range(self.nw):
+                tmp = np.zeros(self._idx.shape, flat.dtype)
+                for c in range(len(self.coefs[iw])):
+                    tmp = tmp + flat[self._idx + self.offsets[iw][c]] * \
+                        self.coefs[iw][c]
+                tmp = tmp * np.asarray(self.weights[iw]).ravel()
+                x = x + tmp
+            dst[m] = x.reshape(self.n)
+
+    def _terms(self, flat, j, sel):
+        """Off-diagonal sum and diagonal of the points ``sel`` (padded
+        indices j), in bmgs_wrelax's order."""
+        x = np.zeros(len(j))
+        coef = np.zeros(len(j))
+        for iw in range(self.nw):
+            weight = np.asarray(self.weights[iw]).ravel()[sel]
+            tmp = np.zeros(len(j))
+            for c in range(1, len(self.coefs[iw])):
+                tmp = tmp + flat[j + self.offsets[iw][c]] * self.coefs[iw][c]
+            tmp = tmp * weight
+            x = x + tmp
+            coef = coef + weight * self.coefs[iw][0]
+        return x, coef
+
+    def relax(self, method, f, s, nrelax, w=1.0):
+        """WOperator_relax (c/woperators.cpp:53-96)."""
+        if w is None:
+            w = 1.0
+        allpts = np.arange(len(self._idx))
+        for _ in range(nrelax):
+            flat = self.bc.unpack(f, None).ravel()
+            b = f.ravel()
+            if method == 1:
+                n0, n1, n2 = self.n
+                mp = max(self.r, 1)
+                beta = 2 * mp + 1
+                alpha = (beta + 1) * mp + 1
+                i0, i1, i2 = np.meshgrid(np.arange(n0), np.arange(n1),
+                                         np.arange(n2), indexing='ij')
+                t = (alpha * i0 + beta * i1 + i2).ravel()
+                order = np.argsort(t, kind='stable')
+                ts = t[order]
+                groups = np.split(order, np.flatnonzero(np.diff(ts)) + 1)
+                for g in groups:
+                    j = self._idx[g]
+                    x, coef = self._terms(flat, j, g)
+                    x = (s.ravel()[g] - x) / coef
+                    b[g] = x
+                    flat[j] = x
+                continue
+            x, coef = self._terms(flat, self._idx, allpts)
+            b[:] = (1.0 - w) * b + w * (s.ravel() - x) / coef
+
+    def get_diagonal_element(self):
+        """c/woperators.cpp:372-398."""
+        coef = np.zeros(int(np.prod(self.n)))
+        for iw in range(self.nw):
+            coef = coef + np.asarray(self.weights[iw]).ravel() * \
+                self.coefs[iw][0]
+        return float(max(0.0, np.abs(coef).max()))
+
+
 # --------------------------------------------------------------------------
 # Transformer (c/transformers.cpp, c/bmgs/restrict.cpp, interpolate.cpp)
 # --------------------------------------------------------------------------

@@ -62,7 +62,25 @@ def cases():
         out.append((f'mst_{bc}_{dt}', ('mst', 0, bc, dt)))
     for bc in ('p', 'z'):
         out.append((f'psM_{bc}', ('psM', 0, bc, 'f')))
+    # weighted operator (Laplacian + three gradients, per-point weights;
+    # appended last)
+    for bc, dt in (('p', 'f'), ('z', 'f'), ('m', 'f'), ('p', 'c'), ('m', 'c')):
+        out.append((f'wfd_{bc}_{dt}', ('wfd', 2, bc, dt)))
     return out
+
+
+def wfd_stencils(gd, nn):
+    """(coefs, offsets_pc) of a Laplacian and the three axis gradients
+    (4th order, no centre point) used by the weighted-operator cases."""
+    lap = L.Laplace(gd, 0.4, nn)
+    ops = [(lap.coef_p, lap.offset_pc)]
+    h = np.diag(gd.h_cv)
+    for c in range(3):
+        e = np.zeros(3, int)
+        e[c] = 1
+        ops.append((np.array([2 / 3, -1 / 12, -2 / 3, 1 / 12]) / h[c],
+                    np.array([e, 2 * e, -e, -2 * e])))
+    return ops
 
 
 def pbc_of(bc):
@@ -164,6 +182,34 @@ def build(kind, nn, bc, dt, rng):
         niter = ps.solve(phi, rho)
         d.update(N=np.array(gd.N_c), pbc=np.array(pbc), rho=rho, phi=phi,
                  niter=np.array(niter), errors=np.array(ps.errors))
+    elif kind == 'wfd':
+        gd = L.GridDescriptor((9, 8, 10), (3.1, 2.7, 3.4), pbc)
+        st = wfd_stencils(gd, nn)
+        ops = [L.FDOperator(c, o, gd, dtype, be='ref') for c, o in st]
+        wop = L.WeightedFDOperator(ops, be='ref')
+        w = [rng.uniform(1.0, 2.0, tuple(gd.n_c))] + \
+            [rng.standard_normal(tuple(gd.n_c)) for _ in range(3)]
+        wop.set_weights(w)
+        a = rand((2,) + tuple(gd.n_c))
+        ph = gd.phase_factor_cd(KPT) if dtype == complex else None
+        b = np.zeros_like(a)
+        wop.apply(a, b, ph)
+        d.update(N=np.array(gd.N_c), pbc=np.array(pbc), inp=a, out=b,
+                 diag=np.array(wop.get_diagonal_element()))
+        for i, (c, o) in enumerate(st):
+            d[f'coefs{i}'] = np.asarray(c, float)
+            d[f'offsets{i}'] = np.asarray(o, int)
+            d[f'w{i}'] = w[i]
+        if ph is not None:
+            d['phases'] = ph
+        if dtype == float:
+            f = rng.standard_normal(tuple(gd.n_c))
+            src = rng.standard_normal(tuple(gd.n_c))
+            for m in (1, 2):
+                g = f.copy()
+                wop.relax(m, g, src, 2, 0.6)
+                d[f'relax{m}'] = g
+            d.update(f=f, s=src)
     elif kind == 'ps':
         gd = L.GridDescriptor((16, 8, 16), (4.0, 2.0, 4.0), pbc)
         x = gd.get_grid_point_coordinates()

@@ -639,3 +639,105 @@ def test_dipole_correction_slab(cuda):
     assert n == n_o
     assert max_rel(to_np(phi), want) <= RTOL_FP64
     assert abs(ps.correction) > 0
+
+
+@pytest.mark.parametrize('n', [1, 2, 3, 4])
+@pytest.mark.parametrize('pbc', [(1, 1, 1), (0, 0, 0), (1, 1, 0)])
+def test_pot_calc_density_transfers(n, pbc, cuda):
+    """FDPotentialCalculator's transfers: interpolation of a two-spin
+    density to the fine grid (rescaled to the coarse integral off periodic
+    grids) and restriction back, against the oracle."""
+    from gpaw_b200 import GridDescriptor
+    from gpaw_b200.pot_calc import FDDensityTransfers
+    N = (20, 16, 24)
+    cell = (4.0, 3.2, 4.8)
+    gd = GridDescriptor(N, cell, pbc)
+    finegd = gd.refine()
+    gdo = L.GridDescriptor(N, cell, pbc)
+    fgo = gdo.refine()
+    rng = np.random.default_rng(n + 3 * sum(pbc))
+    nt = rng.uniform(0.0, 1.0, (2,) + tuple(gdo.n_c))
+    tr = FDDensityTransfers(gd, finegd, n)
+    got = to_np(tr.interpolate_density(to_dev(nt)))
+    ref = L.interpolate_density(gdo, fgo, nt, n)
+    if all(pbc):
+        assert np.array_equal(got, ref)
+    else:
+        assert max_rel(got, ref) <= RTOL_FP64
+        assert np.allclose(gdo.integrate(nt), fgo.integrate(got),
+                           rtol=1e-12, atol=0)
+    back = to_np(tr.restrict(to_dev(ref)))
+    back_o = np.zeros_like(nt)
+    L.Transformer(fgo, gdo, n).apply(ref, back_o)
+    assert np.array_equal(back, back_o)
+    assert str(tr).startswith('interpolation: tri-')
+
+
+def test_golden_weighted_operator(golden, cuda):
+    """WeightedFDOperator (gb_wfd.cu) against the reference's WOperator:
+    apply (real and complex with Bloch phases), Gauss-Seidel and Jacobi
+    relaxation, diagonal element; bit for bit."""
+    from gpaw_b200 import FDOperator
+    from gpaw_b200.wfd_operators import WeightedFDOperator
+    n = 0
+    for name, c in golden.items():
+        if not name.startswith('wfd_'):
+            continue
+        gd = prod_gd(tuple(c['N']), (3.1, 2.7, 3.4), tuple(c['pbc']))
+        dtype = complex if np.iscomplexobj(c['inp']) else float
+        ops = [FDOperator(c[f'coefs{i}'], c[f'offsets{i}'], gd, dtype)
+               for i in range(4)]
+        wop = WeightedFDOperator(ops)
+        ws = [to_dev(c[f'w{i}']) for i in range(4)]
+        wop.set_weights(ws)
+        x = to_dev(c['inp'])
+        y = x.new_zeros(x.shape)
+        wop.apply(x, y, c.get('phases'))
+        assert np.array_equal(to_np(y), c['out']), name
+        assert wop.get_diagonal_element() == float(c['diag']), name
+        wop.apply(x, x, c.get('phases'))          # in place
+        assert np.array_equal(to_np(x), c['out']), name
+        if dtype == float:
+            for m in (1, 2):
+                f = to_dev(c['f'])
+                wop.relax(m, f, to_dev(c['s']), 2, 0.6)
+                assert np.array_equal(to_np(f), c[f'relax{m}']), (name, m)
+        n += 1
+    assert n == 5
+
+
+@pytest.mark.parametrize('pbc', [(1, 1, 1), (0, 0, 0), (0, 1, 1)])
+def test_weighted_operator_solvation_stencils(pbc, cuda):
+    """The solvation solver's operator (nn = 3 Laplacian and the three
+    Gradients weighted by eps and its gradient) on a larger grid and a
+    batch, against the oracle."""
+    from gpaw_b200 import Gradient, Laplace
+    from gpaw_b200.wfd_operators import WeightedFDOperator
+    N, cell = (24, 20, 28), (4.4, 3.6, 5.0)
+    gd = prod_gd(N, cell, pbc)
+    gdo = L.GridDescriptor(N, cell, pbc)
+    ops = [Laplace(gd, -0.25 / np.pi, 3)] + \
+        [Gradient(gd, v, -0.25 / np.pi, 3) for v in range(3)]
+    ops_o = [L.FDOperator(op.coef_p, op.offset_pc, gdo) for op in ops]
+    rng = np.random.default_rng(sum(pbc))
+    w = [rng.uniform(1.0, 80.0, tuple(gdo.n_c))] + \
+        [rng.standard_normal(tuple(gdo.n_c)) for _ in range(3)]
+    wop = WeightedFDOperator(ops)
+    wop.set_weights([to_dev(a) for a in w])
+    wop_o = L.WeightedFDOperator(ops_o)
+    wop_o.set_weights(w)
+    a = rng.standard_normal((3,) + tuple(gdo.n_c))
+    ref = np.zeros_like(a)
+    wop_o.apply(a, ref)
+    x = to_dev(a)
+    y = x.new_zeros(x.shape)
+    wop.apply(x, y)
+    assert np.array_equal(to_np(y), ref)
+    assert wop.get_diagonal_element() == wop_o.get_diagonal_element()
+    f = rng.standard_normal(tuple(gdo.n_c))
+    s = rng.standard_normal(tuple(gdo.n_c))
+    fo = f.copy()
+    wop_o.relax(2, fo, s, 3, 2.0 / 3.0)
+    fd = to_dev(f)
+    wop.relax(2, fd, to_dev(s), 3, 2.0 / 3.0)
+    assert np.array_equal(to_np(fd), fo)

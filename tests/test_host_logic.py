@@ -162,3 +162,16 @@ def test_dipole_moment_matches_oracle():
         rho = rng.standard_normal(tuple(go.n_c))
         assert np.array_equal(calculate_dipole_moment(gd, rho),
                               L.calculate_dipole_moment(go, rho))
+
+
+def test_oracle_interpolate_density_conserves_charge():
+    """The oracle's _interpolate_density restatement keeps each spin's
+    integral on a zero-boundary grid (gpaw/new/fd/pot_calc.py:72-80)."""
+    import numpy as np
+    from oracle import gpaw_layer as L
+    gd = L.GridDescriptor((12, 10, 14), (3.0, 2.5, 3.5), (0, 0, 0))
+    fg = gd.refine()
+    nt = np.random.default_rng(0).uniform(0.0, 1.0, (2,) + tuple(gd.n_c))
+    f = L.interpolate_density(gd, fg, nt, 3)
+    assert f.shape == (2,) + tuple(fg.n_c)
+    assert np.allclose(gd.integrate(nt), fg.integrate(f), rtol=1e-13, atol=0)

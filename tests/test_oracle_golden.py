@@ -167,3 +167,30 @@ def test_mehrstellen_cases(golden):
             assert np.array_equal(phi, c['phi']), name
             n += 1
     assert n == 5
+
+
+def test_weighted_operator_cases(golden):
+    """WOperator restatement (apply real/complex with Bloch phases, both
+    relax methods, diagonal) = the reference's own WOperator, bit for bit."""
+    n = 0
+    for name, c in golden.items():
+        if not name.startswith('wfd_'):
+            continue
+        gd = L.GridDescriptor(tuple(c['N']), (3.1, 2.7, 3.4),
+                              tuple(c['pbc']))
+        dtype = complex if np.iscomplexobj(c['inp']) else float
+        ops = [L.FDOperator(c[f'coefs{i}'], c[f'offsets{i}'], gd, dtype,
+                            be='port') for i in range(4)]
+        wop = L.WeightedFDOperator(ops, be='port')
+        wop.set_weights([c[f'w{i}'] for i in range(4)])
+        out = np.zeros_like(c['inp'])
+        wop.apply(c['inp'], out, c.get('phases'))
+        assert np.array_equal(out, c['out']), name
+        assert wop.get_diagonal_element() == float(c['diag']), name
+        if dtype == float:
+            for m in (1, 2):
+                g = c['f'].copy()
+                wop.relax(m, g, c['s'], 2, 0.6)
+                assert np.array_equal(g, c[f'relax{m}']), (name, m)
+        n += 1
+    assert n == 5
