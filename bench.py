@@ -472,6 +472,56 @@ def precond_c4(dev, nbands=128):
             'blackbox_gbs': 16 * R.numel() / t / 1e9}
 
 
+def weighted_fd(dev, reps=10):
+    """The solvation solver's weighted operator (WeightedFDOperator: nn = 3
+    Laplacian and the three Gradients weighted by eps and its gradient,
+    gpaw/old/solvation/poisson.py:80-85) on one 192^3 zero-BC float64 grid:
+    apply and one weighted-Jacobi sweep, GB/s of the algorithmic bytes
+    (apply: in + out + 4 weights = 48 B/pt; sweep: phi in + rho + phi out
+    + 4 weights = 56 B/pt).  Arrays total 0.5 GB, larger than L2."""
+    import torch
+    from gpaw_b200 import Gradient, GridDescriptor, Laplace
+    from gpaw_b200.wfd_operators import WeightedFDOperator
+    N = (192, 192, 192)
+    gd = GridDescriptor(N, (N[0] * 0.18 / 0.52917721,) * 3, 0, device=dev)
+    scale = -0.25 / np.pi
+    ops = [Laplace(gd, scale, 3)] + [Gradient(gd, v, scale, 3)
+                                     for v in range(3)]
+    wop = WeightedFDOperator(ops)
+    g = torch.Generator(device=dev)
+    g.manual_seed(11)
+    shape = tuple(int(n) for n in gd.n_c)
+    eps = 1.0 + 77.0 * torch.rand(shape, dtype=torch.float64, device=dev,
+                                  generator=g)
+    w = [eps] + [torch.randn(shape, dtype=torch.float64, device=dev,
+                             generator=g) for _ in range(3)]
+    wop.set_weights(w)
+    x = torch.randn(shape, dtype=torch.float64, device=dev, generator=g)
+    y = torch.empty_like(x)
+    rho = torch.randn(shape, dtype=torch.float64, device=dev, generator=g)
+    npts = x.numel()
+    out = {'grid': list(N), 'operators': 'Laplace nn=3 + 3 Gradients nn=3',
+           'weights': 4}
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1e3 / reps
+
+    t = timed(lambda: wop.apply(x, y))
+    out['apply'] = {'ms': t * 1e3, 'gbs': 48 * npts / t / 1e9}
+    t = timed(lambda: wop.relax(2, x, rho, 2, 2.0 / 3.0)) / 2
+    out['jacobi_sweep'] = {'ms': t * 1e3, 'gbs': 56 * npts / t / 1e9}
+    return out
+
+
 def serving_c5(dev, rates=(50, 100, 200, 500, 1000, 2000), count=60):
     """Poisson-arrival stream of mixed-precision Poisson solves (to 1e-10)
     and nn = 3 stencil applications, grid sides log-uniform in [24, 160]
@@ -688,6 +738,8 @@ def run_gpu(args):
     if not args.no_poisson and single:
         line['poisson'] = {'c1': poisson_c1(dev, cpu=cpu_ok),
                            'c3': poisson_c3(dev)}
+    if not args.no_poisson and single:
+        line['weighted_fd'] = weighted_fd(dev)
     if not args.no_batch and single:
         line.setdefault('poisson', {})['c4_batch'] = poisson_c4(dev,
                                                                 cpu=cpu_ok)
@@ -722,7 +774,7 @@ def main():
     p.add_argument('--no-ham', action='store_true',
                    help='skip the fused Hamiltonian section')
     p.add_argument('--poisson-only', default=None,
-                   choices=['c1', 'c3', 'c4', 'pc', 'c5'],
+                   choices=['c1', 'c3', 'c4', 'pc', 'c5', 'wfd'],
                    help='run one Poisson configuration only (profiling)')
     p.add_argument('--batch', type=int, default=NBANDS,
                    help='wave functions per step (profiling runs only)')
@@ -735,8 +787,8 @@ def main():
             f = poisson_c1 if args.poisson_only == 'c1' else poisson_c3
             r = f(dev, nsolve=max(1, args.steps))
         else:
-            r = {'c4': poisson_c4, 'pc': precond_c4,
-                 'c5': serving_c5}[args.poisson_only](dev)
+            r = {'c4': poisson_c4, 'pc': precond_c4, 'c5': serving_c5,
+                 'wfd': weighted_fd}[args.poisson_only](dev)
         print(json.dumps(r), flush=True)
     elif args.impl == 'reference':
         run_reference(args)
