@@ -472,7 +472,7 @@ def precond_c4(dev, nbands=128):
             'blackbox_gbs': 16 * R.numel() / t / 1e9}
 
 
-def weighted_fd(dev, reps=10):
+def weighted_fd(dev, reps=10, cpu=True):
     """The solvation solver's weighted operator (WeightedFDOperator: nn = 3
     Laplacian and the three Gradients weighted by eps and its gradient,
     gpaw/old/solvation/poisson.py:80-85) on one 192^3 zero-BC float64 grid:
@@ -519,6 +519,31 @@ def weighted_fd(dev, reps=10):
     out['apply'] = {'ms': t * 1e3, 'gbs': 48 * npts / t / 1e9}
     t = timed(lambda: wop.relax(2, x, rho, 2, 2.0 / 3.0)) / 2
     out['jacobi_sweep'] = {'ms': t * 1e3, 'gbs': 56 * npts / t / 1e9}
+    if cpu:
+        # the reference's WOperator on the host (one grid: its OpenMP
+        # region splits the batch, so one thread works) and the GPU
+        # result's max error against it
+        from oracle import gpaw_layer as L
+        be = 'ref' if L._REF is not None else 'port'
+        gdo = L.GridDescriptor(N, gd.cell_cv, 0)
+        wo = L.WeightedFDOperator([L.FDOperator(op.coef_p, op.offset_pc, gdo,
+                                                be=be) for op in ops], be=be)
+        wo.set_weights([a.cpu().numpy() for a in w])
+        xin = x.cpu().numpy()
+        ref = np.zeros_like(xin)
+        wop.apply(x, y)
+        got = y.cpu().numpy()
+        ts = []
+        for _ in range(2):
+            t0 = time.perf_counter()
+            wo.apply(xin, ref)
+            ts.append(time.perf_counter() - t0)
+        t = min(ts)
+        out['cpu_reference'] = {
+            'apply_ms': t * 1e3, 'gbs': 48 * npts / t / 1e9, 'threads': 1,
+            'kind': 'reference' if be == 'ref' else 'port',
+            'max_rel_err_gpu_vs_cpu': float(np.abs(got - ref).max() /
+                                            np.abs(ref).max())}
     return out
 
 
@@ -739,7 +764,7 @@ def run_gpu(args):
         line['poisson'] = {'c1': poisson_c1(dev, cpu=cpu_ok),
                            'c3': poisson_c3(dev)}
     if not args.no_poisson and single:
-        line['weighted_fd'] = weighted_fd(dev)
+        line['weighted_fd'] = weighted_fd(dev, cpu=cpu_ok)
     if not args.no_batch and single:
         line.setdefault('poisson', {})['c4_batch'] = poisson_c4(dev,
                                                                 cpu=cpu_ok)

@@ -4,7 +4,9 @@
 // solver of the solvation model builds it from a Laplacian and the three
 // gradients with weights eps, d_x eps, d_y eps, d_z eps.
 //
-// One thread per grid point.  Every operator's inner sum starts from 0 and
+// Axis-aligned operators (the solvation solver's) take a plane-marching
+// kernel with every tap a shared-memory read; others one thread per grid
+// point reading through L1.  Every operator's inner sum starts from 0 and
 // adds c_p v(x + o_p) in coefficient order (each product and sum rounded
 // on its own), is scaled by its weight, and is added to the total, as the
 // reference's loops do, so results are bit-identical to them.  Values off
@@ -70,6 +72,186 @@ k_wfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phases P
         }
         out[(long long)b * ng + p] = x;
     }
+}
+
+// ---------------------------------------------------------------- tiled apply
+// Axis-aligned weighted operators (every offset on one axis, range R):
+// one CTA owns a WX x WY column tile and a chunk of planes along axis 0.
+// Plane tiles (the tile plus an R-wide halo on its four sides; corners are
+// never read) stream through a ring of S shared-memory stages by cp.async,
+// S - (2R + 1) planes ahead; S is a power of two, so the stage of any tap's
+// plane is (centre + o0) & (S - 1).  Every tap is then a shared-memory
+// read, and the sums keep the order of k_wfd.  Wrapped values carry their
+// Bloch phase: in-plane halo cells are multiplied right after they land,
+// a whole plane wrapped along axis 0 by that axis's phase (only its tile
+// columns are read, as axis-0 neighbours).
+constexpr int WX = 32, WY = 8;
+
+__device__ __forceinline__ bool wwrap(int& y, int n, int periodic) {
+    if (y >= 0 && y < n) return true;
+    if (!periodic) return false;
+    y += (y < 0) ? n : -n;
+    return y >= 0 && y < n;
+}
+
+template <int BYTES>
+__device__ __forceinline__ void wcp_async(unsigned sdst, const void* gsrc, bool valid) {
+    const int n = valid ? BYTES : 0;   // 0: zero fill, nothing is read
+    if (BYTES == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sdst), "l"(gsrc),
+                     "r"(n));
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sdst), "l"(gsrc),
+                     "r"(n));
+}
+
+template <class T, int R, int S>
+__global__ void __launch_bounds__(WX * WY)
+k_wfd_tiled(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phases P,
+            const __grid_constant__ WStencil s, int chunk0, int tiles_x) {
+    constexpr int PX = WX + 2 * R, PY = WY + 2 * R, PL = PX * PY;
+    constexpr int NT = WX * WY;
+    constexpr int D = S - (2 * R + 1);          // planes in flight
+    constexpr int NMID = PY * WX, NSIDE = WY * 2 * R;
+    constexpr int NC = (NMID + NSIDE + NT - 1) / NT;
+    constexpr int EB = (int)sizeof(T);
+    static_assert(D >= 1 && (S & (S - 1)) == 0, "ring depth");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    T* ring = reinterpret_cast<T*>(smem_raw);
+
+    const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
+    const int x0 = (blockIdx.x % tiles_x) * WX;
+    const int y0 = (blockIdx.x / tiles_x) * WY;
+    const int pa = blockIdx.y * chunk0;
+    const int pb = min(n0, pa + chunk0);
+    const int b = blockIdx.z;
+    if (pa >= pb || b >= nin) return;
+    const int tid = threadIdx.x;
+    const long long ng = (long long)n0 * n1 * n2;
+    const long long pstride = (long long)n1 * n2;
+    const T* a = in + b * ng;
+    T* o = out + b * ng;
+    const int tx = tid % WX, ty = tid / WX;
+    const int gx = x0 + tx, gy = y0 + ty;
+    const bool own = gx < n2 && gy < n1;
+
+    // this thread's copy cells: stage offset, in-plane source offset,
+    // validity and in-plane phase code (0 none, 1/2 axis 1 high/low,
+    // 3/4 axis 2 high/low)
+    int soff[NC], goff[NC];
+    unsigned vmask = 0, wcode = 0;
+#pragma unroll
+    for (int i = 0; i < NC; i++) {
+        const int e = tid + i * NT;
+        soff[i] = 0;
+        goff[i] = 0;
+        if (e >= NMID + NSIDE) continue;
+        int ry, rx;
+        if (e < NMID) {
+            ry = e / WX - R;
+            rx = e % WX;
+        } else {
+            const int f = e - NMID;
+            ry = f / (2 * R);
+            const int c = f % (2 * R);
+            rx = c < R ? c - R : WX + c - R;
+        }
+        soff[i] = (ry + R) * PX + (rx + R);
+        int y = y0 + ry, x = x0 + rx;
+        const bool yw = y < 0 || y >= n1, xw = x < 0 || x >= n2;
+        const int ys = y < 0, xs = x < 0;
+        if (wwrap(y, n1, g.periodic[1]) && wwrap(x, n2, g.periodic[2])) {
+            vmask |= 1u << i;
+            goff[i] = y * n2 + x;
+            unsigned c = 0;
+            if (yw) c = 1 + ys;
+            else if (xw) c = 3 + xs;
+            wcode |= c << (3 * i);
+        }
+    }
+    if (!P.use) wcode = 0;
+    const unsigned ring_u = (unsigned)__cvta_generic_to_shared(ring);
+    // relative plane j is absolute plane pa - R + j; it lives in stage j & (S-1)
+    auto issue = [&](int j) {
+        int pl = pa - R + j;
+        const bool pv = wwrap(pl, n0, g.periodic[0]);
+        const unsigned su = ring_u + (unsigned)((j & (S - 1)) * PL * EB);
+        const T* src = a + pl * pstride;
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            if (tid + i * NT >= NMID + NSIDE) break;
+            const bool ok = pv && ((vmask >> i) & 1);
+            wcp_async<EB>(su + (unsigned)(soff[i] * EB), ok ? src + goff[i] : a, ok);
+        }
+    };
+    auto fixup = [&](int j) {
+        if constexpr (sizeof(T) == 16) {
+            const int pl = pa - R + j;
+            const bool zw = P.use && g.periodic[0] && (pl < 0 || pl >= n0);
+            if (!wcode && !zw) return;
+            const double2 ph0 = pl >= n0 ? P.ph[0][0] : P.ph[0][1];
+            T* st = ring + (j & (S - 1)) * PL;
+#pragma unroll
+            for (int i = 0; i < NC; i++) {
+                if (tid + i * NT >= NMID + NSIDE) break;
+                if (!((vmask >> i) & 1)) continue;
+                const unsigned c = (wcode >> (3 * i)) & 7u;
+                if (c == 0 && !zw) continue;
+                T v = st[soff[i]];
+                if (c) v = cmul(c == 1 ? P.ph[1][0] : c == 2 ? P.ph[1][1]
+                                : c == 3 ? P.ph[2][0] : P.ph[2][1], v);
+                if (zw) v = cmul(ph0, v);
+                st[soff[i]] = v;
+            }
+        }
+    };
+
+    const int nplanes = pb - pa;
+    const int total = nplanes + 2 * R;     // relative planes 0 .. total-1
+#pragma unroll 1
+    for (int j = 0; j < D; j++) {
+        if (j < total) issue(j);
+        asm volatile("cp.async.commit_group;\n" ::);
+    }
+    // the stencil tables in shared memory (read by every thread at the same
+    // address: broadcasts): per tap its plane offset o0, its in-plane
+    // offset o1 * PX + o2 and its coefficient
+    __shared__ double sh_coef[GB_MAX_WCOEFS];
+    __shared__ int sh_o0[GB_MAX_WCOEFS], sh_ip[GB_MAX_WCOEFS];
+    const int ntap = s.start[s.nw - 1] + s.ncoefs[s.nw - 1];
+    for (int c = tid; c < ntap; c += NT) {
+        sh_coef[c] = s.coef[c];
+        sh_o0[c] = s.off[c][0];
+        sh_ip[c] = s.off[c][1] * PX + s.off[c][2];
+    }
+    const int cen = (ty + R) * PX + (tx + R);
+#pragma unroll 1
+    for (int t = 0; t < total; t++) {
+        asm volatile("cp.async.wait_group %0;\n" ::"n"(D - 1));
+        fixup(t);
+        __syncthreads();
+        if (t + D < total) issue(t + D);
+        asm volatile("cp.async.commit_group;\n" ::);
+        if (t < 2 * R) continue;
+        const int cj = t - R;                  // relative centre plane
+        const int p = pa + cj - R;             // absolute centre plane
+        if (!own) continue;
+        const long long at = p * pstride + (long long)gy * n2 + gx;
+        T x = Num<T>::zero();
+        for (int iw = 0; iw < s.nw; iw++) {
+            T tmp = Num<T>::zero();
+            const int c0 = s.start[iw], c1 = c0 + s.ncoefs[iw];
+#pragma unroll 4
+            for (int c = c0; c < c1; c++) {
+                const T v = ring[((cj + sh_o0[c]) & (S - 1)) * PL + cen + sh_ip[c]];
+                tmp = Num<T>::add(tmp, Num<T>::scale(v, sh_coef[c]));
+            }
+            tmp = Num<T>::scale(tmp, __ldg(s.w[iw] + at));
+            x = Num<T>::add(x, tmp);
+        }
+        o[at] = x;
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::);
 }
 
 // Off-diagonal part and diagonal of the weighted operator at point p:
@@ -179,6 +361,62 @@ struct gb_woperator {
     long long ng() const { return (long long)g.n[0] * g.n[1] * g.n[2]; }
 };
 
+namespace gb {
+// Tiled apply for axis-aligned operators of range 1..6 (complex: 1..3);
+// -1 when the operator does not qualify (the gather kernel runs instead).
+template <class T, int R, int S>
+static int launch_wfd_tiled_rs(const void* in, void* out, int nin, const GridBC& g,
+                               const Phases& P, const WStencil& s, cudaStream_t st) {
+    constexpr size_t smem = (size_t)S * (WX + 2 * R) * (WY + 2 * R) * sizeof(T);
+    static bool attr_done = false;
+    if (!attr_done) {
+        if (cudaFuncSetAttribute(k_wfd_tiled<T, R, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem) != cudaSuccess)
+            return -2;
+        attr_done = true;
+    }
+    const int tiles_x = (g.n[2] + WX - 1) / WX;
+    const int tiles_y = (g.n[1] + WY - 1) / WY;
+    const int chunk0 = cfd_chunk(g, R, nin, WY);
+    const int nch = (g.n[0] + chunk0 - 1) / chunk0;
+    const long long ng = (long long)g.n[0] * g.n[1] * g.n[2];
+    for (int b0 = 0; b0 < nin; b0 += 65535) {
+        const int nb = min(65535, nin - b0);
+        dim3 grid(tiles_x * tiles_y, nch, nb);
+        k_wfd_tiled<T, R, S><<<grid, WX * WY, smem, st>>>((const T*)in + b0 * ng,
+                                                         (T*)out + b0 * ng, nb, g, P, s, chunk0,
+                                                         tiles_x);
+    }
+    return 0;
+}
+
+template <class T>
+static int launch_wfd_tiled(const void* in, void* out, int nin, const GridBC& g,
+                            const Phases& P, const WStencil& s, cudaStream_t st) {
+    if (!s.cfd) return -1;
+    const int nc = s.start[s.nw - 1] + s.ncoefs[s.nw - 1];
+    for (int c = 0; c < nc; c++) {
+        int nz = 0;
+        for (int k = 0; k < 3; k++) nz += s.off[c][k] != 0;
+        if (nz > 1) return -1;
+    }
+    switch (s.range) {
+        case 1: return launch_wfd_tiled_rs<T, 1, 4>(in, out, nin, g, P, s, st);
+        case 2: return launch_wfd_tiled_rs<T, 2, 8>(in, out, nin, g, P, s, st);
+        case 3: return launch_wfd_tiled_rs<T, 3, 8>(in, out, nin, g, P, s, st);
+    }
+    if constexpr (sizeof(T) == 8) {
+        switch (s.range) {
+            case 4: return launch_wfd_tiled_rs<T, 4, 16>(in, out, nin, g, P, s, st);
+            case 5: return launch_wfd_tiled_rs<T, 5, 16>(in, out, nin, g, P, s, st);
+            case 6: return launch_wfd_tiled_rs<T, 6, 16>(in, out, nin, g, P, s, st);
+        }
+    }
+    return -1;
+}
+
+}  // namespace gb
+
 extern "C" int gb_woperator_new(int nweights, const double* const* weights,
                                 const double* const* coefs, const int64_t* const* offsets,
                                 const int* ncoefs, const int64_t size[3], int range,
@@ -264,6 +502,14 @@ extern "C" int gb_woperator_apply(gb_woperator* op, const void* in, void* out, i
         if (int e = op->scratch.ensure(bytes)) return e;
         GB_CUDA_TRY(cudaMemcpyAsync(op->scratch.ptr, in, bytes, cudaMemcpyDeviceToDevice, st));
         in = op->scratch.ptr;
+    }
+    int rc = (dtype == GB_F64)
+                 ? launch_wfd_tiled<double>(in, out, (int)nin, op->g, P, op->s, st)
+                 : launch_wfd_tiled<double2>(in, out, (int)nin, op->g, P, op->s, st);
+    if (rc == -2) return fail(GB_ECUDA, "WOperator: could not raise the shared-memory limit");
+    if (rc == 0) {
+        GB_LAUNCH_CHECK();
+        return 0;
     }
     const int ng = (int)op->ng();
     const dim3 grid((unsigned)((ng + 255) / 256), (unsigned)(nin < 65535 ? nin : 65535));
