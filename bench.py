@@ -348,7 +348,7 @@ def c1_cpu(phi_gpu, n_gpu):
 
 def poisson_c3(dev, nsolve=5):
     """192^3 zero-BC, h = 0.18 A, 64 Gaussians: plain FP64 V-cycle with the
-    reference schedule (7 grids) versus FP32 V-cycles (4 levels, 2 + 2
+    reference schedule (7 grids) versus FP32 V-cycles (6 levels, 2 + 2
     smoothing sweeps) in FP64 defect correction, both to 1e-10 relative
     residual."""
     import torch
@@ -363,7 +363,7 @@ def poisson_c3(dev, nsolve=5):
     fp64 = FDPoissonSolver(nn=3, relax='J',
                            eps=eps_for_relative_residual(rho, gd))
     fp64.set_grid_descriptor(gd)
-    mixed = MixedPoissonSolver(nn=3, tol=1e-10, levels=4)
+    mixed = MixedPoissonSolver(nn=3, tol=1e-10, levels=6)
     mixed.set_grid_descriptor(gd)
     out = {'grid': [192, 192, 192], 'h_angstrom': 0.18, 'gaussians': 64}
     phis = {}
