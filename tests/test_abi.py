@@ -56,3 +56,48 @@ def test_errors_map_to_reference_exceptions():
     rc = lib.gb_operator_new(cp, op, 1, sp, 1, nbp, 1, 1, ctypes.byref(h))
     with pytest.raises(ValueError, match='domain decomposition'):
         _lib.check(rc)
+
+
+def _wop_new(lib, nweights=1, offsets=((0, 1, -1),), range_=1,
+             neighbors=((0, 0), (-1, -1), (-1, -1))):
+    """gb_woperator_new on host-side dummy weight pointers (construction
+    touches no device memory)."""
+    import numpy as np
+    n = len(offsets)
+    keep = []
+    C = (ctypes.c_void_p * n)
+    cs, os_ = [], []
+    for o in offsets:
+        ca, cp = _lib.f64([1.0] * len(o))
+        oa, op = _lib.i64(o)
+        keep += [ca, oa]
+        cs.append(ctypes.cast(cp, ctypes.c_void_p))
+        os_.append(ctypes.cast(op, ctypes.c_void_p))
+    dummy = np.zeros(8)
+    W = C(*([dummy.ctypes.data] * n))
+    NC = (ctypes.c_int * n)(*[len(o) for o in offsets])
+    size, sp = _lib.i64([6, 5, 7])
+    nb, nbp = _lib.i64(neighbors)
+    h = ctypes.c_void_p()
+    rc = lib.gb_woperator_new(nweights, W, C(*cs), C(*os_), NC, sp, range_,
+                              nbp, 1, 1, ctypes.byref(h))
+    if rc == 0:
+        lib.gb_woperator_free(h)
+    return rc
+
+
+def test_woperator_argument_checks():
+    """WOperator construction rejects what the reference's WeightedFDOperator
+    asserts or cannot run: no operators, an operator whose first offset is
+    not the centre, offsets beyond the range, more than one domain."""
+    lib = _lib.load()
+    assert _wop_new(lib) == 0
+    with pytest.raises(ValueError, match='weights'):
+        _lib.check(_wop_new(lib, nweights=0))
+    with pytest.raises(ValueError, match='offset 0'):
+        _lib.check(_wop_new(lib, offsets=((1, 0, -1),)))
+    with pytest.raises(ValueError, match='does not fit'):
+        _lib.check(_wop_new(lib, offsets=((0, 200),)))
+    with pytest.raises(ValueError, match='single-domain'):
+        _lib.check(_wop_new(lib, neighbors=((1, 1), (-1, -1), (-1, -1))))
+    assert lib.gb_poisson_fused_levels(None) == 0
