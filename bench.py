@@ -544,6 +544,77 @@ def weighted_fd(dev, reps=10, cpu=True):
             'kind': 'reference' if be == 'ref' else 'port',
             'max_rel_err_gpu_vs_cpu': float(np.abs(got - ref).max() /
                                             np.abs(ref).max())}
+    out['poisson_dielectric_64'] = weighted_poisson(dev, cpu=cpu)
+    return out
+
+
+def weighted_poisson(dev, nsolve=5, cpu=True):
+    """WeightedFDPoissonSolver (gpaw/old/solvation/poisson.py:75-124) on the
+    C1 grid (64^3 zero BC, h = 0.2 A) with a dielectric of 1 inside a
+    sphere and 80 outside, to the reference's eps = 2e-10: ms per solve,
+    V-cycles, and the reference's C core (WOperator + Transformer, one
+    host thread) on the same solve with the GPU potential's max error."""
+    import torch
+    from gpaw_b200 import Gradient, GridDescriptor, Laplace
+    from gpaw_b200.solvation import WeightedFDPoissonSolver
+    from gpaw_b200.workloads import BOHR, c1_density, neutralize
+    h = 0.2 / BOHR
+    N = (64, 64, 64)
+    cell = (64 * h,) * 3
+    gd = GridDescriptor(N, cell, 0, device=dev)
+    rho = neutralize(c1_density(gd), gd)
+    x = np.stack([a.cpu().numpy() if hasattr(a, 'cpu') else a
+                  for a in gd.get_grid_point_coordinates()]) - 32 * h
+    w2 = (8 * h) ** 2
+    g = np.exp(-(x**2).sum(0) / w2)
+    arrays = [80.0 - 79.0 * g] + [79.0 * g * 2.0 * x[c] / w2 for c in range(3)]
+
+    class Dielectric:
+        eps_gradeps = [torch.from_numpy(a).to(dev) for a in arrays]
+
+    ps = WeightedFDPoissonSolver(nn=3, eps=2e-10)
+    ps.set_grid_descriptor(gd)
+    ps.set_dielectric(Dielectric())
+    ps.restrict_op_weights()
+    rho_d = torch.from_numpy(rho).to(dev)
+    phi = gd.zeros()
+    ps.solve_neutral(phi, rho_d)
+    times = []
+    for _ in range(nsolve):
+        phi.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        n = ps.solve_neutral(phi, rho_d)
+        times.append(time.perf_counter() - t0)
+    t = float(np.median(times))
+    out = {'grid': list(N), 'eps': 2e-10, 'vcycles': n, 'ms_per_solve': t * 1e3,
+           'solves_per_s': 1.0 / t}
+    if cpu:
+        from oracle import gpaw_layer as L
+        be = 'ref' if L._REF is not None else 'port'
+        gdo = L.GridDescriptor(N, cell, 0)
+
+        def stencils(g_, scale, nn):
+            gp = GridDescriptor(tuple(g_.N_c), cell, 0, device=dev)
+            ops = [Laplace(gp, scale, nn)] + [Gradient(gp, j, scale, nn)
+                                              for j in range(3)]
+            return [(op.coef_p, op.offset_pc) for op in ops]
+
+        wo = L.WeightedFDPoissonSolver(stencils, nn=3, eps=2e-10, be=be)
+        wo.set_grid_descriptor(gdo)
+        wo.set_dielectric(arrays)
+        wo.restrict_op_weights()
+        phi_o = gdo.zeros()
+        t0 = time.perf_counter()
+        n_o = wo.solve_neutral(phi_o, rho)
+        tc = time.perf_counter() - t0
+        got = phi.cpu().numpy()
+        out['cpu_reference'] = {
+            'ms_per_solve': tc * 1e3, 'threads': 1,
+            'kind': 'reference' if be == 'ref' else 'port', 'vcycles': n_o,
+            'same_vcycles_as_gpu': n_o == n,
+            'max_rel_err_gpu_vs_cpu': float(np.abs(got - phi_o).max() /
+                                            np.abs(phi_o).max())}
     return out
 
 

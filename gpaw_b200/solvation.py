@@ -1,0 +1,151 @@
+"""Poisson solver with a spatially varying dielectric (drop-in for the
+WeightedFDPoissonSolver of gpaw/old/solvation/poisson.py:75-124).
+
+div(eps(r) grad phi(r)) = -4 pi rho(r) is solved by the FDPoissonSolver
+V-cycle (gpaw/poisson.py:500-537) on weighted operators: every level's
+operator is ``WeightedFDOperator([Laplace, d/dx, d/dy, d/dz])`` weighted by
+eps and its three derivatives (the dielectric's ``eps_gradeps``); the
+weights of each coarser level are the restrictions of the finer level's.
+The relaxation sweeps, operator applications and grid transfers are the
+sm_100a kernels of the weighted operator and the Transformer; the residual
+updates are device arithmetic, and the level-0 error is read once per
+V-cycle to decide whether to stop, as the reference does.
+
+Neutral systems only: the charged branch needs the dielectric-aware
+compensation charge of the reference's ``load_gauss`` (not part of this
+path) and raises NotImplementedError.
+"""
+from __future__ import annotations
+
+from math import pi
+
+import torch
+
+from ._lib import PoissonConvergenceError
+from .fd_operators import Gradient, Laplace
+from .poisson import FDPoissonSolver
+from .wfd_operators import WeightedFDOperator
+
+
+class WeightedFDPoissonSolver(FDPoissonSolver):
+    def __init__(self, nn=3, relax='J', eps=2e-10, maxiter=1000,
+                 remove_moment=None, use_charge_center=False):
+        if remove_moment is not None:
+            raise NotImplementedError(
+                'Removing arbitrary multipole moments is not implemented '
+                'for SolvationPoissonSolver!')
+        if nn == 'M':
+            raise NotImplementedError(
+                'Mehrstellen stencil is not implemented for '
+                'SolvationPoissonSolver!')
+        super().__init__(nn, relax, eps, maxiter)
+        self.dielectric = None
+
+    def set_dielectric(self, dielectric):
+        """``dielectric.eps_gradeps``: [eps, d eps/dx, d eps/dy, d eps/dz],
+        float64 CUDA tensors of the grid shape (kept, not copied)."""
+        self.dielectric = dielectric
+
+    def create_laplace(self, gd, scale=1.0, n=1, dtype=float):
+        """:80-85: the Laplacian and the three gradients, weighted."""
+        operators = [Laplace(gd, scale, n, dtype)]
+        operators += [Gradient(gd, j, scale, n, dtype) for j in (0, 1, 2)]
+        return WeightedFDOperator(operators)
+
+    def get_description(self):
+        return super().get_description().replace(
+            'solver with', 'weighted FD solver with dielectric and')
+
+    def _init(self):
+        """:113-124 and gpaw/poisson.py:451-472: level 0 weighted by the
+        dielectric, coarser levels by arrays that restrict_op_weights
+        fills; work arrays of every level."""
+        if self._initialized:
+            return
+        if self.dielectric is None:
+            raise RuntimeError('WeightedFDPoissonSolver: set_dielectric '
+                               'first')
+        self.operators[0].set_weights(list(self.dielectric.eps_gradeps))
+        self.op_coarse_weights = []
+        for operator in self.operators[1:]:
+            weights = [operator.gd.empty() for _ in range(4)]
+            self.op_coarse_weights.append(weights)
+            operator.set_weights(weights)
+        gd = self.gd
+        self.rhos = [gd.empty()]
+        self.phis = [None]
+        self.residuals = [gd.empty()]
+        for op in self.operators[1:]:
+            self.phis.append(op.gd.empty())
+            self.rhos.append(op.gd.empty())
+            self.residuals.append(op.gd.empty())
+        level = self.levels
+        self.presmooths[level] = 8
+        self.postsmooths[level] = 8
+        self._initialized = True
+
+    def restrict_op_weights(self):
+        """:100-106: restrict the weights to the coarse grids."""
+        self._init()
+        weights = [self.operators[0].weights] + self.op_coarse_weights
+        for i, res in enumerate(self.restrictors):
+            for j in range(4):
+                res.apply(weights[i][j], weights[i + 1][j])
+        self.step = 0.66666666 / self.operators[0].get_diagonal_element()
+
+    def solve(self, phi, rho, charge=None, maxcharge=1e-6,
+              zero_initial_phi=False, timer=None):
+        """:87-98 for a neutral system (gpaw/poisson.py:182-213)."""
+        self._init()
+        actual_charge = self.gd.integrate(rho)
+        if abs(actual_charge) > maxcharge:
+            raise NotImplementedError('charged system with a dielectric')
+        self.restrict_op_weights()
+        background = (actual_charge / self.gd.dv /
+                      self.gd.get_size_of_global_array().prod())
+        return self.solve_neutral(phi, rho - background)
+
+    def solve_neutral(self, phi, rho, timer=None):
+        """gpaw/poisson.py:474-498."""
+        self._init()
+        self.phis[0] = phi
+        self.rhos[0].copy_(rho)
+        niter = 1
+        while self.iterate2(self.step) > self.eps and niter < self.maxiter:
+            niter += 1
+        if niter == self.maxiter:
+            raise PoissonConvergenceError(
+                'Poisson solver did not converge in %d iterations!'
+                % self.maxiter)
+        if bool(self.gd.pbc_c.all()):
+            phi -= phi.sum() / float(self.gd.n_c.prod())
+        self.niter = niter
+        return niter
+
+    def iterate2(self, step, level=0, phi=None, rho=None):
+        """gpaw/poisson.py:500-537: one V-cycle; at level 0 returns
+        sum(r^2) dv."""
+        self._init()
+        if phi is not None:
+            self.phis[0] = phi
+        if rho is not None:
+            self.rhos[0].copy_(rho)
+        residual = self.residuals[level]
+        op = self.operators[level]
+        if level < self.levels:
+            op.relax(self.relax_method, self.phis[level], self.rhos[level],
+                     self.presmooths[level], self.weights[level])
+            op.apply(self.phis[level], residual)
+            residual -= self.rhos[level]
+            self.restrictors[level].apply(residual, self.rhos[level + 1])
+            self.phis[level + 1].zero_()
+            self.iterate2(4.0 * step, level + 1)
+            self.interpolators[level].apply(self.phis[level + 1], residual)
+            self.phis[level] -= residual
+        op.relax(self.relax_method, self.phis[level], self.rhos[level],
+                 self.postsmooths[level], self.weights[level])
+        if level == 0:
+            op.apply(self.phis[level], residual)
+            residual -= self.rhos[level]
+            r = residual.reshape(-1)
+            return float(torch.dot(r, r)) * self.gd.dv

@@ -516,6 +516,70 @@ class FDPoissonSolver:
             return error
 
 
+class WeightedFDPoissonSolver(FDPoissonSolver):
+    """gpaw/old/solvation/poisson.py:75-124, neutral systems: the V-cycle of
+    FDPoissonSolver on WeightedFDOperator([Laplace, d/dx, d/dy, d/dz])
+    weighted by eps and its gradient (div(eps grad phi) = -4 pi rho); the
+    weights of each coarser level are the restrictions of the finer ones.
+    ``stencils(gd, scale, n)`` returns the four (coefs, offsets_pc) pairs
+    of a level (the Laplacian first)."""
+
+    def __init__(self, stencils, nn=3, relax='J', eps=2e-10, maxiter=1000,
+                 be='auto'):
+        super().__init__(nn, relax, eps, maxiter, be)
+        self.stencils = stencils
+        self.eps_gradeps = None
+
+    def set_dielectric(self, eps_gradeps):
+        self.eps_gradeps = [np.ascontiguousarray(a, float)
+                            for a in eps_gradeps]
+
+    def set_grid_descriptor(self, gd):
+        super().set_grid_descriptor(gd)
+        scale = -0.25 / pi
+        gds = [gd]
+        for _ in range(self.levels):
+            gds.append(gds[-1].coarsen())
+        self.operators = [
+            WeightedFDOperator([FDOperator(c, o, g, be=self.be) for c, o in
+                                self.stencils(g, scale,
+                                              self.nn if i == 0 else 1)],
+                               be=self.be)
+            for i, g in enumerate(gds)]
+        self.gds = gds
+
+    def _init(self):
+        """:113-124: level 0 weighted by the dielectric, coarser levels by
+        arrays that restrict_op_weights fills."""
+        if self._initialized:
+            return
+        self.operators[0].set_weights(self.eps_gradeps)
+        self.op_coarse_weights = []
+        for op, g in zip(self.operators[1:], self.gds[1:]):
+            weights = [g.zeros() for _ in range(4)]
+            self.op_coarse_weights.append(weights)
+            op.set_weights(weights)
+        super()._init()
+
+    def restrict_op_weights(self):
+        """:100-106."""
+        self._init()
+        weights = [self.operators[0].weights] + self.op_coarse_weights
+        for i, res in enumerate(self.restrictors):
+            for j in range(4):
+                res.apply(weights[i][j], weights[i + 1][j])
+        self.step = 0.66666666 / self.operators[0].get_diagonal_element()
+
+    def solve(self, phi, rho, charge=None, maxcharge=1e-6,
+              zero_initial_phi=False):
+        """:87-98 for a neutral system."""
+        self._init()
+        self.restrict_op_weights()
+        if abs(self.gd.integrate(rho)) > maxcharge:
+            raise NotImplementedError('charged system with a dielectric')
+        return super().solve(phi, rho, charge, maxcharge, zero_initial_phi)
+
+
 class Preconditioner:
     """gpaw/preconditioner.py:9-73 (C path)."""
 

@@ -776,3 +776,49 @@ def test_weighted_operator_ranges(nn, dtype, pbc, cuda):
     y = x.new_zeros(x.shape)
     wop.apply(x, y, ph)
     assert np.array_equal(to_np(y), ref)
+
+
+def test_weighted_poisson_against_oracle(cuda):
+    """WeightedFDPoissonSolver (gpaw/old/solvation/poisson.py:75-124) with a
+    smooth dielectric (eps 1 inside a sphere, 80 outside) against the
+    oracle's restatement on the reference's WOperator and Transformer: the
+    same V-cycle count and the same potential, bit for bit."""
+    from gpaw_b200 import Gradient, Laplace
+    from gpaw_b200.solvation import WeightedFDPoissonSolver
+    N, cell = (32, 32, 32), (8.0, 8.0, 8.0)
+    gdo = L.GridDescriptor(N, cell, 0)
+    gdp = prod_gd(N, cell, 0)
+    x = gdo.get_grid_point_coordinates() - 4.0
+    g = np.exp(-(x**2).sum(0) / 3.0)
+    eps = 80.0 - 79.0 * g
+    grad = [79.0 * g * 2.0 * x[c] / 3.0 for c in range(3)]
+    rho = np.exp(-((x[0] - 0.6)**2 + x[1]**2 + x[2]**2)) - \
+        np.exp(-((x[0] + 0.6)**2 + x[1]**2 + x[2]**2))
+    rho -= rho.mean()
+
+    def stencils(g_, scale, n):
+        gp = prod_gd(tuple(g_.N_c), cell, 0)
+        ops = [Laplace(gp, scale, n)] + [Gradient(gp, j, scale, n)
+                                         for j in range(3)]
+        return [(op.coef_p, op.offset_pc) for op in ops]
+
+    wo = L.WeightedFDPoissonSolver(stencils, nn=3, eps=1e-14, maxiter=300)
+    wo.set_grid_descriptor(gdo)
+    wo.set_dielectric([eps] + grad)
+    wo.restrict_op_weights()
+    phi_o = gdo.zeros()
+    n_o = wo.solve_neutral(phi_o, rho)
+
+    class Dielectric:
+        eps_gradeps = [to_dev(a) for a in [eps] + grad]
+
+    ps = WeightedFDPoissonSolver(nn=3, eps=1e-14, maxiter=300)
+    ps.set_grid_descriptor(gdp)
+    ps.set_dielectric(Dielectric())
+    ps.restrict_op_weights()
+    assert ps.step == wo.step
+    phi = gdp.zeros()
+    n = ps.solve_neutral(phi, to_dev(rho))
+    assert n == n_o
+    assert np.array_equal(to_np(phi), phi_o)
+    assert 'weighted FD solver with dielectric' in ps.get_description()

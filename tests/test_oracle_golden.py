@@ -194,3 +194,43 @@ def test_weighted_operator_cases(golden):
                 assert np.array_equal(g, c[f'relax{m}']), (name, m)
         n += 1
     assert n == 5
+
+
+def _axis_stencils(gd, scale, n):
+    """A Laplacian and three central first differences (range n) as
+    (coefs, offsets) pairs, for the weighted solver on the oracle alone."""
+    lap = L.Laplace(gd, scale, n, be='port')
+    out = [(lap.coef_p, lap.offset_pc)]
+    for c in range(3):
+        e = np.zeros(3, int)
+        e[c] = 1
+        offs = [j * e for j in range(1, n + 1)] + \
+            [-j * e for j in range(1, n + 1)]
+        coefs = [0.5 / j for j in range(1, n + 1)] + \
+            [-0.5 / j for j in range(1, n + 1)]
+        out.append((np.array(coefs), np.array(offs)))
+    return out
+
+
+def test_weighted_poisson_with_unit_dielectric_is_fd_poisson():
+    """With eps = 1 and grad eps = 0 the weighted operator is the plain
+    Laplacian bit for bit (w * s = s for w = 1, and the gradient terms add
+    zeros), so the dielectric solver (gpaw/old/solvation/poisson.py:75-124)
+    must reproduce FDPoissonSolver's potential and V-cycle count exactly."""
+    gd = L.GridDescriptor((16, 12, 20), (4.0, 3.0, 5.0), (0, 0, 0))
+    x = gd.get_grid_point_coordinates()
+    rho = np.exp(-((x[0] - 2) ** 2 + (x[1] - 1.4) ** 2 + (x[2] - 2.6) ** 2)) \
+        - np.exp(-((x[0] - 1.6) ** 2 + (x[1] - 1.7) ** 2 + (x[2] - 2.2) ** 2))
+    rho -= rho.mean()
+    ps = L.FDPoissonSolver(nn=3, eps=1e-20)
+    ps.set_grid_descriptor(gd)
+    phi = gd.zeros()
+    n = ps.solve(phi, rho)
+    wps = L.WeightedFDPoissonSolver(_axis_stencils, nn=3, eps=1e-20)
+    wps.set_grid_descriptor(gd)
+    wps.set_dielectric([np.ones(tuple(gd.n_c))] +
+                       [np.zeros(tuple(gd.n_c)) for _ in range(3)])
+    wphi = gd.zeros()
+    wn = wps.solve(wphi, rho)
+    assert wn == n
+    assert np.array_equal(wphi, phi)
