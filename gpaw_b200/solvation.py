@@ -11,19 +11,24 @@ sm_100a kernels of the weighted operator and the Transformer; the residual
 updates are device arithmetic, and the level-0 error is read once per
 V-cycle to decide whether to stop, as the reference does.
 
-Neutral systems only: the charged branch needs the dielectric-aware
-compensation charge of the reference's ``load_gauss`` (not part of this
-path) and raises NotImplementedError.
+A charged system in a non-periodic cell is solved as the reference does:
+a compensation charge built from a Gaussian and the dielectric
+(``load_gauss``, :48-72) carries the charge, the neutral rest is solved,
+and the Gaussian's potential (with the same normalisation) is added back.
+Charged periodic systems raise NotImplementedError, as in the reference.
 """
 from __future__ import annotations
 
 from math import pi
 
+import numpy as np
 import torch
+from scipy.special import erf
 
 from ._lib import PoissonConvergenceError
 from .fd_operators import Gradient, Laplace
-from .poisson import FDPoissonSolver
+from .gauss import SQRT_PI, coordinates
+from .poisson import FDPoissonSolver, _solve_monopole
 from .wfd_operators import WeightedFDOperator
 
 
@@ -93,17 +98,61 @@ class WeightedFDPoissonSolver(FDPoissonSolver):
                 res.apply(weights[i][j], weights[i + 1][j])
         self.step = 0.66666666 / self.operators[0].get_diagonal_element()
 
+    def load_gauss(self, center=None):
+        """:48-72: rho = eps g - (grad v_g . grad eps) / (4 pi) for the
+        normalised Gaussian g of gpaw/utilities/gauss.py and its potential
+        v_g, both scaled so that rho carries sqrt(4 pi) of charge.  Host
+        float64, as the reference computes it; the results live on the
+        device."""
+        epsr, dx_epsr, dy_epsr, dz_epsr = [
+            t.detach().cpu().numpy() for t in self.dielectric.eps_gradeps]
+        gd = self.gd
+        xyz, r2 = coordinates(gd, center)
+        r = np.sqrt(r2)
+        if center is None:
+            a = 4 * 19.0 * (gd.icell_cv**2).sum(1).max()
+        else:
+            cell_center = gd.cell_cv.sum(1) / 2
+            r_min = (cell_center - np.abs(center - cell_center)).min()
+            a = 19.0 / r_min**2
+        rho_g = np.sqrt(a**3 * 4) / np.pi * np.exp(-a * r2)
+        phi_g = 2.0 * SQRT_PI * erf(np.sqrt(a) * r) / r
+        x, y, z = xyz
+        fac = 2. * np.sqrt(a) * np.exp(-a * r2)
+        fac /= np.sqrt(np.pi) * r2
+        fac -= erf(np.sqrt(a) * r) / (r2 * r)
+        fac *= 2.0 * SQRT_PI
+        sp = fac * x * dx_epsr + fac * y * dy_epsr + fac * z * dz_epsr
+        rho = epsr * rho_g - 1. / (4. * np.pi) * sp
+        invnorm = np.sqrt(4. * np.pi) / (rho.reshape(-1).sum() * gd.dv)
+        dev = self.dielectric.eps_gradeps[0].device
+        self.phi_gauss = torch.from_numpy(phi_g * invnorm).to(dev)
+        self.rho_gauss = torch.from_numpy(rho * invnorm).to(dev)
+        self._gauss_gd = gd
+
     def solve(self, phi, rho, charge=None, maxcharge=1e-6,
               zero_initial_phi=False, timer=None):
-        """:87-98 for a neutral system (gpaw/poisson.py:182-213)."""
+        """:87-98 and gpaw/poisson.py:182-283: neutral systems, and charged
+        ones in a non-periodic cell."""
         self._init()
         actual_charge = self.gd.integrate(rho)
-        if abs(actual_charge) > maxcharge:
-            raise NotImplementedError('charged system with a dielectric')
+        if bool(self.gd.pbc_c.all()) and abs(actual_charge) > maxcharge:
+            raise NotImplementedError(
+                'charged periodic systems are not implemented')
         self.restrict_op_weights()
-        background = (actual_charge / self.gd.dv /
-                      self.gd.get_size_of_global_array().prod())
-        return self.solve_neutral(phi, rho - background)
+        if charge is None:
+            charge = actual_charge
+        if abs(charge) <= maxcharge:
+            background = (actual_charge / self.gd.dv /
+                          self.gd.get_size_of_global_array().prod())
+            return self.solve_neutral(phi, rho - background)
+        if not bool(self.gd.pbc_c.any()):
+            if getattr(self, '_gauss_gd', None) is not self.gd:
+                self.load_gauss()
+            return _solve_monopole(self, phi, rho, actual_charge,
+                                   zero_initial_phi)
+        raise NotImplementedError(
+            'charged system with mixed boundary conditions')
 
     def solve_neutral(self, phi, rho, timer=None):
         """gpaw/poisson.py:474-498."""

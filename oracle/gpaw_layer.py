@@ -356,6 +356,12 @@ def gauss_l0(gd, a=19.0):
     the middle of the cell (gpaw/utilities/gauss.py:33-56, 94-123;
     coordinates: gpaw/utilities/tools.py:81-100; distance vectors:
     gpaw/old/grid_descriptor.py:716-737, no periodic axis here)."""
+    rho, phi, _, _, _ = _gauss_l0_parts(gd, a)
+    return rho, phi
+
+
+def _gauss_l0_parts(gd, a=19.0):
+    """gauss_l0 plus the distance vectors, r^2 and the exponent a."""
     from scipy.special import erf
     origin = 0.5 * gd.cell_cv.sum(0)
     s_Gc = (np.indices(gd.n_c, float).T + gd.beg_c) / gd.N_c
@@ -372,7 +378,7 @@ def gauss_l0(gd, a=19.0):
     exp_ar2 = np.exp(-a * r2)
     rho = np.sqrt(a**3 * 4) / pi * exp_ar2
     phi = 2.0 * 1.7724538509055159 * erf(np.sqrt(a) * r) / r
-    return rho, phi
+    return rho, phi, r_vG, r2, a
 
 
 class FDPoissonSolver:
@@ -570,13 +576,39 @@ class WeightedFDPoissonSolver(FDPoissonSolver):
                 res.apply(weights[i][j], weights[i + 1][j])
         self.step = 0.66666666 / self.operators[0].get_diagonal_element()
 
+    def load_gauss(self):
+        """:48-72: the compensation charge of a charged system in the
+        dielectric, rho = eps g - (grad v_g . grad eps) / (4 pi), normalised
+        to sqrt(4 pi), and its potential v_g with the same factor."""
+        from scipy.special import erf
+        epsr, dx_epsr, dy_epsr, dz_epsr = self.eps_gradeps
+        rho_g, phi_g, xyz, r2, a = _gauss_l0_parts(self.gd)
+        r = np.sqrt(r2)
+        x, y, z = xyz
+        fac = 2. * np.sqrt(a) * np.exp(-a * r2)
+        fac /= np.sqrt(np.pi) * r2
+        fac -= erf(np.sqrt(a) * r) / (r2 * r)
+        fac *= 2.0 * 1.7724538509055159
+        dx_phi_g = fac * x
+        dy_phi_g = fac * y
+        dz_phi_g = fac * z
+        sp = dx_phi_g * dx_epsr + dy_phi_g * dy_epsr + dz_phi_g * dz_epsr
+        rho = epsr * rho_g - 1. / (4. * np.pi) * sp
+        invnorm = np.sqrt(4. * np.pi) / self.gd.integrate(rho)
+        self.phi_gauss = phi_g * invnorm
+        self.rho_gauss = rho * invnorm
+
     def solve(self, phi, rho, charge=None, maxcharge=1e-6,
               zero_initial_phi=False):
-        """:87-98 for a neutral system."""
+        """:87-98: periodic systems must be neutral; a charged
+        non-periodic one gets the dielectric's compensation charge."""
         self._init()
+        if self.gd.pbc_c.all() and abs(self.gd.integrate(rho)) > maxcharge:
+            raise NotImplementedError(
+                'charged periodic systems are not implemented')
         self.restrict_op_weights()
-        if abs(self.gd.integrate(rho)) > maxcharge:
-            raise NotImplementedError('charged system with a dielectric')
+        if not hasattr(self, 'rho_gauss'):
+            self.load_gauss()
         return super().solve(phi, rho, charge, maxcharge, zero_initial_phi)
 
 
