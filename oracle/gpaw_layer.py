@@ -381,6 +381,142 @@ def _gauss_l0_parts(gd, a=19.0):
     return rho, phi, r_vG, r2, a
 
 
+# ---------------------------------------------------- Gaussian multipoles
+# gpaw/utilities/gauss.py:11-92 (Y_L, gauss_L, gausspot_L for L = 0..8) and
+# :95-160 (Gaussian), written from the definitions: Y_L = r^l times the real
+# harmonic (order 1; y, z, x; xy, yz, 3z^2 - r^2, xz, x^2 - y^2), g_L of unit
+# moment int g_L Y_L dV = 1, v_L its potential (del^2 v_L = -4 pi g_L).
+_MP_L = (0, 1, 1, 1, 2, 2, 2, 2, 2)
+_MP_NORM = (1 / 4, 3 / 4, 3 / 4, 3 / 4, 15 / 4, 15 / 4, 5 / 16, 15 / 4, 15 / 16)
+
+
+def _mp_poly(L, x, y, z, r2):
+    if L == 0:
+        return np.ones_like(r2)
+    return (y, z, x, x * y, y * z, 3 * z * z - r2, x * z, x * x - y * y)[L - 1]
+
+
+def mp_Y(L, x, y, z, r2):
+    return np.sqrt(_MP_NORM[L] / pi) * _mp_poly(L, x, y, z, r2)
+
+
+def mp_gauss(a, L, x, y, z, r2, exp_ar2):
+    from math import gamma
+    l = _MP_L[L]
+    c = np.sqrt(_MP_NORM[L] / pi)
+    k = (2 * pi * c / gamma(l + 1.5))**2
+    return np.sqrt(a**(2 * l + 3) * k) / pi * _mp_poly(L, x, y, z, r2) * \
+        exp_ar2
+
+
+def mp_gausspot(a, L, x, y, z, r, r2, erf_sar, exp_ar2):
+    l = _MP_L[L]
+    c = np.sqrt(_MP_NORM[L] / pi)
+    sa = np.sqrt(a) * r
+    if l == 0:
+        rad, e0 = erf_sar, 1.0
+    elif l == 1:
+        rad, e0 = np.sqrt(pi) * erf_sar - 2 * sa * exp_ar2, np.sqrt(pi)
+    else:
+        rad = 3 * np.sqrt(pi) * erf_sar - (6 + 4 * sa**2) * sa * exp_ar2
+        e0 = 3 * np.sqrt(pi)
+    return 4 * pi * c / ((2 * l + 1) * e0) * rad / r**(2 * l + 1) * \
+        _mp_poly(L, x, y, z, r2)
+
+
+class GaussianMP:
+    """Gaussian(gd, a, center) (gpaw/utilities/gauss.py:95-160) on numpy
+    grids; coordinates as gpaw/utilities/tools.py:81-100 forms them."""
+
+    def __init__(self, gd, a=19., center=None):
+        from scipy.special import erf
+        self.gd = gd
+        origin = 0.5 * gd.cell_cv.sum(0) if center is None else \
+            np.asarray(center, float)
+        s_Gc = (np.indices(gd.n_c, float).T + gd.beg_c) / gd.N_c
+        r_c = np.linalg.solve(gd.cell_cv.T, origin)
+        s_Gc -= np.where(gd.pbc_c, r_c % 1.0, r_c)
+        s_Gc -= gd.pbc_c * (2 * s_Gc).astype(int)
+        self.xyz = np.dot(s_Gc, gd.cell_cv).T.copy()
+        r2 = np.sum(self.xyz**2, axis=0)
+        self.r2 = np.where(r2 < 1e-12, 1e-12, r2)
+        self.r = np.sqrt(self.r2)
+        if center is None:
+            icell_cv = np.linalg.inv(gd.cell_cv).T
+            self.a = 4 * a * (icell_cv**2).sum(1).max()
+        else:
+            cell_center = gd.cell_cv.sum(1) / 2
+            r_min = (cell_center - np.abs(center - cell_center)).min()
+            self.a = a / r_min**2
+        self.exp_ar2 = np.exp(-self.a * self.r2)
+        self.erf_sar = erf(np.sqrt(self.a) * self.r)
+
+    def get_gauss(self, L):
+        x, y, z = self.xyz
+        return mp_gauss(self.a, L, x, y, z, self.r2, self.exp_ar2)
+
+    def get_gauss_pot(self, L):
+        x, y, z = self.xyz
+        return mp_gausspot(self.a, L, x, y, z, self.r, self.r2,
+                           self.erf_sar, self.exp_ar2)
+
+    def get_moment(self, n, L):
+        x, y, z = self.xyz
+        return self.gd.integrate(n * mp_Y(L, x, y, z, self.r2))
+
+    def remove_moment(self, n, L, q=None):
+        if q is None:
+            q = self.get_moment(n, L)
+        if abs(q) < 1e-7:
+            return 0.
+        n -= q * self.get_gauss(L)
+        return q * self.get_gauss_pot(L)
+
+
+class MomentCorrectionPoissonSolver:
+    """gpaw/poisson_moment.py:60-243: moments ``moms`` about each centre
+    (Bohr; None = the middle of the cell) removed with Gaussian multipoles,
+    every grid point assigned to its nearest centre."""
+
+    def __init__(self, poissonsolver, moment_corrections):
+        self.poissonsolver = poissonsolver
+        if isinstance(moment_corrections, int):
+            moment_corrections = [{'moms': range(moment_corrections),
+                                   'center': None}]
+        self.moment_corrections = moment_corrections
+
+    def set_grid_descriptor(self, gd):
+        self.poissonsolver.set_grid_descriptor(gd)
+        self.gd = gd
+        self.gauss_i = [GaussianMP(gd, center=m['center'])
+                        for m in moment_corrections_list(self)]
+        self.mom_ij = [np.asarray(m['moms'])
+                       for m in moment_corrections_list(self)]
+        r_ir = np.array([g.r.ravel() for g in self.gauss_i])
+        mask_ir = np.zeros(r_ir.shape, int)
+        for r in range(r_ir.shape[1]):
+            mask_ir[np.argmin(r_ir[:, r]), r] = 1
+        self.mask_ig = [m.reshape(gd.n_c) for m in mask_ir]
+
+    def solve(self, phi, rho, **kwargs):
+        rho_neutral = rho * 0.0
+        phi_cor_g = self.gd.zeros()
+        for gauss, mask_g, mom_j in zip(self.gauss_i, self.mask_ig,
+                                        self.mom_ij):
+            rho_masked = rho * mask_g
+            for mom in mom_j:
+                phi_cor_g += gauss.remove_moment(rho_masked, mom)
+            rho_neutral += rho_masked
+        phi -= phi_cor_g
+        niter = self.poissonsolver.solve(phi, rho_neutral, **kwargs)
+        phi += phi_cor_g
+        return niter
+
+
+def moment_corrections_list(ps):
+    return ps.moment_corrections
+
+
 class FDPoissonSolver:
     """gpaw/poisson.py:321-537 (neutral, periodic-charged and non-periodic
     charged (Gaussian monopole) branches)."""

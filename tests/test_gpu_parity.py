@@ -866,3 +866,45 @@ def test_weighted_poisson_charged_against_oracle(cuda):
     assert np.array_equal(to_np(ps.phi_gauss), wo.phi_gauss)
     assert n == n_o
     assert max_rel(to_np(phi), phi_o) <= RTOL_FP64
+
+
+@pytest.mark.parametrize('corr', ['center', 'two'])
+def test_moment_correction_against_oracle(corr, cuda):
+    """MomentCorrectionPoissonSolver (gpaw/poisson_moment.py:60-243) around
+    FDPoissonSolver on a charged, polarised zero-boundary system: the
+    moments removed about the middle of the cell (L = 0..8) or about two
+    centres (every point assigned to the nearer), against the oracle's
+    restatement; agreement to the 1e-12 bar (the moments are device
+    sums)."""
+    from gpaw_b200 import FDPoissonSolver
+    from gpaw_b200.poisson_moment import MomentCorrectionPoissonSolver
+    N, cell = (40, 36, 44), (10.0, 9.0, 11.0)
+    gdo = L.GridDescriptor(N, cell, 0)
+    gdp = prod_gd(N, cell, 0)
+    x = gdo.get_grid_point_coordinates()
+    c0 = np.array(cell) / 2
+    d1 = x - (c0 + np.array([1.0, 0.4, -0.6]))[:, None, None, None]
+    d2 = x - (c0 - np.array([1.2, -0.5, 0.8]))[:, None, None, None]
+    rho = np.exp(-(d1**2).sum(0) / 0.7) - 0.4 * np.exp(-(d2**2).sum(0) / 0.5)
+    if corr == 'center':
+        mc_p, mc_o = 9, 9
+    else:
+        ca = [(c0 + [1.0, 0.4, -0.6]) * 0.52917721,
+              (c0 - [1.2, -0.5, 0.8]) * 0.52917721]
+        mc_p = [{'moms': range(4), 'center': ca[0]},
+                {'moms': [0, 3, 6], 'center': ca[1]}]
+        mc_o = [{'moms': range(4), 'center': np.asarray(ca[0]) / 0.52917721},
+                {'moms': [0, 3, 6],
+                 'center': np.asarray(ca[1]) / 0.52917721}]
+    po = L.MomentCorrectionPoissonSolver(L.FDPoissonSolver(nn=3, eps=1e-18),
+                                         mc_o)
+    po.set_grid_descriptor(gdo)
+    phi_o = gdo.zeros()
+    n_o = po.solve(phi_o, rho)
+    pp = MomentCorrectionPoissonSolver(FDPoissonSolver(nn=3, eps=1e-18), mc_p)
+    pp.set_grid_descriptor(gdp)
+    phi = gdp.zeros()
+    n = pp.solve(phi, to_dev(rho))
+    assert n == n_o
+    assert max_rel(to_np(phi), phi_o) <= RTOL_FP64
+    assert 'moment corrections' in pp.get_description()

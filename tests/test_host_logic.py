@@ -175,3 +175,31 @@ def test_oracle_interpolate_density_conserves_charge():
     f = L.interpolate_density(gd, fg, nt, 3)
     assert f.shape == (2,) + tuple(fg.n_c)
     assert np.allclose(gd.integrate(nt), fg.integrate(f), rtol=1e-13, atol=0)
+
+
+def test_gaussian_multipoles_unit_moments_and_far_field():
+    """The multipole Gaussians of the moment corrections (product host code
+    and the oracle's restatement): int g_L Y_L' dV = delta_LL' for
+    L, L' = 0..8 on a fine grid, the potentials tend to the point multipole
+    4 pi / (2l+1) Y_L / r^(2l+1) far out, and both restatements agree."""
+    import numpy as np
+    from oracle import gpaw_layer as L
+    from gpaw_b200 import multipole as M
+    gd = L.GridDescriptor((64, 64, 64), (12.0, 12.0, 12.0), (0, 0, 0))
+    g = L.GaussianMP(gd, a=19.0)
+    x, y, z = g.xyz
+    for La in range(9):
+        gl = g.get_gauss(La)
+        for Lb in range(9):
+            m = gd.integrate(gl * L.mp_Y(Lb, x, y, z, g.r2))
+            assert abs(m - (La == Lb)) < 1e-6, (La, Lb, m)
+        far = g.r > 8.0      # erfc(sqrt(a) r) < 1e-14 there
+        lv = L._MP_L[La]
+        point = 4 * np.pi / (2 * lv + 1) * L.mp_Y(La, x, y, z, g.r2) / \
+            g.r**(2 * lv + 1)
+        v = g.get_gauss_pot(La)
+        assert np.allclose(v[far], point[far], rtol=1e-9, atol=1e-14)
+        mine = M.gausspot_L(g.a, La, x, y, z, g.r, g.r2, g.erf_sar, g.exp_ar2)
+        assert np.allclose(mine, v, rtol=1e-13, atol=0)
+        mineg = M.gauss_L(g.a, La, x, y, z, g.r2, g.exp_ar2)
+        assert np.allclose(mineg, gl, rtol=1e-13, atol=1e-300)
