@@ -14,6 +14,15 @@ Restated from (all single-domain, ``comm.size == 1``):
 * transformer pads  gpaw/transformers.py:19-77
 * Poisson solver    gpaw/poisson.py:182-213, 321-537
 * preconditioner    gpaw/preconditioner.py:9-93
+* weighted operator gpaw/wfd_operators.py:7-81 (C object: the reference's
+  WOperator), dielectric solver gpaw/old/solvation/poisson.py:48-124
+* density transfers gpaw/new/fd/pot_calc.py:37-41, 72-80
+* dipole layer      gpaw/dipole_correction.py:84-172
+* moment correction gpaw/poisson_moment.py:60-243 with the Gaussian
+  multipoles of gpaw/utilities/gauss.py:11-160 written from their
+  definitions: parity unpinned for this part (the reference's Python layer
+  cannot be imported here, so nothing runs the reference's own multipole
+  code); it is checked by unit moments and far fields instead
 """
 from __future__ import annotations
 
