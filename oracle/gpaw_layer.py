@@ -18,6 +18,8 @@ Restated from (all single-domain, ``comm.size == 1``):
   WOperator), dielectric solver gpaw/old/solvation/poisson.py:48-124
 * density transfers gpaw/new/fd/pot_calc.py:37-41, 72-80
 * dipole layer      gpaw/dipole_correction.py:84-172
+* extra vacuum      gpaw/poisson_extravacuum.py:13-232, with
+  gpaw/utilities/extend_grid.py:8-56
 * moment correction gpaw/poisson_moment.py:60-243 with the Gaussian
   multipoles of gpaw/utilities/gauss.py:11-160 written from their
   definitions: parity unpinned for this part (the reference's Python layer
@@ -524,6 +526,111 @@ class MomentCorrectionPoissonSolver:
 
 def moment_corrections_list(ps):
     return ps.moment_corrections
+
+
+# ------------------------------------------------------------ extra vacuum
+def extended_gd(gd, N_c):
+    """gpaw/utilities/extend_grid.py:8-44 with a target size N_c."""
+    N_c = np.array(N_c, dtype=int)
+    ext = np.tile((N_c - gd.N_c) // 2, (2, 1)).T
+    egd = GridDescriptor(N_c, gd.h_cv * N_c, gd.pbc_c)
+    egd.extend_N_cd = ext
+    return egd
+
+
+def _window(gd, egd):
+    o = egd.extend_N_cd[:, 0]
+    return tuple(slice(o[c], o[c] + gd.n_c[c]) for c in range(3))
+
+
+class ExtraVacuumPoissonSolver:
+    """gpaw/poisson_extravacuum.py:13-232 (one domain, zero boundary);
+    grid2grid between a grid and its extension is the copy of the
+    overlapping window (gpaw/utilities/grid.py:127-162)."""
+
+    def __init__(self, gpts, ps_large, ps_small=None, coarses=0,
+                 nn_coarse=3, nn_refine=3, nn_laplace=3, use_aux_grid=True,
+                 be='auto'):
+        self.N_large = np.array(gpts, dtype=int)
+        self.Ncoar = coarses
+        self.ps_large, self.ps_small = ps_large, ps_small
+        self.nn_coarse, self.nn_refine = nn_coarse, nn_refine
+        self.nn_laplace, self.use_aux = nn_laplace, use_aux_grid
+        self.be = be
+
+    def set_grid_descriptor(self, gd):
+        self.gd_sf = gd
+        N_c = self.N_large.copy()
+        self.coarser = []
+        for _ in range(self.Ncoar):
+            gd2 = gd.coarsen()
+            self.coarser.append(Transformer(gd, gd2, self.nn_coarse,
+                                            be=self.be))
+            N_c //= 2
+            gd = gd2
+        self.gd_sc = gd
+        self.gd_lc = extended_gd(self.gd_sc, N_c)
+        self.ps_large.set_grid_descriptor(self.gd_lc)
+        self.phi_lc = self.gd_lc.zeros()
+        if self.Ncoar == 0:
+            return
+        self.ps_small.set_grid_descriptor(self.gd_sf)
+        if self.use_aux:
+            buf = self.nn_refine
+            for _ in range(self.Ncoar):
+                buf = 2 * buf + self.nn_refine
+            buf += self.nn_laplace
+            div = 2**self.Ncoar
+            if buf % div != 0:
+                buf += div - buf % div
+            N_c = self.gd_sf.N_c + 2 * buf
+            if np.any(N_c > self.N_large):
+                self.use_aux = False
+                N_c = self.N_large
+            self.gd_af = extended_gd(self.gd_sf, N_c)
+        else:
+            self.gd_af = extended_gd(self.gd_sf, self.N_large)
+        self.lap = Laplace(self.gd_af, -0.25 / pi, self.nn_laplace,
+                           be=self.be)
+        self.refiner = []
+        gd = self.gd_af
+        for _ in range(self.Ncoar):
+            gd2 = gd.coarsen()
+            self.refiner.append(Transformer(gd2, gd, self.nn_refine,
+                                            be=self.be))
+            gd = gd2
+        self.refiner = self.refiner[::-1]
+        self.gd_ac = gd
+        if self.use_aux:
+            self.gd_lc_aux = extended_gd(self.gd_ac, self.gd_lc.N_c)
+
+    def solve(self, phi, rho):
+        rho_sf = rho.copy()
+        tmp = rho_sf
+        for t in self.coarser:
+            tmp = t.apply(tmp)
+        rho_lc = self.gd_lc.zeros()
+        rho_lc[_window(self.gd_sc, self.gd_lc)] = tmp
+        n_large = self.ps_large.solve(self.phi_lc, rho_lc)
+        if self.Ncoar == 0:
+            phi[:] = self.phi_lc[_window(self.gd_sf, self.gd_lc)]
+            return n_large
+        if self.use_aux:
+            tmp = self.phi_lc[_window(self.gd_ac, self.gd_lc_aux)].copy()
+        else:
+            tmp = self.phi_lc
+        for t in self.refiner:
+            tmp = t.apply(tmp)
+        rho_af = self.gd_af.zeros()
+        self.lap.apply(tmp, rho_af)
+        w = _window(self.gd_sf, self.gd_af)
+        cor_phi = tmp[w].copy()
+        cor_rho = rho_af[w].copy()
+        rho_sf -= cor_rho
+        phi -= cor_phi
+        n_small = self.ps_small.solve(phi, rho_sf)
+        phi += cor_phi
+        return (n_large, n_small)
 
 
 class FDPoissonSolver:

@@ -908,3 +908,35 @@ def test_moment_correction_against_oracle(corr, cuda):
     assert n == n_o
     assert max_rel(to_np(phi), phi_o) <= RTOL_FP64
     assert 'moment corrections' in pp.get_description()
+
+
+@pytest.mark.parametrize('coarses', [0, 1])
+def test_extra_vacuum_against_oracle(coarses, cuda):
+    """ExtraVacuumPoissonSolver (gpaw/poisson_extravacuum.py:13-232): the
+    solve on a larger grid (and, with coarses = 1, on a coarser large grid
+    whose refined potential corrects the solve on the original grid)
+    against the oracle's restatement: the same V-cycle counts, the
+    potential to the 1e-12 bar."""
+    from gpaw_b200 import FDPoissonSolver
+    from gpaw_b200.poisson_extravacuum import ExtraVacuumPoissonSolver
+    N, cell = (24, 24, 24), (6.0, 6.0, 6.0)
+    gdo = L.GridDescriptor(N, cell, 0)
+    gdp = prod_gd(N, cell, 0)
+    x = gdo.get_grid_point_coordinates() - 3.0
+    rho = np.exp(-((x[0] - 0.5)**2 + x[1]**2 + x[2]**2)) - \
+        np.exp(-((x[0] + 0.5)**2 + x[1]**2 + x[2]**2))
+    small_o = L.FDPoissonSolver(eps=1e-18) if coarses else None
+    small_p = FDPoissonSolver(eps=1e-18) if coarses else None
+    evo = L.ExtraVacuumPoissonSolver((48, 48, 48), L.FDPoissonSolver(eps=1e-18),
+                                     small_o, coarses=coarses)
+    evo.set_grid_descriptor(gdo)
+    phi_o = gdo.zeros()
+    n_o = evo.solve(phi_o, rho)
+    evp = ExtraVacuumPoissonSolver((48, 48, 48), FDPoissonSolver(eps=1e-18),
+                                   small_p, coarses=coarses)
+    evp.set_grid_descriptor(gdp)
+    phi = gdp.zeros()
+    n = evp.solve(phi, to_dev(rho))
+    assert n == n_o
+    assert max_rel(to_np(phi), phi_o) <= RTOL_FP64
+    assert 'ExtraVacuum' in evp.get_description()
