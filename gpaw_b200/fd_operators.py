@@ -226,18 +226,74 @@ def find_neighbors_orthogonal(h_cv):
     return M_ib[[i_d[d] for d in h2_d.argsort()]]
 
 
+def minkowski_basis(h_cv):
+    """A Minkowski-reduced basis of the lattice spanned by the rows of h_cv
+    and the integer matrix U_bc with h_bv = U_bc @ h_cv.  In three
+    dimensions the successive minima form a reduced basis: the shortest
+    lattice vector, the shortest one independent of it, and the shortest
+    one independent of both.  Candidates are the combinations with
+    coefficients in -3..3 of the rows of h_cv after a pairwise size
+    reduction (enough for grid spacings of any cell a DFT code meets); on
+    ties the positive combination wins, so an already reduced basis is
+    kept as it is.
+    Serves the role of ASE's reduction_full in gpaw/fd_operators.py:264;
+    the basis may differ from ASE's by order and signs, which changes
+    neither the set of neighbour directions nor the stencil, only the order
+    of its terms."""
+    h = np.array(h_cv, float)
+    U = np.eye(3, dtype=int)
+    # size reduction until no pairwise step shortens a vector
+    for _ in range(100):
+        changed = False
+        for i in range(3):
+            for j in range(3):
+                if i == j:
+                    continue
+                k = int(np.rint(h[i] @ h[j] / (h[j] @ h[j])))
+                if k and np.linalg.norm(h[i] - k * h[j]) < \
+                        np.linalg.norm(h[i]) - 1e-12:
+                    h[i] -= k * h[j]
+                    U[i] -= k * U[j]
+                    changed = True
+        if not changed:
+            break
+    M = np.array(np.meshgrid(*[np.arange(-3, 4)] * 3,
+                             indexing='ij')).reshape(3, -1).T
+    M = M[np.abs(M).sum(1) > 0]
+    vecs = M @ h
+    # shortest first; among equal lengths the combination with the larger
+    # coefficients (so +v before -v, and the size-reduced rows themselves)
+    order = np.lexsort((-M[:, 2], -M[:, 1], -M[:, 0],
+                        np.round((vecs**2).sum(1), 12)))
+    basis = []
+    for i in order:
+        cand = basis + [i]
+        if np.linalg.matrix_rank(M[cand], tol=0.5) == len(cand):
+            basis = cand
+            if len(basis) == 3:
+                break
+    U_bc = M[basis] @ U
+    return U_bc @ np.asarray(h_cv, float), U_bc
+
+
+def find_neighbors(h_cv):
+    """Neighbour directions of a general grid sorted by distance
+    (gpaw/fd_operators.py:241-282): Voronoi ridges of the centre of the
+    27-point block of a reduced basis, mapped back to the grid's axes."""
+    if np.allclose(h_cv, np.diag(np.diag(h_cv)), rtol=0, atol=1e-12):
+        return find_neighbors_orthogonal(h_cv)
+    h_bv, U_bc = minkowski_basis(h_cv)
+    return find_neighbors_orthogonal(h_bv) @ U_bc
+
+
 class Gradient(FDOperator):
     """Symmetric finite-difference derivative along x, y or z
-    (gpaw/fd_operators.py:285-354), O(h^(2n)) error.  Orthorhombic cells:
-    the reference reduces general cells with ASE's Minkowski reduction,
-    which is not available here."""
+    (gpaw/fd_operators.py:285-354), O(h^(2n)) error, for any cell: the
+    neighbour directions come from a reduced basis of the grid (see
+    minkowski_basis)."""
 
     def __init__(self, gd, v, scale=1.0, n=1, dtype=float, xp=None):
-        if not gd.orthogonal:
-            raise NotImplementedError(
-                'Gradient on a non-orthorhombic cell needs the Minkowski '
-                'reduction of the cell')
-        M_dc = find_neighbors_orthogonal(gd.h_cv)
+        M_dc = find_neighbors(gd.h_cv)
         h_dv = M_dc @ gd.h_cv
         D = len(h_dv)
         invh_vc = np.linalg.inv(gd.h_cv)

@@ -203,3 +203,36 @@ def test_gaussian_multipoles_unit_moments_and_far_field():
         assert np.allclose(mine, v, rtol=1e-13, atol=0)
         mineg = M.gauss_L(g.a, La, x, y, z, g.r2, g.exp_ar2)
         assert np.allclose(mineg, gl, rtol=1e-13, atol=1e-300)
+
+
+def test_find_neighbors_reference_examples():
+    """The examples of find_neighbors' docstring in the reference
+    (gpaw/fd_operators.py:241-260), with the reduction of minkowski_basis
+    standing in for ASE's."""
+    import numpy as np
+    from gpaw_b200.fd_operators import find_neighbors
+    assert find_neighbors([[0.1, 0, 0], [0, 0.11, 0],
+                           [0, 0, 0.12]]).tolist() == \
+        [[1, 0, 0], [0, 1, 0], [0, 0, 1]]
+    assert find_neighbors(np.array([[0.1, 0, 0], [0.2, 0.11, 0],
+                                    [0, 0, 0.12]])).tolist() == \
+        [[1, 0, 0], [-2, 1, 0], [0, 0, 1]]
+
+
+def test_gradient_stencil_general_cells():
+    """Gradient on hexagonal and triclinic cells (gpaw/fd_operators.py:
+    285-354): sum_p c_p (o_p h) = scale e_v, so linear functions are
+    differentiated exactly, for every range and direction."""
+    import numpy as np
+    from gpaw_b200 import GridDescriptor, Gradient
+    cells = [[(3.0, 0, 0), (1.5, 3.0 * 3**0.5 / 2, 0), (0, 0, 3.2)],
+             [(3.0, 0, 0), (0.6, 2.8, 0), (0.4, 0.5, 3.1)]]
+    for cell in cells:
+        gd = GridDescriptor((12, 12, 12), cell, True)
+        for n in (1, 2, 3):
+            for v in range(3):
+                g = Gradient(gd, v, 0.7, n)
+                first = (g.coef_p[:, None] * (g.offset_pc @ gd.h_cv)).sum(0)
+                e = np.zeros(3)
+                e[v] = 0.7
+                assert np.allclose(first, e, rtol=0, atol=1e-12), (cell, n, v)
