@@ -7,9 +7,19 @@ Drop-in classes with the reference's Python signatures:
 * ``FDPoissonSolver``                           (gpaw/poisson.py)
 * ``Preconditioner``                            (gpaw/preconditioner.py)
 * ``GridDescriptor``                            (gpaw/old/grid_descriptor.py)
+* ``Gradient``, ``LaplaceA``, ``LaplaceB``      (gpaw/fd_operators.py)
+* ``FDHamiltonian``                             (gpaw/new/fd/hamiltonian.py)
 
-and the C-object layer ``gpaw_b200.cgpaw`` (Operator, Transformer,
-fd_precond).  All arrays are torch CUDA tensors; the arithmetic runs in the
+and, in their own modules: ``wfd_operators.WeightedFDOperator``
+(gpaw/wfd_operators.py), ``solvation.WeightedFDPoissonSolver``
+(gpaw/old/solvation/poisson.py), ``dipole.DipoleCorrection``
+(gpaw/dipole_correction.py), ``poisson_moment.MomentCorrectionPoissonSolver``
+(gpaw/poisson_moment.py), ``poisson_extravacuum.ExtraVacuumPoissonSolver``
+(gpaw/poisson_extravacuum.py), ``pot_calc.FDDensityTransfers``
+(gpaw/new/fd/pot_calc.py); beyond the reference: ``MixedPoissonSolver``,
+``batch.PoissonBatch``, ``serving``, ``pipeline.StepPipeline``,
+``autotune``, ``replicas`` and ``domains``.  The C-object layer is
+``gpaw_b200.cgpaw`` (Operator, WOperator, Transformer, fd_precond).  All arrays are torch CUDA tensors; the arithmetic runs in the
 sm_100a kernels of ``libgpaw_b200.so`` (C ABI: include/gpaw_b200.h).
 """
 from .grid_descriptor import BadGridError, GridDescriptor

@@ -19,8 +19,6 @@ Charged periodic systems raise NotImplementedError, as in the reference.
 """
 from __future__ import annotations
 
-from math import pi
-
 import numpy as np
 import torch
 from scipy.special import erf
