@@ -119,6 +119,35 @@ class DistributedFDOperator:
         self.local.apply(ext, tmp, ph)
         out[...] = tmp[..., R:R + self.dom.m0, :, :]
 
+    def relax(self, relax_method, f, s, n, w=None):
+        """Weighted Jacobi (method 2) on the split grid: before every sweep
+        the halos of f are exchanged, the slab plus halos is swept once,
+        and its interior kept -- the same sweeps as on the whole grid.
+        Gauss-Seidel's lexicographic order does not split across slabs."""
+        if relax_method != 2:
+            raise NotImplementedError('only weighted Jacobi (2) runs on '
+                                      'slabs')
+        R = self.R
+        s_ext = s.new_zeros(s.shape[:-3] + (self.dom.m0 + 2 * R,) +
+                            s.shape[-2:])
+        s_ext[..., R:R + self.dom.m0, :, :] = s
+        for _ in range(n):
+            ext = exchange_halos(f, R, self.dom, None, self.group)
+            self.local.relax(2, ext, s_ext, 1, w)
+            f[...] = ext[..., R:R + self.dom.m0, :, :]
+
+    def residual_norm2(self, phi, rho, dv=1.0):
+        """sum over the whole grid of (L phi - rho)^2 * dv, summed over the
+        ranks (all ranks get it)."""
+        import torch.distributed as dist
+        r = phi.new_zeros(phi.shape)
+        self.apply(phi, r)
+        r -= rho
+        t = (r * r).sum().reshape(1) * dv
+        if self.dom.size > 1:
+            dist.all_reduce(t, group=self.group)
+        return float(t.item())
+
 
 def gpu_local_operator(dtype=float, device=None):
     """``make_local`` for DistributedFDOperator on a GPU: an FDOperator of

@@ -41,19 +41,25 @@ def _free_port():
 
 
 class _OracleLocal:
-    """The oracle's apply on host tensors (the slab plus halos)."""
+    """The oracle's apply and relax on host tensors (the slab plus
+    halos)."""
 
-    def __init__(self, coef_p, offset_pc, n_c, pbc_c):
+    def __init__(self, coef_p, offset_pc, n_c, pbc_c, dtype=complex):
         from oracle import gpaw_layer as L
         self.gd = L.GridDescriptor(_N_for(n_c, pbc_c), (1.0, 1.0, 1.0),
                                    pbc_c)
-        self.op = L.FDOperator(coef_p, offset_pc, self.gd,
-                               complex, be='port')
+        self.dtype = dtype
+        self.op = L.FDOperator(coef_p, offset_pc, self.gd, dtype, be='port')
 
     def apply(self, a, out, phase_cd=None):
-        b = np.zeros(tuple(a.shape), complex)
-        self.op.apply(a.numpy().astype(complex), b, phase_cd)
+        b = np.zeros(tuple(a.shape), self.dtype)
+        self.op.apply(a.numpy().astype(self.dtype), b, phase_cd)
         out.copy_(torch.from_numpy(b))
+
+    def relax(self, method, f, s, n, w=None):
+        g = f.numpy().copy()
+        self.op.relax(method, g, s.numpy(), n, w)
+        f.copy_(torch.from_numpy(g))
 
 
 def _N_for(n_c, pbc_c):
@@ -134,3 +140,58 @@ def test_single_slab_on_gpu_equals_plain_apply(cuda):
     out = x.new_zeros(x.shape)
     op.apply(x, out, ph)
     assert max_rel(to_np(out), to_np(ref)) <= 1e-12
+
+
+def _relax_worker(rank, world, port, q):
+    import torch.distributed as dist
+
+    from gpaw_b200.domains import DistributedFDOperator
+    from oracle import gpaw_layer as L
+    os.environ['MASTER_ADDR'] = '127.0.0.1'
+    os.environ['MASTER_PORT'] = str(port)
+    dist.init_process_group('gloo', rank=rank, world_size=world)
+    try:
+        gd = L.GridDescriptor((16, 12, 10), (4.0, 3.0, 2.5), (0, 0, 1))
+        rng = np.random.default_rng(11)
+        f = rng.standard_normal(tuple(gd.n_c))
+        s = rng.standard_normal(tuple(gd.n_c))
+        lap = L.Laplace(gd, -0.25 / np.pi, 3, be='port')
+        ref = f.copy()
+        lap.relax(2, ref, s, 3, 2.0 / 3.0)
+        r = np.zeros_like(ref)
+        lap.apply(ref, r)
+        r -= s
+        norm_ref = float((r * r).sum()) * gd.dv
+        dom = SlabDomain(gd.n_c, False, rank, world)
+        op = DistributedFDOperator(
+            lap.coef_p, lap.offset_pc, gd, dom,
+            lambda c, o, n, p: _OracleLocal(c, o, n, p, float))
+        fl = torch.from_numpy(f[dom.beg:dom.end].copy())
+        sl = torch.from_numpy(s[dom.beg:dom.end].copy())
+        op.relax(2, fl, sl, 3, 2.0 / 3.0)
+        norm = op.residual_norm2(fl, sl, gd.dv)
+        q.put((rank, bool(np.array_equal(fl.numpy(), ref[dom.beg:dom.end])),
+               norm, norm_ref))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_slab_jacobi_and_norm_equal_whole_grid():
+    """Three Jacobi sweeps on three slabs (halos exchanged before each) are
+    bit-identical to the sweeps on the whole grid; the residual norm summed
+    over the ranks matches the whole grid's to rounding."""
+    ctx = mp.get_context('spawn')
+    q = ctx.Queue()
+    port = _free_port()
+    world = 3
+    procs = [ctx.Process(target=_relax_worker, args=(r, world, port, q))
+             for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=120) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, same, norm, norm_ref in res:
+        assert same, rank
+        assert abs(norm - norm_ref) <= 1e-12 * norm_ref
