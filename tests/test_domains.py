@@ -195,3 +195,27 @@ def test_slab_jacobi_and_norm_equal_whole_grid():
     for rank, same, norm, norm_ref in res:
         assert same, rank
         assert abs(norm - norm_ref) <= 1e-12 * norm_ref
+
+
+@pytest.mark.gpu
+def test_single_slab_jacobi_on_gpu(cuda):
+    """One rank, zero boundary along axis 0: Jacobi sweeps on the slab
+    plus (zero) halos with the library's kernels equal the plain relax bit
+    for bit."""
+    from gpaw_b200 import GridDescriptor, Laplace
+    from gpaw_b200.domains import (DistributedFDOperator, SlabDomain,
+                                   gpu_local_operator)
+    from tests.helpers import to_dev, to_np
+    gd = GridDescriptor((20, 16, 12), (4.0, 3.2, 2.4), (0, 1, 0))
+    rng = np.random.default_rng(5)
+    f = rng.standard_normal(tuple(gd.n_c))
+    s = rng.standard_normal(tuple(gd.n_c))
+    lap = Laplace(gd, -0.25 / np.pi, 3)
+    ref = to_dev(f)
+    lap.relax(2, ref, to_dev(s), 3, 2.0 / 3.0)
+    dom = SlabDomain(gd.n_c, False, 0, 1)
+    op = DistributedFDOperator(lap.coef_p, lap.offset_pc, gd, dom,
+                               gpu_local_operator(float, ref.device))
+    fd = to_dev(f)
+    op.relax(2, fd, to_dev(s), 3, 2.0 / 3.0)
+    assert np.array_equal(to_np(fd), to_np(ref))
