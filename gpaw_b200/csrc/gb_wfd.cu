@@ -105,10 +105,24 @@ __device__ __forceinline__ void wcp_async(unsigned sdst, const void* gsrc, bool 
                      "r"(n));
 }
 
-template <class T, int R, int S>
+// Structured form of an operator list whose every operator is a centre
+// tap followed by groups of 2R taps along one axis, +1..+R then -1..-R
+// (the Laplacians and gradients of orthorhombic cells): the tap positions
+// are then compile-time offsets from the centre, and only the axis of each
+// group and the coefficients are data.
+struct WGroups {
+    int ng[GB_MAX_WEIGHTS];               // groups of operator i (0..3)
+    int axis[GB_MAX_WEIGHTS][3];
+    double c0[GB_MAX_WEIGHTS];
+    double cp[GB_MAX_WEIGHTS][3][6];      // coefficient of +d, d = 1..R
+    double cm[GB_MAX_WEIGHTS][3][6];      // coefficient of -d
+};
+
+template <class T, int R, int S, bool GROUPS>
 __global__ void __launch_bounds__(WX * WY)
 k_wfd_tiled(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phases P,
-            const __grid_constant__ WStencil s, int chunk0, int tiles_x) {
+            const __grid_constant__ WStencil s, const __grid_constant__ WGroups G, int chunk0,
+            int tiles_x) {
     constexpr int PX = WX + 2 * R, PY = WY + 2 * R, PL = PX * PY;
     constexpr int NT = WX * WY;
     constexpr int D = S - (2 * R + 1);          // planes in flight
@@ -238,16 +252,47 @@ k_wfd_tiled(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Ph
         if (!own) continue;
         const long long at = p * pstride + (long long)gy * n2 + gx;
         T x = Num<T>::zero();
-        for (int iw = 0; iw < s.nw; iw++) {
-            T tmp = Num<T>::zero();
-            const int c0 = s.start[iw], c1 = c0 + s.ncoefs[iw];
-#pragma unroll 4
-            for (int c = c0; c < c1; c++) {
-                const T v = ring[((cj + sh_o0[c]) & (S - 1)) * PL + cen + sh_ip[c]];
-                tmp = Num<T>::add(tmp, Num<T>::scale(v, sh_coef[c]));
+        if constexpr (GROUPS) {
+            const T* c = ring + (cj & (S - 1)) * PL + cen;
+            for (int iw = 0; iw < s.nw; iw++) {
+                T tmp = Num<T>::zero();
+                tmp = Num<T>::add(tmp, Num<T>::scale(c[0], G.c0[iw]));
+                for (int k = 0; k < G.ng[iw]; k++) {
+                    const int ax = G.axis[iw][k];
+                    if (ax == 0) {
+#pragma unroll
+                        for (int d = 1; d <= R; d++)
+                            tmp = Num<T>::add(tmp, Num<T>::scale(
+                                ring[((cj + d) & (S - 1)) * PL + cen], G.cp[iw][k][d - 1]));
+#pragma unroll
+                        for (int d = 1; d <= R; d++)
+                            tmp = Num<T>::add(tmp, Num<T>::scale(
+                                ring[((cj - d) & (S - 1)) * PL + cen], G.cm[iw][k][d - 1]));
+                    } else {
+                        const int sd = ax == 1 ? PX : 1;
+#pragma unroll
+                        for (int d = 1; d <= R; d++)
+                            tmp = Num<T>::add(tmp, Num<T>::scale(c[d * sd], G.cp[iw][k][d - 1]));
+#pragma unroll
+                        for (int d = 1; d <= R; d++)
+                            tmp = Num<T>::add(tmp, Num<T>::scale(c[-d * sd], G.cm[iw][k][d - 1]));
+                    }
+                }
+                tmp = Num<T>::scale(tmp, __ldg(s.w[iw] + at));
+                x = Num<T>::add(x, tmp);
             }
-            tmp = Num<T>::scale(tmp, __ldg(s.w[iw] + at));
-            x = Num<T>::add(x, tmp);
+        } else {
+            for (int iw = 0; iw < s.nw; iw++) {
+                T tmp = Num<T>::zero();
+                const int c0 = s.start[iw], c1 = c0 + s.ncoefs[iw];
+#pragma unroll 4
+                for (int c = c0; c < c1; c++) {
+                    const T v = ring[((cj + sh_o0[c]) & (S - 1)) * PL + cen + sh_ip[c]];
+                    tmp = Num<T>::add(tmp, Num<T>::scale(v, sh_coef[c]));
+                }
+                tmp = Num<T>::scale(tmp, __ldg(s.w[iw] + at));
+                x = Num<T>::add(x, tmp);
+            }
         }
         o[at] = x;
     }
@@ -364,13 +409,46 @@ struct gb_woperator {
 namespace gb {
 // Tiled apply for axis-aligned operators of range 1..6 (complex: 1..3);
 // -1 when the operator does not qualify (the gather kernel runs instead).
-template <class T, int R, int S>
-static int launch_wfd_tiled_rs(const void* in, void* out, int nin, const GridBC& g,
-                               const Phases& P, const WStencil& s, cudaStream_t st) {
+// The structured form of s for range R, if every operator has it.
+static bool wfd_groups(const WStencil& s, int R, WGroups& G) {
+    if (R < 1 || R > 6) return false;
+    memset(&G, 0, sizeof G);
+    for (int iw = 0; iw < s.nw; iw++) {
+        const int c0 = s.start[iw], n = s.ncoefs[iw];
+        if (s.off[c0][0] || s.off[c0][1] || s.off[c0][2]) return false;
+        if ((n - 1) % (2 * R) != 0 || (n - 1) / (2 * R) > 3) return false;
+        G.c0[iw] = s.coef[c0];
+        G.ng[iw] = (n - 1) / (2 * R);
+        for (int k = 0; k < G.ng[iw]; k++) {
+            const int base = c0 + 1 + k * 2 * R;
+            int ax = -1;
+            for (int a = 0; a < 3; a++)
+                if (s.off[base][a]) ax = a;
+            if (ax < 0) return false;
+            for (int d = 1; d <= R; d++) {
+                const int ip = base + d - 1, im = base + R + d - 1;
+                for (int a = 0; a < 3; a++) {
+                    if (s.off[ip][a] != (a == ax ? d : 0)) return false;
+                    if (s.off[im][a] != (a == ax ? -d : 0)) return false;
+                }
+                G.cp[iw][k][d - 1] = s.coef[ip];
+                G.cm[iw][k][d - 1] = s.coef[im];
+            }
+            G.axis[iw][k] = ax;
+        }
+    }
+    return true;
+}
+
+template <class T, int R, int S, bool GROUPS>
+static int launch_wfd_tiled_k(const void* in, void* out, int nin, const GridBC& g,
+                              const Phases& P, const WStencil& s, const WGroups& G,
+                              cudaStream_t st) {
     constexpr size_t smem = (size_t)S * (WX + 2 * R) * (WY + 2 * R) * sizeof(T);
     static bool attr_done = false;
     if (!attr_done) {
-        if (cudaFuncSetAttribute(k_wfd_tiled<T, R, S>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if (cudaFuncSetAttribute(k_wfd_tiled<T, R, S, GROUPS>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem) != cudaSuccess)
             return -2;
         attr_done = true;
@@ -383,11 +461,19 @@ static int launch_wfd_tiled_rs(const void* in, void* out, int nin, const GridBC&
     for (int b0 = 0; b0 < nin; b0 += 65535) {
         const int nb = min(65535, nin - b0);
         dim3 grid(tiles_x * tiles_y, nch, nb);
-        k_wfd_tiled<T, R, S><<<grid, WX * WY, smem, st>>>((const T*)in + b0 * ng,
-                                                         (T*)out + b0 * ng, nb, g, P, s, chunk0,
-                                                         tiles_x);
+        k_wfd_tiled<T, R, S, GROUPS><<<grid, WX * WY, smem, st>>>(
+            (const T*)in + b0 * ng, (T*)out + b0 * ng, nb, g, P, s, G, chunk0, tiles_x);
     }
     return 0;
+}
+
+template <class T, int R, int S>
+static int launch_wfd_tiled_rs(const void* in, void* out, int nin, const GridBC& g,
+                               const Phases& P, const WStencil& s, cudaStream_t st) {
+    WGroups G;
+    if (wfd_groups(s, R, G))
+        return launch_wfd_tiled_k<T, R, S, true>(in, out, nin, g, P, s, G, st);
+    return launch_wfd_tiled_k<T, R, S, false>(in, out, nin, g, P, s, G, st);
 }
 
 template <class T>
