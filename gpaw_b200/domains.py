@@ -12,6 +12,10 @@ low edge), as the reference's halo fill multiplies them.  The stencil then
 runs on the local slab plus its halos as a grid whose axis 0 has a zero
 boundary (only the halo planes' own outputs see that boundary, and they
 are dropped), with the global grid's boundary conditions on axes 1 and 2.
+
+Restriction and interpolation gather the input planes each rank's output
+reaches (``gather_planes``), and the FD Poisson V-cycle runs on slabs down
+to the levels too thin to split, which every rank then holds whole.
 """
 from __future__ import annotations
 
@@ -29,12 +33,24 @@ def slab_bounds(n0, size):
 class SlabDomain:
     """Rank ``rank`` of ``size`` owning planes [beg, end) of axis 0."""
 
-    def __init__(self, n_c, periodic0, rank, size):
+    def __init__(self, n_c, periodic0, rank, size, replicated=False):
+        """``replicated``: every rank holds the whole grid (the coarse
+        levels of a split V-cycle); halos then come from the rank's own
+        planes and nothing is sent."""
         self.n_c = tuple(int(x) for x in n_c)
         self.periodic0 = bool(periodic0)
         self.rank, self.size = int(rank), int(size)
-        self.beg, self.end = slab_bounds(self.n_c[0], self.size)[self.rank]
+        self.replicated = bool(replicated)
+        if self.replicated:
+            self.bounds = [(0, self.n_c[0])] * self.size
+        else:
+            self.bounds = slab_bounds(self.n_c[0], self.size)
+        self.beg, self.end = self.bounds[self.rank]
         self.m0 = self.end - self.beg
+        if self.replicated:
+            # the rank's own planes across a periodic edge
+            self.lower = self.upper = self.rank if self.periodic0 else None
+            return
         self.lower = self.rank - 1 if self.rank > 0 else \
             (self.size - 1 if self.periodic0 else None)
         self.upper = self.rank + 1 if self.rank < self.size - 1 else \
@@ -59,7 +75,7 @@ def exchange_halos(a, R, dom, phase_cd=None, group=None):
     hi_send = a[..., dom.m0 - R:, :, :].contiguous()
     lo_recv = torch.zeros_like(lo_send)
     hi_recv = torch.zeros_like(hi_send)
-    if dom.size == 1:
+    if dom.size == 1 or dom.replicated:
         if dom.periodic0:
             lo_recv.copy_(hi_send)
             hi_recv.copy_(lo_send)
@@ -81,9 +97,9 @@ def exchange_halos(a, R, dom, phase_cd=None, group=None):
             req.wait()
     if phase_cd is not None and a.is_complex():
         ph = np.asarray(phase_cd)
-        if dom.rank == 0 and dom.periodic0:
+        if dom.beg == 0 and dom.periodic0:
             lo_recv = lo_recv * complex(ph[0][1])
-        if dom.rank == dom.size - 1 and dom.periodic0:
+        if dom.end == dom.n_c[0] and dom.periodic0:
             hi_recv = hi_recv * complex(ph[0][0])
     if dom.lower is not None:
         ext[..., :R, :, :] = lo_recv
@@ -160,3 +176,357 @@ def gpu_local_operator(dtype=float, device=None):
         gd = GridDescriptor(N, (1.0, 1.0, 1.0), pbc_c, device=device)
         return FDOperator(coef_p, offset_pc, gd, dtype)
     return make
+
+
+def gpu_local_transformer(device=None):
+    """``make_local`` for DistributedTransformer on a GPU: a Transformer
+    object of this library with the given geometry."""
+    def make(size_in, size_out, k, pads, npads, skip, neighbors, real,
+             interpolate):
+        from . import cgpaw
+        return cgpaw.Transformer(size_in, size_out, k, pads, npads, skip,
+                                 neighbors, real, None, interpolate)
+    return make
+
+
+# --------------------------------------------------------------------------
+# any run of planes from the ranks that hold them
+# --------------------------------------------------------------------------
+def _owner(p, bounds, recv):
+    """The rank that sends global plane p to rank ``recv``: recv itself when
+    it holds p (replicated levels), else the first rank whose slab does."""
+    b, e = bounds[recv]
+    if b <= p < e:
+        return recv
+    for r, (b, e) in enumerate(bounds):
+        if b <= p < e:
+            return r
+    raise ValueError('plane %d is held by no rank' % p)
+
+
+def plane_pieces(lo, hi, n0, periodic0, bounds, recv):
+    """The planes [lo, hi) of axis 0 (indices past either edge wrap round a
+    periodic axis and are zeros past a zero boundary) as pieces
+    (owner, src_beg, src_end, dst_beg, wraps): planes src_beg..src_end-1 of
+    the owner's slab go to dst_beg.. of the receiver's buffer; ``wraps`` is
+    how many times the piece crossed the periodic edge (negative: the low
+    one).  Every rank computes every receiver's list the same way, so
+    senders and receivers agree on the pieces and their order."""
+    pieces = []
+    g = lo
+    while g < hi:
+        k, p = divmod(g, n0)
+        if k and not periodic0:
+            if g < 0:
+                g = min(0, hi)
+                continue
+            break
+        owner = _owner(p, bounds, recv)
+        ob, oe = bounds[owner]
+        take = min(oe - p, hi - g)
+        pieces.append((owner, p - ob, p - ob + take, g - lo, k))
+        g += take
+    return pieces
+
+
+def _phase_mul(t, ph):
+    """ph * t in place, each product rounded on its own and summed as
+    (a c - b d) + i (a d + b c), the grouping of the reference's complex
+    halo multiply (c/bmgs/translate.cpp:28)."""
+    import torch
+    a, b = float(ph.real), float(ph.imag)
+    r = torch.view_as_real(t)
+    c, d = r[..., 0].clone(), r[..., 1].clone()
+    r[..., 0] = c * a - d * b
+    r[..., 1] = d * a + c * b
+
+
+def gather_planes(a, needs, n0, periodic0, bounds, rank, phase_cd=None,
+                  group=None):
+    """Collective: every rank gets the global planes [lo, hi) that
+    ``needs[rank]`` names from whichever ranks hold them (``bounds[r]``:
+    the planes rank r holds in ``a``).  Returns (..., hi - lo, n1, n2):
+    zeros past a zero boundary; for complex data with ``phase_cd``, planes
+    that crossed the periodic edge upwards times phase_cd[0][0] per
+    crossing, downwards times phase_cd[0][1], as the reference's halo fill
+    multiplies them (c/bc.cpp:146-258).  The messages are one batch of
+    point-to-point sends and receives, ordered alike on both sides."""
+    import torch
+    import torch.distributed as dist
+    lo, hi = needs[rank]
+    out = a.new_zeros(a.shape[:-3] + (hi - lo,) + a.shape[-2:])
+    ops, recvd = [], []
+    for r, (rlo, rhi) in enumerate(needs):
+        for idx, (owner, sb, se, d, k) in enumerate(
+                plane_pieces(rlo, rhi, n0, periodic0, bounds, r)):
+            if r == rank and owner == rank:
+                out[..., d:d + se - sb, :, :] = a[..., sb:se, :, :]
+                recvd.append((d, se - sb, k))
+            elif r == rank:
+                buf = torch.empty_like(out[..., d:d + se - sb, :, :])
+                ops.append(dist.P2POp(dist.irecv, buf, owner, group,
+                                      tag=idx))
+                recvd.append((d, se - sb, k, buf))
+            elif owner == rank:
+                ops.append(dist.P2POp(dist.isend,
+                                      a[..., sb:se, :, :].contiguous(), r,
+                                      group, tag=idx))
+    if ops:
+        for req in dist.batch_isend_irecv(ops):
+            req.wait()
+    ph = None if phase_cd is None else np.asarray(phase_cd)
+    for item in recvd:
+        d, m, k = item[:3]
+        view = out[..., d:d + m, :, :]
+        if len(item) == 4:
+            view.copy_(item[3])
+        if k and ph is not None and a.is_complex():
+            f = ph[0][0] if k > 0 else ph[0][1]
+            for _ in range(abs(k)):
+                _phase_mul(view, complex(f))
+    return out
+
+
+def gather_full(a, dom, group=None):
+    """Collective: the whole axis 0 of a split grid on every rank."""
+    n0 = dom.n_c[0]
+    return gather_planes(a, [(0, n0)] * dom.size, n0, dom.periodic0,
+                         dom.bounds, dom.rank, None, group)
+
+
+# --------------------------------------------------------------------------
+# restriction and interpolation between split grids
+# --------------------------------------------------------------------------
+class DistributedTransformer:
+    """Restriction or interpolation (gpaw/transformers.py:18-94) from a grid
+    on slabs ``dom_in`` to one on slabs ``dom_out`` (either may be
+    replicated).  Each rank gathers the input planes that its output planes
+    reach (the stencil's K - 1 = 2 nn - 1 fine planes either side of a
+    coarse plane's centre 2 J, or the nn coarse planes either side of a fine
+    point's midpoint) and runs one transformer on them: axis 0 gets no
+    padding of its own (the gathered planes are the padding) and axes 1
+    and 2 keep the whole grid's geometry (transformer_geometry).  Every
+    output point is computed from the same values in the same order as on
+    the whole grid, so the results are identical.
+
+    ``make_local(size_in, size_out, k, pads, npads, skip, neighbors, real,
+    interpolate)`` builds the transformer of one rank (on a GPU:
+    gpu_local_transformer)."""
+
+    def __init__(self, gdin, gdout, nn, dtype, dom_in, dom_out, make_local,
+                 group=None):
+        from .transformers import transformer_geometry
+        pad, npad, skip, self.interpolate = transformer_geometry(gdin, gdout,
+                                                                 nn)
+        self.dom_in, self.dom_out, self.group = dom_in, dom_out, group
+        self.K = K = 2 * int(nn)
+        self.dtype = dtype
+        bi, bo = int(gdin.beg_c[0]), int(gdout.beg_c[0])
+        self.needs, self.keep = [], []
+        shape = None
+        for r in range(dom_out.size):
+            ob, oe = dom_out.bounds[r]
+            if oe <= ob:
+                self.needs.append((0, 0))
+                self.keep.append(0)
+                continue
+            if not self.interpolate:
+                # coarse global J is centred on fine global 2 J
+                lo = 2 * (ob + bo) - bi - (K - 1)
+                hi = 2 * (oe - 1 + bo) - bi + K
+                mcalc, s0 = oe - ob, 0
+            else:
+                # fine global G: even 2 J copies coarse J, odd 2 J + 1 reads
+                # coarse J - nn + 1 .. J + nn; the first output is dropped
+                # when the slab starts on an odd point, and one extra fine
+                # plane is computed (and dropped) so that whole coarse
+                # points are processed
+                g0 = ob + bo
+                s0 = g0 % 2
+                mf = oe - ob
+                mcalc = mf + (mf + s0) % 2
+                n = (mcalc + s0) // 2
+                lo = (g0 - s0) // 2 - bi - K // 2 + 1
+                hi = lo + n + K - 1
+            self.needs.append((lo, hi))
+            self.keep.append(oe - ob)
+            if r == dom_out.rank:
+                shape = (hi - lo, mcalc, s0)
+        self.local = None
+        if shape is not None:
+            L, mcalc, s0 = shape
+            pads = np.array(pad, np.int64).reshape(3, 2)
+            npads = np.array(npad, np.int64).reshape(3, 2)
+            skips = np.array(skip, np.int64).reshape(3, 2)
+            nb = np.array(gdin.neighbor_cd, np.int64).reshape(3, 2).copy()
+            pads[0] = npads[0] = 0
+            skips[0] = (s0, 0)
+            nb[0] = -1
+            size_in = (L,) + tuple(int(x) for x in gdin.n_c[1:])
+            size_out = (mcalc,) + tuple(int(x) for x in gdout.n_c[1:])
+            self.size_in, self.size_out = size_in, size_out
+            self.local = make_local(
+                np.array(size_in, np.int64), np.array(size_out, np.int64),
+                K, pads, npads, skips, nb, dtype == float, self.interpolate)
+
+    def apply(self, a, out, phases=None):
+        """Collective: ``a`` holds this rank's input planes, ``out`` gets its
+        output planes."""
+        ext = gather_planes(a, self.needs, self.dom_in.n_c[0],
+                            self.dom_in.periodic0, self.dom_in.bounds,
+                            self.dom_in.rank, phases, self.group)
+        if self.local is None:
+            return out
+        m = self.keep[self.dom_out.rank]
+        if self.size_out[0] == m:
+            self.local.apply(ext, out, phases)
+        else:
+            tmp = out.new_zeros(out.shape[:-3] + self.size_out)
+            self.local.apply(ext, tmp, phases)
+            out[...] = tmp[..., :m, :, :]
+        return out
+
+
+# --------------------------------------------------------------------------
+# the FD Poisson V-cycle on slabs
+# --------------------------------------------------------------------------
+class DistributedFDPoissonSolver:
+    """The V-cycle of FDPoissonSolver.iterate2 (gpaw/poisson.py:500-537) on
+    a grid split in slabs.  ``ps`` is a solver on the whole grid after
+    set_grid_descriptor: its levels, stencils, sweep counts and weights are
+    used (the coarsest level smooths 8 + 8, :451-472).  Levels stay split
+    while every slab of the level holds at least max(min_planes, R) planes
+    (R: the level's stencil range); the level below the last split one is
+    gathered whole on every rank, which run the rest of the V-cycle alike
+    and keep their own slab of the correction.  Relaxation is weighted
+    Jacobi (Gauss-Seidel's lexicographic order does not split).
+
+    ``make_op`` / ``make_tr`` build the slab-local operators and
+    transformers (gpu_local_operator / gpu_local_transformer on a GPU)."""
+
+    def __init__(self, ps, rank, size, make_op, make_tr, group=None,
+                 min_planes=2):
+        if ps.relax_method != 2:
+            raise NotImplementedError('only weighted Jacobi runs on slabs')
+        self.ps, self.group = ps, group
+        self.rank, self.size = int(rank), int(size)
+        self.levels = ps.levels
+        self.pre = list(ps.presmooths)
+        self.post = list(ps.postsmooths)
+        self.pre[self.levels] = 8
+        self.post[self.levels] = 8
+        self.weights = list(ps.weights)
+        self.relax_method = 2
+        self.gd = ps.gd
+        gds = [op.gd for op in ps.operators]
+        split = True
+        self.doms, self.ops = [], []
+        for level, (gd, op) in enumerate(zip(gds, ps.operators)):
+            offs = np.asarray(op.offset_pc, int)
+            R = int(np.abs(offs[:, 0]).max())
+            thinnest = min(e - b for b, e in slab_bounds(gd.n_c[0], size))
+            split = split and thinnest >= max(int(min_planes), R)
+            if level == 0 and not split:
+                raise ValueError('every slab of the finest grid needs at '
+                                 'least %d planes' % max(min_planes, R))
+            dom = SlabDomain(gd.n_c, bool(gd.pbc_c[0]), rank, size,
+                             replicated=not split)
+            self.doms.append(dom)
+            self.ops.append(DistributedFDOperator(op.coef_p, op.offset_pc,
+                                                  gd, dom, make_op, group))
+        self.split_levels = sum(not d.replicated for d in self.doms)
+        self.restrictors, self.interpolators = [], []
+        for level in range(self.levels):
+            r, i = ps.restrictors[level], ps.interpolators[level]
+            self.restrictors.append(DistributedTransformer(
+                gds[level], gds[level + 1], r.nn, float, self.doms[level],
+                self.doms[level + 1], make_tr, group))
+            self.interpolators.append(DistributedTransformer(
+                gds[level + 1], gds[level], i.nn, float,
+                self.doms[level + 1], self.doms[level], make_tr, group))
+        self._arrays = None
+
+    def _alloc(self, like):
+        if self._arrays is not None and self._arrays[0].device == \
+                like.device:
+            return
+        self.phis = [None]
+        self.rhos = [None]
+        self.residuals = []
+        for level, dom in enumerate(self.doms):
+            z = like.new_zeros(dom.local_shape())
+            self.residuals.append(z)
+            if level:
+                self.phis.append(like.new_zeros(dom.local_shape()))
+                self.rhos.append(like.new_zeros(dom.local_shape()))
+        self._arrays = self.residuals
+
+    def iterate(self, phi, rho):
+        """Collective: one V-cycle on this rank's slabs of phi (updated in
+        place) and rho; returns the level-0 error sum(r^2) dv over the
+        whole grid (every rank gets it)."""
+        self._alloc(phi)
+        self.phis[0] = phi
+        self.rhos[0] = rho
+        return self._cycle(0)
+
+    def _sum(self, t):
+        import torch.distributed as dist
+        t = t.sum().reshape(1)
+        if self.size > 1:
+            dist.all_reduce(t, group=self.group)
+        return float(t.item())
+
+    def solve_neutral(self, phi, rho, eps=None, maxiter=None):
+        """Collective: gpaw/poisson.py:474-498 on slabs -- V-cycles until
+        the level-0 error is at most ``eps`` (the whole-grid solver's by
+        default), then, on a fully periodic grid, the mean of phi over the
+        whole grid removed.  Returns the number of V-cycles; raises
+        PoissonConvergenceError at ``maxiter``."""
+        from ._lib import PoissonConvergenceError
+        eps = self.ps.eps if eps is None else eps
+        maxiter = self.ps.maxiter if maxiter is None else maxiter
+        niter = 1
+        while self.iterate(phi, rho) > eps and niter < maxiter:
+            niter += 1
+        if niter == maxiter:
+            raise PoissonConvergenceError(
+                'Poisson solver did not converge in %d iterations!'
+                % maxiter)
+        if bool(np.all(self.gd.pbc_c)):
+            phi -= self._sum(phi) / float(np.prod(self.gd.n_c))
+        self.niter = niter
+        return niter
+
+    def solve(self, phi, rho, charge=None, maxcharge=1e-6):
+        """Collective: gpaw/poisson.py:182-231 on slabs for neutral systems
+        and charged fully periodic ones (the homogeneous background of the
+        whole grid's charge is subtracted from rho)."""
+        actual_charge = self._sum(rho) * float(self.gd.dv)
+        background = actual_charge / float(self.gd.dv) / \
+            float(np.prod(self.gd.n_c))
+        if charge is None:
+            charge = actual_charge
+        if abs(charge) > maxcharge and not bool(np.all(self.gd.pbc_c)):
+            raise NotImplementedError('charged systems on slabs need a '
+                                      'fully periodic grid')
+        return self.solve_neutral(phi, rho - background)
+
+    def _cycle(self, level):
+        op = self.ops[level]
+        residual = self.residuals[level]
+        if level < self.levels:
+            op.relax(2, self.phis[level], self.rhos[level],
+                     self.pre[level], self.weights[level])
+            op.apply(self.phis[level], residual)
+            residual -= self.rhos[level]
+            self.restrictors[level].apply(residual, self.rhos[level + 1])
+            self.phis[level + 1].zero_()
+            self._cycle(level + 1)
+            self.interpolators[level].apply(self.phis[level + 1], residual)
+            self.phis[level] -= residual
+        op.relax(2, self.phis[level], self.rhos[level], self.post[level],
+                 self.weights[level])
+        if level == 0:
+            return op.residual_norm2(self.phis[0], self.rhos[0],
+                                     float(self.gd.dv))

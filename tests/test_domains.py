@@ -1,8 +1,9 @@
 """Slab decomposition of one grid along axis 0 over gloo ranks on the host
 (world sizes 2 and 3): the halo exchange, with the Bloch phase of axis 0
 across a periodic edge, and a stencil applied slab by slab equal to the
-same stencil on the whole grid.  The local operator here is the oracle's
-CPU apply; on GPUs the slabs run the library's kernels and the exchange
+same stencil on the whole grid; restriction, interpolation and FD Poisson
+V-cycles on slabs equal to the whole grid's.  The local operators here are
+the oracle's CPU ones; on GPUs the slabs run the library's kernels and the exchange
 goes over NCCL (one GPU per process; not run here, where a call has one
 GPU)."""
 import os
@@ -219,3 +220,207 @@ def test_single_slab_jacobi_on_gpu(cuda):
     fd = to_dev(f)
     op.relax(2, fd, to_dev(s), 3, 2.0 / 3.0)
     assert np.array_equal(to_np(fd), to_np(ref))
+
+
+def _run_ranks(world, target, args=()):
+    """Run ``target(rank, world, port, q, *args)`` on ``world`` spawned gloo
+    ranks; every rank puts one result (or ('error', traceback)) on q."""
+    ctx = mp.get_context('spawn')
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=target, args=(r, world, port, q) + args)
+             for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=240) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+    errors = [r[1] for r in res if r[0] == 'error']
+    assert not errors, errors[0]
+    assert all(p.exitcode == 0 for p in procs)
+    return res
+
+
+class _OracleTransfer:
+    """The oracle's Transformer of one rank, on host tensors."""
+
+    def __init__(self, size_in, size_out, k, pads, npads, skip, nb, real,
+                 interpolate):
+        from oracle import port
+        self.t = port.Transformer(size_in, size_out, k, pads, npads, skip,
+                                  nb, real, None, interpolate)
+        self.dtype = float if real else complex
+
+    def apply(self, a, out, phases=None):
+        b = np.zeros(tuple(out.shape), self.dtype)
+        self.t.apply(a.numpy().astype(self.dtype), b, phases)
+        out.copy_(torch.from_numpy(b))
+
+
+def _transfer_worker(rank, world, port, q):
+    import traceback
+
+    import torch.distributed as dist
+
+    from gpaw_b200.domains import DistributedTransformer
+    from oracle import gpaw_layer as L
+    os.environ['MASTER_ADDR'] = '127.0.0.1'
+    os.environ['MASTER_PORT'] = str(port)
+    dist.init_process_group('gloo', rank=rank, world_size=world)
+    try:
+        worst = []
+        for pbc0 in (1, 0):
+            gd = L.GridDescriptor((26, 12, 10), (5.2, 2.4, 2.0),
+                                  (pbc0, 1, 0))
+            gd2 = gd.coarsen()
+            ph = gd.phase_factor_cd((0.3, -0.2, 0.0))
+            for dtype in (float, complex):
+                for nn in (1, 3):
+                    for interp in (False, True):
+                        gi, go = (gd2, gd) if interp else (gd, gd2)
+                        for rep_in, rep_out in ((0, 0), (0, 1), (1, 0)):
+                            rng = np.random.default_rng(nn + 2 * pbc0)
+                            a = rng.standard_normal((2,) + tuple(gi.n_c))
+                            if dtype == complex:
+                                a = a + 1j * rng.standard_normal(a.shape)
+                            phases = ph if dtype == complex else None
+                            ref = np.zeros((2,) + tuple(go.n_c), dtype)
+                            L.Transformer(gi, go, nn, dtype, be='port') \
+                                .apply(a, ref, phases)
+                            di = SlabDomain(gi.n_c, pbc0, rank, world,
+                                            bool(rep_in))
+                            do = SlabDomain(go.n_c, pbc0, rank, world,
+                                            bool(rep_out))
+                            t = DistributedTransformer(gi, go, nn, dtype,
+                                                       di, do,
+                                                       _OracleTransfer)
+                            loc = torch.from_numpy(
+                                a[:, di.beg:di.end].copy())
+                            out = torch.zeros((2,) + do.local_shape(),
+                                              dtype=loc.dtype)
+                            t.apply(loc, out, phases)
+                            same = np.array_equal(out.numpy(),
+                                                  ref[:, do.beg:do.end])
+                            worst.append(((pbc0, dtype.__name__, nn,
+                                           interp, rep_in, rep_out), same))
+        q.put((rank, worst))
+    except Exception:
+        q.put(('error', traceback.format_exc()))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize('world', [2, 3])
+def test_slab_transfers_equal_whole_grid(world):
+    """Restriction and interpolation (nn = 1 and 3; real, and complex with
+    Bloch phases; periodic and zero axis 0; split or replicated input and
+    output) on gloo ranks give each rank exactly the planes the whole-grid
+    transformer gives.  26 planes over 2 or 3 ranks: slabs of odd and even
+    length that start on odd and even points."""
+    for rank, cases in _run_ranks(world, _transfer_worker):
+        bad = [c for c, same in cases if not same]
+        assert not bad, (rank, bad)
+
+
+def _vcycle_worker(rank, world, port, q, pbc0):
+    import traceback
+
+    import torch.distributed as dist
+
+    from gpaw_b200.domains import DistributedFDPoissonSolver
+    from oracle import gpaw_layer as L
+    os.environ['MASTER_ADDR'] = '127.0.0.1'
+    os.environ['MASTER_PORT'] = str(port)
+    dist.init_process_group('gloo', rank=rank, world_size=world)
+    try:
+        gd = L.GridDescriptor((24, 16, 16), (6.0, 4.0, 4.4), (pbc0, 1, 0))
+        rng = np.random.default_rng(17)
+        rho = rng.standard_normal(tuple(gd.n_c))
+        phi = rng.standard_normal(tuple(gd.n_c)) * 0.1
+        ps = L.FDPoissonSolver(nn=3, relax='J', be='port')
+        ps.set_grid_descriptor(gd)
+        ps._init()
+        ps.phis[0] = phi.copy()
+        ps.rhos[0][:] = rho
+        ps.errors = []
+        ref_err = [ps.iterate2(ps.step) for _ in range(3)]
+        dps = DistributedFDPoissonSolver(
+            ps, rank, world,
+            lambda c, o, n, p: _OracleLocal(c, o, n, p, float),
+            _OracleTransfer)
+        dom = dps.doms[0]
+        phl = torch.from_numpy(phi[dom.beg:dom.end].copy())
+        rhl = torch.from_numpy(rho[dom.beg:dom.end].copy())
+        err = [dps.iterate(phl, rhl) for _ in range(3)]
+        q.put((rank, bool(np.array_equal(phl.numpy(),
+                                          ps.phis[0][dom.beg:dom.end])),
+               err, ref_err, dps.split_levels, dps.levels))
+    except Exception:
+        q.put(('error', traceback.format_exc()))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize('world', [2, 3])
+@pytest.mark.parametrize('pbc0', [1, 0])
+def test_slab_vcycles_equal_whole_grid(world, pbc0):
+    """Three FD Poisson V-cycles (nn = 3, Jacobi, 4 levels) on slabs, with
+    the thin coarse levels gathered whole on every rank, leave every rank's
+    slab of phi bit-identical to the whole-grid V-cycles; the level-0
+    error summed over the ranks matches to rounding."""
+    res = _run_ranks(world, _vcycle_worker, (pbc0,))
+    for rank, same, err, ref_err, split, levels in res:
+        assert same, rank
+        assert 1 <= split <= levels
+        for e, r in zip(err, ref_err):
+            assert abs(e - r) <= 1e-12 * abs(r)
+    # some level below the finest is gathered whole in these cases
+    assert any(split < levels + 1 for _, _, _, _, split, levels in res)
+
+
+def _solve_worker(rank, world, port, q, pbc):
+    import traceback
+
+    import torch.distributed as dist
+
+    from gpaw_b200.domains import DistributedFDPoissonSolver
+    from oracle import gpaw_layer as L
+    os.environ['MASTER_ADDR'] = '127.0.0.1'
+    os.environ['MASTER_PORT'] = str(port)
+    dist.init_process_group('gloo', rank=rank, world_size=world)
+    try:
+        gd = L.GridDescriptor((16, 12, 12), (4.0, 3.0, 3.3), pbc)
+        rng = np.random.default_rng(23)
+        rho = rng.standard_normal(tuple(gd.n_c))
+        if not all(pbc):
+            rho -= rho.mean()          # neutral: no Gaussian on slabs
+        ps = L.FDPoissonSolver(nn=3, relax='J', eps=1e-8, be='port')
+        ps.set_grid_descriptor(gd)
+        ref = np.zeros(tuple(gd.n_c))
+        niter_ref = ps.solve(ref, rho)
+        dps = DistributedFDPoissonSolver(
+            ps, rank, world,
+            lambda c, o, n, p: _OracleLocal(c, o, n, p, float),
+            _OracleTransfer)
+        dom = dps.doms[0]
+        phl = torch.zeros(dom.local_shape(), dtype=torch.float64)
+        rhl = torch.from_numpy(rho[dom.beg:dom.end].copy())
+        niter = dps.solve(phl, rhl)
+        err = float(np.abs(phl.numpy() - ref[dom.beg:dom.end]).max())
+        q.put((rank, niter, niter_ref, err, float(np.abs(ref).max())))
+    except Exception:
+        q.put(('error', traceback.format_exc()))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize('pbc', [(1, 1, 1), (0, 1, 0)])
+def test_slab_solve_equals_whole_grid(pbc):
+    """The solve loop on three slabs (a charged periodic grid, whose
+    background comes from the charge summed over the ranks; a neutral
+    mixed-boundary grid) takes as many V-cycles as the whole-grid solve
+    and gives phi to 1e-11 (sums over ranks round differently)."""
+    for rank, niter, niter_ref, err, scale in _run_ranks(3, _solve_worker,
+                                                          (pbc,)):
+        assert niter == niter_ref, rank
+        assert err <= 1e-11 * scale, (rank, err)
