@@ -435,6 +435,10 @@ class DistributedFDPoissonSolver:
             self.ops.append(DistributedFDOperator(op.coef_p, op.offset_pc,
                                                   gd, dom, make_op, group))
         self.split_levels = sum(not d.replicated for d in self.doms)
+        # Mehrstellen (nn = 'M'): rho is replaced by B rho before solving
+        B = getattr(ps, 'B', None)
+        self.B = None if B is None else DistributedFDOperator(
+            B.coef_p, B.offset_pc, gds[0], self.doms[0], make_op, group)
         self.restrictors, self.interpolators = [], []
         for level in range(self.levels):
             r, i = ps.restrictors[level], ps.interpolators[level]
@@ -486,6 +490,10 @@ class DistributedFDPoissonSolver:
         from ._lib import PoissonConvergenceError
         eps = self.ps.eps if eps is None else eps
         maxiter = self.ps.maxiter if maxiter is None else maxiter
+        if self.B is not None:
+            rhob = rho.new_zeros(rho.shape)
+            self.B.apply(rho, rhob)
+            rho = rhob
         niter = 1
         while self.iterate(phi, rho) > eps and niter < maxiter:
             niter += 1
@@ -498,19 +506,46 @@ class DistributedFDPoissonSolver:
         self.niter = niter
         return niter
 
-    def solve(self, phi, rho, charge=None, maxcharge=1e-6):
-        """Collective: gpaw/poisson.py:182-231 on slabs for neutral systems
+    def solve(self, phi, rho, charge=None, maxcharge=1e-6,
+              zero_initial_phi=False, gauss=None):
+        """Collective: gpaw/poisson.py:182-283 on slabs.  Neutral systems
         and charged fully periodic ones (the homogeneous background of the
-        whole grid's charge is subtracted from rho)."""
+        whole grid's charge is subtracted from rho); charged systems in a
+        non-periodic cell through a Gaussian carrying the charge, solved
+        neutral, its potential added back.  ``gauss``: the whole grid's
+        (rho_gauss, phi_gauss), by default gauss.monopole_gaussian of the
+        grid (each rank keeps its slab)."""
         actual_charge = self._sum(rho) * float(self.gd.dv)
         background = actual_charge / float(self.gd.dv) / \
             float(np.prod(self.gd.n_c))
         if charge is None:
             charge = actual_charge
-        if abs(charge) > maxcharge and not bool(np.all(self.gd.pbc_c)):
-            raise NotImplementedError('charged systems on slabs need a '
-                                      'fully periodic grid')
-        return self.solve_neutral(phi, rho - background)
+        pbc = np.asarray(self.gd.pbc_c, bool)
+        if abs(charge) <= maxcharge:
+            return self.solve_neutral(phi, rho - background)
+        if pbc.all():
+            if zero_initial_phi:
+                phi.zero_()
+            return self.solve_neutral(phi, rho - background)
+        if pbc.any():
+            raise NotImplementedError(
+                'charged system with mixed boundary conditions')
+        if gauss is None:
+            from .gauss import monopole_gaussian
+            gauss = monopole_gaussian(self.gd)
+        import torch
+        dom = self.doms[0]
+        rg, pg = [torch.as_tensor(np.ascontiguousarray(
+            np.asarray(g)[dom.beg:dom.end])).to(phi.device) for g in gauss]
+        q = actual_charge / np.sqrt(4 * np.pi)
+        rho_neutral = rho - q * rg
+        if zero_initial_phi:
+            phi.zero_()
+        else:
+            phi -= q * pg
+        niter = self.solve_neutral(phi, rho_neutral)
+        phi += q * pg
+        return niter
 
     def _cycle(self, level):
         op = self.ops[level]

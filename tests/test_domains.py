@@ -378,7 +378,7 @@ def test_slab_vcycles_equal_whole_grid(world, pbc0):
     assert any(split < levels + 1 for _, _, _, _, split, levels in res)
 
 
-def _solve_worker(rank, world, port, q, pbc):
+def _solve_worker(rank, world, port, q, case):
     import traceback
 
     import torch.distributed as dist
@@ -389,12 +389,13 @@ def _solve_worker(rank, world, port, q, pbc):
     os.environ['MASTER_PORT'] = str(port)
     dist.init_process_group('gloo', rank=rank, world_size=world)
     try:
+        pbc, nn = case
         gd = L.GridDescriptor((16, 12, 12), (4.0, 3.0, 3.3), pbc)
         rng = np.random.default_rng(23)
         rho = rng.standard_normal(tuple(gd.n_c))
-        if not all(pbc):
-            rho -= rho.mean()          # neutral: no Gaussian on slabs
-        ps = L.FDPoissonSolver(nn=3, relax='J', eps=1e-8, be='port')
+        if any(pbc) and not all(pbc):
+            rho -= rho.mean()          # mixed boundaries: neutral only
+        ps = L.FDPoissonSolver(nn=nn, relax='J', eps=1e-8, be='port')
         ps.set_grid_descriptor(gd)
         ref = np.zeros(tuple(gd.n_c))
         niter_ref = ps.solve(ref, rho)
@@ -405,7 +406,8 @@ def _solve_worker(rank, world, port, q, pbc):
         dom = dps.doms[0]
         phl = torch.zeros(dom.local_shape(), dtype=torch.float64)
         rhl = torch.from_numpy(rho[dom.beg:dom.end].copy())
-        niter = dps.solve(phl, rhl)
+        gauss = None if any(pbc) else L.gauss_l0(gd)
+        niter = dps.solve(phl, rhl, gauss=gauss)
         err = float(np.abs(phl.numpy() - ref[dom.beg:dom.end]).max())
         q.put((rank, niter, niter_ref, err, float(np.abs(ref).max())))
     except Exception:
@@ -414,13 +416,16 @@ def _solve_worker(rank, world, port, q, pbc):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize('pbc', [(1, 1, 1), (0, 1, 0)])
-def test_slab_solve_equals_whole_grid(pbc):
-    """The solve loop on three slabs (a charged periodic grid, whose
-    background comes from the charge summed over the ranks; a neutral
-    mixed-boundary grid) takes as many V-cycles as the whole-grid solve
-    and gives phi to 1e-11 (sums over ranks round differently)."""
+@pytest.mark.parametrize('case', [((1, 1, 1), 3), ((0, 1, 0), 3),
+                                  ((0, 0, 0), 3), ((1, 1, 1), 'M')])
+def test_slab_solve_equals_whole_grid(case):
+    """The solve loop on three slabs -- a charged periodic grid (the
+    background from the charge summed over the ranks), a neutral
+    mixed-boundary grid, a charged zero-boundary grid (Gaussian monopole
+    removal), the Mehrstellen stencil (B rho on slabs) -- takes as many
+    V-cycles as the whole-grid solve and gives phi to 1e-11 (sums over
+    ranks round differently)."""
     for rank, niter, niter_ref, err, scale in _run_ranks(3, _solve_worker,
-                                                          (pbc,)):
+                                                          (case,)):
         assert niter == niter_ref, rank
         assert err <= 1e-11 * scale, (rank, err)
