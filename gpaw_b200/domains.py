@@ -98,9 +98,9 @@ def exchange_halos(a, R, dom, phase_cd=None, group=None):
     if phase_cd is not None and a.is_complex():
         ph = np.asarray(phase_cd)
         if dom.beg == 0 and dom.periodic0:
-            lo_recv = lo_recv * complex(ph[0][1])
+            _phase_mul(lo_recv, complex(ph[0][1]))
         if dom.end == dom.n_c[0] and dom.periodic0:
-            hi_recv = hi_recv * complex(ph[0][0])
+            _phase_mul(hi_recv, complex(ph[0][0]))
     if dom.lower is not None:
         ext[..., :R, :, :] = lo_recv
     if dom.upper is not None:
@@ -565,3 +565,82 @@ class DistributedFDPoissonSolver:
         if level == 0:
             return op.residual_norm2(self.phis[0], self.rhos[0],
                                      float(self.gd.dv))
+
+
+# --------------------------------------------------------------------------
+# the multigrid preconditioner on slabs
+# --------------------------------------------------------------------------
+class DistributedPreconditioner:
+    """The three-level preconditioner of gpaw/preconditioner.py:9-73 (the
+    sequence of c/fd_preconditioner.cpp:106-351, scalar factors 4 step and
+    16 step) on a grid split in slabs.  ``pre`` is a Preconditioner on the
+    whole grid: its kinetic operators, step and transformer orders are
+    used.  Levels 1 and 2 stay split while every slab holds at least
+    ``min_planes`` planes, else every rank holds them whole.
+    ``make_op`` / ``make_tr`` build the slab-local operators and
+    transformers for the preconditioner's dtype."""
+
+    def __init__(self, pre, rank, size, make_op, make_tr, group=None,
+                 min_planes=2):
+        kins = [pre.kin0, pre.kin1, pre.kin2]
+        gds = [k.gd for k in kins]
+        self.step = float(pre.step)
+        self.group = group
+        dtype = getattr(pre.kin1, 'dtype', float)
+        self.doms, self.kin = [], []
+        split = True
+        for level, (gd, k) in enumerate(zip(gds, kins)):
+            R = int(np.abs(np.asarray(k.offset_pc, int)[:, 0]).max())
+            thinnest = min(e - b for b, e in slab_bounds(gd.n_c[0], size))
+            split = split and thinnest >= max(int(min_planes), R)
+            if level == 0 and not split:
+                raise ValueError('every slab of the finest grid needs at '
+                                 'least %d planes' % max(min_planes, R))
+            dom = SlabDomain(gd.n_c, bool(gd.pbc_c[0]), rank, size,
+                             replicated=not split)
+            self.doms.append(dom)
+            self.kin.append(DistributedFDOperator(k.coef_p, k.offset_pc, gd,
+                                                  dom, make_op, group))
+        d0, d1, d2 = self.doms
+
+        def tr(obj, gi, go, di, do):
+            return DistributedTransformer(gi, go, obj.nn, dtype, di, do,
+                                          make_tr, group)
+        self.rest0 = tr(pre.restrictor_object0, gds[0], gds[1], d0, d1)
+        self.rest1 = tr(pre.restrictor_object1, gds[1], gds[2], d1, d2)
+        self.intp2 = tr(pre.interpolator_object2, gds[2], gds[1], d2, d1)
+        self.intp1 = tr(pre.interpolator_object1, gds[1], gds[0], d1, d0)
+
+    def __call__(self, residuals, phases=None, out=None):
+        """Collective: the preconditioned residuals of this rank's slab
+        (leading batch axes allowed); ``out`` if given receives them."""
+        lead = residuals.shape[:-3]
+        s4, s16 = 4 * self.step, 16 * self.step
+
+        def z(level):
+            return residuals.new_zeros(lead + self.doms[level].local_shape())
+        r1, d1, q1 = z(1), z(1), z(1)
+        r2, q2 = z(2), z(2)
+        d0 = out if out is not None else z(0)
+        q0 = z(0)
+        self.rest0.apply(-residuals, r1, phases)
+        d1.copy_(s4 * r1)
+        self.kin[1].apply(d1, q1, phases)
+        q1 -= r1
+        self.rest1.apply(q1, r2, phases)
+        d2 = s16 * r2
+        self.kin[2].apply(d2, q2, phases)
+        q2 -= r2
+        d2 -= s16 * q2
+        self.intp2.apply(d2, q1, phases)
+        d1 -= q1
+        self.kin[1].apply(d1, q1, phases)
+        q1 -= r1
+        d1 -= s4 * q1
+        d1.neg_()
+        self.intp1.apply(d1, d0, phases)
+        self.kin[0].apply(d0, q0, phases)
+        q0 -= residuals
+        d0 -= self.step * q0
+        d0.neg_()
+        return d0

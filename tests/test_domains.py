@@ -102,6 +102,9 @@ def _worker(rank, world, port, pbc0, q):
 @pytest.mark.parametrize('world', [2, 3])
 @pytest.mark.parametrize('pbc0', [1, 0])
 def test_slab_apply_equals_whole_grid(world, pbc0):
+    """Complex apply with Bloch phases on slabs: the planes that cross the
+    periodic edge take the phase with the reference's complex grouping, so
+    every rank's planes equal the whole grid's exactly."""
     ctx = mp.get_context('spawn')
     q = ctx.Queue()
     port = _free_port()
@@ -114,7 +117,7 @@ def test_slab_apply_equals_whole_grid(world, pbc0):
         p.join(timeout=60)
         assert p.exitcode == 0
     for rank, err, scale in res:
-        assert err <= 1e-12 * scale, (rank, err)
+        assert err == 0.0, (rank, err)
 
 
 @pytest.mark.gpu
@@ -429,3 +432,49 @@ def test_slab_solve_equals_whole_grid(case):
                                                           (case,)):
         assert niter == niter_ref, rank
         assert err <= 1e-11 * scale, (rank, err)
+
+
+def _precond_worker(rank, world, port, q, pbc0):
+    import traceback
+
+    import torch.distributed as dist
+
+    from gpaw_b200.domains import DistributedPreconditioner
+    from oracle import gpaw_layer as L
+    os.environ['MASTER_ADDR'] = '127.0.0.1'
+    os.environ['MASTER_PORT'] = str(port)
+    dist.init_process_group('gloo', rank=rank, world_size=world)
+    try:
+        gd = L.GridDescriptor((24, 16, 12), (4.8, 3.2, 2.4), (pbc0, 1, 1))
+        ph = gd.phase_factor_cd((0.25, -0.1, 0.2))
+        rng = np.random.default_rng(29)
+        res = rng.standard_normal((2,) + tuple(gd.n_c)) + \
+            1j * rng.standard_normal((2,) + tuple(gd.n_c))
+        kin0 = L.Laplace(gd, -0.5, 3, complex, be='port')
+        pre = L.Preconditioner(gd, kin0, complex, block=2, be='port')
+        ref = pre(res, ph).copy()
+        dp = DistributedPreconditioner(
+            pre, rank, world,
+            lambda c, o, n, p: _OracleLocal(c, o, n, p, complex),
+            _OracleTransfer)
+        dom = dp.doms[0]
+        got = dp(torch.from_numpy(res[:, dom.beg:dom.end].copy()), ph)
+        q.put((rank, bool(np.array_equal(got.numpy(),
+                                          ref[:, dom.beg:dom.end])),
+               [d.replicated for d in dp.doms]))
+    except Exception:
+        q.put(('error', traceback.format_exc()))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize('pbc0', [1, 0])
+def test_slab_preconditioner_equals_whole_grid(pbc0):
+    """The three-level preconditioner on three slabs (complex, Bloch
+    phases, two residuals; with a zero axis 0 the coarsest level is held
+    whole on every rank) gives each rank exactly the planes of the
+    whole-grid preconditioner."""
+    res = _run_ranks(3, _precond_worker, (pbc0,))
+    for rank, same, rep in res:
+        assert same, (rank, rep)
+    assert res[0][2][2] == (not pbc0)
