@@ -420,10 +420,9 @@ class DistributedFDPoissonSolver:
         self.gd = ps.gd
         gds = [op.gd for op in ps.operators]
         split = True
-        self.doms, self.ops = [], []
+        self.doms = []
         for level, (gd, op) in enumerate(zip(gds, ps.operators)):
-            offs = np.asarray(op.offset_pc, int)
-            R = int(np.abs(offs[:, 0]).max())
+            R = self._op_range(op)
             thinnest = min(e - b for b, e in slab_bounds(gd.n_c[0], size))
             split = split and thinnest >= max(int(min_planes), R)
             if level == 0 and not split:
@@ -432,13 +431,8 @@ class DistributedFDPoissonSolver:
             dom = SlabDomain(gd.n_c, bool(gd.pbc_c[0]), rank, size,
                              replicated=not split)
             self.doms.append(dom)
-            self.ops.append(DistributedFDOperator(op.coef_p, op.offset_pc,
-                                                  gd, dom, make_op, group))
         self.split_levels = sum(not d.replicated for d in self.doms)
-        # Mehrstellen (nn = 'M'): rho is replaced by B rho before solving
-        B = getattr(ps, 'B', None)
-        self.B = None if B is None else DistributedFDOperator(
-            B.coef_p, B.offset_pc, gds[0], self.doms[0], make_op, group)
+        self.B = None
         self.restrictors, self.interpolators = [], []
         for level in range(self.levels):
             r, i = ps.restrictors[level], ps.interpolators[level]
@@ -449,6 +443,23 @@ class DistributedFDPoissonSolver:
                 gds[level + 1], gds[level], i.nn, float,
                 self.doms[level + 1], self.doms[level], make_tr, group))
         self._arrays = None
+        self._build_ops(make_op, gds)
+
+    @staticmethod
+    def _op_range(op):
+        """Planes of axis 0 the level's stencil reaches."""
+        return int(np.abs(np.asarray(op.offset_pc, int)[:, 0]).max())
+
+    def _build_ops(self, make_op, gds):
+        ps, group = self.ps, self.group
+        self.ops = [DistributedFDOperator(op.coef_p, op.offset_pc, gd, dom,
+                                          make_op, group)
+                    for op, gd, dom in zip(ps.operators, gds, self.doms)]
+        # Mehrstellen (nn = 'M'): rho is replaced by B rho before solving
+        B = getattr(ps, 'B', None)
+        if B is not None:
+            self.B = DistributedFDOperator(B.coef_p, B.offset_pc, gds[0],
+                                           self.doms[0], make_op, group)
 
     def _alloc(self, like):
         if self._arrays is not None and self._arrays[0].device == \
@@ -565,6 +576,98 @@ class DistributedFDPoissonSolver:
         if level == 0:
             return op.residual_norm2(self.phis[0], self.rhos[0],
                                      float(self.gd.dv))
+
+
+# --------------------------------------------------------------------------
+# weighted operators and the dielectric Poisson solver on slabs
+# --------------------------------------------------------------------------
+class DistributedWeightedOperator(DistributedFDOperator):
+    """A WeightedFDOperator (gpaw/wfd_operators.py) on a grid split in
+    slabs: sum_i w_i(x) L_i with this rank's slabs of the weights.  The
+    weights' halo planes are exchanged once, here; apply and the Jacobi
+    sweeps exchange the operand's halos as DistributedFDOperator does.
+    The stencils' flattened offsets depend only on the padded extents of
+    axes 1 and 2, which the slab shares with the whole grid, so they are
+    used unchanged.  ``make_local(nweights, weights, coef_ps, offset_ps,
+    n_c, r, neighbors, real, cfd)`` builds the WOperator of one slab plus
+    halos (on a GPU: gpu_local_woperator)."""
+
+    def __init__(self, wop, weights, dom, make_local, group=None):
+        self.R = R = int(wop.mp)
+        self.dom, self.group = dom, group
+        n_ext = (dom.m0 + 2 * R,) + tuple(int(x) for x in wop.gd.n_c[1:])
+        nb = np.array(wop.gd.neighbor_cd, np.int64).reshape(3, 2).copy()
+        nb[0] = -1
+        self.weights_ext = [exchange_halos(w, R, dom, None, group)
+                            for w in weights]
+        self.local = make_local(wop.nweights, self.weights_ext, wop.coef_ps,
+                                wop.offset_ps, np.array(n_ext, np.int64), R,
+                                nb, wop.dtype == float, wop.cfd)
+
+
+def gpu_local_woperator():
+    """``make_local`` for DistributedWeightedOperator on a GPU: a WOperator
+    of this library."""
+    def make(nweights, weights, coef_ps, offset_ps, n_c, r, neighbors, real,
+             cfd):
+        from . import cgpaw
+        return cgpaw.WOperator(nweights, weights, coef_ps, offset_ps, n_c, r,
+                               neighbors, real, None, cfd)
+    return make
+
+
+class DistributedWeightedFDPoissonSolver(DistributedFDPoissonSolver):
+    """The dielectric Poisson solver's V-cycle
+    (gpaw/old/solvation/poisson.py:75-124) on slabs: level 0 weighted by
+    this rank's slabs of eps and its gradient (``eps_gradeps``), every
+    coarser level by the restrictions of the finer level's weights
+    (restrict_op_weights, :100-106) through the slab transformers.
+    ``ps`` is the whole-grid WeightedFDPoissonSolver after
+    set_grid_descriptor; ``make_op`` builds weighted slab operators."""
+
+    def __init__(self, ps, eps_gradeps, rank, size, make_op, make_tr,
+                 group=None, min_planes=2):
+        self._eps_gradeps = list(eps_gradeps)
+        super().__init__(ps, rank, size, make_op, make_tr, group,
+                         min_planes)
+
+    @staticmethod
+    def _op_range(op):
+        return int(op.mp)
+
+    def solve(self, phi, rho, charge=None, maxcharge=1e-6,
+              zero_initial_phi=False, gauss=None):
+        """Collective: :87-98 on slabs.  Periodic systems must be neutral;
+        a charged one in a non-periodic cell needs the dielectric's
+        compensation charge and its potential on the whole grid,
+        ``gauss=(rho_gauss, phi_gauss)`` (WeightedFDPoissonSolver.
+        load_gauss), of which each rank keeps its slab."""
+        actual_charge = self._sum(rho) * float(self.gd.dv)
+        pbc = np.asarray(self.gd.pbc_c, bool)
+        if pbc.all() and abs(actual_charge) > maxcharge:
+            raise NotImplementedError(
+                'charged periodic systems are not implemented')
+        q = actual_charge if charge is None else charge
+        if abs(q) > maxcharge and not pbc.any() and gauss is None:
+            raise ValueError('a charged system in a dielectric needs '
+                             'gauss=(rho_gauss, phi_gauss) of the whole '
+                             'grid')
+        return super().solve(phi, rho, charge, maxcharge, zero_initial_phi,
+                             gauss)
+
+    def _build_ops(self, make_op, gds):
+        weights = self._eps_gradeps
+        self.ops = []
+        for level, (op, dom) in enumerate(zip(self.ps.operators,
+                                              self.doms)):
+            self.ops.append(DistributedWeightedOperator(op, weights, dom,
+                                                        make_op, self.group))
+            if level < self.levels:
+                nxt = [w.new_zeros(self.doms[level + 1].local_shape())
+                       for w in weights]
+                for w, c in zip(weights, nxt):
+                    self.restrictors[level].apply(w, c)
+                weights = nxt
 
 
 # --------------------------------------------------------------------------
