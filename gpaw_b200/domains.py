@@ -61,51 +61,19 @@ class SlabDomain:
 
 
 def exchange_halos(a, R, dom, phase_cd=None, group=None):
-    """Local slab a (..., m0, n1, n2) -> (..., m0 + 2R, n1, n2) with the
-    neighbours' planes (zeros past a zero boundary).  Works on torch
-    tensors on any device the process group can send from."""
-    import torch
-    import torch.distributed as dist
-    if dom.m0 < R:
-        raise ValueError('every slab needs at least R = %d planes' % R)
-    shape = a.shape[:-3] + (dom.m0 + 2 * R,) + a.shape[-2:]
-    ext = a.new_zeros(shape)
-    ext[..., R:R + dom.m0, :, :] = a
-    lo_send = a[..., :R, :, :].contiguous()
-    hi_send = a[..., dom.m0 - R:, :, :].contiguous()
-    lo_recv = torch.zeros_like(lo_send)
-    hi_recv = torch.zeros_like(hi_send)
-    if dom.size == 1 or dom.replicated:
-        if dom.periodic0:
-            lo_recv.copy_(hi_send)
-            hi_recv.copy_(lo_send)
-    else:
-        # sends: top planes up (tag 0), bottom planes down (tag 1); receives
-        # in the matching order, so that two ranks that are each other's
-        # upper and lower neighbour (two ranks, periodic) pair the messages
-        # correctly on backends that match by order as well as by tag
-        reqs = []
-        if dom.upper is not None:
-            reqs.append(dist.isend(hi_send, dom.upper, group, tag=0))
-        if dom.lower is not None:
-            reqs.append(dist.isend(lo_send, dom.lower, group, tag=1))
-        if dom.lower is not None:
-            reqs.append(dist.irecv(lo_recv, dom.lower, group, tag=0))
-        if dom.upper is not None:
-            reqs.append(dist.irecv(hi_recv, dom.upper, group, tag=1))
-        for req in reqs:
-            req.wait()
-    if phase_cd is not None and a.is_complex():
-        ph = np.asarray(phase_cd)
-        if dom.beg == 0 and dom.periodic0:
-            _phase_mul(lo_recv, complex(ph[0][1]))
-        if dom.end == dom.n_c[0] and dom.periodic0:
-            _phase_mul(hi_recv, complex(ph[0][0]))
-    if dom.lower is not None:
-        ext[..., :R, :, :] = lo_recv
-    if dom.upper is not None:
-        ext[..., R + dom.m0:, :, :] = hi_recv
-    return ext
+    """Collective: local slab a (..., m0, n1, n2) -> (..., m0 + 2R, n1, n2)
+    with the R planes on either side from the ranks that hold them (zeros
+    past a zero boundary; planes that crossed a periodic edge times the
+    Bloch phase of axis 0 when ``phase_cd`` is given: phase_cd[0][1] for the
+    low halo of the first slab, [0][0] for the high halo of the last).  One
+    gather_planes: the sends and receives go as one batch, ordered alike on
+    both sides, so two ranks that are each other's upper and lower
+    neighbour cannot wait on each other; slabs thinner than R take planes
+    from ranks further away.  Works on torch tensors on any device the
+    process group can send from."""
+    needs = [(b - R, e + R) for b, e in dom.bounds]
+    return gather_planes(a, needs, dom.n_c[0], dom.periodic0, dom.bounds,
+                         dom.rank, phase_cd, group)
 
 
 class DistributedFDOperator:
