@@ -30,23 +30,55 @@ def slab_bounds(n0, size):
     return list(zip(beg, end))
 
 
-class SlabDomain:
-    """Rank ``rank`` of ``size`` owning planes [beg, end) of axis 0."""
+class GridDomain:
+    """Rank ``rank`` of a P0 x P1 process grid (rank = r0 P1 + r1) owning
+    the box [beg, end) x [beg1, end1) of axes 0 and 1 (axis 2 whole).
+    ``replicated``: every rank holds the whole grid (the coarse levels of a
+    split V-cycle); halos then come from the rank's own planes and nothing
+    is sent.  Axis 1 counts as split when P1 > 1."""
+
+    def __init__(self, n_c, pbc01, rank, dims, replicated=False):
+        self.n_c = tuple(int(x) for x in n_c)
+        self.periodic = (bool(pbc01[0]), bool(pbc01[1]))
+        self.periodic0 = self.periodic[0]
+        self.dims = (int(dims[0]), int(dims[1]))
+        self.rank = int(rank)
+        self.size = self.dims[0] * self.dims[1]
+        self.replicated = bool(replicated)
+        n0, n1 = self.n_c[:2]
+        if self.replicated:
+            self.boxes = [((0, n0), (0, n1))] * self.size
+        else:
+            b0 = slab_bounds(n0, self.dims[0])
+            b1 = slab_bounds(n1, self.dims[1])
+            self.boxes = [(b0[r // self.dims[1]], b1[r % self.dims[1]])
+                          for r in range(self.size)]
+        self.bounds = [b[0] for b in self.boxes]
+        (self.beg, self.end), (self.beg1, self.end1) = self.boxes[self.rank]
+        self.m0 = self.end - self.beg
+        self.m1 = self.end1 - self.beg1
+        self.split1 = self.dims[1] > 1
+
+    def local_shape(self):
+        return (self.m0, self.m1, self.n_c[2])
+
+    def thinnest(self):
+        """Fewest points of a rank's box along each split axis (axis 0, and
+        axis 1 when split), as a box of an unreplicated split would have."""
+        t = [min(e - b for b, e in slab_bounds(self.n_c[0], self.dims[0]))]
+        if self.split1:
+            t.append(min(e - b for b, e in
+                         slab_bounds(self.n_c[1], self.dims[1])))
+        return tuple(t)
+
+
+class SlabDomain(GridDomain):
+    """Rank ``rank`` of ``size`` owning planes [beg, end) of axis 0: the
+    P0 x 1 grid, with the neighbouring ranks along axis 0."""
 
     def __init__(self, n_c, periodic0, rank, size, replicated=False):
-        """``replicated``: every rank holds the whole grid (the coarse
-        levels of a split V-cycle); halos then come from the rank's own
-        planes and nothing is sent."""
-        self.n_c = tuple(int(x) for x in n_c)
-        self.periodic0 = bool(periodic0)
-        self.rank, self.size = int(rank), int(size)
-        self.replicated = bool(replicated)
-        if self.replicated:
-            self.bounds = [(0, self.n_c[0])] * self.size
-        else:
-            self.bounds = slab_bounds(self.n_c[0], self.size)
-        self.beg, self.end = self.bounds[self.rank]
-        self.m0 = self.end - self.beg
+        super().__init__(n_c, (periodic0, False), rank, (size, 1),
+                         replicated)
         if self.replicated:
             # the rank's own planes across a periodic edge
             self.lower = self.upper = self.rank if self.periodic0 else None
@@ -56,69 +88,95 @@ class SlabDomain:
         self.upper = self.rank + 1 if self.rank < self.size - 1 else \
             (0 if self.periodic0 else None)
 
-    def local_shape(self):
-        return (self.m0,) + self.n_c[1:]
+
+def make_domain(n_c, pbc_c, rank, size, dims=None, replicated=False):
+    """A SlabDomain of ``size`` ranks, or the GridDomain of the P0 x P1
+    grid ``dims``."""
+    if dims is None or int(dims[1]) == 1:
+        return SlabDomain(n_c, bool(pbc_c[0]), rank, size, replicated)
+    if int(dims[0]) * int(dims[1]) != int(size):
+        raise ValueError('dims %s do not make %d ranks' % (dims, size))
+    return GridDomain(n_c, (bool(pbc_c[0]), bool(pbc_c[1])), rank, dims,
+                      replicated)
 
 
 def exchange_halos(a, R, dom, phase_cd=None, group=None):
-    """Collective: local slab a (..., m0, n1, n2) -> (..., m0 + 2R, n1, n2)
-    with the R planes on either side from the ranks that hold them (zeros
-    past a zero boundary; planes that crossed a periodic edge times the
-    Bloch phase of axis 0 when ``phase_cd`` is given: phase_cd[0][1] for the
-    low halo of the first slab, [0][0] for the high halo of the last).  One
-    gather_planes: the sends and receives go as one batch, ordered alike on
-    both sides, so two ranks that are each other's upper and lower
-    neighbour cannot wait on each other; slabs thinner than R take planes
-    from ranks further away.  Works on torch tensors on any device the
-    process group can send from."""
-    needs = [(b - R, e + R) for b, e in dom.bounds]
-    return gather_planes(a, needs, dom.n_c[0], dom.periodic0, dom.bounds,
-                         dom.rank, phase_cd, group)
+    """Collective: local box a (..., m0, m1, n2) -> (..., m0 + 2 R0,
+    m1 + 2 R1, n2) with the R0 planes on either side along axis 0 (and R1
+    along a split axis 1; ``R`` is R0 or (R0, R1)) from the ranks that hold
+    them: zeros past a zero boundary; points that crossed a periodic edge
+    times the Bloch phase when ``phase_cd`` is given (phase_cd[c][1] per
+    crossing of the low edge of axis c, [c][0] of the high edge; axis 0
+    first, then axis 1, as the reference's halo fill of edges and corners
+    multiplies them).  One gather_box: the sends and receives go as one
+    batch, ordered alike on both sides, so two ranks that are each other's
+    upper and lower neighbour cannot wait on each other; boxes thinner than
+    the halo take points from ranks further away.  Works on torch tensors
+    on any device the process group can send from."""
+    R0, R1 = (R, R) if np.isscalar(R) else (int(R[0]), int(R[1]))
+    if not dom.split1:
+        R1 = 0
+    needs = [((b0 - R0, e0 + R0), (b1 - R1, e1 + R1))
+             for (b0, e0), (b1, e1) in dom.boxes]
+    return gather_box(a, needs, dom.boxes, dom.rank, dom.n_c[:2],
+                      dom.periodic, phase_cd, group)
 
 
 class DistributedFDOperator:
-    """A stencil (coef_p, offset_pc) applied to a grid split in slabs.
-    ``make_local(coef_p, offset_pc, n_c, pbc_c)`` builds the operator of
-    one slab plus halos (``n_c`` points, zero boundary along axis 0): on a
-    GPU an FDOperator of gpaw_b200; any object with
-    ``apply(in, out, phase_cd)``."""
+    """A stencil (coef_p, offset_pc) applied to a grid split in slabs (or
+    boxes of a P0 x P1 grid).  ``make_local(coef_p, offset_pc, n_c,
+    pbc_c)`` builds the operator of one box plus halos (``n_c`` points,
+    zero boundary along the split axes): on a GPU an FDOperator of
+    gpaw_b200; any object with ``apply(in, out, phase_cd)``."""
 
     def __init__(self, coef_p, offset_pc, gd, dom, make_local, group=None):
         offset_pc = np.asarray(offset_pc, int)
-        self.R = int(np.abs(offset_pc[:, 0]).max()) if len(offset_pc) else 0
+        reach = np.abs(offset_pc).max(0) if len(offset_pc) else (0, 0, 0)
+        self.R = int(reach[0])
+        self.R1 = int(reach[1]) if dom.split1 else 0
         self.dom, self.group = dom, group
-        n_ext = (dom.m0 + 2 * self.R,) + tuple(int(x) for x in gd.n_c[1:])
-        pbc = (False,) + tuple(bool(p) for p in gd.pbc_c[1:])
+        n1 = dom.m1 + 2 * self.R1 if dom.split1 else int(gd.n_c[1])
+        n_ext = (dom.m0 + 2 * self.R, n1, int(gd.n_c[2]))
+        pbc = (False, False if dom.split1 else bool(gd.pbc_c[1]),
+               bool(gd.pbc_c[2]))
         self.local = make_local(coef_p, offset_pc, n_ext, pbc)
 
+    def _halos(self, a, phase_cd=None):
+        return exchange_halos(a, (self.R, self.R1), self.dom, phase_cd,
+                              self.group)
+
+    def _inner(self, ext):
+        R, R1, dom = self.R, self.R1, self.dom
+        return ext[..., R:R + dom.m0, R1:R1 + dom.m1, :]
+
     def apply(self, a, out, phase_cd=None):
-        R = self.R
-        ext = exchange_halos(a, R, self.dom, phase_cd, self.group) if R \
-            else a
+        ext = self._halos(a, phase_cd)
         tmp = ext.new_zeros(ext.shape)
         ph = None
         if phase_cd is not None:
             ph = np.array(phase_cd, complex)
-            ph[0] = 1.0              # axis 0 phases travelled with the halos
+            ph[0] = 1.0              # split axes' phases travelled with
+            if self.dom.split1:      # the halos
+                ph[1] = 1.0
         self.local.apply(ext, tmp, ph)
-        out[...] = tmp[..., R:R + self.dom.m0, :, :]
+        out[...] = self._inner(tmp)
 
     def relax(self, relax_method, f, s, n, w=None):
         """Weighted Jacobi (method 2) on the split grid: before every sweep
-        the halos of f are exchanged, the slab plus halos is swept once,
+        the halos of f are exchanged, the box plus halos is swept once,
         and its interior kept -- the same sweeps as on the whole grid.
-        Gauss-Seidel's lexicographic order does not split across slabs."""
+        Gauss-Seidel's lexicographic order does not split across ranks."""
         if relax_method != 2:
             raise NotImplementedError('only weighted Jacobi (2) runs on '
                                       'slabs')
-        R = self.R
-        s_ext = s.new_zeros(s.shape[:-3] + (self.dom.m0 + 2 * R,) +
-                            s.shape[-2:])
-        s_ext[..., R:R + self.dom.m0, :, :] = s
+        s_ext = s.new_zeros(s.shape[:-3] + (
+            self.dom.m0 + 2 * self.R, self.dom.m1 + 2 * self.R1,
+            s.shape[-1]))
+        self._inner(s_ext)[...] = s
         for _ in range(n):
-            ext = exchange_halos(f, R, self.dom, None, self.group)
+            ext = self._halos(f)
             self.local.relax(2, ext, s_ext, 1, w)
-            f[...] = ext[..., R:R + self.dom.m0, :, :]
+            f[...] = self._inner(ext)
 
     def residual_norm2(self, phi, rho, dv=1.0):
         """sum over the whole grid of (L phi - rho)^2 * dv, summed over the
@@ -160,40 +218,56 @@ def gpu_local_transformer(device=None):
 # --------------------------------------------------------------------------
 # any run of planes from the ranks that hold them
 # --------------------------------------------------------------------------
-def _owner(p, bounds, recv):
-    """The rank that sends global plane p to rank ``recv``: recv itself when
-    it holds p (replicated levels), else the first rank whose slab does."""
-    b, e = bounds[recv]
-    if b <= p < e:
-        return recv
-    for r, (b, e) in enumerate(bounds):
-        if b <= p < e:
-            return r
-    raise ValueError('plane %d is held by no rank' % p)
-
-
-def plane_pieces(lo, hi, n0, periodic0, bounds, recv):
-    """The planes [lo, hi) of axis 0 (indices past either edge wrap round a
-    periodic axis and are zeros past a zero boundary) as pieces
-    (owner, src_beg, src_end, dst_beg, wraps): planes src_beg..src_end-1 of
-    the owner's slab go to dst_beg.. of the receiver's buffer; ``wraps`` is
-    how many times the piece crossed the periodic edge (negative: the low
-    one).  Every rank computes every receiver's list the same way, so
-    senders and receivers agree on the pieces and their order."""
-    pieces = []
+def _segments(lo, hi, n, periodic, cuts):
+    """[lo, hi) of one axis (indices past either edge wrap round a periodic
+    axis and are zeros past a zero boundary) as runs (dst, p, length, wraps)
+    that cross neither a wrap edge nor any rank's box boundary (``cuts``):
+    global points p.. go to dst.. of the receiver's buffer; ``wraps`` counts
+    the crossings of the periodic edge (negative: the low one)."""
+    segs = []
     g = lo
     while g < hi:
-        k, p = divmod(g, n0)
-        if k and not periodic0:
+        k, p = divmod(g, n)
+        if k and not periodic:
             if g < 0:
                 g = min(0, hi)
                 continue
             break
-        owner = _owner(p, bounds, recv)
-        ob, oe = bounds[owner]
-        take = min(oe - p, hi - g)
-        pieces.append((owner, p - ob, p - ob + take, g - lo, k))
+        nxt = min([c for c in cuts if c > p] + [n])
+        take = min(nxt - p, hi - g)
+        segs.append((g - lo, p, take, k))
         g += take
+    return segs
+
+
+def _owner(p0, p1, boxes, recv):
+    """The rank that sends point (p0, p1) of axes 0 and 1 to rank ``recv``:
+    recv itself when it holds it (replicated levels), else the first rank
+    whose box does."""
+    for r in [recv] + list(range(len(boxes))):
+        (b0, e0), (b1, e1) = boxes[r]
+        if b0 <= p0 < e0 and b1 <= p1 < e1:
+            return r
+    raise ValueError('point (%d, %d) is held by no rank' % (p0, p1))
+
+
+def box_pieces(need, n01, periodic01, boxes, recv):
+    """The box ``need`` = ((lo0, hi0), (lo1, hi1)) of axes 0 and 1 as
+    pieces (owner, (src0, src1), (dst0, dst1), (len0, len1), (k0, k1)):
+    points src.. of the owner's box go to dst.. of the receiver's buffer,
+    having crossed the periodic edges k0 and k1 times.  Every rank computes
+    every receiver's list the same way, so senders and receivers agree on
+    the pieces and their order."""
+    cuts = [sorted({x for b in boxes for x in b[c]}) for c in (0, 1)]
+    segs = [_segments(need[c][0], need[c][1], n01[c], periodic01[c],
+                      cuts[c]) for c in (0, 1)]
+    pieces = []
+    for d0, p0, l0, k0 in segs[0]:
+        for d1, p1, l1, k1 in segs[1]:
+            owner = _owner(p0, p1, boxes, recv)
+            (ob0, _), (ob1, _) = boxes[owner]
+            pieces.append((owner, (p0 - ob0, p1 - ob1), (d0, d1), (l0, l1),
+                           (k0, k1)))
     return pieces
 
 
@@ -209,57 +283,75 @@ def _phase_mul(t, ph):
     r[..., 1] = d * a + c * b
 
 
-def gather_planes(a, needs, n0, periodic0, bounds, rank, phase_cd=None,
-                  group=None):
-    """Collective: every rank gets the global planes [lo, hi) that
-    ``needs[rank]`` names from whichever ranks hold them (``bounds[r]``:
-    the planes rank r holds in ``a``).  Returns (..., hi - lo, n1, n2):
-    zeros past a zero boundary; for complex data with ``phase_cd``, planes
-    that crossed the periodic edge upwards times phase_cd[0][0] per
-    crossing, downwards times phase_cd[0][1], as the reference's halo fill
+def gather_box(a, needs, boxes, rank, n01, periodic01, phase_cd=None,
+               group=None):
+    """Collective: every rank gets the points ``needs[rank]`` = ((lo0,
+    hi0), (lo1, hi1)) of axes 0 and 1 (axis 2 whole) of a grid of n01
+    points on those axes from whichever ranks hold them (``boxes[r]``: the
+    box rank r holds in ``a``).  Returns
+    (..., hi0 - lo0, hi1 - lo1, n2): zeros past a zero boundary; for
+    complex data with ``phase_cd``, points that crossed the periodic edge
+    of axis c upwards times phase_cd[c][0] per crossing, downwards times
+    phase_cd[c][1], axis 0 before axis 1, as the reference's halo fill
     multiplies them (c/bc.cpp:146-258).  The messages are one batch of
     point-to-point sends and receives, ordered alike on both sides."""
     import torch
     import torch.distributed as dist
-    lo, hi = needs[rank]
-    out = a.new_zeros(a.shape[:-3] + (hi - lo,) + a.shape[-2:])
+    (lo0, hi0), (lo1, hi1) = needs[rank]
+    out = a.new_zeros(a.shape[:-3] + (hi0 - lo0, hi1 - lo1, a.shape[-1]))
     ops, recvd = [], []
-    for r, (rlo, rhi) in enumerate(needs):
-        for idx, (owner, sb, se, d, k) in enumerate(
-                plane_pieces(rlo, rhi, n0, periodic0, bounds, r)):
+    for r, need in enumerate(needs):
+        for idx, (owner, src, dst, ln, k) in enumerate(
+                box_pieces(need, n01, periodic01, boxes, r)):
+            sl = (Ellipsis, slice(src[0], src[0] + ln[0]),
+                  slice(src[1], src[1] + ln[1]), slice(None))
+            dl = (Ellipsis, slice(dst[0], dst[0] + ln[0]),
+                  slice(dst[1], dst[1] + ln[1]), slice(None))
             if r == rank and owner == rank:
-                out[..., d:d + se - sb, :, :] = a[..., sb:se, :, :]
-                recvd.append((d, se - sb, k))
+                out[dl] = a[sl]
+                recvd.append((dl, k, None))
             elif r == rank:
-                buf = torch.empty_like(out[..., d:d + se - sb, :, :])
+                buf = torch.empty_like(out[dl])
                 ops.append(dist.P2POp(dist.irecv, buf, owner, group,
                                       tag=idx))
-                recvd.append((d, se - sb, k, buf))
+                recvd.append((dl, k, buf))
             elif owner == rank:
-                ops.append(dist.P2POp(dist.isend,
-                                      a[..., sb:se, :, :].contiguous(), r,
+                ops.append(dist.P2POp(dist.isend, a[sl].contiguous(), r,
                                       group, tag=idx))
     if ops:
         for req in dist.batch_isend_irecv(ops):
             req.wait()
     ph = None if phase_cd is None else np.asarray(phase_cd)
-    for item in recvd:
-        d, m, k = item[:3]
-        view = out[..., d:d + m, :, :]
-        if len(item) == 4:
-            view.copy_(item[3])
-        if k and ph is not None and a.is_complex():
-            f = ph[0][0] if k > 0 else ph[0][1]
-            for _ in range(abs(k)):
-                _phase_mul(view, complex(f))
+    for dl, k, buf in recvd:
+        view = out[dl]
+        if buf is not None:
+            view.copy_(buf)
+        if ph is None or not a.is_complex():
+            continue
+        for c in (0, 1):
+            if k[c]:
+                f = ph[c][0] if k[c] > 0 else ph[c][1]
+                for _ in range(abs(k[c])):
+                    _phase_mul(view, complex(f))
     return out
 
 
+def gather_planes(a, needs, n0, periodic0, bounds, rank, phase_cd=None,
+                  group=None):
+    """Collective: gather_box along axis 0 alone -- every rank gets the
+    global planes [lo, hi) that ``needs[rank]`` names from the ranks whose
+    planes ``bounds`` lists."""
+    n1 = a.shape[-2]
+    return gather_box(a, [(tuple(nd), (0, n1)) for nd in needs],
+                      [(tuple(b), (0, n1)) for b in bounds], rank,
+                      (n0, n1), (periodic0, False), phase_cd, group)
+
+
 def gather_full(a, dom, group=None):
-    """Collective: the whole axis 0 of a split grid on every rank."""
-    n0 = dom.n_c[0]
-    return gather_planes(a, [(0, n0)] * dom.size, n0, dom.periodic0,
-                         dom.bounds, dom.rank, None, group)
+    """Collective: the whole of a split grid on every rank."""
+    n0, n1 = dom.n_c[:2]
+    return gather_box(a, [((0, n0), (0, n1))] * dom.size, dom.boxes,
+                      dom.rank, dom.n_c[:2], dom.periodic, None, group)
 
 
 # --------------------------------------------------------------------------
@@ -267,13 +359,14 @@ def gather_full(a, dom, group=None):
 # --------------------------------------------------------------------------
 class DistributedTransformer:
     """Restriction or interpolation (gpaw/transformers.py:18-94) from a grid
-    on slabs ``dom_in`` to one on slabs ``dom_out`` (either may be
-    replicated).  Each rank gathers the input planes that its output planes
-    reach (the stencil's K - 1 = 2 nn - 1 fine planes either side of a
-    coarse plane's centre 2 J, or the nn coarse planes either side of a fine
-    point's midpoint) and runs one transformer on them: axis 0 gets no
-    padding of its own (the gathered planes are the padding) and axes 1
-    and 2 keep the whole grid's geometry (transformer_geometry).  Every
+    on slabs (or boxes) ``dom_in`` to one on ``dom_out`` of the same shape
+    of process grid (either may be replicated).  Each rank gathers the
+    input points that its output points reach along the split axes (the
+    stencil's K - 1 = 2 nn - 1 fine points either side of a coarse point's
+    centre 2 J, or the nn coarse points either side of a fine midpoint) and
+    runs one transformer on them: the split axes get no padding of their
+    own (the gathered points are the padding) and the others keep the whole
+    grid's geometry (transformer_geometry).  Every
     output point is computed from the same values in the same order as on
     the whole grid, so the results are identical.
 
@@ -289,75 +382,108 @@ class DistributedTransformer:
         self.dom_in, self.dom_out, self.group = dom_in, dom_out, group
         self.K = K = 2 * int(nn)
         self.dtype = dtype
-        bi, bo = int(gdin.beg_c[0]), int(gdout.beg_c[0])
+        axes = (0, 1) if dom_out.split1 else (0,)
+        self.axes = axes
         self.needs, self.keep = [], []
-        shape = None
+        mine = None
         for r in range(dom_out.size):
-            ob, oe = dom_out.bounds[r]
-            if oe <= ob:
-                self.needs.append((0, 0))
-                self.keep.append(0)
+            geo = [self._axis(dom_out.boxes[r][c], int(gdin.beg_c[c]),
+                              int(gdout.beg_c[c]), K) for c in axes]
+            if any(g is None for g in geo):
+                self.needs.append(((0, 0), (0, 0)))
+                self.keep.append(None)
                 continue
-            if not self.interpolate:
-                # coarse global J is centred on fine global 2 J
-                lo = 2 * (ob + bo) - bi - (K - 1)
-                hi = 2 * (oe - 1 + bo) - bi + K
-                mcalc, s0 = oe - ob, 0
-            else:
-                # fine global G: even 2 J copies coarse J, odd 2 J + 1 reads
-                # coarse J - nn + 1 .. J + nn; the first output is dropped
-                # when the slab starts on an odd point, and one extra fine
-                # plane is computed (and dropped) so that whole coarse
-                # points are processed
-                g0 = ob + bo
-                s0 = g0 % 2
-                mf = oe - ob
-                mcalc = mf + (mf + s0) % 2
-                n = (mcalc + s0) // 2
-                lo = (g0 - s0) // 2 - bi - K // 2 + 1
-                hi = lo + n + K - 1
-            self.needs.append((lo, hi))
-            self.keep.append(oe - ob)
+            full1 = (0, int(gdin.n_c[1]))
+            self.needs.append((geo[0][:2], geo[1][:2] if dom_out.split1
+                               else full1))
+            self.keep.append(tuple(e - b for b, e in dom_out.boxes[r]))
             if r == dom_out.rank:
-                shape = (hi - lo, mcalc, s0)
+                mine = geo
         self.local = None
-        if shape is not None:
-            L, mcalc, s0 = shape
+        if mine is not None:
             pads = np.array(pad, np.int64).reshape(3, 2)
             npads = np.array(npad, np.int64).reshape(3, 2)
             skips = np.array(skip, np.int64).reshape(3, 2)
             nb = np.array(gdin.neighbor_cd, np.int64).reshape(3, 2).copy()
-            pads[0] = npads[0] = 0
-            skips[0] = (s0, 0)
-            nb[0] = -1
-            size_in = (L,) + tuple(int(x) for x in gdin.n_c[1:])
-            size_out = (mcalc,) + tuple(int(x) for x in gdout.n_c[1:])
-            self.size_in, self.size_out = size_in, size_out
+            size_in = [int(x) for x in gdin.n_c]
+            size_out = [int(x) for x in gdout.n_c]
+            for c, (lo, hi, mcalc, s0) in zip(axes, mine):
+                pads[c] = npads[c] = 0
+                skips[c] = (s0, 0)
+                nb[c] = -1
+                size_in[c] = hi - lo
+                size_out[c] = mcalc
+            self.size_in, self.size_out = tuple(size_in), tuple(size_out)
             self.local = make_local(
                 np.array(size_in, np.int64), np.array(size_out, np.int64),
                 K, pads, npads, skips, nb, dtype == float, self.interpolate)
 
+    def _axis(self, box, bi, bo, K):
+        """(lo, hi, mcalc, s0) along one split axis for the output points
+        [ob, oe): the input points [lo, hi) they reach, the outputs the
+        local transformer computes and its skip of the first one; None
+        for an empty box."""
+        ob, oe = box
+        if oe <= ob:
+            return None
+        if not self.interpolate:
+            # coarse global J is centred on fine global 2 J
+            lo = 2 * (ob + bo) - bi - (K - 1)
+            hi = 2 * (oe - 1 + bo) - bi + K
+            return lo, hi, oe - ob, 0
+        # fine global G: even 2 J copies coarse J, odd 2 J + 1 reads coarse
+        # J - nn + 1 .. J + nn; the first output is dropped when the box
+        # starts on an odd point, and one extra fine point is computed (and
+        # dropped) so that whole coarse points are processed
+        g0 = ob + bo
+        s0 = g0 % 2
+        mf = oe - ob
+        mcalc = mf + (mf + s0) % 2
+        n = (mcalc + s0) // 2
+        lo = (g0 - s0) // 2 - bi - K // 2 + 1
+        return lo, lo + n + K - 1, mcalc, s0
+
     def apply(self, a, out, phases=None):
-        """Collective: ``a`` holds this rank's input planes, ``out`` gets its
-        output planes."""
-        ext = gather_planes(a, self.needs, self.dom_in.n_c[0],
-                            self.dom_in.periodic0, self.dom_in.bounds,
-                            self.dom_in.rank, phases, self.group)
+        """Collective: ``a`` holds this rank's input box, ``out`` gets its
+        output box."""
+        di = self.dom_in
+        ext = gather_box(a, self.needs, di.boxes, di.rank, di.n_c[:2],
+                         di.periodic, phases, self.group)
         if self.local is None:
             return out
-        m = self.keep[self.dom_out.rank]
-        if self.size_out[0] == m:
+        m0, m1 = self.keep[self.dom_out.rank]
+        if tuple(self.size_out[:2]) == (m0, m1):
             self.local.apply(ext, out, phases)
         else:
             tmp = out.new_zeros(out.shape[:-3] + self.size_out)
             self.local.apply(ext, tmp, phases)
-            out[...] = tmp[..., :m, :, :]
+            out[...] = tmp[..., :m0, :m1, :]
         return out
 
 
 # --------------------------------------------------------------------------
 # the FD Poisson V-cycle on slabs
 # --------------------------------------------------------------------------
+def _level_domains(gds, ranges, rank, size, dims, min_planes):
+    """The domain of every level: split (slabs, or boxes of the process
+    grid ``dims``) while each rank's extent along every split axis is at
+    least max(min_planes, R) points, whole on every rank below."""
+    doms = []
+    split = True
+    for level, (gd, R) in enumerate(zip(gds, ranges)):
+        dom = make_domain(gd.n_c, gd.pbc_c, rank, size, dims)
+        need = max(int(min_planes), int(R))
+        split = split and min(dom.thinnest()) >= need
+        if level == 0 and not split:
+            raise ValueError('every rank needs at least %d points of the '
+                             'finest grid along each split axis' % need)
+        if not split:
+            dom = make_domain(gd.n_c, gd.pbc_c, rank, size, dims,
+                              replicated=True)
+        doms.append(dom)
+    return doms
+
+
 class DistributedFDPoissonSolver:
     """The V-cycle of FDPoissonSolver.iterate2 (gpaw/poisson.py:500-537) on
     a grid split in slabs.  ``ps`` is a solver on the whole grid after
@@ -373,7 +499,7 @@ class DistributedFDPoissonSolver:
     transformers (gpu_local_operator / gpu_local_transformer on a GPU)."""
 
     def __init__(self, ps, rank, size, make_op, make_tr, group=None,
-                 min_planes=2):
+                 min_planes=2, dims=None):
         if ps.relax_method != 2:
             raise NotImplementedError('only weighted Jacobi runs on slabs')
         self.ps, self.group = ps, group
@@ -387,18 +513,9 @@ class DistributedFDPoissonSolver:
         self.relax_method = 2
         self.gd = ps.gd
         gds = [op.gd for op in ps.operators]
-        split = True
-        self.doms = []
-        for level, (gd, op) in enumerate(zip(gds, ps.operators)):
-            R = self._op_range(op)
-            thinnest = min(e - b for b, e in slab_bounds(gd.n_c[0], size))
-            split = split and thinnest >= max(int(min_planes), R)
-            if level == 0 and not split:
-                raise ValueError('every slab of the finest grid needs at '
-                                 'least %d planes' % max(min_planes, R))
-            dom = SlabDomain(gd.n_c, bool(gd.pbc_c[0]), rank, size,
-                             replicated=not split)
-            self.doms.append(dom)
+        self.doms = _level_domains(gds, [self._op_range(op)
+                                         for op in ps.operators],
+                                   rank, size, dims, min_planes)
         self.split_levels = sum(not d.replicated for d in self.doms)
         self.B = None
         self.restrictors, self.interpolators = [], []
@@ -415,8 +532,8 @@ class DistributedFDPoissonSolver:
 
     @staticmethod
     def _op_range(op):
-        """Planes of axis 0 the level's stencil reaches."""
-        return int(np.abs(np.asarray(op.offset_pc, int)[:, 0]).max())
+        """Points the level's stencil reaches along an axis."""
+        return int(np.abs(np.asarray(op.offset_pc, int)).max())
 
     def _build_ops(self, make_op, gds):
         ps, group = self.ps, self.group
@@ -561,7 +678,13 @@ class DistributedWeightedOperator(DistributedFDOperator):
     halos (on a GPU: gpu_local_woperator)."""
 
     def __init__(self, wop, weights, dom, make_local, group=None):
+        if dom.split1:
+            # a split axis 1 changes the padded extent the flattened
+            # offsets were built for
+            raise NotImplementedError('weighted operators split axis 0 '
+                                      'only')
         self.R = R = int(wop.mp)
+        self.R1 = 0
         self.dom, self.group = dom, group
         n_ext = (dom.m0 + 2 * R,) + tuple(int(x) for x in wop.gd.n_c[1:])
         nb = np.array(wop.gd.neighbor_cd, np.int64).reshape(3, 2).copy()
@@ -597,7 +720,7 @@ class DistributedWeightedFDPoissonSolver(DistributedFDPoissonSolver):
                  group=None, min_planes=2):
         self._eps_gradeps = list(eps_gradeps)
         super().__init__(ps, rank, size, make_op, make_tr, group,
-                         min_planes)
+                         min_planes, None)
 
     @staticmethod
     def _op_range(op):
@@ -652,26 +775,19 @@ class DistributedPreconditioner:
     transformers for the preconditioner's dtype."""
 
     def __init__(self, pre, rank, size, make_op, make_tr, group=None,
-                 min_planes=2):
+                 min_planes=2, dims=None):
         kins = [pre.kin0, pre.kin1, pre.kin2]
         gds = [k.gd for k in kins]
         self.step = float(pre.step)
         self.group = group
         dtype = getattr(pre.kin1, 'dtype', float)
-        self.doms, self.kin = [], []
-        split = True
-        for level, (gd, k) in enumerate(zip(gds, kins)):
-            R = int(np.abs(np.asarray(k.offset_pc, int)[:, 0]).max())
-            thinnest = min(e - b for b, e in slab_bounds(gd.n_c[0], size))
-            split = split and thinnest >= max(int(min_planes), R)
-            if level == 0 and not split:
-                raise ValueError('every slab of the finest grid needs at '
-                                 'least %d planes' % max(min_planes, R))
-            dom = SlabDomain(gd.n_c, bool(gd.pbc_c[0]), rank, size,
-                             replicated=not split)
-            self.doms.append(dom)
-            self.kin.append(DistributedFDOperator(k.coef_p, k.offset_pc, gd,
-                                                  dom, make_op, group))
+        ranges = [int(np.abs(np.asarray(k.offset_pc, int)).max())
+                  for k in kins]
+        self.doms = _level_domains(gds, ranges, rank, size, dims,
+                                   min_planes)
+        self.kin = [DistributedFDOperator(k.coef_p, k.offset_pc, gd, dom,
+                                          make_op, group)
+                    for k, gd, dom in zip(kins, gds, self.doms)]
         d0, d1, d2 = self.doms
 
         def tr(obj, gi, go, di, do):
