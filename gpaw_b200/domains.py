@@ -16,6 +16,10 @@ are dropped), with the global grid's boundary conditions on axes 1 and 2.
 Restriction and interpolation gather the input planes each rank's output
 reaches (``gather_planes``), and the FD Poisson V-cycle runs on slabs down
 to the levels too thin to split, which every rank then holds whole.
+
+Axis 1 can be split too (``GridDomain``: boxes of a P0 x P1 process grid);
+the same gathers then run over boxes (``gather_box``), halo corners taking
+the phase of axis 0 and then that of axis 1.
 """
 from __future__ import annotations
 

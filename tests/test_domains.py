@@ -2,7 +2,8 @@
 (world sizes 2 and 3): the halo exchange, with the Bloch phase of axis 0
 across a periodic edge, and a stencil applied slab by slab equal to the
 same stencil on the whole grid; restriction, interpolation and FD Poisson
-V-cycles on slabs equal to the whole grid's.  The local operators here are
+V-cycles on slabs equal to the whole grid's; the same on boxes of a
+P0 x P1 process grid.  The local operators here are
 the oracle's CPU ones; on GPUs the slabs run the library's kernels and the exchange
 goes over NCCL (one GPU per process; not run here, where a call has one
 GPU)."""
@@ -597,3 +598,126 @@ def test_slab_weighted_vcycles_equal_whole_grid(pbc0):
         n, n_ref, d, scale = charged
         assert n == n_ref, rank
         assert d <= 1e-11 * scale, (rank, d)
+
+
+# --------------------------------------------------------------------------
+# boxes of a P0 x P1 process grid (axes 0 and 1 split)
+# --------------------------------------------------------------------------
+def _pencil_worker(rank, world, port, q, dims):
+    """Apply (complex with Bloch phases: the Laplacian and the Mehrstellen
+    stencil, whose edge taps read halo corners), restriction and
+    interpolation, and three V-cycles on the boxes of ``dims``."""
+    import traceback
+
+    import torch.distributed as dist
+
+    from gpaw_b200.domains import (DistributedFDOperator,
+                                   DistributedFDPoissonSolver,
+                                   DistributedPreconditioner,
+                                   DistributedTransformer, make_domain)
+    from oracle import gpaw_layer as L
+    os.environ['MASTER_ADDR'] = '127.0.0.1'
+    os.environ['MASTER_PORT'] = str(port)
+    dist.init_process_group('gloo', rank=rank, world_size=world)
+    try:
+        out = {}
+
+        def box(a, dom):
+            return torch.from_numpy(np.ascontiguousarray(
+                a[..., dom.beg:dom.end, dom.beg1:dom.end1, :]))
+
+        def cut(a, dom):
+            return a[..., dom.beg:dom.end, dom.beg1:dom.end1, :]
+        for pbc in ((1, 1, 0), (0, 0, 1), (1, 0, 1)):
+            gd = L.GridDescriptor((24, 20, 12), (4.8, 4.0, 2.4), pbc)
+            ph = gd.phase_factor_cd((0.3, -0.2, 0.1))
+            rng = np.random.default_rng(41)
+            a = rng.standard_normal((2,) + tuple(gd.n_c)) + \
+                1j * rng.standard_normal((2,) + tuple(gd.n_c))
+            dom = make_domain(gd.n_c, gd.pbc_c, rank, world, dims)
+            for name, op in (('lap', L.Laplace(gd, -0.5, 3, complex,
+                                               be='port')),
+                             ('mehr', L.LaplaceA(gd, 0.5, complex,
+                                                 be='port'))):
+                ref = np.zeros_like(a)
+                op.apply(a, ref, ph)
+                dop = DistributedFDOperator(op.coef_p, op.offset_pc, gd, dom,
+                                            _OracleLocal)
+                got = torch.zeros((2,) + dom.local_shape(),
+                                  dtype=torch.complex128)
+                dop.apply(box(a, dom), got, ph)
+                out[(pbc, name)] = bool(np.array_equal(got.numpy(),
+                                                       cut(ref, dom)))
+            gd2 = gd.coarsen()
+            for nn in (1, 3):
+                for interp in (False, True):
+                    gi, go = (gd2, gd) if interp else (gd, gd2)
+                    x = rng.standard_normal((2,) + tuple(gi.n_c)) + \
+                        1j * rng.standard_normal((2,) + tuple(gi.n_c))
+                    ref = np.zeros((2,) + tuple(go.n_c), complex)
+                    L.Transformer(gi, go, nn, complex, be='port') \
+                        .apply(x, ref, ph)
+                    di = make_domain(gi.n_c, gi.pbc_c, rank, world, dims)
+                    do = make_domain(go.n_c, go.pbc_c, rank, world, dims)
+                    t = DistributedTransformer(gi, go, nn, complex, di, do,
+                                               _OracleTransfer)
+                    got = torch.zeros((2,) + do.local_shape(),
+                                      dtype=torch.complex128)
+                    t.apply(box(x, di), got, ph)
+                    out[(pbc, nn, interp)] = bool(
+                        np.array_equal(got.numpy(), cut(ref, do)))
+        # V-cycles and the preconditioner
+        gd = L.GridDescriptor((24, 16, 16), (6.0, 4.0, 4.4), (0, 1, 0))
+        rng = np.random.default_rng(17)
+        rho = rng.standard_normal(tuple(gd.n_c))
+        phi = rng.standard_normal(tuple(gd.n_c)) * 0.1
+        ps = L.FDPoissonSolver(nn=3, relax='J', be='port')
+        ps.set_grid_descriptor(gd)
+        ps._init()
+        ps.phis[0] = phi.copy()
+        ps.rhos[0][:] = rho
+        ps.errors = []
+        [ps.iterate2(ps.step) for _ in range(3)]
+        dps = DistributedFDPoissonSolver(
+            ps, rank, world,
+            lambda c, o, n, p: _OracleLocal(c, o, n, p, float),
+            _OracleTransfer, dims=dims)
+        d0 = dps.doms[0]
+        phl = box(phi, d0).clone()
+        rhl = box(rho, d0)
+        [dps.iterate(phl, rhl) for _ in range(3)]
+        out['vcycle'] = bool(np.array_equal(phl.numpy(),
+                                            cut(ps.phis[0], d0)))
+        out['split_levels'] = dps.split_levels
+        gdp = L.GridDescriptor((24, 16, 12), (4.8, 3.2, 2.4), (1, 1, 1))
+        php = gdp.phase_factor_cd((0.25, -0.1, 0.2))
+        res = rng.standard_normal((2,) + tuple(gdp.n_c)) + \
+            1j * rng.standard_normal((2,) + tuple(gdp.n_c))
+        kin0 = L.Laplace(gdp, -0.5, 3, complex, be='port')
+        pre = L.Preconditioner(gdp, kin0, complex, block=2, be='port')
+        ref = pre(res, php).copy()
+        dp = DistributedPreconditioner(
+            pre, rank, world,
+            lambda c, o, n, p: _OracleLocal(c, o, n, p, complex),
+            _OracleTransfer, dims=dims)
+        got = dp(box(res, dp.doms[0]), php)
+        out['precond'] = bool(np.array_equal(got.numpy(),
+                                             cut(ref, dp.doms[0])))
+        q.put((rank, out))
+    except Exception:
+        q.put(('error', traceback.format_exc()))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize('dims', [(2, 2), (1, 3)])
+def test_pencils_equal_whole_grid(dims):
+    """Boxes of a 2 x 2 and a 1 x 3 process grid: complex apply with Bloch
+    phases (the Laplacian, and the Mehrstellen stencil whose edge taps
+    read the halo corners, phased along axis 0 then axis 1), restriction
+    and interpolation (nn = 1 and 3), three V-cycles and the
+    preconditioner all give every rank exactly the whole grid's points."""
+    for rank, out in _run_ranks(dims[0] * dims[1], _pencil_worker, (dims,)):
+        bad = [k for k, v in out.items() if v is False]
+        assert not bad, (rank, bad)
+        assert out['split_levels'] >= 1
