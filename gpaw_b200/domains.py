@@ -298,7 +298,10 @@ def gather_box(a, needs, boxes, rank, n01, periodic01, phase_cd=None,
     of axis c upwards times phase_cd[c][0] per crossing, downwards times
     phase_cd[c][1], axis 0 before axis 1, as the reference's halo fill
     multiplies them (c/bc.cpp:146-258).  The messages are one batch of
-    point-to-point sends and receives, ordered alike on both sides."""
+    point-to-point sends and receives, ordered alike on both sides.  Over
+    NCCL, run one collective on the group (a barrier) before the first
+    gather, so that every rank has set up its communicator when the first
+    batch starts."""
     import torch
     import torch.distributed as dist
     (lo0, hi0), (lo1, hi1) = needs[rank]

@@ -721,3 +721,49 @@ def test_pencils_equal_whole_grid(dims):
         bad = [k for k, v in out.items() if v is False]
         assert not bad, (rank, bad)
         assert out['split_levels'] >= 1
+
+
+def test_box_pieces_cover_each_point_once():
+    """For random process grids, grid sizes, boundary flags and needed
+    boxes (reaching past either edge, wider than the grid): the pieces
+    cover every point of the need that lies inside the grid or across a
+    periodic edge exactly once, from a rank whose box holds it (the
+    receiver itself when it does), with the right number of edge
+    crossings; points past a zero boundary are left out."""
+    from gpaw_b200.domains import GridDomain, box_pieces
+    rng = np.random.default_rng(5)
+    for _ in range(300):
+        P0, P1 = int(rng.integers(1, 4)), int(rng.integers(1, 4))
+        n0, n1 = int(rng.integers(1, 9)), int(rng.integers(1, 9))
+        per = (bool(rng.integers(2)), bool(rng.integers(2)))
+        dom = GridDomain((n0, n1, 3), per, 0, (P0, P1),
+                         bool(rng.integers(4) == 0))
+        recv = int(rng.integers(P0 * P1))
+        need = []
+        for n in (n0, n1):
+            lo = int(rng.integers(-2 * n - 2, n + 1))
+            need.append((lo, lo + int(rng.integers(0, 3 * n + 3))))
+        hits = {}
+        for owner, src, dst, ln, k in box_pieces(need, (n0, n1), per,
+                                                 dom.boxes, recv):
+            (ob0, oe0), (ob1, oe1) = dom.boxes[owner]
+            assert 0 <= src[0] and src[0] + ln[0] <= oe0 - ob0
+            assert 0 <= src[1] and src[1] + ln[1] <= oe1 - ob1
+            for i in range(ln[0]):
+                for j in range(ln[1]):
+                    g = (need[0][0] + dst[0] + i, need[1][0] + dst[1] + j)
+                    assert g not in hits
+                    hits[g] = (owner, ob0 + src[0] + i, ob1 + src[1] + j, k)
+        for g0 in range(*need[0]):
+            for g1 in range(*need[1]):
+                k0, p0 = divmod(g0, n0)
+                k1, p1 = divmod(g1, n1)
+                inside = (per[0] or k0 == 0) and (per[1] or k1 == 0)
+                assert (g0, g1) in hits if inside else (g0, g1) not in hits
+                if not inside:
+                    continue
+                owner, q0, q1, k = hits[(g0, g1)]
+                assert (q0, q1, k) == (p0, p1, (k0, k1))
+                (b0, e0), (b1, e1) = dom.boxes[recv]
+                if b0 <= p0 < e0 and b1 <= p1 < e1:
+                    assert owner == recv
