@@ -617,7 +617,7 @@ class DistributedFDPoissonSolver:
         non-periodic cell through a Gaussian carrying the charge, solved
         neutral, its potential added back.  ``gauss``: the whole grid's
         (rho_gauss, phi_gauss), by default gauss.monopole_gaussian of the
-        grid (each rank keeps its slab)."""
+        grid (each rank keeps its own box of them)."""
         actual_charge = self._sum(rho) * float(self.gd.dv)
         background = actual_charge / float(self.gd.dv) / \
             float(np.prod(self.gd.n_c))
@@ -639,7 +639,8 @@ class DistributedFDPoissonSolver:
         import torch
         dom = self.doms[0]
         rg, pg = [torch.as_tensor(np.ascontiguousarray(
-            np.asarray(g)[dom.beg:dom.end])).to(phi.device) for g in gauss]
+            np.asarray(g)[dom.beg:dom.end, dom.beg1:dom.end1])).to(
+                phi.device) for g in gauss]
         q = actual_charge / np.sqrt(4 * np.pi)
         rho_neutral = rho - q * rg
         if zero_initial_phi:
@@ -679,28 +680,47 @@ class DistributedWeightedOperator(DistributedFDOperator):
     weights' halo planes are exchanged once, here; apply and the Jacobi
     sweeps exchange the operand's halos as DistributedFDOperator does.
     The stencils' flattened offsets depend only on the padded extents of
-    axes 1 and 2, which the slab shares with the whole grid, so they are
-    used unchanged.  ``make_local(nweights, weights, coef_ps, offset_ps,
+    axes 1 and 2, which a slab shares with the whole grid, so they are
+    used unchanged; on boxes with a split axis 1 they are re-flattened for
+    the box's extent.  ``make_local(nweights, weights, coef_ps, offset_ps,
     n_c, r, neighbors, real, cfd)`` builds the WOperator of one slab plus
     halos (on a GPU: gpu_local_woperator)."""
 
     def __init__(self, wop, weights, dom, make_local, group=None):
-        if dom.split1:
-            # a split axis 1 changes the padded extent the flattened
-            # offsets were built for
-            raise NotImplementedError('weighted operators split axis 0 '
-                                      'only')
         self.R = R = int(wop.mp)
-        self.R1 = 0
+        self.R1 = R if dom.split1 else 0
         self.dom, self.group = dom, group
-        n_ext = (dom.m0 + 2 * R,) + tuple(int(x) for x in wop.gd.n_c[1:])
+        n_c = [int(x) for x in wop.gd.n_c]
+        n_ext = [dom.m0 + 2 * R, n_c[1], n_c[2]]
         nb = np.array(wop.gd.neighbor_cd, np.int64).reshape(3, 2).copy()
         nb[0] = -1
-        self.weights_ext = [exchange_halos(w, R, dom, None, group)
+        offset_ps = wop.offset_ps
+        if dom.split1:
+            n_ext[1] = dom.m1 + 2 * R
+            nb[1] = -1
+            offset_ps = [_reflatten(o, n_c[1] + 2 * R, n_ext[1] + 2 * R,
+                                    n_c[2] + 2 * R) for o in offset_ps]
+        self.weights_ext = [exchange_halos(w, (R, R), dom, None, group)
                             for w in weights]
         self.local = make_local(wop.nweights, self.weights_ext, wop.coef_ps,
-                                wop.offset_ps, np.array(n_ext, np.int64), R,
+                                offset_ps, np.array(n_ext, np.int64), R,
                                 nb, wop.dtype == float, wop.cfd)
+
+
+def _reflatten(offsets, M1, M1_new, M2):
+    """Flattened stencil offsets (o0 M1 + o1) M2 + o2 of a grid padded to
+    M1 x M2 points on axes 1 and 2, re-flattened for an axis-1 extent of
+    M1_new (every |o1|, |o2| is at most the padding, below half of M1 and
+    M2, so the split is unique)."""
+    out = []
+    for o in np.asarray(offsets, np.int64):
+        o = int(o)
+        o2 = (o + M2 // 2) % M2 - M2 // 2
+        rest = (o - o2) // M2
+        o1 = (rest + M1 // 2) % M1 - M1 // 2
+        o0 = (rest - o1) // M1
+        out.append((o0 * M1_new + o1) * M2 + o2)
+    return np.array(out, np.int64)
 
 
 def gpu_local_woperator():
@@ -724,10 +744,10 @@ class DistributedWeightedFDPoissonSolver(DistributedFDPoissonSolver):
     set_grid_descriptor; ``make_op`` builds weighted slab operators."""
 
     def __init__(self, ps, eps_gradeps, rank, size, make_op, make_tr,
-                 group=None, min_planes=2):
+                 group=None, min_planes=2, dims=None):
         self._eps_gradeps = list(eps_gradeps)
         super().__init__(ps, rank, size, make_op, make_tr, group,
-                         min_planes, None)
+                         min_planes, dims)
 
     @staticmethod
     def _op_range(op):

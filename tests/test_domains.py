@@ -524,7 +524,7 @@ def _grad_stencils(gd, scale, n):
     return out
 
 
-def _weighted_worker(rank, world, port, q, pbc0):
+def _weighted_worker(rank, world, port, q, pbc0, dims=None):
     import traceback
 
     import torch.distributed as dist
@@ -553,15 +553,20 @@ def _weighted_worker(rank, world, port, q, pbc0):
         wps.rhos[0][:] = rho
         wps.errors = []
         ref_err = [wps.iterate2(wps.step) for _ in range(3)]
-        from gpaw_b200.domains import slab_bounds
-        b, e = slab_bounds(gd.n_c[0], world)[rank]
+        from gpaw_b200.domains import make_domain
+        d = make_domain(gd.n_c, gd.pbc_c, rank, world, dims)
+        b, e = d.beg, d.end
+        b1, e1 = d.beg1, d.end1
+
+        def cut(a):
+            return torch.from_numpy(np.ascontiguousarray(a[b:e, b1:e1]))
         dps = DistributedWeightedFDPoissonSolver(
-            wps, [torch.from_numpy(a[b:e].copy()) for a in arrays], rank,
-            world, _OracleWeighted, _OracleTransfer)
-        phl = torch.from_numpy(phi[b:e].copy())
-        rhl = torch.from_numpy(rho[b:e].copy())
+            wps, [cut(a) for a in arrays], rank, world, _OracleWeighted,
+            _OracleTransfer, dims=dims)
+        phl = cut(phi)
+        rhl = cut(rho)
         err = [dps.iterate(phl, rhl) for _ in range(3)]
-        same = bool(np.array_equal(phl.numpy(), wps.phis[0][b:e]))
+        same = bool(np.array_equal(phl.numpy(), wps.phis[0][b:e, b1:e1]))
         # a charged system: the dielectric's compensation charge
         rho_c = rho + 0.5 * np.exp(-(x**2).sum(0)) if not pbc0 else \
             rho - rho.mean()
@@ -569,9 +574,9 @@ def _weighted_worker(rank, world, port, q, pbc0):
         ref_phi = np.zeros(tuple(gd.n_c))
         n_ref = wps.solve(ref_phi, rho_c)
         phc = torch.zeros(phl.shape, dtype=torch.float64)
-        n = dps.solve(phc, torch.from_numpy(rho_c[b:e].copy()),
-                      gauss=(wps.rho_gauss, wps.phi_gauss))
-        charged = (n, n_ref, float(np.abs(phc.numpy() - ref_phi[b:e]).max()),
+        n = dps.solve(phc, cut(rho_c), gauss=(wps.rho_gauss, wps.phi_gauss))
+        charged = (n, n_ref,
+                   float(np.abs(phc.numpy() - ref_phi[b:e, b1:e1]).max()),
                    float(np.abs(ref_phi).max()))
         q.put((rank, same, err, ref_err, dps.split_levels, dps.levels,
                charged))
@@ -581,16 +586,20 @@ def _weighted_worker(rank, world, port, q, pbc0):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize('pbc0', [1, 0])
-def test_slab_weighted_vcycles_equal_whole_grid(pbc0):
-    """The dielectric Poisson solver's V-cycles on three slabs (weights
-    and their halos on slabs, coarse weights restricted on slabs) leave
+@pytest.mark.parametrize('pbc0,dims', [(1, None), (0, None), (1, (2, 2)),
+                                       (0, (1, 3))])
+def test_slab_weighted_vcycles_equal_whole_grid(pbc0, dims):
+    """The dielectric Poisson solver's V-cycles on three slabs, or on the
+    boxes of a 2 x 2 or 1 x 3 process grid (weights and their halos
+    split, coarse weights restricted on the split grid, the flattened
+    stencil offsets re-flattened for a split axis 1) leave
     phi bit-identical to the whole grid's; the level-0 error matches to
     rounding.  A charged system (the dielectric's compensation charge in a
     zero-boundary cell; the neutral part of it on a periodic axis 0) takes
     as many V-cycles as the whole-grid solve, phi to 1e-11."""
+    world = 3 if dims is None else dims[0] * dims[1]
     for rank, same, err, ref_err, split, levels, charged in _run_ranks(
-            3, _weighted_worker, (pbc0,)):
+            world, _weighted_worker, (pbc0, dims)):
         assert same, rank
         assert split <= levels
         for e, r in zip(err, ref_err):
