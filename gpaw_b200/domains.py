@@ -17,9 +17,10 @@ Restriction and interpolation gather the input planes each rank's output
 reaches (``gather_planes``), and the FD Poisson V-cycle runs on slabs down
 to the levels too thin to split, which every rank then holds whole.
 
-Axis 1 can be split too (``GridDomain``: boxes of a P0 x P1 process grid);
-the same gathers then run over boxes (``gather_box``), halo corners taking
-the phase of axis 0 and then that of axis 1.
+Axes 1 and 2 can be split too (``GridDomain``: boxes of a P0 x P1 x P2
+process grid); the same gathers then run over boxes (``gather_box``),
+points past several periodic edges taking the phases axis by axis in
+order.
 """
 from __future__ import annotations
 
@@ -35,53 +36,66 @@ def slab_bounds(n0, size):
 
 
 class GridDomain:
-    """Rank ``rank`` of a P0 x P1 process grid (rank = r0 P1 + r1) owning
-    the box [beg, end) x [beg1, end1) of axes 0 and 1 (axis 2 whole).
-    ``replicated``: every rank holds the whole grid (the coarse levels of a
-    split V-cycle); halos then come from the rank's own planes and nothing
-    is sent.  Axis 1 counts as split when P1 > 1."""
+    """Rank ``rank`` of a P0 x P1 x P2 process grid (rank = (r0 P1 + r1) P2
+    + r2; ``dims`` of two entries means P2 = 1) owning the box [beg, end)
+    x [beg1, end1) x [beg2, end2).  ``replicated``: every rank holds the
+    whole grid (the coarse levels of a split V-cycle); halos then come
+    from the rank's own points and nothing is sent.  Axis 0 is always
+    treated as split; axis 2 when P2 > 1, axis 1 when P1 > 1 or P2 > 1."""
 
-    def __init__(self, n_c, pbc01, rank, dims, replicated=False):
+    def __init__(self, n_c, pbc_c, rank, dims, replicated=False):
         self.n_c = tuple(int(x) for x in n_c)
-        self.periodic = (bool(pbc01[0]), bool(pbc01[1]))
+        pbc = [bool(p) for p in pbc_c] + [False] * (3 - len(pbc_c))
+        self.periodic = tuple(pbc)
         self.periodic0 = self.periodic[0]
-        self.dims = (int(dims[0]), int(dims[1]))
+        d = [int(x) for x in dims] + [1] * (3 - len(dims))
+        self.dims = tuple(d)
         self.rank = int(rank)
-        self.size = self.dims[0] * self.dims[1]
+        self.size = d[0] * d[1] * d[2]
         self.replicated = bool(replicated)
-        n0, n1 = self.n_c[:2]
         if self.replicated:
-            self.boxes = [((0, n0), (0, n1))] * self.size
+            self.boxes = [tuple((0, n) for n in self.n_c)] * self.size
         else:
-            b0 = slab_bounds(n0, self.dims[0])
-            b1 = slab_bounds(n1, self.dims[1])
-            self.boxes = [(b0[r // self.dims[1]], b1[r % self.dims[1]])
+            b = [slab_bounds(n, p) for n, p in zip(self.n_c, d)]
+            self.boxes = [(b[0][r // (d[1] * d[2])],
+                           b[1][(r // d[2]) % d[1]], b[2][r % d[2]])
                           for r in range(self.size)]
-        self.bounds = [b[0] for b in self.boxes]
-        (self.beg, self.end), (self.beg1, self.end1) = self.boxes[self.rank]
+        self.bounds = [bx[0] for bx in self.boxes]
+        ((self.beg, self.end), (self.beg1, self.end1),
+         (self.beg2, self.end2)) = self.boxes[self.rank]
         self.m0 = self.end - self.beg
         self.m1 = self.end1 - self.beg1
-        self.split1 = self.dims[1] > 1
+        self.m2 = self.end2 - self.beg2
+        # axes whose halos the gathers fill: axis 0, and every axis up to
+        # the last split one -- an unsplit axis 1 before a split axis 2 is
+        # gathered too, so that points past several periodic edges take
+        # their phases axis by axis in order, as the whole grid's fill
+        # multiplies them
+        self.split = (True, d[1] > 1 or d[2] > 1, d[2] > 1)
+        self.split1 = self.split[1]
 
     def local_shape(self):
-        return (self.m0, self.m1, self.n_c[2])
+        return (self.m0, self.m1, self.m2)
+
+    def inner(self, a):
+        """This rank's box of a whole-grid array (leading axes kept)."""
+        return a[..., self.beg:self.end, self.beg1:self.end1,
+                 self.beg2:self.end2]
 
     def thinnest(self):
-        """Fewest points of a rank's box along each split axis (axis 0, and
-        axis 1 when split), as a box of an unreplicated split would have."""
-        t = [min(e - b for b, e in slab_bounds(self.n_c[0], self.dims[0]))]
-        if self.split1:
-            t.append(min(e - b for b, e in
-                         slab_bounds(self.n_c[1], self.dims[1])))
-        return tuple(t)
+        """Fewest points of a rank's box along each split axis, as a box of
+        an unreplicated split would have."""
+        return tuple(min(e - b for b, e in slab_bounds(n, p))
+                     for n, p, sp in zip(self.n_c, self.dims, self.split)
+                     if sp)
 
 
 class SlabDomain(GridDomain):
     """Rank ``rank`` of ``size`` owning planes [beg, end) of axis 0: the
-    P0 x 1 grid, with the neighbouring ranks along axis 0."""
+    P0 x 1 x 1 grid, with the neighbouring ranks along axis 0."""
 
     def __init__(self, n_c, periodic0, rank, size, replicated=False):
-        super().__init__(n_c, (periodic0, False), rank, (size, 1),
+        super().__init__(n_c, (periodic0, False, False), rank, (size, 1, 1),
                          replicated)
         if self.replicated:
             # the rank's own planes across a periodic edge
@@ -94,41 +108,42 @@ class SlabDomain(GridDomain):
 
 
 def make_domain(n_c, pbc_c, rank, size, dims=None, replicated=False):
-    """A SlabDomain of ``size`` ranks, or the GridDomain of the P0 x P1
-    grid ``dims``."""
-    if dims is None or int(dims[1]) == 1:
+    """A SlabDomain of ``size`` ranks, or the GridDomain of the process
+    grid ``dims`` (P0, P1) or (P0, P1, P2)."""
+    if dims is None or int(np.prod([int(x) for x in dims[1:]])) == 1:
         return SlabDomain(n_c, bool(pbc_c[0]), rank, size, replicated)
-    if int(dims[0]) * int(dims[1]) != int(size):
+    if int(np.prod([int(x) for x in dims])) != int(size):
         raise ValueError('dims %s do not make %d ranks' % (dims, size))
-    return GridDomain(n_c, (bool(pbc_c[0]), bool(pbc_c[1])), rank, dims,
+    return GridDomain(n_c, tuple(bool(p) for p in pbc_c), rank, dims,
                       replicated)
 
 
 def exchange_halos(a, R, dom, phase_cd=None, group=None):
-    """Collective: local box a (..., m0, m1, n2) -> (..., m0 + 2 R0,
-    m1 + 2 R1, n2) with the R0 planes on either side along axis 0 (and R1
-    along a split axis 1; ``R`` is R0 or (R0, R1)) from the ranks that hold
-    them: zeros past a zero boundary; points that crossed a periodic edge
-    times the Bloch phase when ``phase_cd`` is given (phase_cd[c][1] per
-    crossing of the low edge of axis c, [c][0] of the high edge; axis 0
-    first, then axis 1, as the reference's halo fill of edges and corners
-    multiplies them).  One gather_box: the sends and receives go as one
-    batch, ordered alike on both sides, so two ranks that are each other's
-    upper and lower neighbour cannot wait on each other; boxes thinner than
-    the halo take points from ranks further away.  Works on torch tensors
-    on any device the process group can send from."""
-    R0, R1 = (R, R) if np.isscalar(R) else (int(R[0]), int(R[1]))
-    if not dom.split1:
-        R1 = 0
-    needs = [((b0 - R0, e0 + R0), (b1 - R1, e1 + R1))
-             for (b0, e0), (b1, e1) in dom.boxes]
-    return gather_box(a, needs, dom.boxes, dom.rank, dom.n_c[:2],
+    """Collective: local box a (..., m0, m1, m2) -> the box grown by R_c
+    points on either side along every split axis c (``R`` is one number
+    for all, or one per axis; unsplit axes grow by nothing), the points
+    coming from the ranks that hold them: zeros past a zero boundary;
+    points that crossed a periodic edge times the Bloch phase when
+    ``phase_cd`` is given (phase_cd[c][1] per crossing of the low edge of
+    axis c, [c][0] of the high edge; axis 0 first, then 1, then 2, as the
+    reference's halo fill of edges and corners multiplies them).  One
+    gather_box: the sends and receives go as one batch, ordered alike on
+    both sides, so two ranks that are each other's upper and lower
+    neighbour cannot wait on each other; boxes thinner than the halo take
+    points from ranks further away.  Works on torch tensors on any device
+    the process group can send from."""
+    Rc = [int(R)] * 3 if np.isscalar(R) else \
+        [int(x) for x in R] + [0] * (3 - len(R))
+    Rc = [r if sp else 0 for r, sp in zip(Rc, dom.split)]
+    needs = [tuple((b - r, e + r) for (b, e), r in zip(box, Rc))
+             for box in dom.boxes]
+    return gather_box(a, needs, dom.boxes, dom.rank, dom.n_c,
                       dom.periodic, phase_cd, group)
 
 
 class DistributedFDOperator:
     """A stencil (coef_p, offset_pc) applied to a grid split in slabs (or
-    boxes of a P0 x P1 grid).  ``make_local(coef_p, offset_pc, n_c,
+    boxes of a process grid).  ``make_local(coef_p, offset_pc, n_c,
     pbc_c)`` builds the operator of one box plus halos (``n_c`` points,
     zero boundary along the split axes): on a GPU an FDOperator of
     gpaw_b200; any object with ``apply(in, out, phase_cd)``."""
@@ -136,22 +151,23 @@ class DistributedFDOperator:
     def __init__(self, coef_p, offset_pc, gd, dom, make_local, group=None):
         offset_pc = np.asarray(offset_pc, int)
         reach = np.abs(offset_pc).max(0) if len(offset_pc) else (0, 0, 0)
-        self.R = int(reach[0])
-        self.R1 = int(reach[1]) if dom.split1 else 0
+        self.Rc = tuple(int(r) if sp else 0
+                        for r, sp in zip(reach, dom.split))
+        self.R, self.R1 = self.Rc[0], self.Rc[1]
         self.dom, self.group = dom, group
-        n1 = dom.m1 + 2 * self.R1 if dom.split1 else int(gd.n_c[1])
-        n_ext = (dom.m0 + 2 * self.R, n1, int(gd.n_c[2]))
-        pbc = (False, False if dom.split1 else bool(gd.pbc_c[1]),
-               bool(gd.pbc_c[2]))
+        n_ext = tuple(m + 2 * r if sp else int(n) for m, r, sp, n in
+                      zip(dom.local_shape(), self.Rc, dom.split, gd.n_c))
+        pbc = tuple(False if sp else bool(p)
+                    for sp, p in zip(dom.split, gd.pbc_c))
         self.local = make_local(coef_p, offset_pc, n_ext, pbc)
 
     def _halos(self, a, phase_cd=None):
-        return exchange_halos(a, (self.R, self.R1), self.dom, phase_cd,
-                              self.group)
+        return exchange_halos(a, self.Rc, self.dom, phase_cd, self.group)
 
     def _inner(self, ext):
-        R, R1, dom = self.R, self.R1, self.dom
-        return ext[..., R:R + dom.m0, R1:R1 + dom.m1, :]
+        sl = tuple(slice(r, r + m)
+                   for r, m in zip(self.Rc, self.dom.local_shape()))
+        return ext[(Ellipsis,) + sl]
 
     def apply(self, a, out, phase_cd=None):
         ext = self._halos(a, phase_cd)
@@ -159,9 +175,9 @@ class DistributedFDOperator:
         ph = None
         if phase_cd is not None:
             ph = np.array(phase_cd, complex)
-            ph[0] = 1.0              # split axes' phases travelled with
-            if self.dom.split1:      # the halos
-                ph[1] = 1.0
+            for c, sp in enumerate(self.dom.split):
+                if sp:               # split axes' phases travelled with
+                    ph[c] = 1.0      # the halos
         self.local.apply(ext, tmp, ph)
         out[...] = self._inner(tmp)
 
@@ -173,9 +189,8 @@ class DistributedFDOperator:
         if relax_method != 2:
             raise NotImplementedError('only weighted Jacobi (2) runs on '
                                       'slabs')
-        s_ext = s.new_zeros(s.shape[:-3] + (
-            self.dom.m0 + 2 * self.R, self.dom.m1 + 2 * self.R1,
-            s.shape[-1]))
+        s_ext = s.new_zeros(s.shape[:-3] + tuple(
+            m + 2 * r for m, r in zip(self.dom.local_shape(), self.Rc)))
         self._inner(s_ext)[...] = s
         for _ in range(n):
             ext = self._halos(f)
@@ -244,34 +259,38 @@ def _segments(lo, hi, n, periodic, cuts):
     return segs
 
 
-def _owner(p0, p1, boxes, recv):
-    """The rank that sends point (p0, p1) of axes 0 and 1 to rank ``recv``:
-    recv itself when it holds it (replicated levels), else the first rank
-    whose box does."""
+def _owner(point, boxes, recv):
+    """The rank that sends ``point`` (one index per gathered axis) to rank
+    ``recv``: recv itself when it holds it (replicated levels), else the
+    first rank whose box does."""
     for r in [recv] + list(range(len(boxes))):
-        (b0, e0), (b1, e1) = boxes[r]
-        if b0 <= p0 < e0 and b1 <= p1 < e1:
+        if all(b <= p < e for p, (b, e) in zip(point, boxes[r])):
             return r
-    raise ValueError('point (%d, %d) is held by no rank' % (p0, p1))
+    raise ValueError('point %s is held by no rank' % (point,))
 
 
-def box_pieces(need, n01, periodic01, boxes, recv):
-    """The box ``need`` = ((lo0, hi0), (lo1, hi1)) of axes 0 and 1 as
-    pieces (owner, (src0, src1), (dst0, dst1), (len0, len1), (k0, k1)):
+def box_pieces(need, n_c, periodic_c, boxes, recv):
+    """The box ``need`` = ((lo0, hi0), (lo1, hi1), ...) of the gathered
+    axes as pieces (owner, src, dst, lengths, wraps), one entry per axis:
     points src.. of the owner's box go to dst.. of the receiver's buffer,
-    having crossed the periodic edges k0 and k1 times.  Every rank computes
+    having crossed the periodic edges wraps times.  Every rank computes
     every receiver's list the same way, so senders and receivers agree on
     the pieces and their order."""
-    cuts = [sorted({x for b in boxes for x in b[c]}) for c in (0, 1)]
-    segs = [_segments(need[c][0], need[c][1], n01[c], periodic01[c],
-                      cuts[c]) for c in (0, 1)]
+    import itertools
+    na = len(need)
+    cuts = [sorted({x for b in boxes for x in b[c]}) for c in range(na)]
+    segs = [_segments(need[c][0], need[c][1], n_c[c], periodic_c[c],
+                      cuts[c]) for c in range(na)]
     pieces = []
-    for d0, p0, l0, k0 in segs[0]:
-        for d1, p1, l1, k1 in segs[1]:
-            owner = _owner(p0, p1, boxes, recv)
-            (ob0, _), (ob1, _) = boxes[owner]
-            pieces.append((owner, (p0 - ob0, p1 - ob1), (d0, d1), (l0, l1),
-                           (k0, k1)))
+    for combo in itertools.product(*segs):
+        point = tuple(sg[1] for sg in combo)
+        owner = _owner(point, boxes, recv)
+        pieces.append((owner,
+                       tuple(sg[1] - boxes[owner][c][0]
+                             for c, sg in enumerate(combo)),
+                       tuple(sg[0] for sg in combo),
+                       tuple(sg[2] for sg in combo),
+                       tuple(sg[3] for sg in combo)))
     return pieces
 
 
@@ -287,33 +306,32 @@ def _phase_mul(t, ph):
     r[..., 1] = d * a + c * b
 
 
-def gather_box(a, needs, boxes, rank, n01, periodic01, phase_cd=None,
+def gather_box(a, needs, boxes, rank, n_c, periodic_c, phase_cd=None,
                group=None):
     """Collective: every rank gets the points ``needs[rank]`` = ((lo0,
-    hi0), (lo1, hi1)) of axes 0 and 1 (axis 2 whole) of a grid of n01
-    points on those axes from whichever ranks hold them (``boxes[r]``: the
-    box rank r holds in ``a``).  Returns
-    (..., hi0 - lo0, hi1 - lo1, n2): zeros past a zero boundary; for
-    complex data with ``phase_cd``, points that crossed the periodic edge
-    of axis c upwards times phase_cd[c][0] per crossing, downwards times
-    phase_cd[c][1], axis 0 before axis 1, as the reference's halo fill
-    multiplies them (c/bc.cpp:146-258).  The messages are one batch of
-    point-to-point sends and receives, ordered alike on both sides.  Over
-    NCCL, run one collective on the group (a barrier) before the first
-    gather, so that every rank has set up its communicator when the first
-    batch starts."""
+    hi0), (lo1, hi1), (lo2, hi2)) of a grid of ``n_c`` points from
+    whichever ranks hold them (``boxes[r]``: the box rank r holds in
+    ``a``).  Returns (..., hi0 - lo0, hi1 - lo1, hi2 - lo2): zeros past a
+    zero boundary; for complex data with ``phase_cd``, points that crossed
+    the periodic edge of axis c upwards times phase_cd[c][0] per crossing,
+    downwards times phase_cd[c][1], axis 0 first, then 1, then 2, as the
+    reference's halo fill multiplies them (c/bc.cpp:146-258).  The
+    messages are one batch of point-to-point sends and receives, ordered
+    alike on both sides.  Over NCCL, run one collective on the group (a
+    barrier) before the first gather, so that every rank has set up its
+    communicator when the first batch starts."""
     import torch
     import torch.distributed as dist
-    (lo0, hi0), (lo1, hi1) = needs[rank]
-    out = a.new_zeros(a.shape[:-3] + (hi0 - lo0, hi1 - lo1, a.shape[-1]))
+    out = a.new_zeros(a.shape[:-3] +
+                      tuple(hi - lo for lo, hi in needs[rank]))
     ops, recvd = [], []
     for r, need in enumerate(needs):
         for idx, (owner, src, dst, ln, k) in enumerate(
-                box_pieces(need, n01, periodic01, boxes, r)):
-            sl = (Ellipsis, slice(src[0], src[0] + ln[0]),
-                  slice(src[1], src[1] + ln[1]), slice(None))
-            dl = (Ellipsis, slice(dst[0], dst[0] + ln[0]),
-                  slice(dst[1], dst[1] + ln[1]), slice(None))
+                box_pieces(need, n_c, periodic_c, boxes, r)):
+            sl = (Ellipsis,) + tuple(slice(x, x + m)
+                                     for x, m in zip(src, ln))
+            dl = (Ellipsis,) + tuple(slice(x, x + m)
+                                     for x, m in zip(dst, ln))
             if r == rank and owner == rank:
                 out[dl] = a[sl]
                 recvd.append((dl, k, None))
@@ -335,7 +353,7 @@ def gather_box(a, needs, boxes, rank, n01, periodic01, phase_cd=None,
             view.copy_(buf)
         if ph is None or not a.is_complex():
             continue
-        for c in (0, 1):
+        for c in range(3):
             if k[c]:
                 f = ph[c][0] if k[c] > 0 else ph[c][1]
                 for _ in range(abs(k[c])):
@@ -348,17 +366,18 @@ def gather_planes(a, needs, n0, periodic0, bounds, rank, phase_cd=None,
     """Collective: gather_box along axis 0 alone -- every rank gets the
     global planes [lo, hi) that ``needs[rank]`` names from the ranks whose
     planes ``bounds`` lists."""
-    n1 = a.shape[-2]
-    return gather_box(a, [(tuple(nd), (0, n1)) for nd in needs],
-                      [(tuple(b), (0, n1)) for b in bounds], rank,
-                      (n0, n1), (periodic0, False), phase_cd, group)
+    n1, n2 = a.shape[-2:]
+    return gather_box(a, [(tuple(nd), (0, n1), (0, n2)) for nd in needs],
+                      [(tuple(b), (0, n1), (0, n2)) for b in bounds], rank,
+                      (n0, n1, n2), (periodic0, False, False), phase_cd,
+                      group)
 
 
 def gather_full(a, dom, group=None):
     """Collective: the whole of a split grid on every rank."""
-    n0, n1 = dom.n_c[:2]
-    return gather_box(a, [((0, n0), (0, n1))] * dom.size, dom.boxes,
-                      dom.rank, dom.n_c[:2], dom.periodic, None, group)
+    return gather_box(a, [tuple((0, n) for n in dom.n_c)] * dom.size,
+                      dom.boxes, dom.rank, dom.n_c, dom.periodic, None,
+                      group)
 
 
 # --------------------------------------------------------------------------
@@ -389,20 +408,19 @@ class DistributedTransformer:
         self.dom_in, self.dom_out, self.group = dom_in, dom_out, group
         self.K = K = 2 * int(nn)
         self.dtype = dtype
-        axes = (0, 1) if dom_out.split1 else (0,)
+        axes = tuple(c for c in range(3) if dom_out.split[c])
         self.axes = axes
         self.needs, self.keep = [], []
         mine = None
         for r in range(dom_out.size):
-            geo = [self._axis(dom_out.boxes[r][c], int(gdin.beg_c[c]),
-                              int(gdout.beg_c[c]), K) for c in axes]
-            if any(g is None for g in geo):
-                self.needs.append(((0, 0), (0, 0)))
+            geo = {c: self._axis(dom_out.boxes[r][c], int(gdin.beg_c[c]),
+                                 int(gdout.beg_c[c]), K) for c in axes}
+            if any(g is None for g in geo.values()):
+                self.needs.append(((0, 0),) * 3)
                 self.keep.append(None)
                 continue
-            full1 = (0, int(gdin.n_c[1]))
-            self.needs.append((geo[0][:2], geo[1][:2] if dom_out.split1
-                               else full1))
+            self.needs.append(tuple(geo[c][:2] if c in geo else
+                                    (0, int(gdin.n_c[c])) for c in range(3)))
             self.keep.append(tuple(e - b for b, e in dom_out.boxes[r]))
             if r == dom_out.rank:
                 mine = geo
@@ -414,7 +432,7 @@ class DistributedTransformer:
             nb = np.array(gdin.neighbor_cd, np.int64).reshape(3, 2).copy()
             size_in = [int(x) for x in gdin.n_c]
             size_out = [int(x) for x in gdout.n_c]
-            for c, (lo, hi, mcalc, s0) in zip(axes, mine):
+            for c, (lo, hi, mcalc, s0) in mine.items():
                 pads[c] = npads[c] = 0
                 skips[c] = (s0, 0)
                 nb[c] = -1
@@ -454,17 +472,17 @@ class DistributedTransformer:
         """Collective: ``a`` holds this rank's input box, ``out`` gets its
         output box."""
         di = self.dom_in
-        ext = gather_box(a, self.needs, di.boxes, di.rank, di.n_c[:2],
+        ext = gather_box(a, self.needs, di.boxes, di.rank, di.n_c,
                          di.periodic, phases, self.group)
         if self.local is None:
             return out
-        m0, m1 = self.keep[self.dom_out.rank]
-        if tuple(self.size_out[:2]) == (m0, m1):
+        m = self.keep[self.dom_out.rank]
+        if tuple(self.size_out) == m:
             self.local.apply(ext, out, phases)
         else:
             tmp = out.new_zeros(out.shape[:-3] + self.size_out)
             self.local.apply(ext, tmp, phases)
-            out[...] = tmp[..., :m0, :m1, :]
+            out[...] = tmp[..., :m[0], :m[1], :m[2]]
         return out
 
 
@@ -639,8 +657,7 @@ class DistributedFDPoissonSolver:
         import torch
         dom = self.doms[0]
         rg, pg = [torch.as_tensor(np.ascontiguousarray(
-            np.asarray(g)[dom.beg:dom.end, dom.beg1:dom.end1])).to(
-                phi.device) for g in gauss]
+            dom.inner(np.asarray(g)))).to(phi.device) for g in gauss]
         q = actual_charge / np.sqrt(4 * np.pi)
         rho_neutral = rho - q * rg
         if zero_initial_phi:
@@ -681,36 +698,39 @@ class DistributedWeightedOperator(DistributedFDOperator):
     sweeps exchange the operand's halos as DistributedFDOperator does.
     The stencils' flattened offsets depend only on the padded extents of
     axes 1 and 2, which a slab shares with the whole grid, so they are
-    used unchanged; on boxes with a split axis 1 they are re-flattened for
-    the box's extent.  ``make_local(nweights, weights, coef_ps, offset_ps,
+    used unchanged; on boxes with a split axis 1 or 2 they are re-flattened
+    for the box's extents.  ``make_local(nweights, weights, coef_ps, offset_ps,
     n_c, r, neighbors, real, cfd)`` builds the WOperator of one slab plus
     halos (on a GPU: gpu_local_woperator)."""
 
     def __init__(self, wop, weights, dom, make_local, group=None):
-        self.R = R = int(wop.mp)
-        self.R1 = R if dom.split1 else 0
+        R = int(wop.mp)
+        self.Rc = tuple(R if sp else 0 for sp in dom.split)
+        self.R, self.R1 = self.Rc[0], self.Rc[1]
         self.dom, self.group = dom, group
         n_c = [int(x) for x in wop.gd.n_c]
-        n_ext = [dom.m0 + 2 * R, n_c[1], n_c[2]]
+        n_ext = [m + 2 * r if sp else n for m, r, sp, n in
+                 zip(dom.local_shape(), self.Rc, dom.split, n_c)]
         nb = np.array(wop.gd.neighbor_cd, np.int64).reshape(3, 2).copy()
-        nb[0] = -1
+        for c, sp in enumerate(dom.split):
+            if sp:
+                nb[c] = -1
         offset_ps = wop.offset_ps
-        if dom.split1:
-            n_ext[1] = dom.m1 + 2 * R
-            nb[1] = -1
-            offset_ps = [_reflatten(o, n_c[1] + 2 * R, n_ext[1] + 2 * R,
-                                    n_c[2] + 2 * R) for o in offset_ps]
-        self.weights_ext = [exchange_halos(w, (R, R), dom, None, group)
+        if dom.split[1] or dom.split[2]:
+            offset_ps = [_reflatten(o, n_c[1] + 2 * R, n_c[2] + 2 * R,
+                                    n_ext[1] + 2 * R, n_ext[2] + 2 * R)
+                         for o in offset_ps]
+        self.weights_ext = [exchange_halos(w, self.Rc, dom, None, group)
                             for w in weights]
         self.local = make_local(wop.nweights, self.weights_ext, wop.coef_ps,
                                 offset_ps, np.array(n_ext, np.int64), R,
                                 nb, wop.dtype == float, wop.cfd)
 
 
-def _reflatten(offsets, M1, M1_new, M2):
+def _reflatten(offsets, M1, M2, M1_new, M2_new):
     """Flattened stencil offsets (o0 M1 + o1) M2 + o2 of a grid padded to
-    M1 x M2 points on axes 1 and 2, re-flattened for an axis-1 extent of
-    M1_new (every |o1|, |o2| is at most the padding, below half of M1 and
+    M1 x M2 points on axes 1 and 2, re-flattened for extents M1_new x
+    M2_new (every |o1|, |o2| is at most the padding, below half of M1 and
     M2, so the split is unique)."""
     out = []
     for o in np.asarray(offsets, np.int64):
@@ -719,7 +739,7 @@ def _reflatten(offsets, M1, M1_new, M2):
         rest = (o - o2) // M2
         o1 = (rest + M1 // 2) % M1 - M1 // 2
         o0 = (rest - o1) // M1
-        out.append((o0 * M1_new + o1) * M2 + o2)
+        out.append((o0 * M1_new + o1) * M2_new + o2)
     return np.array(out, np.int64)
 
 

@@ -555,18 +555,16 @@ def _weighted_worker(rank, world, port, q, pbc0, dims=None):
         ref_err = [wps.iterate2(wps.step) for _ in range(3)]
         from gpaw_b200.domains import make_domain
         d = make_domain(gd.n_c, gd.pbc_c, rank, world, dims)
-        b, e = d.beg, d.end
-        b1, e1 = d.beg1, d.end1
 
         def cut(a):
-            return torch.from_numpy(np.ascontiguousarray(a[b:e, b1:e1]))
+            return torch.from_numpy(np.ascontiguousarray(d.inner(a)))
         dps = DistributedWeightedFDPoissonSolver(
             wps, [cut(a) for a in arrays], rank, world, _OracleWeighted,
             _OracleTransfer, dims=dims)
         phl = cut(phi)
         rhl = cut(rho)
         err = [dps.iterate(phl, rhl) for _ in range(3)]
-        same = bool(np.array_equal(phl.numpy(), wps.phis[0][b:e, b1:e1]))
+        same = bool(np.array_equal(phl.numpy(), d.inner(wps.phis[0])))
         # a charged system: the dielectric's compensation charge
         rho_c = rho + 0.5 * np.exp(-(x**2).sum(0)) if not pbc0 else \
             rho - rho.mean()
@@ -576,7 +574,7 @@ def _weighted_worker(rank, world, port, q, pbc0, dims=None):
         phc = torch.zeros(phl.shape, dtype=torch.float64)
         n = dps.solve(phc, cut(rho_c), gauss=(wps.rho_gauss, wps.phi_gauss))
         charged = (n, n_ref,
-                   float(np.abs(phc.numpy() - ref_phi[b:e, b1:e1]).max()),
+                   float(np.abs(phc.numpy() - d.inner(ref_phi)).max()),
                    float(np.abs(ref_phi).max()))
         q.put((rank, same, err, ref_err, dps.split_levels, dps.levels,
                charged))
@@ -587,17 +585,17 @@ def _weighted_worker(rank, world, port, q, pbc0, dims=None):
 
 
 @pytest.mark.parametrize('pbc0,dims', [(1, None), (0, None), (1, (2, 2)),
-                                       (0, (1, 3))])
+                                       (0, (1, 3)), (0, (1, 1, 3))])
 def test_slab_weighted_vcycles_equal_whole_grid(pbc0, dims):
     """The dielectric Poisson solver's V-cycles on three slabs, or on the
-    boxes of a 2 x 2 or 1 x 3 process grid (weights and their halos
-    split, coarse weights restricted on the split grid, the flattened
-    stencil offsets re-flattened for a split axis 1) leave
+    boxes of a 2 x 2, 1 x 3 or 1 x 1 x 3 process grid (weights and their
+    halos split, coarse weights restricted on the split grid, the
+    flattened stencil offsets re-flattened for a split axis 1 or 2) leave
     phi bit-identical to the whole grid's; the level-0 error matches to
     rounding.  A charged system (the dielectric's compensation charge in a
     zero-boundary cell; the neutral part of it on a periodic axis 0) takes
     as many V-cycles as the whole-grid solve, phi to 1e-11."""
-    world = 3 if dims is None else dims[0] * dims[1]
+    world = 3 if dims is None else int(np.prod(dims))
     for rank, same, err, ref_err, split, levels, charged in _run_ranks(
             world, _weighted_worker, (pbc0, dims)):
         assert same, rank
@@ -632,12 +630,11 @@ def _pencil_worker(rank, world, port, q, dims):
         out = {}
 
         def box(a, dom):
-            return torch.from_numpy(np.ascontiguousarray(
-                a[..., dom.beg:dom.end, dom.beg1:dom.end1, :]))
+            return torch.from_numpy(np.ascontiguousarray(dom.inner(a)))
 
         def cut(a, dom):
-            return a[..., dom.beg:dom.end, dom.beg1:dom.end1, :]
-        for pbc in ((1, 1, 0), (0, 0, 1), (1, 0, 1)):
+            return dom.inner(a)
+        for pbc in ((1, 1, 0), (0, 0, 1), (1, 0, 1), (1, 1, 1)):
             gd = L.GridDescriptor((24, 20, 12), (4.8, 4.0, 2.4), pbc)
             ph = gd.phase_factor_cd((0.3, -0.2, 0.1))
             rng = np.random.default_rng(41)
@@ -719,14 +716,15 @@ def _pencil_worker(rank, world, port, q, dims):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize('dims', [(2, 2), (1, 3)])
+@pytest.mark.parametrize('dims', [(2, 2), (1, 3), (2, 1, 2)])
 def test_pencils_equal_whole_grid(dims):
-    """Boxes of a 2 x 2 and a 1 x 3 process grid: complex apply with Bloch
-    phases (the Laplacian, and the Mehrstellen stencil whose edge taps
-    read the halo corners, phased along axis 0 then axis 1), restriction
-    and interpolation (nn = 1 and 3), three V-cycles and the
+    """Boxes of 2 x 2, 1 x 3 and 2 x 1 x 2 process grids: complex apply
+    with Bloch phases (the Laplacian, and the Mehrstellen stencil whose
+    edge taps read the halo edges and corners, phased axis by axis),
+    restriction and interpolation (nn = 1 and 3), three V-cycles and the
     preconditioner all give every rank exactly the whole grid's points."""
-    for rank, out in _run_ranks(dims[0] * dims[1], _pencil_worker, (dims,)):
+    for rank, out in _run_ranks(int(np.prod(dims)), _pencil_worker,
+                                (dims,)):
         bad = [k for k, v in out.items() if v is False]
         assert not bad, (rank, bad)
         assert out['split_levels'] >= 1
@@ -739,40 +737,40 @@ def test_box_pieces_cover_each_point_once():
     periodic edge exactly once, from a rank whose box holds it (the
     receiver itself when it does), with the right number of edge
     crossings; points past a zero boundary are left out."""
+    import itertools
+
     from gpaw_b200.domains import GridDomain, box_pieces
     rng = np.random.default_rng(5)
-    for _ in range(300):
-        P0, P1 = int(rng.integers(1, 4)), int(rng.integers(1, 4))
-        n0, n1 = int(rng.integers(1, 9)), int(rng.integers(1, 9))
-        per = (bool(rng.integers(2)), bool(rng.integers(2)))
-        dom = GridDomain((n0, n1, 3), per, 0, (P0, P1),
-                         bool(rng.integers(4) == 0))
-        recv = int(rng.integers(P0 * P1))
+    for _ in range(200):
+        dims = tuple(int(x) for x in rng.integers(1, 4, 3))
+        n = tuple(int(x) for x in rng.integers(1, 7, 3))
+        per = tuple(bool(x) for x in rng.integers(0, 2, 3))
+        dom = GridDomain(n, per, 0, dims, bool(rng.integers(4) == 0))
+        recv = int(rng.integers(dom.size))
         need = []
-        for n in (n0, n1):
-            lo = int(rng.integers(-2 * n - 2, n + 1))
-            need.append((lo, lo + int(rng.integers(0, 3 * n + 3))))
+        for nc in n:
+            lo = int(rng.integers(-2 * nc - 2, nc + 1))
+            need.append((lo, lo + int(rng.integers(0, 3 * nc + 3))))
         hits = {}
-        for owner, src, dst, ln, k in box_pieces(need, (n0, n1), per,
-                                                 dom.boxes, recv):
-            (ob0, oe0), (ob1, oe1) = dom.boxes[owner]
-            assert 0 <= src[0] and src[0] + ln[0] <= oe0 - ob0
-            assert 0 <= src[1] and src[1] + ln[1] <= oe1 - ob1
-            for i in range(ln[0]):
-                for j in range(ln[1]):
-                    g = (need[0][0] + dst[0] + i, need[1][0] + dst[1] + j)
-                    assert g not in hits
-                    hits[g] = (owner, ob0 + src[0] + i, ob1 + src[1] + j, k)
-        for g0 in range(*need[0]):
-            for g1 in range(*need[1]):
-                k0, p0 = divmod(g0, n0)
-                k1, p1 = divmod(g1, n1)
-                inside = (per[0] or k0 == 0) and (per[1] or k1 == 0)
-                assert (g0, g1) in hits if inside else (g0, g1) not in hits
-                if not inside:
-                    continue
-                owner, q0, q1, k = hits[(g0, g1)]
-                assert (q0, q1, k) == (p0, p1, (k0, k1))
-                (b0, e0), (b1, e1) = dom.boxes[recv]
-                if b0 <= p0 < e0 and b1 <= p1 < e1:
-                    assert owner == recv
+        for owner, src, dst, ln, k in box_pieces(need, n, per, dom.boxes,
+                                                 recv):
+            box = dom.boxes[owner]
+            for c in range(3):
+                assert 0 <= src[c] and src[c] + ln[c] <= box[c][1] - box[c][0]
+            for idx in itertools.product(*[range(m) for m in ln]):
+                g = tuple(need[c][0] + dst[c] + idx[c] for c in range(3))
+                assert g not in hits
+                hits[g] = (owner, tuple(box[c][0] + src[c] + idx[c]
+                                        for c in range(3)), k)
+        for g in itertools.product(*[range(*nd) for nd in need]):
+            kp = [divmod(g[c], n[c]) for c in range(3)]
+            inside = all(per[c] or kp[c][0] == 0 for c in range(3))
+            assert (g in hits) == inside
+            if not inside:
+                continue
+            owner, q, k = hits[g]
+            assert q == tuple(p for _, p in kp)
+            assert k == tuple(kk for kk, _ in kp)
+            if all(b <= p < e for (_, p), (b, e) in
+                   zip(kp, dom.boxes[recv])):
+                assert owner == recv
