@@ -24,6 +24,8 @@ order.
 """
 from __future__ import annotations
 
+import functools
+
 import numpy as np
 
 
@@ -306,6 +308,36 @@ def _phase_mul(t, ph):
     r[..., 1] = d * a + c * b
 
 
+def _tup(x):
+    """Nested lists of bounds as nested tuples of ints (hashable)."""
+    if isinstance(x, (list, tuple, np.ndarray)):
+        return tuple(_tup(y) for y in x)
+    return int(x)
+
+
+@functools.lru_cache(maxsize=512)
+def _gather_plan(needs, boxes, rank, n_c, periodic_c):
+    """This rank's part of a gather, computed once per layout: entries
+    (kind, peer, tag, source slices, destination slices, wraps) with kind
+    'copy' (from its own box), 'recv' or 'send', in the order both sides
+    derive from box_pieces."""
+    plan = []
+    for r, need in enumerate(needs):
+        for idx, (owner, src, dst, ln, k) in enumerate(
+                box_pieces(need, n_c, periodic_c, boxes, r)):
+            sl = (Ellipsis,) + tuple(slice(x, x + m)
+                                     for x, m in zip(src, ln))
+            dl = (Ellipsis,) + tuple(slice(x, x + m)
+                                     for x, m in zip(dst, ln))
+            if r == rank and owner == rank:
+                plan.append(('copy', rank, idx, sl, dl, k))
+            elif r == rank:
+                plan.append(('recv', owner, idx, None, dl, k))
+            elif owner == rank:
+                plan.append(('send', r, idx, sl, None, k))
+    return tuple(plan)
+
+
 def gather_box(a, needs, boxes, rank, n_c, periodic_c, phase_cd=None,
                group=None):
     """Collective: every rank gets the points ``needs[rank]`` = ((lo0,
@@ -322,27 +354,23 @@ def gather_box(a, needs, boxes, rank, n_c, periodic_c, phase_cd=None,
     communicator when the first batch starts."""
     import torch
     import torch.distributed as dist
+    plan = _gather_plan(_tup(needs), _tup(boxes), int(rank),
+                        tuple(int(n) for n in n_c),
+                        tuple(bool(p) for p in periodic_c))
     out = a.new_zeros(a.shape[:-3] +
                       tuple(hi - lo for lo, hi in needs[rank]))
     ops, recvd = [], []
-    for r, need in enumerate(needs):
-        for idx, (owner, src, dst, ln, k) in enumerate(
-                box_pieces(need, n_c, periodic_c, boxes, r)):
-            sl = (Ellipsis,) + tuple(slice(x, x + m)
-                                     for x, m in zip(src, ln))
-            dl = (Ellipsis,) + tuple(slice(x, x + m)
-                                     for x, m in zip(dst, ln))
-            if r == rank and owner == rank:
-                out[dl] = a[sl]
-                recvd.append((dl, k, None))
-            elif r == rank:
-                buf = torch.empty_like(out[dl])
-                ops.append(dist.P2POp(dist.irecv, buf, owner, group,
-                                      tag=idx))
-                recvd.append((dl, k, buf))
-            elif owner == rank:
-                ops.append(dist.P2POp(dist.isend, a[sl].contiguous(), r,
-                                      group, tag=idx))
+    for kind, peer, idx, sl, dl, k in plan:
+        if kind == 'copy':
+            out[dl] = a[sl]
+            recvd.append((dl, k, None))
+        elif kind == 'recv':
+            buf = torch.empty_like(out[dl])
+            ops.append(dist.P2POp(dist.irecv, buf, peer, group, tag=idx))
+            recvd.append((dl, k, buf))
+        else:
+            ops.append(dist.P2POp(dist.isend, a[sl].contiguous(), peer,
+                                  group, tag=idx))
     if ops:
         for req in dist.batch_isend_irecv(ops):
             req.wait()

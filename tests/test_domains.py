@@ -774,3 +774,30 @@ def test_box_pieces_cover_each_point_once():
             if all(b <= p < e for (_, p), (b, e) in
                    zip(kp, dom.boxes[recv])):
                 assert owner == recv
+
+
+def test_domain_errors():
+    """A process grid that does not make the rank count, a finest grid too
+    thin for its stencil, and Gauss-Seidel on a split grid are refused."""
+    from gpaw_b200.domains import (DistributedFDOperator,
+                                   DistributedFDPoissonSolver, make_domain)
+    from oracle import gpaw_layer as L
+    with pytest.raises(ValueError):
+        make_domain((8, 8, 8), (1, 1, 1), 0, 4, dims=(2, 3))
+    gd = L.GridDescriptor((8, 8, 8), (2.0, 2.0, 2.0), (1, 1, 1))
+    ps = L.FDPoissonSolver(nn=3, relax='J', be='port')
+    ps.set_grid_descriptor(gd)
+    with pytest.raises(ValueError):
+        DistributedFDPoissonSolver(ps, 0, 4, None, None)  # 2 planes < R = 3
+    ps_gs = L.FDPoissonSolver(nn=3, relax='GS', be='port')
+    ps_gs.set_grid_descriptor(gd)
+    with pytest.raises(NotImplementedError):
+        DistributedFDPoissonSolver(ps_gs, 0, 2, None, None)
+    lap = L.Laplace(gd, -0.5, 1, be='port')
+    dom = make_domain(gd.n_c, gd.pbc_c, 0, 1)
+    op = DistributedFDOperator(lap.coef_p, lap.offset_pc, gd, dom,
+                               lambda c, o, n, p: _OracleLocal(c, o, n, p,
+                                                               float))
+    f = torch.zeros(dom.local_shape(), dtype=torch.float64)
+    with pytest.raises(NotImplementedError):
+        op.relax(1, f, f.clone(), 1)
