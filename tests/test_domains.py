@@ -694,6 +694,9 @@ def _pencil_worker(rank, world, port, q, dims):
         [dps.iterate(phl, rhl) for _ in range(3)]
         out['vcycle'] = bool(np.array_equal(phl.numpy(),
                                             cut(ps.phis[0], d0)))
+        from gpaw_b200.domains import gather_full
+        out['gather_full'] = bool(np.array_equal(
+            gather_full(phl, d0).numpy(), ps.phis[0]))
         out['split_levels'] = dps.split_levels
         gdp = L.GridDescriptor((24, 16, 12), (4.8, 3.2, 2.4), (1, 1, 1))
         php = gdp.phase_factor_cd((0.25, -0.1, 0.2))
