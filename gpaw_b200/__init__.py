@@ -16,9 +16,11 @@ and, in their own modules: ``wfd_operators.WeightedFDOperator``
 (gpaw/dipole_correction.py), ``poisson_moment.MomentCorrectionPoissonSolver``
 (gpaw/poisson_moment.py), ``poisson_extravacuum.ExtraVacuumPoissonSolver``
 (gpaw/poisson_extravacuum.py), ``pot_calc.FDDensityTransfers``
-(gpaw/new/fd/pot_calc.py); beyond the reference: ``MixedPoissonSolver``,
-``batch.PoissonBatch``, ``serving``, ``pipeline.StepPipeline``,
-``autotune``, ``replicas`` and ``domains``.  The C-object layer is
+(gpaw/new/fd/pot_calc.py), ``domains`` (the domain decomposition of
+gpaw/old/domain.py over a torch.distributed process group); beyond the
+reference: ``MixedPoissonSolver``, ``batch.PoissonBatch``, ``serving``,
+``pipeline.StepPipeline``, ``autotune`` and ``replicas``.  The C-object
+layer is
 ``gpaw_b200.cgpaw`` (Operator, WOperator, Transformer, fd_precond).  All arrays are torch CUDA tensors; the arithmetic runs in the
 sm_100a kernels of ``libgpaw_b200.so`` (C ABI: include/gpaw_b200.h).
 """
