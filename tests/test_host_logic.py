@@ -205,6 +205,33 @@ def test_gaussian_multipoles_unit_moments_and_far_field():
         assert np.allclose(mineg, gl, rtol=1e-13, atol=1e-300)
 
 
+def test_gaussians_reference_known_answers():
+    """The reference's own checks of its Gaussians
+    (gpaw/test/test_gauss_func.py:19-54: a 48^3 zero-boundary grid in a
+    20 Bohr cell), on the product's host Gaussians: the moments of g_L for
+    L = 2..8 are delta_LL' to 1e-4, those of the hydrogen density
+    exp(-2 r) / pi are delta_L0 / sqrt(4 pi) to 1.5e-3 for L < 4, and
+    subtracting its monopole with g_0 leaves a zero moment below 1e-7."""
+    import numpy as np
+    from gpaw_b200 import GridDescriptor
+    from gpaw_b200 import multipole as M
+    gd = GridDescriptor((48, 48, 48), (20.0, 20.0, 20.0), False,
+                        device='cpu')
+    g = M.Gaussian(gd)
+
+    def moment(f, L):
+        return float((f * g.get_Y(L)).sum() * gd.dv)
+    for gL in range(2, 9):
+        gl = g.get_gauss(gL)
+        for mL in range(9):
+            assert abs(moment(gl, mL) - (gL == mL)) < 1e-4, (gL, mL)
+    nH = np.exp(-2 * g.r) / np.pi
+    for L in range(4):
+        assert abs(moment(nH, L) - (L == 0) / np.sqrt(4 * np.pi)) < 1.5e-3
+    nH = nH - moment(nH, 0) * g.get_gauss(0)
+    assert abs(moment(nH, 0)) < 1e-7
+
+
 def test_find_neighbors_reference_examples():
     """The examples of find_neighbors' docstring in the reference
     (gpaw/fd_operators.py:241-260), with the reduction of minkowski_basis
