@@ -22,9 +22,10 @@ Restated from (all single-domain, ``comm.size == 1``):
   gpaw/utilities/extend_grid.py:8-56
 * moment correction gpaw/poisson_moment.py:60-243 with the Gaussian
   multipoles of gpaw/utilities/gauss.py:11-160 written from their
-  definitions: parity unpinned for this part (the reference's Python layer
-  cannot be imported here, so nothing runs the reference's own multipole
-  code); it is checked by unit moments and far fields instead
+  definitions, pinned to the reference's own known-answer test of them
+  (gpaw/test/test_gauss_func.py:19-54: unit moments on its 48^3 grid);
+  the reference's Python layer cannot be imported here, so no output of
+  its own multipole code is compared
 """
 from __future__ import annotations
 

@@ -211,7 +211,8 @@ def test_gaussians_reference_known_answers():
     20 Bohr cell), on the product's host Gaussians: the moments of g_L for
     L = 2..8 are delta_LL' to 1e-4, those of the hydrogen density
     exp(-2 r) / pi are delta_L0 / sqrt(4 pi) to 1.5e-3 for L < 4, and
-    subtracting its monopole with g_0 leaves a zero moment below 1e-7."""
+    subtracting its monopole with g_0 leaves a zero moment below 1e-7;
+    the oracle's Gaussians meet the moment checks too."""
     import numpy as np
     from gpaw_b200 import GridDescriptor
     from gpaw_b200 import multipole as M
@@ -230,6 +231,16 @@ def test_gaussians_reference_known_answers():
         assert abs(moment(nH, L) - (L == 0) / np.sqrt(4 * np.pi)) < 1.5e-3
     nH = nH - moment(nH, 0) * g.get_gauss(0)
     assert abs(moment(nH, 0)) < 1e-7
+    # the oracle's restatement meets the same known answers
+    from oracle import gpaw_layer as L
+    go = L.GaussianMP(L.GridDescriptor((48, 48, 48), (20.0, 20.0, 20.0),
+                                       (0, 0, 0)))
+    x, y, z = go.xyz
+    for gL in range(2, 9):
+        gl = go.get_gauss(gL)
+        for mL in range(9):
+            m = float((gl * L.mp_Y(mL, x, y, z, go.r2)).sum() * gd.dv)
+            assert abs(m - (gL == mL)) < 1e-4, (gL, mL)
 
 
 def test_find_neighbors_reference_examples():
