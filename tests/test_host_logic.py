@@ -243,6 +243,106 @@ def test_gaussians_reference_known_answers():
             assert abs(m - (gL == mL)) < 1e-4, (gL, mL)
 
 
+def _port_apply(op, N, cell, pbc, a):
+    """The product operator's stencil applied by the oracle's restatement
+    of the reference's C apply, on the host."""
+    import numpy as np
+    from oracle import gpaw_layer as L
+    gdo = L.GridDescriptor(N, cell, pbc)
+    o = L.FDOperator(op.coef_p, op.offset_pc, gdo, float, be='port')
+    out = np.zeros_like(a)
+    o.apply(a, out)
+    return out
+
+
+def test_gradient_reference_known_answers():
+    """The reference's gradient checks (gpaw/test/fd_ops/test_gradient.py:
+    29-92), the product's stencils applied by the oracle: d/dx of
+    0..7 on a periodic 8-point line is [-3, 1, ..., 1, -3], the backward
+    difference [-1, 1] gives [-7, 1, ..., 1]; d/dy on a zero-boundary
+    7-point line starts at 0.5 and sums to 3; on a GUC cell it starts at
+    -3.5 and sums to 0 (1e-12)."""
+    import numpy as np
+    from gpaw_b200 import FDOperator, GridDescriptor, Gradient
+    gd = GridDescriptor((8, 1, 1), (8.0, 1.0, 1.0), True)
+    a = np.zeros((8, 1, 1))
+    a[:, 0, 0] = np.arange(8)
+    d = _port_apply(Gradient(gd, 0), (8, 1, 1), (8.0, 1.0, 1.0), True, a)
+    assert d[:, 0, 0].tolist() == [-3, 1, 1, 1, 1, 1, 1, -3]
+    back = FDOperator([-1, 1], [[-1, 0, 0], [0, 0, 0]], gd)
+    d = _port_apply(back, (8, 1, 1), (8.0, 1.0, 1.0), True, a)
+    assert d[:, 0, 0].tolist() == [-7, 1, 1, 1, 1, 1, 1, 1]
+    gd = GridDescriptor((1, 8, 1), (1.0, 8.0, 1.0), (1, 0, 1))
+    a = np.zeros((1, 7, 1))
+    a[0, :, 0] = np.arange(1, 8) - 1
+    d = _port_apply(Gradient(gd, 1), (1, 8, 1), (1.0, 8.0, 1.0), (1, 0, 1),
+                    a)
+    assert d[0, 0, 0] == 0.5 and np.sum(d[0, :, 0]) == 3.0
+    cell = ((1.0, 0.0, 0.0), (5.0, 5.0, 0.0), (0.0, 0.0, 0.7))
+    gd = GridDescriptor((1, 7, 1), cell, True)
+    a = np.zeros((1, 7, 1))
+    a[0, :, 0] = np.arange(0, 7) - 1
+    d = _port_apply(Gradient(gd, 1), (1, 7, 1), cell, True, a)
+    assert abs(d[0, 0, 0] + 3.5) < 1e-12 and abs(np.sum(d[0, :, 0])) < 1e-12
+
+
+def _cellpar_to_cell(a, b, c, alpha, beta, gamma):
+    """Cell vectors from lengths and angles (degrees): a along x, b in the
+    xy plane, c from the remaining two angles; right angles give exact
+    zeros."""
+    import numpy as np
+
+    def cs(t):
+        if t == 90:
+            return 0.0, 1.0
+        r = np.radians(t)
+        return np.cos(r), np.sin(r)
+    ca, _ = cs(alpha)
+    cb, _ = cs(beta)
+    cg, sg = cs(gamma)
+    cy = (ca - cb * cg) / sg
+    return np.array([[a, 0, 0], [b * cg, b * sg, 0],
+                     [c * cb, c * cy, c * np.sqrt(1 - cb**2 - cy**2)]])
+
+
+def test_gradient_strange_cells_reference_known_answer():
+    """gpaw/test/fd_ops/test_gradient.py:10-25: on two strongly skewed
+    periodic cells the x-derivative of x at the middle of the grid is 1
+    (relative 1e-6) -- the product's general-cell stencil applied by the
+    oracle."""
+    import numpy as np
+    from gpaw_b200 import GridDescriptor, Gradient
+    for cellpar, size in (((8.7, 5.7, 7.7, 28, 120, 95), (60, 40, 54)),
+                          ((2, 2, 2, 120.1, 120.1, 90), (20, 20, 20))):
+        cell = _cellpar_to_cell(*cellpar)
+        gd = GridDescriptor(size, cell, True)
+        s = np.indices(size, float).reshape(3, -1).T / np.array(size)
+        x = (s @ cell)[:, 0].reshape(size)
+        d = _port_apply(Gradient(gd, 0), size, cell, True, x)
+        n1, n2, n3 = (k // 2 for k in size)
+        assert abs(d[n1, n2, n3] - 1.0) < 1e-6, cellpar
+
+
+def test_transfers_conserve_integrals_reference_known_answer():
+    """gpaw/test/fd_ops/test_non_periodic.py:6-26 on the oracle's
+    transformers (nn = 1, zero boundary, 20^3 -> 40^3 and back, the
+    fine grid's outer planes zeroed before restricting): the integral is
+    kept to 1e-10 both ways."""
+    import numpy as np
+    from oracle import gpaw_layer as L
+    gd1 = L.GridDescriptor((20, 20, 20), (8.0, 8.0, 8.0), 0)
+    a1 = np.random.default_rng(8).random(tuple(gd1.n_c))
+    gd2 = gd1.refine()
+    a2 = np.zeros(tuple(gd2.n_c))
+    L.Transformer(gd1, gd2, be='port').apply(a1, a2)
+    assert abs(gd1.integrate(a1) - gd2.integrate(a2)) < 1e-10
+    for sl in (np.s_[0], np.s_[:, 0], np.s_[:, :, 0], np.s_[-1],
+               np.s_[:, -1], np.s_[:, :, -1]):
+        a2[sl] = 0.0
+    L.Transformer(gd2, gd1, be='port').apply(a2, a1)
+    assert abs(gd1.integrate(a1) - gd2.integrate(a2)) < 1e-10
+
+
 def test_find_neighbors_reference_examples():
     """The examples of find_neighbors' docstring in the reference
     (gpaw/fd_operators.py:241-260), with the reduction of minkowski_basis
