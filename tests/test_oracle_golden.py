@@ -234,3 +234,28 @@ def test_weighted_poisson_with_unit_dielectric_is_fd_poisson():
     wn = wps.solve(wphi, rho)
     assert wn == n
     assert np.array_equal(wphi, phi)
+
+
+def test_poisson_symmetry_reference_known_answer():
+    """gpaw/test/poisson/test_poisson.py:10-47 on the oracle's solver: two
+    identical neutralised charges half a periodic 16^3 cell apart (here a
+    radial bump and its copy shifted by 8 points, so the density is
+    exactly symmetric) give a potential equal at the two centres -- to
+    8e-16 with Jacobi (every level's shift is a whole number of points),
+    to 3e-6 with Gauss-Seidel (whose sweep order is not shift-invariant);
+    nn = 1, eps = 1e-20."""
+    Lc = 2.87 / 0.529177
+    N = 16
+    gd = L.GridDescriptor((N, N, N), (Lc, Lc, Lc))
+    s = np.indices((N, N, N), float) / N * Lc
+    d = np.minimum(s, Lc - s)
+    r = np.sqrt((d**2).sum(0))
+    bump = np.clip(1.0 - r / (N / 2.0 * 0.9), 0, None)
+    a = bump + np.roll(bump, (N // 2,) * 3, axis=(0, 1, 2))
+    a -= gd.integrate(a) / Lc**3
+    for relax, tol in (('J', 8e-16), ('GS', 3e-6)):
+        ps = L.FDPoissonSolver(nn=1, relax=relax, eps=1e-20)
+        ps.set_grid_descriptor(gd)
+        b = np.zeros((N, N, N))
+        ps.solve(b, a, charge=0)
+        assert abs(b[0, 0, 0] - b[8, 8, 8]) < tol, relax
