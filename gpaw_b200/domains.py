@@ -656,14 +656,17 @@ class DistributedFDPoissonSolver:
         return niter
 
     def solve(self, phi, rho, charge=None, maxcharge=1e-6,
-              zero_initial_phi=False, gauss=None):
+              zero_initial_phi=False, gauss=None, use_charge_center=None):
         """Collective: gpaw/poisson.py:182-283 on slabs.  Neutral systems
         and charged fully periodic ones (the homogeneous background of the
         whole grid's charge is subtracted from rho); charged systems in a
         non-periodic cell through a Gaussian carrying the charge, solved
         neutral, its potential added back.  ``gauss``: the whole grid's
-        (rho_gauss, phi_gauss), by default gauss.monopole_gaussian of the
-        grid (each rank keeps its own box of them)."""
+        (rho_gauss, phi_gauss), or a function of the Gaussian's centre
+        returning them; by default gauss.monopole_gaussian of the grid
+        (each rank keeps its own box of them).  ``use_charge_center``
+        (default: the whole-grid solver's setting) centres the Gaussian on
+        the majority charge, from sums over the ranks (:248-262)."""
         actual_charge = self._sum(rho) * float(self.gd.dv)
         background = actual_charge / float(self.gd.dv) / \
             float(np.prod(self.gd.n_c))
@@ -679,11 +682,27 @@ class DistributedFDPoissonSolver:
         if pbc.any():
             raise NotImplementedError(
                 'charged system with mixed boundary conditions')
-        if gauss is None:
-            from .gauss import monopole_gaussian
-            gauss = monopole_gaussian(self.gd)
         import torch
         dom = self.doms[0]
+        if use_charge_center is None:
+            use_charge_center = getattr(self.ps, 'use_charge_center', False)
+        center = None
+        if use_charge_center:
+            from .gauss import charge_center, charge_center_parts
+            rhog_c, total = charge_center_parts(
+                self.gd, rho, actual_charge, (dom.beg, dom.beg1, dom.beg2))
+            t = torch.tensor(list(rhog_c) + [total], dtype=torch.float64,
+                             device=rho.device)
+            if self.size > 1:
+                import torch.distributed as dist
+                dist.all_reduce(t, group=self.group)
+            t = t.cpu().numpy()
+            center = charge_center(self.gd, t[:3], float(t[3]))
+        if gauss is None:
+            from .gauss import monopole_gaussian
+            gauss = monopole_gaussian(self.gd, center=center)
+        elif callable(gauss):
+            gauss = gauss(center)
         rg, pg = [torch.as_tensor(np.ascontiguousarray(
             dom.inner(np.asarray(g)))).to(phi.device) for g in gauss]
         q = actual_charge / np.sqrt(4 * np.pi)

@@ -46,3 +46,45 @@ def monopole_gaussian(gd, a=19.0, center=None):
     rho = np.sqrt(a**3 * 4) / np.pi * exp_ar2
     phi = 2.0 * SQRT_PI * erf_sar / r
     return rho, phi
+
+
+def charge_center_parts(gd, rho, charge, beg=(0, 0, 0)):
+    """The sums behind the centre of the majority charge
+    (gpaw/poisson.py:248-252): rho times the sign of ``charge``, clipped
+    at zero, then per axis sum_i i rho_i over the global grid index i
+    (gpaw/old/grid_descriptor.py:648-663), and the clipped density's sum.
+    ``rho`` (numpy or torch) holds the box of the grid starting ``beg``
+    points past the grid's first stored point.  Returns (rhog_c, total):
+    host floats that add up over the boxes of a split grid."""
+    sign = 1.0 if charge > 0 else -1.0
+    if hasattr(rho, 'detach'):
+        rs = (rho * sign).clamp(min=0.0)
+        sums = [rs.sum(dim=(1, 2)), rs.sum(dim=(0, 2)), rs.sum(dim=(0, 1))]
+        sums = [x.detach().cpu().numpy() for x in sums]
+        total = float(rs.sum())
+    else:
+        rs = np.clip(np.asarray(rho) * sign, 0.0, None)
+        sums = [rs.sum(axis=(1, 2)), rs.sum(axis=(0, 2)),
+                rs.sum(axis=(0, 1))]
+        total = float(rs.sum())
+    rhog_c = np.array([
+        float(np.dot(np.arange(len(sums[c])) + int(gd.beg_c[c]) +
+                     int(beg[c]), sums[c])) for c in range(3)])
+    return rhog_c, total
+
+
+def charge_center(gd, rhog_c, total):
+    """gpaw/poisson.py:248-262 from the sums of charge_center_parts: the
+    centre of the majority charge, minus the dipole moment
+    -(rhog_c . h_cv) dv over the charge; RuntimeError when it lies within
+    7 grid spacings of the cell's faces (the Gaussian would not fit)."""
+    h_cv = np.asarray(gd.h_cv)
+    absolute_charge = total * gd.dv
+    d_c = -np.dot(rhog_c, h_cv) * gd.dv
+    center = -d_c / absolute_charge
+    border_offset = np.inner(h_cv, np.array((7, 7, 7)))
+    borders = np.inner(h_cv, np.asarray(gd.N_c)) - border_offset
+    if np.any(center > borders) or np.any(center < border_offset):
+        raise RuntimeError('Poisson solver: center of charge outside '
+                           'borders - please increase box')
+    return center

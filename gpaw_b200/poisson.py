@@ -28,11 +28,12 @@ class FDPoissonSolver:
                  remove_moment=None, use_charge_center=False,
                  metallic_electrodes=False,
                  use_charged_periodic_corrections=False, xp=None):
-        if remove_moment or use_charge_center or metallic_electrodes or \
+        if remove_moment or metallic_electrodes or \
                 use_charged_periodic_corrections:
             raise NotImplementedError(
-                'moment removal / charge centre / electrodes / charged '
-                'periodic corrections are not part of this path')
+                'moment removal / electrodes / charged periodic '
+                'corrections are not part of this path')
+        self.use_charge_center = bool(use_charge_center)
         self.eps = eps
         self.relax = relax
         self.nn = nn
@@ -48,8 +49,11 @@ class FDPoissonSolver:
         self._exec = None
 
     def todict(self):
-        return {'name': 'fd', 'nn': self.nn, 'relax': self.relax,
-                'eps': self.eps}
+        d = {'name': 'fd', 'nn': self.nn, 'relax': self.relax,
+             'eps': self.eps}
+        if self.use_charge_center:
+            d['use_charge_center'] = True
+        return d
 
     def get_stencil(self):
         return self.nn
@@ -157,8 +161,13 @@ class FDPoissonSolver:
                 phi.zero_()
             return self.solve_neutral(phi, rho - background)
         if not self.gd.pbc_c.any():
+            center = None
+            if self.use_charge_center:
+                from .gauss import charge_center, charge_center_parts
+                center = charge_center(self.gd, *charge_center_parts(
+                    self.gd, rho, actual_charge))
             return _solve_monopole(self, phi, rho, actual_charge,
-                                   zero_initial_phi)
+                                   zero_initial_phi, center)
         raise NotImplementedError(
             'charged system with mixed boundary conditions (dipole '
             'correction / metallic electrodes)')
@@ -277,17 +286,23 @@ def stencil_spectrum(op, gd):
     return lmin, lmax
 
 
-def _solve_monopole(ps, phi, rho, actual_charge, zero_initial_phi):
+def _solve_monopole(ps, phi, rho, actual_charge, zero_initial_phi,
+                    center=None):
     """Charged system in a non-periodic cell (gpaw/poisson.py:233-283):
     subtract a Gaussian carrying the charge, solve the neutral problem,
     add the Gaussian's potential back.  The Gaussian and its potential are
-    computed once per grid (host, float64) and kept on the device."""
-    if getattr(ps, '_gauss_gd', None) is not ps.gd:
+    computed once per grid, or per ``center`` when the charge centre is
+    used (host, float64), and kept on the device."""
+    key = None if center is None else tuple(float(x) for x in center)
+    if getattr(ps, '_gauss_gd', None) is not ps.gd or \
+            getattr(ps, '_gauss_center', None) != key:
         from .gauss import monopole_gaussian
-        rg, pg = monopole_gaussian(ps.gd)
+        rg, pg = monopole_gaussian(ps.gd, center=None if key is None
+                                   else np.array(key))
         ps.rho_gauss = torch.from_numpy(rg).to(phi.device)
         ps.phi_gauss = torch.from_numpy(pg).to(phi.device)
         ps._gauss_gd = ps.gd
+        ps._gauss_center = key
     q = actual_charge / np.sqrt(4 * pi)
     rho_neutral = rho - q * ps.rho_gauss
     if zero_initial_phi:

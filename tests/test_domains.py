@@ -804,3 +804,67 @@ def test_domain_errors():
     f = torch.zeros(dom.local_shape(), dtype=torch.float64)
     with pytest.raises(NotImplementedError):
         op.relax(1, f, f.clone(), 1)
+
+
+def _asym_worker(rank, world, port, q):
+    import traceback
+
+    import torch.distributed as dist
+
+    from gpaw_b200 import GridDescriptor
+    from gpaw_b200 import multipole as M
+    from gpaw_b200.domains import DistributedFDPoissonSolver
+    from gpaw_b200.gauss import monopole_gaussian
+    from oracle import gpaw_layer as L
+    os.environ['MASTER_ADDR'] = '127.0.0.1'
+    os.environ['MASTER_PORT'] = str(port)
+    dist.init_process_group('gloo', rank=rank, world_size=world)
+    try:
+        a, N = 20.0, 48
+        c0 = np.array((a / 2, a / 2, 3 * a / 4))
+        gd = L.GridDescriptor((N, N, N), (a, a, a), 0)
+        pgd = GridDescriptor((N, N, N), (a, a, a), False, device='cpu')
+        g = M.Gaussian(pgd, a=19, center=c0)
+        ng, vg = g.get_gauss(0), g.get_gauss_pot(0)
+        ps = L.FDPoissonSolver(nn=3, relax='J', be='port')
+        ps.set_grid_descriptor(gd)
+        dps = DistributedFDPoissonSolver(
+            ps, rank, world,
+            lambda c, o, n, p: _OracleLocal(c, o, n, p, float),
+            _OracleTransfer)
+        dom = dps.doms[0]
+        pot = torch.zeros(dom.local_shape(), dtype=torch.float64)
+        dps.solve(pot, torch.from_numpy(np.ascontiguousarray(dom.inner(ng))),
+                  charge=1.0, use_charge_center=True,
+                  gauss=lambda c: monopole_gaussian(pgd, center=c))
+        t = torch.tensor([float(((pot.numpy() - dom.inner(vg))**2).sum())])
+        dist.all_reduce(t)
+        q.put((rank, float(t[0]) * gd.dv))
+    except Exception:
+        q.put(('error', traceback.format_exc()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_charge_center_solve_reference_known_answer():
+    """gpaw/test/poisson/test_poisson_asym.py:9-41 on two slabs: a unit
+    Gaussian centred at (a/2, a/2, 3a/4) in a 20 Bohr zero-boundary cell
+    (48^3, nn = 3), solved as a charged system with the Gaussian placed on
+    the centre of charge (found from sums over the ranks), gives its
+    analytic potential to a residual below 1e-5."""
+    from gpaw_b200 import GridDescriptor
+    from gpaw_b200 import multipole as M
+    from gpaw_b200.gauss import charge_center, charge_center_parts
+    for rank, res2 in _run_ranks(2, _asym_worker):
+        assert res2**0.5 < 1e-5, (rank, res2**0.5)
+    # the centre of charge of that Gaussian is where it was put
+    pgd = GridDescriptor((48, 48, 48), (20.0, 20.0, 20.0), False,
+                         device='cpu')
+    c0 = np.array((10.0, 10.0, 15.0))
+    ng = M.Gaussian(pgd, a=19, center=c0).get_gauss(0)
+    center = charge_center(pgd, *charge_center_parts(pgd, ng, 1.0))
+    assert np.abs(center - c0).max() < 1e-6
+    with pytest.raises(RuntimeError):      # within 7 spacings of a face
+        ng = M.Gaussian(pgd, a=19, center=np.array((10.0, 10.0, 1.5)))
+        charge_center(pgd, *charge_center_parts(pgd, ng.get_gauss(0),
+                                                1.0))
