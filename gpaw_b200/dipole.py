@@ -15,7 +15,8 @@ import numpy as np
 import torch
 from scipy.special import erf
 
-BOHR = 0.52917721
+BOHR = 0.5291772105638411  # Angstrom: ase.units.Bohr (CODATA 2014), the
+#                             reference's conversion
 
 
 def calculate_dipole_moment(gd, rho_g, center=False, origin_c=None):

@@ -19,7 +19,8 @@ import torch
 
 from .multipole import Gaussian
 
-BOHR = 0.52917721
+BOHR = 0.5291772105638411  # Angstrom: ase.units.Bohr (CODATA 2014), the
+#                             reference's conversion
 
 
 class MomentCorrection:
@@ -48,6 +49,12 @@ class MomentCorrection:
         else:
             moms = '(' + ', '.join([f'{m:.0f}' for m in self.moms]) + ')'
         return f'[{center}] {moms}'
+
+    def __repr__(self):
+        """:53-57: the moments and the centre in Angstrom (the reference
+        scales its stored centre in place here; this leaves it as it is)."""
+        center = None if self.center is None else self.center * BOHR
+        return f'{repr(self.moms)} @ {repr(center)}'
 
 
 class MomentCorrectionPoissonSolver:
@@ -177,6 +184,6 @@ class MomentCorrectionPoissonSolver:
     def __repr__(self):
         n = len(self.moment_corrections)
         s = ('no corrections' if n == 0 else
-             repr(str(self.moment_corrections[0])) if n < 2 else
+             repr(self.moment_corrections[0]) if n < 2 else
              f'{n} corrections')
         return f'MomentCorrectionPoissonSolver ({s})'

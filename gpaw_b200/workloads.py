@@ -8,7 +8,8 @@ from __future__ import annotations
 
 import numpy as np
 
-BOHR = 0.52917721  # Angstrom
+BOHR = 0.5291772105638411  # Angstrom: ase.units.Bohr (CODATA 2014), the
+#                             reference's conversion
 
 
 def gaussian_density(gd, centers, widths, charges):

@@ -922,13 +922,14 @@ def test_moment_correction_against_oracle(corr, cuda):
     if corr == 'center':
         mc_p, mc_o = 9, 9
     else:
-        ca = [(c0 + [1.0, 0.4, -0.6]) * 0.52917721,
-              (c0 - [1.2, -0.5, 0.8]) * 0.52917721]
+        from gpaw_b200.poisson_moment import BOHR
+        ca = [(c0 + [1.0, 0.4, -0.6]) * BOHR,
+              (c0 - [1.2, -0.5, 0.8]) * BOHR]
         mc_p = [{'moms': range(4), 'center': ca[0]},
                 {'moms': [0, 3, 6], 'center': ca[1]}]
-        mc_o = [{'moms': range(4), 'center': np.asarray(ca[0]) / 0.52917721},
+        mc_o = [{'moms': range(4), 'center': np.asarray(ca[0]) / BOHR},
                 {'moms': [0, 3, 6],
-                 'center': np.asarray(ca[1]) / 0.52917721}]
+                 'center': np.asarray(ca[1]) / BOHR}]
     po = L.MomentCorrectionPoissonSolver(L.FDPoissonSolver(nn=3, eps=1e-18),
                                          mc_o)
     po.set_grid_descriptor(gdo)

@@ -374,3 +374,61 @@ def test_gradient_stencil_general_cells():
                 e = np.zeros(3)
                 e[v] = 0.7
                 assert np.allclose(first, e, rtol=0, atol=1e-12), (cell, n, v)
+
+
+class _NoSolver:
+    """A stand-in wrapped solver: description and dict only."""
+
+    def get_description(self):
+        return 'No interaction'
+
+    def todict(self):
+        return {'name': 'nointeraction'}
+
+
+_MC_CASES = [
+    (None, 0, None, 'no corrections'),
+    ([], 0, None, 'no corrections'),
+    (4, 1, ['1 moment corrections', 'center', 'range(0, 4)'],
+     'array([0, 1, 2, 3]) @ None'),
+    (9, 1, ['1 moment corrections', 'center', 'range(0, 9)'],
+     'array([0, 1, 2, 3, 4, 5, 6, 7, 8]) @ None'),
+    ([dict(moms=range(4), center=[1., 1., 1.])], 1,
+     ['1 moment corrections', '[1.00, 1.00, 1.00]', 'range(0, 4)'],
+     'array([0, 1, 2, 3]) @ array([1., 1., 1.])'),
+    ([dict(moms=[1, 2, 3], center=[1., 1., 1.])], 1,
+     ['1 moment corrections', '[1.00, 1.00, 1.00]', 'range(1, 4)'],
+     'array([1, 2, 3]) @ array([1., 1., 1.])'),
+    ([dict(moms=[0, 2, 3], center=[1., 1., 1.])], 1,
+     ['1 moment corrections', '[1.00, 1.00, 1.00]', '(0, 2, 3)'],
+     'array([0, 2, 3]) @ array([1., 1., 1.])'),
+    ([dict(moms=range(4), center=[2, 3, 4]),
+      dict(moms=range(4), center=[7.4, 3.1, 0.1])], 2,
+     ['2 moment corrections', '[2.00, 3.00, 4.00]', '[7.40, 3.10, 0.10]',
+      'range(0, 4)'], '2 corrections'),
+]
+
+
+@pytest.mark.parametrize('mc, n, strings, rep', _MC_CASES)
+def test_moment_correction_api_reference_cases(mc, n, strings, rep):
+    """gpaw/test/poisson/test_poisson_moment.py:11-116: the number of
+    corrections each form of ``moment_corrections`` makes, the
+    description (the wrapped solver's, then '<n> moment corrections' and
+    each centre in Angstrom with its moments) and the repr."""
+    import numpy as np
+    from gpaw_b200.poisson_moment import (MomentCorrection,
+                                          MomentCorrectionPoissonSolver)
+    if isinstance(mc, list):
+        mc = [dict(moms=m['moms'], center=np.array(m['center']))
+              for m in mc]
+    ps = MomentCorrectionPoissonSolver(_NoSolver(), mc)
+    assert isinstance(ps.moment_corrections, list)
+    assert len(ps.moment_corrections) == n
+    assert all(isinstance(m, MomentCorrection)
+               for m in ps.moment_corrections)
+    desc = ps.get_description()
+    assert desc.startswith('No interaction')
+    rest = desc[len('No interaction'):]
+    for s in strings or ['0 moment corrections']:
+        assert s in rest, (s, rest)
+    assert repr(ps) == f'MomentCorrectionPoissonSolver ({rep})'
