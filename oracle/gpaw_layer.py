@@ -19,7 +19,8 @@ Restated from (all single-domain, ``comm.size == 1``):
 * density transfers gpaw/new/fd/pot_calc.py:37-41, 72-80
 * dipole layer      gpaw/dipole_correction.py:84-172
 * extra vacuum      gpaw/poisson_extravacuum.py:13-232, with
-  gpaw/utilities/extend_grid.py:8-56
+  gpaw/utilities/extend_grid.py:8-56; pinned to the golden differences of
+  gpaw/test/poisson/test_poisson_extravacuum.py:100-129
 * moment correction gpaw/poisson_moment.py:60-243 with the Gaussian
   multipoles of gpaw/utilities/gauss.py:11-160 written from their
   definitions, pinned to the reference's own known-answer test of them

@@ -259,3 +259,42 @@ def test_poisson_symmetry_reference_known_answer():
         b = np.zeros((N, N, N))
         ps.solve(b, a, charge=0)
         assert abs(b[0, 0, 0] - b[8, 8, 8]) < tol, relax
+
+
+def test_extravacuum_reference_golden_values():
+    """gpaw/test/poisson/test_poisson_extravacuum.py:15-129 on the oracle's
+    restatement: a two-dipole density on a 16 x 16 x 48 zero-boundary
+    grid, eps = 1e-16.  The extra-vacuum solver on the same grid equals the
+    plain solve (1e-15); with 4x the points the largest difference is the
+    reference's 2.6485385144e-02, and against that, one coarsening gives
+    1.5043946611e-04, two 1.2980906205e-03, two cascaded single
+    coarsenings 1.7086531461e-04 (each to 1e-8, the reference's bound)."""
+    eps = 1e-16
+    N_c = np.array((1, 1, 3)) * 16
+    gd = L.GridDescriptor(N_c, N_c / 16.0, False)
+    xyz = gd.get_grid_point_coordinates()
+    rho = gd.zeros()
+    for z0 in (1, 2):
+        rho += 10 * (xyz[2] - z0) * np.exp(
+            -20 * np.sum((xyz.T - np.array([.5, .5, z0])).T**2, axis=0))
+
+    def solve(ps):
+        ps.set_grid_descriptor(gd)
+        phi = gd.zeros()
+        ps.solve(phi, rho)
+        return phi
+
+    def fd():
+        return L.FDPoissonSolver(eps=eps)
+    ref = solve(fd())
+    same = solve(L.ExtraVacuumPoissonSolver(N_c, fd()))
+    assert np.abs(same - ref).max() < 1e-15
+    gpts = N_c * 4
+    big = solve(L.ExtraVacuumPoissonSolver(gpts, fd()))
+    assert abs(np.abs(big - ref).max() - 2.6485385144e-02) < 1e-8
+    for coarses, want in ((1, 1.5043946611e-04), (2, 1.2980906205e-03)):
+        p = solve(L.ExtraVacuumPoissonSolver(gpts, fd(), fd(), coarses))
+        assert abs(np.abs(p - big).max() - want) < 1e-8, coarses
+    inner = L.ExtraVacuumPoissonSolver(gpts // 2, fd(), fd(), 1)
+    p = solve(L.ExtraVacuumPoissonSolver(gpts // 2, inner, fd(), 1))
+    assert abs(np.abs(p - big).max() - 1.7086531461e-04) < 1e-8
