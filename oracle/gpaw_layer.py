@@ -15,7 +15,8 @@ Restated from (all single-domain, ``comm.size == 1``):
 * Poisson solver    gpaw/poisson.py:182-213, 321-537
 * preconditioner    gpaw/preconditioner.py:9-93
 * weighted operator gpaw/wfd_operators.py:7-81 (C object: the reference's
-  WOperator), dielectric solver gpaw/old/solvation/poisson.py:48-124
+  WOperator), dielectric solver gpaw/old/solvation/poisson.py:48-124,
+  checked against gpaw/test/solvation/test_poisson.py:46-156
 * density transfers gpaw/new/fd/pot_calc.py:37-41, 72-80
 * dipole layer      gpaw/dipole_correction.py:84-172
 * extra vacuum      gpaw/poisson_extravacuum.py:13-232, with

@@ -298,3 +298,84 @@ def test_extravacuum_reference_golden_values():
     inner = L.ExtraVacuumPoissonSolver(gpts // 2, fd(), fd(), 1)
     p = solve(L.ExtraVacuumPoissonSolver(gpts // 2, inner, fd(), 1))
     assert abs(np.abs(p - big).max() - 1.7086531461e-04) < 1e-8
+
+
+def test_solvation_poisson_reference_known_answers():
+    """gpaw/test/solvation/test_poisson.py:46-156 on the oracle's dielectric
+    solver (WeightedFDPoissonSolver, nn = 3, Jacobi, eps = 2e-10) with the
+    product's Laplacian and Gradient stencils, on the reference's 60^3
+    zero-boundary grid of a 12 Angstrom box: two opposite Gaussians and one
+    charged Gaussian in a constant permittivity of 80, and a neutral and a
+    charged system in a permittivity dipping to 1 (its gradient taken with
+    the nn = 3 Gradient), each within 1e-3 of the analytic potential."""
+    from scipy.special import erf
+
+    from gpaw_b200 import GridDescriptor, Gradient, Laplace
+    from gpaw_b200 import multipole as M
+    from gpaw_b200.poisson_moment import BOHR
+    box, n = 12.0, 60
+    cell = (box / BOHR,) * 3
+    gd = L.GridDescriptor((n, n, n), cell, False)
+    pgd = GridDescriptor((n, n, n), cell, False, device='cpu')
+
+    def stencils(g, scale, nn):
+        gp = GridDescriptor(tuple(int(x) for x in g.N_c), g.cell_cv, False,
+                            device='cpu')
+        ops = [Laplace(gp, scale, nn)] + [Gradient(gp, j, scale, nn)
+                                          for j in range(3)]
+        return [(op.coef_p, op.offset_pc) for op in ops]
+
+    def gradient(x):
+        out = []
+        for i in range(3):
+            gr = Gradient(pgd, i, 1.0, 3)
+            o = L.FDOperator(gr.coef_p, gr.offset_pc, gd)
+            y = np.zeros_like(x)
+            o.apply(x, y)
+            out.append(y)
+        return np.array(out)
+
+    def solve(eps, rho):
+        ps = L.WeightedFDPoissonSolver(stencils, nn=3, relax='J', eps=2e-10)
+        ps.set_grid_descriptor(gd)
+        ps.set_dielectric([eps] + list(gradient(eps - 80.0)))
+        phi = np.zeros_like(rho)
+        ps.solve(phi, rho)
+        return phi
+
+    def gauss(shift):
+        return M.Gaussian(pgd, center=(box / 2 + shift) * np.ones(3) / BOHR)
+    const = np.full(tuple(gd.n_c), 80.0)
+    rho = np.zeros_like(const)
+    want = np.zeros_like(const)
+    for q, shift in ((-1., -1.), (1., 1.)):
+        g = gauss(shift)
+        rho += q / np.sqrt(4 * np.pi) * g.get_gauss(0)
+        want += q / np.sqrt(4 * np.pi) * g.get_gauss_pot(0) / 80.0
+    assert np.abs(solve(const, rho) - want).max() < 1e-3
+    g = gauss(1.0)
+    qn = -2.0 / np.sqrt(4 * np.pi)
+    assert np.abs(solve(const, qn * g.get_gauss(0)) -
+                  qn * g.get_gauss_pot(0) / 80.0).max() < 1e-3
+    for qs, shifts, epsshift in (((-1., 1.), (-.4, .4), 0.0),
+                                 ((2.,), (-1.,), -1.0)):
+        ge = gauss(epsshift).get_gauss(0)
+        eps = 80.0 - ge / ge.max() * 79.0
+        grad_eps = gradient(eps - 80.0)
+        rho = np.zeros_like(eps)
+        want = np.zeros_like(eps)
+        for q, shift in zip(qs, shifts):
+            g = gauss(shift)
+            phi_t = g.get_gauss_pot(0)
+            fac = 2. * np.sqrt(g.a) * np.exp(-g.a * g.r2)
+            fac /= np.sqrt(np.pi) * g.r2
+            fac -= erf(np.sqrt(g.a) * g.r) / (g.r2 * g.r)
+            fac *= 2.0 * 1.7724538509055159
+            grad_phi = fac * np.array(g.xyz)
+            lap_phi = -4. * np.pi * g.get_gauss(0)
+            rho_t = -1. / (4. * np.pi) * ((grad_eps * grad_phi).sum(0) +
+                                          eps * lap_phi)
+            norm = gd.integrate(rho_t)
+            rho += rho_t / (norm * q)
+            want += phi_t / (norm * q)
+        assert np.abs(solve(eps, rho) - want).max() < 1e-3, qs
