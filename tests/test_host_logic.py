@@ -432,3 +432,34 @@ def test_moment_correction_api_reference_cases(mc, n, strings, rep):
     for s in strings or ['0 moment corrections']:
         assert s in rest, (s, rest)
     assert repr(ps) == f'MomentCorrectionPoissonSolver ({rep})'
+
+
+def test_grid_descriptor_reference_known_answers():
+    """gpaw/test/fd_ops/test_gd.py:7-46 on the product's GridDescriptor:
+    the integral of ones over a 4^3 unit cell is 1; distance vectors fold
+    a point outside the box along periodic axes only (minimum image); on
+    the sheared cell [[1, 1, 0], [0, 1, 0], [0, 0, 1]] the distances of
+    row (1, 1) are [-0.5, -0.25, -1, -0.75]."""
+    import numpy as np
+    import torch
+    from gpaw_b200 import GridDescriptor
+    gd = GridDescriptor([4, 4, 4], (1.0, 1.0, 1.0), True, device='cpu')
+    a = torch.ones(tuple(gd.n_c), dtype=torch.float64)
+    assert float(gd.integrate(a)) == 1.0
+
+    def mic(r_v, pbc_c):
+        r_c = r_v % 1.0
+        r_c -= (2 * r_c).astype(int)
+        return np.where(pbc_c, r_c, r_v)
+    pbc_c = [1, 1, 0]
+    gd = GridDescriptor([10] * 3, (1.0, 1.0, 1.0), pbc_c, device='cpu')
+    for r_v in (np.array([0.01, 2.49, 0.01]), np.array([2.49, 0.01, 0.01])):
+        dr = gd.get_grid_point_distance_vectors(r_v)
+        want = mic(np.dot(gd.h_cv, gd.beg_c) - r_v, pbc_c)
+        assert np.abs(dr[:, 0, 0, 0] - want).max() < 1e-15
+    cell = np.eye(3)
+    cell[0, 1] = 1
+    gd = GridDescriptor([2, 4, 1], cell, True, device='cpu')
+    r = gd.get_grid_point_distance_vectors(np.zeros(3))
+    assert np.allclose(r[1, 1].reshape(4), [-0.5, -0.25, -1., -0.75],
+                       rtol=1e-6, atol=1e-12)
