@@ -1,12 +1,12 @@
-"""Slab decomposition of one grid along axis 0 over gloo ranks on the host
-(world sizes 2 and 3): the halo exchange, with the Bloch phase of axis 0
-across a periodic edge, and a stencil applied slab by slab equal to the
-same stencil on the whole grid; restriction, interpolation and FD Poisson
-V-cycles on slabs equal to the whole grid's; the same on boxes of a
-P0 x P1 process grid.  The local operators here are
-the oracle's CPU ones; on GPUs the slabs run the library's kernels and the exchange
-goes over NCCL (one GPU per process; not run here, where a call has one
-GPU)."""
+"""Domain decomposition of one grid over gloo ranks on the host (2 to 5
+ranks): slabs along axis 0 and boxes of 2-D and 3-D process grids.  The
+halo exchange (Bloch phases across periodic edges), stencils, weighted
+operators, restriction and interpolation, the plain and dielectric FD
+Poisson V-cycles and solves, and the preconditioner, each against the
+same computation on the whole grid.  The local operators here are the
+oracle's CPU ones; on GPUs the boxes run the library's kernels and the
+exchange goes over NCCL (one GPU per process; not run here, where a call
+has one GPU)."""
 import os
 import socket
 
