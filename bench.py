@@ -264,7 +264,8 @@ def run_reference(args):
     steps, warm = args.steps, args.warmup
     cb = cpu_measure(CPU_SAMPLE, reps=max(1, min(steps, 3)))
     line = {'metric': METRIC, 'value': cb['value'], 'unit': 'GB/s',
-            'n_gpus': args.gpus, 'steps': steps, 'warmup': warm,
+            'n_gpus': int(os.environ.get('WORLD_SIZE', '1')),
+            'steps': steps, 'warmup': warm,
             'ms_per_step': sum(algorithmic_bytes(CPU_SAMPLE)) /
             (cb['value'] * 1e9) * 1e3,
             'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
@@ -319,6 +320,54 @@ def poisson_c1(dev, nsolve=20, cpu=True):
     return out
 
 
+def c1_apply(dev, reps=50):
+    """The C1 stand-alone apply: one FDOperator.apply of the Poisson
+    solver's Laplacian (nn = 3, scaled by -1/(4 pi)) on a seeded N(0,1)
+    float64 array of the 64^3 zero-boundary grid (63^3 unknowns).  The
+    array (4 MB) fits in L2, so L2 is flushed (a 256 MB write) before every
+    timed launch; each launch is timed on its own with CUDA events.  Also
+    reported: the same launch back to back with the array L2-resident."""
+    import torch
+    from gpaw_b200 import GridDescriptor, Laplace
+    from gpaw_b200.workloads import BOHR
+    h = 0.2 / BOHR
+    gd = GridDescriptor((64, 64, 64), (64 * h,) * 3, 0, device=dev)
+    op = Laplace(gd, -0.25 / np.pi, 3)
+    rng = np.random.default_rng(0)
+    a = torch.from_numpy(rng.standard_normal(tuple(gd.n_c))).to(dev)
+    b = torch.empty_like(a)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    st = torch.cuda.current_stream()
+    for _ in range(5):
+        op.apply(a, b)
+    cold = []
+    for _ in range(reps):
+        flush.fill_(1)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        op.apply(a, b)
+        e1.record(st)
+        e1.synchronize()
+        cold.append(e0.elapsed_time(e1) / 1e3)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(reps):
+        op.apply(a, b)
+    e1.record(st)
+    e1.synchronize()
+    hot = e0.elapsed_time(e1) / 1e3 / reps
+    t = float(np.median(cold))
+    nbytes = 16 * a.numel()
+    peak, _ = measured_peak()
+    return {'grid': [63, 63, 63], 'dtype': 'f64', 'nn': 3,
+            'us': t * 1e6, 'gbs': nbytes / t / 1e9,
+            'frac': nbytes / t / 1e9 / peak,
+            'us_l2_resident': hot * 1e6, 'gbs_l2_resident': nbytes / hot / 1e9,
+            'how': 'median of %d launches, L2 flushed before each' % reps}
+
+
 def c1_cpu(phi_gpu, n_gpu):
     """The same C1 solve by the reference's C core on the host cores (one
     thread and all threads, the better reported) and the GPU potential's
@@ -348,9 +397,10 @@ def c1_cpu(phi_gpu, n_gpu):
 
 def poisson_c3(dev, nsolve=5):
     """192^3 zero-BC, h = 0.18 A, 64 Gaussians: plain FP64 V-cycle with the
-    reference schedule (7 grids) versus FP32 V-cycles (6 levels, 2 + 2
-    smoothing sweeps) in FP64 defect correction, both to 1e-10 relative
-    residual."""
+    reference schedule (7 grids) versus FP32 V-cycles in FP64 defect
+    correction, both to 1e-10 relative residual.  The mixed solver runs
+    with the stated 4 levels (2 + 2 smoothing sweeps); a 6-level variant is
+    reported beside it (coarsest grid 5^3 instead of 23^3)."""
     import torch
     from gpaw_b200 import FDPoissonSolver, GridDescriptor, MixedPoissonSolver
     from gpaw_b200.workloads import (BOHR, c3_density,
@@ -363,12 +413,15 @@ def poisson_c3(dev, nsolve=5):
     fp64 = FDPoissonSolver(nn=3, relax='J',
                            eps=eps_for_relative_residual(rho, gd))
     fp64.set_grid_descriptor(gd)
-    mixed = MixedPoissonSolver(nn=3, tol=1e-10, levels=6)
-    mixed.set_grid_descriptor(gd)
+    mixed4 = MixedPoissonSolver(nn=3, tol=1e-10, levels=4)
+    mixed4.set_grid_descriptor(gd)
+    mixed6 = MixedPoissonSolver(nn=3, tol=1e-10, levels=6)
+    mixed6.set_grid_descriptor(gd)
     out = {'grid': [192, 192, 192], 'h_angstrom': 0.18, 'gaussians': 64}
     phis = {}
     for tag, ps in (('fp64_reference_schedule', fp64),
-                    ('mixed_fp32_in_fp64', mixed)):
+                    ('mixed_4_levels', mixed4),
+                    ('mixed_6_levels', mixed6)):
         phi = gd.zeros()
         ps.solve_neutral(phi, rho_d)      # warm-up (builds the graph)
         times = []
@@ -386,12 +439,14 @@ def poisson_c3(dev, nsolve=5):
         out[tag] = {'vcycles': n, 'ms_per_solve': t * 1e3,
                     'solves_per_s': 1.0 / t,
                     'rel_residual': float(np.sqrt(n2.item())) / rnorm}
-    a, b = phis['mixed_fp32_in_fp64'], phis['fp64_reference_schedule']
-    out['max_rel_diff_mixed_vs_fp64'] = float(
-        (a - b).abs().max() / b.abs().max())
-    out['speedup_mixed_over_fp64'] = (
-        out['mixed_fp32_in_fp64']['solves_per_s'] /
-        out['fp64_reference_schedule']['solves_per_s'])
+    b = phis['fp64_reference_schedule']
+    for lv in (4, 6):
+        a = phis[f'mixed_{lv}_levels']
+        out[f'mixed_{lv}_levels']['max_rel_diff_vs_fp64'] = float(
+            (a - b).abs().max() / b.abs().max())
+        out[f'speedup_mixed_{lv}_over_fp64'] = (
+            out[f'mixed_{lv}_levels']['solves_per_s'] /
+            out['fp64_reference_schedule']['solves_per_s'])
     return out
 
 
@@ -442,11 +497,36 @@ def poisson_c4(dev, count=512, precisions=('mixed', 'fp64'), cpu=True):
     return out
 
 
+# Algorithmic bytes per fine grid point of each kernel of the fd_precond
+# sequence (gpaw/preconditioner.py:74-93 as gb_fd_precond fuses it), for
+# float64 data of 8 B: level 1 has 1/8 of the fine points, level 2 1/64.
+PRECOND_BYTES_PER_FINE_PT = {
+    'restrict0': 8 + 2 * 8 / 8,            # R in; r1, d1 out
+    'kin1 q1 = K1': 3 * 8 / 8,              # d1, r1 in; q1 out
+    'restrict1': 8 / 8 + 2 * 8 / 64,        # q1 in; r2, d2 out
+    'kin2': 3 * 8 / 64,                     # d2, r2 in; q2 out
+    'interp2': 8 / 64 + 2 * 8 / 8,          # q2, d1 in; d1 out
+    'kin1 q1 = d1': 3 * 8 / 8,              # d1, r1 in; q1 out
+    'interp1': 8 / 8 + 8,                   # q1 in; q0 out
+    'kin0': 3 * 8,                          # q0, R in; d0 out
+}
+
+
+def _precond_key(label):
+    for k in PRECOND_BYTES_PER_FINE_PT:
+        if label.startswith(k):
+            return k
+    return label
+
+
 def precond_c4(dev, nbands=128):
     """Preconditioner (gpaw/preconditioner.py) on 128 float64 band residuals,
-    112^3 periodic (Gamma point), kinetic operator nn = 3."""
+    112^3 periodic (Gamma point), kinetic operator nn = 3: time per call,
+    the black-box figure (R in, d0 out: 16 B/pt) and the per-kernel times
+    and bytes of the executed sequence (the library's kernel trace)."""
     import torch
     from gpaw_b200 import GridDescriptor, Laplace, Preconditioner
+    from gpaw_b200._lib import KernelTrace
     from gpaw_b200.workloads import BOHR
     N = (112, 112, 112)
     gd = GridDescriptor(N, (112 * 0.18 / BOHR,) * 3, 1, device=dev)
@@ -468,8 +548,27 @@ def precond_c4(dev, nbands=128):
     e1.record()
     torch.cuda.synchronize()
     t = e0.elapsed_time(e1) / 1e3 / reps
+    with KernelTrace() as tr:
+        for _ in range(reps):
+            pc(R, None, out=out)
+    per = {}
+    for label, ms in tr.intervals:
+        per.setdefault(_precond_key(label), []).append(ms)
+    npts = R.numel()
+    kernels = []
+    seq_bytes = 0.0
+    for k, bpp in PRECOND_BYTES_PER_FINE_PT.items():
+        ms = float(np.mean(per.get(k, [float('nan')])))
+        nb = bpp * npts
+        seq_bytes += nb
+        kernels.append({'kernel': k, 'ms': ms, 'bytes': nb,
+                        'gbs': nb / ms / 1e6})
+    ksum = sum(k['ms'] for k in kernels) / 1e3
     return {'bands': nbands, 'grid': list(N), 'ms_per_call': t * 1e3,
-            'blackbox_gbs': 16 * R.numel() / t / 1e9}
+            'blackbox_gbs': 16 * npts / t / 1e9,
+            'sequence_bytes': seq_bytes,
+            'sequence_gbs': seq_bytes / t / 1e9,
+            'kernel_sum_ms': ksum * 1e3, 'kernels': kernels}
 
 
 def weighted_fd(dev, reps=10, cpu=True):
@@ -618,12 +717,13 @@ def weighted_poisson(dev, nsolve=5, cpu=True):
     return out
 
 
-def serving_c5(dev, rates=(50, 100, 200, 500, 1000, 2000), count=60):
+def serving_c5(dev, rates=(50, 100, 200, 500, 1000, 2000), count=1000,
+               warm_count=200):
     """Poisson-arrival stream of mixed-precision Poisson solves (to 1e-10)
     and nn = 3 stencil applications, grid sides log-uniform in [24, 160]
     (multiples of 8), admitted against a 16 GB budget, 8 slots, three
-    resident solvers per shape; each rate's stream is served once untimed,
-    then timed."""
+    resident solvers per shape; `count` requests per rate, after an
+    untimed pass of `warm_count` requests at the same rate."""
     from gpaw_b200.serving import Server, latency_stats, make_requests
     # every shape of the stream has resident solvers (graphs captured)
     # before serving starts; the loop never builds one while it serves
@@ -635,15 +735,14 @@ def serving_c5(dev, rates=(50, 100, 200, 500, 1000, 2000), count=60):
     srv.warm([(s, s, s) for s in range(24, 161, 8)], per_shape=3)
     # one untimed burst at the highest rate first: every slot stream and
     # resident solver has run before any timed stream
-    burst = make_requests(max(rates), 4 * count, seed=99)
+    burst = make_requests(max(rates), 4 * warm_count, seed=99)
     srv.run(burst, {r.rid: srv.host_input(r) for r in burst})
     out = {'slots': 8, 'hbm_budget_gb': 16, 'requests_per_rate': count}
     for lam in rates:
+        warm = make_requests(lam, warm_count, seed=10_000 + lam)
+        srv.run(warm, {r.rid: srv.host_input(r) for r in warm})
         reqs = make_requests(lam, count, seed=lam)
         inputs = {r.rid: srv.host_input(r) for r in reqs}
-        # one untimed pass of the same stream first: the first launch of
-        # each captured solver graph on each slot stream costs extra
-        srv.run(make_requests(lam, count, seed=lam), inputs)
         srv.run(reqs, inputs)
         st = latency_stats(reqs)
         st['poisson_vcycles_mean'] = float(np.mean(
@@ -781,6 +880,8 @@ def run_gpu(args):
     peak, peak_src = measured_peak()
     apply_t = float(np.mean(apply_s))
     achieved = ab / apply_t / 1e9
+    rst_t = float(np.mean(rst_s))
+    itp_t = float(np.mean(itp_s))
     line = {
         'metric': METRIC, 'value': value, 'unit': 'GB/s', 'n_gpus': world,
         'steps': args.steps, 'warmup': args.warmup,
@@ -790,23 +891,22 @@ def run_gpu(args):
         'config': {'workload': WORKLOAD, 'batch': NBANDS, 'grid': list(N),
                    'parallelism': f'replicas x{world}',
                    'l2': 'inputs 3.6 GB per array, larger than L2 (no flush)',
-                   'z_block_depth': {k: (v or 'auto') for k, v in depth.items()},
-                   'depth_picked_by': 'gpaw_b200.autotune (timed)'},
+                   'z_block_depth': {k: (v or 'auto') for k, v in depth.items()}},
         'roofline': {'bound': 'hbm', 'achieved': achieved, 'peak': peak,
                      'unit': 'GB/s', 'frac': achieved / peak,
                      'traffic': ncu_traffic(), 'kernel': 'fd apply c128',
                      'peak_source': peak_src},
-        'kernels_ms': {'apply': apply_t * 1e3,
-                       'restrict': float(np.mean(rst_s)) * 1e3,
-                       'interpolate': float(np.mean(itp_s)) * 1e3},
-        'kernels_gbs': {'apply': achieved,
-                        'restrict': rb / float(np.mean(rst_s)) / 1e9,
-                        'interpolate': ib / float(np.mean(itp_s)) / 1e9},
         'gpu_launches': 3 * args.steps,
         'clocks': clk.summary(),
         'e2e': e2e,
         'cpu_baseline': cpu_base,
     }
+    detail = {'c2': {'kernels_ms': {'apply': apply_t * 1e3,
+                                    'restrict': rst_t * 1e3,
+                                    'interpolate': itp_t * 1e3},
+                     'kernels_gbs': {'apply': achieved,
+                                     'restrict': rb / rst_t / 1e9,
+                                     'interpolate': ib / itp_t / 1e9}}}
     # FD Hamiltonian local part on the same batch: kin(psi) + v psi fused
     if (rank == 0 or world == 1) and not args.no_ham:
         from gpaw_b200 import FDHamiltonian
@@ -822,7 +922,7 @@ def run_gpu(args):
         torch.cuda.synchronize()
         ht = h0.elapsed_time(h1) / 1e3 / 5
         hb = ab + vt.numel() * 8
-        line['hamiltonian_c2'] = {
+        detail['c2']['hamiltonian'] = {
             'what': 'kin(psi) + v psi, 256 x 96^3 complex128, one kernel',
             'ms': ht * 1e3, 'gbs': hb / ht / 1e9,
             'vs_apply_alone': ht / apply_t}
@@ -832,22 +932,118 @@ def run_gpu(args):
     cpu_ok = not args.no_cpu and rank == 0 and world == 1
     single = world == 1
     if not args.no_poisson and single:
-        line['poisson'] = {'c1': poisson_c1(dev, cpu=cpu_ok),
-                           'c3': poisson_c3(dev)}
-    if not args.no_poisson and single:
-        line['weighted_fd'] = weighted_fd(dev, cpu=cpu_ok)
+        detail['c1'] = poisson_c1(dev, cpu=cpu_ok)
+        detail['c1']['apply'] = c1_apply(dev)
+        detail['c3'] = poisson_c3(dev)
+        detail['wfd'] = weighted_fd(dev, cpu=cpu_ok)
     if not args.no_batch and single:
-        line.setdefault('poisson', {})['c4_batch'] = poisson_c4(dev,
-                                                                cpu=cpu_ok)
-        line['preconditioner_c4'] = precond_c4(dev)
+        detail['c4'] = poisson_c4(dev, cpu=cpu_ok)
+        detail['pc'] = precond_c4(dev)
     if not args.no_serving and single:
         # in a fresh process: the host-driven loop's latencies should not
         # depend on what this process did before (measured: they do)
-        line['serving_c5'] = serving_subprocess()
+        detail['c5'] = serving_subprocess()
+    line['configs'] = summarize(detail, peak)
+    if args.detail and rank == 0:
+        with open(args.detail, 'w') as f:
+            json.dump({'line': line, 'detail': detail}, f, indent=1)
     if rank == 0:
-        print(json.dumps(line), flush=True)
+        print(json.dumps(line, separators=(',', ':')), flush=True)
     if world > 1:
         dist.destroy_process_group()
+
+
+def _g(x, digits=4):
+    """Round for the compact summary."""
+    if x is None:
+        return None
+    if isinstance(x, bool) or isinstance(x, int):
+        return x
+    return float(f'{x:.{digits}g}')
+
+
+def summarize(d, peak):
+    """A compact per-configuration summary (a few hundred bytes) of the
+    detailed results, so that the figure of every configuration fits the
+    end of the JSON line."""
+    out = {}
+    c2 = d.get('c2')
+    if c2:
+        k = c2['kernels_gbs']
+        out['c2'] = {'gbs': {n: _g(v) for n, v in k.items()},
+                     'frac': {n: _g(v / peak, 3) for n, v in k.items()}}
+        if 'hamiltonian' in c2:
+            out['c2']['ham_gbs'] = _g(c2['hamiltonian']['gbs'])
+    c1 = d.get('c1')
+    if c1:
+        a = c1['apply']
+        e = c1['eps_2e-10']
+        r = c1['rel_1e-10']
+        out['c1'] = {'apply_us': _g(a['us']), 'apply_gbs': _g(a['gbs']),
+                     'apply_frac': _g(a['frac'], 3),
+                     'apply_us_l2': _g(a['us_l2_resident']),
+                     'solve_ms': _g(e['ms_per_solve']), 'vc': e['vcycles'],
+                     'solves_s': _g(e['solves_per_s']),
+                     'rel1e-10_ms': _g(r['ms_per_solve']),
+                     'rel1e-10_vc': r['vcycles']}
+        cr = e.get('cpu_reference')
+        if cr:
+            out['c1']['cpu_ms'] = _g(cr['ms_per_solve'])
+            out['c1']['cpu_err'] = _g(cr['max_rel_err_gpu_vs_cpu'], 2)
+    c3 = d.get('c3')
+    if c3:
+        f = c3['fp64_reference_schedule']
+        m4, m6 = c3['mixed_4_levels'], c3['mixed_6_levels']
+        out['c3'] = {'fp64_ms': _g(f['ms_per_solve']), 'fp64_vc': f['vcycles'],
+                     'mixed4_ms': _g(m4['ms_per_solve']),
+                     'mixed4_vc': m4['vcycles'],
+                     'speedup4': _g(c3['speedup_mixed_4_over_fp64'], 3),
+                     'mixed6_ms': _g(m6['ms_per_solve']),
+                     'speedup6': _g(c3['speedup_mixed_6_over_fp64'], 3),
+                     'rel_res4': _g(m4['rel_residual'], 2),
+                     'diff4': _g(m4['max_rel_diff_vs_fp64'], 2)}
+    c4 = d.get('c4')
+    if c4:
+        out['c4'] = {'mixed_sps': _g(c4['mixed']['solves_per_s']),
+                     'fp64_sps': _g(c4['fp64']['solves_per_s']),
+                     'speedup': _g(c4['speedup_mixed_over_fp64'], 3),
+                     'setup_s': _g(c4['mixed']['setup_s'], 3)}
+        if 'cpu_reference' in c4:
+            out['c4']['cpu_sps'] = _g(c4['cpu_reference']['solves_per_s'], 3)
+    pc = d.get('pc')
+    if pc:
+        out['pc'] = {'ms': _g(pc['ms_per_call']),
+                     'bb_gbs': _g(pc['blackbox_gbs']),
+                     'seq_gbs': _g(pc['sequence_gbs']),
+                     'k_ms_gbs': [[k['kernel'].split(' ')[0], _g(k['ms'], 3),
+                                   _g(k['gbs'], 3)] for k in pc['kernels']]}
+    wfd = d.get('wfd')
+    if wfd:
+        out['wfd'] = {'apply_gbs': _g(wfd['apply']['gbs']),
+                      'jac_gbs': _g(wfd['jacobi_sweep']['gbs']),
+                      'diel_ms': _g(wfd['poisson_dielectric_64']['ms_per_solve'])}
+    c5 = d.get('c5')
+    if c5:
+        out['c5'] = {'n': c5['requests_per_rate'],
+                     'thr_p50_p99': {k.split('_')[1]: [
+                         _g(v['throughput_per_s']), _g(v['p50_ms'], 3),
+                         _g(v['p99_ms'], 3)]
+                         for k, v in c5.items() if k.startswith('lambda_')}}
+    return out
+
+
+def relaunch_with_ranks(args):
+    """`bench.py --gpus N` outside torchrun: start N ranks (one process per
+    GPU) under torch.distributed.run on this node and return its exit
+    status."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(('127.0.0.1', 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, '-m', 'torch.distributed.run', '--nnodes=1',
+           f'--nproc-per-node={args.gpus}', '--master-addr=127.0.0.1',
+           f'--master-port={port}', os.path.abspath(__file__)] + sys.argv[1:]
+    return subprocess.run(cmd, cwd=ROOT).returncode
 
 
 def main():
@@ -870,12 +1066,17 @@ def main():
     p.add_argument('--no-ham', action='store_true',
                    help='skip the fused Hamiltonian section')
     p.add_argument('--poisson-only', default=None,
-                   choices=['c1', 'c3', 'c4', 'pc', 'c5', 'wfd'],
+                   choices=['c1', 'c3', 'c4', 'pc', 'c5', 'wfd', 'c1a'],
                    help='run one Poisson configuration only (profiling)')
     p.add_argument('--batch', type=int, default=NBANDS,
                    help='wave functions per step (profiling runs only)')
+    p.add_argument('--detail', default=None,
+                   help='also write every measured figure to this JSON file')
     args = p.parse_args()
     set_batch(args.batch)
+    if (args.gpus > 1 and 'WORLD_SIZE' not in os.environ and
+            not args.poisson_only):
+        sys.exit(relaunch_with_ranks(args))
     if args.poisson_only:
         import torch
         dev = torch.device('cuda', 0)
@@ -884,7 +1085,7 @@ def main():
             r = f(dev, nsolve=max(1, args.steps))
         else:
             r = {'c4': poisson_c4, 'pc': precond_c4, 'c5': serving_c5,
-                 'wfd': weighted_fd}[args.poisson_only](dev)
+                 'wfd': weighted_fd, 'c1a': c1_apply}[args.poisson_only](dev)
         print(json.dumps(r), flush=True)
     elif args.impl == 'reference':
         run_reference(args)

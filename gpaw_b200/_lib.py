@@ -40,6 +40,9 @@ SIGNATURES = {
     'gb_operator_residual': (C.c_int, [_p, _p, _p, _p, C.c_int64, C.c_int,
                                        _dp, C.c_double, _p, _p]),
     'gb_operator_get_diagonal_element': (C.c_double, [_p]),
+    'gb_trace_begin': (C.c_int, [C.c_int]),
+    'gb_trace_end': (C.c_int, [C.c_int, C.POINTER(C.c_float),
+                               C.POINTER(C.c_char_p), C.POINTER(C.c_int)]),
     'gb_operator_reserve': (C.c_int, [_p, C.c_int64, C.c_int]),
     'gb_transformer_new': (C.c_int, [_i64p, _i64p, C.c_int, _i64p, _i64p,
                                      _i64p, _i64p, C.c_int, C.c_int,
@@ -120,6 +123,34 @@ def check(rc):
     if rc == GB_ENOCONV:
         raise PoissonConvergenceError(msg)
     raise RuntimeError(msg)
+
+
+class KernelTrace:
+    """Per-kernel device times of composite calls (gb_fd_precond), through
+    the library's kernel trace:
+
+        with KernelTrace() as tr:
+            precond(R, None, out=out)
+        tr.intervals   # [(label, ms), ...] in launch order
+    """
+
+    def __init__(self, capacity=4096):
+        self.capacity = int(capacity)
+        self.intervals = []
+
+    def __enter__(self):
+        check(load().gb_trace_begin(self.capacity))
+        return self
+
+    def __exit__(self, *exc):
+        n = self.capacity
+        ms = (C.c_float * n)()
+        labels = (C.c_char_p * n)()
+        count = C.c_int(0)
+        check(load().gb_trace_end(n, ms, labels, C.byref(count)))
+        self.intervals = [(labels[i].decode(), float(ms[i]))
+                          for i in range(min(count.value, n))]
+        return False
 
 
 def i64(a):

@@ -32,6 +32,61 @@ int gb::fail(int code, const char* fmt, ...) {
 extern "C" int gb_version(void) { return 100; }
 extern "C" const char* gb_last_error(void) { return g_err.c_str(); }
 
+// ----------------------------------------------------------- kernel trace
+// Profiling aid for composite entry points: while a trace is open, each
+// kernel of gb_fd_precond is preceded by a CUDA event on the call's stream,
+// and one more event follows the last kernel.
+namespace {
+struct Trace {
+    std::mutex mu;
+    bool on = false;
+    std::vector<cudaEvent_t> ev;
+    std::vector<const char*> label;
+    int used = 0;
+};
+Trace g_trace;
+}  // namespace
+
+static void trace_mark(const char* label, cudaStream_t st) {
+    if (!g_trace.on) return;
+    std::lock_guard<std::mutex> lock(g_trace.mu);
+    if (!g_trace.on || g_trace.used >= (int)g_trace.ev.size()) return;
+    if (cudaEventRecord(g_trace.ev[g_trace.used], st) != cudaSuccess) return;
+    g_trace.label[g_trace.used++] = label;
+}
+
+extern "C" int gb_trace_begin(int capacity) {
+    if (capacity < 2 || capacity > 1 << 16) return fail(GB_EINVAL, "trace: capacity 2..65536");
+    std::lock_guard<std::mutex> lock(g_trace.mu);
+    for (cudaEvent_t e : g_trace.ev) cudaEventDestroy(e);
+    g_trace.ev.assign(capacity, nullptr);
+    g_trace.label.assign(capacity, nullptr);
+    for (int i = 0; i < capacity; i++)
+        GB_CUDA_TRY(cudaEventCreate(&g_trace.ev[i]));
+    g_trace.used = 0;
+    g_trace.on = true;
+    return 0;
+}
+
+extern "C" int gb_trace_end(int max, float* ms, const char** labels, int* count) {
+    std::lock_guard<std::mutex> lock(g_trace.mu);
+    g_trace.on = false;
+    const int n = std::max(0, g_trace.used - 1);
+    if (count) *count = n;
+    if (g_trace.used > 0) GB_CUDA_TRY(cudaEventSynchronize(g_trace.ev[g_trace.used - 1]));
+    for (int i = 0; i < n && i < max; i++) {
+        float t = 0.f;
+        GB_CUDA_TRY(cudaEventElapsedTime(&t, g_trace.ev[i], g_trace.ev[i + 1]));
+        if (ms) ms[i] = t;
+        if (labels) labels[i] = g_trace.label[i];
+    }
+    for (cudaEvent_t e : g_trace.ev) cudaEventDestroy(e);
+    g_trace.ev.clear();
+    g_trace.label.clear();
+    g_trace.used = 0;
+    return 0;
+}
+
 extern "C" int gb_operator_new(const double* coefs, const int64_t* offsets, int ncoefs,
                                const int64_t size[3], int range, const int64_t neighbors[6],
                                int real, int cfd, gb_operator** out) {
@@ -199,12 +254,12 @@ extern "C" int gb_operator_residual(gb_operator* op, const void* phi, const void
     return 0;
 }
 
-static int relax_impl(gb_operator* op, int method, double* f, const double* s, int nrelax,
-                      double w, cudaStream_t st) {
+// The relaxation itself, with its scratch grid X (op->ng() doubles) given by
+// the caller: the operator's own buffer (gb_operator_relax) or the fixed
+// device array of gb_operator_relax_noalloc.
+static int relax_with_scratch(gb_operator* op, int method, double* f, const double* s,
+                              int nrelax, double w, double* X, cudaStream_t st) {
     const size_t bytes = (size_t)op->ng() * sizeof(double);
-    if (nrelax <= 0) return 0;
-    if (int e = op->scratch.ensure(bytes)) return e;
-    double* X = (double*)op->scratch.ptr;
     if (method == 1) {
         // Gauss-Seidel by wavefronts; wrapped reads see the sweep's start.
         const int r = op->st.range;
@@ -241,6 +296,13 @@ static int relax_impl(gb_operator* op, int method, double* f, const double* s, i
     }
     GB_LAUNCH_CHECK();
     return 0;
+}
+
+static int relax_impl(gb_operator* op, int method, double* f, const double* s, int nrelax,
+                      double w, cudaStream_t st) {
+    if (nrelax <= 0) return 0;
+    if (int e = op->scratch.ensure((size_t)op->ng() * sizeof(double))) return e;
+    return relax_with_scratch(op, method, f, s, nrelax, w, (double*)op->scratch.ptr, st);
 }
 
 extern "C" int gb_operator_relax(gb_operator* op, int method, double* f, const double* s,
@@ -373,28 +435,37 @@ extern "C" int gb_fd_precond(gb_transformer* rest0, gb_transformer* rest1, gb_tr
     };
     int rc;
     // r1 = restrict(-R); d1 = 4 s r1
+    trace_mark("restrict0 r1,d1 = R(-R), 4s r1", st);
     if (nresiduals)
         rc = transform_impl(rest0, nresiduals, r1, d1, nin, dtype, P, 0, 0, s4, st);
     else
         rc = transform_impl(rest0, residuals, r1, d1, nin, dtype, P, 1, 0, s4, st);
     if (rc) return rc;
     // q1 = K1 d1 - r1; r2 = restrict(q1); d2 = 16 s r2
+    trace_mark("kin1 q1 = K1 d1 - r1", st);
     if ((rc = op_sweep(kin1, EPI_RESID, d1, q1, r1, n, dtype, P, 0, 0, 0, nullptr, st))) return rc;
     GB_LAUNCH_CHECK();
+    trace_mark("restrict1 r2,d2 = R(q1), 16s r2", st);
     if ((rc = transform_impl(rest1, q1, r2, d2, nin, dtype, P, 0, 0, s16, st))) return rc;
     // d2' = d2 - 16 s (K2 d2 - r2)   (into q2)
+    trace_mark("kin2 q2 = d2 - 16s(K2 d2 - r2)", st);
     if ((rc = step_launch(kin2, d2, r2, q2, s16, 0))) return rc;
     GB_LAUNCH_CHECK();
     // d1 -= interpolate(d2')
+    trace_mark("interp2 d1 -= I(q2)", st);
     if ((rc = transform_impl(intp2, q2, d1, nullptr, nin, dtype, P, 0, 1, 0.0, st))) return rc;
     // d1' = d1 - 4 s (K1 d1 - r1)   (into q1)
+    trace_mark("kin1 q1 = d1 - 4s(K1 d1 - r1)", st);
     if ((rc = step_launch(kin1, d1, r1, q1, s4, 0))) return rc;
     GB_LAUNCH_CHECK();
     // q0 = interpolate(-d1')
+    trace_mark("interp1 q0 = I(-q1)", st);
     if ((rc = transform_impl(intp1, q1, q0, nullptr, nin, dtype, P, 1, 0, 0.0, st))) return rc;
     // d0 = -(q0 - s (K0 q0 - R))
+    trace_mark("kin0 d0 = -(q0 - s(K0 q0 - R))", st);
     if ((rc = step_launch(kin0, q0, residuals, d0, step, 1))) return rc;
     GB_LAUNCH_CHECK();
+    trace_mark("end", st);
     return 0;
 }
 
@@ -1094,26 +1165,67 @@ static __device__ __align__(256) double g_relax_scratch[GB_NOALLOC_MAX_POINTS];
 
 namespace {
 std::mutex g_noalloc_mu;
-void* g_noalloc_ptr[256] = {};   // device address of g_relax_scratch, per device
+// Per device: the address of g_relax_scratch and the CUDA context it was
+// looked up in.  After cudaDeviceReset (or any other re-creation of the
+// primary context) the module is loaded again and the array may move, so a
+// cached address is used only while the current context is the one it came
+// from.
+struct NoallocSlot {
+    void* ptr = nullptr;
+    void* ctx = nullptr;
+};
+NoallocSlot g_noalloc[256];
+
+// cuCtxGetCurrent through the runtime's driver entry point table, so that
+// the library needs no link against libcuda.
+typedef int (*CtxGetCurrentFn)(void**);
+CtxGetCurrentFn ctx_get_current() {
+    static CtxGetCurrentFn fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return (CtxGetCurrentFn) nullptr;
+        return (CtxGetCurrentFn)f;
+    }();
+    return fn;
+}
 }  // namespace
 
 // Host code must not use g_relax_scratch's name as a device address (it is a
-// host-side stand-in); the first call on each device looks the address up
-// with that device current and caches it.
-static int noalloc_scratch(double** out) {
+// host-side stand-in); the array's address is looked up with the device
+// current, on the first call on that device and again whenever the current
+// context has changed since.  The look-up may load the module, which a
+// stream capture does not allow: if `st` is capturing and no address is
+// cached for this context, the call fails with GB_EINVAL and says so.
+static int noalloc_scratch(double** out, cudaStream_t st) {
     int dev = 0;
     GB_CUDA_TRY(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 256) return fail(GB_EINVAL, "relax_noalloc: device index %d", dev);
+    void* ctx = nullptr;
+    if (CtxGetCurrentFn f = ctx_get_current()) {
+        if (f(&ctx) != 0) ctx = nullptr;
+    }
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
+    NoallocSlot& slot = g_noalloc[dev];
+    if (!slot.ptr || slot.ctx != ctx) {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        GB_CUDA_TRY(cudaStreamIsCapturing(st, &cs));
+        if (cs != cudaStreamCaptureStatusNone)
+            return fail(GB_EINVAL,
+                        "relax_noalloc: the first call on a device (or after its context was "
+                        "re-created) looks up the scratch array's address and must not run "
+                        "inside a stream capture; call it once before capturing");
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_relax_scratch);
         if (e != cudaSuccess || !p)
             return fail(GB_ECUDA, "relax_noalloc: cudaGetSymbolAddress: %s",
                         cudaGetErrorString(e));
-        g_noalloc_ptr[dev] = p;
+        slot.ptr = p;
+        slot.ctx = ctx;
     }
-    *out = (double*)g_noalloc_ptr[dev];
+    *out = (double*)slot.ptr;
     return 0;
 }
 
@@ -1128,42 +1240,8 @@ extern "C" int gb_operator_relax_noalloc(gb_operator* op, int method, double* f,
                     "supports; use gb_operator_relax",
                     op->ng(), (int)GB_NOALLOC_MAX_POINTS);
     if (nrelax <= 0) return 0;
-    double* X = nullptr;
-    if (int rc = noalloc_scratch(&X)) return rc;
     cudaStream_t st = (cudaStream_t)stream;
-    const size_t bytes = (size_t)op->ng() * sizeof(double);
-    if (method == 1) {
-        const int r = op->st.range;
-        int wa = 1, wb = 1;
-        if (!op->st.cfd) {
-            wb = 2 * r + 1;
-            wa = (wb + 1) * r + 1;
-        }
-        const GridBC& g = op->g;
-        const int nt = wa * (g.n[0] - 1) + wb * (g.n[1] - 1) + g.n[2];
-        const bool periodic = g.periodic[0] || g.periodic[1] || g.periodic[2];
-        const double inv0 = 1.0 / op->st.coef[0];
-        for (int it = 0; it < nrelax; it++) {
-            if (periodic) GB_CUDA_TRY(cudaMemcpyAsync(X, f, bytes, cudaMemcpyDeviceToDevice, st));
-            for (int t = 0; t < nt; t++)
-                launch_gs_wave(f, periodic ? X : f, s, g, op->st, t, wa, wb, inv0, st);
-            GB_LAUNCH_CHECK();
-        }
-        return 0;
-    }
-    const double* src = f;
-    if (nrelax % 2 == 1) {
-        GB_CUDA_TRY(cudaMemcpyAsync(X, f, bytes, cudaMemcpyDeviceToDevice, st));
-        src = X;
-    }
-    Phases P0;
-    memset(&P0, 0, sizeof P0);
-    for (int it = 0; it < nrelax; it++) {
-        double* dst = (src == f) ? X : f;
-        if (int rc = op_sweep(op, EPI_JACOBI, src, dst, s, 1, GB_F64, P0, w, 0, 0, nullptr, st))
-            return rc;
-        src = dst;
-    }
-    GB_LAUNCH_CHECK();
-    return 0;
+    double* X = nullptr;
+    if (int rc = noalloc_scratch(&X, st)) return rc;
+    return relax_with_scratch(op, method, f, s, nrelax, w, X, st);
 }

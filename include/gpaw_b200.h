@@ -122,12 +122,25 @@ GB_API int gb_operator_relax(gb_operator* op, int method, double* f, const doubl
  * device array of GB_NOALLOC_MAX_POINTS doubles (16 MiB, held by every GPU
  * that loads the library until exit); grids with more points are rejected
  * with GB_EINVAL.  The first call on a device looks the array's address up
- * (cudaGetSymbolAddress), so make that first call before any stream capture.
- * All calls share the array: calls that overlap on the GPU race.  Same
- * results as gb_operator_relax. */
+ * (cudaGetSymbolAddress), and so does the first call after the device's
+ * context was re-created (cudaDeviceReset); make that call before any stream
+ * capture: made inside one, it fails with GB_EINVAL.  All calls share the
+ * array: calls that overlap on the GPU race.  Same results as
+ * gb_operator_relax. */
 #define GB_NOALLOC_MAX_POINTS (2 * 1024 * 1024)
 GB_API int gb_operator_relax_noalloc(gb_operator* op, int method, double* f, const double* s,
                                      int nrelax, double w, void* stream);
+
+/* Kernel timeline of composite calls; a profiling aid with no counterpart
+ * in the reference.  Between gb_trace_begin(capacity) and gb_trace_end,
+ * gb_fd_precond records a CUDA event on its stream before each of its
+ * kernels and one after the last (at most `capacity` events in all).
+ * gb_trace_end waits for the last event and writes, for up to `max`
+ * intervals, the milliseconds between consecutive events and the label of
+ * the kernel each interval starts with; *count receives the number of
+ * intervals.  Not for use inside a stream capture. */
+GB_API int gb_trace_begin(int capacity);
+GB_API int gb_trace_end(int max, float* ms, const char** labels, int* count);
 
 /* Residual r = L(phi) - rho for a batch (gpaw/poisson.py:517-518 done in
  * one pass).  r may be NULL.  If norm2 is not NULL it receives, per grid,
