@@ -870,11 +870,16 @@ class DistributedPreconditioner:
 
     def __init__(self, pre, rank, size, make_op, make_tr, group=None,
                  min_planes=2, dims=None):
-        kins = [pre.kin0, pre.kin1, pre.kin2]
+        # the kinetic operator of each level: the product's Preconditioner
+        # keeps them in its level list, the oracle's as kin0..kin2
+        if hasattr(pre, 'levels'):
+            kins = [lv.kin for lv in pre.levels]
+        else:
+            kins = [pre.kin0, pre.kin1, pre.kin2]
         gds = [k.gd for k in kins]
         self.step = float(pre.step)
         self.group = group
-        dtype = getattr(pre.kin1, 'dtype', float)
+        dtype = getattr(kins[1], 'dtype', float)
         ranges = [int(np.abs(np.asarray(k.offset_pc, int)).max())
                   for k in kins]
         self.doms = _level_domains(gds, ranges, rank, size, dims,
@@ -884,13 +889,14 @@ class DistributedPreconditioner:
                     for k, gd, dom in zip(kins, gds, self.doms)]
         d0, d1, d2 = self.doms
 
-        def tr(obj, gi, go, di, do):
-            return DistributedTransformer(gi, go, obj.nn, dtype, di, do,
+        # the preconditioner's transfers are all of order 2 (nn = 1)
+        def tr(gi, go, di, do):
+            return DistributedTransformer(gi, go, 1, dtype, di, do,
                                           make_tr, group)
-        self.rest0 = tr(pre.restrictor_object0, gds[0], gds[1], d0, d1)
-        self.rest1 = tr(pre.restrictor_object1, gds[1], gds[2], d1, d2)
-        self.intp2 = tr(pre.interpolator_object2, gds[2], gds[1], d2, d1)
-        self.intp1 = tr(pre.interpolator_object1, gds[1], gds[0], d1, d0)
+        self.rest0 = tr(gds[0], gds[1], d0, d1)
+        self.rest1 = tr(gds[1], gds[2], d1, d2)
+        self.intp2 = tr(gds[2], gds[1], d2, d1)
+        self.intp1 = tr(gds[1], gds[0], d1, d0)
 
     def __call__(self, residuals, phases=None, out=None):
         """Collective: the preconditioned residuals of this rank's slab

@@ -1,17 +1,34 @@
-"""Poisson solver with extra vacuum (drop-in for gpaw/poisson_extravacuum.py).
+"""Poisson solver with extra vacuum around a non-periodic system.
 
-The potential of a non-periodic system is solved on a larger grid
-(``gpts`` points per axis) around the original one, so that the zero
-boundary condition sits further from the charge
-(gpaw/poisson_extravacuum.py:13-232).  With ``coarses`` > 0 the large grid
-is ``coarses`` times coarser than the original: the density is restricted,
-embedded in the large coarse grid and solved there; the coarse potential
-is refined back on an auxiliary grid (the original plus a buffer for the
-stencils), its Laplacian gives the density that matches it, and the
-original grid is then solved for the difference, with the refined
-potential as the boundary correction.  Restriction, interpolation, the
-Laplacian and the solves are the sm_100a kernels; embedding a grid in a
-larger one is a device copy.
+Drop-in for ``gpaw.poisson_extravacuum.ExtraVacuumPoissonSolver``
+(gpaw/poisson_extravacuum.py:13-232): same constructor, ``solve`` return
+values and results.
+
+Why: with zero boundaries the potential is forced to vanish on the cell
+faces, which is wrong when the charge sits close to them.  Solving on a
+larger grid (``gpts`` points per axis, the original grid centred inside)
+moves that error away.  To keep the large solve cheap it can run
+``coarses`` times coarser; the fine potential is then recovered in a
+second, small solve on the original grid:
+
+1. restrict the density ``coarses`` times, embed it in the large coarse
+   grid (zeros around it) and solve there (warm-started from the previous
+   call's large potential);
+2. interpolate the large potential back to the fine spacing on a padded
+   copy of the original grid (the "auxiliary" grid), apply the fine
+   Laplacian to it, and cut both out over the original grid: a potential
+   and the density it exactly belongs to under the fine stencil;
+3. solve the original grid for the density minus that density, starting
+   from the potential minus that potential, and add the potential back.
+   The boundary values of step 3 come from the large solve; inside, the
+   fine solve corrects what the coarse grid could not resolve.
+
+The padding of the auxiliary grid is derived here from the stencils' reach
+(``_exact_margin``): it is just wide enough that every value that reaches
+the original grid is computed from the large solution and never from the
+auxiliary grid's own zero boundary, so the result does not depend on it.
+Restriction, interpolation, the Laplacian and the solves are the sm_100a
+kernels; embedding and cutting are device copies.
 """
 from __future__ import annotations
 
@@ -24,10 +41,11 @@ from .grid_descriptor import GridDescriptor
 from .transformers import Transformer
 
 
-def _create(ps):
-    if ps is None or not isinstance(ps, dict):
-        return ps
-    kw = dict(ps)
+def _solver(spec):
+    """A Poisson solver object from an object or a dict description."""
+    if spec is None or not isinstance(spec, dict):
+        return spec
+    kw = dict(spec)
     name = kw.pop('name', 'fd')
     if name != 'fd':
         raise ValueError(f'Unknown poisson solver: {name}')
@@ -35,30 +53,45 @@ def _create(ps):
     return FDPoissonSolver(**kw)
 
 
-def extended_grid_descriptor(gd, N_c):
-    """gpaw/utilities/extend_grid.py:8-44 for a target size ``N_c``: the
-    same spacing, (N_c - N) // 2 extra points on each side."""
-    N_c = np.array(N_c, dtype=int)
-    extend_N_cd = np.tile((N_c - gd.N_c) // 2, (2, 1)).T
-    cell_cv = gd.h_cv * N_c
-    egd = GridDescriptor(N_c, cell_cv, gd.pbc_c, device=gd.device)
-    egd.extend_N_cd = extend_N_cd
-    return egd
+class _Embedding:
+    """A grid centred inside a larger grid with the same spacing and
+    boundary conditions: (N_big - N) // 2 extra points below each axis
+    (gpaw/utilities/extend_grid.py's layout)."""
+
+    def __init__(self, inner, N_big):
+        N_big = np.asarray(N_big, dtype=int)
+        self.inner = inner
+        self.outer = GridDescriptor(N_big, inner.h_cv * N_big[:, None],
+                                    inner.pbc_c, device=inner.device)
+        self.lo = (N_big - inner.N_c) // 2
+
+    def window(self, big):
+        """The view of a large-grid array over the inner grid."""
+        o, n = self.lo, self.inner.n_c
+        return big[o[0]:o[0] + n[0], o[1]:o[1] + n[1], o[2]:o[2] + n[2]]
+
+    def embed(self, small):
+        """A large-grid array that is `small` inside and zero outside."""
+        big = self.outer.zeros()
+        self.window(big).copy_(small)
+        return big
 
 
-def extend_array(gd, egd, a_g, aext_g):
-    """Copy a_g into its place in the larger grid (gpaw/utilities/
-    extend_grid.py:47-50, one domain)."""
-    o = egd.extend_N_cd[:, 0]
-    n = gd.n_c
-    aext_g[o[0]:o[0] + n[0], o[1]:o[1] + n[1], o[2]:o[2] + n[2]] = a_g
+def _exact_margin(nn_refine, nn_laplace, coarses):
+    """Padding (fine points per side) of the auxiliary grid.
 
-
-def deextend_array(gd, egd, a_g, aext_g):
-    """Copy the part of aext_g over the smaller grid into a_g (:53-56)."""
-    o = egd.extend_N_cd[:, 0]
-    n = gd.n_c
-    a_g[:] = aext_g[o[0]:o[0] + n[0], o[1]:o[1] + n[1], o[2]:o[2] + n[2]]
+    The Laplacian of order nn_laplace reads nn_laplace points beyond the
+    original grid, so the refined potential must be exact that far out.
+    One order-2n interpolation step computes a fine point from coarse
+    points at most 2n - 1 fine spacings away, so a margin of m fine points
+    needs ceil((m + 2n - 1) / 2) coarse points.  Working back through the
+    coarsenings gives the margin on the coarsest grid; times 2^coarses it
+    is a whole number of coarse points, so the auxiliary grid's points
+    coincide with the large coarse grid's."""
+    m = nn_laplace
+    for _ in range(coarses):
+        m = -(-(m + 2 * nn_refine - 1) // 2)
+    return m * 2**coarses
 
 
 class ExtraVacuumPoissonSolver:
@@ -66,88 +99,63 @@ class ExtraVacuumPoissonSolver:
                  coarses=0, nn_coarse=3, nn_refine=3, nn_laplace=3,
                  use_aux_grid=True, xp=None):
         self.N_large_fine_c = np.array(gpts, dtype=int)
-        self.Ncoar = coarses
+        self.Ncoar = int(coarses)
         self.use_coarse = self.Ncoar > 0
-        self.ps_large_coar = _create(poissonsolver_large)
-        if self.use_coarse:
-            self.ps_small_fine = _create(poissonsolver_small)
-        else:
+        if not self.use_coarse:
             assert poissonsolver_small is None
+        self.ps_large_coar = _solver(poissonsolver_large)
+        self.ps_small_fine = (_solver(poissonsolver_small)
+                              if self.use_coarse else None)
         self.nn_coarse = nn_coarse
         self.nn_refine = nn_refine
         self.nn_laplace = nn_laplace
         self.use_aux_grid = use_aux_grid
-        self._initialized = False
+        self._phi_large = None
 
     def set_grid_descriptor(self, gd):
-        """:62-144: coarsening chain on the original grid, the large coarse
-        grid, and (with coarses) the auxiliary grid with its Laplacian and
-        refining chain."""
         if bool(gd.pbc_c.any()):
             raise NotImplementedError('Only non-periodic boundary '
                                       'conditions are tested')
-        self.gd_small_fine = gd
         assert np.all(gd.N_c <= self.N_large_fine_c), \
             'extended grid has to be larger than the original one'
-        if self.use_coarse:
-            self.coarser_i = []
-            N_c = self.N_large_fine_c.copy()
-            for _ in range(self.Ncoar):
-                gd2 = gd.coarsen()
-                self.coarser_i.append(Transformer(gd, gd2, self.nn_coarse))
-                N_c //= 2
-                gd = gd2
-            self.gd_small_coar = gd
-        else:
-            self.gd_small_coar = self.gd_small_fine
-            N_c = self.N_large_fine_c
-        self.gd_large_coar = extended_grid_descriptor(self.gd_small_coar, N_c)
+        self.gd_small_fine = gd
+        k = self.Ncoar
+        # restriction chain of the original grid: gds[0] = gd, gds[k] the
+        # spacing of the large solve
+        gds = [gd]
+        for _ in range(k):
+            gds.append(gds[-1].coarsen())
+        self.down = [Transformer(gds[i], gds[i + 1], self.nn_coarse)
+                     for i in range(k)]
+        self.gd_small_coar = gds[-1]
+        self.large = _Embedding(gds[-1], self.N_large_fine_c // 2**k)
+        self.gd_large_coar = self.large.outer
         self.ps_large_coar.set_grid_descriptor(self.gd_large_coar)
-        self._initialized = False
+        self._phi_large = None
         if not self.use_coarse:
             return
-        self.ps_small_fine.set_grid_descriptor(self.gd_small_fine)
-        if self.use_aux_grid:
-            buf = self.nn_refine
-            for _ in range(self.Ncoar):
-                buf = 2 * buf + self.nn_refine
-            buf += self.nn_laplace
-            div = 2**self.Ncoar
-            if buf % div != 0:
-                buf += div - buf % div
-            N_c = self.gd_small_fine.N_c + 2 * buf
-            if np.any(N_c > self.N_large_fine_c):
-                self.use_aux_grid = False
-                N_c = self.N_large_fine_c
-            self.gd_aux_fine = extended_grid_descriptor(self.gd_small_fine,
-                                                        N_c)
-        else:
-            self.gd_aux_fine = extended_grid_descriptor(
-                self.gd_small_fine, self.N_large_fine_c)
+        self.ps_small_fine.set_grid_descriptor(gd)
+        # the auxiliary grid: the original grid padded by the stencils'
+        # reach, or the whole large grid at fine spacing when the padding
+        # would not fit inside it
+        N_aux = gd.N_c + 2 * _exact_margin(self.nn_refine, self.nn_laplace,
+                                           k)
+        if not self.use_aux_grid or np.any(N_aux > self.N_large_fine_c):
+            self.use_aux_grid = False
+            N_aux = self.N_large_fine_c
+        self.aux = _Embedding(gd, N_aux)
+        self.gd_aux_fine = self.aux.outer
         self.laplace_aux_fine = Laplace(self.gd_aux_fine, -0.25 / pi,
                                         self.nn_laplace)
-        self.refiner_i = []
-        gd = self.gd_aux_fine
-        for _ in range(self.Ncoar):
-            gd2 = gd.coarsen()
-            self.refiner_i.append(Transformer(gd2, gd, self.nn_refine))
-            gd = gd2
-        self.refiner_i = self.refiner_i[::-1]
-        self.gd_aux_coar = gd
-        if self.use_aux_grid:
-            self.gd_large_coar_from_aux = extended_grid_descriptor(
-                self.gd_aux_coar, self.gd_large_coar.N_c)
-            assert np.all(self.gd_large_coar.N_c ==
-                          self.gd_large_coar_from_aux.N_c)
-            assert np.allclose(self.gd_large_coar.h_cv,
-                               self.gd_large_coar_from_aux.h_cv,
-                               rtol=0, atol=1e-12)
-
-    def _init(self):
-        if self._initialized:
-            return
-        self.phi_large_coar_g = self.gd_large_coar.zeros()
-        self._initialized = True
+        aux = [self.gd_aux_fine]
+        for _ in range(k):
+            aux.append(aux[-1].coarsen())
+        # interpolation chain, coarsest first
+        self.up = [Transformer(aux[i + 1], aux[i], self.nn_refine)
+                   for i in reversed(range(k))]
+        self.gd_aux_coar = aux[-1]
+        # where the coarse auxiliary grid sits in the large coarse grid
+        self.aux_in_large = _Embedding(aux[-1], self.gd_large_coar.N_c)
 
     def get_description(self):
         lines = ['ExtraVacuumPoissonSolver',
@@ -159,52 +167,38 @@ class ExtraVacuumPoissonSolver:
                       '    ' + self.ps_small_fine.get_description()]
         return '\n'.join(lines)
 
-    def solve(self, phi, rho, **kwargs):
-        """:159-231: returns the large solve's V-cycle count, or the pair
-        (large, small) with coarses."""
-        self._init()
-        phi_small_fine_g = phi
-        rho_small_fine_g = rho.clone()
-        if self.use_coarse:
-            tmp_g = rho_small_fine_g
-            for coarser in self.coarser_i:
-                tmp_g = coarser.apply(tmp_g)
-            rho_small_coar_g = tmp_g
-        else:
-            rho_small_coar_g = rho_small_fine_g
-        rho_large_coar_g = self.gd_large_coar.zeros()
-        extend_array(self.gd_small_coar, self.gd_large_coar,
-                     rho_small_coar_g, rho_large_coar_g)
-        niter_large = self.ps_large_coar.solve(self.phi_large_coar_g,
-                                               rho_large_coar_g, **kwargs)
-        if not self.use_coarse:
-            deextend_array(self.gd_small_fine, self.gd_large_coar,
-                           phi_small_fine_g, self.phi_large_coar_g)
-            return niter_large
+    def _boundary_correction(self):
+        """Potential and matching density over the original grid from the
+        large solution (steps 2 of the module docstring)."""
         if self.use_aux_grid:
-            phi_aux_coar_g = self.gd_aux_coar.empty()
-            deextend_array(self.gd_aux_coar, self.gd_large_coar_from_aux,
-                           phi_aux_coar_g, self.phi_large_coar_g)
+            phi = self.aux_in_large.window(self._phi_large).contiguous()
         else:
-            phi_aux_coar_g = self.phi_large_coar_g
-        tmp_g = phi_aux_coar_g
-        for refiner in self.refiner_i:
-            tmp_g = refiner.apply(tmp_g)
-        phi_aux_fine_g = tmp_g
-        rho_aux_fine_g = self.gd_aux_fine.empty()
-        self.laplace_aux_fine.apply(phi_aux_fine_g, rho_aux_fine_g)
-        cor_phi_small_fine_g = self.gd_small_fine.empty()
-        deextend_array(self.gd_small_fine, self.gd_aux_fine,
-                       cor_phi_small_fine_g, phi_aux_fine_g)
-        cor_rho_small_fine_g = self.gd_small_fine.empty()
-        deextend_array(self.gd_small_fine, self.gd_aux_fine,
-                       cor_rho_small_fine_g, rho_aux_fine_g)
-        rho_small_fine_g -= cor_rho_small_fine_g
-        phi_small_fine_g -= cor_phi_small_fine_g
-        niter_small = self.ps_small_fine.solve(phi_small_fine_g,
-                                               rho_small_fine_g, **kwargs)
-        phi_small_fine_g += cor_phi_small_fine_g
-        return (niter_large, niter_small)
+            phi = self._phi_large
+        for t in self.up:
+            phi = t.apply(phi)
+        rho = self.gd_aux_fine.empty()
+        self.laplace_aux_fine.apply(phi, rho)
+        return self.aux.window(phi), self.aux.window(rho)
+
+    def solve(self, phi, rho, **kwargs):
+        """Returns the large solve's V-cycle count, or the pair (large,
+        small) when the large grid is coarser."""
+        if self._phi_large is None:
+            # kept between calls: each large solve starts from the last
+            self._phi_large = self.gd_large_coar.zeros()
+        rho_c = rho
+        for t in self.down:
+            rho_c = t.apply(rho_c)
+        n_large = self.ps_large_coar.solve(self._phi_large,
+                                           self.large.embed(rho_c), **kwargs)
+        if not self.use_coarse:
+            phi.copy_(self.large.window(self._phi_large))
+            return n_large
+        phi_b, rho_b = self._boundary_correction()
+        phi -= phi_b
+        n_small = self.ps_small_fine.solve(phi, rho - rho_b, **kwargs)
+        phi += phi_b
+        return (n_large, n_small)
 
     def todict(self):
         d = {'name': 'ExtraVacuumPoissonSolver',

@@ -149,8 +149,8 @@ def test_cgpaw_objects_build_without_gpu():
 
 
 def test_dipole_moment_matches_oracle():
-    """The dipole moment of the product's wrapper (numpy path) equals the
-    restatement of the reference's grid method."""
+    """The dipole moment of the product's wrapper (numpy path) agrees with
+    the restatement of the reference's grid method."""
     import numpy as np
     from gpaw_b200 import GridDescriptor
     from gpaw_b200.dipole import calculate_dipole_moment
@@ -160,8 +160,10 @@ def test_dipole_moment_matches_oracle():
         gd = GridDescriptor((12, 10, 14), (3.0, 2.5, 3.5), pbc, device='cpu')
         go = L.GridDescriptor((12, 10, 14), (3.0, 2.5, 3.5), pbc)
         rho = rng.standard_normal(tuple(go.n_c))
-        assert np.array_equal(calculate_dipole_moment(gd, rho),
-                              L.calculate_dipole_moment(go, rho))
+        got = calculate_dipole_moment(gd, rho)
+        want = L.calculate_dipole_moment(go, rho)
+        # the projections are summed in another order than the oracle's
+        assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max()
 
 
 def test_oracle_interpolate_density_conserves_charge():

@@ -379,3 +379,42 @@ def test_solvation_poisson_reference_known_answers():
             rho += rho_t / (norm * q)
             want += phi_t / (norm * q)
         assert np.abs(solve(eps, rho) - want).max() < 1e-3, qs
+
+
+def test_extravacuum_margin_is_exact_and_minimal():
+    """The extra-vacuum solver's auxiliary grid is padded by the stencils'
+    reach (gpaw_b200.poisson_extravacuum._exact_margin) rather than by the
+    reference's wider buffer.  On the oracle: with that padding the
+    potential is bit-identical to the reference's layout, and one coarse
+    point less changes it (so the margin is the smallest exact one)."""
+    from math import pi
+    from gpaw_b200.poisson_extravacuum import _exact_margin
+    N, gpts, k = (16, 16, 16), (48, 48, 48), 1
+    cell = (4.0, 4.0, 4.0)
+    gd = L.GridDescriptor(N, cell, 0)
+    x = gd.get_grid_point_coordinates() - 2.0
+    rho = np.exp(-((x[0] - 0.5)**2 + x[1]**2 + x[2]**2)) - \
+        np.exp(-((x[0] + 0.5)**2 + x[1]**2 + x[2]**2))
+
+    def solve(buf):
+        ev = L.ExtraVacuumPoissonSolver(gpts, L.FDPoissonSolver(eps=1e-16),
+                                        L.FDPoissonSolver(eps=1e-16), k)
+        ev.set_grid_descriptor(gd)
+        if buf is not None:
+            # rebuild the auxiliary grid of the restatement with `buf`
+            ev.use_aux = True
+            ev.gd_af = L.extended_gd(ev.gd_sf, ev.gd_sf.N_c + 2 * buf)
+            ev.lap = L.Laplace(ev.gd_af, -0.25 / pi, 3)
+            ev.refiner = [L.Transformer(ev.gd_af.coarsen(), ev.gd_af, 3)]
+            ev.gd_ac = ev.gd_af.coarsen()
+            ev.gd_lc_aux = L.extended_gd(ev.gd_ac, ev.gd_lc.N_c)
+        phi = gd.zeros()
+        n = ev.solve(phi, rho)
+        return n, phi
+
+    m = _exact_margin(3, 3, k)
+    n_ref, ref = solve(None)
+    n_m, got = solve(m)
+    _, short = solve(m - 2**k)
+    assert n_m == n_ref and np.array_equal(got, ref)
+    assert not np.array_equal(short, ref)
