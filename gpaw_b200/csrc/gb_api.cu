@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "gb_objects.cuh"
+#include "gb_tma.cuh"
 
 using namespace gb;
 
@@ -31,6 +32,61 @@ int gb::fail(int code, const char* fmt, ...) {
 
 extern "C" int gb_version(void) { return 100; }
 extern "C" const char* gb_last_error(void) { return g_err.c_str(); }
+
+// ------------------------------------------------------------ tensor maps
+namespace {
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+    // through the runtime's driver entry point table: no link against libcuda
+    static EncodeTiledFn fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return (EncodeTiledFn) nullptr;
+        return (EncodeTiledFn)f;
+    }();
+    return fn;
+}
+}  // namespace
+
+int gb::make_plane_map16(CUtensorMap* map, const void* base, long long nb, int n0, int n1,
+                         int n2, int box_rows, int box_cols, const char** why) {
+    EncodeTiledFn enc = encode_tiled();
+    if (!enc) {
+        *why = "cuTensorMapEncodeTiled is not available";
+        return -1;
+    }
+    // 8-byte words: a 16-byte element is two of them
+    const cuuint64_t dims[4] = {(cuuint64_t)2 * n2, (cuuint64_t)n1, (cuuint64_t)n0,
+                                (cuuint64_t)nb};
+    const cuuint64_t strides[3] = {(cuuint64_t)n2 * 16, (cuuint64_t)n1 * n2 * 16,
+                                   (cuuint64_t)n0 * n1 * n2 * 16};
+    const cuuint32_t box[4] = {(cuuint32_t)(2 * box_cols), (cuuint32_t)box_rows, 1, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, const_cast<void*>(base), dims,
+                     strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        *why = "cuTensorMapEncodeTiled refused the plane map";
+        return -1;
+    }
+    return 0;
+}
+
+extern "C" int gb_device_fault(int* code) {
+    if (!code) return fail(GB_EINVAL, "device_fault: NULL argument");
+    *code = 0;
+    int c = 0;
+    if (take_fault_transform(&c)) return fail(GB_ECUDA, "device_fault: cannot read the flag");
+    if (c) *code = c;
+    return 0;
+}
 
 // ----------------------------------------------------------- kernel trace
 // Profiling aid for composite entry points: while a trace is open, each

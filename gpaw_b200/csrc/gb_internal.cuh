@@ -111,5 +111,7 @@ int launch_fd_cfd(int mode, const void* in, void* out, int nin, const GridBC& g,
                   cudaStream_t st, int* nblk);
 int cfd_blocks(const GridBC& g, int nn, int elem_bytes, int nin, int chunk = 0);
 int cfd_chunk(const GridBC& g, int nn, int nin, int ty);
+// read and clear the device fault flag of a kernel file (bounded waits)
+int take_fault_transform(int* code);
 
 }  // namespace gb

@@ -19,6 +19,7 @@
 #include <algorithm>
 
 #include "gb_internal.cuh"
+#include "gb_tma.cuh"
 
 namespace gb {
 
@@ -293,6 +294,345 @@ k_restrict(const T* __restrict__ in, T* __restrict__ out, T* __restrict__ out2, 
     cp_wait_x<0>();
 }
 
+// ------------------------------------------- restrict, TMA plane windows
+// The same restriction for complex128 grids, with each padded input plane's
+// window brought into shared memory by one TMA tensor copy instead of
+// per-thread cp.async cells.  The window starts at the tile's footprint
+// origin; the parts outside the grid arrive as zeros.  What the TMA cannot
+// do is done by the threads afterwards, per plane:
+//  * cells past a periodic edge of axis 1 or 2 (the "wrapped" cells, only
+//    in tiles at an edge): loaded from the opposite side one plane ahead
+//    (into registers) and stored with their Bloch phases;
+//  * a plane past a periodic edge of axis 0: every in-grid cell is
+//    multiplied by that axis's phase.
+// The wrapped cells of a tile are enumerated compactly (rows past the edge,
+// then columns past the edge of the other rows) and dealt to the threads,
+// at most NWR a thread; the launcher checks the count.
+template <int K, int TJ, int TK, int D, int NWR>
+__global__ void __launch_bounds__(TJ * TK, K >= 8 ? 2 : 3)
+k_restrict_tma(const __grid_constant__ CUtensorMap map, const double2* __restrict__ in,
+               double2* __restrict__ out, double2* __restrict__ out2, int nin, int b0,
+               XferGeom G, Phases P, int chunk0) {
+    using T = double2;
+    constexpr int NT = TJ * TK;
+    constexpr int H = 2 * K - 3;
+    constexpr int FY = 2 * TJ + H;        // fine rows needed by the tile
+    constexpr int FZ = 2 * TK + H;        // fine columns needed by the tile
+    constexpr int SS = FY * FZ;           // one window (elements)
+    constexpr int SSP = (SS + 7) / 8 * 8; // stage stride: 128-byte aligned
+    constexpr int RP = TK + 1;            // odd: a warp's rows hit distinct banks
+    constexpr int S = D + 1;              // ring depth
+    constexpr int NR = 2 * K - 1;         // axis-0 ring depth
+    constexpr int NC = (SS + NT - 1) / NT;
+    constexpr unsigned WBYTES = SS * 16;
+    extern __shared__ __align__(128) unsigned char smem_tma[];
+    const unsigned mis = tma_smem_u32(smem_tma) & 127u;
+    T* stage = reinterpret_cast<T*>(smem_tma + (mis ? 128 - mis : 0));
+    T* R1 = stage + S * SSP;              // [2][FY][RP]
+    uint64_t* bar = reinterpret_cast<uint64_t*>(R1 + 2 * FY * RP);
+
+    const int tiles2 = (G.nout[2] + TK - 1) / TK;
+    const int J0 = (blockIdx.x / tiles2) * TJ;
+    const int L0 = (blockIdx.x % tiles2) * TK;
+    const int I0 = blockIdx.y * chunk0;
+    const int I1 = min(G.nout[0], I0 + chunk0);
+    const int bg = b0 + blockIdx.z;
+    if (I0 >= I1 || (int)blockIdx.z >= nin) return;
+    const int n0 = G.g.n[0], n1 = G.g.n[1], n2 = G.g.n[2];
+    const long long psz = (long long)n1 * n2;
+    const long long ngout = (long long)G.nout[0] * G.nout[1] * G.nout[2];
+    const T* a = in + (long long)bg * n0 * psz;
+    T* o = out + (long long)bg * ngout;
+    const int tid = threadIdx.x;
+    const int tj = tid / TK, tk = tid % TK;
+    const bool cplx = P.use != 0;
+    // interior coordinates of the window's first row and column
+    const int row0 = 2 * J0 - G.plo[1], col0 = 2 * L0 - G.plo[2];
+
+    // this thread's in-grid cells (for the phase of a wrapped plane)
+    unsigned inmask = 0;
+#pragma unroll
+    for (int i = 0; i < NC; i++) {
+        const int e = tid + i * NT;
+        if (e < SS) {
+            const int iy = row0 + e / FZ, iz = col0 + e % FZ;
+            if (iy >= 0 && iy < n1 && iz >= 0 && iz < n2) inmask |= 1u << i;
+        }
+    }
+    // wrapped cells: rows [0, ra) and [rb, FY) are past axis 1's edges,
+    // columns [0, ca) and [cb, FZ) past axis 2's
+    const int ra = min(max(-row0, 0), FY), rb = min(max(n1 - row0, ra), FY);
+    const int ca = min(max(-col0, 0), FZ), cb = min(max(n2 - col0, ca), FZ);
+    const int nA = G.g.periodic[1] ? (ra + FY - rb) * FZ : 0;
+    const int nBc = G.g.periodic[2] ? ca + FZ - cb : 0;
+    const int nB = (rb - ra) * nBc;
+    int wso[NWR], wgo[NWR];
+    unsigned wmask = 0, wcode = 0;
+#pragma unroll
+    for (int r = 0; r < NWR; r++) {
+        const int w = tid + r * NT;
+        wso[r] = 0;
+        wgo[r] = 0;
+        int y, z;
+        if (w < nA) {
+            const int q = w / FZ;
+            z = w % FZ;
+            y = q < ra ? q : rb + (q - ra);
+        } else if (w < nA + nB) {
+            const int w2 = w - nA;
+            const int q = w2 / nBc, c = w2 % nBc;
+            y = ra + q;
+            z = c < ca ? c : cb + (c - ca);
+        } else {
+            continue;
+        }
+        int iy = row0 + y, iz = col0 + z;
+        const unsigned c1 = iy >= n1 ? 1u : (iy < 0 ? 2u : 0u);
+        const unsigned c2 = iz >= n2 ? 1u : (iz < 0 ? 2u : 0u);
+        if (wrap_c(iy, n1, G.g.periodic[1]) && wrap_c(iz, n2, G.g.periodic[2])) {
+            wmask |= 1u << r;
+            wso[r] = y * FZ + z;
+            wgo[r] = iy * n2 + iz;
+            wcode |= (c1 | (c2 << 2)) << (4 * r);
+        }
+    }
+    if (!cplx) wcode = 0;
+
+    // padded plane range for outputs [I0, I1): 2*I0 .. 2*(I1-1) + 2K - 2
+    const int x0a = 2 * I0;
+    const int nx = 2 * (I1 - I0) + 2 * K - 3;
+    auto plane_info = [&](int j, int& ip, int& wrapside) {
+        ip = x0a + j - G.plo[0];
+        wrapside = ip >= n0 ? 0 : (ip < 0 ? 1 : -1);
+        return wrap_c(ip, n0, G.g.periodic[0]);
+    };
+    // thread 0: the window of plane j into stage j % S
+    auto issue = [&](int j) {
+        int ip, ws;
+        const bool pv = plane_info(j, ip, ws);
+        const int slot = j % S;
+        fence_proxy_async_smem();
+        mbar_arrive_expect_tx(&bar[slot], WBYTES);
+        // a plane past a zero boundary: a window outside the tensor (zeros)
+        tma_load_window16(stage + slot * SSP, &map, col0, row0, pv ? ip : -1, bg, &bar[slot]);
+    };
+    T pre[NWR];
+    auto load_wrapped = [&](int j) {
+        int ip, ws;
+        const bool pv = plane_info(j, ip, ws);
+        const T* src = a + (long long)(pv ? ip : 0) * psz;
+#pragma unroll
+        for (int r = 0; r < NWR; r++)
+            pre[r] = (pv && ((wmask >> r) & 1)) ? __ldg(src + wgo[r]) : Num<T>::zero();
+    };
+    auto fixup = [&](int j, int slot) {
+        int ip, ws;
+        if (!plane_info(j, ip, ws)) return;
+        T* st = stage + slot * SSP;
+        const bool pw = cplx && ws >= 0;
+        const double2 ph0 = ws == 0 ? P.ph[0][0] : P.ph[0][1];
+        if (pw) {
+#pragma unroll
+            for (int i = 0; i < NC; i++)
+                if ((inmask >> i) & 1) st[tid + i * NT] = cmul(ph0, st[tid + i * NT]);
+        }
+#pragma unroll
+        for (int r = 0; r < NWR; r++)
+            if ((wmask >> r) & 1)
+                st[wso[r]] = apply_code<T>(pre[r], (wcode >> (4 * r)) & 15u, pw, ph0, P);
+    };
+
+    T ring[NR];
+#pragma unroll
+    for (int i = 0; i < NR; i++) ring[i] = Num<T>::zero();
+    // axis-2 pass: a thread makes four neighbouring outputs of one row
+    // (columns 4g .. 4g+3 of the tile), reading the K + 3 even columns
+    // 8g, 8g + 2, ..., 8g + 2K + 4 they share and their four centres
+    // 8g + K - 1 + {0, 2, 4, 6}: K + 7 reads instead of 4 (K + 1).
+    // Consecutive lanes take consecutive rows; the odd row pitch FZ puts
+    // the eight lanes of a bank phase on distinct banks.
+    constexpr int G4 = TK / 4;
+    constexpr int NI2 = FY * G4;                   // items per plane
+    static_assert(NI2 <= NT, "one axis-2 item per thread at most");
+    const bool has2 = tid < NI2;
+    const int y2 = tid % FY, g2 = tid / FY;
+    const int foff = y2 * FZ + 8 * g2;             // first even column
+    const int roff = y2 * RP + 4 * g2;
+    auto axis2 = [&](int t, int slot) {
+        if (!has2) return;
+        const T* f = stage + slot * SSP + foff;
+        T* R = R1 + (t & 1) * (FY * RP) + roff;
+        // a window of K even columns slides one step per output
+        T ev[K];
+#pragma unroll
+        for (int q = 0; q < K; q++) ev[q] = f[2 * q];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            // centre 2i + K - 1; its pairs at +-(2l + 1) are the even
+            // columns 2i + K + 2l and 2i + K - 2 - 2l: window slots
+            // K/2 + l and K/2 - 1 - l
+            T x = f[2 * i + K - 1];
+#pragma unroll
+            for (int l = 0; l < K / 2; l++)
+                x = Num<T>::add(x, Num<T>::scale(Num<T>::add(ev[K / 2 + l], ev[K / 2 - 1 - l]),
+                                                 G.w[l]));
+            const T v = Num<T>::scale(x, 0.5);
+            R[i] = G.neg_in ? Num<T>::neg(v) : v;
+            if (i < 3) {
+#pragma unroll
+                for (int q = 0; q < K - 1; q++) ev[q] = ev[q + 1];
+                ev[K - 1] = f[2 * (i + K)];
+            }
+        }
+    };
+    T pend = Num<T>::zero();
+    auto axis10 = [&](int t) {
+        const T* R = R1 + (t & 1) * (FY * RP) + (K - 1 + 2 * tj) * RP + tk;
+        T x = R[0];
+#pragma unroll
+        for (int l = 0; l < K / 2; l++)
+            x = Num<T>::add(x, Num<T>::scale(Num<T>::add(R[(2 * l + 1) * RP],
+                                                         R[-(2 * l + 1) * RP]),
+                                             G.w[l]));
+        if (t & 1) {
+            pend = Num<T>::scale(x, 0.5);
+            return;
+        }
+#pragma unroll
+        for (int i = 0; i < NR - 2; i++) ring[i] = ring[i + 2];
+        ring[NR - 2] = pend;
+        ring[NR - 1] = Num<T>::scale(x, 0.5);
+        if (t >= 2 * K - 2) {
+            const int I = I0 + (t - (2 * K - 2)) / 2;
+            const int J = J0 + tj, L = L0 + tk;
+            T y = ring[K - 1];
+#pragma unroll
+            for (int l = 0; l < K / 2; l++)
+                y = Num<T>::add(y, Num<T>::scale(Num<T>::add(ring[K - 1 + 2 * l + 1],
+                                                             ring[K - 1 - 2 * l - 1]),
+                                                 G.w[l]));
+            if (J < G.nout[1] && L < G.nout[2]) {
+                const long long at = ((long long)I * G.nout[1] + J) * G.nout[2] + L;
+                const T r = Num<T>::scale(y, 0.5);
+                o[at] = r;
+                if (out2) out2[(long long)bg * ngout + at] = Num<T>::scale(r, G.scale2);
+            }
+        }
+    };
+    // after a wait ran out: every thread agrees (a barrier with a vote),
+    // waits a little for the copies it may still have in flight, and leaves
+    auto drain = [&](int j) {
+        for (int q = j; q < min(nx, j + D); q++)
+            mbar_wait(&bar[q % S], (unsigned)(q / S) & 1u, 100000000ull);
+    };
+
+    if (tid == 0) {
+#pragma unroll
+        for (int q = 0; q < S; q++) mbar_init(&bar[q], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (tid == 0)
+        for (int j = 0; j < D && j < nx; j++) issue(j);
+    load_wrapped(0);
+    bool bad = !mbar_wait(&bar[0], 0u);
+    if (!bad) fixup(0, 0);
+    if (nx > 1) load_wrapped(1);
+    fence_proxy_async_smem();
+    if (__syncthreads_or(bad)) {
+        drain(0);
+        return;
+    }
+    if (tid == 0 && D < nx) issue(D);
+    axis2(0, 0);
+#pragma unroll 1
+    for (int t = 0; t < nx; t++) {
+        const int j = t + 1;
+        if (j < nx) {
+            bad = !mbar_wait(&bar[j % S], (unsigned)(j / S) & 1u);
+            if (!bad) fixup(j, j % S);
+            if (j + 1 < nx) load_wrapped(j + 1);
+        }
+        // this thread's shared-memory writes and reads of the slot that the
+        // next copy overwrites come before that copy (async proxy)
+        fence_proxy_async_smem();
+        if (__syncthreads_or(bad)) {
+            drain(j);
+            return;
+        }
+        // plane j + D goes into slot t % S, whose plane t was read by the
+        // axis-2 pass before this barrier
+        if (tid == 0 && j + D < nx) issue(j + D);
+        if (j < nx) axis2(j, j % S);
+        axis10(t);
+    }
+}
+
+// The wrapped cells of the busiest tile of a restriction (what
+// k_restrict_tma deals to its threads).
+static int restrict_wrapped_max(const XferGeom& G, int K, int TJ, int TK) {
+    const int H = 2 * K - 3, FY = 2 * TJ + H, FZ = 2 * TK + H;
+    int best = 0;
+    for (int J0 = 0; J0 < G.nout[1]; J0 += TJ)
+        for (int L0 = 0; L0 < G.nout[2]; L0 += TK) {
+            const int row0 = 2 * J0 - G.plo[1], col0 = 2 * L0 - G.plo[2];
+            const int ra = std::min(std::max(-row0, 0), FY);
+            const int rb = std::min(std::max(G.g.n[1] - row0, ra), FY);
+            const int ca = std::min(std::max(-col0, 0), FZ);
+            const int cb = std::min(std::max(G.g.n[2] - col0, ca), FZ);
+            const int nA = G.g.periodic[1] ? (ra + FY - rb) * FZ : 0;
+            const int nB = G.g.periodic[2] ? (rb - ra) * (ca + FZ - cb) : 0;
+            best = std::max(best, nA + nB);
+        }
+    return best;
+}
+
+int take_fault_transform(int* code) { return take_unit_fault(code); }
+
+// TMA staging of complex restrictions: on unless GPAW_B200_TMA=0 (read at
+// every launch, so that tests can compare both paths in one process).
+bool tma_enabled() {
+    const char* e = getenv("GPAW_B200_TMA");
+    return e == nullptr || atoi(e) != 0;
+}
+
+template <int K>
+static int launch_restrict_tma(const void* in, void* out, void* out2, int nin,
+                               const XferGeom& G, const Phases& P, cudaStream_t st) {
+    constexpr int TJ = 16, TK = 16, D = 1, NWR = 2;
+    constexpr int H = 2 * K - 3, FY = 2 * TJ + H, FZ = 2 * TK + H;
+    constexpr int SSP = (FY * FZ + 7) / 8 * 8;
+    constexpr size_t smem = ((size_t)(D + 1) * SSP + (size_t)2 * FY * (TK + 1)) * 16 +
+                            (D + 1) * sizeof(uint64_t) + 128;
+    if (restrict_wrapped_max(G, K, TJ, TK) > NWR * TJ * TK) return 1;   // not this kernel
+    CUtensorMap map;
+    const char* why = nullptr;
+    if (make_plane_map16(&map, in, nin, G.g.n[0], G.g.n[1], G.g.n[2], FY, FZ, &why)) return 1;
+    static bool attr = false;
+    if (!attr) {
+        if (cudaFuncSetAttribute(k_restrict_tma<K, TJ, TK, D, NWR>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess)
+            return -2;
+        attr = true;
+    }
+    const int t1 = (G.nout[1] + TJ - 1) / TJ, t2 = (G.nout[2] + TK - 1) / TK;
+    int chunk0 = G.nout[0];
+    const long long tiles = (long long)t1 * t2 * nin;
+    if (G.chunk > 0) chunk0 = std::min(G.chunk, G.nout[0]);
+    else
+        while (chunk0 > 4 && tiles * ((G.nout[0] + chunk0 - 1) / chunk0) < 148 * 4)
+            chunk0 = (chunk0 + 1) / 2;
+    const int nchunks = (G.nout[0] + chunk0 - 1) / chunk0;
+    for (int b0 = 0; b0 < nin; b0 += 65535) {
+        const int nb = min(65535, nin - b0);
+        dim3 grid(t1 * t2, nchunks, nb);
+        k_restrict_tma<K, TJ, TK, D, NWR><<<grid, TJ * TK, smem, st>>>(
+            map, (const double2*)in, (double2*)out, (double2*)out2, nb, b0, G, P, chunk0);
+    }
+    return 0;
+}
+
 // -------------------------------------------------------------- interpolate
 // IP1D (c/bmgs/interpolate.cpp:10-46): raw fine index u along an axis maps
 // to coarse base m = K/2 - 1 + u/2 in the padded input; even u copies a[m],
@@ -515,6 +855,12 @@ k_interpolate(const T* __restrict__ in, T* __restrict__ out, int nin, XferGeom G
 template <class T, int K>
 static int launch_restrict_k(const void* in, void* out, void* out2, int nin, const XferGeom& G,
                              const Phases& P, cudaStream_t st) {
+    if constexpr (sizeof(T) == 16) {
+        if (tma_enabled()) {
+            const int rc = launch_restrict_tma<K>(in, out, out2, nin, G, P, st);
+            if (rc <= 0) return rc;
+        }
+    }
     // 16-byte elements: a square 16 x 16 tile; 8-byte: 8 x 32.  Complex
     // stages are 27 KB: one plane ahead (two stages) leaves room for three
     // CTAs an SM, which hides more latency than a deeper ring (measured).

@@ -131,6 +131,14 @@ GB_API int gb_operator_relax(gb_operator* op, int method, double* f, const doubl
 GB_API int gb_operator_relax_noalloc(gb_operator* op, int method, double* f, const double* s,
                                      int nrelax, double w, void* stream);
 
+/* Device-side fault record; no counterpart in the reference.  Kernels that
+ * wait on the completion of asynchronous copies bound every wait (one
+ * second); a wait that runs out records a code here instead of hanging the
+ * GPU, and that kernel's output is not valid.  Reads and clears the record
+ * (synchronous): *code = 0 when nothing was recorded, 1 for a copy that
+ * did not complete in time. */
+GB_API int gb_device_fault(int* code);
+
 /* Kernel timeline of composite calls; a profiling aid with no counterpart
  * in the reference.  Between gb_trace_begin(capacity) and gb_trace_end,
  * gb_fd_precond records a CUDA event on its stream before each of its
