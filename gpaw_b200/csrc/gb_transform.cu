@@ -308,8 +308,8 @@ k_restrict(const T* __restrict__ in, T* __restrict__ out, T* __restrict__ out2, 
 // The wrapped cells of a tile are enumerated compactly (rows past the edge,
 // then columns past the edge of the other rows) and dealt to the threads,
 // at most NWR a thread; the launcher checks the count.
-template <int K, int TJ, int TK, int D, int NWR>
-__global__ void __launch_bounds__(TJ * TK, K >= 8 ? 2 : 3)
+template <int K, int TJ, int TK, int D, int NWR, int MINB>
+__global__ void __launch_bounds__(TJ * TK, MINB)
 k_restrict_tma(const __grid_constant__ CUtensorMap map, const double2* __restrict__ in,
                double2* __restrict__ out, double2* __restrict__ out2, int nin, int b0,
                XferGeom G, Phases P, int chunk0) {
@@ -596,10 +596,10 @@ bool tma_enabled() {
     return e == nullptr || atoi(e) != 0;
 }
 
-template <int K>
-static int launch_restrict_tma(const void* in, void* out, void* out2, int nin,
-                               const XferGeom& G, const Phases& P, cudaStream_t st) {
-    constexpr int TJ = 16, TK = 16, D = 1, NWR = 2;
+template <int K, int D, int MINB>
+static int launch_restrict_tma_v(const void* in, void* out, void* out2, int nin,
+                                 const XferGeom& G, const Phases& P, cudaStream_t st) {
+    constexpr int TJ = 16, TK = 16, NWR = 2;
     constexpr int H = 2 * K - 3, FY = 2 * TJ + H, FZ = 2 * TK + H;
     constexpr int SSP = (FY * FZ + 7) / 8 * 8;
     constexpr size_t smem = ((size_t)(D + 1) * SSP + (size_t)2 * FY * (TK + 1)) * 16 +
@@ -610,7 +610,7 @@ static int launch_restrict_tma(const void* in, void* out, void* out2, int nin,
     if (make_plane_map16(&map, in, nin, G.g.n[0], G.g.n[1], G.g.n[2], FY, FZ, &why)) return 1;
     static bool attr = false;
     if (!attr) {
-        if (cudaFuncSetAttribute(k_restrict_tma<K, TJ, TK, D, NWR>,
+        if (cudaFuncSetAttribute(k_restrict_tma<K, TJ, TK, D, NWR, MINB>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
             cudaSuccess)
             return -2;
@@ -627,10 +627,23 @@ static int launch_restrict_tma(const void* in, void* out, void* out2, int nin,
     for (int b0 = 0; b0 < nin; b0 += 65535) {
         const int nb = min(65535, nin - b0);
         dim3 grid(t1 * t2, nchunks, nb);
-        k_restrict_tma<K, TJ, TK, D, NWR><<<grid, TJ * TK, smem, st>>>(
+        k_restrict_tma<K, TJ, TK, D, NWR, MINB><<<grid, TJ * TK, smem, st>>>(
             map, (const double2*)in, (double2*)out, (double2*)out2, nb, b0, G, P, chunk0);
     }
     return 0;
+}
+
+// Pipeline depth and occupancy of the TMA restriction: one plane ahead with
+// three CTAs an SM, or two planes ahead with two (GPAW_B200_RST_DEPTH=2).
+template <int K>
+static int launch_restrict_tma(const void* in, void* out, void* out2, int nin,
+                               const XferGeom& G, const Phases& P, cudaStream_t st) {
+    static const int depth = [] {
+        const char* e = getenv("GPAW_B200_RST_DEPTH");
+        return e ? atoi(e) : 1;
+    }();
+    if (depth == 2 || K >= 8) return launch_restrict_tma_v<K, 2, 2>(in, out, out2, nin, G, P, st);
+    return launch_restrict_tma_v<K, 1, 3>(in, out, out2, nin, G, P, st);
 }
 
 // -------------------------------------------------------------- interpolate
