@@ -21,11 +21,13 @@
 // wrapped complex value is applied when it is read (register-side, exact
 // complex multiply as in bmgs_translatemz, c/bmgs/translate.cpp:28-47).
 #include <cstdlib>
+#include <cstring>
 #include <utility>
 
 #include <algorithm>
 
 #include "gb_internal.cuh"
+#include "gb_tma.cuh"
 
 namespace gb {
 
@@ -160,14 +162,17 @@ __device__ __forceinline__ T add_direction(T x, const double* cp, const double* 
 // Register caps: three resident CTAs of 256 threads for the complex apply
 // (nn <= 3), two for the other complex modes, four CTAs of 128 threads for
 // real data.
-template <class T, int NN, int TX, int TY, int RY, int D, int MODE, int ORD>
-__global__ void __launch_bounds__(TX * (TY / RY),
-                                  (sizeof(T) == 16 && NN <= 3 &&
-                                   (MODE == EPI_APPLY || MODE == EPI_POT))
-                                      ? 4
-                                      : (512 / (TX * (TY / RY))))
+// LD selects how plane tiles reach shared memory: 0 per-thread cp.async
+// cells (any element type), 1 one TMA tensor copy per plane (16-byte
+// elements; `map` describes the whole batch, `b0` is this launch's first
+// grid in it).  With the TMA the tile arrives with zeros past every edge;
+// the halo cells past a periodic edge of axis 1 or 2 are then stored by the
+// threads (values loaded one plane ahead, times the Bloch phase).
+template <class T, int NN, int TX, int TY, int RY, int D, int MODE, int ORD, int LD, int MINB>
+__global__ void __launch_bounds__(TX * (TY / RY), MINB)
 k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phases P,
-         CfdStencil cs, int chunk0, int tiles_x, Epi ep) {
+         CfdStencil cs, int chunk0, int tiles_x, Epi ep, const __grid_constant__ CUtensorMap map,
+         int b0) {
     constexpr int PX = TX + 2 * NN;          // tile pitch (elements)
     constexpr int PY = TY + 2 * NN;
     constexpr int S = NN + 1 + D;            // ring depth
@@ -175,8 +180,19 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
     constexpr int Q = 2 * NN + 1;
     constexpr int EB = (int)sizeof(T);
     constexpr bool CPLX = sizeof(T) == 16;
+    static_assert(LD == 0 || CPLX, "TMA tiles: 16-byte elements only");
+    // plane stage stride: 128-byte aligned for the TMA
+    constexpr int SP = LD ? (PX * PY + 7) / 8 * 8 : PX * PY;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* ring = reinterpret_cast<T*>(smem_raw);
+    T* ring;
+    uint64_t* bar = nullptr;
+    if constexpr (LD == 1) {
+        const unsigned mis = tma_smem_u32(smem_raw) & 127u;
+        ring = reinterpret_cast<T*>(smem_raw + (mis ? 128 - mis : 0));
+        bar = reinterpret_cast<uint64_t*>(ring + S * SP);
+    } else {
+        ring = reinterpret_cast<T*>(smem_raw);
+    }
 
     const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
     const int x0 = (blockIdx.x % tiles_x) * TX;
@@ -254,7 +270,7 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
     auto issue = [&](int j, int slot) {
         int pl = pa + j;
         const bool pvalid = wrap_coord(pl, n0, g.periodic[0]);
-        T* st = ring + slot * (PX * PY);
+        T* st = ring + slot * SP;
         const T* src = a + pl * pstride;
 #pragma unroll
         for (int i = 0; i < NC; i++) {
@@ -268,7 +284,7 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
     // the opposite side, as bc_unpack1's translate does, c/bc.cpp:242-257).
     // Other threads read them NN iterations later, after a barrier.
     auto fixup = [&](int slot) {
-        T* st = ring + slot * (PX * PY);
+        T* st = ring + slot * SP;
 #pragma unroll
         for (int i = 0; i < NC; i++) {
             const unsigned c = (wcode >> (3 * i)) & 7u;
@@ -279,6 +295,89 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
                 st[soff[i]] = cmul(ph, st[soff[i]]);
             }
         }
+    };
+
+    // -- TMA tiles (LD == 1): the halo cells past a periodic edge ----------
+    // Cells the stencil reads that lie outside the grid on one axis: rows
+    // past axis 1's edges (columns 0..TX-1 of the tile) and columns past
+    // axis 2's edges (rows 0..TY-1), taken from rows/columns beyond the
+    // grid's extent inside [-NN, TY + NN) x [-NN, TX + NN).  They are dealt
+    // to the threads, at most NWR each (the launcher checks the count).
+    constexpr int NWR = LD ? (2 * NN * (TX + TY) + NT - 1) / NT : 1;
+    int wso[NWR], wgo[NWR];
+    unsigned wmask = 0, wph = 0;   // wph: 3 bits a cell, the code of `fixup`
+    if constexpr (LD == 1) {
+        const int rb0 = max(-NN, -y0), rb1 = min(TY + NN, n1 - y0);   // in-grid rows
+        const int cb0 = max(-NN, -x0), cb1 = min(TX + NN, n2 - x0);   // in-grid columns
+        const int ra0 = max(0, cb0), ra1 = min(TX, cb1);              // part A columns
+        const int nrowA = g.periodic[1] ? (TY + 2 * NN) - (rb1 - rb0) : 0;
+        const int ncolA = max(0, ra1 - ra0);
+        const int nA = nrowA * ncolA;
+        const int rB0 = max(0, rb0), rB1 = min(TY, rb1);              // part B rows
+        const int ncolB = g.periodic[2] ? (TX + 2 * NN) - (cb1 - cb0) : 0;
+        const int nB = max(0, rB1 - rB0) * ncolB;
+#pragma unroll
+        for (int r = 0; r < NWR; r++) {
+            const int w = tid + r * NT;
+            wso[r] = 0;
+            wgo[r] = 0;
+            int ry, rx;
+            if (w < nA) {
+                const int q = w / ncolA;
+                rx = ra0 + w % ncolA;
+                // outside rows: [-NN, rb0) then [rb1, TY + NN)
+                ry = q < rb0 + NN ? q - NN : rb1 + (q - (rb0 + NN));
+            } else if (w < nA + nB) {
+                const int w2 = w - nA;
+                ry = rB0 + w2 / ncolB;
+                const int c = w2 % ncolB;
+                rx = c < cb0 + NN ? c - NN : cb1 + (c - (cb0 + NN));
+            } else {
+                continue;
+            }
+            int y = y0 + ry, x = x0 + rx;
+            const bool yw = y < 0 || y >= n1;
+            const int ys = y < 0, xs = x < 0;
+            if (wrap_coord(y, n1, g.periodic[1]) && wrap_coord(x, n2, g.periodic[2])) {
+                wmask |= 1u << r;
+                wso[r] = (ry + NN) * PX + (rx + NN);
+                wgo[r] = y * n2 + x;
+                wph |= (yw ? 1u + ys : 3u + xs) << (3 * r);
+            }
+        }
+        if (!P.use) wph = 0;
+    }
+    T pre[NWR];
+    // this thread's wrapped cells of centre plane p (in the grid), loaded
+    // one plane before they are stored
+    auto load_wrapped = [&](int p) {
+#pragma unroll
+        for (int r = 0; r < NWR; r++)
+            pre[r] = ((wmask >> r) & 1) ? __ldg(a + p * pstride + wgo[r]) : Num<T>::zero();
+    };
+    auto store_wrapped = [&](int slot) {
+        T* st = ring + slot * SP;
+#pragma unroll
+        for (int r = 0; r < NWR; r++) {
+            if (!((wmask >> r) & 1)) continue;
+            T v = pre[r];
+            if constexpr (CPLX) {
+                const unsigned c = (wph >> (3 * r)) & 7u;
+                if (c) v = cmul(c == 1 ? P.ph[1][0] : c == 2 ? P.ph[1][1]
+                                : c == 3 ? P.ph[2][0] : P.ph[2][1], v);
+            }
+            st[wso[r]] = v;
+        }
+    };
+    // thread 0: the tile window of relative plane j into slot j % S
+    auto issue_tma = [&](int j, int slot) {
+        int pl = pa + j;
+        const bool pvalid = wrap_coord(pl, n0, g.periodic[0]);
+        fence_proxy_async_smem();
+        mbar_arrive_expect_tx(&bar[slot], (unsigned)(PX * PY * EB));
+        // a plane past a zero boundary: a window outside the tensor (zeros)
+        tma_load_window16(ring + slot * SP, &map, x0 - NN, y0 - NN, pvalid ? pl : -1,
+                          b0 + b, &bar[slot]);
     };
 
     // -- axis-0 queue ---------------------------------------------------------
@@ -310,11 +409,26 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
 
     // prologue: relative planes 0 .. D-1 into the ring
     const int jend = (pb - pa) + NN;   // relative planes needed: [0, jend)
+    if constexpr (LD == 1) {
+        if (tid == 0) {
+#pragma unroll
+            for (int q = 0; q < S; q++) mbar_init(&bar[q], 1);
+            mbar_fence_init();
+        }
+        __syncthreads();
+        if (tid == 0)
+            for (int j = 0; j < D && j < jend; j++) issue_tma(j, j % S);
+        if (wmask) load_wrapped(pa);
+    } else {
 #pragma unroll 1
-    for (int j = 0; j < D; j++) {
-        if (j < jend) issue(j, j % S);
-        cp_commit();
+        for (int j = 0; j < D; j++) {
+            if (j < jend) issue(j, j % S);
+            cp_commit();
+        }
     }
+    // a bounded wait ran out (all threads agree): no further copies or
+    // waits; the kernel finishes with invalid output and the fault recorded
+    bool dead = false;
 
     const int nplanes = pb - pa;
     const int total = nplanes + NN;
@@ -355,12 +469,26 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
         const int s_t = FIXED ? U : t % S;
         const int s_c = FIXED ? CU : (t - NN) % S;
         const int s_d = FIXED ? (U + D) % Q : (t + D) % S;
-        cp_wait<D - 1>();
-        // this thread's copies of plane t have landed: fix its wrapped halo
-        // cells (read as a centre NN iterations later, after a barrier)
-        if (wcode && t < nplanes) fixup(s_t);
-        __syncthreads();
-        {
+        if constexpr (LD == 1) {
+            bool bad = false;
+            if (!dead) bad = !mbar_wait(&bar[s_t], (unsigned)(t / S) & 1u);
+            // the window of plane t has landed: store the wrapped halo cells
+            // of a centre plane (read NN iterations later, after a barrier)
+            if (wmask && t < nplanes) {
+                store_wrapped(s_t);
+                if (t + 1 < nplanes) load_wrapped(pa + t + 1);
+            }
+            fence_proxy_async_smem();
+            if (__syncthreads_or(bad)) dead = true;
+            const int j = t + D;
+            if (tid == 0 && !dead && j < jend) issue_tma(j, s_d);
+        } else {
+            cp_wait<D - 1>();
+            // this thread's copies of plane t have landed: fix its wrapped
+            // halo cells (read as a centre NN iterations later, after a
+            // barrier)
+            if (wcode && t < nplanes) fixup(s_t);
+            __syncthreads();
             // the slot of plane t+D last held plane t-NN-1, the centre of
             // iteration t-1, which every thread has finished (barrier above)
             const int j = t + D;
@@ -369,7 +497,7 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
         }
         // push plane t's own values (uniform phase for a wrapped plane)
         {
-            const T* st_in = ring + s_t * (PX * PY);
+            const T* st_in = ring + s_t * SP;
             const bool wrapped = CPLX && P.use && pa + t >= n0;
 #pragma unroll
             for (int r = 0; r < RY; r++) {
@@ -381,7 +509,7 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
         }
         if (t >= NN) {
             const int p = pa + t - NN;
-            const T* sc = ring + s_c * (PX * PY);
+            const T* sc = ring + s_c * SP;
             // this thread's column in the centre tile (axis-1 neighbours)
             const T* colp = sc + ty0 * PX + (tx + NN);
 #pragma unroll
@@ -442,7 +570,13 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
             const int t = t0 + decltype(U_)::value;
             if (t < total) step(t, U_);
         });
-    cp_wait<0>();
+    if constexpr (LD == 1) {
+        // copies still in flight after a wait ran out: give them a moment
+        if (dead)
+            for (int j = 0; j < jend; j++) mbar_wait(&bar[j % S], (unsigned)(j / S) & 1u, 1000000ull);
+    } else {
+        cp_wait<0>();
+    }
     if ((MODE == EPI_RESID || MODE == EPI_LIN) && ep.partial) {
         sq = block_sum(sq);
         if (tid == 0)
@@ -450,14 +584,44 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
     }
 }
 
-template <class T, int NN, int TX, int TY, int RY, int D, int MODE, int ORD>
+// The halo cells past a periodic edge in the busiest tile (what the TMA
+// variant of k_fd_cfd deals to its threads; the same count as the kernel's).
+static int cfd_wrapped_max(const GridBC& g, int NN, int TX, int TY) {
+    int best = 0;
+    for (int y0 = 0; y0 < g.n[1]; y0 += TY)
+        for (int x0 = 0; x0 < g.n[2]; x0 += TX) {
+            const int rb0 = std::max(-NN, -y0), rb1 = std::min(TY + NN, g.n[1] - y0);
+            const int cb0 = std::max(-NN, -x0), cb1 = std::min(TX + NN, g.n[2] - x0);
+            const int ncolA = std::max(0, std::min(TX, cb1) - std::max(0, cb0));
+            const int nA = g.periodic[1] ? ((TY + 2 * NN) - (rb1 - rb0)) * ncolA : 0;
+            const int nrowB = std::max(0, std::min(TY, rb1) - std::max(0, rb0));
+            const int nB = g.periodic[2] ? nrowB * ((TX + 2 * NN) - (cb1 - cb0)) : 0;
+            best = std::max(best, nA + nB);
+        }
+    return best;
+}
+
+bool tma_enabled();   // gb_transform.cu
+
+template <class T, int NN, int TX, int TY, int RY, int D, int MODE, int ORD, int LD, int MINB>
 static int launch_cfd_t(const void* in, void* out, int nin, const GridBC& g, const Phases& P,
                         const CfdStencil& cs, const Epi& ep, cudaStream_t st, int* nblk) {
     constexpr int PX = TX + 2 * NN, PY = TY + 2 * NN, S = NN + 1 + D;
-    constexpr size_t smem = (size_t)S * PX * PY * sizeof(T);
+    constexpr int SP = LD ? (PX * PY + 7) / 8 * 8 : PX * PY;
+    constexpr size_t smem =
+        (size_t)S * SP * sizeof(T) + (LD ? S * sizeof(uint64_t) + 128 : 0);
+    CUtensorMap map;
+    memset(&map, 0, sizeof map);
+    if constexpr (LD == 1) {
+        constexpr int NT = TX * (TY / RY);
+        constexpr int NWR = (2 * NN * (TX + TY) + NT - 1) / NT;
+        if (cfd_wrapped_max(g, NN, TX, TY) > NWR * NT) return 1;   // not this kernel
+        const char* why = nullptr;
+        if (make_plane_map16(&map, in, nin, g.n[0], g.n[1], g.n[2], PY, PX, &why)) return 1;
+    }
     static bool attr_done = false;
     if (!attr_done) {
-        cudaError_t e = cudaFuncSetAttribute(k_fd_cfd<T, NN, TX, TY, RY, D, MODE, ORD>,
+        cudaError_t e = cudaFuncSetAttribute(k_fd_cfd<T, NN, TX, TY, RY, D, MODE, ORD, LD, MINB>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)smem);
         if (e != cudaSuccess) return -2;
@@ -475,9 +639,9 @@ static int launch_cfd_t(const void* in, void* out, int nin, const GridBC& g, con
         Epi e2 = ep;
         if (e2.aux) e2.aux = (const T*)ep.aux + b0 * ng;
         if (e2.partial) e2.partial = ep.partial + (long long)b0 * tiles_x * tiles_y * nch;
-        k_fd_cfd<T, NN, TX, TY, RY, D, MODE, ORD><<<grid, TX * (TY / RY), smem, st>>>(
+        k_fd_cfd<T, NN, TX, TY, RY, D, MODE, ORD, LD, MINB><<<grid, TX * (TY / RY), smem, st>>>(
             (const T*)in + b0 * ng, out ? (T*)out + b0 * ng : nullptr, nb, g, P, cs, chunk0,
-            tiles_x, e2);
+            tiles_x, e2, map, b0);
     }
     return 0;
 }
@@ -498,11 +662,18 @@ static int launch_cfd_nn(const void* in, void* out, int nin, const GridBC& g, co
         // tiles of two rows a thread at two CTAs an SM (the rows' shared
         // axis-1 loads do not make up for the lost warps)
         constexpr int D = NN <= 3 ? 2 : 2;
+        constexpr int MB = (NN <= 3 && (MODE == EPI_APPLY || MODE == EPI_POT)) ? 4 : 2;
         if constexpr (MODE == EPI_APPLY && NN == 3)
             if (fused_apply())
-                return launch_cfd_t<T, NN, 32, 8, 1, D, MODE, 2>(in, out, nin, g, P, cs, ep, st,
-                                                                  nblk);
-        return launch_cfd_t<T, NN, 32, 8, 1, D, MODE, 1>(in, out, nin, g, P, cs, ep, st, nblk);
+                return launch_cfd_t<T, NN, 32, 8, 1, D, MODE, 2, 0, MB>(in, out, nin, g, P, cs,
+                                                                         ep, st, nblk);
+        if (tma_enabled()) {
+            const int rc = launch_cfd_t<T, NN, 32, 8, 1, D, MODE, 1, 1, MB>(in, out, nin, g, P,
+                                                                            cs, ep, st, nblk);
+            if (rc <= 0) return rc;
+        }
+        return launch_cfd_t<T, NN, 32, 8, 1, D, MODE, 1, 0, MB>(in, out, nin, g, P, cs, ep, st,
+                                                                 nblk);
     } else {
         constexpr int RY = (NN <= 3 && !AUX) ? 4 : 2;
         // nn = 3: three planes ahead makes the ring exactly 2nn+1 deep, so
@@ -512,8 +683,10 @@ static int launch_cfd_nn(const void* in, void* out, int nin, const GridBC& g, co
         // CTAs an SM) measured faster than 32 x 16 tiles (nn = 3 apply
         // 14 %, preconditioner 9 %, FP64 V-cycles 3-7 %)
         if constexpr (sizeof(T) == 8)
-            return launch_cfd_t<T, NN, 32, 8, 2, D, MODE, 1>(in, out, nin, g, P, cs, ep, st, nblk);
-        return launch_cfd_t<T, NN, 32, 16, RY, D, MODE, 1>(in, out, nin, g, P, cs, ep, st, nblk);
+            return launch_cfd_t<T, NN, 32, 8, 2, D, MODE, 1, 0, 4>(in, out, nin, g, P, cs, ep, st,
+                                                                   nblk);
+        return launch_cfd_t<T, NN, 32, 16, RY, D, MODE, 1, 0, 512 / (32 * (16 / RY))>(
+            in, out, nin, g, P, cs, ep, st, nblk);
     }
 }
 
