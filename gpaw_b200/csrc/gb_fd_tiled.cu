@@ -668,8 +668,28 @@ static int launch_cfd_nn(const void* in, void* out, int nin, const GridBC& g, co
                 return launch_cfd_t<T, NN, 32, 8, 1, D, MODE, 2, 0, MB>(in, out, nin, g, P, cs,
                                                                          ep, st, nblk);
         if (tma_enabled()) {
-            const int rc = launch_cfd_t<T, NN, 32, 8, 1, D, MODE, 1, 1, MB>(in, out, nin, g, P,
-                                                                            cs, ep, st, nblk);
+            int rc = 1;
+            if constexpr (NN <= 3 && MODE != EPI_RESID) {
+                // two rows a thread share their axis-1 neighbours: fewer
+                // shared-memory reads per point (variant picked by
+                // GPAW_B200_CFD_VARIANT while the shapes are measured)
+                static const int var = [] {
+                    const char* e = getenv("GPAW_B200_CFD_VARIANT");
+                    return e ? atoi(e) : 0;
+                }();
+                if (var == 1)
+                    rc = launch_cfd_t<T, NN, 32, 8, 2, D, MODE, 1, 1, 4>(in, out, nin, g, P, cs,
+                                                                         ep, st, nblk);
+                else if (var == 2)
+                    rc = launch_cfd_t<T, NN, 32, 16, 2, D, MODE, 1, 1, 2>(in, out, nin, g, P, cs,
+                                                                          ep, st, nblk);
+                else if (var == 3)
+                    rc = launch_cfd_t<T, NN, 32, 8, 2, 1, MODE, 1, 1, 4>(in, out, nin, g, P, cs,
+                                                                         ep, st, nblk);
+            }
+            if (rc == 1)
+                rc = launch_cfd_t<T, NN, 32, 8, 1, D, MODE, 1, 1, MB>(in, out, nin, g, P, cs,
+                                                                       ep, st, nblk);
             if (rc <= 0) return rc;
         }
         return launch_cfd_t<T, NN, 32, 8, 1, D, MODE, 1, 0, MB>(in, out, nin, g, P, cs, ep, st,

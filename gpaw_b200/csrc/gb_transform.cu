@@ -17,6 +17,7 @@
 // Every intermediate value is formed with the same operations in the same
 // order as in the reference's passes, so outputs are bit-identical.
 #include <algorithm>
+#include <cstring>
 
 #include "gb_internal.cuh"
 #include "gb_tma.cuh"
@@ -663,10 +664,16 @@ __device__ __forceinline__ T ip_value(const T* c, int stride, bool odd, const do
     return x;
 }
 
-template <class T, int K, int TJ, int TK, int D>
-__global__ void __launch_bounds__(TJ * TK)
+// LD = 1 (complex data): each coarse plane's footprint window arrives by
+// one TMA tensor copy (zeros past every edge), then the threads store the
+// cells past a periodic edge of axis 1 or 2 (loaded one plane ahead) and,
+// in a plane past a periodic edge of axis 0, multiply the in-grid cells by
+// that axis's phase.  `map` covers the whole batch; `b0` is this launch's
+// first grid in it.
+template <class T, int K, int TJ, int TK, int D, int LD>
+__global__ void __launch_bounds__(TJ * TK, 4)
 k_interpolate(const T* __restrict__ in, T* __restrict__ out, int nin, XferGeom G, Phases P,
-              int chunk0) {
+              int chunk0, const __grid_constant__ CUtensorMap map, int b0) {
     constexpr int NT = TJ * TK;
     constexpr int CY = TJ / 2 + K + 1;     // coarse rows feeding TJ fine rows
     constexpr int CZ = TK / 2 + K + 1;
@@ -679,9 +686,18 @@ k_interpolate(const T* __restrict__ in, T* __restrict__ out, int nin, XferGeom G
     constexpr int NIP = CY * (TK / 2);                  // items per parity
     constexpr int NQ = (NIP + (NW / 2) * 32 - 1) / ((NW / 2) * 32);
     constexpr int EB = (int)sizeof(T);
+    static_assert(LD == 0 || sizeof(T) == 16, "TMA windows: 16-byte elements only");
+    constexpr int SSP = LD ? (SS + 7) / 8 * 8 : SS;   // stage stride (128-byte aligned)
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* stage = reinterpret_cast<T*>(smem_raw);
-    T* Q = stage + S * SS;                 // [CY][TK]
+    T* stage;
+    if constexpr (LD == 1) {
+        const unsigned mis = tma_smem_u32(smem_raw) & 127u;
+        stage = reinterpret_cast<T*>(smem_raw + (mis ? 128 - mis : 0));
+    } else {
+        stage = reinterpret_cast<T*>(smem_raw);
+    }
+    T* Q = stage + S * SSP;                // [CY][TK]
+    uint64_t* bar = reinterpret_cast<uint64_t*>(Q + CY * TK);
 
     const int tiles2 = (G.nout[2] + TK - 1) / TK;
     const int F1 = (blockIdx.x / tiles2) * TJ;
@@ -698,6 +714,7 @@ k_interpolate(const T* __restrict__ in, T* __restrict__ out, int nin, XferGeom G
     const T* a = in + b * ngin;
     T* o = out + b * ngout;
     const int tid = threadIdx.x;
+    const int bg = b0 + b;                 // this grid's index in the TMA map
     const int lane = tid & 31, wid = tid >> 5;
     // fine row of this thread: a warp's rows share the parity of their
     // fine index (two rows a warp for 16-wide tiles, one for 32-wide)
@@ -770,7 +787,7 @@ k_interpolate(const T* __restrict__ in, T* __restrict__ out, int nin, XferGeom G
     auto issue = [&](int j, int slot) {
         int ip, ws;
         const bool pv = plane_info(j, ip, ws);
-        T* st = stage + slot * SS;
+        T* st = stage + slot * SSP;
         const T* src = pv ? a + (long long)ip * n1 * n2 : a;
 #pragma unroll
         for (int i = 0; i < NC; i++) {
@@ -784,7 +801,7 @@ k_interpolate(const T* __restrict__ in, T* __restrict__ out, int nin, XferGeom G
         const bool pw = cplx && ws >= 0 && G.g.periodic[0];
         if (!pw && !pcode) return;
         const double2 ph0 = ws == 0 ? P.ph[0][0] : P.ph[0][1];
-        T* st = stage + slot * SS;
+        T* st = stage + slot * SSP;
 #pragma unroll
         for (int i = 0; i < NC; i++) {
             if (tid + i * NT >= SS) break;
@@ -792,6 +809,93 @@ k_interpolate(const T* __restrict__ in, T* __restrict__ out, int nin, XferGeom G
             if ((pw || c) && ((vmask >> i) & 1))
                 st[soff[i]] = apply_code<T>(st[soff[i]], c, pw, ph0, P);
         }
+    };
+
+    // -- TMA windows (LD == 1) ----------------------------------------------
+    // in-grid cells of this thread (e-mapping) and the wrapped cells (past
+    // a periodic edge of axis 1 or 2), dealt compactly: rows [0, ra) and
+    // [rb, CY) past axis 1's edges, then columns [0, ca) and [cb, CZ) of
+    // the other rows
+    const int row0 = base1 - G.plo[1], col0 = base2 - G.plo[2];
+    unsigned inmask = 0, wmask = 0, wcode = 0;
+    int wso[NC], wgo[NC];
+    T pre[NC];
+    if constexpr (LD == 1) {
+#pragma unroll
+        for (int i = 0; i < NC; i++) {
+            const int e = tid + i * NT;
+            if (e < SS) {
+                const int iy = row0 + e / CZ, iz = col0 + e % CZ;
+                if (iy >= 0 && iy < n1 && iz >= 0 && iz < n2) inmask |= 1u << i;
+            }
+        }
+        const int ra = min(max(-row0, 0), CY), rb = min(max(n1 - row0, ra), CY);
+        const int ca = min(max(-col0, 0), CZ), cb = min(max(n2 - col0, ca), CZ);
+        const int nA = G.g.periodic[1] ? (ra + CY - rb) * CZ : 0;
+        const int nBc = G.g.periodic[2] ? ca + CZ - cb : 0;
+        const int nB = (rb - ra) * nBc;
+#pragma unroll
+        for (int r = 0; r < NC; r++) {
+            const int w = tid + r * NT;
+            wso[r] = 0;
+            wgo[r] = 0;
+            int y, z;
+            if (w < nA) {
+                const int q = w / CZ;
+                z = w % CZ;
+                y = q < ra ? q : rb + (q - ra);
+            } else if (w < nA + nB) {
+                const int w2 = w - nA;
+                const int q = w2 / nBc, c = w2 % nBc;
+                y = ra + q;
+                z = c < ca ? c : cb + (c - ca);
+            } else {
+                continue;
+            }
+            int iy = row0 + y, iz = col0 + z;
+            const unsigned c1 = iy >= n1 ? 1u : (iy < 0 ? 2u : 0u);
+            const unsigned c2 = iz >= n2 ? 1u : (iz < 0 ? 2u : 0u);
+            if (wrap_c(iy, n1, G.g.periodic[1]) && wrap_c(iz, n2, G.g.periodic[2])) {
+                wmask |= 1u << r;
+                wso[r] = y * CZ + z;
+                wgo[r] = iy * n2 + iz;
+                wcode |= (c1 | (c2 << 2)) << (4 * r);
+            }
+        }
+        if (!cplx) wcode = 0;
+    }
+    auto issue_tma = [&](int j, int slot) {
+        int ip, ws;
+        const bool pv = plane_info(j, ip, ws);
+        fence_proxy_async_smem();
+        mbar_arrive_expect_tx(&bar[slot], (unsigned)(SS * 16));
+        tma_load_window16(stage + slot * SSP, &map, col0, row0, pv ? ip : -1, bg, &bar[slot]);
+    };
+    auto load_wrapped = [&](int j) {
+        int ip, ws;
+        const bool pv = plane_info(j, ip, ws);
+        const T* src = a + (long long)(pv ? ip : 0) * n1 * n2;
+#pragma unroll
+        for (int r = 0; r < NC; r++)
+            pre[r] = (pv && ((wmask >> r) & 1)) ? __ldg(src + wgo[r]) : Num<T>::zero();
+    };
+    auto fixup_tma = [&](int j, int slot) {
+        int ip, ws;
+        if (!plane_info(j, ip, ws)) return;
+        T* st = stage + slot * SSP;
+        const bool pw = cplx && ws >= 0;
+        const double2 ph0 = ws == 0 ? P.ph[0][0] : P.ph[0][1];
+        if constexpr (sizeof(T) == 16) {
+            if (pw) {
+#pragma unroll
+                for (int i = 0; i < NC; i++)
+                    if ((inmask >> i) & 1) st[tid + i * NT] = cmul(ph0, st[tid + i * NT]);
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < NC; r++)
+            if ((wmask >> r) & 1)
+                st[wso[r]] = apply_code<T>(pre[r], (wcode >> (4 * r)) & 15u, pw, ph0, P);
     };
 
     T ring[K];
@@ -811,21 +915,45 @@ k_interpolate(const T* __restrict__ in, T* __restrict__ out, int nin, XferGeom G
         }
     };
 
+    bool dead = false;   // a bounded wait ran out (all threads agree)
+    if constexpr (LD == 1) {
+        if (tid == 0) {
+#pragma unroll
+            for (int q = 0; q < S; q++) mbar_init(&bar[q], 1);
+            mbar_fence_init();
+        }
+        __syncthreads();
+        if (tid == 0)
+            for (int j = 0; j < D && j < nx; j++) issue_tma(j, j);
+        if (wmask) load_wrapped(0);
+    } else {
 #pragma unroll 1
-    for (int j = 0; j < D; j++) {
-        if (j < nx) issue(j, j);
-        cp_commit_x();
+        for (int j = 0; j < D; j++) {
+            if (j < nx) issue(j, j);
+            cp_commit_x();
+        }
     }
     int slot = 0;   // t % S
 #pragma unroll 1
     for (int t = 0; t < nx; t++) {
-        cp_wait_x<D - 1>();
-        fixup(t, slot);
-        __syncthreads();
-        // plane t + D goes into slot (t + D) % S = (t - 1) % S
-        if (t + D < nx) issue(t + D, slot == 0 ? S - 1 : slot - 1);
-        cp_commit_x();
-        const T* A = stage + slot * SS;
+        if constexpr (LD == 1) {
+            bool bad = false;
+            if (!dead) bad = !mbar_wait(&bar[slot], (unsigned)(t / S) & 1u);
+            fixup_tma(t, slot);
+            if (wmask && t + 1 < nx) load_wrapped(t + 1);
+            fence_proxy_async_smem();
+            if (__syncthreads_or(bad)) dead = true;
+            // plane t + D goes into slot (t + D) % S = (t - 1) % S
+            if (tid == 0 && !dead && t + D < nx) issue_tma(t + D, slot == 0 ? S - 1 : slot - 1);
+        } else {
+            cp_wait_x<D - 1>();
+            fixup(t, slot);
+            __syncthreads();
+            // plane t + D goes into slot (t + D) % S = (t - 1) % S
+            if (t + D < nx) issue(t + D, slot == 0 ? S - 1 : slot - 1);
+            cp_commit_x();
+        }
+        const T* A = stage + slot * SSP;
 #pragma unroll
         for (int r = 0; r < NQ; r++) {
             if ((qok >> r) & 1) {
@@ -861,7 +989,13 @@ k_interpolate(const T* __restrict__ in, T* __restrict__ out, int nin, XferGeom G
         }
         slot = slot + 1 == S ? 0 : slot + 1;
     }
-    cp_wait_x<0>();
+    if constexpr (LD == 1) {
+        if (dead)
+            for (int j = 0; j < nx; j++)
+                mbar_wait(&bar[j % S], (unsigned)(j / S) & 1u, 1000000ull);
+    } else {
+        cp_wait_x<0>();
+    }
 }
 
 // ----------------------------------------------------------------- launchers
@@ -912,17 +1046,26 @@ static int launch_restrict_k(const void* in, void* out, void* out2, int nin, con
     return 0;
 }
 
-template <class T, int K>
-static int launch_interp_k(const void* in, void* out, int nin, const XferGeom& G,
+template <class T, int K, int LD>
+static int launch_interp_v(const void* in, void* out, int nin, const XferGeom& G,
                            const Phases& P, cudaStream_t st) {
     constexpr int TK = sizeof(T) == 16 ? 16 : 32;
     constexpr int TJ = 256 / TK;
     constexpr int D = 3;
     constexpr int CY = TJ / 2 + K + 1, CZ = TK / 2 + K + 1;
-    constexpr size_t smem = ((size_t)(D + 1) * CY * CZ + (size_t)CY * TK) * sizeof(T);
+    constexpr int SSP = LD ? (CY * CZ + 7) / 8 * 8 : CY * CZ;
+    constexpr size_t smem = ((size_t)(D + 1) * SSP + (size_t)CY * TK) * sizeof(T) +
+                            (LD ? (D + 1) * sizeof(uint64_t) + 128 : 0);
+    CUtensorMap map;
+    memset(&map, 0, sizeof map);
+    if constexpr (LD == 1) {
+        const char* why = nullptr;
+        if (make_plane_map16(&map, in, nin, G.g.n[0], G.g.n[1], G.g.n[2], CY, CZ, &why))
+            return 1;
+    }
     static bool attr = false;
     if (!attr) {
-        if (cudaFuncSetAttribute(k_interpolate<T, K, TJ, TK, D>,
+        if (cudaFuncSetAttribute(k_interpolate<T, K, TJ, TK, D, LD>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
             cudaSuccess)
             return -2;
@@ -942,10 +1085,22 @@ static int launch_interp_k(const void* in, void* out, int nin, const XferGeom& G
         dim3 grid(t1 * t2, nchunks, nb);
         const long long ngin = (long long)G.g.n[0] * G.g.n[1] * G.g.n[2];
         const long long ngout = (long long)G.nout[0] * G.nout[1] * G.nout[2];
-        k_interpolate<T, K, TJ, TK, D><<<grid, TJ * TK, smem, st>>>(
-            (const T*)in + b0 * ngin, (T*)out + b0 * ngout, nb, G, P, chunk0);
+        k_interpolate<T, K, TJ, TK, D, LD><<<grid, TJ * TK, smem, st>>>(
+            (const T*)in + b0 * ngin, (T*)out + b0 * ngout, nb, G, P, chunk0, map, b0);
     }
     return 0;
+}
+
+template <class T, int K>
+static int launch_interp_k(const void* in, void* out, int nin, const XferGeom& G,
+                           const Phases& P, cudaStream_t st) {
+    if constexpr (sizeof(T) == 16) {
+        if (tma_enabled()) {
+            const int rc = launch_interp_v<T, K, 1>(in, out, nin, G, P, st);
+            if (rc <= 0) return rc;
+        }
+    }
+    return launch_interp_v<T, K, 0>(in, out, nin, G, P, st);
 }
 
 template <class T>

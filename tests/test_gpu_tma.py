@@ -1,5 +1,6 @@
 """Complex128 kernels whose input planes arrive by TMA tensor copies
-(restriction; GPAW_B200_TMA=0 selects the per-thread cp.async staging):
+(restriction, interpolation and the plane-marching stencil kernel;
+GPAW_B200_TMA=0 selects the per-thread cp.async staging):
 both paths against the oracle, bit for bit, on grids that exercise the
 window edges (periodic wrap with Bloch phases on every axis, zero and mixed
 boundaries, odd sizes, tiles cut by the grid's edge, batches) and the
@@ -27,6 +28,20 @@ CASES = [
 ]
 
 
+def _interp(gdp, nn, c, ph, tma):
+    from gpaw_b200 import Transformer
+    old = os.environ.get('GPAW_B200_TMA')
+    os.environ['GPAW_B200_TMA'] = '1' if tma else '0'
+    try:
+        t = Transformer(gdp.coarsen(), gdp, nn, complex)
+        return to_np(t.apply(to_dev(c), phases=ph))
+    finally:
+        if old is None:
+            del os.environ['GPAW_B200_TMA']
+        else:
+            os.environ['GPAW_B200_TMA'] = old
+
+
 def _restrict(gdp, nn, a, ph, tma):
     from gpaw_b200 import Transformer
     old = os.environ.get('GPAW_B200_TMA')
@@ -42,7 +57,7 @@ def _restrict(gdp, nn, a, ph, tma):
 
 
 @pytest.mark.parametrize('N,pbc,nn,nb', CASES)
-def test_restrict_tma_against_oracle(N, pbc, nn, nb, cuda):
+def test_transfers_tma_against_oracle(N, pbc, nn, nb, cuda):
     from gpaw_b200 import GridDescriptor, _lib
     cell = tuple(0.2 * n for n in N)
     gdp = GridDescriptor(N, cell, pbc)
@@ -56,6 +71,12 @@ def test_restrict_tma_against_oracle(N, pbc, nn, nb, cuda):
     got_cp = _restrict(gdp, nn, a, ph, False)
     assert np.array_equal(got_tma, ref)
     assert np.array_equal(got_cp, ref)
+    gc = gdo.coarsen()
+    c = rng.standard_normal((nb,) + tuple(gc.n_c)) + \
+        1j * rng.standard_normal((nb,) + tuple(gc.n_c))
+    ref = L.Transformer(gc, gdo, nn, complex).apply(c, phases=ph)
+    assert np.array_equal(_interp(gdp, nn, c, ph, True), ref)
+    assert np.array_equal(_interp(gdp, nn, c, ph, False), ref)
     code = _lib.C.c_int(-1)
     _lib.check(_lib.load().gb_device_fault(_lib.C.byref(code)))
     assert code.value == 0
