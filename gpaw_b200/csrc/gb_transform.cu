@@ -634,16 +634,20 @@ static int launch_restrict_tma_v(const void* in, void* out, void* out2, int nin,
     return 0;
 }
 
-// Pipeline depth and occupancy of the TMA restriction: one plane ahead with
-// three CTAs an SM, or two planes ahead with two (GPAW_B200_RST_DEPTH=2).
+// Pipeline depth and occupancy of the TMA restriction: two planes ahead
+// with two CTAs an SM for K >= 6 (measured on the 256 x 96^3 complex batch:
+// 3130 GB/s, against 2190 GB/s one plane ahead with three CTAs, whose
+// register cap spills), one plane ahead with three CTAs for K <= 4 (no
+// spills there).  GPAW_B200_RST_DEPTH=1 or 2 overrides.
 template <int K>
 static int launch_restrict_tma(const void* in, void* out, void* out2, int nin,
                                const XferGeom& G, const Phases& P, cudaStream_t st) {
     static const int depth = [] {
         const char* e = getenv("GPAW_B200_RST_DEPTH");
-        return e ? atoi(e) : 1;
+        return e ? atoi(e) : 0;
     }();
-    if (depth == 2 || K >= 8) return launch_restrict_tma_v<K, 2, 2>(in, out, out2, nin, G, P, st);
+    const bool deep = depth == 2 || (depth == 0 && K >= 6) || K >= 8;
+    if (deep) return launch_restrict_tma_v<K, 2, 2>(in, out, out2, nin, G, P, st);
     return launch_restrict_tma_v<K, 1, 3>(in, out, out2, nin, G, P, st);
 }
 
@@ -1091,11 +1095,20 @@ static int launch_interp_v(const void* in, void* out, int nin, const XferGeom& G
     return 0;
 }
 
+// The interpolation keeps per-thread cp.async cells by default: its coarse
+// windows are small (15 x 15 cells for K = 6), and one TMA copy per plane
+// measured slower (3500 against 3820 GB/s on the 256 x 96^3 complex batch).
+// GPAW_B200_TMA_INTERP=1 selects the TMA windows.
+static bool tma_interp() {
+    const char* e = getenv("GPAW_B200_TMA_INTERP");
+    return e != nullptr && atoi(e) != 0;
+}
+
 template <class T, int K>
 static int launch_interp_k(const void* in, void* out, int nin, const XferGeom& G,
                            const Phases& P, cudaStream_t st) {
     if constexpr (sizeof(T) == 16) {
-        if (tma_enabled()) {
+        if (tma_enabled() && tma_interp()) {
             const int rc = launch_interp_v<T, K, 1>(in, out, nin, G, P, st);
             if (rc <= 0) return rc;
         }

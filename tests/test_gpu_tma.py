@@ -30,16 +30,16 @@ CASES = [
 
 def _interp(gdp, nn, c, ph, tma):
     from gpaw_b200 import Transformer
-    old = os.environ.get('GPAW_B200_TMA')
-    os.environ['GPAW_B200_TMA'] = '1' if tma else '0'
+    old = os.environ.get('GPAW_B200_TMA_INTERP')
+    os.environ['GPAW_B200_TMA_INTERP'] = '1' if tma else '0'
     try:
         t = Transformer(gdp.coarsen(), gdp, nn, complex)
         return to_np(t.apply(to_dev(c), phases=ph))
     finally:
         if old is None:
-            del os.environ['GPAW_B200_TMA']
+            del os.environ['GPAW_B200_TMA_INTERP']
         else:
-            os.environ['GPAW_B200_TMA'] = old
+            os.environ['GPAW_B200_TMA_INTERP'] = old
 
 
 def _restrict(gdp, nn, a, ph, tma):
