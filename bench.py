@@ -395,7 +395,7 @@ def c1_cpu(phi_gpu, n_gpu):
     return best
 
 
-def poisson_c3(dev, nsolve=5):
+def poisson_c3(dev, nsolve=5, which=('fp64', 'mixed4', 'mixed6')):
     """192^3 zero-BC, h = 0.18 A, 64 Gaussians: plain FP64 V-cycle with the
     reference schedule (7 grids) versus FP32 V-cycles in FP64 defect
     correction, both to 1e-10 relative residual.  The mixed solver runs
@@ -422,6 +422,9 @@ def poisson_c3(dev, nsolve=5):
     for tag, ps in (('fp64_reference_schedule', fp64),
                     ('mixed_4_levels', mixed4),
                     ('mixed_6_levels', mixed6)):
+        if {'fp64_reference_schedule': 'fp64', 'mixed_4_levels': 'mixed4',
+                'mixed_6_levels': 'mixed6'}[tag] not in which:
+            continue
         phi = gd.zeros()
         ps.solve_neutral(phi, rho_d)      # warm-up (builds the graph)
         times = []
@@ -439,6 +442,8 @@ def poisson_c3(dev, nsolve=5):
         out[tag] = {'vcycles': n, 'ms_per_solve': t * 1e3,
                     'solves_per_s': 1.0 / t,
                     'rel_residual': float(np.sqrt(n2.item())) / rnorm}
+    if len(phis) < 3:
+        return out
     b = phis['fp64_reference_schedule']
     for lv in (4, 6):
         a = phis[f'mixed_{lv}_levels']
@@ -1066,7 +1071,8 @@ def main():
     p.add_argument('--no-ham', action='store_true',
                    help='skip the fused Hamiltonian section')
     p.add_argument('--poisson-only', default=None,
-                   choices=['c1', 'c3', 'c4', 'pc', 'c5', 'wfd', 'c1a'],
+                   choices=['c1', 'c3', 'c4', 'pc', 'c5', 'wfd', 'c1a', 'c3m',
+                            'c3f'],
                    help='run one Poisson configuration only (profiling)')
     p.add_argument('--batch', type=int, default=NBANDS,
                    help='wave functions per step (profiling runs only)')
@@ -1083,6 +1089,12 @@ def main():
         if args.poisson_only in ('c1', 'c3'):
             f = poisson_c1 if args.poisson_only == 'c1' else poisson_c3
             r = f(dev, nsolve=max(1, args.steps))
+        elif args.poisson_only in ('c3m', 'c3f'):
+            # one solver of C3 alone (profiling): the 4-level mixed solver
+            # or the FP64 reference schedule
+            r = poisson_c3(dev, nsolve=max(1, args.steps),
+                           which=('mixed4',) if args.poisson_only == 'c3m'
+                           else ('fp64',))
         else:
             r = {'c4': poisson_c4, 'pc': precond_c4, 'c5': serving_c5,
                  'wfd': weighted_fd, 'c1a': c1_apply}[args.poisson_only](dev)
