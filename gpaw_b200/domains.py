@@ -24,9 +24,110 @@ order.
 """
 from __future__ import annotations
 
+import collections
 import functools
+import threading
 
 import numpy as np
+
+
+# --------------------------------------------------------------------------
+# transports: a torch.distributed group, or ranks emulated in one process
+# --------------------------------------------------------------------------
+class LocalRanks:
+    """Stand-in for a process group: ``size`` ranks run as threads of one
+    process and exchange tensors through in-memory mailboxes, with the
+    same messages in the same order as over torch.distributed.  It lets a
+    decomposition run on one device (all ranks' slabs on one GPU), for
+    tests and debugging: ``LocalRanks(3).run(lambda rank, group: ...)``.
+
+    Point-to-point messages are matched by (source, destination, tag) and
+    a per-pair sequence number, so successive collectives do not mix; sums
+    over the ranks add the ranks' tensors in rank order (deterministic).
+    GPU work stays ordered because every thread enqueues on the device's
+    default stream."""
+
+    def __init__(self, size):
+        self.size = int(size)
+        self._cv = threading.Condition()
+        self._mail = {}
+        self._barrier = threading.Barrier(self.size)
+        self._slots = [None] * self.size
+        self._local = threading.local()
+
+    # per-thread state: the rank and its message counters
+    def _rank(self):
+        return self._local.rank
+
+    def _next(self, key):
+        cnt = self._local.counts
+        cnt[key] += 1
+        return cnt[key]
+
+    def exchange(self, sends, recvs):
+        """sends: [(dst, tag, tensor)], recvs: [(src, tag, buffer)];
+        returns when every buffer is filled."""
+        me = self._rank()
+        with self._cv:
+            for dst, tag, t in sends:
+                key = ('s', me, dst, tag)
+                # a copy taken now: the sender goes on writing its arrays
+                self._mail[(me, dst, tag, self._next(key))] = t.clone()
+            self._cv.notify_all()
+        for src, tag, buf in recvs:
+            k = (src, me, tag, self._next(('r', src, me, tag)))
+            with self._cv:
+                ok = self._cv.wait_for(lambda: k in self._mail, timeout=120)
+                if not ok:
+                    raise RuntimeError(f'LocalRanks: rank {me} got no message '
+                                       f'{k} in 120 s')
+                t = self._mail.pop(k)
+            buf.copy_(t)
+
+    def all_reduce_sum(self, t):
+        me = self._rank()
+        self._slots[me] = t.clone()
+        self._barrier.wait(timeout=120)
+        total = self._slots[0].clone()
+        for r in range(1, self.size):
+            total += self._slots[r]
+        self._barrier.wait(timeout=120)
+        t.copy_(total)
+
+    def run(self, fn):
+        """fn(rank, group) on every rank, each in its own thread; returns
+        the list of results in rank order and re-raises the first error."""
+        results = [None] * self.size
+        errors = []
+
+        def body(rank):
+            self._local.rank = rank
+            self._local.counts = collections.Counter()
+            try:
+                results[rank] = fn(rank, self)
+            except BaseException as e:   # noqa: BLE001 (reported below)
+                errors.append(e)
+                self._barrier.abort()
+                with self._cv:
+                    self._cv.notify_all()
+
+        threads = [threading.Thread(target=body, args=(r,))
+                   for r in range(self.size)]
+        for th in threads:
+            th.start()
+        for th in threads:
+            th.join()
+        if errors:
+            raise errors[0]
+        return results
+
+
+def _all_reduce_sum(t, group):
+    if isinstance(group, LocalRanks):
+        group.all_reduce_sum(t)
+    else:
+        import torch.distributed as dist
+        dist.all_reduce(t, group=group)
 
 
 def slab_bounds(n0, size):
@@ -202,13 +303,12 @@ class DistributedFDOperator:
     def residual_norm2(self, phi, rho, dv=1.0):
         """sum over the whole grid of (L phi - rho)^2 * dv, summed over the
         ranks (all ranks get it)."""
-        import torch.distributed as dist
         r = phi.new_zeros(phi.shape)
         self.apply(phi, r)
         r -= rho
         t = (r * r).sum().reshape(1) * dv
         if self.dom.size > 1:
-            dist.all_reduce(t, group=self.group)
+            _all_reduce_sum(t, self.group)
         return float(t.item())
 
 
@@ -353,25 +453,36 @@ def gather_box(a, needs, boxes, rank, n_c, periodic_c, phase_cd=None,
     barrier) before the first gather, so that every rank has set up its
     communicator when the first batch starts."""
     import torch
-    import torch.distributed as dist
     plan = _gather_plan(_tup(needs), _tup(boxes), int(rank),
                         tuple(int(n) for n in n_c),
                         tuple(bool(p) for p in periodic_c))
     out = a.new_zeros(a.shape[:-3] +
                       tuple(hi - lo for lo, hi in needs[rank]))
-    ops, recvd = [], []
+    sends, recvs, recvd = [], [], []
     for kind, peer, idx, sl, dl, k in plan:
         if kind == 'copy':
             out[dl] = a[sl]
             recvd.append((dl, k, None))
         elif kind == 'recv':
             buf = torch.empty_like(out[dl])
-            ops.append(dist.P2POp(dist.irecv, buf, peer, group, tag=idx))
+            recvs.append((peer, idx, buf))
             recvd.append((dl, k, buf))
         else:
-            ops.append(dist.P2POp(dist.isend, a[sl].contiguous(), peer,
-                                  group, tag=idx))
-    if ops:
+            sends.append((peer, idx, a[sl].contiguous()))
+    if isinstance(group, LocalRanks):
+        group.exchange(sends, recvs)
+    elif sends or recvs:
+        import torch.distributed as dist
+        # the same order of operations as before: the plan's order
+        ops = []
+        si, ri = iter(sends), iter(recvs)
+        for kind, peer, idx, sl, dl, k in plan:
+            if kind == 'recv':
+                _, tag, buf = next(ri)
+                ops.append(dist.P2POp(dist.irecv, buf, peer, group, tag=tag))
+            elif kind == 'send':
+                _, tag, t = next(si)
+                ops.append(dist.P2POp(dist.isend, t, peer, group, tag=tag))
         for req in dist.batch_isend_irecv(ops):
             req.wait()
     ph = None if phase_cd is None else np.asarray(phase_cd)
@@ -624,10 +735,9 @@ class DistributedFDPoissonSolver:
         return self._cycle(0)
 
     def _sum(self, t):
-        import torch.distributed as dist
         t = t.sum().reshape(1)
         if self.size > 1:
-            dist.all_reduce(t, group=self.group)
+            _all_reduce_sum(t, self.group)
         return float(t.item())
 
     def solve_neutral(self, phi, rho, eps=None, maxiter=None):
@@ -694,8 +804,7 @@ class DistributedFDPoissonSolver:
             t = torch.tensor(list(rhog_c) + [total], dtype=torch.float64,
                              device=rho.device)
             if self.size > 1:
-                import torch.distributed as dist
-                dist.all_reduce(t, group=self.group)
+                _all_reduce_sum(t, self.group)
             t = t.cpu().numpy()
             center = charge_center(self.gd, t[:3], float(t[3]))
         if gauss is None:

@@ -868,3 +868,37 @@ def test_charge_center_solve_reference_known_answer():
         ng = M.Gaussian(pgd, a=19, center=np.array((10.0, 10.0, 1.5)))
         charge_center(pgd, *charge_center_parts(pgd, ng.get_gauss(0),
                                                 1.0))
+
+
+def test_local_ranks_vcycles_equal_whole_grid():
+    """The in-process rank emulation (LocalRanks) runs the slab V-cycles of
+    three ranks as threads with the oracle's local operators: every slab of
+    phi equals the whole-grid V-cycles bit for bit, as over gloo."""
+    from gpaw_b200.domains import DistributedFDPoissonSolver, LocalRanks
+    from oracle import gpaw_layer as L
+    gd = L.GridDescriptor((24, 16, 16), (6.0, 4.0, 4.4), (1, 1, 0))
+    rng = np.random.default_rng(17)
+    rho = rng.standard_normal(tuple(gd.n_c))
+    phi = rng.standard_normal(tuple(gd.n_c)) * 0.1
+    ps = L.FDPoissonSolver(nn=3, relax='J', be='port')
+    ps.set_grid_descriptor(gd)
+    ps._init()
+    ps.phis[0] = phi.copy()
+    ps.rhos[0][:] = rho
+    ps.errors = []
+    ref_err = [ps.iterate2(ps.step) for _ in range(2)]
+
+    def body(rank, group):
+        dps = DistributedFDPoissonSolver(
+            ps, rank, 3, lambda c, o, n, p: _OracleLocal(c, o, n, p, float),
+            _OracleTransfer, group=group)
+        dom = dps.doms[0]
+        phl = torch.from_numpy(phi[dom.beg:dom.end].copy())
+        rhl = torch.from_numpy(rho[dom.beg:dom.end].copy())
+        err = [dps.iterate(phl, rhl) for _ in range(2)]
+        return dom.beg, dom.end, phl.numpy(), err
+
+    for beg, end, got, err in LocalRanks(3).run(body):
+        assert np.array_equal(got, ps.phis[0][beg:end])
+        for e, r in zip(err, ref_err):
+            assert abs(e - r) <= 1e-12 * abs(r)
