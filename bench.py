@@ -455,6 +455,44 @@ def poisson_c3(dev, nsolve=5, which=('fp64', 'mixed4', 'mixed6')):
     return out
 
 
+def mixed_vcycle_trace(dev, levels=4, reps=5):
+    """Per-kernel device times of one mixed-precision V-cycle on the C3 grid
+    (the 4-level FP32 V-cycle inside its FP64 defects), launched kernel by
+    kernel through gb_mixed_vcycle_eager under the library's kernel trace;
+    mean over `reps` V-cycles."""
+    import ctypes as C
+    import torch
+    from gpaw_b200 import GridDescriptor, MixedPoissonSolver, _lib
+    from gpaw_b200.workloads import BOHR, c3_density, neutralize
+    h = 0.18 / BOHR
+    gd = GridDescriptor((192, 192, 192), (192 * h,) * 3, 0, device=dev)
+    rho = torch.from_numpy(neutralize(c3_density(gd, 64), gd)).to(dev)
+    ps = MixedPoissonSolver(nn=3, tol=1e-10, levels=levels)
+    ps.set_grid_descriptor(gd)
+    phi = gd.zeros()
+    ps.solve_neutral(phi, rho)          # builds the graph, sets attributes
+    phi.zero_()
+    lib = _lib.load()
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    args = (ps._h.h, C.c_void_p(phi.data_ptr()), C.c_void_p(rho.data_ptr()),
+            st)
+    _lib.check(lib.gb_mixed_vcycle_eager(*args))
+    torch.cuda.synchronize()
+    with _lib.KernelTrace() as tr:
+        for _ in range(reps):
+            _lib.check(lib.gb_mixed_vcycle_eager(*args))
+    per = {}
+    for label, ms in tr.intervals:
+        if label == 'end of defect':
+            continue
+        per.setdefault(label, []).append(ms)
+    rows = sorted(((k, float(np.sum(v)) / reps) for k, v in per.items()),
+                  key=lambda kv: -kv[1])
+    return {'levels': levels, 'grid': [192, 192, 192],
+            'ms_per_vcycle_with_defects': sum(v for _, v in rows),
+            'kernels_ms': [[k, round(v, 4)] for k, v in rows]}
+
+
 def poisson_c4(dev, count=512, precisions=('mixed', 'fp64'), cpu=True):
     """512 zero-BC grids, every side from {32, 40, ..., 128}, each with 4-16
     seeded Gaussians (C3 distributions), solved to 1e-10 relative residual:
@@ -1072,7 +1110,7 @@ def main():
                    help='skip the fused Hamiltonian section')
     p.add_argument('--poisson-only', default=None,
                    choices=['c1', 'c3', 'c4', 'pc', 'c5', 'wfd', 'c1a', 'c3m',
-                            'c3f'],
+                            'c3f', 'c3trace'],
                    help='run one Poisson configuration only (profiling)')
     p.add_argument('--batch', type=int, default=NBANDS,
                    help='wave functions per step (profiling runs only)')
@@ -1089,6 +1127,8 @@ def main():
         if args.poisson_only in ('c1', 'c3'):
             f = poisson_c1 if args.poisson_only == 'c1' else poisson_c3
             r = f(dev, nsolve=max(1, args.steps))
+        elif args.poisson_only == 'c3trace':
+            r = mixed_vcycle_trace(dev)
         elif args.poisson_only in ('c3m', 'c3f'):
             # one solver of C3 alone (profiling): the 4-level mixed solver
             # or the FP64 reference schedule

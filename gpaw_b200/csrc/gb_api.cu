@@ -103,8 +103,11 @@ struct Trace {
 Trace g_trace;
 }  // namespace
 
-static void trace_mark(const char* label, cudaStream_t st) {
+void gb::trace_mark(const char* label, cudaStream_t st) {
     if (!g_trace.on) return;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
+        return;
     std::lock_guard<std::mutex> lock(g_trace.mu);
     if (!g_trace.on || g_trace.used >= (int)g_trace.ev.size()) return;
     if (cudaEventRecord(g_trace.ev[g_trace.used], st) != cudaSuccess) return;

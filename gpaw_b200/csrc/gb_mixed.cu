@@ -416,6 +416,7 @@ static int vcycle32(gb_mixed* m, int l, cudaStream_t st) {
                 else s7.cm[ax] = op->st.coef[c];
             }
         }
+        trace_mark("coarsest: FP64 Chebyshev solve", st);
         if (seven && n <= CLUSTER_COARSE_MAX) {
             const int chunk = (int)((n + CL - 1) / CL);
             const size_t smem = (size_t)2 * chunk * sizeof(double);
@@ -452,24 +453,40 @@ static int vcycle32(gb_mixed* m, int l, cudaStream_t st) {
     const ChebLevel& c = m->ch[l];
     float *b = m->b[l], *e = m->e[l], *t = m->t[l];
     int rc;
+    static const char* const lbl[][6] = {
+        {"L0 pre-smooth", "L0 residual", "L0 restrict", "L0 interpolate", "L0 post-smooth 1",
+         "L0 post-smooth 2 (phi += e)"},
+        {"L1 pre-smooth", "L1 residual", "L1 restrict", "L1 interpolate", "L1 post-smooth 1",
+         "L1 post-smooth 2"},
+        {"L2 pre-smooth", "L2 residual", "L2 restrict", "L2 interpolate", "L2 post-smooth 1",
+         "L2 post-smooth 2"},
+        {"L3+ pre-smooth", "L3+ residual", "L3+ restrict", "L3+ interpolate",
+         "L3+ post-smooth 1", "L3+ post-smooth 2"}};
+    const char* const* lb = lbl[l < 3 ? l : 3];
     // pre-smooth from zero
+    trace_mark(lb[0], st);
     if ((rc = lin<float>(op, b, e, nullptr, nullptr, 0, c.pre_u, c.pre_Lu, 0, nullptr, nullptr,
                          nullptr, st)))
         return rc;
     // residual t = b - A e, restricted to the next level
+    trace_mark(lb[1], st);
     if ((rc = lin<float>(op, e, t, b, nullptr, 1.0, 0.0, -1.0, 0, nullptr, nullptr, nullptr, st)))
         return rc;
     Phases P{};
+    trace_mark(lb[2], st);
     if ((rc = transform_impl(m->rst[l], t, m->b[l + 1], nullptr, 1, GB_F32_INTERNAL, P, 0, 0, 0.0, st)))
         return rc;
     if ((rc = vcycle32(m, l + 1, st))) return rc;
     // e += I(e_{l+1})   (as e -= I(-e_{l+1}), negation exact)
+    trace_mark(lb[3], st);
     if ((rc = transform_impl(m->itp[l], m->e[l + 1], e, nullptr, 1, GB_F32_INTERNAL, P, 1, 1, 0.0, st)))
         return rc;
     // post-smooth: t = (b - A e) / (theta c0); e += k1 t - k2 A t
+    trace_mark(lb[4], st);
     if ((rc = lin<float>(op, e, t, b, nullptr, c.inv_tc0, 0.0, -c.inv_tc0, 0, nullptr, nullptr,
                          nullptr, st)))
         return rc;
+    trace_mark(lb[5], st);
     if (l == 0)
         rc = lin<float>(op, t, e, nullptr, e, 0, c.k1, -c.k2, 1.0, m->phi0, nullptr, nullptr, st);
     else
@@ -479,11 +496,14 @@ static int vcycle32(gb_mixed* m, int l, cudaStream_t st) {
 
 // d = rho - L64 phi  ->  b[0] (float) and |d|^2 -> nrm[0]
 static int defect(gb_mixed* m, cudaStream_t st) {
+    trace_mark("FP64 defect d = rho - L phi, |d|^2", st);
     if (int rc = lin<double>(m->op64, m->phi0, nullptr, m->rho0, nullptr, 1.0, 0.0, -1.0, 0,
                              nullptr, m->b[0], m->partial, st))
         return rc;
+    trace_mark("FP64 defect norm reduction", st);
     launch_reduce_partials(m->partial, m->nres, 1, 1.0, m->nrm, st);
     GB_LAUNCH_CHECK();
+    trace_mark("end of defect", st);
     return 0;
 }
 
@@ -657,6 +677,22 @@ extern "C" int gb_mixed_result(gb_mixed* m, int* niter, double* rel_residual) {
     if (m->ctl_host->rel > m->last_tol)
         return fail(GB_ENOCONV, "mixed-precision Poisson solver did not reach %g in %d V-cycles",
                     m->last_tol, m->last_maxiter);
+    return 0;
+}
+
+// One V-cycle and its defect launched kernel by kernel (no graph), for
+// profilers and kernel traces: phi <- phi + V32(rho - L phi).
+extern "C" int gb_mixed_vcycle_eager(gb_mixed* m, double* phi, const double* rho,
+                                     void* stream) {
+    if (!m || !phi || !rho) return fail(GB_EINVAL, "mixed vcycle: NULL argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t bytes = (size_t)m->op64->ng() * sizeof(double);
+    GB_CUDA_TRY(cudaMemcpyAsync(m->rho0, rho, bytes, cudaMemcpyDeviceToDevice, st));
+    GB_CUDA_TRY(cudaMemcpyAsync(m->phi0, phi, bytes, cudaMemcpyDeviceToDevice, st));
+    if (int rc = defect(m, st)) return rc;
+    if (int rc = vcycle32(m, 0, st)) return rc;
+    if (int rc = defect(m, st)) return rc;
+    GB_CUDA_TRY(cudaMemcpyAsync(phi, m->phi0, bytes, cudaMemcpyDeviceToDevice, st));
     return 0;
 }
 

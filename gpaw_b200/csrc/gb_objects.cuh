@@ -21,6 +21,11 @@ constexpr int GB_F32_INTERNAL = 100;
 // Record the message of a failed call for gb_last_error(); returns code.
 int fail(int code, const char* fmt, ...);
 
+// While a kernel trace is open (gb_trace_begin), record an event on `st`
+// labelled with the kernel launched next; a no-op otherwise, and on a
+// stream that is being captured.
+void trace_mark(const char* label, cudaStream_t st);
+
 #define GB_CUDA_TRY(expr)                                                             \
     do {                                                                              \
         cudaError_t e_ = (expr);                                                      \

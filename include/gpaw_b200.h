@@ -141,8 +141,9 @@ GB_API int gb_device_fault(int* code);
 
 /* Kernel timeline of composite calls; a profiling aid with no counterpart
  * in the reference.  Between gb_trace_begin(capacity) and gb_trace_end,
- * gb_fd_precond records a CUDA event on its stream before each of its
- * kernels and one after the last (at most `capacity` events in all).
+ * gb_fd_precond and gb_mixed_vcycle_eager record a CUDA event on their
+ * stream before each of their kernels and one after the last (at most
+ * `capacity` events in all).
  * gb_trace_end waits for the last event and writes, for up to `max`
  * intervals, the milliseconds between consecutive events and the label of
  * the kernel each interval starts with; *count receives the number of
@@ -296,6 +297,11 @@ GB_API int gb_mixed_new(int nlevels, gb_operator* op64, gb_operator* const* oper
                         gb_transformer* const* interpolators, const double* lam_max,
                         double lam_min_coarse, int coarse_degree, gb_mixed** out);
 GB_API void gb_mixed_free(gb_mixed* m);
+/* One V-cycle of the mixed-precision solver and the defects around it,
+ * launched kernel by kernel instead of through the solver's graph:
+ * phi <- phi + V32(rho - L phi).  For profilers and kernel traces (its
+ * kernels carry gb_trace labels); no counterpart in the reference. */
+GB_API int gb_mixed_vcycle_eager(gb_mixed* m, double* phi, const double* rho, void* stream);
 
 /* Solve until ||rho - L phi|| / ||rho|| <= tol (both norms in FP64, on the
  * device), starting from phi; at most maxiter V-cycles (GB_ENOCONV
