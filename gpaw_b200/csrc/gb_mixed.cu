@@ -15,6 +15,8 @@
 // (coarsest) is solved in FP64 with a fixed-degree Chebyshev iteration over
 // the spectrum of D^-1 A, in one single-CTA kernel.  The whole loop runs on
 // the device: a CUDA graph with a conditional WHILE node.
+#include <cmath>
+#include <cstdlib>
 #include <vector>
 
 #include <cooperative_groups.h>
@@ -300,6 +302,99 @@ k_coarse_cheb_cluster(const float* __restrict__ b, float* __restrict__ e, GridBC
     }
 }
 
+// Exact solve of the coarsest level by fast diagonalisation.  A 7-point
+// operator with symmetric couplings, c0 x_p + sum_a c_a (x_{p+e_a} +
+// x_{p-e_a}), is c0 I + sum_a c_a T_a with T_a the 1-D neighbour matrix of
+// axis a (zero or periodic boundary), so it is diagonal in the tensor
+// product of the T_a's orthonormal eigenvectors Q_a (sine vectors for a
+// zero boundary, cosine/sine pairs for a periodic one):
+//     x = (Q0 x Q1 x Q2) diag(1 / lambda) (Q0 x Q1 x Q2)^T b,
+//     lambda_ijk = c0 + c_0 mu0_i + c_1 mu1_j + c_2 mu2_k.
+// Six passes of small dense products along one axis each, in FP64, by one
+// CTA with the grid (two copies), the Q_a and mu_a in shared memory.  A
+// lambda that vanishes (the constant mode of a fully periodic grid) is
+// left out, as the neutral problem's mean is free.  `tab` holds Q0, Q1,
+// Q2 (row j, column k = component j of eigenvector k), then mu0, mu1, mu2.
+__global__ void __launch_bounds__(1024, 1)
+k_coarse_direct(const float* __restrict__ b, float* __restrict__ e, const double* __restrict__ tab,
+                int n0, int n1, int n2, double c0, double ca0, double ca1, double ca2) {
+    extern __shared__ __align__(16) double smd[];
+    const int n = n0 * n1 * n2;
+    const int ntab = n0 * n0 + n1 * n1 + n2 * n2 + n0 + n1 + n2;
+    double* A = smd;
+    double* B = A + n;
+    double* T = B + n;
+    const double* Q0 = T;
+    const double* Q1 = Q0 + n0 * n0;
+    const double* Q2 = Q1 + n1 * n1;
+    const double* mu0 = Q2 + n2 * n2;
+    const double* mu1 = mu0 + n0;
+    const double* mu2 = mu1 + n1;
+    for (int p = threadIdx.x; p < ntab; p += blockDim.x) T[p] = tab[p];
+    for (int p = threadIdx.x; p < n; p += blockDim.x) A[p] = (double)b[p];
+    __syncthreads();
+    // y = M^T x (fwd) or y = M x along one axis: `len` points apart by
+    // `stride`; the point's coordinate along the axis is (p / stride) % len
+    auto pass = [&](const double* src, double* dst, const double* M, int len, int stride,
+                    bool fwd) {
+        for (int p = threadIdx.x; p < n; p += blockDim.x) {
+            const int k = (p / stride) % len;
+            const double* col = src + (p - k * stride);
+            double acc = 0.0;
+            for (int j = 0; j < len; j++)
+                acc += (fwd ? M[j * len + k] : M[k * len + j]) * col[j * stride];
+            dst[p] = acc;
+        }
+        __syncthreads();
+    };
+    pass(A, B, Q2, n2, 1, true);
+    pass(B, A, Q1, n1, n2, true);
+    pass(A, B, Q0, n0, n1 * n2, true);
+    double lmax = fabs(c0) + 2.0 * (fabs(ca0) + fabs(ca1) + fabs(ca2));
+    for (int p = threadIdx.x; p < n; p += blockDim.x) {
+        const int k2 = p % n2, k1 = (p / n2) % n1, k0 = p / (n1 * n2);
+        const double lam = c0 + ca0 * mu0[k0] + ca1 * mu1[k1] + ca2 * mu2[k2];
+        B[p] = fabs(lam) > 1e-12 * lmax ? B[p] / lam : 0.0;
+    }
+    __syncthreads();
+    pass(B, A, Q0, n0, n1 * n2, false);
+    pass(A, B, Q1, n1, n2, false);
+    pass(B, A, Q2, n2, 1, false);
+    for (int p = threadIdx.x; p < n; p += blockDim.x) e[p] = (float)A[p];
+}
+
+// Orthonormal eigenvectors (columns of Q, n x n, row-major) and eigenvalues
+// of the 1-D neighbour matrix of an axis of n points: (T x)_j = x_{j+1} +
+// x_{j-1}, zero past the ends or wrapped.
+static void neighbour_eigen(int n, bool periodic, double* Q, double* mu) {
+    const double pi = 3.14159265358979323846;
+    if (!periodic) {
+        const double s = std::sqrt(2.0 / (n + 1));
+        for (int k = 0; k < n; k++) {
+            mu[k] = 2.0 * std::cos(pi * (k + 1) / (n + 1));
+            for (int j = 0; j < n; j++) Q[j * n + k] = s * std::sin(pi * (j + 1) * (k + 1) / (n + 1));
+        }
+        return;
+    }
+    // periodic: constant, cosine/sine pairs, and the alternating vector
+    int col = 0;
+    const double c = 1.0 / std::sqrt((double)n), s2 = std::sqrt(2.0 / n);
+    for (int j = 0; j < n; j++) Q[j * n + col] = c;
+    mu[col++] = 2.0;
+    for (int k = 1; 2 * k < n; k++) {
+        for (int j = 0; j < n; j++) {
+            Q[j * n + col] = s2 * std::cos(2 * pi * k * j / n);
+            Q[j * n + col + 1] = s2 * std::sin(2 * pi * k * j / n);
+        }
+        mu[col] = mu[col + 1] = 2.0 * std::cos(2 * pi * k / n);
+        col += 2;
+    }
+    if (n % 2 == 0 && n > 1) {
+        for (int j = 0; j < n; j++) Q[j * n + col] = (j % 2 ? -c : c);
+        mu[col++] = -2.0;
+    }
+}
+
 __global__ void k_sumsq(const double* __restrict__ a, long long n, double* __restrict__ partial) {
     double v = 0.0;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
@@ -338,6 +433,8 @@ struct gb_mixed {
     std::vector<ChebLevel> ch;
     double coarse_lo = 0, coarse_hi = 0;
     int coarse_deg = 0;
+    double* direct_tab = nullptr;   // eigen tables of the exact coarsest solve
+    Seven direct_s7{};
     double last_tol = 0.0;
     int last_maxiter = 0;
     std::vector<float*> b, e, t;       // levels 0..L (b[L], e[L] used at L)
@@ -356,6 +453,7 @@ struct gb_mixed {
         for (float* p : b) cudaFree(p);
         for (float* p : e) cudaFree(p);
         for (float* p : t) cudaFree(p);
+        cudaFree(direct_tab);
         cudaFree(x);
         cudaFree(r);
         cudaFree(da);
@@ -415,6 +513,18 @@ static int vcycle32(gb_mixed* m, int l, cudaStream_t st) {
                 else if (dir > 0) s7.cp[ax] = op->st.coef[c];
                 else s7.cm[ax] = op->st.coef[c];
             }
+        }
+        if (m->direct_tab) {
+            const GridBC& g = op->g;
+            const size_t smem = ((size_t)2 * n + (size_t)g.n[0] * g.n[0] + (size_t)g.n[1] * g.n[1] +
+                                 (size_t)g.n[2] * g.n[2] + g.n[0] + g.n[1] + g.n[2]) *
+                                sizeof(double);
+            trace_mark("coarsest: FP64 exact solve", st);
+            k_coarse_direct<<<1, 1024, smem, st>>>(m->b[l], m->e[l], m->direct_tab, g.n[0], g.n[1],
+                                                   g.n[2], m->direct_s7.c0, m->direct_s7.cp[0],
+                                                   m->direct_s7.cp[1], m->direct_s7.cp[2]);
+            GB_LAUNCH_CHECK();
+            return 0;
         }
         trace_mark("coarsest: FP64 Chebyshev solve", st);
         if (seven && n <= CLUSTER_COARSE_MAX) {
@@ -507,6 +617,58 @@ static int defect(gb_mixed* m, cudaStream_t st) {
     return 0;
 }
 
+// The exact coarsest solve when the coarsest operator is a symmetric
+// 7-point stencil and the grid, two copies of it and the eigen tables fit
+// in one CTA's shared memory (GPAW_B200_COARSE_DIRECT=0 keeps the
+// Chebyshev iteration).
+static int setup_direct(gb_mixed* m) {
+    const char* env = getenv("GPAW_B200_COARSE_DIRECT");
+    if (env && atoi(env) == 0) return 0;
+    gb_operator* op = m->ops[m->L];
+    if (!(op->st.ncoefs == 7 && op->st.range == 1 && op->st.cfd)) return 0;
+    Seven s7{};
+    for (int c = 0; c < 7; c++) {
+        int ax = -1, dir = 0;
+        for (int a = 0; a < 3; a++)
+            if (op->st.off[c][a]) {
+                ax = a;
+                dir = op->st.off[c][a];
+            }
+        if (ax < 0) s7.c0 += op->st.coef[c];
+        else if (dir > 0) s7.cp[ax] = op->st.coef[c];
+        else s7.cm[ax] = op->st.coef[c];
+    }
+    for (int a = 0; a < 3; a++)
+        if (s7.cp[a] != s7.cm[a]) return 0;
+    const GridBC& g = op->g;
+    const long long n = op->ng();
+    const long long ntab = (long long)g.n[0] * g.n[0] + (long long)g.n[1] * g.n[1] +
+                           (long long)g.n[2] * g.n[2] + g.n[0] + g.n[1] + g.n[2];
+    const size_t smem = (size_t)(2 * n + ntab) * sizeof(double);
+    if (smem > 225 * 1024) return 0;
+    std::vector<double> tab(ntab);
+    double* q = tab.data();
+    double* mu = q + (long long)g.n[0] * g.n[0] + (long long)g.n[1] * g.n[1] +
+                 (long long)g.n[2] * g.n[2];
+    for (int a = 0; a < 3; a++) {
+        neighbour_eigen(g.n[a], g.periodic[a] != 0, q, mu);
+        q += (long long)g.n[a] * g.n[a];
+        mu += g.n[a];
+    }
+    static bool attr = false;
+    if (!attr) {
+        GB_CUDA_TRY(cudaFuncSetAttribute(k_coarse_direct,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         225 * 1024));
+        attr = true;
+    }
+    GB_CUDA_TRY(cudaMalloc(&m->direct_tab, ntab * sizeof(double)));
+    GB_CUDA_TRY(cudaMemcpy(m->direct_tab, tab.data(), ntab * sizeof(double),
+                           cudaMemcpyHostToDevice));
+    m->direct_s7 = s7;
+    return 0;
+}
+
 extern "C" int gb_mixed_new(int nlevels, gb_operator* op64, gb_operator* const* operators,
                             gb_transformer* const* restrictors,
                             gb_transformer* const* interpolators, const double* lam_max,
@@ -549,6 +711,10 @@ extern "C" int gb_mixed_new(int nlevels, gb_operator* op64, gb_operator* const* 
     m->coarse_hi = 1.02 * lam_max[m->L];
     m->coarse_lo = lam_min_coarse;
     m->coarse_deg = coarse_degree;
+    if (int rc = setup_direct(m)) {
+        delete m;
+        return rc;
+    }
     cudaError_t ce = cudaSuccess;
     for (int l = 0; l <= m->L && ce == cudaSuccess; l++) {
         const size_t bytes = (size_t)m->ops[l]->ng() * sizeof(float);
