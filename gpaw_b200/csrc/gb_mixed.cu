@@ -617,13 +617,15 @@ static int defect(gb_mixed* m, cudaStream_t st) {
     return 0;
 }
 
-// The exact coarsest solve when the coarsest operator is a symmetric
-// 7-point stencil and the grid, two copies of it and the eigen tables fit
-// in one CTA's shared memory (GPAW_B200_COARSE_DIRECT=0 keeps the
-// Chebyshev iteration).
+// The exact coarsest solve, opt-in (GPAW_B200_COARSE_DIRECT=1), when the
+// coarsest operator is a symmetric 7-point stencil and the grid, two copies
+// of it and the eigen tables fit in one CTA's shared memory.  Measured on
+// the 192^3 grid with 4 levels (coarsest 23^3): 144 us a solve against
+// 75 us for the Chebyshev iteration (shared-memory bound on one SM), and
+// 14 V-cycles instead of 15, so the Chebyshev iteration stays the default.
 static int setup_direct(gb_mixed* m) {
     const char* env = getenv("GPAW_B200_COARSE_DIRECT");
-    if (env && atoi(env) == 0) return 0;
+    if (!env || atoi(env) == 0) return 0;
     gb_operator* op = m->ops[m->L];
     if (!(op->st.ncoefs == 7 && op->st.range == 1 && op->st.cfd)) return 0;
     Seven s7{};
