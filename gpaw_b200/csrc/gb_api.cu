@@ -82,9 +82,12 @@ int gb::make_plane_map16(CUtensorMap* map, const void* base, long long nb, int n
 extern "C" int gb_device_fault(int* code) {
     if (!code) return fail(GB_EINVAL, "device_fault: NULL argument");
     *code = 0;
-    int c = 0;
-    if (take_fault_transform(&c)) return fail(GB_ECUDA, "device_fault: cannot read the flag");
-    if (c) *code = c;
+    int (*units[])(int*) = {take_fault_transform, take_fault_cfd, take_fault_mixed};
+    for (auto take : units) {
+        int c = 0;
+        if (take(&c)) return fail(GB_ECUDA, "device_fault: cannot read the flag");
+        if (c && !*code) *code = c;
+    }
     return 0;
 }
 

@@ -158,7 +158,10 @@ __device__ __forceinline__ T add_direction(T x, const double* cp, const double* 
 // Directions are summed in the order GUCLaplace builds for an orthorhombic
 // cell: axis 2, axis 1, axis 0.  ORD = 1: every product and sum rounded on
 // its own (bit-identical to the reference); ORD = 2: fused multiply-adds
-// (fewer instructions, results within a few ulp; opt-in, apply only).
+// (fewer instructions, results within a few ulp; opt-in, apply only);
+// ORD = 3: fused multiply-adds into one partial sum a direction, the three
+// added at the end (the mixed-precision solver's own passes, EPI_LIN, whose
+// results are checked by tolerance: shorter dependency chains).
 // Register caps: three resident CTAs of 256 threads for the complex apply
 // (nn <= 3), two for the other complex modes, four CTAs of 128 threads for
 // real data.
@@ -519,6 +522,20 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
                 // x = 0; x += v c in coefficient order (Jacobi skips c0)
                 T x = Num<T>::zero();
                 if (MODE != EPI_JACOBI) x = Num<T>::add(x, Num<T>::scale(vc, cs.c0));
+                if constexpr (ORD == 3) {
+                    // three independent fused sums, one a direction, added
+                    // at the end: a third of the serial dependency chain
+                    T x1 = add_direction<T, NN, true>(Num<T>::zero(), cs.cp[1], cs.cm[1],
+                                         [&](int d) { return colp[(r + NN + d) * PX]; },
+                                         [&](int d) { return colp[(r + NN - d) * PX]; });
+                    T x0 = add_direction<T, NN, true>(Num<T>::zero(), cs.cp[2], cs.cm[2],
+                                         [&](int d) { return q[r][(CU + d) % Q]; },
+                                         [&](int d) { return q[r][(CU + Q - d) % Q]; });
+                    x = add_direction<T, NN, true>(x, cs.cp[0], cs.cm[0],
+                                         [&](int d) { return row[d]; },
+                                         [&](int d) { return row[-d]; });
+                    x = Num<T>::add(Num<T>::add(x, x1), x0);
+                } else {
                 // directions: axis 2, axis 1, axis 0 (GUCLaplace's order)
                 x = add_direction<T, NN, ORD == 2>(x, cs.cp[0], cs.cm[0],
                                          [&](int d) { return row[d]; },
@@ -529,6 +546,7 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
                 x = add_direction<T, NN, ORD == 2>(x, cs.cp[2], cs.cm[2],
                                          [&](int d) { return q[r][(CU + d) % Q]; },
                                          [&](int d) { return q[r][(CU + Q - d) % Q]; });
+                }
                 const int gy = y0 + ty0 + r;
                 if (gx < n2 && gy < n1) {
                     const long long at = p * pstride + colr[r];
@@ -583,6 +601,8 @@ k_fd_cfd(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phase
             ep.partial[((long long)b * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = sq;
     }
 }
+
+int take_fault_cfd(int* code) { return take_unit_fault(code); }
 
 // The halo cells past a periodic edge in the busiest tile (what the TMA
 // variant of k_fd_cfd deals to its threads; the same count as the kernel's).
@@ -702,10 +722,11 @@ static int launch_cfd_nn(const void* in, void* out, int nin, const GridBC& g, co
         // float64: 32 x 8 tiles of two rows a thread (128 threads, more
         // CTAs an SM) measured faster than 32 x 16 tiles (nn = 3 apply
         // 14 %, preconditioner 9 %, FP64 V-cycles 3-7 %)
+        constexpr int ORDL = MODE == EPI_LIN ? 3 : 1;
         if constexpr (sizeof(T) == 8)
-            return launch_cfd_t<T, NN, 32, 8, 2, D, MODE, 1, 0, 4>(in, out, nin, g, P, cs, ep, st,
-                                                                   nblk);
-        return launch_cfd_t<T, NN, 32, 16, RY, D, MODE, 1, 0, 512 / (32 * (16 / RY))>(
+            return launch_cfd_t<T, NN, 32, 8, 2, D, MODE, ORDL, 0, 4>(in, out, nin, g, P, cs, ep,
+                                                                      st, nblk);
+        return launch_cfd_t<T, NN, 32, 16, RY, D, MODE, ORDL, 0, 512 / (32 * (16 / RY))>(
             in, out, nin, g, P, cs, ep, st, nblk);
     }
 }

@@ -113,5 +113,7 @@ int cfd_blocks(const GridBC& g, int nn, int elem_bytes, int nin, int chunk = 0);
 int cfd_chunk(const GridBC& g, int nn, int nin, int ty);
 // read and clear the device fault flag of a kernel file (bounded waits)
 int take_fault_transform(int* code);
+int take_fault_cfd(int* code);
+int take_fault_mixed(int* code);
 
 }  // namespace gb

@@ -17,11 +17,13 @@
 // the device: a CUDA graph with a conditional WHILE node.
 #include <cmath>
 #include <cstdlib>
+#include <cstring>
 #include <vector>
 
 #include <cooperative_groups.h>
 
 #include "gb_objects.cuh"
+#include "gb_tma.cuh"
 
 using namespace gb;
 
@@ -395,6 +397,261 @@ static void neighbour_eigen(int n, bool periodic, double* Q, double* mu) {
     }
 }
 
+// ------------------------------------------------ coarse levels in one kernel
+// The FP32 V-cycle below level 0 -- smoothing, residual, restriction and
+// interpolation of every level from `lc` down, and the exact coarsest
+// solve -- as ONE cooperative kernel: every pass is a grid-stride loop over
+// the level's points (FP32 7-point operator, K = 2 transfers, each output
+// formed from its neighbourhood directly), and the passes are separated by
+// a grid-wide barrier instead of a kernel boundary.  On these small, L2-
+// resident levels a kernel boundary costs more than the work it separates.
+// Same passes and coefficients as the per-level kernels of vcycle32.
+constexpr int CV_MAX = 12;
+struct CoopLevel {
+    int n[3], per[3], ng;
+    float c0, cp[3], cm[3];            // the level's 7-point operator
+    float pre_u, pre_Lu, inv_tc0, k1, k2;
+    float *b, *e, *t;
+    int rplo[3];                       // restriction to the next level
+    float rw;
+    int iplo[3], iskip[3];             // interpolation from the next level
+    float iw;
+};
+struct CoopPlan {
+    int nl;                            // levels lc .. L (the last is the coarsest)
+    CoopLevel lv[CV_MAX];
+    const double* tab;                 // eigen tables of the coarsest level
+    double *X, *Y;                     // coarsest-level FP64 work grids
+    double dc0, dca[3];                // coarsest operator (FP64)
+    unsigned* bar;                     // grid barrier: arrivals, generation
+};
+
+// Grid-wide barrier of a cooperative launch (all CTAs resident), bounded by
+// one second: a barrier that runs out records a device fault and the
+// kernel gives up (its output is then not valid).
+__device__ __forceinline__ bool coop_sync(unsigned* bar, bool ok) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        s_ok = ok;
+        if (ok) {
+            volatile unsigned* gen = bar + 1;
+            const unsigned g = *gen;
+            __threadfence();
+            if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+                atomicExch(bar, 0u);
+                __threadfence();
+                atomicAdd(bar + 1, 1u);
+            } else {
+                const uint64_t t0 = global_ns();
+                while (*gen == g) {
+                    if (global_ns() - t0 > 1000000000ull) {
+                        atomicCAS(&g_device_fault, 0, GB_FAULT_TMA_TIMEOUT);
+                        s_ok = 0;
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+            }
+            __threadfence();
+        }
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+__device__ __forceinline__ int cv_at(int j, int n, int per) {
+    if (j >= 0 && j < n) return j;
+    if (!per) return -1;
+    j = j < 0 ? j + n : j - n;
+    return (j >= 0 && j < n) ? j : -1;
+}
+
+// A x at point p = (i0, i1, i2) of level L (reads bypass L1: other CTAs
+// wrote x before the last barrier)
+__device__ __forceinline__ float cv_apply(const float* x, const CoopLevel& L, int p, int i0,
+                                          int i1, int i2) {
+    const int s1 = L.n[2], s0 = L.n[1] * L.n[2];
+    auto nb = [&](int i, int n, int per, int s, int d) -> float {
+        const int j = cv_at(i + d, n, per);
+        return j < 0 ? 0.0f : __ldcg(x + p + (j - i) * s);
+    };
+    float y = L.c0 * __ldcg(x + p);
+    y += L.cp[2] * nb(i2, L.n[2], L.per[2], 1, 1) + L.cm[2] * nb(i2, L.n[2], L.per[2], 1, -1);
+    y += L.cp[1] * nb(i1, L.n[1], L.per[1], s1, 1) + L.cm[1] * nb(i1, L.n[1], L.per[1], s1, -1);
+    y += L.cp[0] * nb(i0, L.n[0], L.per[0], s0, 1) + L.cm[0] * nb(i0, L.n[0], L.per[0], s0, -1);
+    return y;
+}
+
+__device__ __forceinline__ void cv_split(int p, const int n[3], int& i0, int& i1, int& i2) {
+    i2 = p % n[2];
+    const int q = p / n[2];
+    i1 = q % n[1];
+    i0 = q / n[1];
+}
+
+__global__ void __launch_bounds__(512)
+k_coop_vcycle(const __grid_constant__ CoopPlan P) {
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nth = gridDim.x * blockDim.x;
+    bool ok = true;
+    const int nl = P.nl;
+    // descent: pre-smooth, residual, restriction
+    for (int l = 0; l + 1 < nl && ok; l++) {
+        const CoopLevel& L = P.lv[l];
+        const CoopLevel& C = P.lv[l + 1];
+        for (int p = tid; p < L.ng; p += nth) {
+            int i0, i1, i2;
+            cv_split(p, L.n, i0, i1, i2);
+            L.e[p] = L.pre_u * __ldcg(L.b + p) + L.pre_Lu * cv_apply(L.b, L, p, i0, i1, i2);
+        }
+        ok = coop_sync(P.bar, ok);
+        for (int p = tid; p < L.ng; p += nth) {
+            int i0, i1, i2;
+            cv_split(p, L.n, i0, i1, i2);
+            L.t[p] = __ldcg(L.b + p) - cv_apply(L.e, L, p, i0, i1, i2);
+        }
+        ok = coop_sync(P.bar, ok);
+        // restriction: 0.5 (a + w (a+ + a-)) along each axis, centre 2I+1-plo
+        for (int q = tid; q < C.ng; q += nth) {
+            int I0, I1, I2;
+            cv_split(q, C.n, I0, I1, I2);
+            const int c[3] = {2 * I0 + 1 - L.rplo[0], 2 * I1 + 1 - L.rplo[1],
+                              2 * I2 + 1 - L.rplo[2]};
+            int idx[3][3];
+            float wt[3][3];
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+#pragma unroll
+                for (int d = -1; d <= 1; d++) {
+                    idx[a][d + 1] = cv_at(c[a] + d, L.n[a], L.per[a]);
+                    wt[a][d + 1] = d == 0 ? 0.5f : 0.5f * L.rw;
+                }
+            }
+            float acc = 0.0f;
+#pragma unroll
+            for (int d0 = 0; d0 < 3; d0++) {
+                if (idx[0][d0] < 0) continue;
+#pragma unroll
+                for (int d1 = 0; d1 < 3; d1++) {
+                    if (idx[1][d1] < 0) continue;
+                    const float w01 = wt[0][d0] * wt[1][d1];
+                    const float* row = L.t + (idx[0][d0] * L.n[1] + idx[1][d1]) * L.n[2];
+#pragma unroll
+                    for (int d2 = 0; d2 < 3; d2++)
+                        if (idx[2][d2] >= 0) acc += w01 * wt[2][d2] * __ldcg(row + idx[2][d2]);
+                }
+            }
+            C.b[q] = acc;
+        }
+        ok = coop_sync(P.bar, ok);
+    }
+    // coarsest level: exact solve by fast diagonalisation (FP64)
+    if (ok) {
+        const CoopLevel& L = P.lv[nl - 1];
+        const int n0 = L.n[0], n1 = L.n[1], n2 = L.n[2], n = L.ng;
+        const double* Q0 = P.tab;
+        const double* Q1 = Q0 + n0 * n0;
+        const double* Q2 = Q1 + n1 * n1;
+        const double* mu0 = Q2 + n2 * n2;
+        const double* mu1 = mu0 + n0;
+        const double* mu2 = mu1 + n1;
+        for (int p = tid; p < n; p += nth) P.X[p] = (double)__ldcg(L.b + p);
+        ok = coop_sync(P.bar, ok);
+        auto pass = [&](const double* src, double* dst, const double* M, int len, int stride,
+                        bool fwd) {
+            for (int p = tid; p < n; p += nth) {
+                const int k = (p / stride) % len;
+                const double* col = src + (p - k * stride);
+                double acc = 0.0;
+                for (int j = 0; j < len; j++)
+                    acc += (fwd ? __ldg(M + j * len + k) : __ldg(M + k * len + j)) *
+                           __ldcg(col + j * stride);
+                dst[p] = acc;
+            }
+            return coop_sync(P.bar, ok);
+        };
+        if (ok) ok = pass(P.X, P.Y, Q2, n2, 1, true);
+        if (ok) ok = pass(P.Y, P.X, Q1, n1, n2, true);
+        if (ok) ok = pass(P.X, P.Y, Q0, n0, n1 * n2, true);
+        const double lmax = fabs(P.dc0) + 2.0 * (fabs(P.dca[0]) + fabs(P.dca[1]) + fabs(P.dca[2]));
+        for (int p = tid; p < n && ok; p += nth) {
+            const int k2 = p % n2, k1 = (p / n2) % n1, k0 = p / (n1 * n2);
+            const double lam = P.dc0 + P.dca[0] * __ldg(mu0 + k0) + P.dca[1] * __ldg(mu1 + k1) +
+                               P.dca[2] * __ldg(mu2 + k2);
+            P.Y[p] = fabs(lam) > 1e-12 * lmax ? __ldcg(P.Y + p) / lam : 0.0;
+        }
+        ok = coop_sync(P.bar, ok);
+        if (ok) ok = pass(P.Y, P.X, Q0, n0, n1 * n2, false);
+        if (ok) ok = pass(P.X, P.Y, Q1, n1, n2, false);
+        if (ok) ok = pass(P.Y, P.X, Q2, n2, 1, false);
+        for (int p = tid; p < n && ok; p += nth) L.e[p] = (float)__ldcg(P.X + p);
+        ok = coop_sync(P.bar, ok);
+    }
+    // ascent: interpolation, post-smoothing
+    for (int l = nl - 2; l >= 0 && ok; l--) {
+        const CoopLevel& L = P.lv[l];
+        const CoopLevel& C = P.lv[l + 1];
+        // e += I(e_{l+1}): per axis the even fine points copy, the odd ones
+        // are w (a(k) + a(k+1)), k = (f + skip) / 2 - plo
+        for (int p = tid; p < L.ng; p += nth) {
+            int f[3];
+            cv_split(p, L.n, f[0], f[1], f[2]);
+            int idx[3][2];
+            float wt[3][2];
+#pragma unroll
+            for (int a = 0; a < 3; a++) {
+                const int u = f[a] + L.iskip[a];
+                const int k = (u >> 1) - L.iplo[a];
+                idx[a][0] = cv_at(k, C.n[a], C.per[a]);
+                if (u & 1) {
+                    idx[a][1] = cv_at(k + 1, C.n[a], C.per[a]);
+                    wt[a][0] = wt[a][1] = L.iw;
+                } else {
+                    idx[a][1] = -1;
+                    wt[a][0] = 1.0f;
+                    wt[a][1] = 0.0f;
+                }
+            }
+            float acc = 0.0f;
+#pragma unroll
+            for (int d0 = 0; d0 < 2; d0++) {
+                if (idx[0][d0] < 0) continue;
+#pragma unroll
+                for (int d1 = 0; d1 < 2; d1++) {
+                    if (idx[1][d1] < 0) continue;
+                    const float w01 = wt[0][d0] * wt[1][d1];
+                    const float* row = C.e + (idx[0][d0] * C.n[1] + idx[1][d1]) * C.n[2];
+#pragma unroll
+                    for (int d2 = 0; d2 < 2; d2++)
+                        if (idx[2][d2] >= 0) acc += w01 * wt[2][d2] * __ldcg(row + idx[2][d2]);
+                }
+            }
+            L.e[p] = __ldcg(L.e + p) + acc;
+        }
+        ok = coop_sync(P.bar, ok);
+        for (int p = tid; p < L.ng; p += nth) {
+            int i0, i1, i2;
+            cv_split(p, L.n, i0, i1, i2);
+            L.t[p] = L.inv_tc0 * (__ldcg(L.b + p) - cv_apply(L.e, L, p, i0, i1, i2));
+        }
+        ok = coop_sync(P.bar, ok);
+        for (int p = tid; p < L.ng; p += nth) {
+            int i0, i1, i2;
+            cv_split(p, L.n, i0, i1, i2);
+            L.e[p] = __ldcg(L.e + p) + L.k1 * __ldcg(L.t + p) -
+                     L.k2 * cv_apply(L.t, L, p, i0, i1, i2);
+        }
+        ok = coop_sync(P.bar, ok);
+    }
+}
+
+}  // namespace
+
+int gb::take_fault_mixed(int* code) { return take_unit_fault(code); }
+
+namespace {
+
 __global__ void k_sumsq(const double* __restrict__ a, long long n, double* __restrict__ partial) {
     double v = 0.0;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
@@ -435,6 +692,11 @@ struct gb_mixed {
     int coarse_deg = 0;
     double* direct_tab = nullptr;   // eigen tables of the exact coarsest solve
     Seven direct_s7{};
+    // levels lc .. L as one cooperative kernel (coop = 0: per-level kernels)
+    int coop = 0, lc = 0, coop_grid = 0;
+    CoopPlan coop_plan{};
+    double* coop_tab = nullptr;
+    unsigned* coop_bar = nullptr;
     double last_tol = 0.0;
     int last_maxiter = 0;
     std::vector<float*> b, e, t;       // levels 0..L (b[L], e[L] used at L)
@@ -454,6 +716,8 @@ struct gb_mixed {
         for (float* p : e) cudaFree(p);
         for (float* p : t) cudaFree(p);
         cudaFree(direct_tab);
+        cudaFree(coop_tab);
+        cudaFree(coop_bar);
         cudaFree(x);
         cudaFree(r);
         cudaFree(da);
@@ -494,7 +758,27 @@ static int lin(gb_operator* op, const T* in, T* out, const T* aux, const T* aux2
 
 // V-cycle on levels l..L for the FP32 right-hand side b[l]; at level 0 the
 // final correction is added to phi0 (FP64).
+// Set while a batch of solvers is captured: its branches run side by side,
+// and cooperative kernels (which need the whole GPU resident at once) would
+// serialise them, so the batch keeps the per-level kernels.
+static thread_local bool t_no_coop = false;
+
 static int vcycle32(gb_mixed* m, int l, cudaStream_t st) {
+    if (m->coop && !t_no_coop && l == m->lc) {
+        trace_mark("levels lc..L: one cooperative kernel", st);
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(m->coop_grid);
+        cfg.blockDim = dim3(512);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = st;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeCooperative;
+        at[0].val.cooperative = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        GB_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_coop_vcycle, m->coop_plan));
+        return 0;
+    }
     if (l == m->L) {
         gb_operator* op = m->ops[l];
         const long long n = op->ng();
@@ -671,6 +955,109 @@ static int setup_direct(gb_mixed* m) {
     return 0;
 }
 
+// Levels from the first with at most COOP_MAX_POINTS points down to the
+// coarsest go into the cooperative kernel, when the coarsest operator is a
+// symmetric 7-point stencil (its exact solve needs the eigen tables) and
+// every level below 0 has the 7-point operator (what MixedPoissonSolver
+// builds).  GPAW_B200_COOP_COARSE=0 keeps the per-level kernels.
+constexpr long long COOP_MAX_POINTS = 2 << 20;
+
+static int setup_coop(gb_mixed* m) {
+    const char* env = getenv("GPAW_B200_COOP_COARSE");
+    if (env && atoi(env) == 0) return 0;
+    int lc = -1;
+    for (int l = 1; l <= m->L; l++)
+        if (m->ops[l]->ng() <= COOP_MAX_POINTS) {
+            lc = l;
+            break;
+        }
+    if (lc < 0 || m->L - lc + 1 > CV_MAX) return 0;
+    CoopPlan& P = m->coop_plan;
+    memset(&P, 0, sizeof P);
+    for (int l = lc; l <= m->L; l++) {
+        const gb_operator* op = m->ops[l];
+        if (!(op->st.ncoefs == 7 && op->st.range == 1 && op->st.cfd)) return 0;
+        Seven s7{};
+        for (int c = 0; c < 7; c++) {
+            int ax = -1, dir = 0;
+            for (int a = 0; a < 3; a++)
+                if (op->st.off[c][a]) {
+                    ax = a;
+                    dir = op->st.off[c][a];
+                }
+            if (ax < 0) s7.c0 += op->st.coef[c];
+            else if (dir > 0) s7.cp[ax] = op->st.coef[c];
+            else s7.cm[ax] = op->st.coef[c];
+        }
+        CoopLevel& V = P.lv[l - lc];
+        for (int a = 0; a < 3; a++) {
+            V.n[a] = op->g.n[a];
+            V.per[a] = op->g.periodic[a];
+            V.cp[a] = (float)s7.cp[a];
+            V.cm[a] = (float)s7.cm[a];
+        }
+        V.ng = (int)op->ng();
+        V.c0 = (float)s7.c0;
+        V.b = m->b[l];
+        V.e = m->e[l];
+        V.t = m->t[l];
+        if (l < m->L) {
+            const ChebLevel& c = m->ch[l];
+            V.pre_u = (float)c.pre_u;
+            V.pre_Lu = (float)c.pre_Lu;
+            V.inv_tc0 = (float)c.inv_tc0;
+            V.k1 = (float)c.k1;
+            V.k2 = (float)c.k2;
+            const gb_transformer* r = m->rst[l];
+            const gb_transformer* i = m->itp[l];
+            if (r->k != 2 || i->k != 2) return 0;
+            for (int a = 0; a < 3; a++) {
+                V.rplo[a] = r->G.plo[a];
+                V.iplo[a] = i->G.plo[a];
+                V.iskip[a] = i->G.skip0[a];
+            }
+            V.rw = (float)r->G.w[0];
+            V.iw = (float)i->G.w[0];
+        } else {
+            for (int a = 0; a < 3; a++)
+                if (s7.cp[a] != s7.cm[a]) return 0;
+            P.dc0 = s7.c0;
+            for (int a = 0; a < 3; a++) P.dca[a] = s7.cp[a];
+        }
+    }
+    // eigen tables of the coarsest level
+    const GridBC& g = m->ops[m->L]->g;
+    const long long ntab = (long long)g.n[0] * g.n[0] + (long long)g.n[1] * g.n[1] +
+                           (long long)g.n[2] * g.n[2] + g.n[0] + g.n[1] + g.n[2];
+    std::vector<double> tab(ntab);
+    double* q = tab.data();
+    double* mu = q + ntab - (g.n[0] + g.n[1] + g.n[2]);
+    for (int a = 0; a < 3; a++) {
+        neighbour_eigen(g.n[a], g.periodic[a] != 0, q, mu);
+        q += (long long)g.n[a] * g.n[a];
+        mu += g.n[a];
+    }
+    int per_sm = 0, dev = 0, nsm = 0;
+    GB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_coop_vcycle, 512, 0));
+    GB_CUDA_TRY(cudaGetDevice(&dev));
+    GB_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    if (per_sm < 1) return 0;
+    GB_CUDA_TRY(cudaMalloc(&m->coop_tab, ntab * sizeof(double)));
+    GB_CUDA_TRY(cudaMemcpy(m->coop_tab, tab.data(), ntab * sizeof(double),
+                           cudaMemcpyHostToDevice));
+    GB_CUDA_TRY(cudaMalloc(&m->coop_bar, 2 * sizeof(unsigned)));
+    GB_CUDA_TRY(cudaMemset(m->coop_bar, 0, 2 * sizeof(unsigned)));
+    P.nl = m->L - lc + 1;
+    P.tab = m->coop_tab;
+    P.X = m->x;
+    P.Y = m->r;
+    P.bar = m->coop_bar;
+    m->lc = lc;
+    m->coop_grid = std::min(per_sm, 2) * nsm;
+    m->coop = 1;
+    return 0;
+}
+
 extern "C" int gb_mixed_new(int nlevels, gb_operator* op64, gb_operator* const* operators,
                             gb_transformer* const* restrictors,
                             gb_transformer* const* interpolators, const double* lam_max,
@@ -747,6 +1134,10 @@ extern "C" int gb_mixed_new(int nlevels, gb_operator* op64, gb_operator* const* 
         delete m;
         return fail(GB_ECUDA, "mixed: allocation: %s", cudaGetErrorString(ce));
     }
+    if (int rc = setup_coop(m)) {
+        delete m;
+        return rc;
+    }
     *out = m;
     return 0;
 }
@@ -819,8 +1210,17 @@ extern "C" int gb_mixed_solve_async(gb_mixed* m, double* phi, const double* rho,
     if (!m || !phi || !rho) return fail(GB_EINVAL, "mixed solve: NULL argument");
     if (maxiter < 1) return fail(GB_EINVAL, "mixed solve: maxiter must be >= 1");
     cudaStream_t st = (cudaStream_t)stream;
-    if (!m->exec)
-        if (int rc = build_mixed_graph(m)) return rc;
+    if (!m->exec) {
+        int rc = build_mixed_graph(m);
+        if (rc && m->coop) {
+            // a graph that would not take the cooperative kernel: per-level
+            // kernels instead
+            cudaGetLastError();
+            m->coop = 0;
+            rc = build_mixed_graph(m);
+        }
+        if (rc) return rc;
+    }
     const long long n = m->op64->ng();
     const size_t bytes = (size_t)n * sizeof(double);
     GB_CUDA_TRY(cudaMemcpyAsync(m->rho0, rho, bytes, cudaMemcpyDeviceToDevice, st));
@@ -967,7 +1367,9 @@ int add_branch(gb_mixed_batch* bt, cudaGraph_t G, gb_mixed* m, cudaGraphNode_t r
     cudaGraph_t body = cp.conditional.phGraph_out[0];
     GB_CUDA_TRY(cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0,
                                               cudaStreamCaptureModeThreadLocal));
+    t_no_coop = true;
     rc = vcycle32(m, 0, cs);
+    t_no_coop = false;
     if (!rc) rc = defect(m, cs);
     if (!rc) k_mixed_check<<<1, 1, 0, cs>>>(m->ctl, m->nrm, 1, h);
     ce = cudaStreamEndCapture(cs, &gout);
