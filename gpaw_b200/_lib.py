@@ -43,6 +43,7 @@ SIGNATURES = {
     'gb_trace_begin': (C.c_int, [C.c_int]),
     'gb_device_fault': (C.c_int, [C.POINTER(C.c_int)]),
     'gb_mixed_vcycle_eager': (C.c_int, [_p, _p, _p, _p]),
+    'gb_mixed_set_fused_coarse': (C.c_int, [_p, C.c_int]),
     'gb_trace_end': (C.c_int, [C.c_int, C.POINTER(C.c_float),
                                C.POINTER(C.c_char_p), C.POINTER(C.c_int)]),
     'gb_operator_reserve': (C.c_int, [_p, C.c_int64, C.c_int]),

@@ -32,8 +32,11 @@ class PoissonBatch:
         self.solvers = []
         for gd in self.gds:
             if precision == 'mixed':
+                # per-pass coarse kernels: the batch's solves run side by
+                # side, which cooperative kernels (the whole GPU at once)
+                # would serialise
                 ps = MixedPoissonSolver(nn=nn, tol=tol, maxiter=maxiter,
-                                        levels=levels)
+                                        levels=levels, fused_coarse=False)
             else:
                 ps = FDPoissonSolver(nn=nn, relax='J', eps=0.0,
                                      maxiter=maxiter)

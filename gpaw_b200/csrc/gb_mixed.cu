@@ -693,7 +693,7 @@ struct gb_mixed {
     double* direct_tab = nullptr;   // eigen tables of the exact coarsest solve
     Seven direct_s7{};
     // levels lc .. L as one cooperative kernel (coop = 0: per-level kernels)
-    int coop = 0, lc = 0, coop_grid = 0;
+    int coop = 0, coop_ok = 0, lc = 0, coop_grid = 0;
     CoopPlan coop_plan{};
     double* coop_tab = nullptr;
     unsigned* coop_bar = nullptr;
@@ -1054,6 +1054,7 @@ static int setup_coop(gb_mixed* m) {
     P.bar = m->coop_bar;
     m->lc = lc;
     m->coop_grid = std::min(per_sm, 2) * nsm;
+    m->coop_ok = 1;
     m->coop = 1;
     return 0;
 }
@@ -1143,6 +1144,17 @@ extern "C" int gb_mixed_new(int nlevels, gb_operator* op64, gb_operator* const* 
 }
 
 extern "C" void gb_mixed_free(gb_mixed* m) { delete m; }
+
+extern "C" int gb_mixed_set_fused_coarse(gb_mixed* m, int on) {
+    if (!m) return fail(GB_EINVAL, "mixed: NULL solver");
+    const int want = (on && m->coop_ok) ? 1 : 0;
+    if (want != m->coop && m->exec) {
+        cudaGraphExecDestroy(m->exec);   // captured with the other path
+        m->exec = nullptr;
+    }
+    m->coop = want;
+    return 0;
+}
 
 // Graph:  defect; check -> WHILE { V32 (phi += e); defect; check }
 static int build_mixed_graph(gb_mixed* m) {

@@ -323,7 +323,10 @@ class MixedPoissonSolver:
     coarsened as set_grid_descriptor does (gpaw/poisson.py:366-430).  The
     V-cycle spans ``levels`` grids (fewer when the grid cannot be coarsened
     that often) with degree-2 Chebyshev smoothing (two sweeps before, two
-    after); the coarsest grid is solved in FP64 by a Chebyshev iteration;
+    after); the coarsest grid is solved in FP64 by a Chebyshev iteration
+    (``fused_coarse=False``) or, by default, exactly by fast
+    diagonalisation inside one cooperative kernel that also runs every
+    level below the first with at most 2 Mi points;
     the residual, its norm, |rho| and the stopping test
     ||rho - L phi|| <= tol ||rho|| are FP64, on the device.  Six levels by
     default: on a 192^3 grid they solve to 1e-10 in 14 V-cycles and 6.8 ms
@@ -332,7 +335,7 @@ class MixedPoissonSolver:
     """
 
     def __init__(self, nn=3, tol=1e-10, maxiter=200, levels=6,
-                 coarse_accuracy=0.2):
+                 coarse_accuracy=0.2, fused_coarse=True):
         if nn == 'M':
             raise NotImplementedError(
                 'Mehrstellen stencil: use FDPoissonSolver(nn="M")')
@@ -341,6 +344,7 @@ class MixedPoissonSolver:
         self.maxiter = maxiter
         self.nlevels = levels
         self.coarse_accuracy = coarse_accuracy
+        self.fused_coarse = fused_coarse
         self._h = None
 
     def set_grid_descriptor(self, gd):
@@ -387,6 +391,7 @@ class MixedPoissonSolver:
                                itp, lam, float(self.lam_min_coarse),
                                int(self.coarse_degree), C.byref(h)))
         self._h = _MixedHandle(lib, h, self)
+        check(lib.gb_mixed_set_fused_coarse(h, int(bool(self.fused_coarse))))
 
     def solve(self, phi, rho, charge=None, maxcharge=1e-6,
               zero_initial_phi=False, timer=None):

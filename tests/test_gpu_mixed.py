@@ -23,13 +23,17 @@ def _case(N, pbc, seed):
     return gdo, rho
 
 
+@pytest.mark.parametrize('fused', [True, False])
 @pytest.mark.parametrize('N,pbc', [((64, 64, 64), 0), ((48, 40, 56), 0),
                                    ((48, 48, 48), 1)])
-def test_mixed_reaches_1e10_and_matches_fp64(N, pbc, cuda, capsys):
+def test_mixed_reaches_1e10_and_matches_fp64(N, pbc, fused, cuda, capsys):
+    """Both forms of the coarse levels (one cooperative kernel with the
+    exact coarsest solve, or one kernel a pass with the Chebyshev coarsest
+    solve) reach the tolerance and the FP64 solution."""
     from gpaw_b200 import GridDescriptor, MixedPoissonSolver
     gdo, rho = _case(N, pbc, seed=3)
     gdp = GridDescriptor(N, np.diag(gdo.cell_cv), pbc)
-    ps = MixedPoissonSolver(nn=3, tol=1e-10)
+    ps = MixedPoissonSolver(nn=3, tol=1e-10, fused_coarse=fused)
     ps.set_grid_descriptor(gdp)
     phi = gdp.zeros()
     n = ps.solve_neutral(phi, to_dev(rho))
@@ -47,7 +51,8 @@ def test_mixed_reaches_1e10_and_matches_fp64(N, pbc, cuda, capsys):
     po.solve_neutral(ref, rho)
     err = np.abs(got - ref).max() / np.abs(ref).max()
     with capsys.disabled():
-        print(f'\nmixed {N} pbc={pbc}: {n} V-cycles, rel residual {rel:.3e} '
+        print(f'\nmixed {N} pbc={pbc} fused={fused}: {n} V-cycles, '
+              f'rel residual {rel:.3e} '
               f'(device {ps.rel_residual:.3e}), max rel error vs FP64 '
               f'{err:.3e}')
     assert rel <= 1.01e-10
