@@ -722,7 +722,34 @@ static int launch_cfd_nn(const void* in, void* out, int nin, const GridBC& g, co
         // float64: 32 x 8 tiles of two rows a thread (128 threads, more
         // CTAs an SM) measured faster than 32 x 16 tiles (nn = 3 apply
         // 14 %, preconditioner 9 %, FP64 V-cycles 3-7 %)
-        constexpr int ORDL = MODE == EPI_LIN ? 3 : 1;
+        // split sums for the FP64 defect of the mixed solver (measured
+        // faster there); the FP32 levels keep one chain (measured slower
+        // with three: more registers)
+        constexpr int ORDL = (MODE == EPI_LIN && sizeof(T) == 8) ? 3 : 1;
+        if constexpr (MODE == EPI_LIN) {
+            // tile shapes of the mixed solver's passes under measurement
+            // (GPAW_B200_LIN_VARIANT): 1 = one row a thread, 32 x 8 tiles
+            static const int var = [] {
+                const char* e = getenv("GPAW_B200_LIN_VARIANT");
+                return e ? atoi(e) : 0;
+            }();
+            if (var == 1) {
+                if constexpr (sizeof(T) == 8)
+                    return launch_cfd_t<T, NN, 32, 8, 1, D, MODE, ORDL, 0, 3>(in, out, nin, g, P,
+                                                                              cs, ep, st, nblk);
+                else
+                    return launch_cfd_t<T, NN, 32, 8, 1, D, MODE, ORDL, 0, 4>(in, out, nin, g, P,
+                                                                              cs, ep, st, nblk);
+            }
+            if (var == 2) {
+                if constexpr (sizeof(T) == 8)
+                    return launch_cfd_t<T, NN, 32, 8, 1, D, MODE, ORDL, 0, 3>(in, out, nin, g, P,
+                                                                              cs, ep, st, nblk);
+                else
+                    return launch_cfd_t<T, NN, 32, 16, RY, D, MODE, ORDL, 0, 3>(
+                        in, out, nin, g, P, cs, ep, st, nblk);
+            }
+        }
         if constexpr (sizeof(T) == 8)
             return launch_cfd_t<T, NN, 32, 8, 2, D, MODE, ORDL, 0, 4>(in, out, nin, g, P, cs, ep,
                                                                       st, nblk);

@@ -450,7 +450,7 @@ __device__ __forceinline__ bool coop_sync(unsigned* bar, bool ok) {
                         s_ok = 0;
                         break;
                     }
-                    __nanosleep(64);
+                    __nanosleep(20);
                 }
             }
             __threadfence();
@@ -731,12 +731,162 @@ struct gb_mixed {
     }
 };
 
+// ------------------------------------------------------ FP32 level passes
+// One pass y = p0 aux + p1 u + p2 (A u) + p3 aux2 of an FP32 level (A the
+// level's axis-aligned stencil of half-width NN), written to `out` or added
+// to an FP64 array.  The level arrays (a few tens of MB at most) stay in
+// L2 between passes, so this kernel stages nothing in shared memory: a
+// thread owns one (row, column) of the grid and marches along axis 0 with
+// the 2NN+1 values of its column in registers; the in-plane neighbours are
+// read through the L1 cache, which a CTA's 32 x 8 tile shares.  No barriers,
+// no copy bookkeeping: for these passes the plane-marching kernel spent
+// about 150 instructions a point on staging.  FP32 fused multiply-adds
+// (the FP32 V-cycle's arithmetic is its own; it is checked by tolerance).
+// F: 1 = aux, 2 = aux2, 4 = add to acc64 instead of writing out.
+template <int NN, int F>
+__global__ void __launch_bounds__(256)
+k_lin32(const float* __restrict__ u, float* __restrict__ out, const float* __restrict__ aux,
+        const float* __restrict__ aux2, double* __restrict__ acc64, GridBC g, CfdStencil cs,
+        float p0, float p1, float p2, float p3, int chunk, int tiles_x) {
+    constexpr int Q = 2 * NN + 1;
+    const int n0 = g.n[0], n1 = g.n[1], n2 = g.n[2];
+    const int x = (blockIdx.x % tiles_x) * 32 + (threadIdx.x & 31);
+    const int y = (blockIdx.x / tiles_x) * 8 + (threadIdx.x >> 5);
+    const int pa = blockIdx.y * chunk;
+    const int pb = min(n0, pa + chunk);
+    if (x >= n2 || y >= n1 || pa >= pb) return;
+    const long long ps = (long long)n1 * n2;
+    // in-plane neighbours: offsets after the boundary, or -1 (zero)
+    int xo[2 * NN], yo[2 * NN];
+#pragma unroll
+    for (int d = 1; d <= NN; d++) {
+        int a = x + d, b = x - d;
+        xo[d - 1] = (a < n2) ? a : (g.periodic[2] && a - n2 < n2 ? a - n2 : -1);
+        xo[NN + d - 1] = (b >= 0) ? b : (g.periodic[2] && b + n2 >= 0 ? b + n2 : -1);
+        a = y + d;
+        b = y - d;
+        yo[d - 1] = (a < n1) ? a * n2 : (g.periodic[1] && a - n1 < n1 ? (a - n1) * n2 : -1);
+        yo[NN + d - 1] = (b >= 0) ? b * n2 : (g.periodic[1] && b + n1 >= 0 ? (b + n1) * n2 : -1);
+    }
+    const int row = y * n2;
+    auto col_at = [&](int p) -> float {   // u at plane p of this column
+        if (p < 0 || p >= n0) {
+            if (!g.periodic[0]) return 0.0f;
+            p += p < 0 ? n0 : -n0;
+            if (p < 0 || p >= n0) return 0.0f;
+        }
+        return __ldg(u + p * ps + row + x);
+    };
+    float q[Q];
+#pragma unroll
+    for (int k = 0; k < Q - 1; k++) q[k + 1] = col_at(pa - NN + k);
+    const float c0 = (float)cs.c0;
+    float cp[3][NN], cm[3][NN];
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+#pragma unroll
+        for (int d = 0; d < NN; d++) {
+            cp[k][d] = (float)cs.cp[k][d];
+            cm[k][d] = (float)cs.cm[k][d];
+        }
+#pragma unroll 2
+    for (int p = pa; p < pb; p++) {
+#pragma unroll
+        for (int k = 0; k < Q - 1; k++) q[k] = q[k + 1];
+        q[Q - 1] = col_at(p + NN);
+        const float* pl = u + p * ps;
+        // one partial sum a direction (axis 2, 1, 0), added at the end
+        float s2 = c0 * q[NN], s1 = 0.0f, s0 = 0.0f;
+#pragma unroll
+        for (int d = 0; d < NN; d++) {
+            const float a = xo[d] >= 0 ? __ldg(pl + row + xo[d]) : 0.0f;
+            const float b = xo[NN + d] >= 0 ? __ldg(pl + row + xo[NN + d]) : 0.0f;
+            s2 = fmaf(cp[0][d], a, fmaf(cm[0][d], b, s2));
+            const float c = yo[d] >= 0 ? __ldg(pl + yo[d] + x) : 0.0f;
+            const float e = yo[NN + d] >= 0 ? __ldg(pl + yo[NN + d] + x) : 0.0f;
+            s1 = fmaf(cp[1][d], c, fmaf(cm[1][d], e, s1));
+            s0 = fmaf(cp[2][d], q[NN + 1 + d], fmaf(cm[2][d], q[NN - 1 - d], s0));
+        }
+        const float au = (s2 + s1) + s0;
+        const long long at = p * ps + row + x;
+        float v = fmaf(p1, q[NN], p2 * au);
+        if (F & 1) v = fmaf(p0, aux[at], v);
+        if (F & 2) v = fmaf(p3, aux2[at], v);
+        if (F & 4) acc64[at] += (double)v;
+        else out[at] = v;
+    }
+}
+
+template <int NN>
+static void launch_lin32_nn(const gb_operator* op, const float* in, float* out, const float* aux,
+                            const float* aux2, double* acc64, float p0, float p1, float p2,
+                            float p3, cudaStream_t st) {
+    const GridBC& g = op->g;
+    const int tiles_x = (g.n[2] + 31) / 32, tiles_y = (g.n[1] + 7) / 8;
+    int chunk = op->chunk > 0 ? std::min(op->chunk, g.n[0]) : g.n[0];
+    if (op->chunk <= 0)
+        while (chunk > 2 * NN + 2 && (long long)tiles_x * tiles_y * ((g.n[0] + chunk - 1) / chunk) <
+                                         148 * 6)
+            chunk = (chunk + 1) / 2;
+    dim3 grid(tiles_x * tiles_y, (g.n[0] + chunk - 1) / chunk);
+    const int f = (aux ? 1 : 0) | (aux2 ? 2 : 0) | (acc64 ? 4 : 0);
+#define GB_LIN32(F)                                                                          \
+    k_lin32<NN, F><<<grid, 256, 0, st>>>(in, out, aux, aux2, acc64, g, op->cs, p0, p1, p2, p3, \
+                                         chunk, tiles_x)
+    switch (f) {
+        case 0: GB_LIN32(0); break;
+        case 1: GB_LIN32(1); break;
+        case 2: GB_LIN32(2); break;
+        case 3: GB_LIN32(3); break;
+        case 4: GB_LIN32(4); break;
+        case 5: GB_LIN32(5); break;
+        case 6: GB_LIN32(6); break;
+        default: GB_LIN32(7); break;
+    }
+#undef GB_LIN32
+}
+
+// The FP32 passes through k_lin32 unless GPAW_B200_LIN32=0 (the
+// plane-marching kernel's EPI_LIN mode).
+static bool lin32_direct() {
+    static const bool on = [] {
+        const char* e = getenv("GPAW_B200_LIN32");
+        return !(e && atoi(e) == 0);
+    }();
+    return on;
+}
+
+static int lin32(const gb_operator* op, const float* in, float* out, const float* aux,
+                 const float* aux2, double p0, double p1, double p2, double p3, double* acc64,
+                 cudaStream_t st) {
+    const CfdStencil& cs = op->cs;
+    if (!(cs.axis[0] == 2 && cs.axis[1] == 1 && cs.axis[2] == 0)) return -1;
+    const float f0 = (float)p0, f1 = (float)p1, f2 = (float)p2, f3 = (float)p3;
+    switch (op->nn) {
+        case 1: launch_lin32_nn<1>(op, in, out, aux, aux2, acc64, f0, f1, f2, f3, st); break;
+        case 2: launch_lin32_nn<2>(op, in, out, aux, aux2, acc64, f0, f1, f2, f3, st); break;
+        case 3: launch_lin32_nn<3>(op, in, out, aux, aux2, acc64, f0, f1, f2, f3, st); break;
+        case 4: launch_lin32_nn<4>(op, in, out, aux, aux2, acc64, f0, f1, f2, f3, st); break;
+        case 5: launch_lin32_nn<5>(op, in, out, aux, aux2, acc64, f0, f1, f2, f3, st); break;
+        case 6: launch_lin32_nn<6>(op, in, out, aux, aux2, acc64, f0, f1, f2, f3, st); break;
+        default: return -1;
+    }
+    return 0;
+}
+
 // One stencil pass of the linear epilogue on level l (float) or on the
 // level-0 FP64 operator (double).
 template <class T>
 static int lin(gb_operator* op, const T* in, T* out, const T* aux, const T* aux2, double p0,
                double p1, double p2, double p3, double* acc64, float* out32, double* partial,
                cudaStream_t st) {
+    if constexpr (sizeof(T) == 4) {
+        if (lin32_direct() && !partial && !out32 &&
+            lin32(op, in, out, aux, aux2, p0, p1, p2, p3, acc64, st) == 0) {
+            GB_LAUNCH_CHECK();
+            return 0;
+        }
+    }
     Epi ep{};
     ep.aux = aux;
     ep.aux2 = aux2;
@@ -965,9 +1115,11 @@ constexpr long long COOP_MAX_POINTS = 2 << 20;
 static int setup_coop(gb_mixed* m) {
     const char* env = getenv("GPAW_B200_COOP_COARSE");
     if (env && atoi(env) == 0) return 0;
+    const char* emax = getenv("GPAW_B200_COOP_MAX_POINTS");
+    const long long maxpts = emax ? atoll(emax) : COOP_MAX_POINTS;
     int lc = -1;
     for (int l = 1; l <= m->L; l++)
-        if (m->ops[l]->ng() <= COOP_MAX_POINTS) {
+        if (m->ops[l]->ng() <= maxpts) {
             lc = l;
             break;
         }
@@ -1053,7 +1205,9 @@ static int setup_coop(gb_mixed* m) {
     P.Y = m->r;
     P.bar = m->coop_bar;
     m->lc = lc;
-    m->coop_grid = std::min(per_sm, 2) * nsm;
+    const char* eps = getenv("GPAW_B200_COOP_PER_SM");
+    const int want = eps ? std::max(1, atoi(eps)) : 1;
+    m->coop_grid = std::min(per_sm, want) * nsm;
     m->coop_ok = 1;
     m->coop = 1;
     return 0;
