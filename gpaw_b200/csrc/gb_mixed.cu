@@ -846,12 +846,13 @@ static void launch_lin32_nn(const gb_operator* op, const float* in, float* out, 
 #undef GB_LIN32
 }
 
-// The FP32 passes through k_lin32 unless GPAW_B200_LIN32=0 (the
-// plane-marching kernel's EPI_LIN mode).
+// The FP32 passes through k_lin32 only with GPAW_B200_LIN32=1: on the
+// 192^3 grid it measured no faster than the plane-marching kernel's EPI_LIN
+// mode (level-0 passes 55-86 us either way, 6.99 against 6.70 ms a solve).
 static bool lin32_direct() {
     static const bool on = [] {
         const char* e = getenv("GPAW_B200_LIN32");
-        return !(e && atoi(e) == 0);
+        return e && atoi(e) != 0;
     }();
     return on;
 }
@@ -1105,19 +1106,24 @@ static int setup_direct(gb_mixed* m) {
     return 0;
 }
 
-// Levels from the first with at most COOP_MAX_POINTS points down to the
-// coarsest go into the cooperative kernel, when the coarsest operator is a
-// symmetric 7-point stencil (its exact solve needs the eigen tables) and
-// every level below 0 has the 7-point operator (what MixedPoissonSolver
-// builds).  GPAW_B200_COOP_COARSE=0 keeps the per-level kernels.
-constexpr long long COOP_MAX_POINTS = 2 << 20;
+// The cooperative kernel takes the coarsest level (its exact solve), and
+// with GPAW_B200_COOP_MAX_POINTS=n also every level from the first with at
+// most n points, when the coarsest operator is a symmetric 7-point stencil
+// (the exact solve needs the eigen tables) and every level below 0 has the
+// 7-point operator (what MixedPoissonSolver builds).  Measured on the 192^3
+// grid with 4 levels: the coarsest alone 6.70 ms a solve, levels 2-3
+// 7.15 ms, levels 1-3 8.17 ms (grid-stride passes and grid barriers cost
+// more than the tiled kernels on the larger levels).
+// GPAW_B200_COOP_COARSE=0 keeps the per-level kernels and the Chebyshev
+// coarsest solve.
+constexpr long long COOP_MAX_POINTS = 0;
 
 static int setup_coop(gb_mixed* m) {
     const char* env = getenv("GPAW_B200_COOP_COARSE");
     if (env && atoi(env) == 0) return 0;
     const char* emax = getenv("GPAW_B200_COOP_MAX_POINTS");
     const long long maxpts = emax ? atoll(emax) : COOP_MAX_POINTS;
-    int lc = -1;
+    int lc = m->L;
     for (int l = 1; l <= m->L; l++)
         if (m->ops[l]->ng() <= maxpts) {
             lc = l;

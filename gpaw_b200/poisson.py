@@ -325,8 +325,7 @@ class MixedPoissonSolver:
     that often) with degree-2 Chebyshev smoothing (two sweeps before, two
     after); the coarsest grid is solved in FP64 by a Chebyshev iteration
     (``fused_coarse=False``) or, by default, exactly by fast
-    diagonalisation inside one cooperative kernel that also runs every
-    level below the first with at most 2 Mi points;
+    diagonalisation in one cooperative kernel;
     the residual, its norm, |rho| and the stopping test
     ||rho - L phi|| <= tol ||rho|| are FP64, on the device.  Six levels by
     default: on a 192^3 grid they solve to 1e-10 in 14 V-cycles and 6.8 ms

@@ -297,12 +297,11 @@ GB_API int gb_mixed_new(int nlevels, gb_operator* op64, gb_operator* const* oper
                         gb_transformer* const* interpolators, const double* lam_max,
                         double lam_min_coarse, int coarse_degree, gb_mixed** out);
 GB_API void gb_mixed_free(gb_mixed* m);
-/* Levels below the first with at most 2 Mi points as one cooperative
- * kernel (on = 1, the default where the levels allow it) or as one kernel
- * per pass (on = 0).  The two give slightly different FP32 corrections (the
- * fused kernel solves the coarsest level exactly), each deterministic.  No
- * counterpart in the reference.  Returns 0; *on is ignored where the
- * levels do not allow the fused kernel. */
+/* The coarsest level solved exactly (fast diagonalisation) in one
+ * cooperative kernel (on = 1, the default where the level allows it), or by
+ * the Chebyshev iteration (on = 0).  The two give slightly different FP32
+ * corrections, each deterministic.  No counterpart in the reference.
+ * Returns 0; `on` is ignored where the level does not allow the kernel. */
 GB_API int gb_mixed_set_fused_coarse(gb_mixed* m, int on);
 /* One V-cycle of the mixed-precision solver and the defects around it,
  * launched kernel by kernel instead of through the solver's graph:
