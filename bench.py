@@ -279,6 +279,103 @@ def run_reference(args):
 
 
 # ------------------------------------------------------------- Poisson
+def reference_gpu_c2(dev, kin, rst, itp, x, y, c, z, ph, nb, reps=5):
+    """The reference's own GPU kernels (c/gpu/kernels, compiled for sm_100a
+    from its sources into oracle/_ref by `make -C oracle gpu`) on the same
+    C2 step, timed with CUDA events on the same stream: the GPU baseline
+    beside this library's kernels.  Each call pastes the batch, block by
+    block of 16 grids, into the reference's padded buffer, copies the
+    periodic halos with their phases and runs its kernel, as its
+    single-domain GPU path does.  Also the largest relative difference of
+    its outputs from this library's (the reference's GPU kernels sum in
+    their own order)."""
+    import ctypes as C
+    import torch
+    path = os.path.join(ROOT, 'oracle', '_ref', 'libgpaw_ref_gpu.so')
+    if not os.path.exists(path):
+        return {'unavailable': 'oracle/_ref/libgpaw_ref_gpu.so not built'}
+    lib = C.CDLL(path)
+    vp, lp, dp = C.c_void_p, C.POINTER(C.c_long), C.POINTER(C.c_double)
+    lib.refgpu_operator_new.restype = vp
+    lib.refgpu_operator_new.argtypes = [dp, lp, C.c_int, C.c_int, lp, lp,
+                                        C.c_int]
+    lib.refgpu_operator_apply.argtypes = [vp, vp, vp, C.c_int, dp]
+    lib.refgpu_transformer_new.restype = vp
+    lib.refgpu_transformer_new.argtypes = [lp, lp, C.c_int, lp, lp, lp, lp,
+                                           C.c_int, C.c_int]
+    lib.refgpu_transformer_apply.argtypes = [vp, vp, vp, C.c_int, dp]
+
+    def longs(a):
+        a = np.ascontiguousarray(np.asarray(a).ravel(), np.int64)
+        return a, a.ctypes.data_as(lp)
+
+    def dbls(a):
+        a = np.ascontiguousarray(np.asarray(a, float).ravel())
+        return a, a.ctypes.data_as(dp)
+
+    keep = []
+    co, co_p = dbls(kin.coef_p)
+    of, of_p = longs(kin.offset_p)
+    sz, sz_p = longs(kin.gd.n_c)
+    ne, ne_p = longs(kin.gd.neighbor_cd)
+    keep += [co, of, sz, ne]
+    hop = lib.refgpu_operator_new(co_p, of_p, len(kin.coef_p), int(kin.mp),
+                                  sz_p, ne_p, 0)
+
+    def transformer(t):
+        si, si_p = longs(t.gdin.n_c)
+        so, so_p = longs(t.gdout.n_c)
+        pa, pa_p = longs(t.pad_cd)
+        npd, npd_p = longs(t.neighborpad_cd)
+        sk, sk_p = longs(t.skip_cd)
+        nbr, nbr_p = longs(t.gdin.neighbor_cd)
+        keep.extend([si, so, pa, npd, sk, nbr])
+        return lib.refgpu_transformer_new(si_p, so_p, 2 * t.nn, pa_p, npd_p,
+                                          sk_p, nbr_p, 0, int(t.interpolate))
+
+    hr, hi = transformer(rst), transformer(itp)
+    if not (hop and hr and hi):
+        return {'unavailable': 'reference GPU objects could not be built'}
+    phv, ph_p = dbls(np.column_stack([np.asarray(ph).real.ravel(),
+                                      np.asarray(ph).imag.ravel()]))
+    keep.append(phv)
+    ry, rc, rz = torch.empty_like(y), torch.empty_like(c), torch.empty_like(z)
+    calls = {
+        'apply': lambda: lib.refgpu_operator_apply(
+            hop, vp(x.data_ptr()), vp(ry.data_ptr()), nb, ph_p),
+        'restrict': lambda: lib.refgpu_transformer_apply(
+            hr, vp(x.data_ptr()), vp(rc.data_ptr()), nb, ph_p),
+        'interpolate': lambda: lib.refgpu_transformer_apply(
+            hi, vp(c.data_ptr()), vp(rz.data_ptr()), nb, ph_p)}
+    ab, rb, ib = algorithmic_bytes(nb)
+    nbytes = {'apply': ab, 'restrict': rb, 'interpolate': ib}
+    out = {'how': 'reference c/gpu/kernels for sm_100a, blocks of 16 '
+                  'grids, paste + halo copies + kernel per block'}
+    st = torch.cuda.current_stream()
+    for k, f in calls.items():
+        if f() != 0:
+            return {'unavailable': f'reference GPU {k} failed'}
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(reps):
+            f()
+        e1.record(st)
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1) / 1e3 / reps
+        out[k] = {'ms': t * 1e3, 'gbs': nbytes[k] / t / 1e9}
+    # ours on the same inputs (the step just ran: y, c, z hold them)
+    kin.apply(x, y, ph)
+    rst.apply(x, c, phases=ph)
+    itp.apply(c, z, phases=ph)
+    for k, (a, b) in {'apply': (ry, y), 'restrict': (rc, c),
+                      'interpolate': (rz, z)}.items():
+        out[k]['max_rel_diff_vs_ours'] = float((a - b).abs().max() /
+                                               b.abs().max())
+    return out
+
+
 def poisson_c1(dev, nsolve=20, cpu=True):
     """64^3 zero-BC FDPoissonSolver (nn = 3, Jacobi, reference schedule),
     h = 0.2 A, 8 Gaussians: solves/s at the reference's eps = 2e-10 and at
@@ -944,12 +1041,17 @@ def run_gpu(args):
         'e2e': e2e,
         'cpu_baseline': cpu_base,
     }
+    ref_gpu = None
+    if (rank == 0 or world == 1) and not args.no_ref_gpu:
+        ref_gpu = reference_gpu_c2(dev, kin, rst, itp, x, y, c, z, ph, NBANDS)
     detail = {'c2': {'kernels_ms': {'apply': apply_t * 1e3,
                                     'restrict': rst_t * 1e3,
                                     'interpolate': itp_t * 1e3},
                      'kernels_gbs': {'apply': achieved,
                                      'restrict': rb / rst_t / 1e9,
                                      'interpolate': ib / itp_t / 1e9}}}
+    if ref_gpu is not None:
+        detail['c2']['reference_gpu'] = ref_gpu
     # FD Hamiltonian local part on the same batch: kin(psi) + v psi fused
     if (rank == 0 or world == 1) and not args.no_ham:
         from gpaw_b200 import FDHamiltonian
@@ -1017,6 +1119,13 @@ def summarize(d, peak):
                      'frac': {n: _g(v / peak, 3) for n, v in k.items()}}
         if 'hamiltonian' in c2:
             out['c2']['ham_gbs'] = _g(c2['hamiltonian']['gbs'])
+        rg = c2.get('reference_gpu')
+        if rg and 'apply' in rg:
+            out['c2']['ref_gpu_gbs'] = {n: _g(rg[n]['gbs']) for n in k}
+            out['c2']['ours_over_ref_gpu'] = {n: _g(k[n] / rg[n]['gbs'], 3)
+                                              for n in k}
+        elif rg:
+            out['c2']['ref_gpu'] = rg.get('unavailable')
     c1 = d.get('c1')
     if c1:
         a = c1['apply']
@@ -1108,6 +1217,8 @@ def main():
     p.add_argument('--no-serving', action='store_true')
     p.add_argument('--no-ham', action='store_true',
                    help='skip the fused Hamiltonian section')
+    p.add_argument('--no-ref-gpu', action='store_true',
+                   help="skip timing the reference's own GPU kernels")
     p.add_argument('--poisson-only', default=None,
                    choices=['c1', 'c3', 'c4', 'pc', 'c5', 'wfd', 'c1a', 'c3m',
                             'c3f', 'c3trace'],
