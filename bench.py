@@ -888,6 +888,27 @@ def serving_c5(dev, rates=(50, 100, 200, 500, 1000, 2000), count=1000,
         st['poisson_vcycles_mean'] = float(np.mean(
             [r.niter for r in reqs if r.kind == 'poisson'] or [0]))
         out[f'lambda_{lam}'] = st
+    # anisotropic stream: every axis draws its own side (18^3 possible
+    # shapes), so solvers are built on demand while serving and the least
+    # recently used are evicted under the budget; warmed by an untimed
+    # stream of other draws
+    del srv
+    gc.collect()
+    torch.cuda.empty_cache()
+    srv = Server(hbm_budget=16 << 30, nslots=8, device=dev, grow=True)
+    warm = make_requests(200, 300, seed=7, anisotropic=True)
+    srv.run(warm, {r.rid: srv.host_input(r) for r in warm})
+    aniso = {'requests_per_rate': 500}
+    for lam in (50, 200, 1000):
+        reqs = make_requests(lam, 500, seed=20_000 + lam, anisotropic=True)
+        inputs = {r.rid: srv.host_input(r) for r in reqs}
+        b0, e0 = srv.built, srv.evicted
+        srv.run(reqs, inputs)
+        st = latency_stats(reqs)
+        st['solvers_built'] = srv.built - b0
+        st['solvers_evicted'] = srv.evicted - e0
+        aniso[f'lambda_{lam}'] = st
+    out['anisotropic'] = aniso
     return out
 
 
@@ -1181,6 +1202,12 @@ def summarize(d, peak):
                          _g(v['throughput_per_s']), _g(v['p50_ms'], 3),
                          _g(v['p99_ms'], 3)]
                          for k, v in c5.items() if k.startswith('lambda_')}}
+        an = c5.get('anisotropic')
+        if an:
+            out['c5']['aniso_thr_p50_p99_built'] = {k.split('_')[1]: [
+                _g(v['throughput_per_s']), _g(v['p50_ms'], 3),
+                _g(v['p99_ms'], 3), v['solvers_built']]
+                for k, v in an.items() if k.startswith('lambda_')}
     return out
 
 

@@ -45,19 +45,23 @@ class Request:
 
 
 def make_requests(rate, count, seed=0, poisson_fraction=0.5, smin=24,
-                  smax=160):
+                  smax=160, anisotropic=False):
     """Poisson-process arrivals at `rate` per second; grid side log-uniform
     in [smin, smax], rounded to a multiple of 8 (so every grid has at least
-    three multigrid levels)."""
+    three multigrid levels); with `anisotropic` each axis draws its own
+    side."""
     rng = np.random.default_rng(seed)
     t = np.cumsum(rng.exponential(1.0 / rate, count))
+
+    def side():
+        x = np.exp(rng.uniform(np.log(smin), np.log(smax)))
+        return int(max(smin, min(smax, 8 * round(x / 8))))
+
     out = []
     for i in range(count):
-        side = np.exp(rng.uniform(np.log(smin), np.log(smax)))
-        side = int(max(smin, min(smax, 8 * round(side / 8))))
+        N = tuple(side() for _ in range(3)) if anisotropic else (side(),) * 3
         kind = 'poisson' if rng.random() < poisson_fraction else 'apply'
-        out.append(Request(i, kind, (side, side, side), float(t[i]),
-                           int(rng.integers(1 << 30))))
+        out.append(Request(i, kind, N, float(t[i]), int(rng.integers(1 << 30))))
     return out
 
 
@@ -86,6 +90,11 @@ class Server:
         # that the loop allocates no device memory (an allocation can stall
         # every stream)
         self.slabs = [None] * nslots
+        # resident solvers by last use (oldest first), for eviction when a
+        # new shape needs room under the budget; counters of the run
+        self.lru = collections.OrderedDict()     # id(solver) -> (N, solver)
+        self.built = 0
+        self.evicted = 0
 
     # -- resources ---------------------------------------------------------
     def _gd(self, N):
@@ -107,10 +116,23 @@ class Server:
         from .poisson import MixedPoissonSolver
         pool = self.pools[('poisson', req.N)]
         if pool:
-            return pool.pop(), 0
+            ps = pool.pop()
+            self.lru.pop(id(ps), None)
+            return ps, 0
         ps = MixedPoissonSolver(nn=3, tol=self.tol, levels=4)
         ps.set_grid_descriptor(self._gd(req.N))
+        self.built += 1
         return ps, self.solver_bytes(req.N)
+
+    def _evict_for(self, need):
+        """Free idle resident solvers, least recently used first, until
+        `need` more bytes fit the budget; False when they cannot."""
+        while self.resident + self.in_use + need > self.budget and self.lru:
+            _, (N, ps) = self.lru.popitem(last=False)
+            self.pools[('poisson', N)].remove(ps)
+            self.resident -= self.solver_bytes(N)
+            self.evicted += 1
+        return self.resident + self.in_use + need <= self.budget
 
     def warm(self, shapes, per_shape=2):
         """Build `per_shape` resident solvers (graphs captured) and one
@@ -132,6 +154,8 @@ class Server:
                     pass
                 built.append(ps)
             self.pools[('poisson', N)].extend(built)
+            for ps in built:
+                self.lru[id(ps)] = (N, ps)
             # first launch of each kernel loads it (lazy module loading):
             # do that here, not while serving
             op = self._op(N)
@@ -202,6 +226,7 @@ class Server:
         if job['solver'] is not None:
             req.niter = job['solver'].result()
             self.pools[('poisson', req.N)].append(job['solver'])
+            self.lru[id(job['solver'])] = (req.N, job['solver'])
         self.in_use -= self.request_bytes(req)
         self.free_slots.append(job['slot'])
 
@@ -255,7 +280,7 @@ class Server:
                 if req.kind == 'poisson' and not pooled:
                     need += self.solver_bytes(req.N)
                 if self.resident + self.in_use + need > self.budget and \
-                        active:
+                        not self._evict_for(need) and active:
                     break      # wait for memory to free up
                 del pending[i]
                 slot = self.free_slots.pop()

@@ -76,3 +76,24 @@ def test_no_grow_waits_for_a_resident_solver(cuda):
         one = Request(r.rid, r.kind, r.N, 0.0, r.seed)
         alone = srv.run([one], {r.rid: inputs[r.rid]})[0]
         assert np.array_equal(got[r.rid], alone.result)
+
+
+@pytest.mark.gpu
+def test_anisotropic_stream_with_eviction(cuda):
+    """Anisotropic requests (each axis its own side) on a loop that builds
+    solvers on demand under a budget too small to keep them all: solvers
+    are evicted least recently used first, every result equals the request
+    served alone, and the budget holds."""
+    from gpaw_b200.serving import Server
+    reqs = make_requests(rate=5000.0, count=20, seed=8, smin=24, smax=56,
+                         poisson_fraction=0.8, anisotropic=True)
+    assert any(len(set(r.N)) > 1 for r in reqs)
+    srv = Server(hbm_budget=24 << 20, nslots=4, grow=True)
+    inputs = {r.rid: srv.host_input(r) for r in reqs}
+    mixed = {r.rid: r.result for r in srv.run(reqs, inputs)}
+    assert srv.built > 0 and srv.evicted > 0
+    assert srv.resident <= srv.budget + Server.solver_bytes((56, 56, 56))
+    for r in reqs:
+        one = Request(r.rid, r.kind, r.N, 0.0, r.seed)
+        alone = srv.run([one], {r.rid: inputs[r.rid]})[0]
+        assert np.array_equal(mixed[r.rid], alone.result), r
