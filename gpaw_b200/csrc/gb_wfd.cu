@@ -118,11 +118,16 @@ struct WGroups {
     double cm[GB_MAX_WEIGHTS][3][6];      // coefficient of -d
 };
 
-template <class T, int R, int S, bool GROUPS>
+// MODE 0: the apply.  MODE 1 (real data): one weighted-Jacobi sweep, out =
+// (1 - wj) in + (wj (rhs - x)) / d with x the off-diagonal part and d the
+// diagonal of the weighted operator at the point, each operator's inner sum
+// and the accumulation in bmgs_wrelax's order (c/bmgs/wrelax.cpp:71-86),
+// the same arithmetic as k_wjacobi.
+template <class T, int R, int S, bool GROUPS, int MODE>
 __global__ void __launch_bounds__(WX * WY)
 k_wfd_tiled(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phases P,
             const __grid_constant__ WStencil s, const __grid_constant__ WGroups G, int chunk0,
-            int tiles_x) {
+            int tiles_x, const double* __restrict__ rhs, double wj) {
     constexpr int PX = WX + 2 * R, PY = WY + 2 * R, PL = PX * PY;
     constexpr int NT = WX * WY;
     constexpr int D = S - (2 * R + 1);          // planes in flight
@@ -252,11 +257,12 @@ k_wfd_tiled(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Ph
         if (!own) continue;
         const long long at = p * pstride + (long long)gy * n2 + gx;
         T x = Num<T>::zero();
+        double dg = 0.0;     // MODE 1: the diagonal sum_i w_i c_i0
         if constexpr (GROUPS) {
             const T* c = ring + (cj & (S - 1)) * PL + cen;
             for (int iw = 0; iw < s.nw; iw++) {
                 T tmp = Num<T>::zero();
-                tmp = Num<T>::add(tmp, Num<T>::scale(c[0], G.c0[iw]));
+                if (MODE == 0) tmp = Num<T>::add(tmp, Num<T>::scale(c[0], G.c0[iw]));
                 for (int k = 0; k < G.ng[iw]; k++) {
                     const int ax = G.axis[iw][k];
                     if (ax == 0) {
@@ -278,23 +284,33 @@ k_wfd_tiled(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Ph
                             tmp = Num<T>::add(tmp, Num<T>::scale(c[-d * sd], G.cm[iw][k][d - 1]));
                     }
                 }
-                tmp = Num<T>::scale(tmp, __ldg(s.w[iw] + at));
+                const double weight = __ldg(s.w[iw] + at);
+                tmp = Num<T>::scale(tmp, weight);
                 x = Num<T>::add(x, tmp);
+                if (MODE == 1) dg = __dadd_rn(dg, __dmul_rn(weight, G.c0[iw]));
             }
         } else {
             for (int iw = 0; iw < s.nw; iw++) {
                 T tmp = Num<T>::zero();
                 const int c0 = s.start[iw], c1 = c0 + s.ncoefs[iw];
 #pragma unroll 4
-                for (int c = c0; c < c1; c++) {
+                for (int c = c0 + MODE; c < c1; c++) {
                     const T v = ring[((cj + sh_o0[c]) & (S - 1)) * PL + cen + sh_ip[c]];
                     tmp = Num<T>::add(tmp, Num<T>::scale(v, sh_coef[c]));
                 }
-                tmp = Num<T>::scale(tmp, __ldg(s.w[iw] + at));
+                const double weight = __ldg(s.w[iw] + at);
+                tmp = Num<T>::scale(tmp, weight);
                 x = Num<T>::add(x, tmp);
+                if (MODE == 1) dg = __dadd_rn(dg, __dmul_rn(weight, sh_coef[c0]));
             }
         }
-        o[at] = x;
+        if constexpr (MODE == 1 && sizeof(T) == 8) {
+            const double old = ring[(cj & (S - 1)) * PL + cen];
+            o[at] = __dadd_rn(__dmul_rn(1.0 - wj, old),
+                              __ddiv_rn(__dmul_rn(wj, __dsub_rn(rhs[at], x)), dg));
+        } else {
+            o[at] = x;
+        }
     }
     asm volatile("cp.async.wait_group 0;\n" ::);
 }
@@ -440,14 +456,14 @@ static bool wfd_groups(const WStencil& s, int R, WGroups& G) {
     return true;
 }
 
-template <class T, int R, int S, bool GROUPS>
+template <class T, int R, int S, bool GROUPS, int MODE>
 static int launch_wfd_tiled_k(const void* in, void* out, int nin, const GridBC& g,
                               const Phases& P, const WStencil& s, const WGroups& G,
-                              cudaStream_t st) {
+                              cudaStream_t st, const double* rhs, double wj) {
     constexpr size_t smem = (size_t)S * (WX + 2 * R) * (WY + 2 * R) * sizeof(T);
     static bool attr_done = false;
     if (!attr_done) {
-        if (cudaFuncSetAttribute(k_wfd_tiled<T, R, S, GROUPS>,
+        if (cudaFuncSetAttribute(k_wfd_tiled<T, R, S, GROUPS, MODE>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem) != cudaSuccess)
             return -2;
@@ -461,24 +477,28 @@ static int launch_wfd_tiled_k(const void* in, void* out, int nin, const GridBC& 
     for (int b0 = 0; b0 < nin; b0 += 65535) {
         const int nb = min(65535, nin - b0);
         dim3 grid(tiles_x * tiles_y, nch, nb);
-        k_wfd_tiled<T, R, S, GROUPS><<<grid, WX * WY, smem, st>>>(
-            (const T*)in + b0 * ng, (T*)out + b0 * ng, nb, g, P, s, G, chunk0, tiles_x);
+        k_wfd_tiled<T, R, S, GROUPS, MODE><<<grid, WX * WY, smem, st>>>(
+            (const T*)in + b0 * ng, (T*)out + b0 * ng, nb, g, P, s, G, chunk0, tiles_x, rhs, wj);
     }
     return 0;
 }
 
-template <class T, int R, int S>
+template <class T, int R, int S, int MODE>
 static int launch_wfd_tiled_rs(const void* in, void* out, int nin, const GridBC& g,
-                               const Phases& P, const WStencil& s, cudaStream_t st) {
+                               const Phases& P, const WStencil& s, cudaStream_t st,
+                               const double* rhs, double wj) {
     WGroups G;
     if (wfd_groups(s, R, G))
-        return launch_wfd_tiled_k<T, R, S, true>(in, out, nin, g, P, s, G, st);
-    return launch_wfd_tiled_k<T, R, S, false>(in, out, nin, g, P, s, G, st);
+        return launch_wfd_tiled_k<T, R, S, true, MODE>(in, out, nin, g, P, s, G, st, rhs, wj);
+    return launch_wfd_tiled_k<T, R, S, false, MODE>(in, out, nin, g, P, s, G, st, rhs, wj);
 }
 
-template <class T>
+// MODE 1 (weighted Jacobi, real data): `rhs` the source term, `wj` the
+// relaxation weight.
+template <class T, int MODE = 0>
 static int launch_wfd_tiled(const void* in, void* out, int nin, const GridBC& g,
-                            const Phases& P, const WStencil& s, cudaStream_t st) {
+                            const Phases& P, const WStencil& s, cudaStream_t st,
+                            const double* rhs = nullptr, double wj = 0.0) {
     if (!s.cfd) return -1;
     const int nc = s.start[s.nw - 1] + s.ncoefs[s.nw - 1];
     for (int c = 0; c < nc; c++) {
@@ -487,15 +507,15 @@ static int launch_wfd_tiled(const void* in, void* out, int nin, const GridBC& g,
         if (nz > 1) return -1;
     }
     switch (s.range) {
-        case 1: return launch_wfd_tiled_rs<T, 1, 4>(in, out, nin, g, P, s, st);
-        case 2: return launch_wfd_tiled_rs<T, 2, 8>(in, out, nin, g, P, s, st);
-        case 3: return launch_wfd_tiled_rs<T, 3, 8>(in, out, nin, g, P, s, st);
+        case 1: return launch_wfd_tiled_rs<T, 1, 4, MODE>(in, out, nin, g, P, s, st, rhs, wj);
+        case 2: return launch_wfd_tiled_rs<T, 2, 8, MODE>(in, out, nin, g, P, s, st, rhs, wj);
+        case 3: return launch_wfd_tiled_rs<T, 3, 8, MODE>(in, out, nin, g, P, s, st, rhs, wj);
     }
     if constexpr (sizeof(T) == 8) {
         switch (s.range) {
-            case 4: return launch_wfd_tiled_rs<T, 4, 16>(in, out, nin, g, P, s, st);
-            case 5: return launch_wfd_tiled_rs<T, 5, 16>(in, out, nin, g, P, s, st);
-            case 6: return launch_wfd_tiled_rs<T, 6, 16>(in, out, nin, g, P, s, st);
+            case 4: return launch_wfd_tiled_rs<T, 4, 16, MODE>(in, out, nin, g, P, s, st, rhs, wj);
+            case 5: return launch_wfd_tiled_rs<T, 5, 16, MODE>(in, out, nin, g, P, s, st, rhs, wj);
+            case 6: return launch_wfd_tiled_rs<T, 6, 16, MODE>(in, out, nin, g, P, s, st, rhs, wj);
         }
     }
     return -1;
@@ -648,9 +668,14 @@ extern "C" int gb_woperator_relax(gb_woperator* op, int method, double* f, const
         src = X;
     }
     const int ng = (int)op->ng();
+    const Phases P0{};
     for (int it = 0; it < nrelax; it++) {
         double* dst = (src == f) ? X : f;
-        k_wjacobi<<<(ng + 255) / 256, 256, 0, st>>>(src, dst, s, g, op->s, w);
+        // the plane-marching kernel for axis-aligned operators, else one
+        // thread a point
+        const int rc = launch_wfd_tiled<double, 1>(src, dst, 1, g, P0, op->s, st, s, w);
+        if (rc == -2) return fail(GB_ECUDA, "WOperator relax: could not raise the shared-memory limit");
+        if (rc != 0) k_wjacobi<<<(ng + 255) / 256, 256, 0, st>>>(src, dst, s, g, op->s, w);
         src = dst;
     }
     GB_LAUNCH_CHECK();
