@@ -48,6 +48,7 @@ class WeightedFDPoissonSolver(FDPoissonSolver):
         """``dielectric.eps_gradeps``: [eps, d eps/dx, d eps/dy, d eps/dz],
         float64 CUDA tensors of the grid shape (kept, not copied)."""
         self.dielectric = dielectric
+        self._graph = None
 
     def create_laplace(self, gd, scale=1.0, n=1, dtype=float):
         """:80-85: the Laplacian and the three gradients, weighted."""
@@ -65,6 +66,7 @@ class WeightedFDPoissonSolver(FDPoissonSolver):
         fills; work arrays of every level."""
         if self._initialized:
             return
+        self._graph = None      # captured with the previous arrays
         if self.dielectric is None:
             raise RuntimeError('WeightedFDPoissonSolver: set_dielectric '
                                'first')
@@ -152,14 +154,84 @@ class WeightedFDPoissonSolver(FDPoissonSolver):
         raise NotImplementedError(
             'charged system with mixed boundary conditions')
 
+    def _vcycle_graph(self, like):
+        """One V-cycle (iterate2 on the solver's own level-0 arrays, the
+        squared residual left on the device) captured as a CUDA graph, so
+        that a V-cycle costs one graph launch and one scalar read instead
+        of some sixty launches from Python.  Built on first use; the
+        weights it reads are the solver's arrays, refreshed in place by
+        restrict_op_weights."""
+        g = getattr(self, '_graph', None)
+        if g is not None and self._graph_phi.device == like.device:
+            return g
+        import torch
+        self._graph_phi = torch.zeros_like(like)
+        self._graph_err = torch.zeros((), dtype=like.dtype,
+                                      device=like.device)
+
+        def body():
+            self.phis[0] = self._graph_phi
+            self._cycle_no_read(0)
+            r = self.residuals[0].reshape(-1)
+            self._graph_err.copy_(torch.dot(r, r))
+
+        side = torch.cuda.Stream(device=like.device)
+        side.wait_stream(torch.cuda.current_stream())
+        saved = self._graph_phi.clone()
+        with torch.cuda.stream(side):
+            body()                        # allocates scratch, loads kernels
+        torch.cuda.current_stream().wait_stream(side)
+        self._graph_phi.copy_(saved)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=side):
+            body()
+        self._graph = g
+        return g
+
+    def _cycle_no_read(self, level):
+        """iterate2's V-cycle below `level` without the final host read."""
+        residual = self.residuals[level]
+        op = self.operators[level]
+        if level < self.levels:
+            op.relax(self.relax_method, self.phis[level], self.rhos[level],
+                     self.presmooths[level], self.weights[level])
+            op.apply(self.phis[level], residual)
+            residual -= self.rhos[level]
+            self.restrictors[level].apply(residual, self.rhos[level + 1])
+            self.phis[level + 1].zero_()
+            self._cycle_no_read(level + 1)
+            self.interpolators[level].apply(self.phis[level + 1], residual)
+            self.phis[level] -= residual
+        op.relax(self.relax_method, self.phis[level], self.rhos[level],
+                 self.postsmooths[level], self.weights[level])
+        if level == 0:
+            op.apply(self.phis[level], residual)
+            residual -= self.rhos[level]
+
     def solve_neutral(self, phi, rho, timer=None):
-        """gpaw/poisson.py:474-498."""
+        """gpaw/poisson.py:474-498.  On a GPU every V-cycle is one replay
+        of a captured graph (GPAW_B200_WGRAPH=0: launched op by op)."""
+        import os
         self._init()
-        self.phis[0] = phi
         self.rhos[0].copy_(rho)
-        niter = 1
-        while self.iterate2(self.step) > self.eps and niter < self.maxiter:
-            niter += 1
+        if phi.is_cuda and os.environ.get('GPAW_B200_WGRAPH', '1') != '0':
+            g = self._vcycle_graph(phi)
+            self._graph_phi.copy_(phi)
+            niter = 1
+            while True:
+                g.replay()
+                err = float(self._graph_err) * self.gd.dv
+                if not (err > self.eps and niter < self.maxiter):
+                    break
+                niter += 1
+            phi.copy_(self._graph_phi)
+            self.phis[0] = phi
+        else:
+            self.phis[0] = phi
+            niter = 1
+            while self.iterate2(self.step) > self.eps and \
+                    niter < self.maxiter:
+                niter += 1
         if niter == self.maxiter:
             raise PoissonConvergenceError(
                 'Poisson solver did not converge in %d iterations!'
