@@ -28,11 +28,12 @@ class FDPoissonSolver:
                  remove_moment=None, use_charge_center=False,
                  metallic_electrodes=False,
                  use_charged_periodic_corrections=False, xp=None):
-        if remove_moment or metallic_electrodes or \
-                use_charged_periodic_corrections:
-            raise NotImplementedError(
-                'moment removal / electrodes / charged periodic '
-                'corrections are not part of this path')
+        assert metallic_electrodes in [False, None, 'single', 'both']
+        self.remove_moment = remove_moment
+        self.metallic_electrodes = metallic_electrodes
+        self.use_charged_periodic_corrections = \
+            use_charged_periodic_corrections
+        self.charged_periodic_correction = None
         self.use_charge_center = bool(use_charge_center)
         self.eps = eps
         self.relax = relax
@@ -51,8 +52,14 @@ class FDPoissonSolver:
     def todict(self):
         d = {'name': 'fd', 'nn': self.nn, 'relax': self.relax,
              'eps': self.eps}
+        if self.remove_moment:
+            d['remove_moment'] = self.remove_moment
         if self.use_charge_center:
             d['use_charge_center'] = True
+        if self.use_charged_periodic_corrections:
+            d['use_charged_periodic_corrections'] = True
+        if self.metallic_electrodes:
+            d['metallic_electrodes'] = self.metallic_electrodes
         return d
 
     def get_stencil(self):
@@ -144,14 +151,20 @@ class FDPoissonSolver:
 
     def solve(self, phi, rho, charge=None, maxcharge=1e-6,
               zero_initial_phi=False, timer=None):
-        """gpaw/poisson.py:182-231: neutral systems, and charged periodic
-        ones (homogeneous background).  Returns the number of V-cycles."""
+        """gpaw/poisson.py:182-312: neutral systems; multipole removal
+        (``remove_moment``, non-periodic cells); charged periodic ones
+        (homogeneous background, plus the Madelung correction with
+        ``use_charged_periodic_corrections``); charged non-periodic ones
+        (Gaussian monopole); charged ones with mixed boundaries
+        (``metallic_electrodes``).  Returns the number of V-cycles."""
         self._init()
         assert tuple(phi.shape) == tuple(self.gd.n_c)
         assert tuple(rho.shape) == tuple(self.gd.n_c)
         actual_charge = self.gd.integrate(rho)
         background = (actual_charge / self.gd.dv /
                       self.gd.get_size_of_global_array().prod())
+        if self.remove_moment:
+            return _solve_removing_moments(self, phi, rho)
         if charge is None:
             charge = actual_charge
         if abs(charge) <= maxcharge:
@@ -159,7 +172,14 @@ class FDPoissonSolver:
         if self.gd.pbc_c.all():
             if zero_initial_phi:
                 phi.zero_()
-            return self.solve_neutral(phi, rho - background)
+            niter = self.solve_neutral(phi, rho - background)
+            if self.use_charged_periodic_corrections:
+                if self.charged_periodic_correction is None:
+                    from .ewald import madelung
+                    self.charged_periodic_correction = madelung(
+                        self.gd.cell_cv)
+                phi += actual_charge * self.charged_periodic_correction
+            return niter
         if not self.gd.pbc_c.any():
             center = None
             if self.use_charge_center:
@@ -168,9 +188,23 @@ class FDPoissonSolver:
                     self.gd, rho, actual_charge))
             return _solve_monopole(self, phi, rho, actual_charge,
                                    zero_initial_phi, center)
+        if self.metallic_electrodes == 'single':
+            # a dipole layer against the far electrode along axis 2
+            # (gpaw/poisson.py:286-301)
+            from .dipole import dipole_correction
+            origin = [0, 0, int(self.gd.N_c[2])]
+            drho, dphi, corr = dipole_correction(2, self.gd, rho,
+                                                 origin_c=origin)
+            phi -= dphi
+            niter = self.solve_neutral(phi, rho + drho)
+            phi += dphi
+            phi -= corr
+            self.correction = 0.0
+            return niter
+        if self.metallic_electrodes == 'both':
+            return self.solve_neutral(phi, rho)
         raise NotImplementedError(
-            'charged system with mixed boundary conditions (dipole '
-            'correction / metallic electrodes)')
+            'Charged systems with mixed periodic/zero boundary conditions')
 
     def _rhs(self, rho):
         """rho, or B rho for the Mehrstellen stencil (gpaw/poisson.py:
@@ -284,6 +318,44 @@ def stencil_spectrum(op, gd):
     flat = np.sort(lam.ravel())
     lmin = float(flat[1] if gd.pbc_c.all() else flat[0])
     return lmin, lmax
+
+
+def _solve_removing_moments(ps, phi, rho):
+    """``remove_moment = n`` (gpaw/poisson.py:192-208, non-periodic cells):
+    the density's multipole moments L = 0 .. n-1 about the cell centre are
+    taken out with the generalised Gaussians g_L (moments below 1e-7 are
+    left), the rest is solved, and the Gaussians' potentials are added back
+    (they also shift the initial guess).  Gaussians, their potentials and
+    the harmonics are built once per grid (host float64) and kept on the
+    device; the moments are device sums."""
+    assert not ps.gd.pbc_c.any()
+    n = int(ps.remove_moment)
+    cache = getattr(ps, '_moment_gd', None)
+    dev = phi.device
+    if cache is not ps.gd or len(ps._moment_g) < n:
+        from .multipole import Gaussian
+        G = Gaussian(ps.gd)
+        ps._moment_g = [torch.from_numpy(G.get_gauss(L)).to(dev)
+                        for L in range(n)]
+        ps._moment_v = [torch.from_numpy(G.get_gauss_pot(L)).to(dev)
+                        for L in range(n)]
+        ps._moment_y = [torch.from_numpy(G.get_Y(L)).to(dev)
+                        for L in range(n)]
+        ps._moment_gd = ps.gd
+    rho_n = rho.clone()
+    cors = []
+    for L in range(n):
+        q = float((rho_n * ps._moment_y[L]).sum()) * ps.gd.dv
+        if abs(q) < 1e-7:
+            continue
+        rho_n -= q * ps._moment_g[L]
+        cors.append(q * ps._moment_v[L])
+    for c in cors:
+        phi -= c
+    niter = ps.solve_neutral(phi, rho_n)
+    for c in cors:
+        phi += c
+    return niter
 
 
 def _solve_monopole(ps, phi, rho, actual_charge, zero_initial_phi,

@@ -951,9 +951,11 @@ def interpolate_density(gd, finegd, nt_sR, n=3):
     return f[0] if one else f
 
 
-def calculate_dipole_moment(gd, rho_g):
-    """gpaw/old/grid_descriptor.py:648-663 (center=False, no origin)."""
+def calculate_dipole_moment(gd, rho_g, origin_c=None):
+    """gpaw/old/grid_descriptor.py:648-663 (center=False)."""
     r_cz = [np.arange(gd.beg_c[c], gd.end_c[c]) for c in range(3)]
+    if origin_c is not None:
+        r_cz = [r_cz[c] - origin_c[c] for c in range(3)]
     rho_01 = rho_g.sum(axis=2)
     rho_02 = rho_g.sum(axis=1)
     rho_cz = [rho_01.sum(axis=1), rho_01.sum(axis=0), rho_02.sum(axis=0)]
@@ -961,10 +963,10 @@ def calculate_dipole_moment(gd, rho_g):
     return -np.dot(rhog_c, gd.h_cv) * gd.dv
 
 
-def dipole_correction(c, gd, rhot_g):
+def dipole_correction(c, gd, rhot_g, origin_c=None):
     """gpaw/dipole_correction.py:125-172 (center=False)."""
     from scipy.special import erf
-    moment = calculate_dipole_moment(gd, rhot_g)[c]
+    moment = calculate_dipole_moment(gd, rhot_g, origin_c)[c]
     if abs(moment) < 1e-12:
         return gd.zeros(), gd.zeros(), 0.0
     r_g = gd.get_grid_point_coordinates()[c]
@@ -972,7 +974,7 @@ def dipole_correction(c, gd, rhot_g):
     sr_g = 2.0 / cellsize * r_g - 1.0
     alpha = 12.0
     drho_g = sr_g * np.exp(-alpha * sr_g**2)
-    moment2 = calculate_dipole_moment(gd, drho_g)[c]
+    moment2 = calculate_dipole_moment(gd, drho_g, origin_c)[c]
     factor = -moment / moment2
     drho_g *= factor
     phifactor = factor * (np.pi / alpha)**1.5 * cellsize**2 / 4.0

@@ -977,3 +977,96 @@ def test_extra_vacuum_against_oracle(coarses, gpts, cuda):
     assert n == n_o
     assert max_rel(to_np(phi), phi_o) <= RTOL_FP64
     assert 'ExtraVacuum' in evp.get_description()
+
+
+# ----------------------------------- FDPoissonSolver's remaining options
+def test_remove_moment_against_oracle(cuda):
+    """FDPoissonSolver(remove_moment=4) (gpaw/poisson.py:192-208) on a
+    charged, polarised density in a zero-boundary cell against the
+    reference's algorithm restated with the oracle's Gaussians and
+    solver: the same V-cycle count, phi to the 1e-12 bar."""
+    from gpaw_b200 import FDPoissonSolver
+    N, cell = (40, 36, 44), (7.0, 6.3, 7.7)
+    gdo = L.GridDescriptor(N, cell, 0)
+    gdp = prod_gd(N, cell, 0)
+    x = gdo.get_grid_point_coordinates()
+    c = np.array(cell)[:, None, None, None] / 2
+    rho = 1.3 * np.exp(-((x - c + 0.6)**2).sum(0)) - \
+        0.4 * np.exp(-1.5 * ((x - c - 0.8)**2).sum(0))
+    po = L.FDPoissonSolver(nn=3, eps=1e-16)
+    po.set_grid_descriptor(gdo)
+    G = L.GaussianMP(gdo)
+    rho_n = rho.copy()
+    cors = [G.remove_moment(rho_n, Lm) for Lm in range(4)]
+    ref = gdo.zeros()
+    for cor in cors:
+        ref -= cor
+    n_ref = po.solve_neutral(ref, rho_n)
+    for cor in cors:
+        ref += cor
+    ps = FDPoissonSolver(nn=3, eps=1e-16, remove_moment=4)
+    ps.set_grid_descriptor(gdp)
+    phi = gdp.zeros()
+    n = ps.solve(phi, to_dev(rho))
+    assert n == n_ref
+    assert max_rel(to_np(phi), ref) <= RTOL_FP64
+    assert ps.todict()['remove_moment'] == 4
+
+
+def test_charged_periodic_madelung_correction(cuda):
+    """use_charged_periodic_corrections (gpaw/poisson.py:214-231): the
+    potential of a charged periodic cell shifted by charge x the Madelung
+    potential of the lattice (pinned to the reference's Ewald values on the
+    CPU), i.e. exactly the plain solve plus that constant."""
+    from gpaw_b200 import FDPoissonSolver
+    from gpaw_b200.ewald import madelung
+    N, cell = (32, 28, 36), (5.0, 4.4, 5.6)
+    gdp = prod_gd(N, cell, 1)
+    rng = np.random.default_rng(4)
+    rho = to_dev(rng.standard_normal(N) + 0.3)
+    out = {}
+    for corr in (False, True):
+        ps = FDPoissonSolver(nn=3, eps=1e-14,
+                             use_charged_periodic_corrections=corr)
+        ps.set_grid_descriptor(gdp)
+        phi = gdp.zeros()
+        out[corr] = (ps.solve(phi, rho), to_np(phi))
+    q = float(gdp.integrate(rho))
+    assert out[True][0] == out[False][0]
+    shift = out[True][1] - out[False][1]
+    want = q * madelung(np.diag(cell))
+    assert np.abs(shift - want).max() <= 1e-12 * abs(want)
+
+
+@pytest.mark.parametrize('electrodes', ['single', 'both'])
+def test_metallic_electrodes_against_oracle(electrodes, cuda):
+    """metallic_electrodes (gpaw/poisson.py:284-310) for a charged slab,
+    periodic in x and y: 'both' solves the charged density as it is,
+    'single' adds a dipole layer against the electrode at the top of z
+    and shifts by its potential step; against the reference's branch
+    restated on the oracle."""
+    from gpaw_b200 import FDPoissonSolver
+    N, cell, pbc = (24, 24, 48), (5.0, 5.0, 12.0), (1, 1, 0)
+    gdo = L.GridDescriptor(N, cell, pbc)
+    gdp = prod_gd(N, cell, pbc)
+    x = gdo.get_grid_point_coordinates()
+    rho = np.exp(-((x[2] - 5.0)**2) / 0.8) * (1.0 + 0.2 * np.cos(
+        2 * np.pi * x[0] / 5.0))
+    po = L.FDPoissonSolver(nn=3, eps=1e-16)
+    po.set_grid_descriptor(gdo)
+    ref = gdo.zeros()
+    if electrodes == 'both':
+        n_ref = po.solve_neutral(ref, rho)
+    else:
+        drho, dphi, corr = L.dipole_correction(2, gdo, rho,
+                                               origin_c=[0, 0, N[2]])
+        ref -= dphi
+        n_ref = po.solve_neutral(ref, rho + drho)
+        ref += dphi
+        ref -= corr
+    ps = FDPoissonSolver(nn=3, eps=1e-16, metallic_electrodes=electrodes)
+    ps.set_grid_descriptor(gdp)
+    phi = gdp.zeros()
+    n = ps.solve(phi, to_dev(rho))
+    assert n == n_ref
+    assert max_rel(to_np(phi), ref) <= RTOL_FP64

@@ -465,3 +465,18 @@ def test_grid_descriptor_reference_known_answers():
     r = gd.get_grid_point_distance_vectors(np.zeros(3))
     assert np.allclose(r[1, 1].reshape(4), [-0.5, -0.25, -1., -0.75],
                        rtol=1e-6, atol=1e-12)
+
+
+def test_madelung_matches_reference_golden():
+    """The Madelung potential of the charged-periodic correction
+    (gpaw_b200.ewald, an Ewald sum of our own) equals the reference's own
+    Ewald code (gpaw/utilities/ewald.py:143-145) on four cells, cubic to
+    triclinic: golden values made by tests/golden/make_madelung_golden.py."""
+    import json
+    import os
+    import numpy as np
+    from gpaw_b200.ewald import madelung
+    path = os.path.join(os.path.dirname(__file__), 'golden', 'madelung.json')
+    for case in json.load(open(path)):
+        got = madelung(np.array(case['cell']))
+        assert abs(got - case['madelung']) <= 1e-12 * abs(case['madelung'])
