@@ -42,6 +42,10 @@ SIGNATURES = {
     'gb_operator_get_diagonal_element': (C.c_double, [_p]),
     'gb_trace_begin': (C.c_int, [C.c_int]),
     'gb_device_fault': (C.c_int, [C.POINTER(C.c_int)]),
+    'gb_pool_set': (C.c_int, [C.c_int, C.c_size_t]),
+    'gb_pool_release': (C.c_int, []),
+    'gb_pool_stats': (C.c_int, [C.POINTER(C.c_size_t),
+                                C.POINTER(C.c_size_t)]),
     'gb_mixed_vcycle_eager': (C.c_int, [_p, _p, _p, _p]),
     'gb_mixed_set_fused_coarse': (C.c_int, [_p, C.c_int]),
     'gb_trace_end': (C.c_int, [C.c_int, C.POINTER(C.c_float),
@@ -154,6 +158,48 @@ class KernelTrace:
         self.intervals = [(labels[i].decode(), float(ms[i]))
                           for i in range(min(count.value, n))]
         return False
+
+
+def set_solver_pool(on=True, cache_limit=16 << 30):
+    """Switch the library's caching allocator of solver objects on or off
+    (gb_pool_set).  With it on, drop a solver only when none of its work
+    is in flight."""
+    check(load().gb_pool_set(int(bool(on)), int(cache_limit)))
+
+
+class solver_pool:
+    """Context manager: the solver-object pool on inside, its previous
+    state (off by default) restored on exit.  Objects built inside may be
+    dropped later; drop them only when none of their work is in flight."""
+
+    _depth = 0
+
+    def __init__(self, cache_limit=16 << 30):
+        self.cache_limit = int(cache_limit)
+
+    def __enter__(self):
+        if solver_pool._depth == 0:
+            set_solver_pool(True, self.cache_limit)
+        solver_pool._depth += 1
+        return self
+
+    def __exit__(self, *exc):
+        solver_pool._depth -= 1
+        if solver_pool._depth == 0:
+            set_solver_pool(False)
+        return False
+
+
+def solver_pool_stats():
+    """(bytes handed out, bytes cached) of the solver-object pool."""
+    live, cached = C.c_size_t(0), C.c_size_t(0)
+    check(load().gb_pool_stats(C.byref(live), C.byref(cached)))
+    return live.value, cached.value
+
+
+def release_solver_pool():
+    """Return every cached block of the pool to the driver."""
+    check(load().gb_pool_release())
 
 
 def i64(a):

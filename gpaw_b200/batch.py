@@ -16,7 +16,7 @@ import torch
 
 import ctypes as C
 
-from ._lib import check
+from ._lib import check, solver_pool
 from .cgpaw import _stream
 from .poisson import FDPoissonSolver, MixedPoissonSolver
 
@@ -30,18 +30,10 @@ class PoissonBatch:
         self.tol = tol
         self.precision = precision
         self.solvers = []
-        for gd in self.gds:
-            if precision == 'mixed':
-                # per-pass coarse kernels: the batch's solves run side by
-                # side, which cooperative kernels (the whole GPU at once)
-                # would serialise
-                ps = MixedPoissonSolver(nn=nn, tol=tol, maxiter=maxiter,
-                                        levels=levels, fused_coarse=False)
-            else:
-                ps = FDPoissonSolver(nn=nn, relax='J', eps=0.0,
-                                     maxiter=maxiter)
-            ps.set_grid_descriptor(gd)
-            self.solvers.append(ps)
+        # hundreds of solvers are built at once: through the library's
+        # caching allocator, which carves their buffers from a few slabs
+        with solver_pool():
+            self._build(nn, tol, maxiter, levels, precision)
         dev = self.gds[0].device if self.gds else torch.device('cuda')
         self.streams = [torch.cuda.Stream(device=dev)
                         for _ in range(max(1, nstreams))]
@@ -54,6 +46,20 @@ class PoissonBatch:
             check(lib.gb_mixed_batch_new(len(self.solvers), hs, float(tol),
                                          int(maxiter), C.byref(h)))
             self._batch = (lib, h)
+
+    def _build(self, nn, tol, maxiter, levels, precision):
+        for gd in self.gds:
+            if precision == 'mixed':
+                # per-pass coarse kernels: the batch's solves run side by
+                # side, which cooperative kernels (the whole GPU at once)
+                # would serialise
+                ps = MixedPoissonSolver(nn=nn, tol=tol, maxiter=maxiter,
+                                        levels=levels, fused_coarse=False)
+            else:
+                ps = FDPoissonSolver(nn=nn, relax='J', eps=0.0,
+                                     maxiter=maxiter)
+            ps.set_grid_descriptor(gd)
+            self.solvers.append(ps)
 
     def __del__(self):
         b = getattr(self, '_batch', None)

@@ -826,17 +826,17 @@ struct gb_poisson {
     ~gb_poisson() {
         if (solve_exec) cudaGraphExecDestroy(solve_exec);
         if (cap) cudaStreamDestroy(cap);
-        cudaFree(phi0);
-        cudaFree(rho0);
-        cudaFree(ctl);
-        if (ctl_host) cudaFreeHost(ctl_host);
-        for (size_t l = 1; l < phi.size(); l++) cudaFree(phi[l]);
-        for (size_t l = 1; l < rho.size(); l++) cudaFree(rho[l]);
-        for (double* p : res) cudaFree(p);
-        cudaFree(partial);
-        cudaFree(err_dev);
-        cudaFree(mean_dev);
-        if (err_host) cudaFreeHost(err_host);
+        dfree(phi0);
+        dfree(rho0);
+        dfree(ctl);
+        if (ctl_host) hfree(ctl_host);
+        for (size_t l = 1; l < phi.size(); l++) dfree(phi[l]);
+        for (size_t l = 1; l < rho.size(); l++) dfree(rho[l]);
+        for (double* p : res) dfree(p);
+        dfree(partial);
+        dfree(err_dev);
+        dfree(mean_dev);
+        if (err_host) hfree(err_host);
     }
 };
 
@@ -993,9 +993,9 @@ extern "C" int gb_poisson_new(int nlevels, gb_operator* const* operators,
     p->res.assign(nlevels, nullptr);
     for (int l = 0; l < nlevels; l++) {
         const size_t bytes = (size_t)p->ops[l]->ng() * sizeof(double);
-        cudaError_t e = cudaMalloc(&p->res[l], bytes);
-        if (e == cudaSuccess && l > 0) e = cudaMalloc(&p->phi[l], bytes);
-        if (e == cudaSuccess && l > 0) e = cudaMalloc(&p->rho[l], bytes);
+        cudaError_t e = pool_malloc(&p->res[l], bytes);
+        if (e == cudaSuccess && l > 0) e = pool_malloc(&p->phi[l], bytes);
+        if (e == cudaSuccess && l > 0) e = pool_malloc(&p->rho[l], bytes);
         if (e != cudaSuccess) {
             delete p;
             return fail(GB_ECUDA, "Poisson: cudaMalloc: %s", cudaGetErrorString(e));
@@ -1006,15 +1006,15 @@ extern "C" int gb_poisson_new(int nlevels, gb_operator* const* operators,
         }
     }
     const int nblk = std::max(residual_blocks(p->ops[0]->g), op_resid_blocks(p->ops[0], 1, 8));
-    cudaError_t e = cudaMalloc(&p->partial, (size_t)nblk * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc(&p->err_dev, sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc(&p->mean_dev, sizeof(double));
-    if (e == cudaSuccess) e = cudaMallocHost(&p->err_host, sizeof(double));
+    cudaError_t e = pool_malloc(&p->partial, (size_t)nblk * sizeof(double));
+    if (e == cudaSuccess) e = pool_malloc(&p->err_dev, sizeof(double));
+    if (e == cudaSuccess) e = pool_malloc(&p->mean_dev, sizeof(double));
+    if (e == cudaSuccess) e = pool_malloc_host(&p->err_host, sizeof(double));
     const size_t bytes0 = (size_t)p->ops[0]->ng() * sizeof(double);
-    if (e == cudaSuccess) e = cudaMalloc(&p->phi0, bytes0);
-    if (e == cudaSuccess) e = cudaMalloc(&p->rho0, bytes0);
-    if (e == cudaSuccess) e = cudaMalloc(&p->ctl, sizeof(SolveCtl));
-    if (e == cudaSuccess) e = cudaMallocHost(&p->ctl_host, sizeof(SolveCtl));
+    if (e == cudaSuccess) e = pool_malloc(&p->phi0, bytes0);
+    if (e == cudaSuccess) e = pool_malloc(&p->rho0, bytes0);
+    if (e == cudaSuccess) e = pool_malloc(&p->ctl, sizeof(SolveCtl));
+    if (e == cudaSuccess) e = pool_malloc_host(&p->ctl_host, sizeof(SolveCtl));
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p->cap, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         delete p;

@@ -116,4 +116,19 @@ int take_fault_transform(int* code);
 int take_fault_cfd(int* code);
 int take_fault_mixed(int* code);
 
+// caching allocator of the solver objects (gb_pool.cu): device memory and
+// pinned host memory; with the pool off these are cudaMalloc/cudaFree
+int dmalloc(void** p, size_t bytes);
+void dfree(void* p);
+int hmalloc(void** p, size_t bytes);
+void hfree(void* p);
+template <class T>
+inline cudaError_t pool_malloc(T** p, size_t bytes) {
+    return dmalloc((void**)p, bytes) ? cudaErrorMemoryAllocation : cudaSuccess;
+}
+template <class T>
+inline cudaError_t pool_malloc_host(T** p, size_t bytes) {
+    return hmalloc((void**)p, bytes) ? cudaErrorMemoryAllocation : cudaSuccess;
+}
+
 }  // namespace gb

@@ -712,22 +712,22 @@ struct gb_mixed {
     ~gb_mixed() {
         if (exec) cudaGraphExecDestroy(exec);
         if (cap) cudaStreamDestroy(cap);
-        for (float* p : b) cudaFree(p);
-        for (float* p : e) cudaFree(p);
-        for (float* p : t) cudaFree(p);
-        cudaFree(direct_tab);
-        cudaFree(coop_tab);
-        cudaFree(coop_bar);
-        cudaFree(x);
-        cudaFree(r);
-        cudaFree(da);
-        cudaFree(db);
-        cudaFree(phi0);
-        cudaFree(rho0);
-        cudaFree(partial);
-        cudaFree(nrm);
-        cudaFree(ctl);
-        if (ctl_host) cudaFreeHost(ctl_host);
+        for (float* p : b) dfree(p);
+        for (float* p : e) dfree(p);
+        for (float* p : t) dfree(p);
+        dfree(direct_tab);
+        dfree(coop_tab);
+        dfree(coop_bar);
+        dfree(x);
+        dfree(r);
+        dfree(da);
+        dfree(db);
+        dfree(phi0);
+        dfree(rho0);
+        dfree(partial);
+        dfree(nrm);
+        dfree(ctl);
+        if (ctl_host) hfree(ctl_host);
     }
 };
 
@@ -1099,7 +1099,7 @@ static int setup_direct(gb_mixed* m) {
                                          225 * 1024));
         attr = true;
     }
-    GB_CUDA_TRY(cudaMalloc(&m->direct_tab, ntab * sizeof(double)));
+    GB_CUDA_TRY(pool_malloc(&m->direct_tab, ntab * sizeof(double)));
     GB_CUDA_TRY(cudaMemcpy(m->direct_tab, tab.data(), ntab * sizeof(double),
                            cudaMemcpyHostToDevice));
     m->direct_s7 = s7;
@@ -1200,10 +1200,10 @@ static int setup_coop(gb_mixed* m) {
     GB_CUDA_TRY(cudaGetDevice(&dev));
     GB_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
     if (per_sm < 1) return 0;
-    GB_CUDA_TRY(cudaMalloc(&m->coop_tab, ntab * sizeof(double)));
+    GB_CUDA_TRY(pool_malloc(&m->coop_tab, ntab * sizeof(double)));
     GB_CUDA_TRY(cudaMemcpy(m->coop_tab, tab.data(), ntab * sizeof(double),
                            cudaMemcpyHostToDevice));
-    GB_CUDA_TRY(cudaMalloc(&m->coop_bar, 2 * sizeof(unsigned)));
+    GB_CUDA_TRY(pool_malloc(&m->coop_bar, 2 * sizeof(unsigned)));
     GB_CUDA_TRY(cudaMemset(m->coop_bar, 0, 2 * sizeof(unsigned)));
     P.nl = m->L - lc + 1;
     P.tab = m->coop_tab;
@@ -1269,9 +1269,9 @@ extern "C" int gb_mixed_new(int nlevels, gb_operator* op64, gb_operator* const* 
     for (int l = 0; l <= m->L && ce == cudaSuccess; l++) {
         const size_t bytes = (size_t)m->ops[l]->ng() * sizeof(float);
         float *bb = nullptr, *ee = nullptr, *tt = nullptr;
-        ce = cudaMalloc(&bb, bytes);
-        if (ce == cudaSuccess) ce = cudaMalloc(&ee, bytes);
-        if (ce == cudaSuccess) ce = cudaMalloc(&tt, bytes);
+        ce = pool_malloc(&bb, bytes);
+        if (ce == cudaSuccess) ce = pool_malloc(&ee, bytes);
+        if (ce == cudaSuccess) ce = pool_malloc(&tt, bytes);
         m->b.push_back(bb);
         m->e.push_back(ee);
         m->t.push_back(tt);
@@ -1280,16 +1280,16 @@ extern "C" int gb_mixed_new(int nlevels, gb_operator* op64, gb_operator* const* 
     const size_t n0 = (size_t)op64->ng() * sizeof(double);
     m->nres = op_resid_blocks(op64, 1, 8);
     m->nblk64 = std::max(m->nres, 1024);
-    if (ce == cudaSuccess) ce = cudaMalloc(&m->x, nc);
-    if (ce == cudaSuccess) ce = cudaMalloc(&m->r, nc);
-    if (ce == cudaSuccess) ce = cudaMalloc(&m->da, nc);
-    if (ce == cudaSuccess) ce = cudaMalloc(&m->db, nc);
-    if (ce == cudaSuccess) ce = cudaMalloc(&m->phi0, n0);
-    if (ce == cudaSuccess) ce = cudaMalloc(&m->rho0, n0);
-    if (ce == cudaSuccess) ce = cudaMalloc(&m->partial, (size_t)m->nblk64 * sizeof(double));
-    if (ce == cudaSuccess) ce = cudaMalloc(&m->nrm, 2 * sizeof(double));
-    if (ce == cudaSuccess) ce = cudaMalloc(&m->ctl, sizeof(Ctl));
-    if (ce == cudaSuccess) ce = cudaMallocHost(&m->ctl_host, sizeof(Ctl));
+    if (ce == cudaSuccess) ce = pool_malloc(&m->x, nc);
+    if (ce == cudaSuccess) ce = pool_malloc(&m->r, nc);
+    if (ce == cudaSuccess) ce = pool_malloc(&m->da, nc);
+    if (ce == cudaSuccess) ce = pool_malloc(&m->db, nc);
+    if (ce == cudaSuccess) ce = pool_malloc(&m->phi0, n0);
+    if (ce == cudaSuccess) ce = pool_malloc(&m->rho0, n0);
+    if (ce == cudaSuccess) ce = pool_malloc(&m->partial, (size_t)m->nblk64 * sizeof(double));
+    if (ce == cudaSuccess) ce = pool_malloc(&m->nrm, 2 * sizeof(double));
+    if (ce == cudaSuccess) ce = pool_malloc(&m->ctl, sizeof(Ctl));
+    if (ce == cudaSuccess) ce = pool_malloc_host(&m->ctl_host, sizeof(Ctl));
     if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&m->cap, cudaStreamNonBlocking);
     if (ce != cudaSuccess) {
         delete m;

@@ -49,15 +49,14 @@ struct Scratch {
     void* ptr = nullptr;
     size_t bytes = 0;
     ~Scratch() {
-        if (ptr) cudaFree(ptr);
+        if (ptr) dfree(ptr);
     }
     int ensure(size_t want) {
         if (want <= bytes) return 0;
-        if (ptr) cudaFree(ptr);
+        if (ptr) dfree(ptr);
         ptr = nullptr;
         bytes = 0;
-        cudaError_t e = cudaMalloc(&ptr, want);
-        if (e != cudaSuccess) return fail(GB_ECUDA, "cudaMalloc(%zu): %s", want, cudaGetErrorString(e));
+        if (int rc = dmalloc(&ptr, want)) return rc;
         bytes = want;
         return 0;
     }

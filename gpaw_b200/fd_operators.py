@@ -157,11 +157,66 @@ class GUCLaplace(FDOperator):
 
 
 def Laplace(gd, scale=1.0, n=1, dtype=float, xp=None):
-    """gpaw/fd_operators.py:177-181 (n = 9, the FFT Laplacian, is not part
-    of the finite-difference path)."""
+    """gpaw/fd_operators.py:177-181: n = 9 selects the spectral Laplacian
+    of a periodic cell, 1..6 the finite-difference stencils."""
     if n == 9:
-        raise NotImplementedError('FFT Laplacian (n=9) is not provided')
+        return FTLaplace(gd, scale, dtype)
     return GUCLaplace(gd, scale, n, dtype, xp=xp)
+
+
+class FTLaplace:
+    """Spectral Laplacian of a fully periodic cell (gpaw/fd_operators.py:
+    399-424): the input's discrete Fourier transform is multiplied by
+    -scale |k|^2, with k = 2 pi B^T i for the integer frequencies i folded
+    into [-N/2, N/2), and transformed back; the real part is kept (for
+    complex input too, as the reference does, and Bloch phases are
+    ignored).  The transforms are cuFFT's (through torch.fft); the factor
+    table lives on the device.  For real input the half-spectrum transform
+    is used with the table averaged over i and -i (folded): the real part
+    of the full transform equals exactly that, because the spectrum of real
+    data is Hermitian.  (The table itself is not symmetric on the Nyquist
+    planes of a non-orthogonal cell.)"""
+
+    def __init__(self, gd, scale, dtype=float):
+        import torch
+        assert gd.pbc_c.all(), 'the spectral Laplacian needs a periodic cell'
+        N = np.asarray(gd.N_c)
+        i_cq = np.indices(tuple(N)).reshape((3, -1))
+        i_cq = (i_cq + N[:, None] // 2) % N[:, None] - N[:, None] // 2
+        k_vq = np.dot(2.0 * np.pi * gd.icell_cv.T, i_cq)
+        k2 = (k_vq * k_vq).sum(axis=0).reshape(tuple(N)) * (-scale)
+        self.gd = gd
+        self.dtype = dtype
+        self.shape = tuple(int(n) for n in N)
+        self.k2_Q = torch.from_numpy(k2).to(gd.device)
+        k2_neg = np.roll(np.flip(k2), 1, axis=(0, 1, 2))   # k2 at -i
+        half = self.shape[2] // 2 + 1
+        self.k2_half = torch.from_numpy(
+            np.ascontiguousarray(0.5 * (k2 + k2_neg)[:, :, :half])).to(
+                gd.device)
+        self.d = 6.0 / gd.h_cv[0, 0]**2
+        self.npoints = 1000
+        self.description = 'FFT Laplacian'
+
+    def apply(self, in_xg, out_xg, phase_cd=None):
+        import torch
+        if not (in_xg.is_cuda and out_xg.is_cuda):
+            raise TypeError('FTLaplace works on CUDA tensors')
+        assert tuple(in_xg.shape[-3:]) == self.shape
+        dims = (-3, -2, -1)
+        if in_xg.is_complex():
+            out = torch.fft.ifftn(torch.fft.fftn(in_xg, dim=dims) *
+                                  self.k2_Q, dim=dims).real
+        else:
+            out = torch.fft.irfftn(torch.fft.rfftn(in_xg, dim=dims) *
+                                   self.k2_half, s=self.shape, dim=dims)
+        out_xg.copy_(out)
+
+    def get_diagonal_element(self):
+        return self.d
+
+    def get_description(self):
+        return self.description
 
 
 class LaplaceA(FDOperator):

@@ -74,7 +74,7 @@ class Server:
     SPACING = 0.18 / 0.52917721   # Bohr
 
     def __init__(self, hbm_budget=8 << 30, nslots=8, tol=1e-10,
-                 device=None, grow=True):
+                 device=None, grow=True, pool=True):
         self.device = torch.device(device if device is not None else 'cuda')
         self.budget = int(hbm_budget)
         self.tol = tol
@@ -95,6 +95,10 @@ class Server:
         self.lru = collections.OrderedDict()     # id(solver) -> (N, solver)
         self.built = 0
         self.evicted = 0
+        # solvers are built and evicted through the library's caching
+        # allocator while the loop runs (an evicted solver is idle), so a
+        # new shape costs no driver allocation and no device-wide sync
+        self.pool = pool
 
     # -- resources ---------------------------------------------------------
     def _gd(self, N):
@@ -119,7 +123,11 @@ class Server:
             ps = pool.pop()
             self.lru.pop(id(ps), None)
             return ps, 0
-        ps = MixedPoissonSolver(nn=3, tol=self.tol, levels=4)
+        # per-pass coarse kernels: concurrent solves run side by side, where
+        # a cooperative coarse kernel (one block on every SM) would wait for
+        # the whole GPU
+        ps = MixedPoissonSolver(nn=3, tol=self.tol, levels=4,
+                                fused_coarse=False)
         ps.set_grid_descriptor(self._gd(req.N))
         self.built += 1
         return ps, self.solver_bytes(req.N)
@@ -134,10 +142,19 @@ class Server:
             self.evicted += 1
         return self.resident + self.in_use + need <= self.budget
 
+    def _pooled(self):
+        from contextlib import nullcontext
+        from ._lib import solver_pool
+        return solver_pool(self.budget) if self.pool else nullcontext()
+
     def warm(self, shapes, per_shape=2):
         """Build `per_shape` resident solvers (graphs captured) and one
         operator per shape ahead of time, run each once, and size the
         slot slabs."""
+        with self._pooled():
+            self._warm(shapes, per_shape)
+
+    def _warm(self, shapes, per_shape):
         for N in shapes:
             built = []
             for _ in range(per_shape):
@@ -222,7 +239,7 @@ class Server:
     def _finish(self, job, now):
         req = job['req']
         req.done = now
-        req.result = job['out'].numpy().copy()
+        req.result = job['out'].numpy()     # the request's own buffer
         if job['solver'] is not None:
             req.niter = job['solver'].result()
             self.pools[('poisson', req.N)].append(job['solver'])
@@ -250,7 +267,8 @@ class Server:
         gc.collect()
         gc.disable()
         try:
-            return self._serve(pending, active, inputs, outputs)
+            with self._pooled():
+                return self._serve(pending, active, inputs, outputs)
         finally:
             if gc_was_on:
                 gc.enable()

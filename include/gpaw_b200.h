@@ -28,6 +28,7 @@
 #ifndef GPAW_B200_H
 #define GPAW_B200_H
 
+#include <stddef.h>
 #include <stdint.h>
 
 #if defined(__GNUC__)
@@ -138,6 +139,20 @@ GB_API int gb_operator_relax_noalloc(gb_operator* op, int method, double* f, con
  * (synchronous): *code = 0 when nothing was recorded, 1 for a copy that
  * did not complete in time. */
 GB_API int gb_device_fault(int* code);
+
+/* Caching allocator of the solver objects (gb_poisson, gb_mixed and the
+ * operators' scratch); no counterpart in the reference, whose C objects
+ * hold static buffers.  With the pool on, memory an object frees is kept,
+ * binned by size class (four per power of two), and handed to the next
+ * object that needs that class, so that building and dropping solvers
+ * neither calls the driver nor synchronises the device.  The caller then
+ * must free an object only when none of its work is in flight.  The cache
+ * holds at most `cache_limit` bytes (the largest blocks go first);
+ * gb_pool_release returns every cached block to the driver; gb_pool_stats
+ * gives the bytes handed out and the bytes cached.  Off by default. */
+GB_API int gb_pool_set(int on, size_t cache_limit);
+GB_API int gb_pool_release(void);
+GB_API int gb_pool_stats(size_t* live, size_t* cached);
 
 /* Kernel timeline of composite calls; a profiling aid with no counterpart
  * in the reference.  Between gb_trace_begin(capacity) and gb_trace_end,

@@ -269,6 +269,20 @@ def Laplace(gd, scale=1.0, n=1, dtype=float, be='auto'):
     return FDOperator(coefs, offsets, gd, dtype, be=be)
 
 
+def ft_laplace(gd, scale, in_xg):
+    """FTLaplace.apply (gpaw/fd_operators.py:399-421) in numpy: the full
+    transforms of every grid of in_xg times -scale |k|^2, real part."""
+    N_c1 = gd.N_c[:, np.newaxis]
+    i_cq = np.indices(gd.N_c).reshape((3, -1))
+    i_cq = (i_cq + N_c1 // 2) % N_c1 - N_c1 // 2
+    icell_cv = np.linalg.inv(gd.cell_cv).T
+    k_vq = np.dot(2.0 * pi * icell_cv.T, i_cq)
+    k2_Q = (k_vq**2).sum(axis=0).reshape(gd.N_c) * (-scale)
+    ax = (-3, -2, -1)
+    out = np.fft.ifftn(np.fft.fftn(in_xg, axes=ax) * k2_Q, axes=ax).real
+    return out.astype(in_xg.dtype)
+
+
 def _mehrstellen_a(gd, scale):
     """LaplaceA's coefficients and offsets (gpaw/fd_operators.py:357-384)."""
     c = np.divide(-1 / 12, gd.h_cv.diagonal()**2) * scale

@@ -70,3 +70,41 @@ def test_mixed_nonconvergence_raises(cuda):
     with pytest.raises(PoissonConvergenceError):
         ps.solve_neutral(gdp.zeros(), to_dev(rho))
     assert ps.niter == 2
+
+
+def test_solver_pool_reuses_memory_and_results(cuda):
+    """Solvers built through the library's caching allocator (gb_pool_*):
+    a dropped solver's blocks are cached and handed to the next one of the
+    same size classes (no new driver memory), the results are bit-identical
+    to solvers built without the pool, and release empties the cache."""
+    import gc
+    from gpaw_b200 import GridDescriptor, MixedPoissonSolver
+    from gpaw_b200._lib import (release_solver_pool, solver_pool,
+                                solver_pool_stats)
+    from gpaw_b200.workloads import neutral_density_device
+    shapes = [(40, 56, 48), (32, 32, 64)]
+
+    def solve(N):
+        gd = GridDescriptor(N, tuple(0.34 * n for n in N), 0)
+        ps = MixedPoissonSolver(nn=3, tol=1e-10, levels=4)
+        ps.set_grid_descriptor(gd)
+        rho = neutral_density_device(gd, 6, 3)
+        phi = gd.zeros()
+        n = ps.solve_neutral(phi, rho)
+        return n, phi.cpu().numpy()
+
+    plain = [solve(N) for N in shapes]
+    gc.collect()
+    with solver_pool():
+        first = [solve(N) for N in shapes]
+        gc.collect()
+        live0, cached0 = solver_pool_stats()
+        assert cached0 > 0
+        again = [solve(N) for N in shapes]
+        gc.collect()
+        live1, cached1 = solver_pool_stats()
+        assert cached1 == cached0          # every block came from the cache
+    for a, b, c in zip(plain, first, again):
+        assert a[0] == b[0] == c[0]
+        assert np.array_equal(a[1], b[1]) and np.array_equal(a[1], c[1])
+    release_solver_pool()

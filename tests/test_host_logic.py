@@ -480,3 +480,33 @@ def test_madelung_matches_reference_golden():
     for case in json.load(open(path)):
         got = madelung(np.array(case['cell']))
         assert abs(got - case['madelung']) <= 1e-12 * abs(case['madelung'])
+
+
+def test_stencil_spectrum_bounds_equal_dense_sort():
+    """The solver's eigenvalue bounds of D^-1 A come from the per-axis
+    terms (rounded addition is monotone), in O(N): they equal, bit for bit,
+    the smallest / second smallest and largest of all N^3 values sorted."""
+    import numpy as np
+    from gpaw_b200 import GridDescriptor
+    from gpaw_b200.fd_operators import Laplace
+    from gpaw_b200.poisson import _stencil_spectrum_dense, stencil_spectrum
+    rng = np.random.default_rng(0)
+    n = 0
+    for t in range(120):
+        N = tuple(int(x) for x in rng.integers(2, 30, 3))
+        pbc = (1, 1, 1) if t % 3 == 0 else \
+            tuple(int(x) for x in rng.integers(0, 2, 3))
+        cell = tuple(float(x) for x in rng.uniform(2, 12, 3))
+        try:
+            gd = GridDescriptor(N, cell, pbc, device='cpu')
+        except Exception:
+            continue
+        for nn in (1, 3):
+            try:
+                op = Laplace(gd, -0.25 / np.pi, nn)
+            except AssertionError:      # stencil longer than the grid
+                continue
+            assert stencil_spectrum(op, gd) == \
+                _stencil_spectrum_dense(op, gd), (N, pbc, nn)
+            n += 1
+    assert n > 100
