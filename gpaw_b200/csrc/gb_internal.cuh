@@ -116,6 +116,17 @@ int take_fault_transform(int* code);
 int take_fault_cfd(int* code);
 int take_fault_mixed(int* code);
 
+// stencil pass with a linear epilogue for the mixed solver (gb_pass.cu):
+// v = p0 aux + p1 u + p2 (A u) + p3 aux2 written to out, added to acc64, or
+// written as float to out32 with per-CTA partials of v^2; -1 when the
+// operator or grid is not supported (caller falls back)
+bool pass_supported_grid(const GridBC& g, const CfdStencil& cs, int nn);
+int pass_blocks(const GridBC& g, int elem_bytes);
+template <class T>
+int launch_pass(const GridBC& g, const CfdStencil& cs, int nn, const T* in, T* out, const T* aux,
+                const T* aux2, double p0, double p1, double p2, double p3, double* acc64,
+                float* out32, double* partial, cudaStream_t st);
+
 // caching allocator of the solver objects (gb_pool.cu): device memory and
 // pinned host memory; with the pool off these are cudaMalloc/cudaFree
 int dmalloc(void** p, size_t bytes);

@@ -40,6 +40,9 @@ struct ChebLevel {
     double k1, k2;            // post-smooth coefficients
 };
 
+// Chebyshev smoothing on [lam_max / 8, 1.05 lam_max]: on the 192^3 grid
+// with four levels, lower bounds lam_max / 5 .. / 16 and upper factors
+// 1.0 .. 1.2 all took 14 to 23 V-cycles against 14 for this choice.
 ChebLevel cheb_level(double lam_max, double c0) {
     const double a = lam_max / 8.0, b = 1.05 * lam_max;
     const double theta = 0.5 * (b + a), delta = 0.5 * (b - a);
@@ -857,6 +860,16 @@ static bool lin32_direct() {
     return on;
 }
 
+// The level passes and the FP64 defect through k_pass (gb_pass.cu) unless
+// GPAW_B200_PASS=0 (the plane-marching kernel's EPI_LIN mode instead).
+static bool pass_on() {
+    static const bool on = [] {
+        const char* e = getenv("GPAW_B200_PASS");
+        return !(e && atoi(e) == 0);
+    }();
+    return on;
+}
+
 static int lin32(const gb_operator* op, const float* in, float* out, const float* aux,
                  const float* aux2, double p0, double p1, double p2, double p3, double* acc64,
                  cudaStream_t st) {
@@ -884,6 +897,15 @@ static int lin(gb_operator* op, const T* in, T* out, const T* aux, const T* aux2
     if constexpr (sizeof(T) == 4) {
         if (lin32_direct() && !partial && !out32 &&
             lin32(op, in, out, aux, aux2, p0, p1, p2, p3, acc64, st) == 0) {
+            GB_LAUNCH_CHECK();
+            return 0;
+        }
+    }
+    if (pass_on()) {
+        const int rc = launch_pass<T>(op->g, op->cs, op->nn, in, out, aux, aux2, p0, p1, p2, p3,
+                                      acc64, out32, partial, st);
+        if (rc == -2) return fail(GB_ECUDA, "mixed: could not raise the shared-memory limit");
+        if (rc == 0) {
             GB_LAUNCH_CHECK();
             return 0;
         }
@@ -1278,7 +1300,11 @@ extern "C" int gb_mixed_new(int nlevels, gb_operator* op64, gb_operator* const* 
     }
     const size_t nc = (size_t)m->ops[m->L]->ng() * sizeof(double);
     const size_t n0 = (size_t)op64->ng() * sizeof(double);
-    m->nres = op_resid_blocks(op64, 1, 8);
+    // partial sums of the defect: one per CTA of the pass kernel when it
+    // takes the level-0 operator, else of the plane-marching kernel
+    m->nres = (pass_on() && pass_supported_grid(op64->g, op64->cs, op64->nn))
+                  ? pass_blocks(op64->g, 8)
+                  : op_resid_blocks(op64, 1, 8);
     m->nblk64 = std::max(m->nres, 1024);
     if (ce == cudaSuccess) ce = pool_malloc(&m->x, nc);
     if (ce == cudaSuccess) ce = pool_malloc(&m->r, nc);
