@@ -123,7 +123,11 @@ struct WGroups {
 // diagonal of the weighted operator at the point, each operator's inner sum
 // and the accumulation in bmgs_wrelax's order (c/bmgs/wrelax.cpp:71-86),
 // the same arithmetic as k_wjacobi.
-template <class T, int R, int S, bool GROUPS, int MODE>
+// GR: 0 = tap tables, 1 = structured groups, 2 = structured groups of
+// exactly four operators (the solvation operator), with every operator and
+// group loop unrolled so that each coefficient is a compile-time operand and
+// the four weights are loaded before the taps.
+template <class T, int R, int S, int GR, int MODE>
 __global__ void __launch_bounds__(WX * WY)
 k_wfd_tiled(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Phases P,
             const __grid_constant__ WStencil s, const __grid_constant__ WGroups G, int chunk0,
@@ -244,6 +248,18 @@ k_wfd_tiled(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Ph
         sh_ip[c] = s.off[c][1] * PX + s.off[c][2];
     }
     const int cen = (ty + R) * PX + (tx + R);
+    // GR == 2: the weights (and the Jacobi source) of the next centre plane,
+    // loaded a plane ahead so that their latency overlaps a plane's taps
+    double wn[4] = {0.0, 0.0, 0.0, 0.0}, rn = 0.0;
+    auto fetch = [&](int pp) {
+        if (GR == 2 && own && pp < pb) {
+            const long long a2 = pp * pstride + (long long)gy * n2 + gx;
+#pragma unroll
+            for (int iw = 0; iw < 4; iw++) wn[iw] = __ldg(s.w[iw] + a2);
+            if (MODE == 1) rn = __ldg(rhs + a2);
+        }
+    };
+    fetch(pa);
 #pragma unroll 1
     for (int t = 0; t < total; t++) {
         asm volatile("cp.async.wait_group %0;\n" ::"n"(D - 1));
@@ -258,12 +274,22 @@ k_wfd_tiled(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Ph
         const long long at = p * pstride + (long long)gy * n2 + gx;
         T x = Num<T>::zero();
         double dg = 0.0;     // MODE 1: the diagonal sum_i w_i c_i0
-        if constexpr (GROUPS) {
+        double src = 0.0;    // MODE 1: the source term at the point
+        if constexpr (GR >= 1) {
             const T* c = ring + (cj & (S - 1)) * PL + cen;
-            for (int iw = 0; iw < s.nw; iw++) {
+            // one operator's term: inner sum from zero in coefficient order,
+            // scaled by its weight, added to the total (bmgs_wfd's order)
+            // one operator's term: inner sum from zero in coefficient order,
+            // scaled by its weight, added to the total (bmgs_wfd's order).
+            // Every tap is a shared-memory read: holding the 6 R neighbours
+            // in registers for the four operators to share measured slower
+            // (79-90 registers, half the CTAs an SM).
+            auto term = [&](int iw, double weight) {
                 T tmp = Num<T>::zero();
                 if (MODE == 0) tmp = Num<T>::add(tmp, Num<T>::scale(c[0], G.c0[iw]));
-                for (int k = 0; k < G.ng[iw]; k++) {
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    if (k >= G.ng[iw]) break;
                     const int ax = G.axis[iw][k];
                     if (ax == 0) {
 #pragma unroll
@@ -284,10 +310,20 @@ k_wfd_tiled(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Ph
                             tmp = Num<T>::add(tmp, Num<T>::scale(c[-d * sd], G.cm[iw][k][d - 1]));
                     }
                 }
-                const double weight = __ldg(s.w[iw] + at);
                 tmp = Num<T>::scale(tmp, weight);
                 x = Num<T>::add(x, tmp);
                 if (MODE == 1) dg = __dadd_rn(dg, __dmul_rn(weight, G.c0[iw]));
+            };
+            if constexpr (GR == 2) {
+                double wv[4];
+#pragma unroll
+                for (int iw = 0; iw < 4; iw++) wv[iw] = wn[iw];
+                src = rn;
+                fetch(p + 1);
+#pragma unroll
+                for (int iw = 0; iw < 4; iw++) term(iw, wv[iw]);
+            } else {
+                for (int iw = 0; iw < s.nw; iw++) term(iw, __ldg(s.w[iw] + at));
             }
         } else {
             for (int iw = 0; iw < s.nw; iw++) {
@@ -306,8 +342,9 @@ k_wfd_tiled(const T* __restrict__ in, T* __restrict__ out, int nin, GridBC g, Ph
         }
         if constexpr (MODE == 1 && sizeof(T) == 8) {
             const double old = ring[(cj & (S - 1)) * PL + cen];
+            if constexpr (GR != 2) src = rhs[at];
             o[at] = __dadd_rn(__dmul_rn(1.0 - wj, old),
-                              __ddiv_rn(__dmul_rn(wj, __dsub_rn(rhs[at], x)), dg));
+                              __ddiv_rn(__dmul_rn(wj, __dsub_rn(src, x)), dg));
         } else {
             o[at] = x;
         }
@@ -456,14 +493,14 @@ static bool wfd_groups(const WStencil& s, int R, WGroups& G) {
     return true;
 }
 
-template <class T, int R, int S, bool GROUPS, int MODE>
+template <class T, int R, int S, int GR, int MODE>
 static int launch_wfd_tiled_k(const void* in, void* out, int nin, const GridBC& g,
                               const Phases& P, const WStencil& s, const WGroups& G,
                               cudaStream_t st, const double* rhs, double wj) {
     constexpr size_t smem = (size_t)S * (WX + 2 * R) * (WY + 2 * R) * sizeof(T);
     static bool attr_done = false;
     if (!attr_done) {
-        if (cudaFuncSetAttribute(k_wfd_tiled<T, R, S, GROUPS, MODE>,
+        if (cudaFuncSetAttribute(k_wfd_tiled<T, R, S, GR, MODE>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem) != cudaSuccess)
             return -2;
@@ -477,7 +514,7 @@ static int launch_wfd_tiled_k(const void* in, void* out, int nin, const GridBC& 
     for (int b0 = 0; b0 < nin; b0 += 65535) {
         const int nb = min(65535, nin - b0);
         dim3 grid(tiles_x * tiles_y, nch, nb);
-        k_wfd_tiled<T, R, S, GROUPS, MODE><<<grid, WX * WY, smem, st>>>(
+        k_wfd_tiled<T, R, S, GR, MODE><<<grid, WX * WY, smem, st>>>(
             (const T*)in + b0 * ng, (T*)out + b0 * ng, nb, g, P, s, G, chunk0, tiles_x, rhs, wj);
     }
     return 0;
@@ -488,9 +525,12 @@ static int launch_wfd_tiled_rs(const void* in, void* out, int nin, const GridBC&
                                const Phases& P, const WStencil& s, cudaStream_t st,
                                const double* rhs, double wj) {
     WGroups G;
-    if (wfd_groups(s, R, G))
-        return launch_wfd_tiled_k<T, R, S, true, MODE>(in, out, nin, g, P, s, G, st, rhs, wj);
-    return launch_wfd_tiled_k<T, R, S, false, MODE>(in, out, nin, g, P, s, G, st, rhs, wj);
+    if (wfd_groups(s, R, G)) {
+        if (s.nw == 4)
+            return launch_wfd_tiled_k<T, R, S, 2, MODE>(in, out, nin, g, P, s, G, st, rhs, wj);
+        return launch_wfd_tiled_k<T, R, S, 1, MODE>(in, out, nin, g, P, s, G, st, rhs, wj);
+    }
+    return launch_wfd_tiled_k<T, R, S, 0, MODE>(in, out, nin, g, P, s, G, st, rhs, wj);
 }
 
 // MODE 1 (weighted Jacobi, real data): `rhs` the source term, `wj` the
