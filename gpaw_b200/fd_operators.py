@@ -7,6 +7,8 @@ path: a non-CUDA tensor raises TypeError.
 """
 from __future__ import annotations
 
+import functools
+
 import numpy as np
 
 from . import cgpaw
@@ -112,15 +114,26 @@ def laplace_stencil(gd, scale=1.0, n=1):
     (gpaw/fd_operators.py:184-238): pick the 3..6 shortest lattice
     directions whose second differences reproduce x^2, y^2, z^2 and no
     cross terms (least squares), then lay Chelikowsky's 1-D coefficients
-    along each."""
+    along each.  They depend on the grid spacing only, so they are cached
+    per (spacing vectors, scale, n): a solver hierarchy, or a serving loop
+    building solvers for many grid shapes of one spacing, computes them
+    once."""
+    coefs, offsets = _laplace_stencil(np.asarray(gd.h_cv, float).tobytes(),
+                                      float(scale), int(n))
+    return list(coefs), [np.array(o) for o in offsets]
+
+
+@functools.lru_cache(maxsize=256)
+def _laplace_stencil(h_bytes, scale, n):
+    h_cv = np.frombuffer(h_bytes).reshape(3, 3)
     M_ic = np.indices((3, 3, 3)).reshape((3, -3)).T[-13:] - 1
-    u_cv = gd.h_cv / (gd.h_cv**2).sum(1)[:, np.newaxis]**0.5
+    u_cv = h_cv / (h_cv**2).sum(1)[:, np.newaxis]**0.5
     u2_i = (np.dot(M_ic, u_cv)**2).sum(1)
     i_d = u2_i.argsort()
     m_mv = np.array([(2, 0, 0), (0, 2, 0), (0, 0, 2),
                      (0, 1, 1), (1, 0, 1), (1, 1, 0)])
     for D in range(3, 7):
-        h_dv = np.dot(M_ic[i_d[:D]], gd.h_cv)
+        h_dv = np.dot(M_ic[i_d[:D]], h_cv)
         A_md = (h_dv**m_mv[:, np.newaxis, :]).prod(2)
         a_d, residual, rank, s = np.linalg.lstsq(A_md, [1, 1, 1, 0, 0, 0],
                                                  rcond=-1)
@@ -139,7 +152,7 @@ def laplace_stencil(gd, scale=1.0, n=1):
         coefs.extend(a_d[d] * np.array(laplace[n][1:]))
         offsets.extend(np.arange(-1, -n - 1, -1)[:, np.newaxis] * M_c)
         coefs.extend(a_d[d] * np.array(laplace[n][1:]))
-    return coefs, offsets
+    return tuple(coefs), tuple(tuple(int(x) for x in o) for o in offsets)
 
 
 class GUCLaplace(FDOperator):
