@@ -700,6 +700,11 @@ struct gb_mixed {
     CoopPlan coop_plan{};
     double* coop_tab = nullptr;
     unsigned* coop_bar = nullptr;
+    // the single-CTA form of the same kernel over levels lt..L (each at most
+    // TAIL_MAX_POINTS points), for solves that run beside others
+    int tail_ok = 0, lt = 0;
+    CoopPlan tail_plan{};
+    unsigned* tail_bar = nullptr;
     double last_tol = 0.0;
     int last_maxiter = 0;
     std::vector<float*> b, e, t;       // levels 0..L (b[L], e[L] used at L)
@@ -720,6 +725,7 @@ struct gb_mixed {
         for (float* p : t) dfree(p);
         dfree(direct_tab);
         dfree(coop_tab);
+        dfree(tail_bar);
         dfree(coop_bar);
         dfree(x);
         dfree(r);
@@ -937,7 +943,14 @@ static int lin(gb_operator* op, const T* in, T* out, const T* aux, const T* aux2
 static thread_local bool t_no_coop = false;
 
 static int vcycle32(gb_mixed* m, int l, cudaStream_t st) {
-    if (m->coop && !t_no_coop && l == m->lc) {
+    const bool coop = m->coop && !t_no_coop;
+    if (!coop && m->tail_ok && l == m->lt) {
+        trace_mark("levels lt..L: one single-CTA kernel", st);
+        k_coop_vcycle<<<1, 512, 0, st>>>(m->tail_plan);
+        GB_LAUNCH_CHECK();
+        return 0;
+    }
+    if (coop && l == m->lc) {
         trace_mark("levels lc..L: one cooperative kernel", st);
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(m->coop_grid);
@@ -1140,23 +1153,13 @@ static int setup_direct(gb_mixed* m) {
 // coarsest solve.
 constexpr long long COOP_MAX_POINTS = 0;
 
-static int setup_coop(gb_mixed* m) {
-    const char* env = getenv("GPAW_B200_COOP_COARSE");
-    if (env && atoi(env) == 0) return 0;
-    const char* emax = getenv("GPAW_B200_COOP_MAX_POINTS");
-    const long long maxpts = emax ? atoll(emax) : COOP_MAX_POINTS;
-    int lc = m->L;
-    for (int l = 1; l <= m->L; l++)
-        if (m->ops[l]->ng() <= maxpts) {
-            lc = l;
-            break;
-        }
-    if (lc < 0 || m->L - lc + 1 > CV_MAX) return 0;
-    CoopPlan& P = m->coop_plan;
-    memset(&P, 0, sizeof P);
+// The levels lc..L of a cooperative-kernel plan; false when one of them
+// does not have the 7-point operator and order-2 transfers it assumes (or
+// the coarsest operator is not symmetric).
+static bool fill_coop_levels(gb_mixed* m, int lc, CoopPlan& P) {
     for (int l = lc; l <= m->L; l++) {
         const gb_operator* op = m->ops[l];
-        if (!(op->st.ncoefs == 7 && op->st.range == 1 && op->st.cfd)) return 0;
+        if (!(op->st.ncoefs == 7 && op->st.range == 1 && op->st.cfd)) return false;
         Seven s7{};
         for (int c = 0; c < 7; c++) {
             int ax = -1, dir = 0;
@@ -1190,7 +1193,7 @@ static int setup_coop(gb_mixed* m) {
             V.k2 = (float)c.k2;
             const gb_transformer* r = m->rst[l];
             const gb_transformer* i = m->itp[l];
-            if (r->k != 2 || i->k != 2) return 0;
+            if (r->k != 2 || i->k != 2) return false;
             for (int a = 0; a < 3; a++) {
                 V.rplo[a] = r->G.plo[a];
                 V.iplo[a] = i->G.plo[a];
@@ -1200,11 +1203,29 @@ static int setup_coop(gb_mixed* m) {
             V.iw = (float)i->G.w[0];
         } else {
             for (int a = 0; a < 3; a++)
-                if (s7.cp[a] != s7.cm[a]) return 0;
+                if (s7.cp[a] != s7.cm[a]) return false;
             P.dc0 = s7.c0;
             for (int a = 0; a < 3; a++) P.dca[a] = s7.cp[a];
         }
     }
+    return true;
+}
+
+static int setup_coop(gb_mixed* m) {
+    const char* env = getenv("GPAW_B200_COOP_COARSE");
+    if (env && atoi(env) == 0) return 0;
+    const char* emax = getenv("GPAW_B200_COOP_MAX_POINTS");
+    const long long maxpts = emax ? atoll(emax) : COOP_MAX_POINTS;
+    int lc = m->L;
+    for (int l = 1; l <= m->L; l++)
+        if (m->ops[l]->ng() <= maxpts) {
+            lc = l;
+            break;
+        }
+    if (lc < 0 || m->L - lc + 1 > CV_MAX) return 0;
+    CoopPlan& P = m->coop_plan;
+    memset(&P, 0, sizeof P);
+    if (!fill_coop_levels(m, lc, P)) return 0;
     // eigen tables of the coarsest level
     const GridBC& g = m->ops[m->L]->g;
     const long long ntab = (long long)g.n[0] * g.n[0] + (long long)g.n[1] * g.n[1] +
@@ -1238,6 +1259,40 @@ static int setup_coop(gb_mixed* m) {
     m->coop_grid = std::min(per_sm, want) * nsm;
     m->coop_ok = 1;
     m->coop = 1;
+    return 0;
+}
+
+// The single-CTA tail: levels from the first below 0 with at most
+// TAIL_MAX_POINTS points down to the coarsest, in one launch of the same
+// kernel with one block (its grid barrier is then a block barrier), so
+// that solves running side by side (a batch graph, the serving loop) each
+// take their coarse levels in one kernel instead of six a level.  Uses the
+// coarsest level's eigen tables, so it needs setup_coop to have built
+// them.  GPAW_B200_TAIL=0 keeps the per-level kernels.
+constexpr long long TAIL_MAX_POINTS = 4096;
+
+static int setup_tail(gb_mixed* m) {
+    const char* env = getenv("GPAW_B200_TAIL");
+    if ((env && atoi(env) == 0) || !m->coop_tab) return 0;
+    int lt = -1;
+    for (int l = 1; l <= m->L; l++)
+        if (m->ops[l]->ng() <= TAIL_MAX_POINTS) {
+            lt = l;
+            break;
+        }
+    if (lt < 0 || m->L - lt + 1 > CV_MAX) return 0;
+    CoopPlan& P = m->tail_plan;
+    memset(&P, 0, sizeof P);
+    if (!fill_coop_levels(m, lt, P)) return 0;
+    GB_CUDA_TRY(pool_malloc(&m->tail_bar, 2 * sizeof(unsigned)));
+    GB_CUDA_TRY(cudaMemset(m->tail_bar, 0, 2 * sizeof(unsigned)));
+    P.nl = m->L - lt + 1;
+    P.tab = m->coop_tab;
+    P.X = m->x;
+    P.Y = m->r;
+    P.bar = m->tail_bar;
+    m->lt = lt;
+    m->tail_ok = 1;
     return 0;
 }
 
@@ -1322,6 +1377,10 @@ extern "C" int gb_mixed_new(int nlevels, gb_operator* op64, gb_operator* const* 
         return fail(GB_ECUDA, "mixed: allocation: %s", cudaGetErrorString(ce));
     }
     if (int rc = setup_coop(m)) {
+        delete m;
+        return rc;
+    }
+    if (int rc = setup_tail(m)) {
         delete m;
         return rc;
     }
