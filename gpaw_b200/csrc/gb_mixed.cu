@@ -1268,15 +1268,20 @@ static int setup_coop(gb_mixed* m) {
 // that solves running side by side (a batch graph, the serving loop) each
 // take their coarse levels in one kernel instead of six a level.  Uses the
 // coarsest level's eigen tables, so it needs setup_coop to have built
-// them.  GPAW_B200_TAIL=0 keeps the per-level kernels.
-constexpr long long TAIL_MAX_POINTS = 4096;
+// them.  GPAW_B200_TAIL=0 keeps the per-level kernels;
+// GPAW_B200_TAIL_MAX_POINTS sets the size bound (512-grid batch: 2146,
+// 2158, 2176, 2183 and 2189 solves/s for bounds of 2048, 4096, 8192, 16384
+// and 40000 points).
+constexpr long long TAIL_MAX_POINTS = 16384;
 
 static int setup_tail(gb_mixed* m) {
     const char* env = getenv("GPAW_B200_TAIL");
     if ((env && atoi(env) == 0) || !m->coop_tab) return 0;
+    const char* emax = getenv("GPAW_B200_TAIL_MAX_POINTS");
+    const long long maxpts = emax ? atoll(emax) : TAIL_MAX_POINTS;
     int lt = -1;
     for (int l = 1; l <= m->L; l++)
-        if (m->ops[l]->ng() <= TAIL_MAX_POINTS) {
+        if (m->ops[l]->ng() <= maxpts) {
             lt = l;
             break;
         }
