@@ -1271,12 +1271,18 @@ static int setup_coop(gb_mixed* m) {
 // them.  GPAW_B200_TAIL=0 keeps the per-level kernels;
 // GPAW_B200_TAIL_MAX_POINTS sets the size bound (512-grid batch: 2146,
 // 2158, 2176, 2183 and 2189 solves/s for bounds of 2048, 4096, 8192, 16384
-// and 40000 points).
+// and 40000 points).  The coarsest level itself must have at most
+// TAIL_MAX_COARSEST points: the exact solve's dense passes on one SM cost
+// about n (n0 + n1 + n2) multiply-adds (on the 192^3 grid's 23^3 coarsest
+// level the single block took 10.0 ms a solve against 5.2 with the whole
+// GPU's cooperative kernel).
 constexpr long long TAIL_MAX_POINTS = 16384;
+constexpr long long TAIL_MAX_COARSEST = 4096;
 
 static int setup_tail(gb_mixed* m) {
     const char* env = getenv("GPAW_B200_TAIL");
     if ((env && atoi(env) == 0) || !m->coop_tab) return 0;
+    if (m->ops[m->L]->ng() > TAIL_MAX_COARSEST) return 0;
     const char* emax = getenv("GPAW_B200_TAIL_MAX_POINTS");
     const long long maxpts = emax ? atoll(emax) : TAIL_MAX_POINTS;
     int lt = -1;
