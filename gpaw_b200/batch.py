@@ -50,11 +50,11 @@ class PoissonBatch:
     def _build(self, nn, tol, maxiter, levels, precision):
         for gd in self.gds:
             if precision == 'mixed':
-                # per-pass coarse kernels: the batch's solves run side by
-                # side, which cooperative kernels (the whole GPU at once)
-                # would serialise
+                # the coarse levels in one single-block kernel a solve: the
+                # batch's solves run side by side, which cooperative kernels
+                # (the whole GPU at once) would serialise
                 ps = MixedPoissonSolver(nn=nn, tol=tol, maxiter=maxiter,
-                                        levels=levels, fused_coarse=False)
+                                        levels=levels, fused_coarse='tail')
             else:
                 ps = FDPoissonSolver(nn=nn, relax='J', eps=0.0,
                                      maxiter=maxiter)

@@ -702,7 +702,7 @@ struct gb_mixed {
     unsigned* coop_bar = nullptr;
     // the single-CTA form of the same kernel over levels lt..L (each at most
     // TAIL_MAX_POINTS points), for solves that run beside others
-    int tail_ok = 0, lt = 0;
+    int tail_ok = 0, lt = 0, tail = 0;
     CoopPlan tail_plan{};
     unsigned* tail_bar = nullptr;
     double last_tol = 0.0;
@@ -944,7 +944,7 @@ static thread_local bool t_no_coop = false;
 
 static int vcycle32(gb_mixed* m, int l, cudaStream_t st) {
     const bool coop = m->coop && !t_no_coop;
-    if (!coop && m->tail_ok && l == m->lt) {
+    if (!coop && m->tail && m->tail_ok && l == m->lt) {
         trace_mark("levels lt..L: one single-CTA kernel", st);
         k_coop_vcycle<<<1, 512, 0, st>>>(m->tail_plan);
         GB_LAUNCH_CHECK();
@@ -1401,14 +1401,16 @@ extern "C" int gb_mixed_new(int nlevels, gb_operator* op64, gb_operator* const* 
 
 extern "C" void gb_mixed_free(gb_mixed* m) { delete m; }
 
-extern "C" int gb_mixed_set_fused_coarse(gb_mixed* m, int on) {
+extern "C" int gb_mixed_set_fused_coarse(gb_mixed* m, int mode) {
     if (!m) return fail(GB_EINVAL, "mixed: NULL solver");
-    const int want = (on && m->coop_ok) ? 1 : 0;
-    if (want != m->coop && m->exec) {
+    const int coop = (mode == 1 && m->coop_ok) ? 1 : 0;
+    const int tail = (mode == 2 && m->tail_ok) ? 1 : 0;
+    if ((coop != m->coop || tail != m->tail) && m->exec) {
         cudaGraphExecDestroy(m->exec);   // captured with the other path
         m->exec = nullptr;
     }
-    m->coop = want;
+    m->coop = coop;
+    m->tail = tail;
     return 0;
 }
 

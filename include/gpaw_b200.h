@@ -312,12 +312,16 @@ GB_API int gb_mixed_new(int nlevels, gb_operator* op64, gb_operator* const* oper
                         gb_transformer* const* interpolators, const double* lam_max,
                         double lam_min_coarse, int coarse_degree, gb_mixed** out);
 GB_API void gb_mixed_free(gb_mixed* m);
-/* The coarsest level solved exactly (fast diagonalisation) in one
- * cooperative kernel (on = 1, the default where the level allows it), or by
- * the Chebyshev iteration (on = 0).  The two give slightly different FP32
- * corrections, each deterministic.  No counterpart in the reference.
- * Returns 0; `on` is ignored where the level does not allow the kernel. */
-GB_API int gb_mixed_set_fused_coarse(gb_mixed* m, int on);
+/* How the coarse levels are solved: mode 1 (the default where the levels
+ * allow it) the coarsest level exactly (fast diagonalisation) in one
+ * cooperative kernel over every SM; mode 0 per-level kernels and the
+ * Chebyshev iteration on the coarsest level; mode 2 the levels from the
+ * first with at most 16384 points down to a coarsest of at most 4096 points
+ * in one single-block kernel with the exact solve (for solves that run side
+ * by side, as in a batch graph), else as mode 0.  The modes give slightly
+ * different FP32 corrections, each deterministic.  No counterpart in the
+ * reference.  Returns 0; a mode the levels do not allow falls back to 0. */
+GB_API int gb_mixed_set_fused_coarse(gb_mixed* m, int mode);
 /* One V-cycle of the mixed-precision solver and the defects around it,
  * launched kernel by kernel instead of through the solver's graph:
  * phi <- phi + V32(rho - L phi).  For profilers and kernel traces (its

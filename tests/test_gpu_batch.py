@@ -45,7 +45,7 @@ def test_graph_batch_equals_streams_and_single(cuda):
     for p, q in zip(out['graph'][1], out['streams'][1]):
         assert np.array_equal(p, q)
     # one solver alone
-    ps = MixedPoissonSolver(tol=1e-10, maxiter=400, fused_coarse=False)
+    ps = MixedPoissonSolver(tol=1e-10, maxiter=400, fused_coarse='tail')
     ps.set_grid_descriptor(gds[2])
     phi = gds[2].zeros()
     ps.solve_neutral(phi, rhos[2])

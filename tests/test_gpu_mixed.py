@@ -23,7 +23,7 @@ def _case(N, pbc, seed):
     return gdo, rho
 
 
-@pytest.mark.parametrize('fused', [True, False])
+@pytest.mark.parametrize('fused', [True, False, 'tail'])
 @pytest.mark.parametrize('N,pbc', [((64, 64, 64), 0), ((48, 40, 56), 0),
                                    ((48, 48, 48), 1)])
 def test_mixed_reaches_1e10_and_matches_fp64(N, pbc, fused, cuda, capsys):
