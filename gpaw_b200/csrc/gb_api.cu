@@ -491,8 +491,26 @@ extern "C" int gb_fd_precond(gb_transformer* rest0, gb_transformer* rest1, gb_tr
     read_phases(dtype, phases, P);
     const int n = (int)nin;
     const double s4 = 4 * step, s16 = 16 * step;
+    // real grids of at least 2^18 points: the pass kernel (two points a
+    // thread from 16-byte shared-memory reads, the same arithmetic) unless
+    // GPAW_B200_PASS=0.  128 x 112^3 (C4): 1.64 -> 1.16 ms for the level-0
+    // step; on the 56^3 level it was slower (0.13 -> 0.16 ms).
+    static const bool pass = [] {
+        const char* e = getenv("GPAW_B200_PASS");
+        return !(e && atoi(e) == 0);
+    }();
     auto step_launch = [&](gb_operator* op, const void* d, const void* r, void* o, double sc,
                            int negate) {
+        if (pass && dtype == GB_F64 && op->tiled && d != o && r != o &&
+            op->ng() >= (1ll << 18)) {
+            const int rc = launch_pass_precond(op->g, op->cs, op->nn, (const double*)d,
+                                               (double*)o, (const double*)r, n, sc, negate, st);
+            if (rc == 0) {
+                GB_LAUNCH_CHECK();
+                return 0;
+            }
+            if (rc == -2) return fail(GB_ECUDA, "precond: could not raise the shared-memory limit");
+        }
         return op_sweep(op, EPI_PRECOND, d, o, r, n, dtype, P, 0, sc, negate, nullptr, st);
     };
     int rc;

@@ -127,6 +127,13 @@ int launch_pass(const GridBC& g, const CfdStencil& cs, int nn, const T* in, T* o
                 const T* aux2, double p0, double p1, double p2, double p3, double* acc64,
                 float* out32, double* partial, cudaStream_t st);
 
+// the preconditioner step out = +-(in - sc (A in - aux)) on a batch of nin
+// real grids, bit-identical to the plane-marching kernel's EPI_PRECOND
+// (gb_pass.cu); -1 when not supported
+int launch_pass_precond(const GridBC& g, const CfdStencil& cs, int nn, const double* in,
+                        double* out, const double* aux, int nin, double sc, int negate,
+                        cudaStream_t st);
+
 // caching allocator of the solver objects (gb_pool.cu): device memory and
 // pinned host memory; with the pool off these are cudaMalloc/cudaFree
 int dmalloc(void** p, size_t bytes);

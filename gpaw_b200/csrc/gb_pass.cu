@@ -49,7 +49,13 @@ struct PassCoef {
     T cm[3][3];
 };
 
-enum : int { PF_AUX = 1, PF_AUX2 = 2, PF_ACC64 = 4, PF_OUT32 = 8, PF_PARTIAL = 16 };
+enum : int {
+    PF_AUX = 1, PF_AUX2 = 2, PF_ACC64 = 4, PF_OUT32 = 8, PF_PARTIAL = 16,
+    // double only: the preconditioner step out = +-(u - sc (A u - aux)) with
+    // the stencil summed and every product and sum rounded as the
+    // reference's C loop does (bit-identical); p0 = sc, p1 != 0 negates
+    PF_EXACT_PRECOND = 32
+};
 
 template <class T>
 __device__ __forceinline__ void vload(T* dst, const T* src) {
@@ -111,6 +117,13 @@ k_pass(const T* __restrict__ u, T* __restrict__ out, const T* __restrict__ aux,
     const int x = x0 + VX * tx, y = y0 + ty;
     const int pa = blockIdx.y * chunk;
     const int pb = min(n0, pa + chunk);
+    {   // grid blockIdx.z of a batch
+        const long long off = (long long)blockIdx.z * n0 * ps;
+        u += off;
+        if (out) out += off;
+        if (aux) aux += off;
+        if (aux2) aux2 += off;
+    }
 
     // staging map: in-plane offset of each element this thread copies, or
     // -1 for a zero (outside a zero boundary); the boundary is fixed per CTA
@@ -222,6 +235,49 @@ k_pass(const T* __restrict__ u, T* __restrict__ out, const T* __restrict__ aux,
         for (int v = 0; v < 2 * NL + 1; v++)
             vload<T>(w + v * VX, cur + (ty + NN) * C + col0 + (v - NL) * VX);
         T acc[VX];
+        if constexpr ((F & PF_EXACT_PRECOND) != 0 && sizeof(T) == 8) {
+            // x = 0; x += v c in coefficient order: the centre, then per
+            // direction (columns, rows, planes) +1..+NN and -1..-NN, every
+            // product and sum rounded on its own
+#pragma unroll
+            for (int j = 0; j < VX; j++) acc[j] = __dadd_rn(0.0, __dmul_rn(w[NL * VX + j], c.c0));
+#pragma unroll
+            for (int d = 1; d <= NN; d++)
+#pragma unroll
+                for (int j = 0; j < VX; j++)
+                    acc[j] = __dadd_rn(acc[j], __dmul_rn(w[NL * VX + j + d], c.cp[0][d - 1]));
+#pragma unroll
+            for (int d = 1; d <= NN; d++)
+#pragma unroll
+                for (int j = 0; j < VX; j++)
+                    acc[j] = __dadd_rn(acc[j], __dmul_rn(w[NL * VX + j - d], c.cm[0][d - 1]));
+#pragma unroll
+            for (int d = 1; d <= NN; d++) {
+                T yv[VX];
+                vload<T>(yv, cur + (ty + NN + d) * C + col0);
+#pragma unroll
+                for (int j = 0; j < VX; j++)
+                    acc[j] = __dadd_rn(acc[j], __dmul_rn(yv[j], c.cp[1][d - 1]));
+            }
+#pragma unroll
+            for (int d = 1; d <= NN; d++) {
+                T yv[VX];
+                vload<T>(yv, cur + (ty + NN - d) * C + col0);
+#pragma unroll
+                for (int j = 0; j < VX; j++)
+                    acc[j] = __dadd_rn(acc[j], __dmul_rn(yv[j], c.cm[1][d - 1]));
+            }
+#pragma unroll
+            for (int d = 1; d <= NN; d++)
+#pragma unroll
+                for (int j = 0; j < VX; j++)
+                    acc[j] = __dadd_rn(acc[j], __dmul_rn(q[NN + d][j], c.cp[2][d - 1]));
+#pragma unroll
+            for (int d = 1; d <= NN; d++)
+#pragma unroll
+                for (int j = 0; j < VX; j++)
+                    acc[j] = __dadd_rn(acc[j], __dmul_rn(q[NN - d][j], c.cm[2][d - 1]));
+        } else {
 #pragma unroll
         for (int j = 0; j < VX; j++) acc[j] = c.c0 * w[NL * VX + j];
 #pragma unroll
@@ -241,11 +297,17 @@ k_pass(const T* __restrict__ u, T* __restrict__ out, const T* __restrict__ aux,
                 acc[j] = a;
             }
         }
+        }
         if (y < n1) {
             const long long row = (long long)p * ps + (long long)y * n2 + x;
 #pragma unroll
             for (int j = 0; j < VX; j++) {
                 if (x + j >= n2) break;
+                if constexpr ((F & PF_EXACT_PRECOND) != 0 && sizeof(T) == 8) {
+                    const T yv = __dsub_rn(w[NL * VX + j], __dmul_rn(__dsub_rn(acc[j], ca[j]), p0));
+                    out[row + j] = p1 != T(0) ? -yv : yv;
+                    continue;
+                }
                 T v = fma(p1, w[NL * VX + j], p2 * acc[j]);
                 if (F & PF_AUX) v = fma(p0, ca[j], v);
                 if (F & PF_AUX2) v = fma(p3, cb[j], v);
@@ -272,14 +334,15 @@ struct PassGeom {
 };
 
 template <class T>
-PassGeom pass_geom(const GridBC& g, int per_sm) {
+PassGeom pass_geom(const GridBC& g, int per_sm, int nin = 1) {
     constexpr int TX = 16 * PassVec<T>::N;
     PassGeom G;
     G.tiles_x = (g.n[2] + TX - 1) / TX;
     G.tiles_y = (g.n[1] + PT_ROWS - 1) / PT_ROWS;
     const int tiles = G.tiles_x * G.tiles_y;
-    // one wave: at most as many CTAs as fit on the GPU at once
-    int want = 148 * per_sm / tiles;
+    // one wave: at most as many CTAs as fit on the GPU at once (a batch of
+    // nin grids: whole grids a CTA column once the batch fills the GPU)
+    int want = 148 * per_sm / (tiles * std::max(1, nin));
     want = std::max(1, std::min(want, g.n[0]));
     G.chunk = (g.n[0] + want - 1) / want;
     G.nchunk = (g.n[0] + G.chunk - 1) / G.chunk;
@@ -299,7 +362,7 @@ bool pass_supported(const GridBC& g, const CfdStencil& cs, int nn) {
 template <class T, int NN, int F>
 int launch_pass_f(const GridBC& g, const PassCoef<T>& c, const T* in, T* out, const T* aux,
                   const T* aux2, double* acc64, float* out32, double* partial, T p0, T p1, T p2,
-                  T p3, cudaStream_t st) {
+                  T p3, cudaStream_t st, int nin = 1) {
     constexpr int VX = PassVec<T>::N;
     constexpr size_t smem = (size_t)PT_RING * (PT_ROWS + 2 * NN) * (16 * VX + 2 * PT_HX) * sizeof(T);
     static bool attr = false;
@@ -309,8 +372,8 @@ int launch_pass_f(const GridBC& g, const PassCoef<T>& c, const T* in, T* out, co
             return -2;
         attr = true;
     }
-    const PassGeom G = pass_geom<T>(g, pass_min_blocks<F>());
-    dim3 grid(G.tiles_x * G.tiles_y, G.nchunk);
+    const PassGeom G = pass_geom<T>(g, pass_min_blocks<F>(), nin);
+    dim3 grid(G.tiles_x * G.tiles_y, G.nchunk, nin);
     k_pass<T, NN, F><<<grid, 256, smem, st>>>(in, out, aux, aux2, acc64, out32, partial, g, c, p0,
                                              p1, p2, p3, G.chunk, G.tiles_x);
     return 0;
@@ -373,6 +436,27 @@ int launch_pass(const GridBC& g, const CfdStencil& cs, int nn, const T* in, T* o
         case 1: return launch_pass_nn<T, 1>(f, g, c, in, out, aux, aux2, acc64, out32, partial, a0, a1, a2, a3, st);
         case 2: return launch_pass_nn<T, 2>(f, g, c, in, out, aux, aux2, acc64, out32, partial, a0, a1, a2, a3, st);
         default: return launch_pass_nn<T, 3>(f, g, c, in, out, aux, aux2, acc64, out32, partial, a0, a1, a2, a3, st);
+    }
+}
+
+int launch_pass_precond(const GridBC& g, const CfdStencil& cs, int nn, const double* in,
+                        double* out, const double* aux, int nin, double sc, int negate,
+                        cudaStream_t st) {
+    if (!pass_supported<double>(g, cs, nn) || nin < 1 || nin > 65535 || !in || !out || !aux)
+        return -1;
+    PassCoef<double> c{};
+    c.c0 = cs.c0;
+    for (int k = 0; k < 3; k++)
+        for (int d = 0; d < nn; d++) {
+            c.cp[k][d] = cs.cp[k][d];
+            c.cm[k][d] = cs.cm[k][d];
+        }
+    constexpr int F = PF_AUX | PF_EXACT_PRECOND;
+    const double ng = negate ? 1.0 : 0.0;
+    switch (nn) {
+        case 1: return launch_pass_f<double, 1, F>(g, c, in, out, aux, nullptr, nullptr, nullptr, nullptr, sc, ng, 0.0, 0.0, st, nin);
+        case 2: return launch_pass_f<double, 2, F>(g, c, in, out, aux, nullptr, nullptr, nullptr, nullptr, sc, ng, 0.0, 0.0, st, nin);
+        default: return launch_pass_f<double, 3, F>(g, c, in, out, aux, nullptr, nullptr, nullptr, nullptr, sc, ng, 0.0, 0.0, st, nin);
     }
 }
 
