@@ -84,6 +84,7 @@ SIGNATURES = {
                                              C.POINTER(_p), _p]),
     'gb_mixed_batch_result': (C.c_int, [_p, C.POINTER(C.c_int), _dp]),
     'gb_mixed_solve_async': (C.c_int, [_p, _p, _p, C.c_double, C.c_int, _p]),
+    'gb_mixed_prepare': (C.c_int, [_p]),
     'gb_mixed_result': (C.c_int, [_p, C.POINTER(C.c_int), _dp]),
     'gb_poisson_solve_neutral_async': (C.c_int, [_p, _p, _p, C.c_double,
                                                  C.c_int, _p]),

@@ -1475,11 +1475,8 @@ static int build_mixed_graph(gb_mixed* m) {
     return 0;
 }
 
-extern "C" int gb_mixed_solve_async(gb_mixed* m, double* phi, const double* rho, double tol,
-                                    int maxiter, void* stream) {
-    if (!m || !phi || !rho) return fail(GB_EINVAL, "mixed solve: NULL argument");
-    if (maxiter < 1) return fail(GB_EINVAL, "mixed solve: maxiter must be >= 1");
-    cudaStream_t st = (cudaStream_t)stream;
+extern "C" int gb_mixed_prepare(gb_mixed* m) {
+    if (!m) return fail(GB_EINVAL, "mixed prepare: NULL solver");
     if (!m->exec) {
         int rc = build_mixed_graph(m);
         if (rc && m->coop) {
@@ -1491,6 +1488,15 @@ extern "C" int gb_mixed_solve_async(gb_mixed* m, double* phi, const double* rho,
         }
         if (rc) return rc;
     }
+    return 0;
+}
+
+extern "C" int gb_mixed_solve_async(gb_mixed* m, double* phi, const double* rho, double tol,
+                                    int maxiter, void* stream) {
+    if (!m || !phi || !rho) return fail(GB_EINVAL, "mixed solve: NULL argument");
+    if (maxiter < 1) return fail(GB_EINVAL, "mixed solve: maxiter must be >= 1");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (int rc = gb_mixed_prepare(m)) return rc;
     const long long n = m->op64->ng();
     const size_t bytes = (size_t)n * sizeof(double);
     GB_CUDA_TRY(cudaMemcpyAsync(m->rho0, rho, bytes, cudaMemcpyDeviceToDevice, st));

@@ -556,7 +556,14 @@ def _mixed_result(self):
     return niter.value
 
 
+def _mixed_prepare(self):
+    """Capture the solve now (synchronous; otherwise the first
+    solve_neutral_async does it)."""
+    check(self._h.lib.gb_mixed_prepare(self._h.h))
+
+
 MixedPoissonSolver.solve_neutral_async = _mixed_async
+MixedPoissonSolver.prepare = _mixed_prepare
 MixedPoissonSolver.result = _mixed_result
 
 

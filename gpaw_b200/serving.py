@@ -23,6 +23,9 @@ from __future__ import annotations
 import collections
 import dataclasses
 import gc
+import queue
+import sys
+import threading
 import time
 from math import pi
 
@@ -74,13 +77,12 @@ class Server:
     SPACING = 0.18 / 0.52917721   # Bohr
 
     def __init__(self, hbm_budget=8 << 30, nslots=8, tol=1e-10,
-                 device=None, grow=True, pool=True):
+                 device=None, grow=True, pool=True, background=True):
         self.device = torch.device(device if device is not None else 'cuda')
         self.budget = int(hbm_budget)
         self.tol = tol
         self.grow = grow
-        self.streams = [torch.cuda.Stream(device=self.device)
-                        for _ in range(nslots)]
+        self.streams = [self._make_stream() for _ in range(nslots)]
         self.free_slots = list(range(nslots))
         self.pools = collections.defaultdict(list)   # (kind, N) -> free objs
         self.resident = 0        # bytes held by pooled solvers/operators
@@ -99,6 +101,11 @@ class Server:
         # allocator while the loop runs (an evicted solver is idle), so a
         # new shape costs no driver allocation and no device-wide sync
         self.pool = pool
+        # with `background`, a solver for a new shape is built (and its
+        # solve captured) by a builder thread while the loop keeps serving;
+        # the request waits for it, later arrivals pass it
+        self.background = background
+        self.building = set()
 
     # -- resources ---------------------------------------------------------
     def _gd(self, N):
@@ -116,27 +123,70 @@ class Server:
         n = int(np.prod([x - 1 for x in N]))
         return 48 * n        # FP64 copies, FP32 levels, scratch (estimate)
 
-    def _take_solver(self, req):
+    def _make_stream(self):
+        return torch.cuda.Stream(device=self.device)
+
+    def _alloc_outputs(self, reqs, inputs):
+        return {r.rid: torch.empty(tuple(inputs[r.rid].shape),
+                                   dtype=torch.float64).pin_memory()
+                for r in reqs}
+
+    def _sync(self):
+        torch.cuda.synchronize()
+
+    def _new_solver(self, N):
         from .poisson import MixedPoissonSolver
+        # per-level coarse kernels: concurrent solves run side by side,
+        # where a cooperative coarse kernel (one block on every SM) would
+        # wait for the whole GPU
+        ps = MixedPoissonSolver(nn=3, tol=self.tol, levels=4,
+                                fused_coarse=False)
+        ps.set_grid_descriptor(self._gd(N))
+        return ps
+
+    def _take_solver(self, req):
         pool = self.pools[('poisson', req.N)]
         if pool:
             ps = pool.pop()
             self.lru.pop(id(ps), None)
             return ps, 0
-        # per-pass coarse kernels: concurrent solves run side by side, where
-        # a cooperative coarse kernel (one block on every SM) would wait for
-        # the whole GPU
-        ps = MixedPoissonSolver(nn=3, tol=self.tol, levels=4,
-                                fused_coarse=False)
-        ps.set_grid_descriptor(self._gd(req.N))
+        ps = self._new_solver(req.N)
         self.built += 1
         return ps, self.solver_bytes(req.N)
 
-    def _evict_for(self, need):
+    def _builder(self, todo, done, device_index):
+        """Builder thread: a solver per shape taken from `todo`, its solve
+        captured, handed back through `done` (None ends the thread).  Any
+        failure goes back through `done` too, so that the loop raises it
+        instead of waiting for a build that will not come."""
+        try:
+            if device_index is not None:
+                torch.cuda.set_device(device_index)
+        except BaseException as exc:
+            done.put((None, exc))
+            return
+        while True:
+            N = todo.get()
+            if N is None:
+                return
+            try:
+                ps = self._new_solver(N)
+                ps.prepare()
+                done.put((N, ps))
+            except BaseException as exc:      # re-raised by the loop
+                done.put((N, exc))
+
+    def _evict_for(self, need, keep=None):
         """Free idle resident solvers, least recently used first, until
-        `need` more bytes fit the budget; False when they cannot."""
-        while self.resident + self.in_use + need > self.budget and self.lru:
-            _, (N, ps) = self.lru.popitem(last=False)
+        `need` more bytes fit the budget; False when they cannot.  Solvers
+        of shape `keep` (the one the request is about to take) stay."""
+        for key in list(self.lru):
+            if self.resident + self.in_use + need <= self.budget:
+                break
+            N, ps = self.lru[key]
+            if N == keep:
+                continue
+            del self.lru[key]
             self.pools[('poisson', N)].remove(ps)
             self.resident -= self.solver_bytes(N)
             self.evicted += 1
@@ -239,13 +289,16 @@ class Server:
     def _finish(self, job, now):
         req = job['req']
         req.done = now
-        req.result = job['out'].numpy()     # the request's own buffer
+        req.result = self._result_of(job)
         if job['solver'] is not None:
             req.niter = job['solver'].result()
             self.pools[('poisson', req.N)].append(job['solver'])
             self.lru[id(job['solver'])] = (req.N, job['solver'])
         self.in_use -= self.request_bytes(req)
         self.free_slots.append(job['slot'])
+
+    def _result_of(self, job):
+        return job['out'].numpy()     # the request's own pinned buffer
 
     # -- the loop --------------------------------------------------------------
     def run(self, requests, inputs=None):
@@ -254,31 +307,76 @@ class Server:
         reqs = sorted(requests, key=lambda r: r.arrival)
         if inputs is None:
             inputs = {r.rid: self.host_input(r) for r in reqs}
-        outputs = {r.rid: torch.empty(tuple(inputs[r.rid].shape),
-                                      dtype=torch.float64).pin_memory()
-                   for r in reqs}
+        outputs = self._alloc_outputs(reqs, inputs)
         self.reserve({r.N for r in reqs})
         pending = list(reqs)
         active = []
-        torch.cuda.synchronize()
+        self._sync()
         # no garbage-collector pauses inside the loop (it allocates little:
         # per-request bookkeeping only)
         gc_was_on = gc.isenabled()
         gc.collect()
         gc.disable()
+        self._todo = self._done = None
+        thread = None
+        switch = sys.getswitchinterval()
+        if self.background and self.grow:
+            self._todo, self._done = queue.Queue(), queue.Queue()
+            index = None
+            if self.device.type == 'cuda':
+                index = (self.device.index if self.device.index is not None
+                         else torch.cuda.current_device())
+            thread = threading.Thread(target=self._builder,
+                                      args=(self._todo, self._done, index),
+                                      daemon=True)
+            thread.start()
+            # the loop and the builder share the interpreter: short slices
+            # keep the loop's polling prompt while the builder runs
+            sys.setswitchinterval(1e-4)
         try:
             with self._pooled():
                 return self._serve(pending, active, inputs, outputs)
         finally:
+            if thread is not None:
+                self._todo.put(None)
+                thread.join()
+                sys.setswitchinterval(switch)
+                self._install_built()
+                # solvers built but not used in this run become evictable
+                for (kind, N), pool in self.pools.items():
+                    for ps in pool:
+                        if id(ps) not in self.lru:
+                            self.lru[id(ps)] = (N, ps)
             if gc_was_on:
                 gc.enable()
+
+    def _install_built(self):
+        """Solvers finished by the builder thread join the pools; True when
+        any did."""
+        got = False
+        while self._done is not None:
+            try:
+                N, ps = self._done.get_nowait()
+            except queue.Empty:
+                break
+            self.building.discard(N)
+            if isinstance(ps, BaseException):
+                raise ps
+            self.built += 1
+            # not in the eviction order until a request has used it: the
+            # request that asked for it is still waiting (otherwise two
+            # waiting requests could evict each other's new solvers
+            # before either runs)
+            self.pools[('poisson', N)].append(ps)
+            got = True
+        return got
 
     def _serve(self, pending, active, inputs, outputs):
         reqs = list(pending)
         t0 = time.perf_counter()
         while pending or active:
             now = time.perf_counter() - t0
-            progressed = False
+            progressed = self._install_built()
             for job in list(active):
                 if job['event'].query():
                     active.remove(job)
@@ -294,11 +392,27 @@ class Server:
                 if req.kind == 'poisson' and not pooled and not self.grow:
                     i += 1
                     continue
+                if req.kind == 'poisson' and not pooled and \
+                        self._todo is not None:
+                    # built by the builder thread; the request waits for it
+                    if req.N not in self.building:
+                        need = self.solver_bytes(req.N)
+                        # over the budget only when nothing else could
+                        # ever free memory (as the synchronous path does)
+                        if self.resident + self.in_use + need <= \
+                                self.budget or self._evict_for(need) or \
+                                not (active or self.building):
+                            self.building.add(req.N)
+                            self.resident += need
+                            self._todo.put(req.N)
+                    i += 1
+                    continue
                 need = self.request_bytes(req)
                 if req.kind == 'poisson' and not pooled:
                     need += self.solver_bytes(req.N)
+                keep = req.N if (req.kind == 'poisson' and pooled) else None
                 if self.resident + self.in_use + need > self.budget and \
-                        not self._evict_for(need) and active:
+                        not self._evict_for(need, keep) and active:
                     break      # wait for memory to free up
                 del pending[i]
                 slot = self.free_slots.pop()

@@ -348,6 +348,12 @@ GB_API int gb_poisson_result(gb_poisson* p, int* niter, double* error);
 GB_API int gb_mixed_solve_async(gb_mixed* m, double* phi, const double* rho, double tol,
                                 int maxiter, void* stream);
 GB_API int gb_mixed_result(gb_mixed* m, int* niter, double* rel_residual);
+/* Build the solver's captured solve now (what the first gb_mixed_solve_async
+ * otherwise does): one uncaptured pass on the solver's own stream, then the
+ * capture; synchronous.  Lets a host thread prepare solvers while another
+ * thread enqueues solves of other solvers.  No counterpart in the
+ * reference. */
+GB_API int gb_mixed_prepare(gb_mixed* m);
 
 /* Many mixed-precision solves as one CUDA graph (no reference counterpart):
  * one branch per solver (distinct solvers, grids of any sizes), each the

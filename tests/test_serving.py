@@ -97,3 +97,123 @@ def test_anisotropic_stream_with_eviction(cuda):
         one = Request(r.rid, r.kind, r.N, 0.0, r.seed)
         alone = srv.run([one], {r.rid: inputs[r.rid]})[0]
         assert np.array_equal(mixed[r.rid], alone.result), r
+
+
+# ------------------------------------------------ the loop's scheduling (CPU)
+class _Done:
+    """An event that completes a fixed time after its launch."""
+
+    def __init__(self, seconds):
+        import time
+        self.t = time.perf_counter() + seconds
+
+    def query(self):
+        import time
+        return time.perf_counter() >= self.t
+
+
+class _Solver:
+    def __init__(self, N):
+        self.N = N
+        self.prepared = False
+
+    def prepare(self):
+        import time
+        time.sleep(0.0005)
+        self.prepared = True
+
+    def result(self):
+        return 3
+
+
+def _host_server(**kw):
+    """The serving loop with its device work replaced by timers: requests
+    run for 0.1-0.3 ms, solvers are dummies that the builder thread
+    prepares; the admission, budget, eviction and build logic is the
+    product's."""
+    import contextlib
+    from gpaw_b200.serving import Server
+
+    class HostServer(Server):
+        def _make_stream(self):
+            return None
+
+        def _alloc_outputs(self, reqs, inputs):
+            return {r.rid: None for r in reqs}
+
+        def _sync(self):
+            pass
+
+        def reserve(self, shapes):
+            pass
+
+        def _pooled(self):
+            return contextlib.nullcontext()
+
+        def _new_solver(self, N):
+            return _Solver(N)
+
+        def _launch(self, req, host_in, host_out, slot):
+            solver, extra = None, 0
+            if req.kind == 'poisson':
+                solver, extra = self._take_solver(req)
+                self.resident += extra
+                assert solver.prepared or not self.background
+            return {'req': req, 'slot': slot, 'solver': solver,
+                    'event': _Done(1e-4 * (1 + req.rid % 3)), 'out': None,
+                    'extra': extra}
+
+        def _result_of(self, job):
+            return job['req'].rid
+
+    return HostServer(**kw)
+
+
+@pytest.mark.parametrize('background', [True, False])
+def test_builds_and_evictions_always_finish(background):
+    """Anisotropic streams under budgets from a few solvers to many: every
+    request completes (no request waits forever for a solver that others
+    keep evicting), solvers are built, and with a small budget evicted."""
+    import threading
+    for seed, budget in [(1, 12 << 20), (2, 24 << 20), (3, 256 << 20)]:
+        reqs = make_requests(rate=20000.0, count=80, seed=seed, smin=24,
+                             smax=56, poisson_fraction=0.8,
+                             anisotropic=True)
+        srv = _host_server(hbm_budget=budget, nslots=4, grow=True,
+                           background=background, pool=False, device='cpu')
+        t = threading.Thread(target=srv.run,
+                             args=(reqs, {r.rid: None for r in reqs}),
+                             daemon=True)
+        t.start()
+        t.join(timeout=60)
+        assert not t.is_alive(), (seed, budget, 'the loop did not finish')
+        assert all(r.done > 0 and r.result == r.rid for r in reqs)
+        assert srv.built > 0
+        if budget == 12 << 20:
+            assert srv.evicted > 0
+        assert not srv.building
+
+
+def test_failed_build_is_raised_not_waited_for():
+    """A solver build that fails in the builder thread ends the loop with
+    that error instead of leaving its request waiting."""
+    import threading
+    reqs = make_requests(rate=20000.0, count=20, seed=4, smin=24, smax=48,
+                         poisson_fraction=1.0, anisotropic=True)
+    srv = _host_server(hbm_budget=1 << 30, nslots=4, grow=True,
+                       background=True, pool=False, device='cpu')
+
+    def broken(N):
+        raise MemoryError('no room for a solver')
+    srv._new_solver = broken
+    err = []
+
+    def go():
+        try:
+            srv.run(reqs, {r.rid: None for r in reqs})
+        except MemoryError as e:
+            err.append(e)
+    t = threading.Thread(target=go, daemon=True)
+    t.start()
+    t.join(timeout=30)
+    assert not t.is_alive() and err
