@@ -437,9 +437,15 @@ def c1_apply(dev, reps=50):
     st = torch.cuda.current_stream()
     for _ in range(5):
         op.apply(a, b)
+    # The host takes longer to issue a launch through the Python API than
+    # the kernel runs, so a short device-side wait is queued in front of
+    # each timed region: the events then bracket the kernel's device time
+    # instead of the host's launch latency.
+    hold = int(2e-4 * 1.9e9)           # about 0.2 ms of SM cycles
     cold = []
     for _ in range(reps):
         flush.fill_(1)
+        torch.cuda._sleep(hold)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(st)
@@ -447,6 +453,7 @@ def c1_apply(dev, reps=50):
         e1.record(st)
         e1.synchronize()
         cold.append(e0.elapsed_time(e1) / 1e3)
+    torch.cuda._sleep(hold * 20)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(st)
@@ -462,7 +469,9 @@ def c1_apply(dev, reps=50):
             'us': t * 1e6, 'gbs': nbytes / t / 1e9,
             'frac': nbytes / t / 1e9 / peak,
             'us_l2_resident': hot * 1e6, 'gbs_l2_resident': nbytes / hot / 1e9,
-            'how': 'median of %d launches, L2 flushed before each' % reps}
+            'how': 'median of %d launches, L2 flushed before each, a device '
+                   'wait queued ahead so that the events time the kernel, '
+                   'not the host launch' % reps}
 
 
 def c1_cpu(phi_gpu, n_gpu):
